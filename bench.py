@@ -1,0 +1,288 @@
+#!/usr/bin/env python
+"""Benchmark of the split HLLD sweep: FP64 ideal-MHD cell-updates/s at 256^3.
+
+Workload (one "step" = one iteration of PIERNIK's main loop, i.e. time_step +
+fluid_update = two time steps of X,Y,Z then Z,Y,X sweeps, each sweep two RK2
+stages): decaying ideal-MHD turbulence on one periodic 256^3 block, HLLD
+fluxes with GLM divergence cleaning, moncen limiter, CFL 0.5, FP64, seeded
+synthetic initial state (density 1 + 1% white noise, velocity from Fourier
+modes |k| = 1..4 with amplitude k^-2 at rms Mach 1, B = (0.2,0,0) plus 10%
+divergence-free modes, psi = 0).  A cell-update is one cell advanced by one
+dt, so one step is 2 * 256^3 cell-updates.
+
+Arms:
+  default            the CUDA library through Simulation.run (state resident in HBM)
+  --impl reference   the reference's CPU algorithm (the oracle port in oracle/,
+                     the Fortran reference cannot be compiled here) on all host
+                     threads, each step a bounded 128^3 sample of the workload
+
+Multi-GPU (torchrun): every rank advances its own 256^3 replica (weak scaling);
+timing is the max over ranks of CUDA-event time on the library's stream.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 MHD cell-updates/s at 256^3 on 1 B200; adjoint-gradient cost ÷ forward step"
+UNIT = "cell-updates/s"
+NVAR = 9                         # dn, mx, my, mz, en, Bx, By, Bz, psi
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_config(n):
+    return {"workload": f"3D ideal-MHD decaying turbulence, one periodic {n}^3 block, HLLD + GLM, moncen, "
+                        f"RK2, CFL 0.5, FP64", "n": n, "nvar": NVAR, "riemann": "hlld", "limiter": "moncen",
+            "cfl": 0.5, "step": "time_step + fluid_update (2 dt, 6 sweeps)",
+            "l2": "state %.2f GB > 126 MB L2, no flush needed" % (NVAR * 8 * (n + 8) ** 3 / 1e9)}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.proc = None
+        self.path = None
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 7 and parts[0].isdigit():
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [int(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][1]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_sample(n, seed):
+    """Time the oracle (reference algorithm on the CPU) on one step of the
+    workload recipe at n^3; returns (cell-updates/s, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from piernik_b200 import problems
+    setup, u, b, psi = problems.mhd_turbulence(n=n, seed=seed)
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    t0 = time.perf_counter()
+    ob.run(1)
+    el = time.perf_counter() - t0
+    return 2.0 * n ** 3 / el, el, oracle.get_threads()
+
+
+def reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from piernik_b200 import problems
+    ns = 128 if args.n >= 128 else args.n
+    setup, u, b, psi = problems.mhd_turbulence(n=ns, seed=args.seed)
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    ob.run(args.warmup)
+    t0 = time.perf_counter()
+    ob.run(args.steps)
+    el = time.perf_counter() - t0
+    value = 2.0 * ns ** 3 * args.steps / el
+    threads = oracle.get_threads()
+    sample = (f"{args.steps} steps of the workload recipe at {ns}^3 (oracle/pk_oracle.c, OpenMP over pencils, "
+              f"{threads} threads); the Fortran reference has no compiler here")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": workload_config(args.n), "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def our_arm(args):
+    import numpy as np
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from piernik_b200 import build, problems
+    from piernik_b200._lib import PK_LAYOUT_FORTRAN
+    from piernik_b200.sim import Simulation
+    build.build()
+    n = args.n
+    setup, u, b, psi = problems.mhd_turbulence(n=n, seed=args.seed + rank)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    stream = torch.cuda.ExternalStream(sim.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also compiles nothing: the library is prebuilt)
+    sim.run(args.warmup)
+    barrier()
+    clocks = Clocks(local)
+    sim.profile(True)
+    launches0, _, _ = sim.profile_read()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    launches1, nsweep, sweep_ms = sim.profile_read()
+    sim.profile(False)
+    ck = clocks.stop()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    cell_updates = 2.0 * n ** 3 * args.steps * world
+    value = cell_updates / (ms / 1e3)
+
+    # roofline of the fused sweep kernel (algorithmic bytes: read + write 9 planes of n^3)
+    hbm, src = peaks()
+    bytes_per_launch = 2.0 * NVAR * 8 * n ** 3
+    launch_ms = sweep_ms / max(nsweep, 1)
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        traffic = tj["bytes_per_cell"] * n ** 3
+    except Exception:
+        traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "kernel": "k_sweep_fused<MHD> (one sweep direction, both RK2 stages)",
+                "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms, "peak_source": src}
+
+    # end to end through the C ABI with host buffers in the reference's layout
+    e2e = None
+    if not args.no_e2e:
+        pu = torch.empty(u.shape, dtype=torch.float64).pin_memory().numpy()
+        pb = torch.empty(b.shape, dtype=torch.float64).pin_memory().numpy()
+        pp = torch.empty(psi.shape, dtype=torch.float64).pin_memory().numpy()
+        pu[...] = u
+        pb[...] = b
+        pp[...] = psi
+        st0 = sim.time_state
+        barrier()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            sim.upload(pu, pb, pp, layout=PK_LAYOUT_FORTRAN)
+            sim.run(1)
+            sim.download(layout=PK_LAYOUT_FORTRAN, out=(pu, pb, pp))
+        e3.record(stream)
+        e3.synchronize()
+        barrier()
+        ms2 = max_over_ranks(e2.elapsed_time(e3))
+        nbytes = (pu.nbytes + pb.nbytes + pp.nbytes)
+        e2e = {"value": cell_updates / (ms2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": ms2 / args.steps,
+               "path": "pk_upload(Fortran layout, pinned) + pk_run(1) + pk_download per step"}
+        sim.time_state = st0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cn = n
+        v, el, thr = cpu_sample(cn, args.seed)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"1 step of the workload at {cn}^3 ({2 * cn ** 3} cell-updates, {el:.1f} s) with "
+                         f"oracle/pk_oracle.c on {thr} OpenMP threads"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": dict(workload_config(n), parallelism=f"replicas{world}"),
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+               "gpu_launches": launches1 - launches0, "clocks": ck,
+               "adjoint_cost_ratio": None}
+        print(json.dumps(out), flush=True)
+    sim.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

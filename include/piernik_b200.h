@@ -1,0 +1,166 @@
+/*
+ * piernik_b200.h -- C ABI of the B200 split-sweep library (libpiernik_b200.so).
+ *
+ * The library replaces PIERNIK's RIEMANN_SPLIT fluid-update hot path: the
+ * per-block Riemann solve (solve_cg_riemann), the directional sweep with its
+ * RK2 stages and guardcell refresh (sweep, update_boundaries), the CFL time
+ * step reduction (time_step / timestep_fluid), the GLM psi speed and damping
+ * (update_chspeed, glmdamping) and the XYZ/ZYX pair of time steps
+ * (fluid_update_full).  All arithmetic is IEEE binary64.
+ *
+ * Conventions: every entry point returns PK_OK (0) or a negative PK_E* code;
+ * pk_last_error() gives a one-line message.  No entry point aborts the
+ * process and no kernel traps: numerical trouble (negative density or
+ * internal energy) is reported through pk_status().  One CUDA stream per
+ * handle; a handle must not be used from two host threads at once.
+ *
+ * Array layouts accepted by pk_upload/pk_download:
+ *   PK_LAYOUT_FORTRAN  the reference's named arrays with guard cells:
+ *                      u(nvar, i, j, k), b(3, i, j, k), psi(i, j, k),
+ *                      column-major, i over lhn(x), j over lhn(y), k over lhn(z)
+ *                      (src/grid/grid_container_base.F90 lhn extents)
+ *   PK_LAYOUT_SOA      u[v][k][j][i], b[d][k][j][i], psi[k][j][i], same extents
+ * Component order of u is the reference's flind order: for each fluid
+ * (ionized, neutral, dust) [dn, mx, my, mz, (en)] (fluids/fluidtypes.F90:279-330).
+ */
+#ifndef PIERNIK_B200_H
+#define PIERNIK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PK_ABI_VERSION 1
+
+enum {
+    PK_OK = 0,
+    PK_E_ARG = -1,         /* invalid argument / configuration */
+    PK_E_CUDA = -2,        /* CUDA runtime error (message in pk_last_error) */
+    PK_E_NOMEM = -3,       /* device allocation failed */
+    PK_E_UNSUPPORTED = -4, /* configuration not provided by this build */
+    PK_E_STATE = -5,       /* call out of order (e.g. no block registered) */
+    PK_E_DTMIN = -6        /* dt < dt_min: the reference calls write_crashed */
+};
+
+enum { PK_FLUID_ION = 0, PK_FLUID_NEU = 1, PK_FLUID_DST = 2 };
+enum { PK_LIM_VANLEER = 0, PK_LIM_MINMOD = 1, PK_LIM_MONCEN = 2, PK_LIM_SUPERBEE = 3 };
+enum { PK_BND_PER = 0, PK_BND_OUT = 1, PK_BND_REF = 2 };
+enum { PK_LAYOUT_FORTRAN = 0, PK_LAYOUT_SOA = 1 };
+enum { PK_ST_DN_NEGATIVE = 1, PK_ST_EI_NEGATIVE = 2 };
+/* RK stage identifiers, numerically equal to the reference's istep enumerators
+ * (src/base/constants.F90:230-238) */
+enum { PK_EULER = 10000, PK_RK2_1 = 10001, PK_RK2_2 = 10002 };
+
+/* NUMERICAL_SETUP / FLUID_* / END_CONTROL parameters the path reads
+ * (src/base/global.F90:118-120 and defaults :196-260). */
+typedef struct pk_config {
+    int32_t nfluids;            /* 1..3, in flind order */
+    int32_t fluid_kind[3];      /* PK_FLUID_* */
+    double gamma[3];            /* FLUID_*: gamma (dust: ignored, -1 used) */
+    int32_t magnetic;           /* MAGNETIC with divB_0 = 'HDC' (B + psi) */
+    int32_t limiter;            /* NUMERICAL_SETUP: limiter   (PK_LIM_*) */
+    int32_t limiter_b;          /* NUMERICAL_SETUP: limiter_b (PK_LIM_*) */
+    int32_t use_smalld, use_smallei, disallow_negatives;
+    double smalld, smallei;
+    double cfl, cfl_glm, glm_alpha;
+    int32_t integration_order;  /* 1 or 2 */
+    int32_t nb;                 /* guard cells (dom%nb) */
+    double dt_initial, dt_max_grow, dt_min, dt_max;
+    double tend;                /* END_CONTROL: tend */
+    int32_t skip_sweep[3];
+} pk_config;
+
+/* Time-integration state the reference keeps in module global (global.F90). */
+typedef struct pk_time_state {
+    double t, dt, dt_old, c_all, chspeed;
+    int32_t nstep;
+} pk_time_state;
+
+typedef struct pk_ctx* pk_handle;
+
+/* Fill cfg with the reference defaults (global.F90:196-260, ionized gamma 5/3). */
+void pk_config_default(pk_config* cfg);
+
+/* Create / destroy a library instance on the current CUDA device. */
+int pk_create(const pk_config* cfg, pk_handle* out);
+int pk_destroy(pk_handle h);
+const char* pk_last_error(pk_handle h);
+int pk_abi_version(void);
+
+/* Register a block (grid_container): n interior cells, cell sizes dl, external
+ * boundary types per direction and side.  Single-block runs with periodic
+ * boundaries are swept by the fused two-stage kernel. */
+int pk_block_add(pk_handle h, const int32_t n[3], const double dl[3], const int32_t bnd[6], int32_t* id_out);
+
+/* Copy a block's u (all fluids), b and psi between host and device.
+ * b/psi are ignored when the run is not magnetised.  Guard cells come back as
+ * the last stage left them; after fused sweeps (which read periodic images and
+ * never store guards) they are refreshed before the copy. */
+int pk_upload(pk_handle h, int32_t id, const double* u, const double* b, const double* psi, int32_t layout);
+int pk_download(pk_handle h, int32_t id, double* u, double* b, double* psi, int32_t layout);
+
+/* solve_cg(cg, ddim, istep) for one block and one RK stage on the device
+ * copy: replaces the procedure pointer target solve_cg_riemann
+ * (src/scheme/sweeps.F90:138-153,245; Riemann_Solver/solve_cg_riemann.F90:68-107).
+ * ddim is 1..3 (xdim..zdim), istep is PK_EULER / PK_RK2_1 / PK_RK2_2.
+ * Guard cells are not refreshed (the caller's update_boundaries does that,
+ * or pk_fill_guards). */
+int pk_solve_cg(pk_handle h, int32_t id, int32_t ddim, int32_t istep, double dt, double chspeed);
+
+/* update_boundaries for all blocks (sweeps.F90:66-107, single level). */
+int pk_fill_guards(pk_handle h);
+
+/* sweep(cdim): all RK stages over all blocks with guardcell refresh
+ * (src/scheme/sweeps.F90:114-279); cdim is 1..3. */
+int pk_sweep(pk_handle h, int32_t cdim, double dt, double chspeed);
+
+/* glmdamping: psi *= fac on every block (Riemann_Solver/hdc.F90:289-349). */
+int pk_glm_damp(pk_handle h, double fac);
+
+/* timestep_fluid over all fluids and blocks, before clamps
+ * (src/base/timestep.F90:431-495): dt = cfl*min_d(dl_d/max c_d), c_all. */
+int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out);
+
+/* time_step(dt, flind, .true.) with the sanity clamps (timestep.F90:112-240);
+ * updates the handle's pk_time_state.  Returns PK_E_DTMIN when dt < dt_min. */
+int pk_time_step(pk_handle h, double* dt_out);
+
+/* fluid_update_full (src/scheme/fluidupdate.F90:99-136): update_chspeed,
+ * X->Y->Z sweeps, glmdamping, Z->Y->X sweeps, glmdamping; t += 2 dt. */
+int pk_fluid_update(pk_handle h);
+
+/* nsteps iterations of the reference main loop body (time_step +
+ * fluid_update, piernik.F90:125-213 without I/O); stops at t >= tend. */
+int pk_run(pk_handle h, int32_t nsteps);
+
+int pk_get_time_state(pk_handle h, pk_time_state* st);
+int pk_set_time_state(pk_handle h, const pk_time_state* st);
+
+/* OR of PK_ST_* bits raised since the last call; clears them. */
+int pk_status(pk_handle h, uint32_t* flags);
+
+/* Wait for all work of the handle's stream. */
+int pk_sync(pk_handle h);
+
+/* Tile shape of the fused sweep for direction d (0..2): P pencils per CTA,
+ * L output cells per pencil (the CTA also computes a 4-cell halo each side).
+ * Used by the autotuner; 0 keeps the built-in choice. */
+int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length);
+
+/* CUDA stream of the handle (cudaStream_t), for callers that interleave work. */
+void* pk_stream(pk_handle h);
+
+/* Kernel accounting.  With profiling on, every sweep kernel is bracketed by a
+ * pair of CUDA events on the handle's stream.  pk_profile_read waits for the
+ * stream and returns the number of this library's kernel launches since the
+ * handle was created, the number of sweep launches timed since the last read
+ * and their summed device time in milliseconds. */
+int pk_profile_enable(pk_handle h, int32_t on);
+int pk_profile_read(pk_handle h, int64_t* launches, int64_t* sweep_launches, double* sweep_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

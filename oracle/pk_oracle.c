@@ -1,0 +1,961 @@
+/*
+ * pk_oracle.c -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * A CPU restatement of PIERNIK's RIEMANN_SPLIT fluid update, written to be the
+ * checker for the CUDA library (see pk_oracle.h for the parity status: the
+ * restatement is UNPINNED because the Fortran reference cannot be built here
+ * and holds no golden vectors for this path).
+ *
+ * Every routine cites the reference routine it restates, by path within the
+ * PIERNIK source tree.  Floating-point expressions keep the reference's
+ * evaluation order (Fortran evaluates a*b*c as (a*b)*c, a+b-c as (a+b)-c,
+ * sum() left to right, x**2 as x*x).  Build with -O2 -ffp-contract=off and no
+ * -ffast-math so that no operation is fused or reassociated, which is also
+ * what gfortran -O2 emits for x86-64 (no FMA without -march).
+ */
+#include "pk_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Fortran intrinsics                                                  */
+/* ------------------------------------------------------------------ */
+
+/* SPACING(x) for real(8): 2**max(exponent(x)-53, -1022); TINY at zero
+ * (Fortran 2008 13.7.157; used at src/scheme/Riemann_Solver/hlld.F90:325,364,373). */
+static double f_spacing(double x)
+{
+    uint64_t bits;
+    memcpy(&bits, &x, sizeof bits);
+    int be = (int)((bits >> 52) & 0x7ff);
+    if (be == 0x7ff) return NAN;
+    if (be >= 53) {
+        uint64_t r = (uint64_t)(be - 52) << 52;
+        double d;
+        memcpy(&d, &r, sizeof d);
+        return d;
+    }
+    return DBL_MIN; /* tiny(1.d0) */
+}
+
+/* SIGN(one, x): +-1 with the sign bit of x (gfortran honours -0.0). */
+static inline double f_sign1(double x) { return copysign(1.0, x); }
+static inline double f_min(double a, double b) { return (b < a) ? b : a; }
+static inline double f_max(double a, double b) { return (b > a) ? b : a; }
+
+/* constants.F90:99-104 */
+static const double SMALL = (double)FLT_MIN;   /* tiny(real(1.0,4)) */
+
+/* ------------------------------------------------------------------ */
+/* Fluid index layout (fluids/fluidtypes.F90:279-339, fluidindex.F90)  */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    int nv, nfl;
+    int beg[O_MAXFL], idn[O_MAXFL], imx[O_MAXFL], imy[O_MAXFL], imz[O_MAXFL], ien[O_MAXFL];
+    int has_en[O_MAXFL], magn[O_MAXFL], kind[O_MAXFL];
+    double gam[O_MAXFL], gam_1[O_MAXFL];
+} o_lay;
+
+static void o_layout(const o_cfg *cfg, o_lay *L)
+{
+    int all = 0;
+    L->nfl = cfg->nfluids;
+    for (int f = 0; f < cfg->nfluids; ++f) {
+        int k = cfg->kind[f];
+        L->kind[f] = k;
+        L->beg[f] = all;
+        L->idn[f] = all;
+        L->imx[f] = all + 1;
+        L->imy[f] = all + 2;
+        L->imz[f] = all + 3;
+        all += 4;
+        L->has_en[f] = (k != O_DST);
+        L->ien[f] = L->has_en[f] ? all++ : -1;
+        L->magn[f] = (k == O_ION) && cfg->magnetic;
+        /* dust registers gamma = -1 (fluids/dust/initdust.F90:70) */
+        L->gam[f] = (k == O_DST) ? -1.0 : cfg->gamma[f];
+        L->gam_1[f] = L->gam[f] - 1.0;
+    }
+    L->nv = all;
+}
+
+int o_nvar(const o_cfg *cfg)
+{
+    o_lay L;
+    o_layout(cfg, &L);
+    return L.nv;
+}
+
+void o_extents(const o_block *blk, int ext[3], int g[3])
+{
+    for (int d = 0; d < 3; ++d) {
+        g[d] = (blk->n[d] > 1) ? blk->nb : 0;
+        ext[d] = blk->n[d] + 2 * g[d];
+    }
+}
+
+/* swept position of original component k (x,y,z) of momentum or B:
+ * iarr_swp (fluidtypes.F90:318-320) and iarr_mag_swp (fluidindex.F90:190-192) */
+static const int PERM3[3][3] = { {0, 1, 2}, {1, 0, 2}, {2, 1, 0} };
+
+/* ------------------------------------------------------------------ */
+/* Reconstruction: utoq + linear + limiters                            */
+/* ------------------------------------------------------------------ */
+
+/* interpolations.F90:69-106 (utoq).  u, q are column-major (n, nv); b (n, >=3) swept. */
+static void o_utoq(const o_lay *L, int n, const double *u, const double *b, double *q)
+{
+    for (int f = 0; f < L->nfl; ++f) {
+        const double *dn = u + (size_t)L->idn[f] * n;
+        const double *mx = u + (size_t)L->imx[f] * n;
+        const double *my = u + (size_t)L->imy[f] * n;
+        const double *mz = u + (size_t)L->imz[f] * n;
+        for (int i = 0; i < n; ++i) {
+            q[(size_t)L->idn[f] * n + i] = dn[i];
+            q[(size_t)L->imx[f] * n + i] = mx[i] / dn[i];
+            q[(size_t)L->imy[f] * n + i] = my[i] / dn[i];
+            q[(size_t)L->imz[f] * n + i] = mz[i] / dn[i];
+        }
+        if (L->has_en[f]) {
+            const double *en = u + (size_t)L->ien[f] * n;
+            double *qe = q + (size_t)L->ien[f] * n;
+            for (int i = 0; i < n; ++i) {
+                /* ekin = emag(mx,my,mz)/dn, emag = half*sq_sum3 (base/func.F90:54-88) */
+                double ek = (0.5 * ((mx[i] * mx[i] + my[i] * my[i]) + mz[i] * mz[i])) / dn[i];
+                qe[i] = L->gam_1[f] * (en[i] - ek);
+            }
+            if (L->magn[f]) {
+                const double *bx = b, *by = b + n, *bz = b + 2 * (size_t)n;
+                for (int i = 0; i < n; ++i) {
+                    double bb = (bx[i] * bx[i] + by[i] * by[i]) + bz[i] * bz[i];
+                    qe[i] = qe[i] - (0.5 * L->gam_1[f]) * bb;
+                }
+            }
+        }
+    }
+}
+
+/* fluxlimiters.F90:109-216 applied to one column of length n; dq gets the slope */
+static void o_limiter(int kind, int n, const double *u, double *dq)
+{
+    if (kind == O_LIM_VANLEER) {            /* fluxlimiters.F90:109-136 */
+        dq[0] = 0.0;
+        dq[n - 1] = 0.0;
+        double dlft = u[1] - u[0];
+        for (int i = 1; i < n - 1; ++i) {
+            double drgt = u[i + 1] - u[i];
+            double dcen = dlft * drgt;
+            if (dcen > 0.0) dq[i] = (2.0 * dcen) / (dlft + drgt);
+            else dq[i] = 0.0;
+            dlft = drgt;
+        }
+        return;
+    }
+    for (int i = 0; i < n; ++i) {
+        /* dlft(2:n) = u(2:n)-u(1:n-1); dlft(1) = dlft(2); drgt(1:n-1) = dlft(2:n); drgt(n) = drgt(n-1) */
+        double dl, dr;
+        if (i == 0) { dl = u[1] - u[0]; dr = dl; }
+        else if (i == n - 1) { dl = u[n - 1] - u[n - 2]; dr = dl; }
+        else { dl = u[i] - u[i - 1]; dr = u[i + 1] - u[i]; }
+        double s = f_sign1(dl) + f_sign1(dr);
+        if (kind == O_LIM_MINMOD) {          /* fluxlimiters.F90:142-162 */
+            dq[i] = (s * f_min(fabs(dl), fabs(dr))) * 0.5;
+        } else if (kind == O_LIM_MONCEN) {   /* fluxlimiters.F90:169-189 */
+            double m = f_min(f_min(2.0 * fabs(dl), 2.0 * fabs(dr)), 0.5 * fabs(dl + dr));
+            dq[i] = (s * m) * 0.5;
+        } else {                             /* superbee, fluxlimiters.F90:194-216 */
+            double m = (fabs(dl) > fabs(dr)) ? f_min(fabs(dl), fabs(2.0 * dr))
+                                             : f_min(fabs(2.0 * dl), fabs(dr));
+            dq[i] = (s * 0.5) * m;
+        }
+    }
+}
+
+/* interpolations.F90:170-204 (linear) for ncol columns; ql, qr are (n-1, ncol) */
+static void o_linear(int kind, int n, int ncol, const double *q, double *ql, double *qr, double *dq)
+{
+    for (int c = 0; c < ncol; ++c) {
+        const double *qc = q + (size_t)c * n;
+        o_limiter(kind, n, qc, dq);
+        for (int i = 0; i < n; ++i) dq[i] = 0.5 * dq[i];          /* dq_interp = half * f_limiter(q) */
+        double *l = ql + (size_t)c * (n - 1), *r = qr + (size_t)c * (n - 1);
+        for (int i = 0; i < n - 1; ++i) {
+            l[i] = qc[i] + dq[i];
+            r[i] = qc[i + 1] - dq[i + 1];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Riemann solvers                                                     */
+/* ------------------------------------------------------------------ */
+
+/* One interface of riemann_hlld (hlld.F90:235-603).  ul/ur: primitive states
+ * [dn, vx, vy, vz, (p)] (swept); bl/br: swept B (zeros for unmagnetised fluids);
+ * f: fluid fluxes; bf: transverse B fluxes (y, z). */
+static void o_hlld_iface(int has_energy, double gamma, const double *ul, const double *ur,
+                         const double *bl, const double *br, double *f, double *bf)
+{
+    enum { idn = 0, imx = 1, imy = 2, imz = 3, ien = 4 };
+    double fl[5], fr[5], usl[5], usr[5], u2l[5], u2r[5];
+    double vsl[3], vsr[3], v2[3], bsl[3], bsr[3], b2[3], bclf[3] = {0, 0, 0}, bcrf[3] = {0, 0, 0};
+    double prl, prr, c_fastm, enl = DBL_MAX, enr = DBL_MAX, ue = 0.0;
+    int nc = has_energy ? 5 : 4;
+
+    double magprl = 0.5 * ((bl[0] * bl[0] + bl[1] * bl[1]) + bl[2] * bl[2]);   /* :239-240 */
+    double magprr = 0.5 * ((br[0] * br[0] + br[1] * br[1]) + br[2] * br[2]);
+
+    if (gamma < 0.0) {                                                           /* :245-249 dust */
+        prl = 0.0;
+        prr = 0.0;
+        c_fastm = 0.0;
+    } else {
+        prl = ul[ien] + magprl;                                                   /* :258-259 */
+        prr = ur[ien] + magprr;
+        double bbl = (bl[0] * bl[0] + bl[1] * bl[1]) + bl[2] * bl[2];
+        double bbr = (br[0] * br[0] + br[1] * br[1]) + br[2] * br[2];
+        enl = ((ul[ien] / (gamma - 1.0)) + ((0.5 * ul[idn]) * ((ul[imx] * ul[imx] + ul[imy] * ul[imy]) + ul[imz] * ul[imz]))) + (0.5 * bbl);
+        enr = ((ur[ien] / (gamma - 1.0)) + ((0.5 * ur[idn]) * ((ur[imx] * ur[imx] + ur[imy] * ur[imy]) + ur[imz] * ur[imz]))) + (0.5 * bbr);
+        double gampr_l = gamma * ul[ien];
+        double gampr_r = gamma * ur[ien];
+        double al = gampr_l + bbl, ar = gampr_r + bbr;                            /* :272-274 */
+        double cl = (al + sqrt(al * al - ((4.0 * gampr_l) * (bl[0] * bl[0])))) / ul[idn];
+        double cr = (ar + sqrt(ar * ar - ((4.0 * gampr_r) * (br[0] * br[0])))) / ur[idn];
+        c_fastm = sqrt(0.5 * f_max(cl, cr));
+    }
+
+    double sl = f_min(ul[imx], ur[imx]) - c_fastm;                               /* :291-292 */
+    double sr = f_max(ul[imx], ur[imx]) + c_fastm;
+
+    fl[idn] = ul[idn] * ul[imx];                                                  /* :296-300 */
+    fl[imx] = ((ul[idn] * (ul[imx] * ul[imx])) + prl) - (bl[0] * bl[0]);
+    fl[imy] = ((ul[idn] * ul[imy]) * ul[imx]) - (bl[0] * bl[1]);
+    fl[imz] = ((ul[idn] * ul[imz]) * ul[imx]) - (bl[0] * bl[2]);
+    if (has_energy) fl[ien] = ((enl + prl) * ul[imx]) - (bl[0] * ((ul[imx] * bl[0] + ul[imy] * bl[1]) + ul[imz] * bl[2]));
+    bclf[1] = (bl[1] * ul[imx]) - (bl[0] * ul[imy]);
+    bclf[2] = (bl[2] * ul[imx]) - (bl[0] * ul[imz]);
+
+    fr[idn] = ur[idn] * ur[imx];                                                  /* :304-308 */
+    fr[imx] = ((ur[idn] * (ur[imx] * ur[imx])) + prr) - (br[0] * br[0]);
+    fr[imy] = ((ur[idn] * ur[imy]) * ur[imx]) - (br[0] * br[1]);
+    fr[imz] = ((ur[idn] * ur[imz]) * ur[imx]) - (br[0] * br[2]);
+    if (has_energy) fr[ien] = ((enr + prr) * ur[imx]) - (br[0] * ((ur[imx] * br[0] + ur[imy] * br[1]) + ur[imz] * br[2]));
+    bcrf[1] = (br[1] * ur[imx]) - (br[0] * ur[imy]);
+    bcrf[2] = (br[2] * ur[imx]) - (br[0] * ur[imz]);
+
+    if (sl >= 0.0) {                                                              /* :312-319 */
+        for (int c = 0; c < nc; ++c) f[c] = fl[c];
+        bf[0] = bclf[1];
+        bf[1] = bclf[2];
+        return;
+    }
+    if (sr <= 0.0) {
+        for (int c = 0; c < nc; ++c) f[c] = fr[c];
+        bf[0] = bcrf[1];
+        bf[1] = bcrf[2];
+        return;
+    }
+
+    double sm;                                                                    /* :323-330 */
+    {
+        double auxr = (sr - ur[imx]) * ur[idn];
+        double auxl = (sl - ul[imx]) * ul[idn];
+        if (fabs(auxr - auxl) < f_spacing(auxr + auxl)) sm = (sl + sr) / 2.0;
+        else sm = ((auxr * ur[imx] - prr) - (auxl * ul[imx] - prl)) / (auxr - auxl);
+    }
+
+    double slsm = sl - sm, srsm = sr - sm;                                        /* :334-340 */
+    double slvxl = sl - ul[imx], srvxr = sr - ur[imx];
+    double srmsl = sr - sl;
+    double dn_l = ul[idn] * slvxl, dn_r = ur[idn] * srvxr;                        /* :344-347 */
+    double b_lr = bl[0] * br[0];
+    double b_lrgam = b_lr / gamma;
+    double prt_star = 0.5 * ((prl + dn_l * (sm - ul[imx])) + (prr + dn_r * (sm - ur[imx])));
+
+    vsl[0] = sm;                                                                  /* :354-358 */
+    vsr[0] = sm;
+    bsl[0] = bl[0];
+    bsr[0] = br[0];
+
+    double coeff_1 = dn_l * slsm - b_lr;                                          /* :362-369 */
+    if (has_energy) ue = ul[ien];
+    if ((fabs(coeff_1) > f_spacing(b_lr)) && b_lrgam <= ue) {
+        for (int c = 1; c < 3; ++c) bsl[c] = (bl[c] * (dn_l * slvxl - b_lr)) / coeff_1;
+    } else {
+        for (int c = 1; c < 3; ++c) bsl[c] = ((sr * br[c] - sl * bl[c]) - (bcrf[c] - bclf[c])) / srmsl;
+    }
+    coeff_1 = dn_r * srsm - b_lr;                                                 /* :371-378 */
+    if (has_energy) ue = ur[ien];
+    if ((fabs(coeff_1) > f_spacing(b_lr)) && b_lrgam <= ue) {
+        for (int c = 1; c < 3; ++c) bsr[c] = (br[c] * (dn_r * srvxr - b_lr)) / coeff_1;
+    } else {
+        for (int c = 1; c < 3; ++c) bsr[c] = ((sr * br[c] - sl * bl[c]) - (bcrf[c] - bclf[c])) / srmsl;
+    }
+
+    for (int c = 1; c < 3; ++c) {                                                 /* :381-382 */
+        vsl[c] = ul[imx + c] + ((bl[0] / dn_l) * (bl[c] - bsl[c]));
+        vsr[c] = ur[imx + c] + ((br[0] / dn_r) * (br[c] - bsr[c]));
+    }
+
+    double vb_l = (ul[imx] * bl[0] + ul[imy] * bl[1]) + ul[imz] * bl[2];          /* :386-389 */
+    double vb_r = (ur[imx] * br[0] + ur[imy] * br[1]) + ur[imz] * br[2];
+    double vb_starl = (vsl[0] * bsl[0] + vsl[1] * bsl[1]) + vsl[2] * bsl[2];
+    double vb_starr = (vsr[0] * bsr[0] + vsr[1] * bsr[1]) + vsr[2] * bsr[2];
+
+    usl[idn] = dn_l / slsm;                                                       /* :393-399 */
+    for (int c = 0; c < 3; ++c) usl[imx + c] = usl[idn] * vsl[c];
+    usr[idn] = dn_r / srsm;
+    for (int c = 0; c < 3; ++c) usr[imx + c] = usr[idn] * vsr[c];
+
+    if (has_energy) {                                                             /* :403-404 */
+        usl[ien] = ((((slvxl * enl) - (prl * ul[imx])) + (prt_star * sm)) + (bl[0] * (vb_l - vb_starl))) / slsm;
+        usr[ien] = ((((srvxr * enr) - (prr * ur[imx])) + (prt_star * sm)) + (br[0] * (vb_r - vb_starr))) / srsm;
+    }
+
+    double ucl[5], ucr[5];                      /* [ ul(idn), ul(idn)*ul(imx:imz), enl ] */
+    ucl[0] = ul[idn];
+    ucr[0] = ur[idn];
+    for (int c = 0; c < 3; ++c) {
+        ucl[1 + c] = ul[idn] * ul[imx + c];
+        ucr[1 + c] = ur[idn] * ur[imx + c];
+    }
+    ucl[4] = enl;
+    ucr[4] = enr;
+
+    if (fabs(bl[0]) > 0.0) {                                                      /* :410 */
+        double dn_lsqt = sqrt(usl[idn]);                                          /* :414-418 */
+        double dn_rsqt = sqrt(usr[idn]);
+        double alfven_l = sm - fabs(bl[0]) / dn_lsqt;
+        double alfven_r = sm + fabs(br[0]) / dn_rsqt;
+
+        if (alfven_l > 0.0) {                                                     /* :422-434 */
+            for (int c = 0; c < nc; ++c) f[c] = fl[c] + sl * (usl[c] - ucl[c]);
+            for (int c = 1; c < 3; ++c) bf[c - 1] = bclf[c] + sl * (bsl[c] - bl[c]);
+        } else if (alfven_r < 0.0) {                                              /* :436-448 */
+            for (int c = 0; c < nc; ++c) f[c] = fr[c] + sr * (usr[c] - ucr[c]);
+            for (int c = 1; c < 3; ++c) bf[c - 1] = bcrf[c] + sr * (bsr[c] - br[c]);
+        } else {
+            double b_sig = (bl[0] >= 0.0) ? 1.0 : -1.0;                           /* :452-456 */
+            double add_dnsq = dn_lsqt + dn_rsqt;                                  /* :460-461 */
+            double mul_dnsq = dn_lsqt * dn_rsqt;
+            v2[0] = sm;                                                           /* :465-470 */
+            for (int c = 1; c < 3; ++c)
+                v2[c] = ((dn_lsqt * vsl[c] + dn_rsqt * vsr[c]) + b_sig * (bsr[c] - bsl[c])) / add_dnsq;
+            b2[0] = 0.5 * (bl[0] + br[0]);
+            for (int c = 1; c < 3; ++c)
+                b2[c] = ((dn_lsqt * bsr[c] + dn_rsqt * bsl[c]) + (b_sig * mul_dnsq) * (vsr[c] - vsl[c])) / add_dnsq;
+            double vb_2star = (v2[0] * b2[0] + v2[1] * b2[1]) + v2[2] * b2[2];   /* :474 */
+
+            if (sm >= 0.0) {                                                      /* :478-485 */
+                u2l[idn] = usl[idn];
+                for (int c = 0; c < 3; ++c) u2l[imx + c] = usl[idn] * v2[c];
+                if (has_energy) u2l[ien] = usl[ien] - (b_sig * dn_lsqt) * (vb_starl - vb_2star);
+            }
+            if (sm <= 0.0) {                                                      /* :487-494 */
+                u2r[idn] = usr[idn];
+                for (int c = 0; c < 3; ++c) u2r[imx + c] = usr[idn] * v2[c];
+                if (has_energy) u2r[ien] = usr[ien] + (b_sig * dn_rsqt) * (vb_starr - vb_2star);
+            }
+
+            if (sm > 0.0) {                                                       /* :496-508 */
+                for (int c = 0; c < nc; ++c)
+                    f[c] = ((fl[c] + alfven_l * u2l[c]) - (alfven_l - sl) * usl[c]) - sl * ucl[c];
+                for (int c = 1; c < 3; ++c)
+                    bf[c - 1] = ((bclf[c] + alfven_l * b2[c]) - (alfven_l - sl) * bsl[c]) - sl * bl[c];
+            } else if (sm < 0.0) {                                                /* :510-522 */
+                for (int c = 0; c < nc; ++c)
+                    f[c] = ((fr[c] + alfven_r * u2r[c]) - (alfven_r - sr) * usr[c]) - sr * ucr[c];
+                for (int c = 1; c < 3; ++c)
+                    bf[c - 1] = ((bcrf[c] + alfven_r * b2[c]) - (alfven_r - sr) * bsr[c]) - sr * br[c];
+            } else {                                                              /* :524-544 */
+                for (int c = 0; c < nc; ++c)
+                    f[c] = 0.5 * ((((fl[c] + alfven_l * u2l[c]) - (alfven_l - sl) * usl[c]) - sl * ucl[c]) +
+                                  (((fr[c] + alfven_r * u2r[c]) - (alfven_r - sr) * usr[c]) - sr * ucr[c]));
+                for (int c = 1; c < 3; ++c)
+                    bf[c - 1] = 0.5 * ((((bclf[c] + alfven_l * b2[c]) - (alfven_l - sl) * bsl[c]) - sl * bl[c]) +
+                                       (((bcrf[c] + alfven_r * b2[c]) - (alfven_r - sr) * bsr[c]) - sr * br[c]));
+            }
+        }
+    } else {                                                                      /* :548-599 B_x = 0 */
+        if (sm > 0.0) {
+            for (int c = 0; c < nc; ++c) f[c] = fl[c] + sl * (usl[c] - ucl[c]);
+            for (int c = 1; c < 3; ++c) bf[c - 1] = bclf[c] + sl * (bsl[c] - bl[c]);
+        } else if (sm < 0.0) {
+            for (int c = 0; c < nc; ++c) f[c] = fr[c] + sr * (usr[c] - ucr[c]);
+            for (int c = 1; c < 3; ++c) bf[c - 1] = bcrf[c] + sr * (bsr[c] - br[c]);
+        } else {
+            for (int c = 0; c < nc; ++c)
+                f[c] = 0.5 * (((fl[c] + sl * (usl[c] - ucl[c])) + fr[c]) + sr * (usr[c] - ucr[c]));
+            for (int c = 1; c < 3; ++c)
+                bf[c - 1] = 0.5 * (((bclf[c] + sl * (bsl[c] - bl[c])) + bcrf[c]) + sr * (bsr[c] - br[c]));
+        }
+    }
+}
+
+/* One interface of riemann_hlld_u, the B-free HLLC (hlld.F90:665-835) */
+static void o_hllc_iface(int has_energy, double gamma, const double *ul, const double *ur, double *f)
+{
+    enum { idn = 0, imx = 1, imy = 2, imz = 3, ien = 4 };
+    double fl[5], fr[5], usl[5], usr[5], vsl[3], vsr[3];
+    double prl, prr, c_fastm, enl = DBL_MAX, enr = DBL_MAX;
+    int nc = has_energy ? 5 : 4;
+
+    if (gamma < 0.0) {                                                            /* :673-677 */
+        prl = 0.0;
+        prr = 0.0;
+        c_fastm = 0.0;
+    } else {
+        prl = ul[ien];                                                            /* :689-703 */
+        prr = ur[ien];
+        enl = (ul[ien] / (gamma - 1.0)) + ((0.5 * ul[idn]) * ((ul[imx] * ul[imx] + ul[imy] * ul[imy]) + ul[imz] * ul[imz]));
+        enr = (ur[ien] / (gamma - 1.0)) + ((0.5 * ur[idn]) * ((ur[imx] * ur[imx] + ur[imy] * ur[imy]) + ur[imz] * ur[imz]));
+        double gampr_l = gamma * ul[ien];
+        double gampr_r = gamma * ur[ien];
+        c_fastm = sqrt(f_max(gampr_l / ul[idn], gampr_r / ur[idn]));
+    }
+
+    double sl = f_min(ul[imx], ur[imx]) - c_fastm;                               /* :719-720 */
+    double sr = f_max(ul[imx], ur[imx]) + c_fastm;
+
+    fl[idn] = ul[idn] * ul[imx];                                                  /* :724-734 */
+    fl[imx] = (ul[idn] * (ul[imx] * ul[imx])) + prl;
+    fl[imy] = (ul[idn] * ul[imy]) * ul[imx];
+    fl[imz] = (ul[idn] * ul[imz]) * ul[imx];
+    if (has_energy) fl[ien] = (enl + prl) * ul[imx];
+    fr[idn] = ur[idn] * ur[imx];
+    fr[imx] = (ur[idn] * (ur[imx] * ur[imx])) + prr;
+    fr[imy] = (ur[idn] * ur[imy]) * ur[imx];
+    fr[imz] = (ur[idn] * ur[imz]) * ur[imx];
+    if (has_energy) fr[ien] = (enr + prr) * ur[imx];
+
+    if (sl >= 0.0) {                                                              /* :738-743 */
+        for (int c = 0; c < nc; ++c) f[c] = fl[c];
+        return;
+    }
+    if (sr <= 0.0) {
+        for (int c = 0; c < nc; ++c) f[c] = fr[c];
+        return;
+    }
+
+    double sm;                                                                    /* :747-754 */
+    {
+        double auxr = (sr - ur[imx]) * ur[idn];
+        double auxl = (sl - ul[imx]) * ul[idn];
+        if (fabs(auxr - auxl) < f_spacing(auxr + auxl)) sm = (sl + sr) / 2.0;
+        else sm = ((auxr * ur[imx] - prr) - (auxl * ul[imx] - prl)) / (auxr - auxl);
+    }
+    double slvxl = sl - ul[imx], srvxr = sr - ur[imx];                            /* :758-764 */
+    double dn_l = ul[idn] * slvxl, dn_r = ur[idn] * srvxr;
+    double prt_star = 0.5 * ((prl + dn_l * (sm - ul[imx])) + (prr + dn_r * (sm - ur[imx])));
+    double slsm = 0.0, srsm = 0.0;
+
+    if (sm >= 0.0) {                                                              /* :771-784 */
+        slsm = sl - sm;
+        vsl[0] = sm;
+        vsl[1] = ul[imy];
+        vsl[2] = ul[imz];
+        usl[idn] = dn_l / slsm;
+        for (int c = 0; c < 3; ++c) usl[imx + c] = usl[idn] * vsl[c];
+        if (has_energy) usl[ien] = (((slvxl * enl) - (prl * ul[imx])) + (prt_star * sm)) / slsm;
+    }
+    if (sm <= 0.0) {                                                              /* :786-796 */
+        srsm = sr - sm;
+        vsr[0] = sm;
+        vsr[1] = ur[imy];
+        vsr[2] = ur[imz];
+        usr[idn] = dn_r / srsm;
+        for (int c = 0; c < 3; ++c) usr[imx + c] = usr[idn] * vsr[c];
+        if (has_energy) usr[ien] = (((srvxr * enr) - (prr * ur[imx])) + (prt_star * sm)) / srsm;
+    }
+    (void)slsm;
+    (void)srsm;
+
+    double ucl[5], ucr[5];
+    ucl[0] = ul[idn];
+    ucr[0] = ur[idn];
+    for (int c = 0; c < 3; ++c) {
+        ucl[1 + c] = ul[idn] * ul[imx + c];
+        ucr[1 + c] = ur[idn] * ur[imx + c];
+    }
+    ucl[4] = enl;
+    ucr[4] = enr;
+
+    if (sm > 0.0) {                                                               /* :798-806 */
+        for (int c = 0; c < nc; ++c) f[c] = fl[c] + sl * (usl[c] - ucl[c]);
+    } else if (sm < 0.0) {                                                        /* :808-815 */
+        for (int c = 0; c < nc; ++c) f[c] = fr[c] + sr * (usr[c] - ucr[c]);
+    } else {                                                                      /* :817-829 */
+        for (int c = 0; c < nc; ++c)
+            f[c] = 0.5 * (((fl[c] + sl * (usl[c] - ucl[c])) + fr[c]) + sr * (usr[c] - ucr[c]));
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Pencil solve: solve / solve_u + internal_sources + care_for_positives */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    int cap;
+    double *u0, *u1, *b0, *b1, *q, *ql, *qr, *bl, *br, *flx, *mflx, *dq;
+} o_work;
+
+static void o_work_init(o_work *w, int n, int nv)
+{
+    size_t nn = (size_t)n;
+    w->cap = n;
+    w->u0 = malloc(nn * nv * sizeof(double));
+    w->u1 = malloc(nn * nv * sizeof(double));
+    w->b0 = malloc(nn * 4 * sizeof(double));
+    w->b1 = malloc(nn * 4 * sizeof(double));
+    w->q = malloc(nn * nv * sizeof(double));
+    w->ql = malloc(nn * nv * sizeof(double));
+    w->qr = malloc(nn * nv * sizeof(double));
+    w->bl = malloc(nn * 4 * sizeof(double));
+    w->br = malloc(nn * 4 * sizeof(double));
+    w->flx = malloc(nn * nv * sizeof(double));
+    w->mflx = malloc(nn * 4 * sizeof(double));
+    w->dq = malloc(nn * sizeof(double));
+}
+
+static void o_work_free(o_work *w)
+{
+    free(w->u0); free(w->u1); free(w->b0); free(w->b1); free(w->q); free(w->ql);
+    free(w->qr); free(w->bl); free(w->br); free(w->flx); free(w->mflx); free(w->dq);
+}
+
+/* solve (solve_cg_riemann.F90:318-376) or solve_u (:378-414) on one pencil of
+ * length n: u1/b1 enter as the current state and leave as the Euler update of
+ * u0/b0 by dtodx.  No f/c flux substitution (single-level blocks). */
+static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx, double ch, o_work *w)
+{
+    const int nv = L->nv, m = n - 1;
+    const int mag = cfg->magnetic;
+
+    /* interpol (interpolations.F90:112-132) */
+    o_utoq(L, n, w->u1, mag ? w->b1 : NULL, w->q);
+    o_linear(cfg->limiter, n, nv, w->q, w->ql, w->qr, w->dq);
+    if (mag) o_linear(cfg->limiter_b, n, 4, w->b1, w->bl, w->br, w->dq);
+
+    /* riemann_wrap / riemann_wrap_u (hlld.F90:62-155) */
+    if (mag) {
+        /* GLM fluxes of Bx and psi for the magnetised fluid (hlld.F90:227-233) */
+        const double *bxl = w->bl, *bxr = w->br, *psl = w->bl + 3 * (size_t)m, *psr = w->br + 3 * (size_t)m;
+        double *fbx = w->mflx, *fps = w->mflx + 3 * (size_t)m;
+        for (int i = 0; i < m; ++i) {
+            fps[i] = ((ch * ch) * 0.5) * ((bxr[i] + bxl[i]) - (psr[i] - psl[i]) / ch);
+            fbx[i] = 0.5 * ((psr[i] + psl[i]) - ch * (bxr[i] - bxl[i]));
+        }
+    }
+    for (int f = 0; f < L->nfl; ++f) {
+        int nc = L->has_en[f] ? 5 : 4;
+        for (int i = 0; i < m; ++i) {
+            double ul[5], ur[5], fx[5];
+            for (int c = 0; c < nc; ++c) {
+                ul[c] = w->ql[(size_t)(L->beg[f] + c) * m + i];
+                ur[c] = w->qr[(size_t)(L->beg[f] + c) * m + i];
+            }
+            if (mag) {
+                double blv[3] = {0, 0, 0}, brv[3] = {0, 0, 0}, bf[2];
+                if (L->magn[f])
+                    for (int c = 0; c < 3; ++c) {
+                        blv[c] = w->bl[(size_t)c * m + i];
+                        brv[c] = w->br[(size_t)c * m + i];
+                    }
+                o_hlld_iface(L->has_en[f], L->gam[f], ul, ur, blv, brv, fx, bf);
+                if (L->magn[f]) {
+                    w->mflx[(size_t)1 * m + i] = bf[0];
+                    w->mflx[(size_t)2 * m + i] = bf[1];
+                }
+            } else {
+                o_hllc_iface(L->has_en[f], L->gam[f], ul, ur, fx);
+            }
+            for (int c = 0; c < nc; ++c) w->flx[(size_t)(L->beg[f] + c) * m + i] = fx[c];
+        }
+    }
+
+    /* u1(2:nx-1,:) = u0(2:nx-1,:) + dtodx * (flx(:nx-2,:) - flx(2:,:))  (:365-374) */
+    for (int c = 0; c < nv; ++c) {
+        const double *u0c = w->u0 + (size_t)c * n, *fc = w->flx + (size_t)c * m;
+        double *u1c = w->u1 + (size_t)c * n;
+        for (int i = 1; i < n - 1; ++i) u1c[i] = u0c[i] + dtodx * (fc[i - 1] - fc[i]);
+    }
+    if (mag)
+        for (int c = 0; c < 4; ++c) {
+            const double *b0c = w->b0 + (size_t)c * n, *fc = w->mflx + (size_t)c * m;
+            double *b1c = w->b1 + (size_t)c * n;
+            for (int i = 1; i < n - 1; ++i) b1c[i] = b0c[i] + dtodx * (fc[i - 1] - fc[i]);
+        }
+}
+
+/* internal_sources (fluids/sources.F90:151-244) adds usrc*coeffdt with usrc == +0
+ * for Cartesian geometry and no interactions: this turns -0.0 into +0.0. */
+static void o_internal_sources(const o_lay *L, int n, o_work *w)
+{
+    for (size_t i = 0; i < (size_t)L->nv * n; ++i) w->u1[i] = w->u1[i] + 0.0;
+}
+
+/* care_for_positives (fluids/sources.F90:299-433) */
+static void o_care_for_positives(const o_cfg *cfg, const o_lay *L, int n, o_work *w, int *dnneg, int *eineg)
+{
+    for (int f = 0; f < L->nfl; ++f) {                   /* limit_minimal_density :326-392 */
+        double *dn = w->u1 + (size_t)L->idn[f] * n;
+        for (int i = 0; i < n; ++i)
+            if (dn[i] < 0.0) *dnneg = 1;
+        if (cfg->use_smalld)
+            for (int i = 0; i < n; ++i) dn[i] = f_max(dn[i], cfg->smalld);
+    }
+    for (int f = 0; f < L->nfl; ++f) {                   /* limit_minimal_intener :394-433 */
+        if (!L->has_en[f]) continue;
+        double *dn = w->u1 + (size_t)L->idn[f] * n, *mx = w->u1 + (size_t)L->imx[f] * n;
+        double *my = w->u1 + (size_t)L->imy[f] * n, *mz = w->u1 + (size_t)L->imz[f] * n;
+        double *en = w->u1 + (size_t)L->ien[f] * n;
+        for (int i = 0; i < n; ++i) {
+            double kin = (0.5 * ((mx[i] * mx[i] + my[i] * my[i]) + mz[i] * mz[i])) / dn[i];
+            double mag = 0.0, eint;
+            if (L->magn[f]) {
+                double bx = w->b1[i], by = w->b1[(size_t)n + i], bz = w->b1[2 * (size_t)n + i];
+                mag = 0.5 * ((bx * bx + by * by) + bz * bz);
+                eint = (en[i] - kin) - mag;
+            } else {
+                eint = en[i] - kin;
+            }
+            if (cfg->disallow_negatives && eint < 0.0) *eineg = 1;
+            if (cfg->use_smallei) eint = f_max(eint, cfg->smallei);
+            en[i] = eint + kin;
+            if (L->magn[f]) en[i] = en[i] + mag;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Block-level stage: solve_cg_ub / solve_cg_u                         */
+/* ------------------------------------------------------------------ */
+
+/* pdims (constants.F90:127-128): ORTHO1/ORTHO2 for each sweep direction */
+static const int ORTHO[3][2] = { {1, 2}, {2, 0}, {0, 1} };
+
+int o_solve_cg(const o_cfg *cfg, o_block *blk, int ddim, int istep, double dt, double ch)
+{
+    o_lay L;
+    o_layout(cfg, &L);
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    const int nv = L.nv, mag = cfg->magnetic;
+    const size_t cst[3] = {1, (size_t)ext[0], (size_t)ext[0] * ext[1]};   /* cell strides */
+    const int n = ext[ddim];
+    const int o1 = ORTHO[ddim][0], o2 = ORTHO[ddim][1];
+    const int first = (istep == 1);
+    /* rk_coef (constants.F90:230-238): EULER 1, RK2_1 1/2, RK2_2 1 */
+    double rk = (cfg->integration_order == 1) ? 1.0 : (istep == 1 ? 0.5 : 1.0);
+    const double dtodx = (rk * dt) / blk->dl[ddim];
+    const int *pm = PERM3[ddim];
+    int dnneg = 0, eineg = 0;
+
+#pragma omp parallel reduction(| : dnneg, eineg)
+    {
+        o_work w;
+        o_work_init(&w, n, nv);
+#pragma omp for collapse(2) schedule(static)
+        for (int i2 = g[o2]; i2 < g[o2] + blk->n[o2]; ++i2) {
+            for (int i1 = g[o1]; i1 < g[o1] + blk->n[o1]; ++i1) {
+                size_t base = (size_t)i1 * cst[o1] + (size_t)i2 * cst[o2];
+                size_t st = cst[ddim];
+                /* pu0 => uh, pu => u; if first stage: pu0 = pu (solve_cg_riemann.F90:174-176) */
+                for (int i = 0; i < n; ++i) {
+                    size_t cell = base + (size_t)i * st;
+                    double *pu = blk->u + cell * nv, *pu0 = blk->uh + cell * nv;
+                    if (first) memcpy(pu0, pu, nv * sizeof(double));
+                    for (int f = 0; f < L.nfl; ++f) {
+                        int b = L.beg[f];
+                        int cols[5] = {L.idn[f], L.imx[f] + pm[0], L.imx[f] + pm[1], L.imx[f] + pm[2], L.ien[f]};
+                        for (int c = 0; c < (L.has_en[f] ? 5 : 4); ++c) {
+                            w.u0[(size_t)cols[c] * n + i] = pu0[b + c];
+                            w.u1[(size_t)cols[c] * n + i] = pu[b + c];    /* u1 = u (:193) */
+                        }
+                    }
+                    if (mag) {
+                        double *pb = blk->b + cell * 3, *pb0 = blk->bh + cell * 3;
+                        if (first) {
+                            memcpy(pb0, pb, 3 * sizeof(double));
+                            blk->psih[cell] = blk->psi[cell];
+                        }
+                        for (int c = 0; c < 3; ++c) {
+                            w.b0[(size_t)pm[c] * n + i] = pb0[c];
+                            w.b1[(size_t)pm[c] * n + i] = pb[c];
+                        }
+                        w.b0[3 * (size_t)n + i] = blk->psih[cell];
+                        w.b1[3 * (size_t)n + i] = blk->psi[cell];
+                    }
+                }
+                o_pencil_solve(cfg, &L, n, dtodx, ch, &w);
+                o_internal_sources(&L, n, &w);
+                o_care_for_positives(cfg, &L, n, &w, &dnneg, &eineg);
+                /* transpose back (:225-227) */
+                for (int i = 0; i < n; ++i) {
+                    size_t cell = base + (size_t)i * st;
+                    double *pu = blk->u + cell * nv;
+                    for (int f = 0; f < L.nfl; ++f) {
+                        int b = L.beg[f];
+                        int cols[5] = {L.idn[f], L.imx[f] + pm[0], L.imx[f] + pm[1], L.imx[f] + pm[2], L.ien[f]};
+                        for (int c = 0; c < (L.has_en[f] ? 5 : 4); ++c) pu[b + c] = w.u1[(size_t)cols[c] * n + i];
+                    }
+                    if (mag) {
+                        double *pb = blk->b + cell * 3;
+                        for (int c = 0; c < 3; ++c) pb[c] = w.b1[(size_t)pm[c] * n + i];
+                        blk->psi[cell] = w.b1[3 * (size_t)n + i];
+                    }
+                }
+            }
+        }
+        o_work_free(&w);
+    }
+    blk->dn_negative |= dnneg;
+    blk->ei_negative |= eineg;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Guard cells                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Single-block guardcell refresh: periodic wrap (internal_boundaries with
+ * BND_PER, grid/cg_list_bnd.F90:251-324), outflow copy and reflecting mirror
+ * for u (bnd_u, :785-866).  Directions are filled x, y, z in turn, each over
+ * the full extent of the others, so corners come out as periodic images. */
+void o_fill_guards(const o_cfg *cfg, o_block *blk)
+{
+    o_lay L;
+    o_layout(cfg, &L);
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    const size_t cst[3] = {1, (size_t)ext[0], (size_t)ext[0] * ext[1]};
+    const int nv = L.nv, mag = cfg->magnetic;
+
+    for (int d = 0; d < 3; ++d) {
+        if (g[d] == 0) continue;
+        const int a = (d + 1) % 3, c = (d + 2) % 3;
+        const int nd = blk->n[d], gd = g[d];
+        for (int side = 0; side < 2; ++side) {
+            const int bt = blk->bnd[d][side];
+            for (int ib = 1; ib <= gd; ++ib) {
+                int dst = side == 0 ? gd - ib : gd + nd - 1 + ib;
+                int src;
+                if (bt == O_BND_PER) src = side == 0 ? gd + nd - ib : gd + ib - 1;
+                else if (bt == O_BND_OUT) src = side == 0 ? gd : gd + nd - 1;
+                else src = side == 0 ? gd + ib - 1 : gd + nd - ib;   /* mirror */
+                for (int ic = 0; ic < ext[c]; ++ic)
+                    for (int ia = 0; ia < ext[a]; ++ia) {
+                        size_t o = (size_t)ia * cst[a] + (size_t)ic * cst[c];
+                        size_t cd = o + (size_t)dst * cst[d], cs = o + (size_t)src * cst[d];
+                        memcpy(blk->u + cd * nv, blk->u + cs * nv, nv * sizeof(double));
+                        if (bt == O_BND_REF)
+                            for (int f = 0; f < L.nfl; ++f) blk->u[cd * nv + L.idn[f] + 1 + d] = -blk->u[cd * nv + L.idn[f] + 1 + d];
+                        if (mag) {
+                            memcpy(blk->b + cd * 3, blk->b + cs * 3, 3 * sizeof(double));
+                            blk->psi[cd] = blk->psi[cs];
+                        }
+                    }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Sweep, GLM, time step, pair of steps                                */
+/* ------------------------------------------------------------------ */
+
+int o_sweep(const o_cfg *cfg, o_block *blk, int cdim, double dt, double ch)
+{
+    int nst = (cfg->integration_order == 1) ? 1 : 2;     /* sweeps.F90:217-272 */
+    for (int s = 1; s <= nst; ++s) {
+        int rc = o_solve_cg(cfg, blk, cdim, (cfg->integration_order == 1) ? 1 : s, dt, ch);
+        if (rc) return rc;
+        o_fill_guards(cfg, blk);                          /* update_boundaries (:271) */
+    }
+    return 0;
+}
+
+static double o_min_dl(const o_block *blk, int *eff_dim)
+{
+    double m = DBL_MAX;
+    int e = 0;
+    for (int d = 0; d < 3; ++d)
+        if (blk->n[d] > 1) {
+            m = f_min(m, blk->dl[d]);
+            ++e;
+        }
+    if (eff_dim) *eff_dim = e;
+    return m;
+}
+
+double o_chspeed(const o_cfg *cfg, const o_block *blk, double dt)
+{
+    (void)cfg;
+    int eff;
+    double mdl = o_min_dl(blk, &eff);
+    double ch = DBL_MAX;                                   /* hdc.F90:112 */
+    if (eff > 0) ch = f_min(ch, (cfg->cfl_glm * mdl) / dt);   /* :118-119 */
+    return ch;
+}
+
+double o_glm_fac(const o_cfg *cfg, const o_block *blk, double dt, double ch)
+{
+    int eff;
+    double mdl = o_min_dl(blk, &eff);
+    double fac = 0.0;                                      /* hdc.F90:310-330 */
+    if (eff > 0) fac = f_max(fac, (cfg->glm_alpha * ch) / (mdl / dt));
+    return exp(-fac);
+}
+
+void o_glm_apply(const o_cfg *cfg, o_block *blk, double fac)
+{
+    (void)cfg;
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    size_t nc = (size_t)ext[0] * ext[1] * ext[2];
+    for (size_t i = 0; i < nc; ++i) blk->psi[i] = blk->psi[i] * fac;   /* :338 */
+}
+
+/* sound speeds: ion_cs (fluids/ionized/initionized.F90:89-145), neu_cs
+ * (fluids/neutral/initneutral.F90:82-109), dust_cs (fluids/dust/initdust.F90:74-87) */
+static double o_get_cs(const o_cfg *cfg, const o_lay *L, int f, const double *u, const double *b)
+{
+    if (L->kind[f] == O_DST) return 0.0;
+    double dn = u[L->idn[f]], mx = u[L->imx[f]], my = u[L->imy[f]], mz = u[L->imz[f]], en = u[L->ien[f]];
+    double ek = (0.5 * ((mx * mx + my * my) + mz * mz)) / dn;
+    if (L->kind[f] == O_ION) {
+        double pmag = 0.0;
+        if (cfg->magnetic) pmag = 0.5 * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2]);
+        double ps = (en - ek) * L->gam_1[f] + (2.0 - L->gam[f]) * pmag;
+        double p = ps - pmag;
+        return sqrt(fabs((2.0 * pmag + L->gam[f] * p) / dn));
+    }
+    double p = (en - ek) * L->gam_1[f];
+    return sqrt(fabs((L->gam[f] * p) / dn));
+}
+
+void o_timestep_raw(const o_cfg *cfg, const o_block *blk, double *dt_out, double *c_all_out)
+{
+    o_lay L;
+    o_layout(cfg, &L);
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    const int nv = L.nv;
+    double dt = DBL_MAX, c_all = 0.0;                     /* timestep.F90:161-162 */
+    for (int f = 0; f < L.nfl; ++f) {
+        double c_fl = SMALL, dtp[3] = {DBL_MAX, DBL_MAX, DBL_MAX};   /* :460-461 */
+#pragma omp parallel
+        {
+            double c_loc = SMALL, dtp_loc[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
+#pragma omp for collapse(2) schedule(static)
+            for (int k = g[2]; k < g[2] + blk->n[2]; ++k)
+                for (int j = g[1]; j < g[1] + blk->n[1]; ++j)
+                    for (int i = g[0]; i < g[0] + blk->n[0]; ++i) {
+                        size_t cell = ((size_t)k * ext[1] + j) * ext[0] + i;
+                        const double *u = blk->u + cell * nv;
+                        const double *b = cfg->magnetic ? blk->b + cell * 3 : NULL;
+                        double v[3], c[3];
+                        if (u[L.idn[f]] > 0.0) {                           /* :466-471 */
+                            for (int d = 0; d < 3; ++d) v[d] = fabs(u[L.imx[f] + d] / u[L.idn[f]]);
+                        } else {
+                            v[0] = v[1] = v[2] = 0.0;
+                        }
+                        double cs = o_get_cs(cfg, &L, f, u, b);
+                        for (int d = 0; d < 3; ++d) c[d] = f_max(v[d] + cs, SMALL);
+                        c_loc = f_max(c_loc, f_max(f_max(c[0], c[1]), c[2]));
+                        for (int d = 0; d < 3; ++d) {                     /* :477-486 */
+                            if (blk->n[d] > 1 && c[d] > 0.0) dtp_loc[d] = f_min(dtp_loc[d], blk->dl[d] / c[d]);
+                            else dtp_loc[d] = DBL_MAX;
+                        }
+                    }
+#pragma omp critical
+            {
+                c_fl = f_max(c_fl, c_loc);
+                for (int d = 0; d < 3; ++d) dtp[d] = f_min(dtp[d], dtp_loc[d]);
+            }
+        }
+        double dtf = cfg->cfl * f_min(f_min(dtp[0], dtp[1]), dtp[2]);   /* :493 */
+        dt = f_min(dt, dtf);
+        c_all = f_max(c_all, c_fl);
+    }
+    *dt_out = dt;
+    *c_all_out = c_all;
+}
+
+int o_time_step(const o_cfg *cfg, const o_block *blk, o_state *st)
+{
+    double dt, c_all;
+    st->dt_old = st->dt;                                  /* timestep.F90:158 */
+    o_timestep_raw(cfg, blk, &dt, &c_all);
+    if (st->nstep < 1) {                                  /* :200-208 */
+        if (cfg->dt_initial > 0.0) dt = f_min(dt, cfg->dt_initial);
+        else if (cfg->dt_initial < 0.0) dt = f_min(dt, -cfg->dt_initial * dt);
+    } else {
+        if (st->dt_old > 0.0) dt = f_min(dt, st->dt_old * cfg->dt_max_grow);
+    }
+    st->c_all = c_all;
+    if (dt < cfg->dt_min) {                               /* :213-219 write_crashed */
+        st->dt = dt;
+        return 3;
+    }
+    double rem = cfg->tend - st->t;                       /* :224 */
+    dt = f_min(f_min(dt, cfg->dt_max), (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem));
+    st->dt = dt;
+    return 0;
+}
+
+int o_fluid_update(const o_cfg *cfg, o_block *blk, o_state *st)
+{
+    const double dt = st->dt;
+    int rc;
+    if (cfg->magnetic) st->chspeed = o_chspeed(cfg, blk, dt);   /* update_chspeed (fluidupdate.F90:113) */
+    for (int half = 0; half < 2; ++half) {
+        st->t = st->t + dt;                                 /* :116, :126 */
+        for (int s = 0; s < 3; ++s) {                       /* make_3sweeps (:141-232) */
+            int d = half == 0 ? s : 2 - s;
+            if (cfg->skip_sweep[d] || blk->n[d] <= 1) continue;
+            if ((rc = o_sweep(cfg, blk, d, dt, st->chspeed))) return rc;
+        }
+        if (cfg->magnetic) o_glm_apply(cfg, blk, o_glm_fac(cfg, blk, dt, st->chspeed));   /* glmdamping */
+    }
+    return 0;
+}
+
+int o_run(const o_cfg *cfg, o_block *blk, o_state *st, int nsteps)
+{
+    for (int s = 0; s < nsteps; ++s) {
+        if (!(st->t < cfg->tend)) break;
+        int rc = o_time_step(cfg, blk, st);
+        if (rc) return rc;
+        rc = o_fluid_update(cfg, blk, st);
+        if (rc) return rc;
+        st->nstep += 1;
+    }
+    return 0;
+}
+
+void o_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int o_get_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

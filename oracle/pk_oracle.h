@@ -1,0 +1,96 @@
+/*
+ * pk_oracle.h -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * CPU restatement of PIERNIK's split Riemann sweep (RIEMANN_SPLIT solver),
+ * used only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg, as the checker the CUDA library is compared against.
+ *
+ * Parity status: UNPINNED.  The reference is Fortran 2008 and no Fortran
+ * compiler exists in this environment, and the reference tree holds no golden
+ * vectors for this path (its gold tests regenerate outputs from upstream git).
+ * The restatement follows the reference sources operation by operation
+ * (evaluation order, Fortran intrinsics spacing/sign/min/max, the -0.0
+ * normalisation done by internal_sources) and is cross-checked by physics
+ * properties in tests/ (conservation, axis-permutation symmetry).
+ *
+ * Layout mirrors the reference's named arrays with guard cells:
+ *   u  (nvar, i, j, k)  -> u[((k*NY + j)*NX + i)*nvar + v]   (cg%u, cg%w(uh))
+ *   b  (3,    i, j, k)  -> b[((k*NY + j)*NX + i)*3 + d]      (cg%b, magh)
+ *   psi(i, j, k)        -> psi[(k*NY + j)*NX + i]            (cg%q(psi), psih)
+ * where NX = n[0] + 2*g[0] and g[d] = nb when the direction exists, else 0
+ * (src/grid/grid_container_base.F90 extents lhn/ijkse).
+ */
+#ifndef PK_ORACLE_H
+#define PK_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { O_ION = 0, O_NEU = 1, O_DST = 2 };
+enum { O_LIM_VANLEER = 0, O_LIM_MINMOD = 1, O_LIM_MONCEN = 2, O_LIM_SUPERBEE = 3 };
+enum { O_BND_PER = 0, O_BND_OUT = 1, O_BND_REF = 2 };
+
+#define O_MAXFL 3
+
+typedef struct o_cfg {
+    int nfluids;                 /* fluids in flind order: ionized, neutral, dust */
+    int kind[O_MAXFL];           /* O_ION / O_NEU / O_DST */
+    double gamma[O_MAXFL];       /* adiabatic index; dust uses gamma < 0 */
+    int magnetic;                /* 1: B + GLM psi registered (divB_0 = HDC) */
+    int limiter, limiter_b;      /* flimiter / blimiter */
+    int use_smalld, use_smallei;
+    int disallow_negatives;
+    double smalld, smallei;
+    double cfl, cfl_glm, glm_alpha;
+    int ch_grid;
+    int integration_order;       /* 1 (EULER) or 2 (RK2) */
+    double dt_initial, dt_max_grow, dt_min, dt_max, tend;
+    int skip_sweep[3];
+} o_cfg;
+
+typedef struct o_block {
+    int n[3];                    /* interior cells per direction */
+    int nb;                      /* guard cells (dom%nb) */
+    double dl[3];                /* cell sizes */
+    int bnd[3][2];               /* O_BND_* per side */
+    double *u, *uh;              /* nvar components */
+    double *b, *bh;              /* 3 components (NULL when !magnetic) */
+    double *psi, *psih;          /* (NULL when !magnetic) */
+    int dn_negative, ei_negative;
+} o_block;
+
+typedef struct o_state {         /* the reference's global time-step state */
+    double t, dt, dt_old, c_all, chspeed;
+    int nstep;
+} o_state;
+
+int    o_nvar(const o_cfg *cfg);
+void   o_extents(const o_block *blk, int ext[3], int g[3]);
+
+/* one stage of solve_cg_riemann on one block (solve_cg_riemann.F90:68-233,241-307) */
+int    o_solve_cg(const o_cfg *cfg, o_block *blk, int ddim, int istep, double dt, double ch);
+/* guardcell refresh of u, b, psi (sweeps.F90:66-107 for a single block) */
+void   o_fill_guards(const o_cfg *cfg, o_block *blk);
+/* sweep(cdim): RK stages + boundary update (sweeps.F90:114-279) */
+int    o_sweep(const o_cfg *cfg, o_block *blk, int cdim, double dt, double ch);
+/* glmdamping factor and application (hdc.F90:289-349) */
+double o_glm_fac(const o_cfg *cfg, const o_block *blk, double dt, double ch);
+void   o_glm_apply(const o_cfg *cfg, o_block *blk, double fac);
+/* update_chspeed with ch_grid (hdc.F90:90-140) */
+double o_chspeed(const o_cfg *cfg, const o_block *blk, double dt);
+/* timestep_fluid over all fluids, before clamps (timestep.F90:431-495) */
+void   o_timestep_raw(const o_cfg *cfg, const o_block *blk, double *dt, double *c_all);
+/* time_step(dt, flind, .true.) including the sanity clamps (timestep.F90:112-240) */
+int    o_time_step(const o_cfg *cfg, const o_block *blk, o_state *st);   /* 3: dt < dt_min */
+/* fluid_update_full (fluidupdate.F90:99-136) */
+int    o_fluid_update(const o_cfg *cfg, o_block *blk, o_state *st);
+/* main-loop body repeated nsteps times (piernik.F90:125-213 without I/O) */
+int    o_run(const o_cfg *cfg, o_block *blk, o_state *st, int nsteps);
+void   o_set_threads(int n);
+int    o_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

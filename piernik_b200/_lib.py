@@ -1,0 +1,119 @@
+"""ctypes binding of libpiernik_b200.so (declarations in include/piernik_b200.h).
+
+The shared library is built in-tree by ``piernik_b200.build`` and is required:
+there is no CPU fallback, and loading fails with an explicit error when the
+library is missing or cannot be opened.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libpiernik_b200.so")
+
+PK_OK = 0
+ERRORS = {-1: "PK_E_ARG", -2: "PK_E_CUDA", -3: "PK_E_NOMEM", -4: "PK_E_UNSUPPORTED", -5: "PK_E_STATE",
+          -6: "PK_E_DTMIN"}
+PK_FLUID = {"ion": 0, "neu": 1, "dst": 2}
+PK_LIM = {"vanleer": 0, "minmod": 1, "moncen": 2, "superbee": 3}
+PK_LAYOUT_FORTRAN, PK_LAYOUT_SOA = 0, 1
+PK_EULER, PK_RK2_1, PK_RK2_2 = 10000, 10001, 10002
+PK_ST_DN_NEGATIVE, PK_ST_EI_NEGATIVE = 1, 2
+
+# every symbol include/piernik_b200.h declares
+EXPORTS = (
+    "pk_config_default", "pk_create", "pk_destroy", "pk_last_error", "pk_abi_version", "pk_block_add",
+    "pk_upload", "pk_download", "pk_solve_cg", "pk_fill_guards", "pk_sweep", "pk_glm_damp",
+    "pk_timestep_raw", "pk_time_step", "pk_fluid_update", "pk_run", "pk_get_time_state",
+    "pk_set_time_state", "pk_status", "pk_sync", "pk_set_tile", "pk_stream", "pk_profile_enable",
+    "pk_profile_read",
+)
+
+
+class PkConfig(C.Structure):
+    _fields_ = [
+        ("nfluids", C.c_int32),
+        ("fluid_kind", C.c_int32 * 3),
+        ("gamma", C.c_double * 3),
+        ("magnetic", C.c_int32),
+        ("limiter", C.c_int32),
+        ("limiter_b", C.c_int32),
+        ("use_smalld", C.c_int32),
+        ("use_smallei", C.c_int32),
+        ("disallow_negatives", C.c_int32),
+        ("smalld", C.c_double),
+        ("smallei", C.c_double),
+        ("cfl", C.c_double),
+        ("cfl_glm", C.c_double),
+        ("glm_alpha", C.c_double),
+        ("integration_order", C.c_int32),
+        ("nb", C.c_int32),
+        ("dt_initial", C.c_double),
+        ("dt_max_grow", C.c_double),
+        ("dt_min", C.c_double),
+        ("dt_max", C.c_double),
+        ("tend", C.c_double),
+        ("skip_sweep", C.c_int32 * 3),
+    ]
+
+
+class PkTimeState(C.Structure):
+    _fields_ = [
+        ("t", C.c_double),
+        ("dt", C.c_double),
+        ("dt_old", C.c_double),
+        ("c_all", C.c_double),
+        ("chspeed", C.c_double),
+        ("nstep", C.c_int32),
+    ]
+
+
+class PkError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: str = LIBPATH):
+    """Open the CUDA library; raises PkError when it is absent (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise PkError(f"{path} is missing: build it with piernik_b200.build.build() "
+                      "(the sweep has no CPU implementation)")
+    L = C.CDLL(path)
+    for name in EXPORTS:
+        getattr(L, name)
+    H = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    L.pk_config_default.argtypes = [C.POINTER(PkConfig)]
+    L.pk_config_default.restype = None
+    L.pk_create.argtypes = [C.POINTER(PkConfig), C.POINTER(H)]
+    L.pk_destroy.argtypes = [H]
+    L.pk_last_error.argtypes = [H]
+    L.pk_last_error.restype = C.c_char_p
+    L.pk_block_add.argtypes = [H, C.POINTER(C.c_int32), dp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.pk_upload.argtypes = [H, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    L.pk_download.argtypes = [H, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    L.pk_solve_cg.argtypes = [H, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double]
+    L.pk_fill_guards.argtypes = [H]
+    L.pk_sweep.argtypes = [H, C.c_int32, C.c_double, C.c_double]
+    L.pk_glm_damp.argtypes = [H, C.c_double]
+    L.pk_timestep_raw.argtypes = [H, dp, dp]
+    L.pk_time_step.argtypes = [H, dp]
+    L.pk_fluid_update.argtypes = [H]
+    L.pk_run.argtypes = [H, C.c_int32]
+    L.pk_get_time_state.argtypes = [H, C.POINTER(PkTimeState)]
+    L.pk_set_time_state.argtypes = [H, C.POINTER(PkTimeState)]
+    L.pk_status.argtypes = [H, C.POINTER(C.c_uint32)]
+    L.pk_sync.argtypes = [H]
+    L.pk_set_tile.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
+    L.pk_stream.argtypes = [H]
+    L.pk_stream.restype = C.c_void_p
+    L.pk_profile_enable.argtypes = [H, C.c_int32]
+    L.pk_profile_read.argtypes = [H, C.POINTER(C.c_int64), C.POINTER(C.c_int64), dp]
+    _lib = L
+    return L

@@ -1,0 +1,89 @@
+"""Run configuration of the sweep path, with PIERNIK's names and defaults.
+
+The fields mirror the reference namelists the split Riemann path reads:
+``NUMERICAL_SETUP`` (src/base/global.F90:118-120, defaults :196-260),
+``FLUID_IONIZED`` / ``FLUID_NEUTRAL`` / ``FLUID_DUST`` (gamma), ``BASE_DOMAIN``
+(n_d, bnd_*, xmin..zmax; src/grid/domain.F90:139) and ``END_CONTROL`` (tend).
+"""
+from __future__ import annotations
+
+import dataclasses
+import sys
+from dataclasses import dataclass, field
+from typing import List, Tuple
+
+BND_PER, BND_OUT, BND_REF = 0, 1, 2
+BND_NAMES = {"per": BND_PER, "out": BND_OUT, "ref": BND_REF}
+LIMITER_NAMES = ("vanleer", "minmod", "moncen", "superbee")
+FLT_TINY = 1.1754943508222875e-38        # tiny(real(1.0,4))  (constants.F90:104)
+DBL_HUGE = sys.float_info.max            # huge(1.)
+DBL_TINY = sys.float_info.min            # tiny(1.)
+
+
+@dataclass
+class Setup:
+    # BASE_DOMAIN
+    n: Tuple[int, int, int] = (64, 64, 64)
+    nb: int = 4
+    xmin: Tuple[float, float, float] = (-1.0, -1.0, -1.0)
+    xmax: Tuple[float, float, float] = (1.0, 1.0, 1.0)
+    bnd: Tuple[Tuple[int, int], ...] = ((BND_PER, BND_PER),) * 3
+    # fluids, in flind order (ionized, neutral, dust): (kind, gamma)
+    fluids: List[Tuple[str, float]] = field(default_factory=lambda: [("ion", 5.0 / 3.0)])
+    magnetic: bool = True            # MAGNETIC with divB_0 = 'HDC' (global.F90:189)
+    # NUMERICAL_SETUP
+    cfl: float = 0.7
+    cfl_glm: float = 0.7             # set from the default cfl before the namelist is read (:253)
+    glm_alpha: float = 0.1
+    limiter: str = "vanleer"
+    limiter_b: str = "vanleer"       # limiter_b = limiter (:212-213)
+    smalld: float = 1.0e-3
+    smallei: float = 1.0e-10
+    use_smalld: bool = True
+    use_smallei: bool = True
+    disallow_negatives: bool = True
+    integration_order: int = 2
+    dt_initial: float = -1.0
+    dt_max_grow: float = 2.0
+    dt_min: float = DBL_TINY
+    dt_max: float = DBL_HUGE
+    cflcontrol: str = "none"
+    skip_sweep: Tuple[bool, bool, bool] = (False, False, False)
+    # END_CONTROL
+    tend: float = DBL_HUGE
+    nend: int = 0
+
+    @property
+    def dl(self) -> Tuple[float, float, float]:
+        return tuple((self.xmax[d] - self.xmin[d]) / self.n[d] for d in range(3))
+
+    @property
+    def guards(self) -> Tuple[int, int, int]:
+        return tuple(self.nb if self.n[d] > 1 else 0 for d in range(3))
+
+    @property
+    def ext(self) -> Tuple[int, int, int]:
+        g = self.guards
+        return tuple(self.n[d] + 2 * g[d] for d in range(3))
+
+    @property
+    def nvar(self) -> int:
+        return sum(4 if k == "dst" else 5 for k, _ in self.fluids)
+
+    def replace(self, **kw) -> "Setup":
+        return dataclasses.replace(self, **kw)
+
+    def validate(self) -> None:
+        if self.limiter not in LIMITER_NAMES or self.limiter_b not in LIMITER_NAMES:
+            raise ValueError(f"unknown limiter {self.limiter!r}/{self.limiter_b!r}")
+        if not (0.0 < self.cfl <= 1.0):
+            raise ValueError("CFL value should be >0. and <=1.")      # global.F90:303
+        if self.integration_order not in (1, 2):
+            raise ValueError("integration_order must be 1 or 2")
+        kinds = [k for k, _ in self.fluids]
+        if kinds != sorted(kinds, key=("ion", "neu", "dst").index) or len(set(kinds)) != len(kinds):
+            raise ValueError("fluids must be a subset of (ion, neu, dst) in that order")
+        if self.magnetic and "ion" not in kinds:
+            raise ValueError("a magnetised run needs the ionized fluid")
+        if self.magnetic and any(b != (BND_PER, BND_PER) for d, b in enumerate(self.bnd) if self.n[d] > 1):
+            raise ValueError("magnetised runs support periodic boundaries only")

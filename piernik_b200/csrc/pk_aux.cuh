@@ -1,0 +1,218 @@
+// pk_aux.cuh -- bandwidth kernels around the sweep: CFL reduction, psi
+// damping, guard-cell refresh, host-layout conversion.
+#pragma once
+#include "pk_device.cuh"
+
+namespace pk {
+
+struct BoxGeom {
+    int ext[3], g[3], n[3];
+    long long plane;
+};
+
+PK_DEV long long cell_index(const BoxGeom& b, int i, int j, int k)
+{
+    return ((long long)k * b.ext[1] + j) * b.ext[0] + i;
+}
+
+struct CflFluid {
+    int kind;        // K_ION / K_NEU / K_DST
+    int beg;         // first component plane of the fluid
+    double gam, gam_1;
+};
+
+struct CflArgs {
+    int nfl;
+    CflFluid fl[3];
+    int magnetic;    // B planes start at ib
+    int ib;
+};
+
+// timestep_fluid (src/base/timestep.F90:431-495) over the interior cells:
+// per fluid, the maxima of c_d = max(|v_d| + c_s, small) for d = x, y, z and of
+// max_d c_d.  Because dl/c is monotone in c under correct rounding,
+// min_cells(dl/c_d) == dl/max_cells(c_d) exactly, so the host finishes the
+// reduction with one division per direction.  Maxima of positive doubles are
+// reduced as their bit patterns (order-independent, deterministic).
+// out[f*4 + d] (d < 3) and out[f*4 + 3] hold the bit patterns.
+__global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsigned long long* __restrict__ out)
+{
+    const double small = 1.1754943508222875e-38;   // tiny(real(1.0,4)), constants.F90:104
+    const long long ncell = (long long)b.n[0] * b.n[1] * b.n[2];
+    double cm[3][4];
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int d = 0; d < 4; ++d) cm[f][d] = small;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % b.n[0]);
+        const long long r = c / b.n[0];
+        const int j = (int)(r % b.n[1]);
+        const int k = (int)(r / b.n[1]);
+        const long long off = cell_index(b, i + b.g[0], j + b.g[1], k + b.g[2]);
+        double pmag = 0.0;
+        if (a.magnetic) {
+            const double bx = u[(long long)(a.ib + 0) * b.plane + off];
+            const double by = u[(long long)(a.ib + 1) * b.plane + off];
+            const double bz = u[(long long)(a.ib + 2) * b.plane + off];
+            pmag = 0.5 * ((bx * bx + by * by) + bz * bz);      // emag(b(x), b(y), b(z))
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            if (f >= a.nfl) break;
+            const CflFluid fl = a.fl[f];
+            const double dn = u[(long long)fl.beg * b.plane + off];
+            const double mx = u[(long long)(fl.beg + 1) * b.plane + off];
+            const double my = u[(long long)(fl.beg + 2) * b.plane + off];
+            const double mz = u[(long long)(fl.beg + 3) * b.plane + off];
+            double v[3];
+            if (dn > 0.0) {                                     // timestep.F90:466-471
+                v[0] = fabs(mx / dn);
+                v[1] = fabs(my / dn);
+                v[2] = fabs(mz / dn);
+            } else {
+                v[0] = v[1] = v[2] = 0.0;
+            }
+            double cs = 0.0;
+            if (fl.kind != K_DST) {
+                const double en = u[(long long)(fl.beg + 4) * b.plane + off];
+                const double ek = (0.5 * ((mx * mx + my * my) + mz * mz)) / dn;
+                if (fl.kind == K_ION) {                         // ion_cs, initionized.F90:131-139
+                    const double ps = (en - ek) * fl.gam_1 + (2.0 - fl.gam) * pmag;
+                    const double p = ps - pmag;
+                    cs = sqrt(fabs((2.0 * pmag + fl.gam * p) / dn));
+                } else {                                        // neu_cs, initneutral.F90:102-105
+                    const double p = (en - ek) * fl.gam_1;
+                    cs = sqrt(fabs((fl.gam * p) / dn));
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double cd = f_max(v[d] + cs, small);
+                cm[f][d] = f_max(cm[f][d], cd);
+                cm[f][3] = f_max(cm[f][3], cd);
+            }
+        }
+    }
+    __shared__ unsigned long long red[32][12];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            unsigned long long x = (unsigned long long)__double_as_longlong(cm[f][d]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = y > x ? y : x;
+            }
+            if (lane == 0) red[wid][f * 4 + d] = x;
+        }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        unsigned long long x = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x = red[w][threadIdx.x] > x ? red[w][threadIdx.x] : x;
+        atomicMax(out + threadIdx.x, x);
+    }
+}
+
+// psi *= fac over the whole plane, guard cells included (hdc.F90:338)
+__global__ void k_scale(double* __restrict__ p, long long n, double fac)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = p[i] * fac;
+}
+
+struct GuardArgs {
+    int bnd[3][2];      // 0 per, 1 out, 2 ref
+    int nplanes;
+    int mom_plane[3][3];    // momentum planes per fluid and direction (-1: none)
+    int nfl;
+};
+
+// Guard-cell refresh of one block, all components.  Filling x, then y over
+// the x-extended range, then z (the order of the reference's per-direction
+// exchanges) composes to: guard cell (i,j,k) takes the interior cell obtained
+// by mapping each coordinate that lies in a guard layer through its boundary
+// rule (periodic wrap, outflow clamp, reflecting mirror with the normal
+// momentum negated) -- see bnd_u, src/grid/cg_list_bnd.F90:785-866.
+__device__ __forceinline__ int map_guard(int i, int n, int g, int side_lo, int side_hi, bool& flip)
+{
+    if (i >= g && i < g + n) return i;
+    if (i < g) {
+        const int ib = g - i;                          // 1..g
+        if (side_lo == 0) return g + n - ib;
+        if (side_lo == 1) return g;
+        flip = !flip;
+        return g + ib - 1;
+    }
+    const int ib = i - (g + n - 1);                    // 1..g
+    if (side_hi == 0) return g + ib - 1;
+    if (side_hi == 1) return g + n - 1;
+    flip = !flip;
+    return g + n - ib;
+}
+
+__global__ void k_fill_guards(BoxGeom b, double* __restrict__ u, GuardArgs a)
+{
+    const long long ncell = (long long)b.ext[0] * b.ext[1] * b.ext[2];
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % b.ext[0]);
+        const long long r = c / b.ext[0];
+        const int j = (int)(r % b.ext[1]);
+        const int k = (int)(r / b.ext[1]);
+        const bool inside = i >= b.g[0] && i < b.g[0] + b.n[0] && j >= b.g[1] && j < b.g[1] + b.n[1] &&
+                            k >= b.g[2] && k < b.g[2] + b.n[2];
+        if (inside) continue;
+        bool fl[3] = {false, false, false};
+        const int si = map_guard(i, b.n[0], b.g[0], a.bnd[0][0], a.bnd[0][1], fl[0]);
+        const int sj = map_guard(j, b.n[1], b.g[1], a.bnd[1][0], a.bnd[1][1], fl[1]);
+        const int sk = map_guard(k, b.n[2], b.g[2], a.bnd[2][0], a.bnd[2][1], fl[2]);
+        const long long src = cell_index(b, si, sj, sk);
+        for (int v = 0; v < a.nplanes; ++v) u[(long long)v * b.plane + c] = u[(long long)v * b.plane + src];
+        for (int d = 0; d < 3; ++d)
+            if (fl[d])
+                for (int f = 0; f < a.nfl; ++f) {
+                    const int pl = a.mom_plane[f][d];
+                    u[(long long)pl * b.plane + c] = -u[(long long)pl * b.plane + c];
+                }
+    }
+}
+
+// Fortran-order arrays (u(nvar,i,j,k), b(3,i,j,k), psi(i,j,k)) <-> component planes.
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long long ncell, int ncomp,
+                             int plane0, long long plane)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+        for (int v = 0; v < ncomp; ++v) soa[(long long)(plane0 + v) * plane + c] = aos[c * ncomp + v];
+}
+
+__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, long long ncell, int ncomp,
+                             int plane0, long long plane)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+        for (int v = 0; v < ncomp; ++v) aos[c * ncomp + v] = soa[(long long)(plane0 + v) * plane + c];
+}
+
+// copy the pencils a stage touched (full extent along dir, interior in the
+// other two directions) from src to dst, all planes
+__global__ void k_copy_pencils(BoxGeom b, int dir, const double* __restrict__ src, double* __restrict__ dst, int nplanes)
+{
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = (d == dir) ? 0 : b.g[d];
+        hi[d] = (d == dir) ? b.ext[d] : b.g[d] + b.n[d];
+    }
+    const long long nx = hi[0] - lo[0], ny = hi[1] - lo[1], nz = hi[2] - lo[2];
+    const long long ncell = nx * ny * nz;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int i = lo[0] + (int)(c % nx);
+        const long long r = c / nx;
+        const int j = lo[1] + (int)(r % ny);
+        const int k = lo[2] + (int)(r / ny);
+        const long long o = cell_index(b, i, j, k);
+        for (int v = 0; v < nplanes; ++v) dst[(long long)v * b.plane + o] = src[(long long)v * b.plane + o];
+    }
+}
+
+}  // namespace pk

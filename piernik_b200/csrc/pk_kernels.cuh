@@ -1,0 +1,277 @@
+// pk_kernels.cuh -- sweep kernels over pencil tiles staged in shared memory.
+//
+// Storage of one block on the device (structure of arrays, guard cells kept):
+//   u[v][k][j][i], v over the fluid components in flind order, then Bx, By,
+//   Bz, psi; i over ext_x = n_x + 2*g_x, etc.  One plane per component.
+//
+// A CTA owns a tile of P pencils x T cells along the sweep direction; one
+// thread per tile cell holds that cell's conservative state in registers for
+// the whole launch.  A stage of the reference's pencil solve
+// (solve_cg_riemann.F90:318-376) runs as four shared-memory phases separated
+// by __syncthreads:
+//   1. utoq          -> Q (primitives)
+//   2. limited slope -> ql in registers, qr of the cell's left face -> R
+//   3. Riemann flux at the cell's right face (own ql, neighbour's R) -> Q
+//   4. u1 = u0 + dtodx*(F(i-1/2) - F(i+1/2)), internal_sources, floors
+// Which cells do what is decided per thread from its pencil position:
+//   * fused mode (periodic single block): both RK2 stages in one launch over a
+//     tile with a 4-cell halo read with periodic wrap, output written to a
+//     second buffer.  With nb = 4 this equals the reference's stage 1 ->
+//     guardcell exchange -> stage 2 bit for bit: every cell the second stage
+//     reads was computed from the same inputs by the same operations.
+//   * stage mode (any block with guard cells): one stage over a tile with a
+//     2-cell halo, pencil ends (the outermost guard cells) handled with the
+//     reference's one-sided rules, written back in place.
+#pragma once
+#include "pk_device.cuh"
+
+namespace pk {
+
+struct Geom {
+    long long plane;        // elements per component plane
+    long long sd, s1, s2;   // element strides along the sweep direction and the two ortho directions
+    int ext_d;              // pencil length with guards
+    int n_d, g_d;           // interior length / guard offset along the sweep direction
+    int n1, g1, n2, g2;     // interior extent / guard offset of the ortho directions
+    int perm[3];            // slot b+1+j of a swept cell holds plane b+1+perm[j]
+};
+
+struct Tile {
+    int P, T, L;            // pencils, tile length, output cells per pencil
+    int xfast;              // 1: lanes run along the pencil (x sweeps)
+    int halo;               // stage mode: tile cells before the first owned cell (0 or 2)
+};
+
+// -------------------------------------------------------------------------
+// swept load / store of one cell
+// -------------------------------------------------------------------------
+template <class PH>
+PK_DEV int plane_of(int slot, const int (&perm)[3])
+{
+    // slot -> component plane; fluids [dn, m_n, m_t1, m_t2, en], then B_n, B_t1, B_t2, psi
+#pragma unroll
+    for (int f = 0; f < PH::NFL; ++f) {
+        const int b = PH::beg(f);
+        if (slot == b + 1) return b + 1 + perm[0];
+        if (slot == b + 2) return b + 1 + perm[1];
+        if (slot == b + 3) return b + 1 + perm[2];
+    }
+    if (PH::MHD) {
+        if (slot == PH::IB) return PH::IB + perm[0];
+        if (slot == PH::IB + 1) return PH::IB + perm[1];
+        if (slot == PH::IB + 2) return PH::IB + perm[2];
+    }
+    return slot;
+}
+
+template <class PH>
+PK_DEV void load_cell(const double* __restrict__ u, long long off, const Geom& g, double (&w)[PH::NV])
+{
+    const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
+#pragma unroll
+    for (int v = 0; v < PH::NV; ++v) w[v] = __ldg(u + (long long)plane_of<PH>(v, perm) * g.plane + off);
+}
+
+template <class PH>
+PK_DEV void store_cell(double* __restrict__ u, long long off, const Geom& g, const double (&w)[PH::NV])
+{
+    const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
+#pragma unroll
+    for (int v = 0; v < PH::NV; ++v) u[(long long)plane_of<PH>(v, perm) * g.plane + off] = w[v];
+}
+
+// roles of one tile cell within one stage
+struct Roles {
+    bool q;        // has a valid input state -> computes primitives
+    bool slope;    // computes its limited slope
+    int end;       // 0 interior slope, -1 pencil start rule, +1 pencil end rule
+    bool flux;     // computes the flux through its right face
+    bool upd;      // Euler-updated from the two face fluxes
+    bool care;     // internal_sources + care_for_positives applied
+};
+
+template <class PH>
+PK_DEV void rk_stage(double* __restrict__ Q, double* __restrict__ R, int me, int st, int PT, const Roles& r,
+                     double (&w)[PH::NV], const double (&u0)[PH::NV], double dtodx, double ch,
+                     const PhysParams& pp, unsigned& status)
+{
+    constexpr int NV = PH::NV;
+    double q[NV];
+    if (r.q) {
+        utoq<PH>(w, q, pp);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Q[v * PT + me] = q[v];
+    }
+    __syncthreads();
+    double ql[NV];
+    if (r.slope) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const int lim = (PH::MHD && v >= PH::IB) ? pp.limb : pp.lim;
+            double s;
+            if (r.end < 0) s = slope_end(lim, Q[v * PT + me + st] - q[v]);
+            else if (r.end > 0) s = slope_end(lim, q[v] - Q[v * PT + me - st]);
+            else s = slope_interior(lim, q[v] - Q[v * PT + me - st], Q[v * PT + me + st] - q[v]);
+            const double dqh = 0.5 * s;                       // dq_interp = half * f_limiter(q)
+            ql[v] = q[v] + dqh;                               // left state of the right face
+            R[v * PT + me] = q[v] - dqh;                      // right state of the left face
+        }
+    }
+    __syncthreads();
+    if (r.flux) {
+        double qr[NV], fx[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) qr[v] = R[v * PT + me + st];
+        riemann<PH>(ql, qr, ch, pp, fx);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Q[v * PT + me] = fx[v];
+    }
+    __syncthreads();
+    if (r.upd) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) w[v] = u0[v] + dtodx * (Q[v * PT + me - st] - Q[v * PT + me]);
+    }
+    if (r.care) sources_and_floors<PH>(w, pp, status);
+    __syncthreads();
+}
+
+PK_DEV void flush_status(unsigned status, unsigned* gstatus)
+{
+    const unsigned s = __reduce_or_sync(0xffffffffu, status);
+    if (s && (threadIdx.x & 31) == 0) atomicOr(gstatus, s);
+}
+
+PK_DEV int wrap(int s, int n)
+{
+    int r = s % n;
+    return r < 0 ? r + n : r;
+}
+
+// -------------------------------------------------------------------------
+// Fused two-stage sweep of a periodic block: uin -> uout.
+// grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2.
+// -------------------------------------------------------------------------
+template <class PH, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
+                                                     double* __restrict__ uout, PhysParams pp, double dtodx1,
+                                                     double dtodx2, double ch, double psi_fac,
+                                                     unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    constexpr int NV = PH::NV;
+    const int P = tl.P, T = tl.T, PT = P * T;
+    double* Q = smem;
+    double* R = smem + NV * PT;
+    const int tid = threadIdx.x;
+    int p, t;
+    if (tl.xfast) { t = tid % T; p = tid / T; }
+    else { p = tid % P; t = tid / P; }
+    const int sp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
+    const int me = p * sp + t * st;
+    const int i1 = blockIdx.x * P + p;
+    const int c0 = blockIdx.y * tl.L;
+    const int i2 = blockIdx.z;
+    const bool active = (tid < PT) && (i1 < g.n1);
+    const int s = c0 - 4 + t;                                  // position along the pencil (interior coords)
+    const long long off = (long long)(g.g_d + wrap(s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
+                          (long long)(g.g2 + i2) * g.s2;
+    double u0[NV], w[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u0[v] = 0.0;
+    if (active) load_cell<PH>(uin, off, g, u0);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) w[v] = u0[v];
+    unsigned status = 0;
+    Roles r;
+    // stage 1 (RK2_1) on tile cells [0, T)
+    r.q = active;
+    r.slope = active && t >= 1 && t < T - 1;
+    r.end = 0;
+    r.flux = active && t >= 1 && t < T - 2;
+    r.upd = active && t >= 2 && t < T - 2;
+    r.care = r.upd;
+    rk_stage<PH>(Q, R, me, st, PT, r, w, u0, dtodx1, ch, pp, status);
+    // stage 2 (RK2_2) on tile cells [2, T-2)
+    r.q = active && t >= 2 && t < T - 2;
+    r.slope = active && t >= 3 && t < T - 3;
+    r.flux = active && t >= 3 && t < T - 4;
+    r.upd = active && t >= 4 && t < T - 4;
+    r.care = r.upd;
+    rk_stage<PH>(Q, R, me, st, PT, r, w, u0, dtodx2, ch, pp, status);
+    if (r.upd && s < c0 + tl.L && s < g.n_d) {
+        if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
+        store_cell<PH>(uout, off, g, w);
+    }
+    flush_status(status, gstatus);
+}
+
+// -------------------------------------------------------------------------
+// One RK stage of solve_cg on a block with guard cells.
+// grid: x = ortho-1 tiles, y = chunks of L cells of the full pencil, z = ortho-2.
+// The tile spans [c0-halo, c0-halo+T) of the pencil: the whole pencil
+// (halo 0, T = L = ext) or a chunk with a 2-cell halo; pencil ends (storage index 0
+// and ext-1) follow the reference's one-sided limiter rules and get floors
+// without an update, exactly like cells 1 and n of solve().
+// first != 0: u0 = u and the owned cells are copied to uh (pu0 = pu).
+// uin and uout may alias only when one chunk covers the whole pencil (every
+// load of a pencil then precedes every store of it, within one CTA).
+// -------------------------------------------------------------------------
+template <class PH, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* uin, double* uout,
+                                               double* uh, PhysParams pp, int first, double dtodx, double ch,
+                                               unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    constexpr int NV = PH::NV;
+    const int P = tl.P, T = tl.T, PT = P * T;
+    double* Q = smem;
+    double* R = smem + NV * PT;
+    const int tid = threadIdx.x;
+    int p, t;
+    if (tl.xfast) { t = tid % T; p = tid / T; }
+    else { p = tid % P; t = tid / P; }
+    const int sp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
+    const int me = p * sp + t * st;
+    const int i1 = blockIdx.x * P + p;
+    const int c0 = blockIdx.y * tl.L;
+    const int i2 = blockIdx.z;
+    const int n = g.ext_d;
+    const int s = c0 - tl.halo + t;                            // storage index along the pencil
+    const bool valid = (tid < PT) && (i1 < g.n1) && s >= 0 && s < n;
+    const long long off = (long long)s * g.sd + (long long)(g.g1 + i1) * g.s1 + (long long)(g.g2 + i2) * g.s2;
+    double u0[NV], w[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u0[v] = w[v] = 0.0;
+    if (valid) {
+        const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
+#pragma unroll
+        for (int v = 0; v < NV; ++v) w[v] = uin[(long long)plane_of<PH>(v, perm) * g.plane + off];
+        if (first) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u0[v] = w[v];
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u0[v] = uh[(long long)plane_of<PH>(v, perm) * g.plane + off];
+        }
+    }
+    unsigned status = 0;
+    Roles r;
+    r.q = valid;
+    r.end = (s == 0) ? -1 : ((s == n - 1) ? 1 : 0);
+    r.slope = valid && (r.end != 0 || (t >= 1 && t <= T - 2));
+    // the flux through the right face needs this cell's slope and the next cell's
+    const bool next_slope = (s + 1 < n) && (t + 1 <= T - 1) && ((s + 1 == n - 1) || (t + 1 <= T - 2));
+    r.flux = r.slope && next_slope;
+    // the update needs the left-face flux computed by tile cell t-1
+    const bool prev_flux = (t >= 1) && (s >= 1) && ((s - 1 == 0) || (t - 1 >= 1));
+    r.upd = valid && s >= 1 && s <= n - 2 && prev_flux && r.flux;
+    r.care = r.upd || (valid && (s == 0 || s == n - 1));
+    rk_stage<PH>(Q, R, me, st, PT, r, w, u0, dtodx, ch, pp, status);
+    if (valid && s >= c0 && s < c0 + tl.L) {
+        if (first) store_cell<PH>(uh, off, g, u0);
+        store_cell<PH>(uout, off, g, w);
+    }
+    flush_status(status, gstatus);
+}
+
+}  // namespace pk

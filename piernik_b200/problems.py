@@ -1,0 +1,237 @@
+"""Seeded synthetic initial conditions for the benchmark configurations.
+
+Arrays are returned in the reference's guard-cell layout (Fortran ``cg%u(v,i,j,k)``
+seen from C as ``u[k, j, i, v]``, ``b[k, j, i, d]``, ``psi[k, j, i]``) with the
+guard cells already filled periodically.  The recipes follow the reference's
+problem setups where one exists (problems/sedov/initproblem.F90:179-292,
+problems/otvortex/initproblem.F90:99-166); no external dataset is involved.
+"""
+from __future__ import annotations
+
+import math
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .config import BND_PER, Setup
+
+
+def _empty(setup: Setup):
+    ez, ey, ex = setup.ext[2], setup.ext[1], setup.ext[0]
+    u = np.zeros((ez, ey, ex, setup.nvar))
+    b = np.zeros((ez, ey, ex, 3)) if setup.magnetic else None
+    psi = np.zeros((ez, ey, ex)) if setup.magnetic else None
+    return u, b, psi
+
+
+def _centres(setup: Setup, d: int) -> np.ndarray:
+    g = setup.guards[d]
+    dl = setup.dl[d]
+    i = np.arange(setup.ext[d]) - g
+    return setup.xmin[d] + (i + 0.5) * dl
+
+
+def fill_periodic(setup: Setup, arr: Optional[np.ndarray]) -> None:
+    """Copy interior cells into guard cells periodically, x then y then z."""
+    if arr is None:
+        return
+    g = setup.guards
+    for d in range(3):
+        if g[d] == 0:
+            continue
+        ax = 2 - d                    # array axis of direction d (k, j, i order)
+        n = setup.n[d]
+        sl = [slice(None)] * arr.ndim
+        for ib in range(g[d]):
+            lo_dst, lo_src = g[d] - 1 - ib, g[d] + n - 1 - ib
+            hi_dst, hi_src = g[d] + n + ib, g[d] + ib
+            for dst, src in ((lo_dst, lo_src), (hi_dst, hi_src)):
+                a = list(sl)
+                bsl = list(sl)
+                a[ax] = dst
+                bsl[ax] = src
+                arr[tuple(a)] = arr[tuple(bsl)]
+
+
+def _set_fluid(setup, u, f, rho, vx, vy, vz, p, emag=None):
+    """Conservative variables of fluid index f from primitives (broadcasting)."""
+    beg = sum(4 if k == "dst" else 5 for k, _ in setup.fluids[:f])
+    kind, gam = setup.fluids[f]
+    u[..., beg + 0] = rho
+    u[..., beg + 1] = rho * vx
+    u[..., beg + 2] = rho * vy
+    u[..., beg + 3] = rho * vz
+    if kind != "dst":
+        e = p / (gam - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+        if emag is not None:
+            e = e + emag
+        u[..., beg + 4] = e
+
+
+def sedov(n: int = 64, r_cells: float = 3.5, e_total: float = 1.0, p0: float = 1.0e-5,
+          gamma: float = 5.0 / 3.0, setup: Optional[Setup] = None):
+    """3D Sedov blast, plain hydro (neutral fluid, no B), periodic box [-1,1]^3.
+
+    Total energy ``e_total`` is deposited as thermal energy in cells whose 4^3
+    sub-samples lie within ``r_cells`` cells of the centre, weighted per
+    sub-sample as in problems/sedov/initproblem.F90:226-255.
+    """
+    if setup is None:
+        setup = Setup(n=(n, n, n), fluids=[("neu", gamma)], magnetic=False, limiter="vanleer",
+                      limiter_b="vanleer", cfl=0.7, cfl_glm=0.7, smalld=1.0e-3)
+    u, _, _ = _empty(setup)
+    x, y, z = (_centres(setup, d) for d in range(3))
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    _set_fluid(setup, u, 0, 1.0, 0.0, 0.0, 0.0, p0)
+    dx = setup.dl[0]
+    r0 = r_cells * dx
+    isub = 4
+    offs = (2 * np.arange(1, isub + 1) - isub - 1) / (2.0 * isub)
+    frac = np.zeros(X.shape)
+    for ox in offs:
+        for oy in offs:
+            for oz in offs:
+                r = np.sqrt((X + ox * dx) ** 2 + (Y + oy * dx) ** 2 + (Z + oz * dx) ** 2)
+                frac += (r < r0)
+    frac /= isub ** 3
+    g = setup.guards
+    interior = frac[g[2]:g[2] + setup.n[2], g[1]:g[1] + setup.n[1], g[0]:g[0] + setup.n[0]]
+    vol = float(np.prod(setup.dl))
+    eexpl = e_total / (interior.sum() * vol)        # energy density of the deposit
+    ien = 4
+    u[..., ien] += eexpl * frac
+    fill_periodic(setup, u)
+    return setup, u, None, None
+
+
+def _rng(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def _fourier_field(n: Tuple[int, int, int], kmin: float, kmax: float, slope: float,
+                   rng: np.random.Generator, ncomp: int = 3) -> np.ndarray:
+    """Real periodic field on an (nz, ny, nx) grid with random-phase modes of
+    integer wavenumber kmin <= |k| <= kmax and amplitude |k|**slope."""
+    nx, ny, nz = n
+    kz = np.fft.fftfreq(nz, 1.0 / nz)[:, None, None]
+    ky = np.fft.fftfreq(ny, 1.0 / ny)[None, :, None]
+    kx = np.fft.rfftfreq(nx, 1.0 / nx)[None, None, :]
+    kk = np.sqrt(kx * kx + ky * ky + kz * kz)
+    mask = (kk >= kmin) & (kk <= kmax)
+    out = np.empty((ncomp, nz, ny, nx))
+    amp = np.where(mask, np.where(kk > 0, kk, 1.0) ** slope, 0.0)
+    for c in range(ncomp):
+        ph = rng.uniform(0.0, 2.0 * np.pi, size=kk.shape)
+        spec = amp * np.exp(1j * ph)
+        out[c] = np.fft.irfftn(spec, s=(nz, ny, nx), axes=(0, 1, 2))
+    return out, (kx, ky, kz, mask)
+
+
+def mhd_turbulence(n: int = 256, seed: int = 1, mach: float = 1.0, b0: float = 0.2,
+                   db_frac: float = 0.1, gamma: float = 5.0 / 3.0, limiter: str = "moncen",
+                   cfl: float = 0.5):
+    """3D ideal-MHD decaying turbulence on one periodic block.
+
+    rho = 1 + 1% white noise (seed); v from random-phase Fourier modes with
+    1 <= |k| <= 4, amplitude ~ k^-2 (seed+1), scaled to rms Mach ``mach`` for the
+    sound speed of p0 = 1/gamma (c_s = 1); B = (b0, 0, 0) + curl of a random
+    vector potential (seed+2) scaled to rms ``db_frac * b0``; psi = 0.
+    """
+    setup = Setup(n=(n, n, n), xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0),
+                  fluids=[("ion", gamma)], magnetic=True, limiter=limiter, limiter_b=limiter,
+                  cfl=cfl, cfl_glm=0.7, smalld=1.0e-3)
+    p0 = 1.0 / gamma
+    g = setup.guards
+    u, b, psi = _empty(setup)
+    shp = (n, n, n)
+    rho = 1.0 + 0.01 * _rng(seed).standard_normal((n, n, n))
+    v, _ = _fourier_field(shp, 1.0, 4.0, -2.0, _rng(seed + 1))
+    vrms = math.sqrt(float(np.mean(v[0] ** 2 + v[1] ** 2 + v[2] ** 2)))
+    v *= mach * 1.0 / vrms
+    a, (kx, ky, kz, mask) = _fourier_field(shp, 1.0, 4.0, -2.0, _rng(seed + 2))
+    # curl of A, spectrally
+    ah = [np.fft.rfftn(a[c]) for c in range(3)]
+    bh = [1j * (ky * ah[2] - kz * ah[1]), 1j * (kz * ah[0] - kx * ah[2]), 1j * (kx * ah[1] - ky * ah[0])]
+    db = np.stack([np.fft.irfftn(bh[c], s=shp, axes=(0, 1, 2)) for c in range(3)])
+    dbrms = math.sqrt(float(np.mean(db[0] ** 2 + db[1] ** 2 + db[2] ** 2)))
+    db *= db_frac * b0 / dbrms
+    bx, by, bz = b0 + db[0], db[1], db[2]
+    emag = 0.5 * (bx * bx + by * by + bz * bz)
+    sl = (slice(g[2], g[2] + n), slice(g[1], g[1] + n), slice(g[0], g[0] + n))
+    ui = u[sl]
+    _set_fluid(setup, ui, 0, rho, v[0], v[1], v[2], p0, emag)
+    b[sl + (0,)] = bx
+    b[sl + (1,)] = by
+    b[sl + (2,)] = bz
+    fill_periodic(setup, u)
+    fill_periodic(setup, b)
+    return setup, u, b, psi
+
+
+def orszag_tang(n: int = 512, seed: int = 1, amp: float = 1.0e-3, corr_cells: float = 8.0,
+                limiter: str = "vanleer"):
+    """2D Orszag-Tang vortex (problems/otvortex/initproblem.F90:99-166) on [0,1]^2
+    with a seeded Gaussian-random density perturbation (amplitude ``amp``,
+    Gaussian correlation length ``corr_cells`` cells)."""
+    gamma = 5.0 / 3.0
+    setup = Setup(n=(n, n, 1), xmin=(0.0, 0.0, -0.5), xmax=(1.0, 1.0, 0.5),
+                  fluids=[("ion", gamma)], magnetic=True, limiter=limiter, limiter_b=limiter,
+                  cfl=0.8, cfl_glm=0.7, smalld=1.0e-3, smallei=1.0e-5)
+    u, b, psi = _empty(setup)
+    x, y = _centres(setup, 0), _centres(setup, 1)
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    rho0 = 25.0 / (36.0 * math.pi)
+    pre = 5.0 / (12.0 * math.pi)
+    b0 = 1.0 / math.sqrt(4.0 * math.pi)
+    pert = gaussian_random_field((n, n), corr_cells, _rng(seed))
+    g = setup.guards
+    rho = np.full(X.shape, rho0)
+    rho[g[1]:g[1] + n, g[0]:g[0] + n] *= 1.0 + amp * pert
+    vx = -np.sin(2 * math.pi * Y)
+    vy = np.sin(2 * math.pi * X)
+    bx = b0 * vx
+    by = b0 * np.sin(4 * math.pi * X)
+    emag = 0.5 * (bx * bx + by * by)
+    _set_fluid(setup, u[0], 0, rho, vx, vy, 0.0, pre, emag)
+    b[0, ..., 0] = bx
+    b[0, ..., 1] = by
+    fill_periodic(setup, u)
+    fill_periodic(setup, b)
+    return setup, u, b, psi
+
+
+def gaussian_random_field(shape, corr_cells: float, rng: np.random.Generator) -> np.ndarray:
+    """Unit-rms periodic Gaussian random field with a Gaussian correlation kernel."""
+    w = rng.standard_normal(shape)
+    ks = np.meshgrid(*[np.fft.fftfreq(s) for s in shape], indexing="ij")
+    k2 = sum(k * k for k in ks)
+    f = np.fft.ifftn(np.fft.fftn(w) * np.exp(-2.0 * (math.pi ** 2) * (corr_cells ** 2) * k2)).real
+    f = f - f.mean()
+    return f / f.std()
+
+
+def random_state(setup: Setup, seed: int = 0, dv: float = 0.3, db: float = 0.3):
+    """Small random MHD/HD state for parity tests: smooth background plus noise,
+    positive density and pressure."""
+    rng = _rng(seed)
+    u, b, psi = _empty(setup)
+    g = setup.guards
+    sl = (slice(g[2], g[2] + setup.n[2]), slice(g[1], g[1] + setup.n[1]), slice(g[0], g[0] + setup.n[0]))
+    shp = (setup.n[2], setup.n[1], setup.n[0])
+    emag = None
+    if setup.magnetic:
+        bi = rng.uniform(-db, db, size=shp + (3,))
+        bi[..., 0] += 0.4
+        b[sl] = bi
+        emag = 0.5 * (bi ** 2).sum(-1)
+        psi[sl] = rng.uniform(-0.01, 0.01, size=shp)
+    for f, (kind, gam) in enumerate(setup.fluids):
+        rho = rng.uniform(0.5, 1.5, size=shp)
+        vel = rng.uniform(-dv, dv, size=shp + (3,))
+        p = rng.uniform(0.3, 1.0, size=shp)
+        _set_fluid(setup, u[sl], f, rho, vel[..., 0], vel[..., 1], vel[..., 2], p,
+                   emag if kind == "ion" else None)
+    fill_periodic(setup, u)
+    fill_periodic(setup, b)
+    fill_periodic(setup, psi)
+    return u, b, psi

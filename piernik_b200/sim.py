@@ -1,0 +1,209 @@
+"""Host-side mirror of the reference's interface for the split Riemann path.
+
+``Simulation`` owns one library handle and exposes the reference's routine
+names with their argument meaning:
+
+=====================  ==============================================================
+``solve_cg``            solve_cg_riemann(cg, ddim, istep)  src/scheme/Riemann_Solver/solve_cg_riemann.F90:68
+``update_boundaries``   update_boundaries                  src/scheme/sweeps.F90:66
+``sweep``               sweep(cdim)                        src/scheme/sweeps.F90:114
+``glmdamping``          glmdamping                         src/scheme/Riemann_Solver/hdc.F90:289
+``time_step``           time_step(dt, flind, .true.)       src/base/timestep.F90:112
+``fluid_update``        fluid_update -> fluid_update_full  src/scheme/fluidupdate.F90:60,99
+``run``                 main loop body                     src/base/piernik.F90:125-213
+=====================  ==============================================================
+
+Directions are 1-based (xdim=1, ydim=2, zdim=3) as in the reference.  Arrays
+use the reference's memory layout: a C-ordered numpy array ``u[k, j, i, v]`` is
+Fortran's ``cg%u(v, i, j, k)`` (guard cells included), ``b[k, j, i, d]`` is
+``cg%b(d, i, j, k)`` and ``psi[k, j, i]`` is ``cg%q(psi)%arr(i, j, k)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _lib as L
+from .config import Setup
+
+
+def _check(lib, h, rc, what):
+    if rc != L.PK_OK:
+        msg = lib.pk_last_error(h).decode() if h else ""
+        raise L.PkError(f"{what} failed: {L.ERRORS.get(rc, rc)} {msg}")
+
+
+def make_config(setup: Setup) -> L.PkConfig:
+    setup.validate()
+    lib = L.load()
+    c = L.PkConfig()
+    lib.pk_config_default(C.byref(c))
+    c.nfluids = len(setup.fluids)
+    for i, (kind, gam) in enumerate(setup.fluids):
+        c.fluid_kind[i] = L.PK_FLUID[kind]
+        c.gamma[i] = gam
+    c.magnetic = int(setup.magnetic)
+    c.limiter = L.PK_LIM[setup.limiter]
+    c.limiter_b = L.PK_LIM[setup.limiter_b]
+    c.use_smalld = int(setup.use_smalld)
+    c.use_smallei = int(setup.use_smallei)
+    c.disallow_negatives = int(setup.disallow_negatives)
+    c.smalld = setup.smalld
+    c.smallei = setup.smallei
+    c.cfl = setup.cfl
+    c.cfl_glm = setup.cfl_glm
+    c.glm_alpha = setup.glm_alpha
+    c.integration_order = setup.integration_order
+    c.nb = setup.nb
+    c.dt_initial = setup.dt_initial
+    c.dt_max_grow = setup.dt_max_grow
+    c.dt_min = setup.dt_min
+    c.dt_max = setup.dt_max
+    c.tend = setup.tend
+    for d in range(3):
+        c.skip_sweep[d] = int(setup.skip_sweep[d])
+    return c
+
+
+class Simulation:
+    """One device-resident block of a PIERNIK run, swept by the CUDA library."""
+
+    def __init__(self, setup: Setup):
+        self.setup = setup
+        self.lib = L.load()
+        cfg = make_config(setup)
+        h = C.c_void_p()
+        rc = self.lib.pk_create(C.byref(cfg), C.byref(h))
+        if rc != L.PK_OK:
+            raise L.PkError(f"pk_create failed: {L.ERRORS.get(rc, rc)}")
+        self.h = h
+        n = (C.c_int32 * 3)(*setup.n)
+        dl = (C.c_double * 3)(*setup.dl)
+        bnd = (C.c_int32 * 6)(*[setup.bnd[d][s] for d in range(3) for s in range(2)])
+        bid = C.c_int32()
+        self._chk(self.lib.pk_block_add(self.h, n, dl, bnd, C.byref(bid)), "pk_block_add")
+        self.block = bid.value
+
+    # -- plumbing ---------------------------------------------------------
+    def _chk(self, rc, what):
+        _check(self.lib, self.h, rc, what)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _shapes(self):
+        ez, ey, ex = self.setup.ext[2], self.setup.ext[1], self.setup.ext[0]
+        return (ez, ey, ex, self.setup.nvar), (ez, ey, ex, 3), (ez, ey, ex)
+
+    # -- state transfer ------------------------------------------------------
+    def upload(self, u: np.ndarray, b: Optional[np.ndarray] = None, psi: Optional[np.ndarray] = None,
+               layout: int = L.PK_LAYOUT_FORTRAN) -> None:
+        su, sb, sp = self._shapes()
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.size != int(np.prod(su)):
+            raise ValueError(f"u has {u.size} elements, expected {int(np.prod(su))}")
+        bp = pp = None
+        if self.setup.magnetic:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            psi = np.ascontiguousarray(psi, dtype=np.float64)
+            if b.size != int(np.prod(sb)) or psi.size != int(np.prod(sp)):
+                raise ValueError("b / psi have the wrong size")
+            bp, pp = b.ctypes.data, psi.ctypes.data
+        self._keep = (u, b, psi)
+        self._chk(self.lib.pk_upload(self.h, self.block, u.ctypes.data, bp, pp, layout), "pk_upload")
+        self.sync()
+
+    def download(self, layout: int = L.PK_LAYOUT_FORTRAN, out=None) -> Tuple[np.ndarray, Optional[np.ndarray], Optional[np.ndarray]]:
+        su, sb, sp = self._shapes()
+        if layout == L.PK_LAYOUT_SOA:
+            su = (su[3],) + su[:3]
+            sb = (3,) + sb[:3]
+        if out is None:
+            u = np.empty(su)
+            b = np.empty(sb) if self.setup.magnetic else None
+            psi = np.empty(sp) if self.setup.magnetic else None
+        else:
+            u, b, psi = out
+        self._chk(self.lib.pk_download(self.h, self.block, u.ctypes.data,
+                                       b.ctypes.data if b is not None else None,
+                                       psi.ctypes.data if psi is not None else None, layout), "pk_download")
+        return u, b, psi
+
+    def sync(self):
+        self._chk(self.lib.pk_sync(self.h), "pk_sync")
+
+    # -- the reference's routines ------------------------------------------
+    def solve_cg(self, ddim: int, istep: int, dt: float, chspeed: float = 0.0) -> None:
+        self._chk(self.lib.pk_solve_cg(self.h, self.block, ddim, istep, dt, chspeed), "pk_solve_cg")
+
+    def update_boundaries(self) -> None:
+        self._chk(self.lib.pk_fill_guards(self.h), "pk_fill_guards")
+
+    def sweep(self, cdim: int, dt: float, chspeed: float = 0.0) -> None:
+        self._chk(self.lib.pk_sweep(self.h, cdim, dt, chspeed), "pk_sweep")
+
+    def glmdamping(self, fac: float) -> None:
+        self._chk(self.lib.pk_glm_damp(self.h, fac), "pk_glm_damp")
+
+    def timestep_raw(self) -> Tuple[float, float]:
+        dt, c = C.c_double(), C.c_double()
+        self._chk(self.lib.pk_timestep_raw(self.h, C.byref(dt), C.byref(c)), "pk_timestep_raw")
+        return dt.value, c.value
+
+    def time_step(self) -> float:
+        dt = C.c_double()
+        self._chk(self.lib.pk_time_step(self.h, C.byref(dt)), "pk_time_step")
+        return dt.value
+
+    def fluid_update(self) -> None:
+        self._chk(self.lib.pk_fluid_update(self.h), "pk_fluid_update")
+
+    def run(self, nsteps: int) -> None:
+        self._chk(self.lib.pk_run(self.h, nsteps), "pk_run")
+
+    @property
+    def time_state(self) -> L.PkTimeState:
+        st = L.PkTimeState()
+        self._chk(self.lib.pk_get_time_state(self.h, C.byref(st)), "pk_get_time_state")
+        return st
+
+    @time_state.setter
+    def time_state(self, st: L.PkTimeState) -> None:
+        self._chk(self.lib.pk_set_time_state(self.h, C.byref(st)), "pk_set_time_state")
+
+    def status(self) -> int:
+        s = C.c_uint32()
+        self._chk(self.lib.pk_status(self.h, C.byref(s)), "pk_status")
+        return s.value
+
+    def profile(self, on: bool = True) -> None:
+        self._chk(self.lib.pk_profile_enable(self.h, int(on)), "pk_profile_enable")
+
+    def profile_read(self):
+        """(kernel launches since creation, sweep launches timed, their device ms)."""
+        a, b, ms = C.c_int64(), C.c_int64(), C.c_double()
+        self._chk(self.lib.pk_profile_read(self.h, C.byref(a), C.byref(b), C.byref(ms)), "pk_profile_read")
+        return a.value, b.value, ms.value
+
+    @property
+    def stream(self) -> int:
+        return self.lib.pk_stream(self.h) or 0
+
+    def set_tile(self, direction: int, pencils: int, length: int) -> None:
+        self._chk(self.lib.pk_set_tile(self.h, direction, pencils, length), "pk_set_tile")

@@ -1,0 +1,181 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+The bar is bit-for-bit equality: the kernels are built with --fmad=false and
+keep the reference's operation order, so every double must match the oracle's.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import assert_bitexact, interior, random_state, setup_for
+from piernik_b200 import problems
+from piernik_b200._lib import PK_EULER, PK_RK2_1, PK_RK2_2, PK_ST_DN_NEGATIVE
+from piernik_b200.config import BND_OUT, BND_PER, BND_REF
+from piernik_b200.sim import Simulation
+
+pytestmark = pytest.mark.gpu
+
+LIMS = ["vanleer", "minmod", "moncen", "superbee"]
+
+
+def both(setup, seed=0):
+    u, b, psi = random_state(setup, seed)
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    return ob, sim
+
+
+def compare(ob, sim, what, full=True):
+    u, b, psi = sim.download()
+    s = ob.setup
+    if full:
+        assert_bitexact(u, ob.u, what + " u")
+        if s.magnetic:
+            assert_bitexact(b, ob.b, what + " b")
+            assert_bitexact(psi, ob.psi, what + " psi")
+    else:
+        assert_bitexact(interior(s, u), interior(s, ob.u), what + " u")
+        if s.magnetic:
+            assert_bitexact(interior(s, b), interior(s, ob.b), what + " b")
+            assert_bitexact(interior(s, psi), interior(s, ob.psi), what + " psi")
+
+
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+@pytest.mark.parametrize("lim", LIMS)
+def test_solve_cg_stage_bitexact(gpu_lib, oracle_lib, phys, lim):
+    """pk_solve_cg == solve_cg_riemann for every direction and RK stage, guard cells included."""
+    s = setup_for(phys, n=(12, 10, 8), lim=lim, limb="moncen" if lim != "moncen" else "minmod")
+    ob, sim = both(s, seed=11)
+    dt, ch = 0.013, 1.7
+    for ddim in (1, 2, 3):
+        for istep, oi in ((PK_RK2_1, 1), (PK_RK2_2, 2)):
+            sim.solve_cg(ddim, istep, dt, ch)
+            ob.solve_cg(ddim - 1, oi, dt, ch)
+            compare(ob, sim, f"solve_cg d{ddim} s{istep}")
+
+
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+def test_solve_cg_euler(gpu_lib, oracle_lib, phys):
+    s = setup_for(phys, n=(10, 9, 7), lim="moncen", integration_order=1)
+    ob, sim = both(s, seed=3)
+    for ddim in (1, 2, 3):
+        sim.solve_cg(ddim, PK_EULER, 0.01, 1.2)
+        ob.solve_cg(ddim - 1, 1, 0.01, 1.2)
+        compare(ob, sim, f"euler d{ddim}")
+
+
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+@pytest.mark.parametrize("lim", LIMS)
+def test_fused_sweep_bitexact(gpu_lib, oracle_lib, phys, lim):
+    """The fused two-stage sweep of a periodic block equals stage/exchange/stage."""
+    s = setup_for(phys, n=(20, 14, 11), lim=lim)
+    ob, sim = both(s, seed=5)
+    dt, ch = 0.011, 1.3
+    for d in (0, 1, 2, 2, 1, 0):
+        sim.sweep(d + 1, dt, ch)
+        ob.sweep(d, dt, ch)
+    compare(ob, sim, "fused sweeps")
+
+
+@pytest.mark.parametrize("tile", [(1, 8), (3, 16), (4, 40), (2, 64), (8, 24)])
+def test_fused_tiles_agree(gpu_lib, oracle_lib, tile):
+    """Tile shapes (pencils per CTA, cells per chunk) do not change any bit."""
+    s = setup_for("mhd", n=(50, 37, 29), lim="moncen")
+    ob, sim = both(s, seed=9)
+    for d in range(3):
+        sim.set_tile(d, *tile)
+    dt, ch = 0.009, 1.1
+    for d in (0, 1, 2):
+        sim.sweep(d + 1, dt, ch)
+        ob.sweep(d, dt, ch)
+    compare(ob, sim, f"tile {tile}")
+
+
+def test_stage_path_long_pencil(gpu_lib, oracle_lib):
+    """Pencils longer than one CTA tile go through the chunked out-of-place stage."""
+    s = setup_for("mhd", n=(400, 6, 5), lim="vanleer", integration_order=1)
+    ob, sim = both(s, seed=2)
+    for ddim in (1, 2, 3):
+        sim.solve_cg(ddim, PK_EULER, 0.004, 1.0)
+        ob.solve_cg(ddim - 1, 1, 0.004, 1.0)
+    compare(ob, sim, "long pencil")
+
+
+@pytest.mark.parametrize("bnd", [BND_OUT, BND_REF])
+def test_nonperiodic_hd_sweeps(gpu_lib, oracle_lib, bnd):
+    """Outflow / reflecting boundaries take the stage + guard-refresh path."""
+    s = setup_for("hd", n=(16, 12, 10), lim="moncen", bnd=((bnd, bnd), (BND_PER, BND_PER), (bnd, BND_OUT)))
+    ob, sim = both(s, seed=4)
+    for d in (0, 1, 2, 2, 1, 0):
+        sim.sweep(d + 1, 0.01, 0.0)
+        ob.sweep(d, 0.01, 0.0)
+    compare(ob, sim, "non-periodic")
+
+
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+def test_timestep_raw_bitexact(gpu_lib, oracle_lib, phys):
+    s = setup_for(phys, n=(24, 17, 9), lim="vanleer")
+    ob, sim = both(s, seed=8)
+    dt_g, c_g = sim.timestep_raw()
+    dt_o, c_o = ob.timestep_raw()
+    assert dt_g == dt_o and c_g == c_o
+
+
+def run_pair(setup, u, b, psi, nsteps):
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    ob.run(nsteps)
+    sim.run(nsteps)
+    return ob, sim
+
+
+def test_run_sedov_hd_bitexact(gpu_lib, oracle_lib):
+    """Sedov blast (HLLC, van Leer, CFL 0.7), 10 pairs of steps through pk_run."""
+    setup, u, b, psi = problems.sedov(n=24)
+    ob, sim = run_pair(setup, u, b, psi, 10)
+    st = sim.time_state
+    assert st.nstep == ob.state.nstep == 10
+    assert st.t == ob.state.t and st.dt == ob.state.dt
+    compare(ob, sim, "sedov run")
+
+
+def test_run_mhd_turbulence_bitexact(gpu_lib, oracle_lib):
+    """Decaying MHD turbulence (HLLD + GLM, moncen, CFL 0.5), 10 pairs of steps."""
+    setup, u, b, psi = problems.mhd_turbulence(n=20, seed=3)
+    ob, sim = run_pair(setup, u, b, psi, 10)
+    st = sim.time_state
+    assert st.t == ob.state.t and st.dt == ob.state.dt and st.chspeed == ob.state.chspeed
+    compare(ob, sim, "mhd run")
+
+
+def test_run_orszag_tang_2d_bitexact(gpu_lib, oracle_lib):
+    """2D run (no z extent, so no z sweep and no z guard cells)."""
+    setup, u, b, psi = problems.orszag_tang(n=32, seed=1)
+    ob, sim = run_pair(setup, u, b, psi, 8)
+    compare(ob, sim, "orszag-tang")
+
+
+def test_status_flags_negative_density(gpu_lib, oracle_lib):
+    """A negative density is reported through pk_status, never by a trap."""
+    s = setup_for("hd", n=(8, 8, 8), lim="minmod")
+    u, b, psi = random_state(s, seed=1)
+    g = s.guards
+    u[g[2] + 3, g[1] + 3, g[0] + 3, 0] = -0.2
+    sim = Simulation(s)
+    sim.upload(u, b, psi)
+    sim.sweep(1, 0.001, 0.0)
+    assert sim.status() & PK_ST_DN_NEGATIVE
+    assert sim.status() == 0
+
+
+def test_soa_layout_roundtrip(gpu_lib):
+    s = setup_for("mhd", n=(9, 8, 7))
+    u, b, psi = random_state(s, seed=6)
+    sim = Simulation(s)
+    sim.upload(u, b, psi)
+    su, sb, sp = sim.download(layout=1)
+    assert_bitexact(np.moveaxis(su, 0, -1), u, "soa u")
+    assert_bitexact(np.moveaxis(sb, 0, -1), b, "soa b")
+    assert_bitexact(sp, psi, "soa psi")
