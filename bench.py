@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--tune-log", default=None)
     return p.parse_args()
 
 
@@ -178,6 +180,15 @@ def our_arm(args):
     sim = Simulation(setup)
     sim.upload(u, b, psi)
     stream = torch.cuda.ExternalStream(sim.stream)
+    tiles = None
+    if not args.no_autotune:
+        from piernik_b200.autotune import autotune
+        log = open(args.tune_log, "w") if (args.tune_log and rank == 0) else None
+        best = autotune(sim, reps=2, verbose=False)
+        tiles = {"xyz"[d]: [v["P"], v["L"], v["V"], round(v["ms"], 4)] for d, v in best.items()}
+        if log:
+            json.dump(best, log, indent=1)
+            log.close()
 
     def barrier():
         torch.cuda.synchronize()
@@ -266,7 +277,8 @@ def our_arm(args):
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": dict(workload_config(n), parallelism=f"replicas{world}"),
+               "config": dict(workload_config(n), parallelism=f"replicas{world}",
+                              tiles_P_L_variant_ms=tiles),
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": launches1 - launches0, "clocks": ck,
                "adjoint_cost_ratio": None}

@@ -145,9 +145,14 @@ int pk_status(pk_handle h, uint32_t* flags);
 int pk_sync(pk_handle h);
 
 /* Tile shape of the fused sweep for direction d (0..2): P pencils per CTA,
- * L output cells per pencil (the CTA also computes a 4-cell halo each side).
- * Used by the autotuner; 0 keeps the built-in choice. */
-int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length);
+ * L output cells per pencil (the CTA also computes a 4-cell halo each side),
+ * and the launch-bound variant (register budget) of the kernel, -1 for the
+ * default.  Used by the autotuner; 0 keeps the built-in P / L. */
+int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32_t variant);
+
+/* Launch-bound variants of the fused sweep: count, CTA size and CTAs per SM
+ * each was compiled for (arrays of at least 16 entries). */
+int pk_tile_variants(int32_t* n, int32_t* threads, int32_t* ctas_per_sm);
 
 /* CUDA stream of the handle (cudaStream_t), for callers that interleave work. */
 void* pk_stream(pk_handle h);

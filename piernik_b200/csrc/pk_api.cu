@@ -23,7 +23,14 @@ using PhMHD1 = Phys<K_ION, K_NONE, K_NONE, true>;    // ionized fluid + B + psi 
 
 enum PhysId { PHYS_HD1 = 0, PHYS_MHD1 = 1 };
 
-constexpr int MAXT = 320;          // threads per CTA of the sweep kernels
+constexpr int MAXT = 320;          // threads per CTA of the stage kernel
+// Launch-bound variants of the fused sweep (threads per CTA, CTAs per SM): the
+// register budget the compiler may use is 65536 / (threads * CTAs); tighter
+// budgets trade spills for resident warps.  The autotuner picks per direction.
+constexpr int NVARIANT = 6;
+constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192};
+constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2};
+constexpr int DEF_VARIANT[3] = {0, 0, 0};
 constexpr int DEF_P[3] = {2, 4, 4};
 constexpr int DEF_L[3] = {64, 64, 64};
 // ORTHO pairs with the memory-fastest ortho direction first (lanes/coalescing)
@@ -58,7 +65,7 @@ struct pk_ctx {
     int red_cap = 0;
     pk_time_state ts;
     std::string err;
-    int tileP[3] = {0, 0, 0}, tileL[3] = {0, 0, 0};
+    int tileP[3] = {0, 0, 0}, tileL[3] = {0, 0, 0}, tileV[3] = {-1, -1, -1};
     long long launches = 0;          // kernels of this library launched on the handle's stream
     long long sweep_launches = 0;    // of which sweep kernels (fused or stage)
     bool profiling = false;          // bracket sweep kernels with CUDA events
@@ -134,11 +141,28 @@ static Geom make_geom(const Block& b, int dir)
 }
 
 template <class PH>
+using FusedFn = void (*)(Geom, Tile, const double*, double*, PhysParams, double, double, double, double, unsigned*);
+
+template <class PH>
+static FusedFn<PH> fused_variant(int v)
+{
+    switch (v) {
+    case 0: return k_sweep_fused<PH, 320, 1>;
+    case 1: return k_sweep_fused<PH, 256, 1>;
+    case 2: return k_sweep_fused<PH, 256, 2>;
+    case 3: return k_sweep_fused<PH, 128, 3>;
+    case 4: return k_sweep_fused<PH, 128, 4>;
+    default: return k_sweep_fused<PH, 192, 2>;
+    }
+}
+
+template <class PH>
 static int set_smem_attr(pk_ctx* h)
 {
     static bool done = false;
     if (!done) {
-        PK_CUDA(h, cudaFuncSetAttribute(k_sweep_fused<PH, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        for (int v = 0; v < NVARIANT; ++v)
+            PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         done = true;
     }
@@ -155,22 +179,24 @@ static int launch_fused(pk_ctx* h, Block& b, int dir, double dt, double ch, doub
     if (L > b.n[dir]) L = b.n[dir];
     int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
     if (P > g.n1) P = g.n1;
+    const int var = h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir];
+    const int maxt = VAR_T[var];
     int T = L + 8;
-    while (P * T > MAXT && P > 1) --P;
-    if (P * T > MAXT) return fail(h, PK_E_ARG, "fused sweep tile too long: L + 8 must be <= 320");
+    while (P * T > maxt && P > 1) --P;
+    if (P * T > maxt) return fail(h, PK_E_ARG, "fused sweep tile longer than the variant's CTA size");
     tl.P = P;
     tl.T = T;
     tl.L = L;
     tl.halo = 4;
     tl.xfast = (dir == 0);
     dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
-    size_t smem = 2ull * PH::NV * P * T * sizeof(double);
+    size_t smem = 3ull * PH::NV * P * T * sizeof(double);
     const double dtodx1 = (0.5 * dt) / b.dl[dir];   // rk_coef(RK2_1) * dt / dl
     const double dtodx2 = (1.0 * dt) / b.dl[dir];   // rk_coef(RK2_2) * dt / dl
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    k_sweep_fused<PH, MAXT><<<grid, P * T, smem, h->stream>>>(g, tl, b.u, b.tmp, h->pp, dtodx1, dtodx2, ch, psi_fac,
-                                                             h->d_status);
+    fused_variant<PH>(var)<<<grid, P * T, smem, h->stream>>>(g, tl, b.u, b.tmp, h->pp, dtodx1, dtodx2, ch, psi_fac,
+                                                            h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
@@ -206,7 +232,7 @@ static int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, d
     }
     tl.xfast = (dir == 0);
     dim3 grid((g.n1 + tl.P - 1) / tl.P, (ext + tl.L - 1) / tl.L, g.n2);
-    size_t smem = 2ull * PH::NV * tl.P * tl.T * sizeof(double);
+    size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
     k_stage<PH, MAXT><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, b.u, uout, b.uh, h->pp, first, dtodx, ch,
@@ -761,12 +787,24 @@ int pk_sync(pk_handle h)
     return PK_OK;
 }
 
-int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length)
+int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32_t variant)
 {
-    if (!h || dir < 0 || dir > 2 || pencils < 0 || length < 0) return PK_E_ARG;
-    if (length > 0 && length + 8 > MAXT) return fail(h, PK_E_ARG, "length + 8 must be <= 320");
+    if (!h || dir < 0 || dir > 2 || pencils < 0 || length < 0 || variant < -1 || variant >= NVARIANT) return PK_E_ARG;
+    const int maxt = VAR_T[variant >= 0 ? variant : DEF_VARIANT[dir]];
+    if (length > 0 && length + 8 > maxt) return fail(h, PK_E_ARG, "length + 8 exceeds the variant's CTA size");
     h->tileP[dir] = pencils;
     h->tileL[dir] = length;
+    h->tileV[dir] = variant;
+    return PK_OK;
+}
+
+int pk_tile_variants(int32_t* n, int32_t* threads, int32_t* ctas_per_sm)
+{
+    if (n) *n = NVARIANT;
+    for (int v = 0; v < NVARIANT; ++v) {
+        if (threads) threads[v] = VAR_T[v];
+        if (ctas_per_sm) ctas_per_sm[v] = VAR_B[v];
+    }
     return PK_OK;
 }
 

@@ -138,14 +138,35 @@ PK_DEV double slope_end(int lim, double d)
 // bf: transverse B fluxes.
 // -------------------------------------------------------------------------
 
+// Physical flux of one side (hlld.F90:296-308): fluid part f[0..nc) and the
+// transverse B fluxes bf[1..2].  Computed where needed so that neither side's
+// flux is held in registers through the star-state algebra.
+PK_DEV void side_flux(bool has_energy, const double* u, const double* b, double pr, double en, double* f)
+{
+    f[0] = u[0] * u[1];
+    f[1] = ((u[0] * (u[1] * u[1])) + pr) - (b[0] * b[0]);
+    f[2] = ((u[0] * u[2]) * u[1]) - (b[0] * b[1]);
+    f[3] = ((u[0] * u[3]) * u[1]) - (b[0] * b[2]);
+    if (has_energy) f[4] = ((en + pr) * u[1]) - (b[0] * ((u[1] * b[0] + u[2] * b[1]) + u[3] * b[2]));
+}
+
+PK_DEV double side_bflux(const double* u, const double* b, int c)
+{
+    return (b[c] * u[1]) - (b[0] * u[1 + c]);     // b_cclf(ydim:zdim), hlld.F90:301,309
+}
+
+// [ u(idn), u(idn)*u(imx:imz), en ] of one side
+PK_DEV double side_cons(const double* u, double en, int c)
+{
+    return c == 0 ? u[0] : (c == 4 ? en : u[0] * u[c]);
+}
+
 PK_DEV void hlld_iface(bool has_energy, double gamma, const double* ul, const double* ur, const double* bl,
                        const double* br, double* f, double* bf)
 {
-    double fl[5], fr[5], usl[5], usr[5], u2l[5], u2r[5];
-    double vsl[3], vsr[3], v2[3], bsl[3], bsr[3], b2[3], bclf[3], bcrf[3];
+    const int nc = has_energy ? 5 : 4;
     double prl, prr, c_fastm;
     double enl = 1.7976931348623157e308, enr = 1.7976931348623157e308, ue = 0.0;
-    const int nc = has_energy ? 5 : 4;
 
     const double magprl = 0.5 * ((bl[0] * bl[0] + bl[1] * bl[1]) + bl[2] * bl[2]);   // hlld.F90:239-240
     const double magprr = 0.5 * ((br[0] * br[0] + br[1] * br[1]) + br[2] * br[2]);
@@ -154,7 +175,7 @@ PK_DEV void hlld_iface(bool has_energy, double gamma, const double* ul, const do
         prr = 0.0;
         c_fastm = 0.0;
     } else {
-        prl = ul[4] + magprl;
+        prl = ul[4] + magprl;                                                         // :258-259
         prr = ur[4] + magprr;
         const double bbl = (bl[0] * bl[0] + bl[1] * bl[1]) + bl[2] * bl[2];
         const double bbr = (br[0] * br[0] + br[1] * br[1]) + br[2] * br[2];
@@ -170,35 +191,13 @@ PK_DEV void hlld_iface(bool has_energy, double gamma, const double* ul, const do
     const double sl = f_min(ul[1], ur[1]) - c_fastm;                                // :291-292
     const double sr = f_max(ul[1], ur[1]) + c_fastm;
 
-    fl[0] = ul[0] * ul[1];                                                           // :296-300
-    fl[1] = ((ul[0] * (ul[1] * ul[1])) + prl) - (bl[0] * bl[0]);
-    fl[2] = ((ul[0] * ul[2]) * ul[1]) - (bl[0] * bl[1]);
-    fl[3] = ((ul[0] * ul[3]) * ul[1]) - (bl[0] * bl[2]);
-    if (has_energy) fl[4] = ((enl + prl) * ul[1]) - (bl[0] * ((ul[1] * bl[0] + ul[2] * bl[1]) + ul[3] * bl[2]));
-    bclf[1] = (bl[1] * ul[1]) - (bl[0] * ul[2]);
-    bclf[2] = (bl[2] * ul[1]) - (bl[0] * ul[3]);
-    fr[0] = ur[0] * ur[1];                                                           // :304-308
-    fr[1] = ((ur[0] * (ur[1] * ur[1])) + prr) - (br[0] * br[0]);
-    fr[2] = ((ur[0] * ur[2]) * ur[1]) - (br[0] * br[1]);
-    fr[3] = ((ur[0] * ur[3]) * ur[1]) - (br[0] * br[2]);
-    if (has_energy) fr[4] = ((enr + prr) * ur[1]) - (br[0] * ((ur[1] * br[0] + ur[2] * br[1]) + ur[3] * br[2]));
-    bcrf[1] = (br[1] * ur[1]) - (br[0] * ur[2]);
-    bcrf[2] = (br[2] * ur[1]) - (br[0] * ur[3]);
-
-    if (sl >= 0.0) {                                                                 // :312-315
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            if (c < nc) f[c] = fl[c];
-        bf[0] = bclf[1];
-        bf[1] = bclf[2];
-        return;
-    }
-    if (sr <= 0.0) {                                                                 // :316-319
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            if (c < nc) f[c] = fr[c];
-        bf[0] = bcrf[1];
-        bf[1] = bcrf[2];
+    if (sl >= 0.0 || sr <= 0.0) {                                                    // :312-319
+        const bool left = sl >= 0.0;
+        const double* u = left ? ul : ur;
+        const double* b = left ? bl : br;
+        side_flux(has_energy, u, b, left ? prl : prr, left ? enl : enr, f);
+        bf[0] = side_bflux(u, b, 1);
+        bf[1] = side_bflux(u, b, 2);
         return;
     }
 
@@ -217,150 +216,154 @@ PK_DEV void hlld_iface(bool has_energy, double gamma, const double* ul, const do
     const double b_lrgam = b_lr / gamma;
     const double prt_star = 0.5 * ((prl + dn_l * (sm - ul[1])) + (prr + dn_r * (sm - ur[1])));
 
-    vsl[0] = sm;                                                                     // :354-358
-    vsr[0] = sm;
+    // transverse B of the star states, with the HLL fallback (:362-378)
+    double bsl[3], bsr[3];
     bsl[0] = bl[0];
     bsr[0] = br[0];
-
-    double coeff_1 = dn_l * slsm - b_lr;                                             // :362-369
-    if (has_energy) ue = ul[4];
-    if ((fabs(coeff_1) > f_spacing(b_lr)) && b_lrgam <= ue) {
-        const double a = dn_l * slvxl - b_lr;
-        bsl[1] = (bl[1] * a) / coeff_1;
-        bsl[2] = (bl[2] * a) / coeff_1;
-    } else {
-        bsl[1] = ((sr * br[1] - sl * bl[1]) - (bcrf[1] - bclf[1])) / srmsl;
-        bsl[2] = ((sr * br[2] - sl * bl[2]) - (bcrf[2] - bclf[2])) / srmsl;
+    {
+        const double bclf1 = side_bflux(ul, bl, 1), bclf2 = side_bflux(ul, bl, 2);
+        const double bcrf1 = side_bflux(ur, br, 1), bcrf2 = side_bflux(ur, br, 2);
+        double coeff_1 = dn_l * slsm - b_lr;
+        if (has_energy) ue = ul[4];
+        if ((fabs(coeff_1) > f_spacing(b_lr)) && b_lrgam <= ue) {
+            const double a = dn_l * slvxl - b_lr;
+            bsl[1] = (bl[1] * a) / coeff_1;
+            bsl[2] = (bl[2] * a) / coeff_1;
+        } else {
+            bsl[1] = ((sr * br[1] - sl * bl[1]) - (bcrf1 - bclf1)) / srmsl;
+            bsl[2] = ((sr * br[2] - sl * bl[2]) - (bcrf2 - bclf2)) / srmsl;
+        }
+        coeff_1 = dn_r * srsm - b_lr;
+        if (has_energy) ue = ur[4];
+        if ((fabs(coeff_1) > f_spacing(b_lr)) && b_lrgam <= ue) {
+            const double a = dn_r * srvxr - b_lr;
+            bsr[1] = (br[1] * a) / coeff_1;
+            bsr[2] = (br[2] * a) / coeff_1;
+        } else {
+            bsr[1] = ((sr * br[1] - sl * bl[1]) - (bcrf1 - bclf1)) / srmsl;
+            bsr[2] = ((sr * br[2] - sl * bl[2]) - (bcrf2 - bclf2)) / srmsl;
+        }
     }
-    coeff_1 = dn_r * srsm - b_lr;                                                    // :371-378
-    if (has_energy) ue = ur[4];
-    if ((fabs(coeff_1) > f_spacing(b_lr)) && b_lrgam <= ue) {
-        const double a = dn_r * srvxr - b_lr;
-        bsr[1] = (br[1] * a) / coeff_1;
-        bsr[2] = (br[2] * a) / coeff_1;
-    } else {
-        bsr[1] = ((sr * br[1] - sl * bl[1]) - (bcrf[1] - bclf[1])) / srmsl;
-        bsr[2] = ((sr * br[2] - sl * bl[2]) - (bcrf[2] - bclf[2])) / srmsl;
-    }
-    {                                                                                // :381-382
+    double vsl[3], vsr[3];                                                           // :354-355, :381-382
+    vsl[0] = sm;
+    vsr[0] = sm;
+    {
         const double bxl_dnl = bl[0] / dn_l, bxr_dnr = br[0] / dn_r;
         vsl[1] = ul[2] + (bxl_dnl * (bl[1] - bsl[1]));
         vsl[2] = ul[3] + (bxl_dnl * (bl[2] - bsl[2]));
         vsr[1] = ur[2] + (bxr_dnr * (br[1] - bsr[1]));
         vsr[2] = ur[3] + (bxr_dnr * (br[2] - bsr[2]));
     }
-    const double vb_l = (ul[1] * bl[0] + ul[2] * bl[1]) + ul[3] * bl[2];             // :386-389
-    const double vb_r = (ur[1] * br[0] + ur[2] * br[1]) + ur[3] * br[2];
-    const double vb_starl = (vsl[0] * bsl[0] + vsl[1] * bsl[1]) + vsl[2] * bsl[2];
+    const double vb_starl = (vsl[0] * bsl[0] + vsl[1] * bsl[1]) + vsl[2] * bsl[2];  // :388-389
     const double vb_starr = (vsr[0] * bsr[0] + vsr[1] * bsr[1]) + vsr[2] * bsr[2];
 
-    usl[0] = dn_l / slsm;                                                            // :393-399
-    usl[1] = usl[0] * vsl[0];
-    usl[2] = usl[0] * vsl[1];
-    usl[3] = usl[0] * vsl[2];
+    double usl[5], usr[5];                                                           // :393-404
+    usl[0] = dn_l / slsm;
     usr[0] = dn_r / srsm;
-    usr[1] = usr[0] * vsr[0];
-    usr[2] = usr[0] * vsr[1];
-    usr[3] = usr[0] * vsr[2];
-    if (has_energy) {                                                                // :403-404
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        usl[1 + c] = usl[0] * vsl[c];
+        usr[1 + c] = usr[0] * vsr[c];
+    }
+    if (has_energy) {
+        const double vb_l = (ul[1] * bl[0] + ul[2] * bl[1]) + ul[3] * bl[2];
+        const double vb_r = (ur[1] * br[0] + ur[2] * br[1]) + ur[3] * br[2];
         usl[4] = ((((slvxl * enl) - (prl * ul[1])) + (prt_star * sm)) + (bl[0] * (vb_l - vb_starl))) / slsm;
         usr[4] = ((((srvxr * enr) - (prr * ur[1])) + (prt_star * sm)) + (br[0] * (vb_r - vb_starr))) / srsm;
     }
-    double ucl[5], ucr[5];                        // [ u(idn), u(idn)*u(imx:imz), en ]
-    ucl[0] = ul[0];
-    ucr[0] = ur[0];
+
+    // flux through the outer (star) state of one side: fl + s*(u_star - u) (Eq. 64)
+    auto star_flux = [&](bool left, double* out, double* bout) {
+        const double* u = left ? ul : ur;
+        const double* b = left ? bl : br;
+        const double* us = left ? usl : usr;
+        const double* bs = left ? bsl : bsr;
+        const double s = left ? sl : sr;
+        const double en = left ? enl : enr;
+        double fs[5];
+        side_flux(has_energy, u, b, left ? prl : prr, en, fs);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        ucl[1 + c] = ul[0] * ul[1 + c];
-        ucr[1 + c] = ur[0] * ur[1 + c];
-    }
-    ucl[4] = enl;
-    ucr[4] = enr;
+        for (int c = 0; c < 5; ++c)
+            if (c < nc) out[c] = fs[c] + s * (us[c] - side_cons(u, en, c));
+        bout[0] = side_bflux(u, b, 1) + s * (bs[1] - b[1]);
+        bout[1] = side_bflux(u, b, 2) + s * (bs[2] - b[2]);
+    };
 
     if (fabs(bl[0]) > 0.0) {                                                         // :410
         const double dn_lsqt = sqrt(usl[0]);                                        // :414-418
         const double dn_rsqt = sqrt(usr[0]);
         const double alfven_l = sm - fabs(bl[0]) / dn_lsqt;
         const double alfven_r = sm + fabs(br[0]) / dn_rsqt;
-        if (alfven_l > 0.0) {                                                        // :422-434
+        if (alfven_l > 0.0 || alfven_r < 0.0) {                                      // :422-448
+            star_flux(alfven_l > 0.0, f, bf);
+            return;
+        }
+        const double b_sig = (bl[0] >= 0.0) ? 1.0 : -1.0;                            // :452-456
+        const double add_dnsq = dn_lsqt + dn_rsqt;                                   // :460-461
+        const double mul_dnsq = dn_lsqt * dn_rsqt;
+        double v2[3], b2[3];                                                         // :465-470
+        v2[0] = sm;
+        v2[1] = ((dn_lsqt * vsl[1] + dn_rsqt * vsr[1]) + b_sig * (bsr[1] - bsl[1])) / add_dnsq;
+        v2[2] = ((dn_lsqt * vsl[2] + dn_rsqt * vsr[2]) + b_sig * (bsr[2] - bsl[2])) / add_dnsq;
+        b2[0] = 0.5 * (bl[0] + br[0]);
+        const double bsm = b_sig * mul_dnsq;
+        b2[1] = ((dn_lsqt * bsr[1] + dn_rsqt * bsl[1]) + bsm * (vsr[1] - vsl[1])) / add_dnsq;
+        b2[2] = ((dn_lsqt * bsr[2] + dn_rsqt * bsl[2]) + bsm * (vsr[2] - vsl[2])) / add_dnsq;
+        const double vb_2star = (v2[0] * b2[0] + v2[1] * b2[1]) + v2[2] * b2[2];   // :474
+
+        // flux through the Alfven (2-star) state of one side (Eq. 65, :478-522)
+        auto alfven_flux = [&](bool left, double* out, double* bout) {
+            const double* u = left ? ul : ur;
+            const double* b = left ? bl : br;
+            const double* us = left ? usl : usr;
+            const double* bs = left ? bsl : bsr;
+            const double s = left ? sl : sr;
+            const double en = left ? enl : enr;
+            const double a = left ? alfven_l : alfven_r;
+            double u2[5], fs[5];
+            u2[0] = us[0];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) u2[1 + c] = us[0] * v2[c];
+            if (has_energy)
+                u2[4] = left ? us[4] - (b_sig * dn_lsqt) * (vb_starl - vb_2star)
+                             : us[4] + (b_sig * dn_rsqt) * (vb_starr - vb_2star);
+            side_flux(has_energy, u, b, left ? prl : prr, en, fs);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                if (c < nc) f[c] = fl[c] + sl * (usl[c] - ucl[c]);
-            bf[0] = bclf[1] + sl * (bsl[1] - bl[1]);
-            bf[1] = bclf[2] + sl * (bsl[2] - bl[2]);
-        } else if (alfven_r < 0.0) {                                                 // :436-448
+                if (c < nc) out[c] = ((fs[c] + a * u2[c]) - (a - s) * us[c]) - s * side_cons(u, en, c);
+#pragma unroll
+            for (int c = 1; c < 3; ++c)
+                bout[c - 1] = ((side_bflux(u, b, c) + a * b2[c]) - (a - s) * bs[c]) - s * b[c];
+        };
+        if (sm > 0.0 || sm < 0.0) {                                                  // :496-522
+            alfven_flux(sm > 0.0, f, bf);
+        } else {                                                                     // :524-544
+            double fl2[5], fr2[5], bl2[2], br2[2];
+            alfven_flux(true, fl2, bl2);
+            alfven_flux(false, fr2, br2);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                if (c < nc) f[c] = fr[c] + sr * (usr[c] - ucr[c]);
-            bf[0] = bcrf[1] + sr * (bsr[1] - br[1]);
-            bf[1] = bcrf[2] + sr * (bsr[2] - br[2]);
-        } else {
-            const double b_sig = (bl[0] >= 0.0) ? 1.0 : -1.0;                        // :452-456
-            const double add_dnsq = dn_lsqt + dn_rsqt;                               // :460-461
-            const double mul_dnsq = dn_lsqt * dn_rsqt;
-            v2[0] = sm;                                                              // :465-470
-            v2[1] = ((dn_lsqt * vsl[1] + dn_rsqt * vsr[1]) + b_sig * (bsr[1] - bsl[1])) / add_dnsq;
-            v2[2] = ((dn_lsqt * vsl[2] + dn_rsqt * vsr[2]) + b_sig * (bsr[2] - bsl[2])) / add_dnsq;
-            b2[0] = 0.5 * (bl[0] + br[0]);
-            const double bsm = b_sig * mul_dnsq;
-            b2[1] = ((dn_lsqt * bsr[1] + dn_rsqt * bsl[1]) + bsm * (vsr[1] - vsl[1])) / add_dnsq;
-            b2[2] = ((dn_lsqt * bsr[2] + dn_rsqt * bsl[2]) + bsm * (vsr[2] - vsl[2])) / add_dnsq;
-            const double vb_2star = (v2[0] * b2[0] + v2[1] * b2[1]) + v2[2] * b2[2];  // :474
-            if (sm >= 0.0) {                                                         // :478-485
-                u2l[0] = usl[0];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) u2l[1 + c] = usl[0] * v2[c];
-                if (has_energy) u2l[4] = usl[4] - (b_sig * dn_lsqt) * (vb_starl - vb_2star);
-            }
-            if (sm <= 0.0) {                                                         // :487-494
-                u2r[0] = usr[0];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) u2r[1 + c] = usr[0] * v2[c];
-                if (has_energy) u2r[4] = usr[4] + (b_sig * dn_rsqt) * (vb_starr - vb_2star);
-            }
-            if (sm > 0.0) {                                                          // :496-508
-#pragma unroll
-                for (int c = 0; c < 5; ++c)
-                    if (c < nc) f[c] = ((fl[c] + alfven_l * u2l[c]) - (alfven_l - sl) * usl[c]) - sl * ucl[c];
-                bf[0] = ((bclf[1] + alfven_l * b2[1]) - (alfven_l - sl) * bsl[1]) - sl * bl[1];
-                bf[1] = ((bclf[2] + alfven_l * b2[2]) - (alfven_l - sl) * bsl[2]) - sl * bl[2];
-            } else if (sm < 0.0) {                                                   // :510-522
-#pragma unroll
-                for (int c = 0; c < 5; ++c)
-                    if (c < nc) f[c] = ((fr[c] + alfven_r * u2r[c]) - (alfven_r - sr) * usr[c]) - sr * ucr[c];
-                bf[0] = ((bcrf[1] + alfven_r * b2[1]) - (alfven_r - sr) * bsr[1]) - sr * br[1];
-                bf[1] = ((bcrf[2] + alfven_r * b2[2]) - (alfven_r - sr) * bsr[2]) - sr * br[2];
-            } else {                                                                 // :524-544
-#pragma unroll
-                for (int c = 0; c < 5; ++c)
-                    if (c < nc)
-                        f[c] = 0.5 * ((((fl[c] + alfven_l * u2l[c]) - (alfven_l - sl) * usl[c]) - sl * ucl[c]) +
-                                      (((fr[c] + alfven_r * u2r[c]) - (alfven_r - sr) * usr[c]) - sr * ucr[c]));
-#pragma unroll
-                for (int c = 1; c < 3; ++c)
-                    bf[c - 1] = 0.5 * ((((bclf[c] + alfven_l * b2[c]) - (alfven_l - sl) * bsl[c]) - sl * bl[c]) +
-                                       (((bcrf[c] + alfven_r * b2[c]) - (alfven_r - sr) * bsr[c]) - sr * br[c]));
-            }
+                if (c < nc) f[c] = 0.5 * (fl2[c] + fr2[c]);
+            bf[0] = 0.5 * (bl2[0] + br2[0]);
+            bf[1] = 0.5 * (bl2[1] + br2[1]);
         }
     } else {                                                                         // :548-599, B_x = 0
-        if (sm > 0.0) {
-#pragma unroll
-            for (int c = 0; c < 5; ++c)
-                if (c < nc) f[c] = fl[c] + sl * (usl[c] - ucl[c]);
-            bf[0] = bclf[1] + sl * (bsl[1] - bl[1]);
-            bf[1] = bclf[2] + sl * (bsl[2] - bl[2]);
-        } else if (sm < 0.0) {
-#pragma unroll
-            for (int c = 0; c < 5; ++c)
-                if (c < nc) f[c] = fr[c] + sr * (usr[c] - ucr[c]);
-            bf[0] = bcrf[1] + sr * (bsr[1] - br[1]);
-            bf[1] = bcrf[2] + sr * (bsr[2] - br[2]);
+        if (sm > 0.0 || sm < 0.0) {
+            star_flux(sm > 0.0, f, bf);
         } else {
+            // half * (fl + sl*(usl-ucl) + fr + sr*(usr-ucr)), summed left to right
+            double fsl[5], fsr[5];
+            side_flux(has_energy, ul, bl, prl, enl, fsl);
+            side_flux(has_energy, ur, br, prr, enr, fsr);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                if (c < nc) f[c] = 0.5 * (((fl[c] + sl * (usl[c] - ucl[c])) + fr[c]) + sr * (usr[c] - ucr[c]));
-            bf[0] = 0.5 * (((bclf[1] + sl * (bsl[1] - bl[1])) + bcrf[1]) + sr * (bsr[1] - br[1]));
-            bf[1] = 0.5 * (((bclf[2] + sl * (bsl[2] - bl[2])) + bcrf[2]) + sr * (bsr[2] - br[2]));
+                if (c < nc)
+                    f[c] = 0.5 * (((fsl[c] + sl * (usl[c] - side_cons(ul, enl, c))) + fsr[c]) +
+                                  sr * (usr[c] - side_cons(ur, enr, c)));
+#pragma unroll
+            for (int c = 1; c < 3; ++c)
+                bf[c - 1] = 0.5 * (((side_bflux(ul, bl, c) + sl * (bsl[c] - bl[c])) + side_bflux(ur, br, c)) +
+                                   sr * (bsr[c] - br[c]));
         }
     }
 }

@@ -65,15 +65,15 @@ PK_DEV int plane_of(int slot, const int (&perm)[3])
 }
 
 template <class PH>
-PK_DEV void load_cell(const double* __restrict__ u, long long off, const Geom& g, double (&w)[PH::NV])
+PK_DEV void load_cell(const double* u, long long off, const Geom& g, double (&w)[PH::NV])
 {
     const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
 #pragma unroll
-    for (int v = 0; v < PH::NV; ++v) w[v] = __ldg(u + (long long)plane_of<PH>(v, perm) * g.plane + off);
+    for (int v = 0; v < PH::NV; ++v) w[v] = u[(long long)plane_of<PH>(v, perm) * g.plane + off];
 }
 
 template <class PH>
-PK_DEV void store_cell(double* __restrict__ u, long long off, const Geom& g, const double (&w)[PH::NV])
+PK_DEV void store_cell(double* u, long long off, const Geom& g, const double (&w)[PH::NV])
 {
     const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
 #pragma unroll
@@ -87,51 +87,75 @@ struct Roles {
     int end;       // 0 interior slope, -1 pencil start rule, +1 pencil end rule
     bool flux;     // computes the flux through its right face
     bool upd;      // Euler-updated from the two face fluxes
-    bool care;     // internal_sources + care_for_positives applied
+    bool keep;     // not updated but kept (pencil end cell): u1 = u, then floors
 };
 
+// Shared-memory planes of a tile: Q holds primitives and then face fluxes, L
+// the left state of each cell's right face, R the right state of its left face.
+struct Smem {
+    double* Q;
+    double* L;
+    double* R;
+    int PT;
+};
+
+// One stage of solve() on the tile.  Nothing but the cell's own state w crosses
+// a barrier in registers: primitives and face states live in shared memory and
+// the stage's initial state u0 is re-read (from L2) at the update, so the
+// Riemann solver runs with a small live set.
+//   w      in: the stage's input state (valid where r.q); out: u1 where r.upd or r.keep
+//   u0src  where u0 (uh / the sweep's input) is read for the update
+//   wsrc   where an unchanged end cell re-reads its state (r.keep)
 template <class PH>
-PK_DEV void rk_stage(double* __restrict__ Q, double* __restrict__ R, int me, int st, int PT, const Roles& r,
-                     double (&w)[PH::NV], const double (&u0)[PH::NV], double dtodx, double ch,
+PK_DEV void rk_stage(const Smem& sm, int me, int st, const Roles& r, double (&w)[PH::NV], const double* u0src,
+                     const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
                      const PhysParams& pp, unsigned& status)
 {
     constexpr int NV = PH::NV;
-    double q[NV];
+    const int PT = sm.PT;
     if (r.q) {
+        double q[NV];
         utoq<PH>(w, q, pp);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Q[v * PT + me] = q[v];
+        for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = q[v];
     }
     __syncthreads();
-    double ql[NV];
     if (r.slope) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             const int lim = (PH::MHD && v >= PH::IB) ? pp.limb : pp.lim;
+            const double qc = sm.Q[v * PT + me];
             double s;
-            if (r.end < 0) s = slope_end(lim, Q[v * PT + me + st] - q[v]);
-            else if (r.end > 0) s = slope_end(lim, q[v] - Q[v * PT + me - st]);
-            else s = slope_interior(lim, q[v] - Q[v * PT + me - st], Q[v * PT + me + st] - q[v]);
+            if (r.end < 0) s = slope_end(lim, sm.Q[v * PT + me + st] - qc);
+            else if (r.end > 0) s = slope_end(lim, qc - sm.Q[v * PT + me - st]);
+            else s = slope_interior(lim, qc - sm.Q[v * PT + me - st], sm.Q[v * PT + me + st] - qc);
             const double dqh = 0.5 * s;                       // dq_interp = half * f_limiter(q)
-            ql[v] = q[v] + dqh;                               // left state of the right face
-            R[v * PT + me] = q[v] - dqh;                      // right state of the left face
+            sm.L[v * PT + me] = qc + dqh;                     // left state of the right face
+            sm.R[v * PT + me] = qc - dqh;                     // right state of the left face
         }
     }
     __syncthreads();
     if (r.flux) {
-        double qr[NV], fx[NV];
+        double ql[NV], qr[NV], fx[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) qr[v] = R[v * PT + me + st];
+        for (int v = 0; v < NV; ++v) {
+            ql[v] = sm.L[v * PT + me];
+            qr[v] = sm.R[v * PT + me + st];
+        }
         riemann<PH>(ql, qr, ch, pp, fx);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Q[v * PT + me] = fx[v];
+        for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = fx[v];
     }
     __syncthreads();
     if (r.upd) {
+        double u0[NV];
+        load_cell<PH>(u0src, off, g, u0);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) w[v] = u0[v] + dtodx * (Q[v * PT + me - st] - Q[v * PT + me]);
+        for (int v = 0; v < NV; ++v) w[v] = u0[v] + dtodx * (sm.Q[v * PT + me - st] - sm.Q[v * PT + me]);
+    } else if (r.keep) {
+        load_cell<PH>(wsrc, off, g, w);
     }
-    if (r.care) sources_and_floors<PH>(w, pp, status);
+    if (r.upd || r.keep) sources_and_floors<PH>(w, pp, status);
     __syncthreads();
 }
 
@@ -151,8 +175,8 @@ PK_DEV int wrap(int s, int n)
 // Fused two-stage sweep of a periodic block: uin -> uout.
 // grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2.
 // -------------------------------------------------------------------------
-template <class PH, int MAXT>
-__global__ void __launch_bounds__(MAXT) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
+template <class PH, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
                                                      double* __restrict__ uout, PhysParams pp, double dtodx1,
                                                      double dtodx2, double ch, double psi_fac,
                                                      unsigned* __restrict__ gstatus)
@@ -160,8 +184,7 @@ __global__ void __launch_bounds__(MAXT) k_sweep_fused(Geom g, Tile tl, const dou
     extern __shared__ double smem[];
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
-    double* Q = smem;
-    double* R = smem + NV * PT;
+    const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
     const int tid = threadIdx.x;
     int p, t;
     if (tl.xfast) { t = tid % T; p = tid / T; }
@@ -175,29 +198,26 @@ __global__ void __launch_bounds__(MAXT) k_sweep_fused(Geom g, Tile tl, const dou
     const int s = c0 - 4 + t;                                  // position along the pencil (interior coords)
     const long long off = (long long)(g.g_d + wrap(s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
                           (long long)(g.g2 + i2) * g.s2;
-    double u0[NV], w[NV];
+    double w[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) u0[v] = 0.0;
-    if (active) load_cell<PH>(uin, off, g, u0);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) w[v] = u0[v];
+    for (int v = 0; v < NV; ++v) w[v] = 0.0;
+    if (active) load_cell<PH>(uin, off, g, w);
     unsigned status = 0;
     Roles r;
+    r.end = 0;
+    r.keep = false;
     // stage 1 (RK2_1) on tile cells [0, T)
     r.q = active;
     r.slope = active && t >= 1 && t < T - 1;
-    r.end = 0;
     r.flux = active && t >= 1 && t < T - 2;
     r.upd = active && t >= 2 && t < T - 2;
-    r.care = r.upd;
-    rk_stage<PH>(Q, R, me, st, PT, r, w, u0, dtodx1, ch, pp, status);
-    // stage 2 (RK2_2) on tile cells [2, T-2)
+    rk_stage<PH>(sm, me, st, r, w, uin, uin, off, g, dtodx1, ch, pp, status);
+    // stage 2 (RK2_2) on tile cells [2, T-2); u0 is again the sweep's input
     r.q = active && t >= 2 && t < T - 2;
     r.slope = active && t >= 3 && t < T - 3;
     r.flux = active && t >= 3 && t < T - 4;
     r.upd = active && t >= 4 && t < T - 4;
-    r.care = r.upd;
-    rk_stage<PH>(Q, R, me, st, PT, r, w, u0, dtodx2, ch, pp, status);
+    rk_stage<PH>(sm, me, st, r, w, uin, uin, off, g, dtodx2, ch, pp, status);
     if (r.upd && s < c0 + tl.L && s < g.n_d) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);
@@ -224,8 +244,7 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     extern __shared__ double smem[];
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
-    double* Q = smem;
-    double* R = smem + NV * PT;
+    const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
     const int tid = threadIdx.x;
     int p, t;
     if (tl.xfast) { t = tid % T; p = tid / T; }
@@ -238,22 +257,13 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     const int n = g.ext_d;
     const int s = c0 - tl.halo + t;                            // storage index along the pencil
     const bool valid = (tid < PT) && (i1 < g.n1) && s >= 0 && s < n;
+    const bool own = valid && s >= c0 && s < c0 + tl.L;
     const long long off = (long long)s * g.sd + (long long)(g.g1 + i1) * g.s1 + (long long)(g.g2 + i2) * g.s2;
-    double u0[NV], w[NV];
+    double w[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) u0[v] = w[v] = 0.0;
-    if (valid) {
-        const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
-#pragma unroll
-        for (int v = 0; v < NV; ++v) w[v] = uin[(long long)plane_of<PH>(v, perm) * g.plane + off];
-        if (first) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) u0[v] = w[v];
-        } else {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) u0[v] = uh[(long long)plane_of<PH>(v, perm) * g.plane + off];
-        }
-    }
+    for (int v = 0; v < NV; ++v) w[v] = 0.0;
+    if (valid) load_cell<PH>(uin, off, g, w);
+    if (first && own) store_cell<PH>(uh, off, g, w);           // pu0 = pu (solve_cg_riemann.F90:176)
     unsigned status = 0;
     Roles r;
     r.q = valid;
@@ -265,12 +275,9 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     // the update needs the left-face flux computed by tile cell t-1
     const bool prev_flux = (t >= 1) && (s >= 1) && ((s - 1 == 0) || (t - 1 >= 1));
     r.upd = valid && s >= 1 && s <= n - 2 && prev_flux && r.flux;
-    r.care = r.upd || (valid && (s == 0 || s == n - 1));
-    rk_stage<PH>(Q, R, me, st, PT, r, w, u0, dtodx, ch, pp, status);
-    if (valid && s >= c0 && s < c0 + tl.L) {
-        if (first) store_cell<PH>(uh, off, g, u0);
-        store_cell<PH>(uout, off, g, w);
-    }
+    r.keep = !r.upd && valid && (s == 0 || s == n - 1);        // u1 = u at the pencil ends, then floors
+    rk_stage<PH>(sm, me, st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status);
+    if (own) store_cell<PH>(uout, off, g, w);
     flush_status(status, gstatus);
 }
 

@@ -205,5 +205,7 @@ class Simulation:
     def stream(self) -> int:
         return self.lib.pk_stream(self.h) or 0
 
-    def set_tile(self, direction: int, pencils: int, length: int) -> None:
-        self._chk(self.lib.pk_set_tile(self.h, direction, pencils, length), "pk_set_tile")
+    def set_tile(self, direction: int, pencils: int, length: int, variant: int = -1) -> None:
+        """Tile of the fused sweep along ``direction`` (0..2): pencils per CTA,
+        output cells per pencil, launch-bound variant (-1: default)."""
+        self._chk(self.lib.pk_set_tile(self.h, direction, pencils, length, variant), "pk_set_tile")

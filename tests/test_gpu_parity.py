@@ -78,9 +78,10 @@ def test_fused_sweep_bitexact(gpu_lib, oracle_lib, phys, lim):
     compare(ob, sim, "fused sweeps")
 
 
-@pytest.mark.parametrize("tile", [(1, 8), (3, 16), (4, 40), (2, 64), (8, 24)])
+@pytest.mark.parametrize("tile", [(1, 8, 3), (3, 16, 4), (4, 40, 1), (2, 64, 0), (8, 24, 2), (2, 56, 5)])
 def test_fused_tiles_agree(gpu_lib, oracle_lib, tile):
-    """Tile shapes (pencils per CTA, cells per chunk) do not change any bit."""
+    """Tile shapes (pencils per CTA, cells per chunk, launch-bound variant) do
+    not change any bit."""
     s = setup_for("mhd", n=(50, 37, 29), lim="moncen")
     ob, sim = both(s, seed=9)
     for d in range(3):
@@ -179,3 +180,17 @@ def test_soa_layout_roundtrip(gpu_lib):
     assert_bitexact(np.moveaxis(su, 0, -1), u, "soa u")
     assert_bitexact(np.moveaxis(sb, 0, -1), b, "soa b")
     assert_bitexact(sp, psi, "soa psi")
+
+
+def test_autotune_keeps_state(gpu_lib, oracle_lib):
+    """The autotuner restores the state it times on and keeps results bit-exact."""
+    from piernik_b200.autotune import autotune
+    setup, u, b, psi = problems.mhd_turbulence(n=24, seed=5)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    best = autotune(sim, reps=1)
+    assert set(best) == {0, 1, 2}
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    ob.run(3)
+    sim.run(3)
+    compare(ob, sim, "after autotune")
