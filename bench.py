@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--tune-log", default=None)
+    p.add_argument("--tiles", default=None,
+                   help="fix fused-sweep tiles instead of autotuning, e.g. 'x:1,88,3;y:4,56,2;z:4,56,2' (P,L,variant)")
     return p.parse_args()
 
 
@@ -181,7 +183,14 @@ def our_arm(args):
     sim.upload(u, b, psi)
     stream = torch.cuda.ExternalStream(sim.stream)
     tiles = None
-    if not args.no_autotune:
+    if args.tiles:
+        tiles = {}
+        for item in args.tiles.split(";"):
+            ax, vals = item.split(":")
+            P, Lc, V = (int(x) for x in vals.split(","))
+            sim.set_tile("xyz".index(ax), P, Lc, V)
+            tiles[ax] = [P, Lc, V]
+    elif not args.no_autotune:
         from piernik_b200.autotune import autotune
         log = open(args.tune_log, "w") if (args.tune_log and rank == 0) else None
         best = autotune(sim, reps=2, verbose=False)

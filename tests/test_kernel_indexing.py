@@ -1,0 +1,140 @@
+"""CPU emulation of the sweep kernels' index arithmetic.
+
+For every launch shape the library can produce for the given block sizes
+(fused tiles of every variant the autotuner tries, the whole-pencil and
+chunked stage tiles), each thread's global offset and every shared-memory
+slot it reads are computed exactly as the kernels do and checked to be in
+bounds; owned cells must be updated.  This runs before any GPU sees a new
+tile shape.  Mirrors k_sweep_fused / k_stage in piernik_b200/csrc/pk_kernels.cuh
+and launch_fused / launch_stage in pk_api.cu.
+"""
+import pytest
+
+ORTHO1 = [1, 0, 0]
+ORTHO2 = [2, 2, 1]
+STAGE_MAXT = 320
+VARIANT_T = [320, 256, 256, 128, 128, 192]
+
+
+def geom(n, nb, d):
+    g = [nb if x > 1 else 0 for x in n]
+    ext = [n[k] + 2 * g[k] for k in range(3)]
+    st = [1, ext[0], ext[0] * ext[1]]
+    o1, o2 = ORTHO1[d], ORTHO2[d]
+    return dict(plane=ext[0] * ext[1] * ext[2], sd=st[d], s1=st[o1], s2=st[o2], ext_d=ext[d], n_d=n[d],
+                g_d=g[d], n1=n[o1], g1=g[o1], n2=n[o2], g2=g[o2])
+
+
+def fused_shape(n, d, P, L, maxt):
+    G = geom(n, 4, d)
+    L = min(L, n[d])
+    P = min(P, G["n1"])
+    T = L + 8
+    while P * T > maxt and P > 1:
+        P -= 1
+    assert P * T <= maxt
+    return G, P, L, T
+
+
+def check_fused(n, d, P, L, maxt):
+    G, P, L, T = fused_shape(n, d, P, L, maxt)
+    PT = P * T
+    xfast = d == 0
+    covered = set()
+    for bx in range((G["n1"] + P - 1) // P):
+        for by in range((n[d] + L - 1) // L):
+            for bz in sorted({0, G["n2"] - 1}):
+                for tid in range(PT):
+                    t, p = (tid % T, tid // T) if xfast else (tid // P, tid % P)
+                    sp, st = (T, 1) if xfast else (1, P)
+                    me = p * sp + t * st
+                    assert 0 <= me < PT
+                    i1 = bx * P + p
+                    if i1 >= G["n1"]:
+                        continue
+                    s = by * L - 4 + t
+                    w = s % G["n_d"]
+                    off = (G["g_d"] + w) * G["sd"] + (G["g1"] + i1) * G["s1"] + (G["g2"] + bz) * G["s2"]
+                    assert 0 <= off < G["plane"]
+                    for lo, hi in ((0, T), (2, T - 2)):
+                        if lo < t < hi - 1:
+                            assert me - st >= 0 and me + st < PT
+                        if lo + 1 <= t < hi - 2:
+                            assert me + st < PT
+                        if lo + 2 <= t < hi - 2:
+                            assert me - st >= 0
+                    if 4 <= t < T - 4 and s < by * L + L and s < G["n_d"] and bz == 0:
+                        covered.add((i1, s))
+    assert len(covered) == G["n1"] * G["n_d"]
+
+
+def check_stage(n, d):
+    G = geom(n, 4, d)
+    ext = G["ext_d"]
+    if ext <= STAGE_MAXT:
+        P = STAGE_MAXT // ext
+        if P >= 4:
+            P -= P % 4
+        P = min(P, G["n1"])
+        T, L, halo = ext, ext, 0
+    else:
+        P, L, T, halo = 4, 64, 68, 2
+    PT = P * T
+    xfast = d == 0
+    for bx in range((G["n1"] + P - 1) // P):
+        for by in range((ext + L - 1) // L):
+            for bz in sorted({0, G["n2"] - 1}):
+                for tid in range(PT):
+                    t, p = (tid % T, tid // T) if xfast else (tid // P, tid % P)
+                    sp, st = (T, 1) if xfast else (1, P)
+                    me = p * sp + t * st
+                    i1 = bx * P + p
+                    c0 = by * L
+                    s = c0 - halo + t
+                    if not (i1 < G["n1"] and 0 <= s < ext):
+                        continue
+                    off = s * G["sd"] + (G["g1"] + i1) * G["s1"] + (G["g2"] + bz) * G["s2"]
+                    assert 0 <= off < G["plane"]
+                    end = -1 if s == 0 else (1 if s == ext - 1 else 0)
+                    slope = end != 0 or (1 <= t <= T - 2)
+                    next_slope = s + 1 < ext and t + 1 <= T - 1 and (s + 1 == ext - 1 or t + 1 <= T - 2)
+                    flux = slope and next_slope
+                    prev_flux = t >= 1 and s >= 1 and (s - 1 == 0 or t - 1 >= 1)
+                    upd = 1 <= s <= ext - 2 and prev_flux and flux
+                    if slope:
+                        if end < 0:
+                            assert me + st < PT
+                        elif end > 0:
+                            assert me - st >= 0
+                        else:
+                            assert me - st >= 0 and me + st < PT
+                    if flux:
+                        assert me + st < PT
+                    if upd:
+                        assert me - st >= 0
+                    if c0 <= s < c0 + L and 1 <= s <= ext - 2:
+                        assert upd
+
+
+CASES = [(12, 10, 8), (20, 14, 11), (50, 37, 29), (400, 6, 5), (24, 17, 9), (32, 32, 1), (9, 8, 7),
+         (64, 64, 64), (16, 24, 48)]
+
+
+@pytest.mark.parametrize("n", CASES)
+def test_stage_kernel_indexing(n):
+    for d in range(3):
+        if n[d] > 1:
+            check_stage(n, d)
+
+
+@pytest.mark.parametrize("n", CASES)
+def test_fused_kernel_indexing(n):
+    from piernik_b200.autotune import LENGTHS
+    for d in range(3):
+        if n[d] <= 1:
+            continue
+        for maxt in sorted(set(VARIANT_T)):
+            for L in LENGTHS[:6] + (8, 16):
+                for P in (1, 2, 3, 4, 8):
+                    if L + 8 <= maxt:
+                        check_fused(n, d, P, L, maxt)
