@@ -37,6 +37,11 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 MHD cell-updates/s at 256^3 on 1 B200; adjoint-gradient cost ÷ forward step"
 UNIT = "cell-updates/s"
 NVAR = 9                         # dn, mx, my, mz, en, Bx, By, Bz, psi
+# DRAM bytes per cell of one fused-sweep launch from the ncu capture in
+# profiles/k_sweep_fused_mhd_128cube.md (y sweep, 128^3: 161.76 MB read +
+# 125.97 MB written over 128^3 cells); traffic grows with the cell count, so the
+# full-size figure is this times n^3.
+TRAFFIC_BYTES_PER_CELL = (161.756672e6 + 125.965568e6) / 128 ** 3
 
 
 def parse():
@@ -236,13 +241,7 @@ def our_arm(args):
     bytes_per_launch = 2.0 * NVAR * 8 * n ** 3
     launch_ms = sweep_ms / max(nsweep, 1)
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            tj = json.load(f)
-        traffic = tj["bytes_per_cell"] * n ** 3
-    except Exception:
-        traffic = None
+    traffic = TRAFFIC_BYTES_PER_CELL * n ** 3
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": "k_sweep_fused<MHD> (one sweep direction, both RK2 stages)",
                 "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms, "peak_source": src}
