@@ -31,6 +31,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -56,6 +58,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--tune-log", default=None)
+    p.add_argument("--workload", default="mhd256", choices=["mhd256", "batched"],
+                   help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks")
+    p.add_argument("--nblocks", type=int, default=512)
     p.add_argument("--tiles", default=None,
                    help="fix fused-sweep tiles instead of autotuning, e.g. 'x:1,88,3;y:4,56,2;z:4,56,2' (P,L,variant)")
     return p.parse_args()
@@ -296,8 +301,87 @@ def our_arm(args):
         torch.distributed.destroy_process_group()
 
 
+def batched_arm(args):
+    """512 independent periodic blocks with edges from {16,24,32,48,64}, three
+    fluids (ion MHD 5/3, neutral 7/5, dust), one persistent launch per sweep,
+    each step's sweeps replayed from a CUDA graph; timed beside one block of
+    the same physics and a similar cell count through the single-block path."""
+    import torch
+    from piernik_b200 import build, problems
+    from piernik_b200.autotune import autotune
+    from piernik_b200.sim import Simulation
+    build.build()
+    torch.cuda.set_device(0)
+    data = problems.batched_blocks(nblocks=args.nblocks, seed=args.seed)
+    cells = sum(int(np.prod(s.n)) for s, *_ in data)
+    sim = Simulation(data[0][0])
+    for s, *_ in data[1:]:
+        sim.add_block(s)
+    for i, (s, u, b, psi) in enumerate(data):
+        sim.upload(u, b, psi, block=i)
+    best = None
+    for L, V in ((56, 1), (56, 0), (40, 0), (24, 1), (56, 2)):
+        sim.set_batch(True, L, V)
+        sim.profile(True)
+        sim.profile_read()
+        dt, _ = sim.timestep_raw()
+        for d in (1, 2, 3):
+            sim.sweep(d, 0.25 * dt, 1.0)
+        _, nl, ms = sim.profile_read()
+        sim.profile(False)
+        if best is None or ms < best[0]:
+            best = (ms, L, V)
+    for i, (s, u, b, psi) in enumerate(data):   # undo the tuning sweeps
+        sim.upload(u, b, psi, block=i)
+    sim.set_batch(True, best[1], best[2])
+    sim.use_graph(True)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.run(args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(0)
+    l0, _, _ = sim.profile_read()
+    e0.record(stream)
+    sim.run(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    l1, _, _ = sim.profile_read()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    batched = 2.0 * cells * args.steps / (ms / 1e3)
+    sim.close()
+    # one block of the same physics and a similar number of cells
+    side = int(round(cells ** (1.0 / 3.0) / 8.0)) * 8
+    one = problems.batched_blocks(nblocks=1, seed=args.seed, sizes=(side,), levels=1)[0]
+    s1 = Simulation(one[0])
+    s1.upload(*one[1:])
+    autotune(s1, reps=1)
+    s1.run(args.warmup)
+    st1 = torch.cuda.ExternalStream(s1.stream)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(st1)
+    s1.run(args.steps)
+    e3.record(st1)
+    e3.synchronize()
+    single = 2.0 * side ** 3 * args.steps / (e2.elapsed_time(e3) / 1e3)
+    s1.close()
+    out = {"metric": "FP64 3-fluid MHD cell-updates/s, %d uneven blocks, one persistent launch per sweep" % args.nblocks,
+           "value": batched, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "batched uneven blocks (edges 16..64, 3 levels, off-centre Sedov), ion MHD + "
+                                  "neutral + dust, vanleer, CFL 0.7, CUDA graph per step",
+                      "blocks": args.nblocks, "cells": cells, "batch_L_variant": [best[1], best[2]]},
+           "single_block": {"n": side, "value": single, "ratio_batched_to_single": batched / single},
+           "gpu_launches": l1 - l0, "clocks": ck}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "batched":
+        batched_arm(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
     else:

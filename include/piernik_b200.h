@@ -150,6 +150,17 @@ int pk_sync(pk_handle h);
  * default.  Used by the autotuner; 0 keeps the built-in P / L. */
 int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32_t variant);
 
+/* Sweep all blocks in one persistent launch over a work list of tiles (the
+ * default whenever more than one block is registered; enable = 1 forces it for
+ * a single block), with chunks of at most `length` cells and the given
+ * launch-bound variant (-1 keeps the current one). */
+int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant);
+
+/* Replay the sweeps of a step (fluid_update) as one captured CUDA graph; the
+ * step scalars (dt, chspeed, glmdamping factor) are read by the kernels from
+ * device memory, so one capture serves every step. */
+int pk_use_graph(pk_handle h, int32_t enable);
+
 /* Launch-bound variants of the fused sweep: count, CTA size and CTAs per SM
  * each was compiled for (arrays of at least 16 entries). */
 int pk_tile_variants(int32_t* n, int32_t* threads, int32_t* ctas_per_sm);

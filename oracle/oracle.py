@@ -112,6 +112,7 @@ def lib():
         L.o_fluid_update.argtypes = [P, B, S]
         L.o_run.argtypes = [P, B, S, C.c_int]
         L.o_nvar.argtypes = [P]
+        L.o_run_multi.argtypes = [P, C.POINTER(B), C.c_int, S, C.c_int]
         L.o_set_threads.argtypes = [C.c_int]
         L.o_get_threads.restype = C.c_int
         _lib = L
@@ -207,6 +208,19 @@ class OracleBlock:
 
     def chspeed(self, dt):
         return lib().o_chspeed(C.byref(self.cfg), C.byref(self.blk), dt)
+
+
+def run_multi(blocks, nsteps: int, state: OState = None) -> OState:
+    """Advance several OracleBlocks (same Setup apart from n/dl) with one
+    global dt, as the reference's leaves loop does."""
+    if state is None:
+        state = OState()
+        state.dt_old = -1.0
+    arr = (C.POINTER(OBlock) * len(blocks))(*[C.pointer(b.blk) for b in blocks])
+    rc = lib().o_run_multi(C.byref(blocks[0].cfg), arr, len(blocks), C.byref(state), nsteps)
+    if rc:
+        raise RuntimeError(f"o_run_multi failed: {rc}")
+    return state
 
 
 def set_threads(n: int) -> None:

@@ -959,3 +959,88 @@ int o_get_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------ */
+/* Several blocks (the leaves list): one dt and one chspeed for all    */
+/* ------------------------------------------------------------------ */
+
+/* time_step over all leaves (timestep.F90:165-177 loop over cgl), clamps as o_time_step */
+int o_time_step_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st)
+{
+    double dt = DBL_MAX, c_all = 0.0;
+    st->dt_old = st->dt;
+    for (int i = 0; i < nb; ++i) {
+        double d, c;
+        o_timestep_raw(cfg, blks[i], &d, &c);
+        dt = f_min(dt, d);
+        c_all = f_max(c_all, c);
+    }
+    if (st->nstep < 1) {
+        if (cfg->dt_initial > 0.0) dt = f_min(dt, cfg->dt_initial);
+        else if (cfg->dt_initial < 0.0) dt = f_min(dt, -cfg->dt_initial * dt);
+    } else {
+        if (st->dt_old > 0.0) dt = f_min(dt, st->dt_old * cfg->dt_max_grow);
+    }
+    st->c_all = c_all;
+    if (dt < cfg->dt_min) {
+        st->dt = dt;
+        return 3;
+    }
+    double rem = cfg->tend - st->t;
+    dt = f_min(f_min(dt, cfg->dt_max), (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem));
+    st->dt = dt;
+    return 0;
+}
+
+/* fluid_update_full over all leaves: chspeed and the damping factor are the
+ * minimum / maximum over blocks (hdc.F90:112-138, 310-332) */
+int o_fluid_update_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st)
+{
+    const double dt = st->dt;
+    int rc;
+    if (cfg->magnetic) {
+        double ch = DBL_MAX;
+        for (int i = 0; i < nb; ++i) ch = f_min(ch, o_chspeed(cfg, blks[i], dt));
+        st->chspeed = ch;
+    }
+    double fac = 1.0;
+    if (cfg->magnetic) {
+        double f = 0.0;
+        for (int i = 0; i < nb; ++i) {
+            int eff;
+            double mdl = o_min_dl(blks[i], &eff);
+            if (eff > 0) f = f_max(f, (cfg->glm_alpha * st->chspeed) / (mdl / dt));
+        }
+        fac = exp(-f);
+    }
+    for (int half = 0; half < 2; ++half) {
+        st->t = st->t + dt;
+        for (int s = 0; s < 3; ++s) {
+            int d = half == 0 ? s : 2 - s;
+            if (cfg->skip_sweep[d] || blks[0]->n[d] <= 1) continue;
+            /* sweep(d): every stage over all blocks, then the boundary update */
+            int nst = (cfg->integration_order == 1) ? 1 : 2;
+            for (int stg = 1; stg <= nst; ++stg) {
+                for (int i = 0; i < nb; ++i)
+                    if ((rc = o_solve_cg(cfg, blks[i], d, (cfg->integration_order == 1) ? 1 : stg, dt, st->chspeed))) return rc;
+                for (int i = 0; i < nb; ++i) o_fill_guards(cfg, blks[i]);
+            }
+        }
+        if (cfg->magnetic)
+            for (int i = 0; i < nb; ++i) o_glm_apply(cfg, blks[i], fac);
+    }
+    return 0;
+}
+
+int o_run_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st, int nsteps)
+{
+    for (int s = 0; s < nsteps; ++s) {
+        if (!(st->t < cfg->tend)) break;
+        int rc = o_time_step_multi(cfg, blks, nb, st);
+        if (rc) return rc;
+        rc = o_fluid_update_multi(cfg, blks, nb, st);
+        if (rc) return rc;
+        st->nstep += 1;
+    }
+    return 0;
+}

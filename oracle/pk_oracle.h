@@ -87,6 +87,10 @@ int    o_time_step(const o_cfg *cfg, const o_block *blk, o_state *st);   /* 3: d
 int    o_fluid_update(const o_cfg *cfg, o_block *blk, o_state *st);
 /* main-loop body repeated nsteps times (piernik.F90:125-213 without I/O) */
 int    o_run(const o_cfg *cfg, o_block *blk, o_state *st, int nsteps);
+/* the same over several independent blocks sharing one dt (the leaves list) */
+int    o_time_step_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st);
+int    o_fluid_update_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st);
+int    o_run_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st, int nsteps);
 void   o_set_threads(int n);
 int    o_get_threads(void);
 

@@ -27,7 +27,7 @@ EXPORTS = (
     "pk_upload", "pk_download", "pk_solve_cg", "pk_fill_guards", "pk_sweep", "pk_glm_damp",
     "pk_timestep_raw", "pk_time_step", "pk_fluid_update", "pk_run", "pk_get_time_state",
     "pk_set_time_state", "pk_status", "pk_sync", "pk_set_tile", "pk_stream", "pk_profile_enable",
-    "pk_profile_read", "pk_tile_variants",
+    "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_use_graph",
 )
 
 
@@ -112,6 +112,8 @@ def load(path: str = LIBPATH):
     L.pk_sync.argtypes = [H]
     L.pk_set_tile.argtypes = [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.pk_tile_variants.argtypes = [C.POINTER(C.c_int32)] * 3
+    L.pk_set_batch.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
+    L.pk_use_graph.argtypes = [H, C.c_int32]
     L.pk_stream.argtypes = [H]
     L.pk_stream.restype = C.c_void_p
     L.pk_profile_enable.argtypes = [H, C.c_int32]

@@ -12,13 +12,15 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "csrc", "pk_api.cu")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("pk_api.cu", "pk_device.cuh", "pk_kernels.cuh", "pk_aux.cuh")]
+CSRC = os.path.join(HERE, "csrc")
+UNITS = ["pk_api.cu", "pk_phys_hd1.cu", "pk_phys_hd2.cu", "pk_phys_mhd1.cu", "pk_phys_mhd2.cu", "pk_phys_mhd3.cu"]
+HEADERS = ["pk_device.cuh", "pk_kernels.cuh", "pk_aux.cuh", "pk_internal.h", "pk_launch.cuh"]
+DEPS = [os.path.join(CSRC, f) for f in UNITS + HEADERS]
 INC = os.path.join(os.path.dirname(HERE), "include")
 OUT = os.path.join(HERE, "libpiernik_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--fmad=false", "-lineinfo", "-std=c++17",
-         "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "-shared"]
+         "-Xcompiler", "-fPIC,-O2,-ffp-contract=off"]
 
 
 def needs_build() -> bool:
@@ -29,11 +31,23 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if force or needs_build():
-        cmd = [NVCC] + FLAGS + ["-I", INC, "-o", OUT, SRC]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        subprocess.check_call(cmd)
+    """Compile each translation unit to an object (in parallel) and link the .so."""
+    if not (force or needs_build()):
+        return OUT
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs = []
+    objs = []
+    for unit in UNITS:
+        obj = os.path.join(objdir, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        cmd = [NVCC] + FLAGS + (["-Xptxas=-v"] if verbose else []) + ["-I", INC, "-c", "-o", obj,
+                                                                    os.path.join(CSRC, unit)]
+        procs.append((unit, subprocess.Popen(cmd)))
+    bad = [u for u, p in procs if p.wait() != 0]
+    if bad:
+        raise RuntimeError(f"nvcc failed for {bad}")
+    subprocess.check_call([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT] + objs)
     return OUT
 
 

@@ -10,69 +10,20 @@
 #include <string>
 #include <vector>
 
-#include "../../include/piernik_b200.h"
 #include "pk_aux.cuh"
-#include "pk_kernels.cuh"
+#include "pk_internal.h"
 
 using namespace pk;
 
-namespace {
+namespace pk {
 
-using PhHD1 = Phys<K_NEU, K_NONE, K_NONE, false>;    // one fluid with energy, no B (solve_cg_u)
-using PhMHD1 = Phys<K_ION, K_NONE, K_NONE, true>;    // ionized fluid + B + psi (solve_cg_ub)
+int fail(pk_ctx* h, int code, const std::string& msg)
+{
+    h->err = msg;
+    return code;
+}
 
-enum PhysId { PHYS_HD1 = 0, PHYS_MHD1 = 1 };
-
-constexpr int MAXT = 320;          // threads per CTA of the stage kernel
-// Launch-bound variants of the fused sweep (threads per CTA, CTAs per SM): the
-// register budget the compiler may use is 65536 / (threads * CTAs); tighter
-// budgets trade spills for resident warps.  The autotuner picks per direction.
-constexpr int NVARIANT = 6;
-constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192};
-constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2};
-constexpr int DEF_VARIANT[3] = {0, 0, 0};
-constexpr int DEF_P[3] = {2, 4, 4};
-constexpr int DEF_L[3] = {64, 64, 64};
-// ORTHO pairs with the memory-fastest ortho direction first (lanes/coalescing)
-constexpr int ORTHO1[3] = {1, 0, 0};
-constexpr int ORTHO2[3] = {2, 2, 1};
-constexpr int PERM3[3][3] = {{0, 1, 2}, {1, 0, 2}, {2, 1, 0}};
-
-struct Block {
-    int n[3], g[3], ext[3];
-    double dl[3];
-    int bnd[3][2];
-    long long plane = 0;
-    double* u = nullptr;
-    double* uh = nullptr;
-    double* tmp = nullptr;
-    double* stage = nullptr;   // host-layout conversion buffer
-    bool guards_stale = false; // set by the fused sweep, which reads periodic images instead of guards
-};
-
-}  // namespace
-
-struct pk_ctx {
-    pk_config cfg;
-    PhysParams pp;
-    int phys = 0;
-    int nvf = 0, nplanes = 0, ib = 0;
-    std::vector<Block> blocks;
-    cudaStream_t stream = nullptr;
-    unsigned* d_status = nullptr;
-    unsigned long long* d_red = nullptr;
-    unsigned long long* h_red = nullptr;
-    int red_cap = 0;
-    pk_time_state ts;
-    std::string err;
-    int tileP[3] = {0, 0, 0}, tileL[3] = {0, 0, 0}, tileV[3] = {-1, -1, -1};
-    long long launches = 0;          // kernels of this library launched on the handle's stream
-    long long sweep_launches = 0;    // of which sweep kernels (fused or stage)
-    bool profiling = false;          // bracket sweep kernels with CUDA events
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used, ev_free;
-};
-
-static int ev_begin(pk_ctx* h, std::pair<cudaEvent_t, cudaEvent_t>* p)
+int ev_begin(pk_ctx* h, std::pair<cudaEvent_t, cudaEvent_t>* p)
 {
     if (!h->profiling) return PK_OK;
     if (h->ev_free.empty()) {
@@ -86,7 +37,7 @@ static int ev_begin(pk_ctx* h, std::pair<cudaEvent_t, cudaEvent_t>* p)
     return PK_OK;
 }
 
-static int ev_end(pk_ctx* h, const std::pair<cudaEvent_t, cudaEvent_t>& p)
+int ev_end(pk_ctx* h, const std::pair<cudaEvent_t, cudaEvent_t>& p)
 {
     if (!h->profiling) return PK_OK;
     if (cudaEventRecord(p.second, h->stream) != cudaSuccess) return PK_E_CUDA;
@@ -94,33 +45,12 @@ static int ev_end(pk_ctx* h, const std::pair<cudaEvent_t, cudaEvent_t>& p)
     return PK_OK;
 }
 
-#define PK_CUDA(h, call)                                                                      \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess) {                                                              \
-            (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
-            return PK_E_CUDA;                                                                 \
-        }                                                                                     \
-    } while (0)
+// ORTHO pairs with the memory-fastest ortho direction first (lanes/coalescing)
+static constexpr int ORTHO1[3] = {1, 0, 0};
+static constexpr int ORTHO2[3] = {2, 2, 1};
+static constexpr int PERM3[3][3] = {{0, 1, 2}, {1, 0, 2}, {2, 1, 0}};
 
-static int fail(pk_ctx* h, int code, const std::string& msg)
-{
-    h->err = msg;
-    return code;
-}
-
-static int grid1d(long long n, int threads)
-{
-    long long b = (n + threads - 1) / threads;
-    if (b > 148LL * 16) b = 148LL * 16;
-    return (int)(b < 1 ? 1 : b);
-}
-
-// ---------------------------------------------------------------------------
-// kernel launches
-// ---------------------------------------------------------------------------
-
-static Geom make_geom(const Block& b, int dir)
+Geom make_geom(const Block& b, int dir)
 {
     Geom g;
     const long long st[3] = {1, b.ext[0], (long long)b.ext[0] * b.ext[1]};
@@ -140,123 +70,29 @@ static Geom make_geom(const Block& b, int dir)
     return g;
 }
 
-template <class PH>
-using FusedFn = void (*)(Geom, Tile, const double*, double*, PhysParams, double, double, double, double, unsigned*);
+}  // namespace pk
 
-template <class PH>
-static FusedFn<PH> fused_variant(int v)
+namespace {
+
+int grid1d(long long n, int threads)
 {
-    switch (v) {
-    case 0: return k_sweep_fused<PH, 320, 1>;
-    case 1: return k_sweep_fused<PH, 256, 1>;
-    case 2: return k_sweep_fused<PH, 256, 2>;
-    case 3: return k_sweep_fused<PH, 128, 3>;
-    case 4: return k_sweep_fused<PH, 128, 4>;
-    default: return k_sweep_fused<PH, 192, 2>;
+    long long b = (n + threads - 1) / threads;
+    if (b > 148LL * 16) b = 148LL * 16;
+    return (int)(b < 1 ? 1 : b);
+}
+
+const PhysOps* ops_of(pk_ctx* h)
+{
+    switch (h->phys) {
+    case 0: return ops_hd1();
+    case 1: return ops_hd2();
+    case 2: return ops_mhd1();
+    case 3: return ops_mhd2();
+    default: return ops_mhd3();
     }
 }
 
-template <class PH>
-static int set_smem_attr(pk_ctx* h)
-{
-    static bool done = false;
-    if (!done) {
-        for (int v = 0; v < NVARIANT; ++v)
-            PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        done = true;
-    }
-    return PK_OK;
-}
-
-template <class PH>
-static int launch_fused(pk_ctx* h, Block& b, int dir, double dt, double ch, double psi_fac)
-{
-    if (int rc = set_smem_attr<PH>(h)) return rc;
-    Geom g = make_geom(b, dir);
-    Tile tl;
-    int L = h->tileL[dir] > 0 ? h->tileL[dir] : DEF_L[dir];
-    if (L > b.n[dir]) L = b.n[dir];
-    int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
-    if (P > g.n1) P = g.n1;
-    const int var = h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir];
-    const int maxt = VAR_T[var];
-    int T = L + 8;
-    while (P * T > maxt && P > 1) --P;
-    if (P * T > maxt) return fail(h, PK_E_ARG, "fused sweep tile longer than the variant's CTA size");
-    tl.P = P;
-    tl.T = T;
-    tl.L = L;
-    tl.halo = 4;
-    tl.xfast = (dir == 0);
-    dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
-    size_t smem = 3ull * PH::NV * P * T * sizeof(double);
-    const double dtodx1 = (0.5 * dt) / b.dl[dir];   // rk_coef(RK2_1) * dt / dl
-    const double dtodx2 = (1.0 * dt) / b.dl[dir];   // rk_coef(RK2_2) * dt / dl
-    std::pair<cudaEvent_t, cudaEvent_t> ev;
-    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    fused_variant<PH>(var)<<<grid, P * T, smem, h->stream>>>(g, tl, b.u, b.tmp, h->pp, dtodx1, dtodx2, ch, psi_fac,
-                                                            h->d_status);
-    PK_CUDA(h, cudaGetLastError());
-    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
-    h->launches += 1;
-    h->sweep_launches += 1;
-    std::swap(b.u, b.tmp);
-    b.guards_stale = true;
-    return PK_OK;
-}
-
-template <class PH>
-static int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch)
-{
-    if (int rc = set_smem_attr<PH>(h)) return rc;
-    Geom g = make_geom(b, dir);
-    Tile tl;
-    const int ext = b.ext[dir];
-    double* uout = b.u;
-    if (ext <= MAXT) {                       // whole pencil per tile: in place
-        int P = MAXT / ext;
-        if (P >= 4) P -= P % 4;
-        if (P > g.n1) P = g.n1;
-        tl.P = P;
-        tl.T = ext;
-        tl.L = ext;
-        tl.halo = 0;
-    } else {                                 // chunked with a 2-cell halo: out of place
-        tl.P = 4;
-        tl.L = 64;
-        tl.T = tl.L + 4;
-        tl.halo = 2;
-        if (!b.tmp) PK_CUDA(h, cudaMalloc(&b.tmp, sizeof(double) * h->nplanes * b.plane));
-        uout = b.tmp;
-    }
-    tl.xfast = (dir == 0);
-    dim3 grid((g.n1 + tl.P - 1) / tl.P, (ext + tl.L - 1) / tl.L, g.n2);
-    size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
-    std::pair<cudaEvent_t, cudaEvent_t> ev;
-    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    k_stage<PH, MAXT><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, b.u, uout, b.uh, h->pp, first, dtodx, ch,
-                                                             h->d_status);
-    PK_CUDA(h, cudaGetLastError());
-    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
-    h->launches += 1;
-    h->sweep_launches += 1;
-    if (uout != b.u) {
-        BoxGeom bg;
-        for (int d = 0; d < 3; ++d) {
-            bg.ext[d] = b.ext[d];
-            bg.g[d] = b.g[d];
-            bg.n[d] = b.n[d];
-        }
-        bg.plane = b.plane;
-        k_copy_pencils<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(bg, dir, b.tmp, b.u, h->nplanes);
-        PK_CUDA(h, cudaGetLastError());
-        h->launches += 1;
-    }
-    return PK_OK;
-}
-
-static BoxGeom box_of(const Block& b)
+BoxGeom box_of(const Block& b)
 {
     BoxGeom bg;
     for (int d = 0; d < 3; ++d) {
@@ -268,28 +104,30 @@ static BoxGeom box_of(const Block& b)
     return bg;
 }
 
-static int fill_guards_block(pk_ctx* h, Block& b)
+double* state(pk_ctx* h, Block& b) { return b.buf[h->cur]; }
+
+int fill_guards_block(pk_ctx* h, Block& b)
 {
     GuardArgs a;
-    int f = 0, beg = 0;
+    int beg = 0;
     for (int d = 0; d < 3; ++d)
         for (int s = 0; s < 2; ++s) a.bnd[d][s] = b.bnd[d][s];
     for (int i = 0; i < 3; ++i)
         for (int d = 0; d < 3; ++d) a.mom_plane[i][d] = -1;
-    for (f = 0; f < h->cfg.nfluids; ++f) {
+    for (int f = 0; f < h->cfg.nfluids; ++f) {
         for (int d = 0; d < 3; ++d) a.mom_plane[f][d] = beg + 1 + d;
         beg += (h->cfg.fluid_kind[f] == PK_FLUID_DST) ? 4 : 5;
     }
     a.nfl = h->cfg.nfluids;
     a.nplanes = h->nplanes;
-    k_fill_guards<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(box_of(b), b.u, a);
+    k_fill_guards<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(box_of(b), state(h, b), a);
     PK_CUDA(h, cudaGetLastError());
     h->launches += 1;
     b.guards_stale = false;
     return PK_OK;
 }
 
-static bool fused_ok(pk_ctx* h)
+bool fused_ok(pk_ctx* h)
 {
     if (h->cfg.integration_order != 2) return false;
     for (auto& b : h->blocks)
@@ -298,38 +136,122 @@ static bool fused_ok(pk_ctx* h)
     return true;
 }
 
-static int dispatch_fused(pk_ctx* h, Block& b, int dir, double dt, double ch, double psi_fac)
+int ensure_pingpong(pk_ctx* h)
 {
-    if (!b.tmp) PK_CUDA(h, cudaMalloc(&b.tmp, sizeof(double) * h->nplanes * b.plane));
-    if (h->phys == PHYS_MHD1) return launch_fused<PhMHD1>(h, b, dir, dt, ch, psi_fac);
-    return launch_fused<PhHD1>(h, b, dir, dt, ch, psi_fac);
+    for (auto& b : h->blocks)
+        if (!b.buf[1 - h->cur]) {
+            double* p = nullptr;
+            PK_CUDA(h, cudaMalloc(&p, sizeof(double) * h->nplanes * b.plane));
+            PK_CUDA(h, cudaMemsetAsync(p, 0, sizeof(double) * h->nplanes * b.plane, h->stream));
+            b.buf[1 - h->cur] = p;
+            h->batch_dirty = true;
+        }
+    return PK_OK;
 }
 
-static int dispatch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch)
+// block tables (both parities) and per-direction work lists of the batched sweep
+int build_batch(pk_ctx* h)
 {
-    if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
-    if (h->phys == PHYS_MHD1) return launch_stage<PhMHD1>(h, b, dir, first, dtodx, ch);
-    return launch_stage<PhHD1>(h, b, dir, first, dtodx, ch);
+    if (int rc = ensure_pingpong(h)) return rc;
+    if (!h->batch_dirty) return PK_OK;
+    const int nb = (int)h->blocks.size();
+    std::vector<BlockDesc> desc(nb);
+    for (int p = 0; p < 2; ++p) {
+        for (int i = 0; i < nb; ++i) {
+            const Block& b = h->blocks[i];
+            BlockDesc& d = desc[i];
+            d.in = b.buf[p];
+            d.out = b.buf[1 - p];
+            d.plane = b.plane;
+            for (int k = 0; k < 3; ++k) {
+                d.ext[k] = b.ext[k];
+                d.g[k] = b.g[k];
+                d.n[k] = b.n[k];
+                d.dl[k] = b.dl[k];
+            }
+        }
+        cudaFree(h->d_desc[p]);
+        h->d_desc[p] = nullptr;
+        PK_CUDA(h, cudaMalloc(&h->d_desc[p], sizeof(BlockDesc) * (nb > 0 ? nb : 1)));
+        PK_CUDA(h, cudaMemcpyAsync(h->d_desc[p], desc.data(), sizeof(BlockDesc) * nb, cudaMemcpyHostToDevice, h->stream));
+        PK_CUDA(h, cudaStreamSynchronize(h->stream));   // desc is reused for the other parity
+    }
+    const int threads = VAR_T[h->batch_variant];
+    for (int dir = 0; dir < 3; ++dir) {
+        BatchList& bl = h->batch[dir];
+        bl.host.clear();
+        const int o1 = ORTHO1[dir], o2 = ORTHO2[dir];
+        for (int i = 0; i < nb; ++i) {
+            const Block& b = h->blocks[i];
+            if (b.n[dir] <= 1) continue;
+            const int L = b.n[dir] < h->batch_L ? b.n[dir] : h->batch_L;
+            const int T = L + 8;
+            if (T > threads) return fail(h, PK_E_ARG, "batched tile longer than the CTA");
+            int P = threads / T;
+            if (P > b.n[o1]) P = b.n[o1];
+            for (int i2 = 0; i2 < b.n[o2]; ++i2)
+                for (int c0 = 0; c0 < b.n[dir]; c0 += L)
+                    for (int i1 = 0; i1 < b.n[o1]; i1 += P) bl.host.push_back(WorkItem{i, i1, c0, i2, P, L});
+        }
+        cudaFree(bl.dev);
+        bl.dev = nullptr;
+        bl.n = (int)bl.host.size();
+        if (bl.n) {
+            PK_CUDA(h, cudaMalloc(&bl.dev, sizeof(WorkItem) * bl.n));
+            PK_CUDA(h, cudaMemcpyAsync(bl.dev, bl.host.data(), sizeof(WorkItem) * bl.n, cudaMemcpyHostToDevice, h->stream));
+        }
+    }
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));   // host vectors of the tables may change after return
+    h->batch_dirty = false;
+    return PK_OK;
 }
 
-static int glm_scale(pk_ctx* h, double fac)
+void invalidate_graph(pk_ctx* h)
+{
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+}
+
+int put_step_params(pk_ctx* h, double dt, double ch, double fac)
+{
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));   // the previous copy out of h_step has completed
+    h->h_step->dt = dt;
+    h->h_step->ch = ch;
+    h->h_step->psi_fac = fac;
+    PK_CUDA(h, cudaMemcpyAsync(h->d_step, h->h_step, sizeof(StepParams), cudaMemcpyHostToDevice, h->stream));
+    return PK_OK;
+}
+
+int glm_scale(pk_ctx* h, double fac)
 {
     for (auto& b : h->blocks) {
-        k_scale<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(b.u + (long long)(h->ib + 3) * b.plane, b.plane, fac);
+        k_scale<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(state(h, b) + (long long)(h->ib + 3) * b.plane, b.plane, fac);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
     return PK_OK;
 }
 
-// sweep(cdim) with an optional psi damping factor folded into its last write
-static int sweep_impl(pk_ctx* h, int dir, double dt, double ch, double psi_fac)
+// sweep(cdim) of all blocks; the step scalars are already in d_step.
+// apply_fac: the psi damping of glmdamping is folded into this sweep.
+int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double fac)
 {
     if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
+    const PhysOps* ops = ops_of(h);
     if (fused_ok(h)) {
-        for (auto& b : h->blocks)
-            if (b.n[dir] > 1)
-                if (int rc = dispatch_fused(h, b, dir, dt, ch, psi_fac)) return rc;
+        if (int rc = ensure_pingpong(h)) return rc;
+        if (h->batched || h->blocks.size() > 1) {
+            if (int rc = build_batch(h)) return rc;
+            if (int rc = ops->batched(h, dir, apply_fac, h->d_counter + dir)) return rc;
+            for (auto& b : h->blocks) b.guards_stale = true;
+        } else {
+            for (auto& b : h->blocks)
+                if (b.n[dir] > 1)
+                    if (int rc = ops->fused(h, b, dir, apply_fac)) return rc;
+        }
+        h->cur ^= 1;
         return PK_OK;
     }
     const int nst = h->cfg.integration_order == 1 ? 1 : 2;
@@ -337,17 +259,20 @@ static int sweep_impl(pk_ctx* h, int dir, double dt, double ch, double psi_fac)
         const double rk = (h->cfg.integration_order == 1) ? 1.0 : (s == 1 ? 0.5 : 1.0);
         for (auto& b : h->blocks) {
             if (b.n[dir] <= 1) continue;
+            if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+            if (b.ext[dir] > STAGE_MAXT)
+                if (int rc = ensure_pingpong(h)) return rc;
             const double dtodx = (rk * dt) / b.dl[dir];
-            if (int rc = dispatch_stage(h, b, dir, s == 1, dtodx, ch)) return rc;
+            if (int rc = ops->stage(h, b, dir, s == 1, dtodx, ch)) return rc;
         }
         for (auto& b : h->blocks)
             if (int rc = fill_guards_block(h, b)) return rc;
     }
-    if (h->cfg.magnetic && psi_fac != 1.0) return glm_scale(h, psi_fac);
+    if (h->cfg.magnetic && apply_fac) return glm_scale(h, fac);
     return PK_OK;
 }
 
-static double min_dl(pk_ctx* h, int* eff)
+double min_dl(pk_ctx* h, int* eff)
 {
     double m = DBL_MAX;
     int e = 0;
@@ -360,6 +285,57 @@ static double min_dl(pk_ctx* h, int* eff)
     if (eff) *eff = e;
     return m;
 }
+
+void step_dirs(pk_ctx* h, int* dirs, int* nd)
+{
+    *nd = 0;
+    for (int d = 0; d < 3; ++d) {
+        bool has = false;
+        for (auto& b : h->blocks) has = has || b.n[d] > 1;
+        if (has && !h->cfg.skip_sweep[d]) dirs[(*nd)++] = d;
+    }
+}
+
+// the launches of fluid_update_full after the step scalars are on the device
+int step_sweeps(pk_ctx* h, double dt, double ch, double fac)
+{
+    int dirs[3], nd;
+    step_dirs(h, dirs, &nd);
+    for (int half = 0; half < 2; ++half) {
+        for (int s = 0; s < nd; ++s) {
+            const int d = half == 0 ? dirs[s] : dirs[nd - 1 - s];
+            const int last = h->cfg.magnetic && s == nd - 1;
+            if (int rc = sweep_impl(h, d, dt, ch, last, fac)) return rc;
+        }
+        if (h->cfg.magnetic && nd == 0)
+            if (int rc = glm_scale(h, fac)) return rc;
+    }
+    return PK_OK;
+}
+
+// update_chspeed and the glmdamping factor for dt (hdc.F90:112-119, 310-330)
+void glm_scalars(pk_ctx* h, double dt, double* ch, double* fac)
+{
+    int eff;
+    const double mdl = min_dl(h, &eff);
+    *ch = h->ts.chspeed;
+    *fac = 1.0;
+    if (!h->cfg.magnetic) return;
+    double c = DBL_MAX;
+    if (eff) {
+        const double x = (h->cfg.cfl_glm * mdl) / dt;
+        c = (x < c) ? x : c;
+    }
+    double f = 0.0;
+    if (eff) {
+        const double x = (h->cfg.glm_alpha * c) / (mdl / dt);
+        f = (x > f) ? x : f;
+    }
+    *ch = c;
+    *fac = std::exp(-f);
+}
+
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -399,28 +375,32 @@ int pk_create(const pk_config* cfg, pk_handle* out)
 {
     if (!cfg || !out) return PK_E_ARG;
     *out = nullptr;
-    pk_ctx* h = new pk_ctx();
-    h->cfg = *cfg;
     const pk_config& c = *cfg;
-    int nvf = 0;
     bool ok = c.nfluids >= 1 && c.nfluids <= 3 && c.nb >= 2 && c.cfl > 0.0 && c.cfl <= 1.0 &&
-              (c.integration_order == 1 || c.integration_order == 2);
-    for (int f = 0; ok && f < c.nfluids; ++f) {
+              (c.integration_order == 1 || c.integration_order == 2) && c.limiter >= 0 && c.limiter <= 3 &&
+              c.limiter_b >= 0 && c.limiter_b <= 3;
+    for (int f = 0; ok && f < c.nfluids; ++f)
         if (c.fluid_kind[f] < 0 || c.fluid_kind[f] > 2 || (f > 0 && c.fluid_kind[f] <= c.fluid_kind[f - 1])) ok = false;
+    if (!ok) return PK_E_ARG;
+    // structure of the fluid set: energy fluids then dust; the ionized fluid carries B
+    const int ndst = (c.fluid_kind[c.nfluids - 1] == PK_FLUID_DST) ? 1 : 0;
+    const int nen = c.nfluids - ndst;
+    int phys;
+    if (!c.magnetic && nen == 1 && ndst == 0) phys = 0;
+    else if (!c.magnetic && nen == 1 && ndst == 1) phys = 1;
+    else if (c.magnetic && c.fluid_kind[0] == PK_FLUID_ION && nen == 1 && ndst == 0) phys = 2;
+    else if (c.magnetic && c.fluid_kind[0] == PK_FLUID_ION && nen == 2 && ndst == 0) phys = 3;
+    else if (c.magnetic && c.fluid_kind[0] == PK_FLUID_ION && nen == 2 && ndst == 1) phys = 4;
+    else return PK_E_UNSUPPORTED;
+
+    pk_ctx* h = new pk_ctx();
+    h->cfg = c;
+    h->phys = phys;
+    int nvf = 0;
+    for (int f = 0; f < c.nfluids; ++f) {
         nvf += (c.fluid_kind[f] == PK_FLUID_DST) ? 4 : 5;
         h->pp.gam[f] = (c.fluid_kind[f] == PK_FLUID_DST) ? -1.0 : c.gamma[f];
         h->pp.gam_1[f] = h->pp.gam[f] - 1.0;
-    }
-    ok = ok && c.limiter >= 0 && c.limiter <= 3 && c.limiter_b >= 0 && c.limiter_b <= 3;
-    if (!ok) {
-        delete h;
-        return PK_E_ARG;
-    }
-    if (c.nfluids == 1 && c.fluid_kind[0] != PK_FLUID_DST && !c.magnetic) h->phys = PHYS_HD1;
-    else if (c.nfluids == 1 && c.fluid_kind[0] == PK_FLUID_ION && c.magnetic) h->phys = PHYS_MHD1;
-    else {
-        delete h;
-        return PK_E_UNSUPPORTED;
     }
     h->nvf = nvf;
     h->ib = nvf;
@@ -436,7 +416,10 @@ int pk_create(const pk_config* cfg, pk_handle* out)
     h->ts.dt_old = -1.0;
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&h->d_status, sizeof(unsigned)) != cudaSuccess ||
-        cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&h->d_counter, 8 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&h->d_step, sizeof(StepParams)) != cudaSuccess ||
+        cudaMallocHost(&h->h_step, sizeof(StepParams)) != cudaSuccess || ops_of(h)->prepare(h) != PK_OK) {
         delete h;
         return PK_E_CUDA;
     }
@@ -448,17 +431,24 @@ int pk_destroy(pk_handle h)
 {
     if (!h) return PK_E_ARG;
     cudaStreamSynchronize(h->stream);
+    invalidate_graph(h);
     for (auto& b : h->blocks) {
-        cudaFree(b.u);
+        cudaFree(b.buf[0]);
+        cudaFree(b.buf[1]);
         cudaFree(b.uh);
-        cudaFree(b.tmp);
         cudaFree(b.stage);
     }
     for (auto& p : h->ev_used) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
     for (auto& p : h->ev_free) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+    for (int d = 0; d < 3; ++d) cudaFree(h->batch[d].dev);
+    cudaFree(h->d_desc[0]);
+    cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
+    cudaFree(h->d_counter);
     cudaFree(h->d_red);
+    cudaFree(h->d_step);
     cudaFreeHost(h->h_red);
+    cudaFreeHost(h->h_step);
     cudaStreamDestroy(h->stream);
     delete h;
     return PK_OK;
@@ -484,22 +474,29 @@ int pk_block_add(pk_handle h, const int32_t n[3], const double dl[3], const int3
         }
         if (n[d] > 1 && n[d] < h->cfg.nb && b.bnd[d][0] == PK_BND_PER)
             return fail(h, PK_E_ARG, "periodic direction shorter than the guard width");
+        if (!h->blocks.empty() && ((h->blocks[0].n[d] > 1) != (n[d] > 1)))
+            return fail(h, PK_E_ARG, "all blocks must have the same directions (dom%has_dir)");
     }
     if (h->cfg.magnetic)
         for (int d = 0; d < 3; ++d)
             if (b.n[d] > 1 && (b.bnd[d][0] != PK_BND_PER || b.bnd[d][1] != PK_BND_PER))
                 return fail(h, PK_E_UNSUPPORTED, "magnetised blocks support periodic boundaries only");
     b.plane = (long long)b.ext[0] * b.ext[1] * b.ext[2];
-    if (cudaMalloc(&b.u, sizeof(double) * h->nplanes * b.plane) != cudaSuccess)
+    double* p = nullptr;
+    if (cudaMalloc(&p, sizeof(double) * h->nplanes * b.plane) != cudaSuccess)
         return fail(h, PK_E_NOMEM, "cudaMalloc of the block state failed");
-    PK_CUDA(h, cudaMemsetAsync(b.u, 0, sizeof(double) * h->nplanes * b.plane, h->stream));
+    PK_CUDA(h, cudaMemsetAsync(p, 0, sizeof(double) * h->nplanes * b.plane, h->stream));
+    b.buf[h->cur] = p;                      // the state lives in the current parity's buffer
     h->blocks.push_back(b);
+    h->batch_dirty = true;
+    invalidate_graph(h);
     if (id_out) *id_out = (int32_t)h->blocks.size() - 1;
     const int need = (int)h->blocks.size() * 12;
     if (need > h->red_cap) {
+        PK_CUDA(h, cudaStreamSynchronize(h->stream));
         cudaFree(h->d_red);
         cudaFreeHost(h->h_red);
-        h->red_cap = need + 120;
+        h->red_cap = need + 1200;
         PK_CUDA(h, cudaMalloc(&h->d_red, sizeof(unsigned long long) * h->red_cap));
         PK_CUDA(h, cudaMallocHost(&h->h_red, sizeof(unsigned long long) * h->red_cap));
     }
@@ -520,27 +517,31 @@ int pk_upload(pk_handle h, int32_t id, const double* u, const double* bf, const 
     if (int rc = get_block(h, id, &b)) return rc;
     if (!u || (h->cfg.magnetic && (!bf || !psi))) return fail(h, PK_E_ARG, "null array");
     const long long nc = b->plane;
+    double* s = state(h, *b);
     if (layout == PK_LAYOUT_SOA) {
-        PK_CUDA(h, cudaMemcpyAsync(b->u, u, sizeof(double) * h->nvf * nc, cudaMemcpyHostToDevice, h->stream));
+        PK_CUDA(h, cudaMemcpyAsync(s, u, sizeof(double) * h->nvf * nc, cudaMemcpyHostToDevice, h->stream));
         if (h->cfg.magnetic) {
-            PK_CUDA(h, cudaMemcpyAsync(b->u + (long long)h->ib * nc, bf, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice, h->stream));
-            PK_CUDA(h, cudaMemcpyAsync(b->u + (long long)(h->ib + 3) * nc, psi, sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream));
+            PK_CUDA(h, cudaMemcpyAsync(s + (long long)h->ib * nc, bf, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice, h->stream));
+            PK_CUDA(h, cudaMemcpyAsync(s + (long long)(h->ib + 3) * nc, psi, sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream));
         }
     } else if (layout == PK_LAYOUT_FORTRAN) {
         if (!b->stage) PK_CUDA(h, cudaMalloc(&b->stage, sizeof(double) * h->nvf * nc));
         PK_CUDA(h, cudaMemcpyAsync(b->stage, u, sizeof(double) * h->nvf * nc, cudaMemcpyHostToDevice, h->stream));
-        k_aos_to_soa<<<grid1d(nc, 256), 256, 0, h->stream>>>(b->stage, b->u, nc, h->nvf, 0, nc);
-        PK_CUDA(h, cudaGetLastError()); h->launches += 1;
+        k_aos_to_soa<<<grid1d(nc, 256), 256, 0, h->stream>>>(b->stage, s, nc, h->nvf, 0, nc);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
         if (h->cfg.magnetic) {
             // the staging buffer is reused once the first conversion has run (same stream)
             PK_CUDA(h, cudaMemcpyAsync(b->stage, bf, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice, h->stream));
-            k_aos_to_soa<<<grid1d(nc, 256), 256, 0, h->stream>>>(b->stage, b->u, nc, 3, h->ib, nc);
-            PK_CUDA(h, cudaGetLastError()); h->launches += 1;
-            PK_CUDA(h, cudaMemcpyAsync(b->u + (long long)(h->ib + 3) * nc, psi, sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream));
+            k_aos_to_soa<<<grid1d(nc, 256), 256, 0, h->stream>>>(b->stage, s, nc, 3, h->ib, nc);
+            PK_CUDA(h, cudaGetLastError());
+            h->launches += 1;
+            PK_CUDA(h, cudaMemcpyAsync(s + (long long)(h->ib + 3) * nc, psi, sizeof(double) * nc, cudaMemcpyHostToDevice, h->stream));
         }
     } else {
         return fail(h, PK_E_ARG, "unknown layout");
     }
+    b->guards_stale = false;
     return PK_OK;
 }
 
@@ -552,23 +553,26 @@ int pk_download(pk_handle h, int32_t id, double* u, double* bf, double* psi, int
     if (b->guards_stale)
         if (int rc = fill_guards_block(h, *b)) return rc;
     const long long nc = b->plane;
+    double* s = state(h, *b);
     if (layout == PK_LAYOUT_SOA) {
-        PK_CUDA(h, cudaMemcpyAsync(u, b->u, sizeof(double) * h->nvf * nc, cudaMemcpyDeviceToHost, h->stream));
+        PK_CUDA(h, cudaMemcpyAsync(u, s, sizeof(double) * h->nvf * nc, cudaMemcpyDeviceToHost, h->stream));
         if (h->cfg.magnetic) {
-            PK_CUDA(h, cudaMemcpyAsync(bf, b->u + (long long)h->ib * nc, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream));
-            PK_CUDA(h, cudaMemcpyAsync(psi, b->u + (long long)(h->ib + 3) * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream));
+            PK_CUDA(h, cudaMemcpyAsync(bf, s + (long long)h->ib * nc, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream));
+            PK_CUDA(h, cudaMemcpyAsync(psi, s + (long long)(h->ib + 3) * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream));
         }
     } else if (layout == PK_LAYOUT_FORTRAN) {
         if (!b->stage) PK_CUDA(h, cudaMalloc(&b->stage, sizeof(double) * h->nvf * nc));
-        k_soa_to_aos<<<grid1d(nc, 256), 256, 0, h->stream>>>(b->u, b->stage, nc, h->nvf, 0, nc);
-        PK_CUDA(h, cudaGetLastError()); h->launches += 1;
+        k_soa_to_aos<<<grid1d(nc, 256), 256, 0, h->stream>>>(s, b->stage, nc, h->nvf, 0, nc);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
         PK_CUDA(h, cudaMemcpyAsync(u, b->stage, sizeof(double) * h->nvf * nc, cudaMemcpyDeviceToHost, h->stream));
         if (h->cfg.magnetic) {
             PK_CUDA(h, cudaStreamSynchronize(h->stream));   // the staging buffer is reused for b
-            k_soa_to_aos<<<grid1d(nc, 256), 256, 0, h->stream>>>(b->u, b->stage, nc, 3, h->ib, nc);
-            PK_CUDA(h, cudaGetLastError()); h->launches += 1;
+            k_soa_to_aos<<<grid1d(nc, 256), 256, 0, h->stream>>>(s, b->stage, nc, 3, h->ib, nc);
+            PK_CUDA(h, cudaGetLastError());
+            h->launches += 1;
             PK_CUDA(h, cudaMemcpyAsync(bf, b->stage, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, h->stream));
-            PK_CUDA(h, cudaMemcpyAsync(psi, b->u + (long long)(h->ib + 3) * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream));
+            PK_CUDA(h, cudaMemcpyAsync(psi, s + (long long)(h->ib + 3) * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, h->stream));
         }
     } else {
         return fail(h, PK_E_ARG, "unknown layout");
@@ -592,8 +596,11 @@ int pk_solve_cg(pk_handle h, int32_t id, int32_t ddim, int32_t istep, double dt,
     if (b->n[dir] <= 1) return PK_OK;
     if (b->guards_stale)
         if (int rc = fill_guards_block(h, *b)) return rc;
+    if (!b->uh) PK_CUDA(h, cudaMalloc(&b->uh, sizeof(double) * h->nplanes * b->plane));
+    if (b->ext[dir] > STAGE_MAXT)
+        if (int rc = ensure_pingpong(h)) return rc;
     const double dtodx = (rk * dt) / b->dl[dir];   // rk_coef(istep) * dt / cg%dl(ddim)
-    return dispatch_stage(h, *b, dir, first, dtodx, chspeed);
+    return ops_of(h)->stage(h, *b, dir, first, dtodx, chspeed);
 }
 
 int pk_fill_guards(pk_handle h)
@@ -608,7 +615,8 @@ int pk_sweep(pk_handle h, int32_t cdim, double dt, double chspeed)
 {
     if (!h) return PK_E_ARG;
     if (cdim < 1 || cdim > 3) return fail(h, PK_E_ARG, "cdim must be 1..3");
-    return sweep_impl(h, cdim - 1, dt, chspeed, 1.0);
+    if (int rc = put_step_params(h, dt, chspeed, 1.0)) return rc;
+    return sweep_impl(h, cdim - 1, dt, chspeed, 0, 1.0);
 }
 
 int pk_glm_damp(pk_handle h, double fac)
@@ -636,10 +644,16 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out)
     }
     a.magnetic = h->cfg.magnetic;
     a.ib = h->ib;
-    for (int i = 0; i < nb; ++i) {
-        Block& b = h->blocks[i];
+    if (nb > 1) {
+        if (int rc = build_batch(h)) return rc;
+        dim3 grid(64, nb);
+        k_cfl_blocks<<<grid, 256, 0, h->stream>>>(h->d_desc[h->cur], a, h->d_red);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+    } else {
+        Block& b = h->blocks[0];
         const long long ncell = (long long)b.n[0] * b.n[1] * b.n[2];
-        k_cfl<<<grid1d(ncell, 256), 256, 0, h->stream>>>(box_of(b), b.u, a, h->d_red + 12 * i);
+        k_cfl<<<grid1d(ncell, 256), 256, 0, h->stream>>>(box_of(b), state(h, b), a, h->d_red);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
@@ -704,42 +718,42 @@ int pk_time_step(pk_handle h, double* dt_out)
 int pk_fluid_update(pk_handle h)
 {
     if (!h) return PK_E_ARG;
+    if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
     const double dt = h->ts.dt;
-    int eff;
-    const double mdl = min_dl(h, &eff);
-    if (h->cfg.magnetic) {                            // update_chspeed, hdc.F90:112-119
-        double ch = DBL_MAX;
-        if (eff) {
-            const double x = (h->cfg.cfl_glm * mdl) / dt;
-            ch = (x < ch) ? x : ch;
+    double ch, fac;
+    glm_scalars(h, dt, &ch, &fac);
+    h->ts.chspeed = ch;
+    if (int rc = put_step_params(h, dt, ch, fac)) return rc;
+    if (h->use_graph && !h->profiling) {
+        if (fused_ok(h) && h->blocks.size() > 1)
+            if (int rc = build_batch(h)) return rc;   // tables are built outside the capture
+        if (int rc = ensure_pingpong(h)) return rc;
+        for (auto& b : h->blocks)
+            if (!b.uh && !fused_ok(h)) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+        if (!h->graph_exec) {
+            // capture the sweeps of one step once; the step scalars are read from d_step
+            const int cur0 = h->cur;
+            PK_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = step_sweeps(h, dt, ch, fac);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+            h->cur = cur0;   // 2 x (number of directions) sweeps: the parity is back where it was
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return fail(h, PK_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            h->graph = g;
+            PK_CUDA(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
         }
-        h->ts.chspeed = ch;
+        PK_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+        if (fused_ok(h))
+            for (auto& b : h->blocks) b.guards_stale = true;
+    } else {
+        if (int rc = step_sweeps(h, dt, ch, fac)) return rc;
     }
-    double fac = 1.0;
-    if (h->cfg.magnetic) {                            // glmdamping, hdc.F90:310-330
-        double f = 0.0;
-        if (eff) {
-            const double x = (h->cfg.glm_alpha * h->ts.chspeed) / (mdl / dt);
-            f = (x > f) ? x : f;
-        }
-        fac = std::exp(-f);
-    }
-    int dirs[3], nd = 0;
-    for (int d = 0; d < 3; ++d) {
-        bool has = false;
-        for (auto& b : h->blocks) has = has || b.n[d] > 1;
-        if (has && !h->cfg.skip_sweep[d]) dirs[nd++] = d;
-    }
-    for (int half = 0; half < 2; ++half) {            // fluidupdate.F90:115-130
-        h->ts.t = h->ts.t + dt;
-        for (int s = 0; s < nd; ++s) {
-            const int d = half == 0 ? dirs[s] : dirs[nd - 1 - s];
-            const double pf = (h->cfg.magnetic && s == nd - 1) ? fac : 1.0;
-            if (int rc = sweep_impl(h, d, dt, h->ts.chspeed, pf)) return rc;
-        }
-        if (h->cfg.magnetic && nd == 0)
-            if (int rc = glm_scale(h, fac)) return rc;
-    }
+    h->ts.t = h->ts.t + dt;                            // fluidupdate.F90:116
+    h->ts.t = h->ts.t + dt;                            // :126
     return PK_OK;
 }
 
@@ -790,11 +804,34 @@ int pk_sync(pk_handle h)
 int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32_t variant)
 {
     if (!h || dir < 0 || dir > 2 || pencils < 0 || length < 0 || variant < -1 || variant >= NVARIANT) return PK_E_ARG;
-    const int maxt = VAR_T[variant >= 0 ? variant : DEF_VARIANT[dir]];
+    const int maxt = VAR_T[variant >= 0 ? variant : 0];
     if (length > 0 && length + 8 > maxt) return fail(h, PK_E_ARG, "length + 8 exceeds the variant's CTA size");
     h->tileP[dir] = pencils;
     h->tileL[dir] = length;
     h->tileV[dir] = variant;
+    invalidate_graph(h);
+    return PK_OK;
+}
+
+int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant)
+{
+    if (!h || length < 0 || variant < -1 || variant >= NVARIANT) return PK_E_ARG;
+    const int v = variant >= 0 ? variant : h->batch_variant;
+    const int L = length > 0 ? length : h->batch_L;
+    if (L + 8 > VAR_T[v]) return fail(h, PK_E_ARG, "length + 8 exceeds the variant's CTA size");
+    h->batched = enable != 0;
+    h->batch_variant = v;
+    h->batch_L = L;
+    h->batch_dirty = true;
+    invalidate_graph(h);
+    return PK_OK;
+}
+
+int pk_use_graph(pk_handle h, int32_t enable)
+{
+    if (!h) return PK_E_ARG;
+    h->use_graph = enable != 0;
+    invalidate_graph(h);
     return PK_OK;
 }
 

@@ -2,6 +2,7 @@
 // damping, guard-cell refresh, host-layout conversion.
 #pragma once
 #include "pk_device.cuh"
+#include "pk_kernels.cuh"
 
 namespace pk {
 
@@ -35,7 +36,8 @@ struct CflArgs {
 // reduction with one division per direction.  Maxima of positive doubles are
 // reduced as their bit patterns (order-independent, deterministic).
 // out[f*4 + d] (d < 3) and out[f*4 + 3] hold the bit patterns.
-__global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsigned long long* __restrict__ out)
+PK_DEV void cfl_block(const BoxGeom& b, const double* __restrict__ u, const CflArgs& a, unsigned long long* __restrict__ out,
+                      long long first, long long stride)
 {
     const double small = 1.1754943508222875e-38;   // tiny(real(1.0,4)), constants.F90:104
     const long long ncell = (long long)b.n[0] * b.n[1] * b.n[2];
@@ -44,7 +46,7 @@ __global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsign
     for (int f = 0; f < 3; ++f)
 #pragma unroll
         for (int d = 0; d < 4; ++d) cm[f][d] = small;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+    for (long long c = first; c < ncell; c += stride) {
         const int i = (int)(c % b.n[0]);
         const long long r = c / b.n[0];
         const int j = (int)(r % b.n[1]);
@@ -116,8 +118,28 @@ __global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsign
     }
 }
 
+static __global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsigned long long* __restrict__ out)
+{
+    cfl_block(b, u, a, out, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
+// the same over a table of blocks: blockIdx.y picks the block, out has 12 slots per block
+static __global__ void k_cfl_blocks(const BlockDesc* __restrict__ blocks, CflArgs a, unsigned long long* __restrict__ out)
+{
+    const BlockDesc d = blocks[blockIdx.y];
+    BoxGeom b;
+    for (int k = 0; k < 3; ++k) {
+        b.ext[k] = d.ext[k];
+        b.g[k] = d.g[k];
+        b.n[k] = d.n[k];
+    }
+    b.plane = d.plane;
+    cfl_block(b, d.in, a, out + 12 * blockIdx.y, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+              (long long)gridDim.x * blockDim.x);
+}
+
 // psi *= fac over the whole plane, guard cells included (hdc.F90:338)
-__global__ void k_scale(double* __restrict__ p, long long n, double fac)
+static __global__ void k_scale(double* __restrict__ p, long long n, double fac)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         p[i] = p[i] * fac;
@@ -153,7 +175,7 @@ __device__ __forceinline__ int map_guard(int i, int n, int g, int side_lo, int s
     return g + n - ib;
 }
 
-__global__ void k_fill_guards(BoxGeom b, double* __restrict__ u, GuardArgs a)
+static __global__ void k_fill_guards(BoxGeom b, double* __restrict__ u, GuardArgs a)
 {
     const long long ncell = (long long)b.ext[0] * b.ext[1] * b.ext[2];
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
@@ -180,14 +202,14 @@ __global__ void k_fill_guards(BoxGeom b, double* __restrict__ u, GuardArgs a)
 }
 
 // Fortran-order arrays (u(nvar,i,j,k), b(3,i,j,k), psi(i,j,k)) <-> component planes.
-__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long long ncell, int ncomp,
+static __global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long long ncell, int ncomp,
                              int plane0, long long plane)
 {
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
         for (int v = 0; v < ncomp; ++v) soa[(long long)(plane0 + v) * plane + c] = aos[c * ncomp + v];
 }
 
-__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, long long ncell, int ncomp,
+static __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, long long ncell, int ncomp,
                              int plane0, long long plane)
 {
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
@@ -196,7 +218,7 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
 
 // copy the pencils a stage touched (full extent along dir, interior in the
 // other two directions) from src to dst, all planes
-__global__ void k_copy_pencils(BoxGeom b, int dir, const double* __restrict__ src, double* __restrict__ dst, int nplanes)
+static __global__ void k_copy_pencils(BoxGeom b, int dir, const double* __restrict__ src, double* __restrict__ dst, int nplanes)
 {
     int lo[3], hi[3];
     for (int d = 0; d < 3; ++d) {

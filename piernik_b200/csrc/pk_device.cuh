@@ -500,6 +500,54 @@ PK_DEV void riemann(const double (&ql)[PH::NV], const double (&qr)[PH::NV], doub
     }
 }
 
+// The same for a tile in shared memory: left states at L[v*PT + me], right
+// states at R[v*PT + me + st], fluxes written to F[v*PT + me].  Each fluid's
+// states are loaded just before its solve, so the register footprint does not
+// grow with the number of fluids.
+template <class PH>
+PK_DEV void riemann_tile(const double* __restrict__ L, const double* __restrict__ R, double* __restrict__ F, int PT,
+                         int me, int st, double ch, const PhysParams& pp)
+{
+    double blv[3] = {0.0, 0.0, 0.0}, brv[3] = {0.0, 0.0, 0.0};
+    if (PH::MHD) {
+        const double bxl = L[PH::IB * PT + me], bxr = R[PH::IB * PT + me + st];
+        const double psl = L[(PH::IB + 3) * PT + me], psr = R[(PH::IB + 3) * PT + me + st];
+        F[(PH::IB + 3) * PT + me] = ((ch * ch) * 0.5) * ((bxr + bxl) - (psr - psl) / ch);   // hlld.F90:229
+        F[PH::IB * PT + me] = 0.5 * ((psr + psl) - ch * (bxr - bxl));                      // :230
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            blv[c] = L[(PH::IB + c) * PT + me];
+            brv[c] = R[(PH::IB + c) * PT + me + st];
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < PH::NFL; ++f) {
+        const int b = PH::beg(f);
+        const int nc = PH::ncomp(PH::kind(f));
+        double ul[5] = {0, 0, 0, 0, 0}, ur[5] = {0, 0, 0, 0, 0}, fv[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            if (c < nc) {
+                ul[c] = L[(b + c) * PT + me];
+                ur[c] = R[(b + c) * PT + me + st];
+            }
+        if (PH::MHD) {
+            const double zero[3] = {0.0, 0.0, 0.0};
+            double bf[2];
+            hlld_iface(PH::has_en(f), pp.gam[f], ul, ur, PH::magn(f) ? blv : zero, PH::magn(f) ? brv : zero, fv, bf);
+            if (PH::magn(f)) {
+                F[(PH::IB + 1) * PT + me] = bf[0];
+                F[(PH::IB + 2) * PT + me] = bf[1];
+            }
+        } else {
+            hllc_iface(PH::has_en(f), pp.gam[f], ul, ur, fv);
+        }
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            if (c < nc) F[(b + c) * PT + me] = fv[c];
+    }
+}
+
 // internal_sources (+0 added to every fluid component) and care_for_positives
 // on one updated cell; B used for emag is the updated one (b1).
 template <class PH>

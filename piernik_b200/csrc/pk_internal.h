@@ -1,0 +1,109 @@
+// pk_internal.h -- host-side state of a library handle, shared by the C ABI
+// (pk_api.cu) and the per-physics launch units (pk_phys_*.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/piernik_b200.h"
+#include "pk_kernels.cuh"
+
+namespace pk {
+
+// Launch-bound variants of the fused sweep (threads per CTA, CTAs per SM):
+// the register budget the compiler may use is 65536 / (threads * CTAs);
+// tighter budgets trade spills for resident warps.  The autotuner picks one
+// per direction.
+constexpr int NVARIANT = 6;
+constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192};
+constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2};
+constexpr int STAGE_MAXT = 320;        // threads per CTA of the stage kernel
+
+struct Block {
+    int n[3], g[3], ext[3];
+    double dl[3];
+    int bnd[3][2];
+    long long plane = 0;
+    double* buf[2] = {nullptr, nullptr};   // state and its ping-pong partner
+    double* uh = nullptr;                  // stage path: state at the start of the step (cg%w(uh))
+    double* stage = nullptr;               // host-layout conversion buffer
+    bool guards_stale = false;             // fused sweeps read periodic images and never store guards
+};
+
+struct pk_dir_tile { int P, L, V; };
+
+// work list of the batched sweep for one direction
+struct BatchList {
+    std::vector<WorkItem> host;
+    WorkItem* dev = nullptr;
+    int n = 0;
+};
+
+}  // namespace pk
+
+struct pk_ctx {
+    pk_config cfg;
+    pk::PhysParams pp;
+    int phys = 0;
+    int nvf = 0, nplanes = 0, ib = 0;
+    std::vector<pk::Block> blocks;
+    int cur = 0;                        // which of Block::buf holds the state (all blocks alike)
+    cudaStream_t stream = nullptr;
+    unsigned* d_status = nullptr;
+    unsigned* d_counter = nullptr;      // work-list counters of the batched sweep (one per launch slot)
+    unsigned long long* d_red = nullptr;
+    unsigned long long* h_red = nullptr;
+    int red_cap = 0;
+    pk::StepParams* d_step = nullptr;   // device copy of the step scalars
+    pk::StepParams* h_step = nullptr;   // pinned host copy
+    pk::BlockDesc* d_desc[2] = {nullptr, nullptr};   // block tables for cur = 0 / 1
+    bool batch_dirty = true;
+    pk::BatchList batch[3];
+    pk_time_state ts;
+    std::string err;
+    int tileP[3] = {0, 0, 0}, tileL[3] = {0, 0, 0}, tileV[3] = {-1, -1, -1};
+    int batched = 0;                    // 1: sweep all blocks in one persistent launch
+    int batch_variant = 2;              // launch-bound variant of the batched kernel
+    int batch_L = 56;                   // longest chunk of the batched tiles
+    long long launches = 0;             // kernels of this library launched on the handle's stream
+    bool profiling = false;             // bracket sweep kernels with CUDA events
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used, ev_free;
+    cudaGraph_t graph = nullptr;        // captured sweeps of one step (pk_run with graphs)
+    cudaGraphExec_t graph_exec = nullptr;
+    int use_graph = 0;
+};
+
+namespace pk {
+
+int fail(pk_ctx* h, int code, const std::string& msg);
+int ev_begin(pk_ctx* h, std::pair<cudaEvent_t, cudaEvent_t>* p);
+int ev_end(pk_ctx* h, const std::pair<cudaEvent_t, cudaEvent_t>& p);
+Geom make_geom(const Block& b, int dir);
+
+// launches of one physics configuration (pk_phys_*.cu)
+struct PhysOps {
+    int nv;
+    int (*prepare)(pk_ctx* h);      // kernel attributes; called before any launch or graph capture
+    int (*fused)(pk_ctx* h, Block& b, int dir, int apply_fac);
+    int (*stage)(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch);
+    int (*batched)(pk_ctx* h, int dir, int apply_fac, unsigned* counter);
+};
+
+const PhysOps* ops_hd1();
+const PhysOps* ops_hd2();
+const PhysOps* ops_mhd1();
+const PhysOps* ops_mhd2();
+const PhysOps* ops_mhd3();
+
+}  // namespace pk
+
+#define PK_CUDA(h, call)                                                                      \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+            return PK_E_CUDA;                                                                 \
+        }                                                                                     \
+    } while (0)

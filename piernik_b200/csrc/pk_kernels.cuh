@@ -135,17 +135,7 @@ PK_DEV void rk_stage(const Smem& sm, int me, int st, const Roles& r, double (&w)
         }
     }
     __syncthreads();
-    if (r.flux) {
-        double ql[NV], qr[NV], fx[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            ql[v] = sm.L[v * PT + me];
-            qr[v] = sm.R[v * PT + me + st];
-        }
-        riemann<PH>(ql, qr, ch, pp, fx);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = fx[v];
-    }
+    if (r.flux) riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, st, ch, pp);
     __syncthreads();
     if (r.upd) {
         double u0[NV];
@@ -171,17 +161,22 @@ PK_DEV int wrap(int s, int n)
     return r < 0 ? r + n : r;
 }
 
-// -------------------------------------------------------------------------
-// Fused two-stage sweep of a periodic block: uin -> uout.
-// grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2.
-// -------------------------------------------------------------------------
-template <class PH, int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
-                                                     double* __restrict__ uout, PhysParams pp, double dtodx1,
-                                                     double dtodx2, double ch, double psi_fac,
-                                                     unsigned* __restrict__ gstatus)
+// Scalars of one step that change from step to step.  Kernels read them from
+// device memory so that a captured CUDA graph of the step stays valid.
+struct StepParams {
+    double dt;        // time step
+    double ch;        // GLM psi speed (update_chspeed)
+    double psi_fac;   // glmdamping factor, applied by the last sweep of each triple
+};
+
+// One tile of the fused two-stage sweep of a periodic block (uin -> uout):
+// P pencils starting at ortho-1 index i1_0, output cells [c0, c0+L) along the
+// sweep, ortho-2 index i2.  The tile reads a 4-cell halo with periodic wrap.
+template <class PH>
+PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
+                       const PhysParams& pp, double dtodx1, double dtodx2, double ch, double psi_fac,
+                       double* smem, unsigned& status)
 {
-    extern __shared__ double smem[];
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
     const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
@@ -191,9 +186,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, con
     else { p = tid % P; t = tid / P; }
     const int sp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
     const int me = p * sp + t * st;
-    const int i1 = blockIdx.x * P + p;
-    const int c0 = blockIdx.y * tl.L;
-    const int i2 = blockIdx.z;
+    const int i1 = i1_0 + p;
     const bool active = (tid < PT) && (i1 < g.n1);
     const int s = c0 - 4 + t;                                  // position along the pencil (interior coords)
     const long long off = (long long)(g.g_d + wrap(s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
@@ -202,7 +195,6 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, con
 #pragma unroll
     for (int v = 0; v < NV; ++v) w[v] = 0.0;
     if (active) load_cell<PH>(uin, off, g, w);
-    unsigned status = 0;
     Roles r;
     r.end = 0;
     r.keep = false;
@@ -221,6 +213,93 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, con
     if (r.upd && s < c0 + tl.L && s < g.n_d) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);
+    }
+}
+
+// -------------------------------------------------------------------------
+// Fused two-stage sweep of one periodic block.
+// grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2.
+// -------------------------------------------------------------------------
+template <class PH, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
+                                                           double* __restrict__ uout, PhysParams pp, double dl,
+                                                           const StepParams* __restrict__ sp, int apply_fac,
+                                                           unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    const double dt = sp->dt;
+    const double dtodx1 = (0.5 * dt) / dl;        // rk_coef(RK2_1) * dt / cg%dl(ddim)
+    const double dtodx2 = (1.0 * dt) / dl;        // rk_coef(RK2_2) * dt / cg%dl(ddim)
+    unsigned status = 0;
+    fused_tile<PH>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, dtodx1, dtodx2, sp->ch,
+                   apply_fac ? sp->psi_fac : 1.0, smem, status);
+    flush_status(status, gstatus);
+}
+
+// -------------------------------------------------------------------------
+// Batched fused sweep over many periodic blocks of different sizes: one
+// persistent launch; CTAs take tiles from a work list through an atomic
+// counter (reset to zero before each launch).
+// -------------------------------------------------------------------------
+struct BlockDesc {
+    const double* in;       // the sweep's input state (structure of arrays with guards)
+    double* out;            // where the swept state goes
+    long long plane;
+    int ext[3], g[3], n[3];
+    double dl[3];
+};
+
+struct WorkItem {
+    int block;              // index into the block table
+    int i1_0, c0, i2;       // first pencil, first output cell, ortho-2 index
+    int P, L;               // tile of this item (T = L + 8)
+};
+
+template <class PH, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* __restrict__ blocks,
+                                                             const WorkItem* __restrict__ items, int nitems, int dir,
+                                                             PhysParams pp, const StepParams* __restrict__ sp,
+                                                             int apply_fac, unsigned* __restrict__ counter,
+                                                             unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    __shared__ int next;
+    const int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;
+    const double dt = sp->dt, ch = sp->ch, fac = apply_fac ? sp->psi_fac : 1.0;
+    unsigned status = 0;
+    for (;;) {
+        if (threadIdx.x == 0) next = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = next;
+        __syncthreads();
+        if (it >= nitems) break;
+        const WorkItem w = items[it];
+        const BlockDesc b = blocks[w.block];
+        Geom g;
+        const long long st3[3] = {1, b.ext[0], (long long)b.ext[0] * b.ext[1]};
+        g.plane = b.plane;
+        g.sd = st3[dir];
+        g.s1 = st3[o1];
+        g.s2 = st3[o2];
+        g.ext_d = b.ext[dir];
+        g.n_d = b.n[dir];
+        g.g_d = b.g[dir];
+        g.n1 = b.n[o1];
+        g.g1 = b.g[o1];
+        g.n2 = b.n[o2];
+        g.g2 = b.g[o2];
+        g.perm[0] = dir;                          // iarr_swp: (x,y,z) (y,x,z) (z,y,x)
+        g.perm[1] = dir == 1 ? 0 : 1;
+        g.perm[2] = dir == 2 ? 0 : 2;
+        Tile tl;
+        tl.P = w.P;
+        tl.L = w.L;
+        tl.T = w.L + 8;
+        tl.xfast = dir == 0;
+        tl.halo = 4;
+        const double dl = b.dl[dir];
+        fused_tile<PH>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, (0.5 * dt) / dl, (1.0 * dt) / dl, ch, fac, smem,
+                       status);
     }
     flush_status(status, gstatus);
 }

@@ -1,0 +1,184 @@
+// pk_launch.cuh -- kernel launches for one physics configuration PH.  Each
+// pk_phys_*.cu instantiates these for its PH, so the heavy kernels compile in
+// parallel translation units.
+#pragma once
+#include "pk_aux.cuh"
+#include "pk_internal.h"
+
+namespace pk {
+
+template <class PH>
+using FusedFn = void (*)(Geom, Tile, const double*, double*, PhysParams, double, const StepParams*, int, unsigned*);
+template <class PH>
+using BatchedFn = void (*)(const BlockDesc*, const WorkItem*, int, int, PhysParams, const StepParams*, int, unsigned*,
+                           unsigned*);
+
+template <class PH>
+FusedFn<PH> fused_variant(int v)
+{
+    switch (v) {
+    case 0: return k_sweep_fused<PH, 320, 1>;
+    case 1: return k_sweep_fused<PH, 256, 1>;
+    case 2: return k_sweep_fused<PH, 256, 2>;
+    case 3: return k_sweep_fused<PH, 128, 3>;
+    case 4: return k_sweep_fused<PH, 128, 4>;
+    default: return k_sweep_fused<PH, 192, 2>;
+    }
+}
+
+template <class PH>
+BatchedFn<PH> batched_variant(int v)
+{
+    switch (v) {
+    case 0: return k_sweep_batched<PH, 320, 1>;
+    case 1: return k_sweep_batched<PH, 256, 1>;
+    case 2: return k_sweep_batched<PH, 256, 2>;
+    case 3: return k_sweep_batched<PH, 128, 3>;
+    case 4: return k_sweep_batched<PH, 128, 4>;
+    default: return k_sweep_batched<PH, 192, 2>;
+    }
+}
+
+template <class PH>
+int set_smem_attr(pk_ctx* h)
+{
+    static bool done = false;
+    if (!done) {
+        for (int v = 0; v < NVARIANT; ++v) {
+            PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        }
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        done = true;
+    }
+    return PK_OK;
+}
+
+constexpr int DEF_VARIANT[3] = {0, 0, 0};
+constexpr int DEF_P[3] = {2, 4, 4};
+constexpr int DEF_L[3] = {64, 64, 64};
+
+template <class PH>
+int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
+{
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    Geom g = make_geom(b, dir);
+    Tile tl;
+    int L = h->tileL[dir] > 0 ? h->tileL[dir] : DEF_L[dir];
+    if (L > b.n[dir]) L = b.n[dir];
+    int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
+    if (P > g.n1) P = g.n1;
+    const int var = h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir];
+    const int maxt = VAR_T[var];
+    int T = L + 8;
+    while (P * T > maxt && P > 1) --P;
+    if (P * T > maxt) return fail(h, PK_E_ARG, "fused sweep tile longer than the variant's CTA size");
+    tl.P = P;
+    tl.T = T;
+    tl.L = L;
+    tl.halo = 4;
+    tl.xfast = (dir == 0);
+    dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
+    const size_t smem = 3ull * PH::NV * P * T * sizeof(double);
+    double* in = b.buf[h->cur];
+    double* out = b.buf[1 - h->cur];
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+    fused_variant<PH>(var)<<<grid, P * T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir], h->d_step, apply_fac,
+                                                            h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+    h->launches += 1;
+    b.guards_stale = true;
+    return PK_OK;
+}
+
+template <class PH>
+int launch_batched(pk_ctx* h, int dir, int apply_fac, unsigned* counter)
+{
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    BatchList& bl = h->batch[dir];
+    if (bl.n == 0) return PK_OK;
+    const int var = h->batch_variant;
+    int maxP = 1;
+    for (const auto& w : bl.host) maxP = (w.P * (w.L + 8) > maxP) ? w.P * (w.L + 8) : maxP;
+    const int threads = VAR_T[var];
+    const size_t smem = 3ull * PH::NV * threads * sizeof(double);
+    int dev = 0, nsm = 0, per_sm = 0;
+    PK_CUDA(h, cudaGetDevice(&dev));
+    PK_CUDA(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_variant<PH>(var), threads, smem));
+    if (per_sm < 1) return fail(h, PK_E_ARG, "batched sweep tile does not fit on an SM");
+    int grid = nsm * per_sm;
+    if (grid > bl.n) grid = bl.n;
+    PK_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream));
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+    batched_variant<PH>(var)<<<grid, threads, smem, h->stream>>>(h->d_desc[h->cur], bl.dev, bl.n, dir, h->pp,
+                                                                 h->d_step, apply_fac, counter, h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+    h->launches += 1;
+    (void)maxP;
+    return PK_OK;
+}
+
+template <class PH>
+int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch)
+{
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    Geom g = make_geom(b, dir);
+    Tile tl;
+    const int ext = b.ext[dir];
+    double* u = b.buf[h->cur];
+    double* uout = u;
+    if (ext <= STAGE_MAXT) {                 // whole pencil per tile: in place
+        int P = STAGE_MAXT / ext;
+        if (P >= 4) P -= P % 4;
+        if (P > g.n1) P = g.n1;
+        tl.P = P;
+        tl.T = ext;
+        tl.L = ext;
+        tl.halo = 0;
+    } else {                                 // chunked with a 2-cell halo: out of place
+        tl.P = 4;
+        tl.L = 64;
+        tl.T = tl.L + 4;
+        tl.halo = 2;
+        uout = b.buf[1 - h->cur];
+    }
+    tl.xfast = (dir == 0);
+    dim3 grid((g.n1 + tl.P - 1) / tl.P, (ext + tl.L - 1) / tl.L, g.n2);
+    const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+    k_stage<PH, STAGE_MAXT><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx, ch,
+                                                                   h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+    h->launches += 1;
+    if (uout != u) {
+        BoxGeom bg;
+        for (int d = 0; d < 3; ++d) {
+            bg.ext[d] = b.ext[d];
+            bg.g[d] = b.g[d];
+            bg.n[d] = b.n[d];
+        }
+        bg.plane = b.plane;
+        long long nb = (b.plane + 255) / 256;
+        if (nb > 148LL * 16) nb = 148LL * 16;
+        k_copy_pencils<<<(int)nb, 256, 0, h->stream>>>(bg, dir, uout, u, h->nplanes);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+    }
+    return PK_OK;
+}
+
+template <class PH>
+const PhysOps* make_ops()
+{
+    static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_batched<PH>};
+    return &o;
+}
+
+}  // namespace pk

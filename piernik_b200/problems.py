@@ -235,3 +235,51 @@ def random_state(setup: Setup, seed: int = 0, dv: float = 0.3, db: float = 0.3):
     fill_periodic(setup, b)
     fill_periodic(setup, psi)
     return u, b, psi
+
+
+def batched_blocks(nblocks: int = 512, seed: int = 1, sizes=(16, 24, 32, 48, 64), levels: int = 3,
+                   fluids=(("ion", 5.0 / 3.0), ("neu", 7.0 / 5.0), ("dst", -1.0)), magnetic: bool = True,
+                   n0: int = 64, limiter: str = "vanleer", centre=(0.3, -0.2, 0.1)):
+    """Many independent periodic blocks of uneven sizes sampling an off-centre
+    Sedov blast at three refinement levels.
+
+    Block edges are drawn per axis from ``sizes`` (seeded).  A block's level l
+    has cell size 2/n0 / 2**l; level-2 blocks are placed within 0.25 of the
+    blast centre, level-1 blocks within 0.6, level-0 blocks anywhere in
+    [-1,1]^3, each block's cells sampling the same analytic initial state:
+    every fluid at rest with density 1 (dust 0.01) and pressure 1e-5, the
+    gaseous fluids carrying a thermal energy density 10 inside r < 0.12 of the
+    centre; uniform B = (0.1, 0.05, 0) with psi = 0 when magnetised.
+    Returns a list of (Setup, u, b, psi).
+    """
+    rng = _rng(seed)
+    out = []
+    fl = list(fluids)
+    for ib in range(nblocks):
+        n = tuple(int(x) for x in rng.choice(sizes, size=3))
+        lev = int(rng.integers(0, levels))
+        dl = 2.0 / n0 / 2 ** lev
+        reach = (0.25, 0.6, 1.0)[min(lev, 2)]
+        origin = [centre[d] + rng.uniform(-reach, reach) - 0.5 * n[d] * dl for d in range(3)]
+        setup = Setup(n=n, xmin=tuple(origin), xmax=tuple(origin[d] + n[d] * dl for d in range(3)),
+                      fluids=fl, magnetic=magnetic, limiter=limiter, limiter_b=limiter, cfl=0.7, cfl_glm=0.7,
+                      smalld=1.0e-4)
+        u, b, psi = _empty(setup)
+        x, y, z = (_centres(setup, d) for d in range(3))
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        r = np.sqrt((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2)
+        hot = np.where(r < 0.12, 10.0, 0.0)
+        emag = None
+        if magnetic:
+            b[..., 0] = 0.1
+            b[..., 1] = 0.05
+            emag = 0.5 * (0.1 ** 2 + 0.05 ** 2)
+        for f, (kind, gam) in enumerate(fl):
+            rho = 0.01 if kind == "dst" else 1.0
+            _set_fluid(setup, u, f, rho, 0.0, 0.0, 0.0, 1.0e-5, emag if kind == "ion" else None)
+            if kind != "dst":
+                beg = sum(4 if k == "dst" else 5 for k, _ in fl[:f])
+                u[..., beg + 4] += hot
+        fill_periodic(setup, u)
+        out.append((setup, u, b, psi))
+    return out

@@ -82,9 +82,19 @@ class Simulation:
         n = (C.c_int32 * 3)(*setup.n)
         dl = (C.c_double * 3)(*setup.dl)
         bnd = (C.c_int32 * 6)(*[setup.bnd[d][s] for d in range(3) for s in range(2)])
+        self.blocks = {}
+        self.block = self.add_block(setup)
+
+    def add_block(self, setup: Setup) -> int:
+        """Register one more block (grid_container) with its own extent, cell
+        size and boundaries; physics parameters come from the first Setup."""
+        n = (C.c_int32 * 3)(*setup.n)
+        dl = (C.c_double * 3)(*setup.dl)
+        bnd = (C.c_int32 * 6)(*[setup.bnd[d][s] for d in range(3) for s in range(2)])
         bid = C.c_int32()
         self._chk(self.lib.pk_block_add(self.h, n, dl, bnd, C.byref(bid)), "pk_block_add")
-        self.block = bid.value
+        self.blocks[bid.value] = setup
+        return bid.value
 
     # -- plumbing ---------------------------------------------------------
     def _chk(self, rc, what):
@@ -107,14 +117,15 @@ class Simulation:
     def __exit__(self, *exc):
         self.close()
 
-    def _shapes(self):
-        ez, ey, ex = self.setup.ext[2], self.setup.ext[1], self.setup.ext[0]
+    def _shapes(self, block: int = 0):
+        s = self.blocks.get(block, self.setup)
+        ez, ey, ex = s.ext[2], s.ext[1], s.ext[0]
         return (ez, ey, ex, self.setup.nvar), (ez, ey, ex, 3), (ez, ey, ex)
 
     # -- state transfer ------------------------------------------------------
     def upload(self, u: np.ndarray, b: Optional[np.ndarray] = None, psi: Optional[np.ndarray] = None,
-               layout: int = L.PK_LAYOUT_FORTRAN) -> None:
-        su, sb, sp = self._shapes()
+               layout: int = L.PK_LAYOUT_FORTRAN, block: int = 0) -> None:
+        su, sb, sp = self._shapes(block)
         u = np.ascontiguousarray(u, dtype=np.float64)
         if u.size != int(np.prod(su)):
             raise ValueError(f"u has {u.size} elements, expected {int(np.prod(su))}")
@@ -126,11 +137,12 @@ class Simulation:
                 raise ValueError("b / psi have the wrong size")
             bp, pp = b.ctypes.data, psi.ctypes.data
         self._keep = (u, b, psi)
-        self._chk(self.lib.pk_upload(self.h, self.block, u.ctypes.data, bp, pp, layout), "pk_upload")
+        self._chk(self.lib.pk_upload(self.h, block, u.ctypes.data, bp, pp, layout), "pk_upload")
         self.sync()
 
-    def download(self, layout: int = L.PK_LAYOUT_FORTRAN, out=None) -> Tuple[np.ndarray, Optional[np.ndarray], Optional[np.ndarray]]:
-        su, sb, sp = self._shapes()
+    def download(self, layout: int = L.PK_LAYOUT_FORTRAN, out=None,
+                 block: int = 0) -> Tuple[np.ndarray, Optional[np.ndarray], Optional[np.ndarray]]:
+        su, sb, sp = self._shapes(block)
         if layout == L.PK_LAYOUT_SOA:
             su = (su[3],) + su[:3]
             sb = (3,) + sb[:3]
@@ -140,7 +152,7 @@ class Simulation:
             psi = np.empty(sp) if self.setup.magnetic else None
         else:
             u, b, psi = out
-        self._chk(self.lib.pk_download(self.h, self.block, u.ctypes.data,
+        self._chk(self.lib.pk_download(self.h, block, u.ctypes.data,
                                        b.ctypes.data if b is not None else None,
                                        psi.ctypes.data if psi is not None else None, layout), "pk_download")
         return u, b, psi
@@ -149,8 +161,8 @@ class Simulation:
         self._chk(self.lib.pk_sync(self.h), "pk_sync")
 
     # -- the reference's routines ------------------------------------------
-    def solve_cg(self, ddim: int, istep: int, dt: float, chspeed: float = 0.0) -> None:
-        self._chk(self.lib.pk_solve_cg(self.h, self.block, ddim, istep, dt, chspeed), "pk_solve_cg")
+    def solve_cg(self, ddim: int, istep: int, dt: float, chspeed: float = 0.0, block: int = 0) -> None:
+        self._chk(self.lib.pk_solve_cg(self.h, block, ddim, istep, dt, chspeed), "pk_solve_cg")
 
     def update_boundaries(self) -> None:
         self._chk(self.lib.pk_fill_guards(self.h), "pk_fill_guards")
@@ -204,6 +216,14 @@ class Simulation:
     @property
     def stream(self) -> int:
         return self.lib.pk_stream(self.h) or 0
+
+    def set_batch(self, enable: bool = True, length: int = 0, variant: int = -1) -> None:
+        """Sweep all blocks in one persistent launch over a tile work list."""
+        self._chk(self.lib.pk_set_batch(self.h, int(enable), length, variant), "pk_set_batch")
+
+    def use_graph(self, enable: bool = True) -> None:
+        """Replay each step's sweeps as a captured CUDA graph."""
+        self._chk(self.lib.pk_use_graph(self.h, int(enable)), "pk_use_graph")
 
     def set_tile(self, direction: int, pencils: int, length: int, variant: int = -1) -> None:
         """Tile of the fused sweep along ``direction`` (0..2): pencils per CTA,

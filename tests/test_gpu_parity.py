@@ -194,3 +194,53 @@ def test_autotune_keeps_state(gpu_lib, oracle_lib):
     ob.run(3)
     sim.run(3)
     compare(ob, sim, "after autotune")
+
+
+def _multi(blocks_data, nsteps, batched=True, graph=False, batch_L=0, batch_V=-1):
+    setup0 = blocks_data[0][0]
+    sim = Simulation(setup0)
+    for s, u, b, psi in blocks_data[1:]:
+        sim.add_block(s)
+    for i, (s, u, b, psi) in enumerate(blocks_data):
+        sim.upload(u, b, psi, block=i)
+    if batched:
+        sim.set_batch(True, batch_L, batch_V)
+    if graph:
+        sim.use_graph(True)
+    obs = [oracle.OracleBlock(s, u, b, psi) for s, u, b, psi in blocks_data]
+    st = oracle.run_multi(obs, nsteps)
+    sim.run(nsteps)
+    ts = sim.time_state
+    assert ts.t == st.t and ts.dt == st.dt and ts.nstep == st.nstep
+    for i, ob in enumerate(obs):
+        gu, gb, gp = sim.download(block=i)
+        assert_bitexact(gu, ob.u, f"block {i} u")
+        if ob.setup.magnetic:
+            assert_bitexact(gb, ob.b, f"block {i} b")
+            assert_bitexact(gp, ob.psi, f"block {i} psi")
+
+
+@pytest.mark.parametrize("fluids,mag", [
+    ((("ion", 5 / 3),), True),
+    ((("ion", 5 / 3), ("neu", 1.4)), True),
+    ((("ion", 5 / 3), ("neu", 1.4), ("dst", -1.0)), True),
+    ((("neu", 1.4), ("dst", -1.0)), False),
+    ((("neu", 1.4),), False),
+])
+def test_batched_uneven_blocks_bitexact(gpu_lib, oracle_lib, fluids, mag):
+    """Independent blocks of uneven sizes (3 refinement levels, one global dt)
+    swept in one persistent launch per direction, against the oracle's leaves loop."""
+    data = problems.batched_blocks(nblocks=6, seed=3, sizes=(8, 12, 16, 20), fluids=fluids, magnetic=mag, n0=16)
+    _multi(data, 4)
+
+
+def test_batched_graph_bitexact(gpu_lib, oracle_lib):
+    """The same with each step's sweeps replayed from one captured CUDA graph."""
+    data = problems.batched_blocks(nblocks=5, seed=7, sizes=(8, 16, 24), n0=16)
+    _multi(data, 5, graph=True, batch_L=16, batch_V=3)
+
+
+def test_single_block_graph_and_forced_batch(gpu_lib, oracle_lib):
+    setup, u, b, psi = problems.mhd_turbulence(n=24, seed=4)
+    _multi([(setup, u, b, psi)], 4, batched=False, graph=True)
+    _multi([(setup, u, b, psi)], 3, batched=True, graph=False)
