@@ -733,8 +733,11 @@ int pk_fluid_update(pk_handle h)
         if (!h->graph_exec) {
             // capture the sweeps of one step once; the step scalars are read from d_step
             const int cur0 = h->cur;
+            const long long l0 = h->launches;
             PK_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
             const int rc = step_sweeps(h, dt, ch, fac);
+            h->graph_kernels = h->launches - l0;
+            h->launches = l0;                 // counted when the graph is launched
             cudaGraph_t g = nullptr;
             const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
             h->cur = cur0;   // 2 x (number of directions) sweeps: the parity is back where it was
@@ -747,6 +750,7 @@ int pk_fluid_update(pk_handle h)
             PK_CUDA(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
         }
         PK_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+        h->launches += h->graph_kernels;
         if (fused_ok(h))
             for (auto& b : h->blocks) b.guards_stale = true;
     } else {

@@ -73,6 +73,7 @@ struct pk_ctx {
     cudaGraph_t graph = nullptr;        // captured sweeps of one step (pk_run with graphs)
     cudaGraphExec_t graph_exec = nullptr;
     int use_graph = 0;
+    long long graph_kernels = 0;        // kernel nodes of the captured step
 };
 
 namespace pk {
