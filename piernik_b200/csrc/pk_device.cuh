@@ -20,10 +20,14 @@
 // (iarr_all_swp, fluids/fluidtypes.F90:318-320; iarr_mag_swp,
 // fluids/fluidindex.F90:190-192).
 #pragma once
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #define PK_DEV __device__ __forceinline__
 #define PK_HD __host__ __device__ __forceinline__
+// physics functions compile for the host too (unit tests of the adjoints)
+#define PK_PHYS __host__ __device__ __forceinline__
 
 namespace pk {
 
@@ -35,17 +39,37 @@ enum Limiter { L_VANLEER = 0, L_MINMOD = 1, L_MONCEN = 2, L_SUPERBEE = 3 };
 // -------------------------------------------------------------------------
 
 // SPACING(x) for real(8): 2**max(exponent(x)-53, -1022), TINY(x) at zero.
-PK_DEV double f_spacing(double x)
+PK_PHYS unsigned long long f_bits(double x)
 {
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(x);
+#ifdef __CUDA_ARCH__
+    return (unsigned long long)__double_as_longlong(x);
+#else
+    unsigned long long b;
+    memcpy(&b, &x, sizeof b);
+    return b;
+#endif
+}
+PK_PHYS double f_from_bits(unsigned long long b)
+{
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+#endif
+}
+PK_PHYS double f_spacing(double x)
+{
+    const unsigned long long bits = f_bits(x);
     const int be = (int)((bits >> 52) & 0x7ffu);
-    if (be == 0x7ff) return __longlong_as_double(0x7ff8000000000000LL);
-    if (be >= 53) return __longlong_as_double((long long)((unsigned long long)(be - 52) << 52));
+    if (be == 0x7ff) return f_from_bits(0x7ff8000000000000ULL);
+    if (be >= 53) return f_from_bits((unsigned long long)(be - 52) << 52);
     return 2.2250738585072014e-308;
 }
-PK_DEV double f_sign1(double x) { return copysign(1.0, x); }
-PK_DEV double f_min(double a, double b) { return (b < a) ? b : a; }
-PK_DEV double f_max(double a, double b) { return (b > a) ? b : a; }
+PK_PHYS double f_sign1(double x) { return copysign(1.0, x); }
+PK_PHYS double f_min(double a, double b) { return (b < a) ? b : a; }
+PK_PHYS double f_max(double a, double b) { return (b > a) ? b : a; }
 
 // -------------------------------------------------------------------------
 // Compile-time description of the fluid set (flind order: ion, neu, dst)
@@ -83,7 +107,7 @@ enum StatusBits : unsigned {
 // utoq: conservative -> primitive, one cell (interpolations.F90:69-106)
 // -------------------------------------------------------------------------
 template <class PH>
-PK_DEV void utoq(const double (&u)[PH::NV], double (&q)[PH::NV], const PhysParams& pp)
+PK_PHYS void utoq(const double (&u)[PH::NV], double (&q)[PH::NV], const PhysParams& pp)
 {
 #pragma unroll
     for (int f = 0; f < PH::NFL; ++f) {
@@ -113,7 +137,7 @@ PK_DEV void utoq(const double (&u)[PH::NV], double (&q)[PH::NV], const PhysParam
 // Limited slopes.  Interior cell: dl = q(i)-q(i-1), dr = q(i+1)-q(i).
 // Pencil end cells use the reference's one-sided rules (dl = dr, vanleer 0).
 // -------------------------------------------------------------------------
-PK_DEV double slope_interior(int lim, double dl, double dr)
+PK_PHYS double slope_interior(int lim, double dl, double dr)
 {
     if (lim == L_VANLEER) {                       // fluxlimiters.F90:122-133
         const double dcen = dl * dr;
@@ -126,7 +150,7 @@ PK_DEV double slope_interior(int lim, double dl, double dr)
     return (s * 0.5) * m;
 }
 
-PK_DEV double slope_end(int lim, double d)
+PK_PHYS double slope_end(int lim, double d)
 {
     if (lim == L_VANLEER) return 0.0;             // "sanitizing endpoints" (:119-120)
     return slope_interior(lim, d, d);
@@ -141,7 +165,7 @@ PK_DEV double slope_end(int lim, double d)
 // Physical flux of one side (hlld.F90:296-308): fluid part f[0..nc) and the
 // transverse B fluxes bf[1..2].  Computed where needed so that neither side's
 // flux is held in registers through the star-state algebra.
-PK_DEV void side_flux(bool has_energy, const double* u, const double* b, double pr, double en, double* f)
+PK_PHYS void side_flux(bool has_energy, const double* u, const double* b, double pr, double en, double* f)
 {
     f[0] = u[0] * u[1];
     f[1] = ((u[0] * (u[1] * u[1])) + pr) - (b[0] * b[0]);
@@ -150,18 +174,18 @@ PK_DEV void side_flux(bool has_energy, const double* u, const double* b, double 
     if (has_energy) f[4] = ((en + pr) * u[1]) - (b[0] * ((u[1] * b[0] + u[2] * b[1]) + u[3] * b[2]));
 }
 
-PK_DEV double side_bflux(const double* u, const double* b, int c)
+PK_PHYS double side_bflux(const double* u, const double* b, int c)
 {
     return (b[c] * u[1]) - (b[0] * u[1 + c]);     // b_cclf(ydim:zdim), hlld.F90:301,309
 }
 
 // [ u(idn), u(idn)*u(imx:imz), en ] of one side
-PK_DEV double side_cons(const double* u, double en, int c)
+PK_PHYS double side_cons(const double* u, double en, int c)
 {
     return c == 0 ? u[0] : (c == 4 ? en : u[0] * u[c]);
 }
 
-PK_DEV void hlld_iface(bool has_energy, double gamma, const double* ul, const double* ur, const double* bl,
+PK_PHYS void hlld_iface(bool has_energy, double gamma, const double* ul, const double* ur, const double* bl,
                        const double* br, double* f, double* bf)
 {
     const int nc = has_energy ? 5 : 4;
@@ -368,7 +392,7 @@ PK_DEV void hlld_iface(bool has_energy, double gamma, const double* ul, const do
     }
 }
 
-PK_DEV void hllc_iface(bool has_energy, double gamma, const double* ul, const double* ur, double* f)
+PK_PHYS void hllc_iface(bool has_energy, double gamma, const double* ul, const double* ur, double* f)
 {
     double fl[5], fr[5], usl[5], usr[5];
     double prl, prr, c_fastm;
@@ -465,7 +489,7 @@ PK_DEV void hllc_iface(bool has_energy, double gamma, const double* ul, const do
 // riemann_wrap / riemann_wrap_u (hlld.F90:62-155) for one interface of the
 // whole state: fluid fluxes, then (MHD) fluxes of Bx, By, Bz, psi.
 template <class PH>
-PK_DEV void riemann(const double (&ql)[PH::NV], const double (&qr)[PH::NV], double ch, const PhysParams& pp,
+PK_PHYS void riemann(const double (&ql)[PH::NV], const double (&qr)[PH::NV], double ch, const PhysParams& pp,
                     double (&fx)[PH::NV])
 {
     if (PH::MHD) {
@@ -551,7 +575,7 @@ PK_DEV void riemann_tile(const double* __restrict__ L, const double* __restrict_
 // internal_sources (+0 added to every fluid component) and care_for_positives
 // on one updated cell; B used for emag is the updated one (b1).
 template <class PH>
-PK_DEV void sources_and_floors(double (&u)[PH::NV], const PhysParams& pp, unsigned& status)
+PK_PHYS void sources_and_floors(double (&u)[PH::NV], const PhysParams& pp, unsigned& status)
 {
 #pragma unroll
     for (int c = 0; c < PH::NVF; ++c) u[c] = u[c] + 0.0;
