@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--adj-steps", type=int, default=8)
     p.add_argument("--tune-log", default=None)
     p.add_argument("--workload", default="mhd256", choices=["mhd256", "batched"],
                    help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks")
@@ -174,6 +176,52 @@ def reference_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def adjoint_cost(sim, stream, args, fwd_ms_per_step, barrier, max_over_ranks):
+    """Cost of the gradient of K steps relative to K forward steps.
+
+    backward = pk_grad_backward: recompute each checkpointed segment once
+    (fused sweeps) plus one adjoint sweep kernel per forward sweep.  The ratio
+    reported is backward / forward; the recorded forward (pk_grad_forward,
+    which adds the checkpoint copies) is reported beside it."""
+    import numpy as np
+    import torch
+    K = args.adj_steps
+    every = max(1, int(round(np.sqrt(K))))
+    st0 = sim.time_state
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    barrier()
+    ev[0].record(stream)
+    sim.grad_forward(K, every)
+    ev[1].record(stream)
+    ev[1].synchronize()
+    lam = np.ones(sim.state_shape())
+    sim.adjoint_set(lam)
+    barrier()
+    ev[2].record(stream)
+    sim.grad_backward()
+    ev[3].record(stream)
+    ev[3].synchronize()
+    # one adjoint sweep kernel per direction, timed alone
+    st = sim.time_state
+    reps = 3
+    ev[4].record(stream)
+    for _ in range(reps):
+        for d in (1, 2, 3):
+            sim.adjoint_sweep(d, st.dt, st.chspeed)
+    ev[5].record(stream)
+    ev[5].synchronize()
+    sim.grad_release()
+    sim.time_state = st0
+    fwd_rec = max_over_ranks(ev[0].elapsed_time(ev[1]))
+    bwd = max_over_ranks(ev[2].elapsed_time(ev[3]))
+    adj_sweep = max_over_ranks(ev[4].elapsed_time(ev[5])) / (3 * reps)
+    fwd = fwd_ms_per_step * K
+    return {"value": bwd / fwd, "definition": "pk_grad_backward time / time of the same K forward steps (pk_run)",
+            "steps": K, "checkpoint_every": every, "forward_ms": fwd, "recorded_forward_ms": fwd_rec,
+            "backward_ms": bwd, "gradient_total_over_forward": (fwd_rec + bwd) / fwd,
+            "adjoint_sweep_ms": adj_sweep, "fused_sweep_ms": fwd_ms_per_step / 6}
+
+
 def our_arm(args):
     import numpy as np
     import torch
@@ -278,6 +326,10 @@ def our_arm(args):
                "path": "pk_upload(Fortran layout, pinned) + pk_run(1) + pk_download per step"}
         sim.time_state = st0
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_cost(sim, stream, args, ms / args.steps, barrier, max_over_ranks)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cn = n
@@ -294,7 +346,7 @@ def our_arm(args):
                               tiles_P_L_variant_ms=tiles),
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": launches1 - launches0, "clocks": ck,
-               "adjoint_cost_ratio": None}
+               "adjoint_cost_ratio": adjoint}
         print(json.dumps(out), flush=True)
     sim.close()
     if world > 1:

@@ -161,6 +161,35 @@ int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant);
  * device memory, so one capture serves every step. */
 int pk_use_graph(pk_handle h, int32_t enable);
 
+/* ---- Differentiable path (one periodic block, one fluid, RK2) ----
+ * Not in the reference, which has no derivatives: the adjoint (reverse
+ * mode) of the sweep path at a fixed sequence of time steps. */
+
+/* Device-to-device state transfer (structure of arrays with guard cells,
+ * nplanes x ext_x*ext_y*ext_z doubles; guards are refreshed on upload). */
+int pk_upload_device(pk_handle h, int32_t id, const double* soa_dev);
+int pk_download_device(pk_handle h, int32_t id, double* soa_dev);
+
+/* The adjoint state dL/dU in the same layout, from/to host (on_device = 0) or
+ * device memory.  Guard values are ignored on input and zero on output. */
+int pk_adjoint_set(pk_handle h, int32_t id, const double* lam, int32_t on_device);
+int pk_adjoint_get(pk_handle h, int32_t id, double* lam, int32_t on_device);
+
+/* lam <- (d sweep(cdim)/dU)^T lam at the current state (one fused sweep). */
+int pk_adjoint_sweep(pk_handle h, int32_t cdim, double dt, double chspeed);
+
+/* Advance nsteps steps like pk_run, recording dt / chspeed / glmdamping per
+ * step and checkpointing the state every `every` steps.  dt_in (nsteps
+ * values, or NULL for the CFL time step) replays a prescribed sequence;
+ * dt_out (or NULL) receives the steps taken. */
+int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt_in, double* dt_out);
+
+/* Given lam = dL/d(final state) (pk_adjoint_set), leave lam = dL/d(state at
+ * the start of pk_grad_forward): each checkpointed segment is recomputed once
+ * and its steps' sweeps are reversed with the adjoint sweep kernel. */
+int pk_grad_backward(pk_handle h);
+int pk_grad_release(pk_handle h);
+
 /* Launch-bound variants of the fused sweep: count, CTA size and CTAs per SM
  * each was compiled for (arrays of at least 16 entries). */
 int pk_tile_variants(int32_t* n, int32_t* threads, int32_t* ctas_per_sm);

@@ -28,6 +28,8 @@ EXPORTS = (
     "pk_timestep_raw", "pk_time_step", "pk_fluid_update", "pk_run", "pk_get_time_state",
     "pk_set_time_state", "pk_status", "pk_sync", "pk_set_tile", "pk_stream", "pk_profile_enable",
     "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_use_graph",
+    "pk_upload_device", "pk_download_device", "pk_adjoint_set", "pk_adjoint_get", "pk_adjoint_sweep",
+    "pk_grad_forward", "pk_grad_backward", "pk_grad_release",
 )
 
 
@@ -114,6 +116,14 @@ def load(path: str = LIBPATH):
     L.pk_tile_variants.argtypes = [C.POINTER(C.c_int32)] * 3
     L.pk_set_batch.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
     L.pk_use_graph.argtypes = [H, C.c_int32]
+    L.pk_upload_device.argtypes = [H, C.c_int32, C.c_void_p]
+    L.pk_download_device.argtypes = [H, C.c_int32, C.c_void_p]
+    L.pk_adjoint_set.argtypes = [H, C.c_int32, C.c_void_p, C.c_int32]
+    L.pk_adjoint_get.argtypes = [H, C.c_int32, C.c_void_p, C.c_int32]
+    L.pk_adjoint_sweep.argtypes = [H, C.c_int32, C.c_double, C.c_double]
+    L.pk_grad_forward.argtypes = [H, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+    L.pk_grad_backward.argtypes = [H]
+    L.pk_grad_release.argtypes = [H]
     L.pk_stream.argtypes = [H]
     L.pk_stream.restype = C.c_void_p
     L.pk_profile_enable.argtypes = [H, C.c_int32]

@@ -441,6 +441,10 @@ int pk_destroy(pk_handle h)
     for (auto& p : h->ev_used) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
     for (auto& p : h->ev_free) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
     for (int d = 0; d < 3; ++d) cudaFree(h->batch[d].dev);
+    for (double* p : h->grad_ckpt) cudaFree(p);
+    for (double* p : h->grad_pool) cudaFree(p);
+    cudaFree(h->lam);
+    cudaFree(h->lam_tmp);
     cudaFree(h->d_desc[0]);
     cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
@@ -872,6 +876,222 @@ int pk_profile_read(pk_handle h, int64_t* launches, int64_t* sweep_launches, dou
     if (launches) *launches = h->launches;
     if (sweep_launches) *sweep_launches = timed;
     if (sweep_ms) *sweep_ms = ms;
+    return PK_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Differentiable path: recorded forward with checkpoints, adjoint backward
+// ---------------------------------------------------------------------------
+
+namespace {
+
+void grad_release(pk_ctx* h)
+{
+    cudaStreamSynchronize(h->stream);
+    for (double* p : h->grad_ckpt) cudaFree(p);
+    for (double* p : h->grad_pool) cudaFree(p);
+    h->grad_ckpt.clear();
+    h->grad_pool.clear();
+    h->grad_steps.clear();
+}
+
+int grad_check(pk_ctx* h)
+{
+    if (h->blocks.size() != 1) return fail(h, PK_E_UNSUPPORTED, "the differentiable path runs on one block");
+    if (!fused_ok(h)) return fail(h, PK_E_UNSUPPORTED, "the differentiable path needs RK2 and periodic boundaries");
+    if (h->cfg.nfluids != 1) return fail(h, PK_E_UNSUPPORTED, "the differentiable path is built for one fluid");
+    int dirs[3], nd;
+    step_dirs(h, dirs, &nd);
+    if (nd == 0) return fail(h, PK_E_UNSUPPORTED, "the differentiable path needs at least one swept direction");
+    return ensure_pingpong(h);
+}
+
+int alloc_state(pk_ctx* h, const Block& b, double** p)
+{
+    if (cudaMalloc(p, sizeof(double) * h->nplanes * b.plane) != cudaSuccess)
+        return fail(h, PK_E_NOMEM, "cudaMalloc for the differentiable path failed");
+    PK_CUDA(h, cudaMemsetAsync(*p, 0, sizeof(double) * h->nplanes * b.plane, h->stream));
+    return PK_OK;
+}
+
+// the sweeps of one step as (direction, damping applied) pairs, in step_sweeps' order
+int step_plan(pk_ctx* h, int* dir, int* fac)
+{
+    int dirs[3], nd;
+    step_dirs(h, dirs, &nd);
+    int k = 0;
+    for (int half = 0; half < 2; ++half)
+        for (int s = 0; s < nd; ++s) {
+            dir[k] = half == 0 ? dirs[s] : dirs[nd - 1 - s];
+            fac[k] = h->cfg.magnetic && s == nd - 1;
+            ++k;
+        }
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pk_upload_device(pk_handle h, int32_t id, const double* soa_dev)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!soa_dev) return fail(h, PK_E_ARG, "null array");
+    PK_CUDA(h, cudaMemcpyAsync(state(h, *b), soa_dev, sizeof(double) * h->nplanes * b->plane, cudaMemcpyDeviceToDevice,
+                               h->stream));
+    return fill_guards_block(h, *b);
+}
+
+int pk_download_device(pk_handle h, int32_t id, double* soa_dev)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!soa_dev) return fail(h, PK_E_ARG, "null array");
+    if (b->guards_stale)
+        if (int rc = fill_guards_block(h, *b)) return rc;
+    PK_CUDA(h, cudaMemcpyAsync(soa_dev, state(h, *b), sizeof(double) * h->nplanes * b->plane, cudaMemcpyDeviceToDevice,
+                               h->stream));
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_adjoint_set(pk_handle h, int32_t id, const double* lam, int32_t on_device)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!lam) return fail(h, PK_E_ARG, "null array");
+    if (!h->lam)
+        if (int rc = alloc_state(h, *b, &h->lam)) return rc;
+    if (!h->lam_tmp)
+        if (int rc = alloc_state(h, *b, &h->lam_tmp)) return rc;
+    PK_CUDA(h, cudaMemcpyAsync(h->lam, lam, sizeof(double) * h->nplanes * b->plane,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+    // the sweeps read periodic images of the interior only: guard values carry no derivative
+    k_zero_guards<<<grid1d(b->plane, 256), 256, 0, h->stream>>>(box_of(*b), h->lam, h->nplanes);
+    PK_CUDA(h, cudaGetLastError());
+    h->launches += 1;
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_adjoint_get(pk_handle h, int32_t id, double* lam, int32_t on_device)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!lam || !h->lam) return fail(h, PK_E_STATE, "no adjoint state");
+    PK_CUDA(h, cudaMemcpyAsync(lam, h->lam, sizeof(double) * h->nplanes * b->plane,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_adjoint_sweep(pk_handle h, int32_t cdim, double dt, double chspeed)
+{
+    if (!h) return PK_E_ARG;
+    if (cdim < 1 || cdim > 3) return fail(h, PK_E_ARG, "cdim must be 1..3");
+    if (int rc = grad_check(h)) return rc;
+    if (!h->lam) return fail(h, PK_E_STATE, "set the adjoint first (pk_adjoint_set)");
+    Block& b = h->blocks[0];
+    if (int rc = put_step_params(h, dt, chspeed, 1.0)) return rc;
+    if (int rc = ops_of(h)->adj(h, b, cdim - 1, 0, state(h, b), h->lam, h->lam_tmp)) return rc;
+    std::swap(h->lam, h->lam_tmp);
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt_in, double* dt_out)
+{
+    if (!h || nsteps < 0 || every < 1) return PK_E_ARG;
+    if (int rc = grad_check(h)) return rc;
+    grad_release(h);
+    Block& b = h->blocks[0];
+    h->grad_every = every;
+    h->grad_ts0 = h->ts;
+    for (int s = 0; s < nsteps; ++s) {
+        if (s % every == 0) {
+            double* p;
+            if (int rc = alloc_state(h, b, &p)) return rc;
+            h->grad_ckpt.push_back(p);
+            PK_CUDA(h, cudaMemcpyAsync(p, state(h, b), sizeof(double) * h->nplanes * b.plane,
+                                       cudaMemcpyDeviceToDevice, h->stream));
+        }
+        double dt;
+        if (dt_in) {
+            h->ts.dt_old = h->ts.dt;
+            dt = dt_in[s];
+            h->ts.dt = dt;
+        } else {
+            if (int rc = pk_time_step(h, &dt)) return rc;
+        }
+        double ch, fac;
+        glm_scalars(h, dt, &ch, &fac);
+        h->ts.chspeed = ch;
+        if (int rc = put_step_params(h, dt, ch, fac)) return rc;
+        if (int rc = step_sweeps(h, dt, ch, fac)) return rc;
+        h->ts.t = h->ts.t + dt;                        // two half steps of dt, as pk_fluid_update
+        h->ts.t = h->ts.t + dt;
+        h->ts.nstep += 1;
+        h->grad_steps.push_back(StepRec{dt, ch, fac});
+        if (dt_out) dt_out[s] = dt;
+    }
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_grad_backward(pk_handle h)
+{
+    if (!h) return PK_E_ARG;
+    if (int rc = grad_check(h)) return rc;
+    if (!h->lam) return fail(h, PK_E_STATE, "set the adjoint of the final state first (pk_adjoint_set)");
+    Block& b = h->blocks[0];
+    const PhysOps* ops = ops_of(h);
+    int dir[6], fac[6];
+    const int nsw = step_plan(h, dir, fac);
+    const int K = (int)h->grad_steps.size(), C = h->grad_every;
+    if (K == 0) return PK_OK;
+    const int need = C * nsw;
+    while ((int)h->grad_pool.size() < need) {
+        double* p;
+        if (int rc = alloc_state(h, b, &p)) return rc;
+        h->grad_pool.push_back(p);
+    }
+    const int nseg = (K + C - 1) / C;
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int s0 = seg * C, len = (K - s0 < C) ? K - s0 : C;
+        // recompute the segment, keeping every sweep's output
+        const double* x = h->grad_ckpt[seg];
+        for (int j = 0; j < len; ++j) {
+            const StepRec& r = h->grad_steps[s0 + j];
+            if (int rc = put_step_params(h, r.dt, r.ch, r.fac)) return rc;
+            for (int k = 0; k < nsw; ++k) {
+                double* out = h->grad_pool[j * nsw + k];
+                if (int rc = ops->fused_ptr(h, b, dir[k], fac[k], x, out)) return rc;
+                x = out;
+            }
+        }
+        // adjoint sweeps back to the segment's start
+        for (int j = len - 1; j >= 0; --j) {
+            const StepRec& r = h->grad_steps[s0 + j];
+            if (int rc = put_step_params(h, r.dt, r.ch, r.fac)) return rc;
+            for (int k = nsw - 1; k >= 0; --k) {
+                const double* uin = k > 0 ? h->grad_pool[j * nsw + k - 1]
+                                          : (j > 0 ? h->grad_pool[(j - 1) * nsw + nsw - 1] : h->grad_ckpt[seg]);
+                if (int rc = ops->adj(h, b, dir[k], fac[k], uin, h->lam, h->lam_tmp)) return rc;
+                std::swap(h->lam, h->lam_tmp);
+            }
+        }
+    }
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_grad_release(pk_handle h)
+{
+    if (!h) return PK_E_ARG;
+    grad_release(h);
     return PK_OK;
 }
 

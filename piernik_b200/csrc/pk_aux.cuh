@@ -201,6 +201,22 @@ static __global__ void k_fill_guards(BoxGeom b, double* __restrict__ u, GuardArg
     }
 }
 
+// zero every guard cell of all planes (adjoint states carry no guard values)
+static __global__ void k_zero_guards(BoxGeom b, double* __restrict__ u, int nplanes)
+{
+    const long long ncell = (long long)b.ext[0] * b.ext[1] * b.ext[2];
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % b.ext[0]);
+        const long long r = c / b.ext[0];
+        const int j = (int)(r % b.ext[1]);
+        const int k = (int)(r / b.ext[1]);
+        const bool inside = i >= b.g[0] && i < b.g[0] + b.n[0] && j >= b.g[1] && j < b.g[1] + b.n[1] &&
+                            k >= b.g[2] && k < b.g[2] + b.n[2];
+        if (!inside)
+            for (int v = 0; v < nplanes; ++v) u[(long long)v * b.plane + c] = 0.0;
+    }
+}
+
 // Fortran-order arrays (u(nvar,i,j,k), b(3,i,j,k), psi(i,j,k)) <-> component planes.
 static __global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long long ncell, int ncomp,
                              int plane0, long long plane)

@@ -606,4 +606,52 @@ PK_PHYS void sources_and_floors(double (&u)[PH::NV], const PhysParams& pp, unsig
     }
 }
 
+// ---------------------------------------------------------------------------
+// internal_sources + care_for_positives with a record of the floors taken
+// ---------------------------------------------------------------------------
+struct FloorRec {
+    unsigned dn;   // bit f: the density floor of fluid f clipped
+    unsigned en;   // bit f: the internal-energy floor of fluid f clipped
+};
+
+template <class PH>
+PK_PHYS void floors_rec(double (&u)[PH::NV], const PhysParams& pp, unsigned& status, FloorRec& rec)
+{
+    rec.dn = 0;
+    rec.en = 0;
+#pragma unroll
+    for (int c = 0; c < PH::NVF; ++c) u[c] = u[c] + 0.0;
+#pragma unroll
+    for (int f = 0; f < PH::NFL; ++f) {
+        const int b = PH::beg(f);
+        if (u[b] < 0.0) status |= ST_DN_NEGATIVE;
+        if (pp.use_smalld) {
+            if (pp.smalld > u[b]) rec.dn |= 1u << f;
+            u[b] = f_max(u[b], pp.smalld);
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < PH::NFL; ++f) {
+        if (!PH::has_en(f)) continue;
+        const int b = PH::beg(f);
+        const double kin = (0.5 * ((u[b + 1] * u[b + 1] + u[b + 2] * u[b + 2]) + u[b + 3] * u[b + 3])) / u[b];
+        double mag = 0.0, eint;
+        if (PH::magn(f)) {
+            const double bx = u[PH::IB], by = u[PH::IB + 1], bz = u[PH::IB + 2];
+            mag = 0.5 * ((bx * bx + by * by) + bz * bz);
+            eint = (u[b + 4] - kin) - mag;
+        } else {
+            eint = u[b + 4] - kin;
+        }
+        if (pp.disallow_negatives && eint < 0.0) status |= ST_EI_NEGATIVE;
+        if (pp.use_smallei) {
+            if (pp.smallei > eint) rec.en |= 1u << f;
+            eint = f_max(eint, pp.smallei);
+        }
+        double e = eint + kin;
+        if (PH::magn(f)) e = e + mag;
+        u[b + 4] = e;
+    }
+}
+
 }  // namespace pk

@@ -34,6 +34,11 @@ struct Block {
 
 struct pk_dir_tile { int P, L, V; };
 
+// scalars of one recorded step of the differentiable path
+struct StepRec {
+    double dt, ch, fac;
+};
+
 // work list of the batched sweep for one direction
 struct BatchList {
     std::vector<WorkItem> host;
@@ -74,6 +79,15 @@ struct pk_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int use_graph = 0;
     long long graph_kernels = 0;        // kernel nodes of the captured step
+    // differentiable path (single block, fused sweeps)
+    int adjL = 0;                       // chunk length of the adjoint tiles (0: default)
+    std::vector<pk::StepRec> grad_steps;        // dt, chspeed, damping of each recorded step
+    std::vector<double*> grad_ckpt;             // checkpointed states (every grad_every steps)
+    int grad_every = 0;
+    double* lam = nullptr;                      // adjoint of the state (structure of arrays)
+    double* lam_tmp = nullptr;
+    std::vector<double*> grad_pool;             // states of a recomputed segment's sweeps
+    pk_time_state grad_ts0;                     // time state at the start of the recording
 };
 
 namespace pk {
@@ -90,6 +104,8 @@ struct PhysOps {
     int (*fused)(pk_ctx* h, Block& b, int dir, int apply_fac);
     int (*stage)(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch);
     int (*batched)(pk_ctx* h, int dir, int apply_fac, unsigned* counter);
+    int (*fused_ptr)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out);
+    int (*adj)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* lam_out, double* lam_in);
 };
 
 const PhysOps* ops_hd1();

@@ -106,10 +106,11 @@ struct Smem {
 //   w      in: the stage's input state (valid where r.q); out: u1 where r.upd or r.keep
 //   u0src  where u0 (uh / the sweep's input) is read for the update
 //   wsrc   where an unchanged end cell re-reads its state (r.keep)
-template <class PH>
+//   REC    record which floors clipped in *rec (the adjoint sweep's recomputation)
+template <class PH, bool REC = false>
 PK_DEV void rk_stage(const Smem& sm, int me, int st, const Roles& r, double (&w)[PH::NV], const double* u0src,
                      const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
-                     const PhysParams& pp, unsigned& status)
+                     const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr)
 {
     constexpr int NV = PH::NV;
     const int PT = sm.PT;
@@ -145,7 +146,10 @@ PK_DEV void rk_stage(const Smem& sm, int me, int st, const Roles& r, double (&w)
     } else if (r.keep) {
         load_cell<PH>(wsrc, off, g, w);
     }
-    if (r.upd || r.keep) sources_and_floors<PH>(w, pp, status);
+    if (r.upd || r.keep) {
+        if constexpr (REC) floors_rec<PH>(w, pp, status, *rec);
+        else sources_and_floors<PH>(w, pp, status);
+    }
     __syncthreads();
 }
 

@@ -2,6 +2,7 @@
 // pk_phys_*.cu instantiates these for its PH, so the heavy kernels compile in
 // parallel translation units.
 #pragma once
+#include "pk_adjoint_kernels.cuh"
 #include "pk_aux.cuh"
 #include "pk_internal.h"
 
@@ -59,7 +60,7 @@ constexpr int DEF_P[3] = {2, 4, 4};
 constexpr int DEF_L[3] = {64, 64, 64};
 
 template <class PH>
-int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
+int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out)
 {
     if (int rc = set_smem_attr<PH>(h)) return rc;
     Geom g = make_geom(b, dir);
@@ -80,8 +81,6 @@ int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
     tl.xfast = (dir == 0);
     dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
     const size_t smem = 3ull * PH::NV * P * T * sizeof(double);
-    double* in = b.buf[h->cur];
-    double* out = b.buf[1 - h->cur];
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
     fused_variant<PH>(var)<<<grid, P * T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir], h->d_step, apply_fac,
@@ -89,8 +88,53 @@ int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
+    return PK_OK;
+}
+
+template <class PH>
+int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
+{
+    if (int rc = launch_fused_ptr<PH>(h, b, dir, apply_fac, b.buf[h->cur], b.buf[1 - h->cur])) return rc;
     b.guards_stale = true;
     return PK_OK;
+}
+
+// Adjoint of one fused sweep: lam_in = (d sweep / d uin)^T lam_out
+template <class PH>
+int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* lam_out, double* lam_in)
+{
+    if constexpr (PH::NFL != 1) {
+        return fail(h, PK_E_UNSUPPORTED, "the adjoint sweep is built for one-fluid HD and MHD");
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            PK_CUDA(h, cudaFuncSetAttribute(k_sweep_adj<PH, 256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            attr = true;
+        }
+        Geom g = make_geom(b, dir);
+        Tile tl;
+        int L = h->adjL > 0 ? h->adjL : 48;
+        if (L > b.n[dir]) L = b.n[dir];
+        const int T = L + 16;
+        int P = 256 / T;
+        if (P < 1) return fail(h, PK_E_ARG, "adjoint tile longer than 256");
+        if (P > g.n1) P = g.n1;
+        tl.P = P;
+        tl.T = T;
+        tl.L = L;
+        tl.halo = 8;
+        tl.xfast = dir == 0;
+        dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
+        const size_t smem = 4ull * PH::NV * P * T * sizeof(double);
+        std::pair<cudaEvent_t, cudaEvent_t> ev;
+        if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+        k_sweep_adj<PH, 256, 1><<<grid, P * T, smem, h->stream>>>(g, tl, uin, lam_out, lam_in, h->pp, b.dl[dir],
+                                                                h->d_step, apply_fac, h->d_status);
+        PK_CUDA(h, cudaGetLastError());
+        if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+        h->launches += 1;
+        return PK_OK;
+    }
 }
 
 template <class PH>
@@ -177,7 +221,8 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double c
 template <class PH>
 const PhysOps* make_ops()
 {
-    static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_batched<PH>};
+    static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_batched<PH>,
+                     launch_fused_ptr<PH>, launch_adj<PH>};
     return &o;
 }
 

@@ -200,6 +200,28 @@ def orszag_tang(n: int = 512, seed: int = 1, amp: float = 1.0e-3, corr_cells: fl
     return setup, u, b, psi
 
 
+def orszag_tang_fields(n: int):
+    """Interior (ny, nx) fields of the unperturbed Orszag-Tang vortex and its
+    scalars: (setup, rho0, pre, vx, vy, bx, by)."""
+    gamma = 5.0 / 3.0
+    setup = Setup(n=(n, n, 1), xmin=(0.0, 0.0, -0.5), xmax=(1.0, 1.0, 0.5),
+                  fluids=[("ion", gamma)], magnetic=True, limiter="vanleer", limiter_b="vanleer",
+                  cfl=0.8, cfl_glm=0.7, smalld=1.0e-3, smallei=1.0e-5)
+    g = setup.guards
+    x = _centres(setup, 0)[g[0]:g[0] + n]
+    y = _centres(setup, 1)[g[1]:g[1] + n]
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    b0 = 1.0 / math.sqrt(4.0 * math.pi)
+    vx = -np.sin(2 * math.pi * Y)
+    vy = np.sin(2 * math.pi * X)
+    return setup, 25.0 / (36.0 * math.pi), 5.0 / (12.0 * math.pi), vx, vy, b0 * vx, b0 * np.sin(4 * math.pi * X)
+
+
+def orszag_tang_perturbation(n: int, seed: int = 1, corr_cells: float = 8.0) -> np.ndarray:
+    """The seeded unit-rms density perturbation field of the Orszag-Tang setup."""
+    return gaussian_random_field((n, n), corr_cells, _rng(seed))
+
+
 def gaussian_random_field(shape, corr_cells: float, rng: np.random.Generator) -> np.ndarray:
     """Unit-rms periodic Gaussian random field with a Gaussian correlation kernel."""
     w = rng.standard_normal(shape)

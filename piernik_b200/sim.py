@@ -225,6 +225,70 @@ class Simulation:
         """Replay each step's sweeps as a captured CUDA graph."""
         self._chk(self.lib.pk_use_graph(self.h, int(enable)), "pk_use_graph")
 
+    # -- differentiable path (one periodic block, one fluid, RK2) -------------
+    @property
+    def nplanes(self) -> int:
+        """Component planes of the device state: u, then bx, by, bz, psi."""
+        return self.setup.nvar + (4 if self.setup.magnetic else 0)
+
+    def state_shape(self, block: int = 0) -> Tuple[int, int, int, int]:
+        """Shape of the structure-of-arrays state with guard cells."""
+        su, _, _ = self._shapes(block)
+        return (self.nplanes,) + su[:3]
+
+    def upload_device(self, ptr: int, block: int = 0) -> None:
+        """Copy a device SoA state (``state_shape()`` doubles at ``ptr``) in."""
+        self._chk(self.lib.pk_upload_device(self.h, block, ptr), "pk_upload_device")
+
+    def download_device(self, ptr: int, block: int = 0) -> None:
+        self._chk(self.lib.pk_download_device(self.h, block, ptr), "pk_download_device")
+
+    def adjoint_set(self, lam, block: int = 0, on_device: bool = False) -> None:
+        """Set dL/dU (SoA with guard cells; guard values are ignored).  ``lam``
+        is a numpy array, or a device address when ``on_device``."""
+        if on_device:
+            self._chk(self.lib.pk_adjoint_set(self.h, block, lam, 1), "pk_adjoint_set")
+            return
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        if lam.shape != self.state_shape(block):
+            raise ValueError(f"adjoint has shape {lam.shape}, expected {self.state_shape(block)}")
+        self._chk(self.lib.pk_adjoint_set(self.h, block, lam.ctypes.data, 0), "pk_adjoint_set")
+
+    def adjoint_get(self, out=None, block: int = 0, on_device: bool = False):
+        if on_device:
+            self._chk(self.lib.pk_adjoint_get(self.h, block, out, 1), "pk_adjoint_get")
+            return out
+        if out is None:
+            out = np.empty(self.state_shape(block))
+        self._chk(self.lib.pk_adjoint_get(self.h, block, out.ctypes.data, 0), "pk_adjoint_get")
+        return out
+
+    def adjoint_sweep(self, cdim: int, dt: float, chspeed: float = 0.0) -> None:
+        """lam <- (d sweep(cdim) / dU)^T lam at the current state."""
+        self._chk(self.lib.pk_adjoint_sweep(self.h, cdim, dt, chspeed), "pk_adjoint_sweep")
+
+    def grad_forward(self, nsteps: int, every: int = 0, dts=None) -> np.ndarray:
+        """Advance ``nsteps`` steps recording what the adjoint needs; checkpoint
+        every ``every`` steps (0: about sqrt(nsteps)).  ``dts`` replays a
+        prescribed dt sequence.  Returns the dt of each step."""
+        if every <= 0:
+            every = max(1, int(round(np.sqrt(max(nsteps, 1)))))
+        out = np.empty(max(nsteps, 1))
+        dp = None
+        if dts is not None:
+            dts = np.ascontiguousarray(dts, dtype=np.float64)
+            if dts.size < nsteps:
+                raise ValueError("dts has fewer than nsteps values")
+            dp = dts.ctypes.data
+        self._chk(self.lib.pk_grad_forward(self.h, nsteps, every, dp, out.ctypes.data), "pk_grad_forward")
+        return out[:nsteps]
+
+    def grad_backward(self) -> None:
+        self._chk(self.lib.pk_grad_backward(self.h), "pk_grad_backward")
+
+    def grad_release(self) -> None:
+        self._chk(self.lib.pk_grad_release(self.h), "pk_grad_release")
+
     def set_tile(self, direction: int, pencils: int, length: int, variant: int = -1) -> None:
         """Tile of the fused sweep along ``direction`` (0..2): pencils per CTA,
         output cells per pencil, launch-bound variant (-1: default)."""

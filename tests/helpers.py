@@ -35,3 +35,48 @@ def assert_bitexact(a, b, what=""):
 
 def random_state(setup: Setup, seed=0):
     return problems.random_state(setup, seed=seed)
+
+
+def smooth_state(setup: Setup, seed=0):
+    """Smooth periodic state (a few random-phase sinusoids per field) for
+    derivative checks: no cell-to-cell noise, so a small perturbation rarely
+    crosses a limiter or wave-speed switch."""
+    rng = np.random.default_rng(seed)
+    u, b, psi = problems._empty(setup)
+    x, y, z = (problems._centres(setup, d) for d in range(3))
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    L = [setup.xmax[d] - setup.xmin[d] for d in range(3)]
+
+    def wave(amp):
+        k = rng.integers(1, 3, size=3) * [int(setup.n[d] > 1) for d in range(3)]
+        ph = rng.uniform(0, 2 * np.pi, size=3)
+        return amp * (np.sin(2 * np.pi * k[0] * X / L[0] + ph[0]) * np.cos(2 * np.pi * k[1] * Y / L[1] + ph[1])
+                      + np.sin(2 * np.pi * k[2] * Z / L[2] + ph[2]))
+
+    emag = None
+    if setup.magnetic:
+        for d in range(3):
+            b[..., d] = (0.5 if d == 0 else 0.2) + wave(0.15)
+        psi[...] = wave(0.02)
+        emag = 0.5 * (b ** 2).sum(-1)
+    for f, (kind, gam) in enumerate(setup.fluids):
+        rho = 1.0 + wave(0.2)
+        p = 0.8 + wave(0.15)
+        problems._set_fluid(setup, u, f, rho, wave(0.3), wave(0.3), wave(0.3), p,
+                            emag if kind == "ion" else None)
+    return u, b, psi
+
+
+def to_soa(setup: Setup, u, b, psi):
+    """(u, b, psi) in the guard-cell layout -> one (nplanes, ez, ey, ex) array."""
+    planes = [np.moveaxis(u, -1, 0)]
+    if setup.magnetic:
+        planes += [np.moveaxis(b, -1, 0), psi[None]]
+    return np.ascontiguousarray(np.concatenate(planes, 0))
+
+
+def from_soa(setup: Setup, x):
+    nv = setup.nvar
+    if setup.magnetic:
+        return x[:nv], x[nv:nv + 3], x[nv + 3]
+    return x[:nv], None, None

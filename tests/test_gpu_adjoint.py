@@ -1,0 +1,279 @@
+"""The differentiable path: adjoint sweep kernel and checkpointed backward
+pass against central finite differences of the forward CUDA path.
+
+Directional check: for random interior directions V and weights W,
+<J^T W, V> must match (<W, F(X + eps V)> - <W, F(X - eps V)>) / (2 eps) with
+eps = 1e-6 to a relative 1e-8, along 16 directions; F is one fused sweep or
+K whole steps at a fixed dt sequence.  The error is relative to the larger of
+|FD| and the l2 norm of the per-value terms w_i (F+ - F-)_i / (2 eps): a sum
+of random-sign terms can cancel to far below its terms, and the rounding of
+the finite difference scales with the terms, not with the sum.
+
+The sweep is piecewise smooth: min/max of the two face states' wave speeds,
+limiter switches and HLLD region tests are kinks, and a direction whose
++-eps segment crosses one has no central difference to compare with.  Such a
+direction shows itself by a finite difference that changes with eps (eps and
+eps/10 disagree beyond the tolerance); it is counted and replaced by a fresh
+draw.  A direction whose finite difference is stable must match.
+
+Over several steps nearly every full-grid direction crosses some kink (tens
+of thousands of face evaluations), so the multi-step checks perturb one cell
+(all its variables) at a time; the rounding of such a small derivative's
+finite difference is near 1e-8 of it, so their tolerance is 1e-6.  The
+moncen limiter switches between its centred and one-sided slopes wherever a
+neighbour difference is three times the other, so on a 16 x 12 x 10 block a
+full-grid direction almost always crosses one: its single-sweep check also
+perturbs one cell at a time.  The Orszag-Tang check follows the workload's
+definition: the loss is the central magnetic energy, the directions are
+seeded Gaussian random fields of the relative density perturbation.
+"""
+import numpy as np
+import pytest
+
+from helpers import from_soa, setup_for, smooth_state, to_soa
+from piernik_b200 import problems
+from piernik_b200._lib import PK_LAYOUT_SOA
+from piernik_b200.sim import Simulation
+
+pytestmark = pytest.mark.gpu
+
+EPS = 1.0e-6
+RTOL = 1.0e-8
+NDIR = 16
+MAX_DRAWS = 64
+
+
+def interior_mask(setup, nplanes):
+    m = np.zeros((nplanes,) + tuple(setup.ext[::-1]), dtype=bool)
+    g, n = setup.guards, setup.n
+    m[:, g[2]:g[2] + n[2], g[1]:g[1] + n[1], g[0]:g[0] + n[0]] = True
+    return m
+
+
+def put(sim, x):
+    u, b, psi = from_soa(sim.setup, x)
+    sim.upload(np.ascontiguousarray(u), None if b is None else np.ascontiguousarray(b),
+               None if psi is None else np.ascontiguousarray(psi), layout=PK_LAYOUT_SOA)
+
+
+def get(sim):
+    u, b, psi = sim.download(layout=PK_LAYOUT_SOA)
+    planes = [u] + ([b, psi[None]] if sim.setup.magnetic else [])
+    return np.concatenate(planes, 0)
+
+
+def directions(setup, nplanes, seed, count=MAX_DRAWS, one_cell=False):
+    rng = np.random.default_rng(seed)
+    m = interior_mask(setup, nplanes)
+    cells = np.argwhere(m[0])
+    for _ in range(count):
+        if one_cell:
+            v = np.zeros(m.shape)
+            v[(slice(None),) + tuple(cells[rng.integers(0, len(cells))])] = rng.standard_normal(nplanes)
+        else:
+            v = np.where(m, rng.standard_normal(m.shape), 0.0)
+        w = np.where(m, rng.standard_normal(m.shape), 0.0)
+        yield v, w
+
+
+def central(fwd, x0, v, w, m, eps):
+    """Central difference of <W, F> along V and the l2 scale of its terms."""
+    terms = np.where(m, w * (fwd(x0 + eps * v) - fwd(x0 - eps * v)), 0.0) / (2 * eps)
+    return float(np.sum(terms)), float(np.sqrt(np.sum(terms * terms)))
+
+
+def directional_check(fwd, adj, x0, setup, nplanes, seed, what, rtol=RTOL, one_cell=False):
+    """fwd(x) -> F(x); adj(x, w, k) -> J(x)^T w for draw k.  Passes when NDIR
+    directions with a stable finite difference all match."""
+    m = interior_mask(setup, nplanes)
+    clean = kinks = 0
+    worst = 0.0
+    for k, (v, w) in enumerate(directions(setup, nplanes, seed, one_cell=one_cell)):
+        ad = float(np.sum(adj(x0, w, k) * v))
+        fd, scale = central(fwd, x0, v, w, m, EPS)
+        rel = abs(ad - fd) / max(abs(fd), scale, 1e-300)
+        if rel > rtol:
+            fd2, scale2 = central(fwd, x0, v, w, m, EPS / 10)
+            if abs(fd - fd2) > rtol * max(abs(fd), scale, scale2):
+                kinks += 1
+                continue
+            raise AssertionError(f"{what} direction {k}: adjoint {ad!r} vs finite difference {fd!r} "
+                                 f"(rel {rel:.2e}, eps/10 gives {fd2!r})")
+        worst = max(worst, rel)
+        clean += 1
+        if clean == NDIR:
+            break
+    assert clean == NDIR, f"{what}: only {clean} directions with a stable finite difference ({kinks} crossed kinks)"
+    return worst, kinks
+
+
+@pytest.mark.parametrize("phys,lim", [("hd", "vanleer"), ("hd", "minmod"), ("mhd", "vanleer"), ("mhd", "moncen")])
+def test_adjoint_sweep_vs_fd(gpu_lib, phys, lim):
+    s = setup_for(phys, n=(16, 12, 10), lim=lim)
+    x0 = to_soa(s, *smooth_state(s, seed=2))
+    sim = Simulation(s)
+    dt, ch = 0.004, 1.1
+    for cdim in (1, 2, 3):
+        def fwd(x):
+            put(sim, x)
+            sim.sweep(cdim, dt, ch)
+            return get(sim)
+
+        def adj(x, w, k):
+            put(sim, x)
+            sim.adjoint_set(w)
+            sim.adjoint_sweep(cdim, dt, ch)
+            return sim.adjoint_get()
+
+        directional_check(fwd, adj, x0, s, sim.nplanes, 7 + cdim, f"{phys}/{lim} sweep {cdim}",
+                          one_cell=(lim == "moncen"))
+    sim.close()
+
+
+def grad_at(sim, x0, w, nsteps, every, dts=None):
+    put(sim, x0)
+    sim.time_state = type(sim.time_state)()
+    got = sim.grad_forward(nsteps, every, dts)
+    sim.adjoint_set(w)
+    sim.grad_backward()
+    return sim.adjoint_get(), got
+
+
+def final_state(sim, x0, nsteps, dts):
+    put(sim, x0)
+    sim.time_state = type(sim.time_state)()
+    sim.grad_forward(nsteps, nsteps, dts)
+    return get(sim)
+
+
+def multistep_check(sim, x0, K, every, seed, what):
+    put(sim, x0)
+    sim.time_state = type(sim.time_state)()
+    dts = sim.grad_forward(K, every)
+    return directional_check(lambda x: final_state(sim, x, K, dts),
+                             lambda x, w, k: grad_at(sim, x, w, K, every, dts)[0],
+                             x0, sim.setup, sim.nplanes, seed, what, rtol=1.0e-6, one_cell=True)
+
+
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+def test_multistep_gradient_vs_fd(gpu_lib, phys):
+    s = setup_for(phys, n=(12, 12, 12), lim="vanleer")
+    x0 = to_soa(s, *smooth_state(s, seed=4))
+    sim = Simulation(s)
+    multistep_check(sim, x0, 4, 2, 9, f"{phys} 4 steps")
+    sim.close()
+
+
+def test_orszag_tang_gradient_vs_fd(gpu_lib):
+    """The differentiable Orszag-Tang workload at 32^2: loss = magnetic energy
+    of the central 8^2 cells after K = 6 steps, gradient with respect to the
+    relative density perturbation field (1e-3 x a seeded unit-rms Gaussian
+    random field at the base point) through torch.autograd (checkpoint every
+    2 steps), against central differences along 16 seeded Gaussian random
+    directions at the dt sequence of the unperturbed run."""
+    import torch
+    from piernik_b200.autograd import advance, central_magnetic_energy, last_dts, orszag_tang_state
+
+    n, K = 32, 6
+    s = problems.orszag_tang_fields(n)[0]
+    sim = Simulation(s)
+    d0 = torch.tensor(1.0e-3 * problems.orszag_tang_perturbation(n, seed=1), device="cuda", requires_grad=True)
+    out = advance(sim, orszag_tang_state(sim, d0), K, every=2)
+    loss = central_magnetic_energy(sim, out)
+    loss.backward()
+    dts = last_dts(out)
+    grad = d0.grad.detach().cpu().numpy()
+
+    def L(d):
+        with torch.no_grad():
+            return float(central_magnetic_energy(sim, advance(sim, orszag_tang_state(sim, d), K, dts=dts)))
+
+    clean = kinks = 0
+    rng = np.random.default_rng(21)
+    for k in range(MAX_DRAWS):
+        v = problems.gaussian_random_field((n, n), 8.0, rng)
+        vt = torch.tensor(v, device="cuda")
+        ad = float(np.sum(grad * v))
+        fd = (L(d0.detach() + EPS * vt) - L(d0.detach() - EPS * vt)) / (2 * EPS)
+        rel = abs(ad - fd) / max(abs(fd), 1e-300)
+        if rel > RTOL:
+            fd2 = (L(d0.detach() + 0.1 * EPS * vt) - L(d0.detach() - 0.1 * EPS * vt)) / (0.2 * EPS)
+            if abs(fd - fd2) > RTOL * abs(fd):
+                kinks += 1
+                continue
+            raise AssertionError(f"Orszag-Tang direction {k}: adjoint {ad!r} vs finite difference {fd!r} "
+                                 f"(rel {rel:.2e}, eps/10 gives {fd2!r})")
+        clean += 1
+        if clean == NDIR:
+            break
+    assert clean == NDIR, f"only {clean} directions with a stable finite difference ({kinks} crossed kinks)"
+    sim.close()
+
+
+def test_checkpoint_interval_is_exact(gpu_lib):
+    """Recomputing segments reproduces the forward bit for bit, so the gradient
+    does not depend on the checkpoint interval."""
+    s = setup_for("mhd", n=(12, 10, 8), lim="vanleer")
+    x0 = to_soa(s, *smooth_state(s, seed=5))
+    sim = Simulation(s)
+    w = next(directions(s, sim.nplanes, seed=3, count=1))[1]
+    K = 6
+    put(sim, x0)
+    dts = sim.grad_forward(K, 1)
+    ref, _ = grad_at(sim, x0, w, K, 1, dts)
+    for every in (2, 3, 4, 6, 7):
+        g, _ = grad_at(sim, x0, w, K, every, dts)
+        assert np.array_equal(g.view(np.uint64), ref.view(np.uint64)), f"every={every}"
+    assert not np.any(ref[~interior_mask(s, sim.nplanes)]), "guard cells of the gradient are not zero"
+    sim.close()
+
+
+def test_recorded_forward_equals_run(gpu_lib):
+    """pk_grad_forward without a dt sequence takes the same steps as pk_run."""
+    s = setup_for("mhd", n=(12, 10, 8), lim="moncen")
+    x0 = to_soa(s, *smooth_state(s, seed=6))
+    a, b = Simulation(s), Simulation(s)
+    put(a, x0)
+    put(b, x0)
+    dts = a.grad_forward(5, 2)
+    b.run(5)
+    assert np.array_equal(get(a).view(np.uint64), get(b).view(np.uint64))
+    assert a.time_state.t == b.time_state.t and a.time_state.nstep == b.time_state.nstep == 5
+    assert dts[0] > 0
+    a.close()
+    b.close()
+
+
+def test_torch_autograd(gpu_lib):
+    """advance() under torch.autograd gives the library's gradient."""
+    import torch
+    from piernik_b200.autograd import advance, last_dts
+
+    s = setup_for("mhd", n=(12, 12, 8), lim="vanleer")
+    x0 = to_soa(s, *smooth_state(s, seed=8))
+    sim = Simulation(s)
+    g, n = s.guards, s.n
+    inner = (slice(None), slice(g[2], g[2] + n[2]), slice(g[1], g[1] + n[1]), slice(g[0], g[0] + n[0]))
+    xi = torch.tensor(np.ascontiguousarray(x0[inner]), device="cuda", requires_grad=True)
+    out = advance(sim, xi, 3, every=2)
+    dts = last_dts(out)
+    assert dts is not None and len(dts) == 3
+    w = np.random.default_rng(1).standard_normal(tuple(out.shape))
+    (out * torch.tensor(w, device="cuda")).sum().backward()
+    grad = xi.grad.detach().cpu().numpy()
+    # the same gradient through the C ABI directly
+    wf = np.zeros_like(x0)
+    wf[inner] = w
+    ref, _ = grad_at(sim, x0, wf, 3, 2, dts)
+    assert np.array_equal(grad.view(np.uint64), np.ascontiguousarray(ref[inner]).view(np.uint64))
+    sim.close()
+
+
+def test_adjoint_rejects_unsupported(gpu_lib):
+    from piernik_b200.config import BND_OUT
+    s = setup_for("hd", n=(8, 8, 8), bnd=((BND_OUT, BND_OUT),) * 3)
+    sim = Simulation(s)
+    put(sim, to_soa(s, *smooth_state(s)))
+    with pytest.raises(RuntimeError, match="periodic"):
+        sim.grad_forward(1, 1)
+    sim.close()
