@@ -170,7 +170,16 @@ def test_orszag_tang_gradient_vs_fd(gpu_lib):
     relative density perturbation field (1e-3 x a seeded unit-rms Gaussian
     random field at the base point) through torch.autograd (checkpoint every
     2 steps), against central differences along 16 seeded Gaussian random
-    directions at the dt sequence of the unperturbed run."""
+    directions at the dt sequence of the unperturbed run.
+
+    The vortex's velocity and field are uniform along one axis each, so after
+    a density perturbation of 1e-3 the two face states of most faces differ by
+    about 1e-3 of their size: min/max switches of the wave-speed estimates sit
+    that close to the base point everywhere, and a central difference over
+    +-eps crosses a share of them that grows with eps.  Its error therefore
+    falls in proportion to eps (measured: about 1e-5 at eps = 1e-6, 1e-7 to
+    1e-8 at eps = 1e-7); the check asks for that convergence and for
+    agreement to 1e-6 of the directions' rms derivative at eps = 1e-7."""
     import torch
     from piernik_b200.autograd import advance, central_magnetic_energy, last_dts, orszag_tang_state
 
@@ -183,30 +192,34 @@ def test_orszag_tang_gradient_vs_fd(gpu_lib):
     loss.backward()
     dts = last_dts(out)
     grad = d0.grad.detach().cpu().numpy()
+    nv, cy = s.nvar, n // 4
+    y0 = (n - cy) // 2
+    dV = float(np.prod(s.dl))
 
-    def L(d):
+    def central_b(d):
         with torch.no_grad():
-            return float(central_magnetic_energy(sim, advance(sim, orszag_tang_state(sim, d), K, dts=dts)))
+            o = advance(sim, orszag_tang_state(sim, d), K, dts=dts)
+            return o[nv:nv + 3, 0, y0:y0 + cy, y0:y0 + cy].cpu().numpy()
 
-    clean = kinks = 0
+    def fd(vt, eps):
+        # the loss difference summed cell by cell, (b+ - b-)(b+ + b-) / 2, so
+        # that the sum of squares does not cancel
+        bp, bm = central_b(d0.detach() + eps * vt), central_b(d0.detach() - eps * vt)
+        return float(0.5 * ((bp - bm) * (bp + bm)).sum() * dV / (2 * eps))
+
     rng = np.random.default_rng(21)
-    for k in range(MAX_DRAWS):
+    ads, err6, err7 = [], [], []
+    for k in range(NDIR):
         v = problems.gaussian_random_field((n, n), 8.0, rng)
         vt = torch.tensor(v, device="cuda")
         ad = float(np.sum(grad * v))
-        fd = (L(d0.detach() + EPS * vt) - L(d0.detach() - EPS * vt)) / (2 * EPS)
-        rel = abs(ad - fd) / max(abs(fd), 1e-300)
-        if rel > RTOL:
-            fd2 = (L(d0.detach() + 0.1 * EPS * vt) - L(d0.detach() - 0.1 * EPS * vt)) / (0.2 * EPS)
-            if abs(fd - fd2) > RTOL * abs(fd):
-                kinks += 1
-                continue
-            raise AssertionError(f"Orszag-Tang direction {k}: adjoint {ad!r} vs finite difference {fd!r} "
-                                 f"(rel {rel:.2e}, eps/10 gives {fd2!r})")
-        clean += 1
-        if clean == NDIR:
-            break
-    assert clean == NDIR, f"only {clean} directions with a stable finite difference ({kinks} crossed kinks)"
+        ads.append(ad)
+        err6.append(abs(ad - fd(vt, EPS)))
+        err7.append(abs(ad - fd(vt, EPS / 10)))
+    rms = float(np.sqrt(np.mean(np.square(ads))))
+    err6, err7 = np.array(err6) / rms, np.array(err7) / rms
+    assert err7.max() <= 1.0e-6, f"eps=1e-7 errors {err7}"
+    assert np.median(err7) < np.median(err6) / 3, f"no convergence in eps: {np.median(err6)} -> {np.median(err7)}"
     sim.close()
 
 
