@@ -190,6 +190,27 @@ int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt
 int pk_grad_backward(pk_handle h);
 int pk_grad_release(pk_handle h);
 
+/* ---- Raw CFL time step without allocation ----
+ * No counterpart in the reference.  For host codes that cannot let this
+ * library allocate device memory (all of it is reserved for their own pool,
+ * or a cudaMalloc would synchronise the device inside their step loop) and so
+ * cannot create a handle: the same result as pk_timestep_raw over nblocks
+ * blocks whose states the caller holds in device memory, each in the
+ * handle's layout (component planes u, then bx, by, bz, psi when magnetic;
+ * each plane ext_x*ext_y*ext_z doubles with ext = n + 2*nb where n > 1,
+ * else 1).  n and dl hold 3 values per block; states holds nblocks device
+ * pointers; stream may be NULL (the legacy default stream).  The call is
+ * synchronous and allocates nothing: its reduction slots are a fixed 6 KiB
+ * device array, kept by every GPU that loads the library until exit and
+ * shared by all calls, so calls that overlap on one GPU race.  At most
+ * PK_NOALLOC_MAX_BLOCKS blocks per call (PK_E_ARG beyond).  The first call
+ * on a device looks up the array's address there: make it before any stream
+ * capture.  err (errlen bytes, or NULL) receives a message. */
+#define PK_NOALLOC_MAX_BLOCKS 64
+int pk_timestep_raw_noalloc(const pk_config* cfg, int32_t nblocks, const int32_t* n, const double* dl,
+                            const double* const* states, void* stream, double* dt_out, double* c_all_out,
+                            char* err, int32_t errlen);
+
 /* Launch-bound variants of the fused sweep: count, CTA size and CTAs per SM
  * each was compiled for (arrays of at least 16 entries). */
 int pk_tile_variants(int32_t* n, int32_t* threads, int32_t* ctas_per_sm);
