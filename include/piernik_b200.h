@@ -190,6 +190,10 @@ int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt
 int pk_grad_backward(pk_handle h);
 int pk_grad_release(pk_handle h);
 
+/* Tile of the adjoint sweep kernels along dir (0..2, -1: all): owned cells
+ * per pencil (0: default) and launch-bound variant (-1: default). */
+int pk_set_adjoint_tile(pk_handle h, int32_t dir, int32_t length, int32_t variant);
+
 /* ---- Raw CFL time step without allocation ----
  * No counterpart in the reference.  For host codes that cannot let this
  * library allocate device memory (all of it is reserved for their own pool,

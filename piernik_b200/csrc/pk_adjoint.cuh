@@ -8,9 +8,17 @@
 // is piecewise constant).  Evaluation order of the recomputed primal follows
 // pk_device.cuh exactly, so branch decisions match the forward kernels.
 #pragma once
+#include <type_traits>
+
 #include "pk_device.cuh"
 
 namespace pk {
+
+// Compile-time side of a Riemann interface.  The adjoints below pick the left
+// or right state's arrays with it, so that no array has to live in local
+// memory for a run-time pointer choice.
+template <bool B>
+using Side = std::integral_constant<bool, B>;
 
 // ---------------------------------------------------------------------------
 // utoq (interpolations.F90:69-106): ub += (dq/du)^T qb
@@ -202,11 +210,10 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
     const double zb[2] = {0.0, 0.0}, zbv[3] = {0.0, 0.0, 0.0};
     double bdump[3] = {0.0, 0.0, 0.0};
     if (sl >= 0.0 || sr <= 0.0) {
-        const bool left = sl >= 0.0;
         double fb5[5] = {0, 0, 0, 0, 0};
         for (int c = 0; c < nc; ++c) fb5[c] = fb[c];
-        side_flux_adj(has_energy, left ? ul : ur, zbv, left ? prl : prr, left ? enl : enr, fb5, zb,
-                      left ? ulb : urb, bdump, left ? prlb : prrb, left ? enlb : enrb);
+        if (sl >= 0.0) side_flux_adj(has_energy, ul, zbv, prl, enl, fb5, zb, ulb, bdump, prlb, enlb);
+        else side_flux_adj(has_energy, ur, zbv, prr, enr, fb5, zb, urb, bdump, prrb, enrb);
     } else {
         const double auxr = (sr - ur[1]) * ur[0];
         const double auxl = (sl - ul[1]) * ul[0];
@@ -219,7 +226,8 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
         const double prt = 0.5 * ((prl + dn_l * (sm - ul[1])) + (prr + dn_r * (sm - ur[1])));
         double prtb = 0.0, dn_lb = 0.0, dn_rb = 0.0, slvxlb = 0.0, srvxrb = 0.0;
         // one side's star flux f = fs + s*(us - cons), scaled by w (1 or 1/2)
-        auto side = [&](bool left, double w) {
+        auto side = [&](auto sd, double w) {
+            constexpr bool left = decltype(sd)::value;
             const double* u = left ? ul : ur;
             double* ub = left ? ulb : urb;
             const double s = left ? sl : sr;
@@ -270,9 +278,9 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
             if (left) { slb += sb; prlb += prb; enlb += enb; }
             else { srb += sb; prrb += prb; enrb += enb; }
         };
-        if (sm > 0.0) side(true, 1.0);
-        else if (sm < 0.0) side(false, 1.0);
-        else { side(true, 0.5); side(false, 0.5); }
+        if (sm > 0.0) side(Side<true>{}, 1.0);
+        else if (sm < 0.0) side(Side<false>{}, 1.0);
+        else { side(Side<true>{}, 0.5); side(Side<false>{}, 0.5); }
         // prt
         prlb += 0.5 * prtb;
         prrb += 0.5 * prtb;
@@ -365,9 +373,8 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
     for (int c = 0; c < nc; ++c) fb5[c] = fb[c];
 
     if (sl >= 0.0 || sr <= 0.0) {                                        // :312-319
-        const bool left = sl >= 0.0;
-        side_flux_adj(has_energy, left ? ul : ur, left ? bl : br, left ? prl : prr, left ? enl : enr, fb5, bfb,
-                      left ? ulb : urb, left ? blb : brb, left ? prlb : prrb, left ? enlb : enrb);
+        if (sl >= 0.0) side_flux_adj(has_energy, ul, bl, prl, enl, fb5, bfb, ulb, blb, prlb, enlb);
+        else side_flux_adj(has_energy, ur, br, prr, enr, fb5, bfb, urb, brb, prrb, enrb);
     } else {
         // ---- primal of the star / Alfven states (hlld.F90:323-474) ----
         const double auxr = (sr - ur[1]) * ur[0];
@@ -445,7 +452,8 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
         double v2b[3] = {0, 0, 0}, b2b[3] = {0, 0, 0}, vb2b = 0.0;
 
         // star flux of one side (Eq. 64), weight w
-        auto star_adj = [&](bool left, double w) {
+        auto star_adj = [&](auto sd, double w) {
+            constexpr bool left = decltype(sd)::value;
             const double* u = left ? ul : ur;
             const double* b = left ? bl : br;
             double* ub = left ? ulb : urb;
@@ -480,7 +488,8 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             else { srb += sb; prrb += prb; enrb += enb; }
         };
         // Alfven (2-star) flux of one side (Eq. 65), weight w
-        auto alfven_adj = [&](bool left, double w) {
+        auto alfven_adj = [&](auto sd, double w) {
+            constexpr bool left = decltype(sd)::value;
             const double* u = left ? ul : ur;
             const double* b = left ? bl : br;
             double* ub = left ? ulb : urb;
@@ -543,11 +552,12 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
 
         if (bx_nz) {
             if (alfl > 0.0 || alfr < 0.0) {
-                star_adj(alfl > 0.0, 1.0);
+                if (alfl > 0.0) star_adj(Side<true>{}, 1.0);
+                else star_adj(Side<false>{}, 1.0);
             } else {
-                if (sm > 0.0) alfven_adj(true, 1.0);
-                else if (sm < 0.0) alfven_adj(false, 1.0);
-                else { alfven_adj(true, 0.5); alfven_adj(false, 0.5); }
+                if (sm > 0.0) alfven_adj(Side<true>{}, 1.0);
+                else if (sm < 0.0) alfven_adj(Side<false>{}, 1.0);
+                else { alfven_adj(Side<true>{}, 0.5); alfven_adj(Side<false>{}, 0.5); }
                 // vb2 = (v2.b2)
                 for (int c = 0; c < 3; ++c) {
                     v2b[c] += vb2b * b2[c];
@@ -597,13 +607,14 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             uslb[0] += sqlb * 0.5 / sql;
             usrb[0] += sqrb * 0.5 / sqr;
         } else {
-            if (sm > 0.0) star_adj(true, 1.0);
-            else if (sm < 0.0) star_adj(false, 1.0);
-            else { star_adj(true, 0.5); star_adj(false, 0.5); }
+            if (sm > 0.0) star_adj(Side<true>{}, 1.0);
+            else if (sm < 0.0) star_adj(Side<false>{}, 1.0);
+            else { star_adj(Side<true>{}, 0.5); star_adj(Side<false>{}, 0.5); }
         }
 
         // usl[4] = n4l/slsm with n4l = (((slvxl*enl) - (prl*ul1)) + (prt*sm)) + (bl0*(vbl - vbsl))
-        auto us4_adj = [&](bool left) {
+        auto us4_adj = [&](auto sd) {
+            constexpr bool left = decltype(sd)::value;
             const double ub4 = left ? uslb[4] : usrb[4];
             if (!has_energy || ub4 == 0.0) return;
             const double ssm = left ? slsm : srsm;
@@ -632,11 +643,11 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             bb[1] += vbb * u[2];
             bb[2] += vbb * u[3];
         };
-        us4_adj(true);
-        us4_adj(false);
+        us4_adj(Side<true>{});
+        us4_adj(Side<false>{});
         // us[1..3] = us0 * vs[0..2]; us0 = dn/ssm
-        for (int side = 0; side < 2; ++side) {
-            const bool left = side == 0;
+        auto side_part1 = [&](auto sd) {
+            constexpr bool left = decltype(sd)::value;
             double* usb = left ? uslb : usrb;
             const double* us = left ? usl : usr;
             const double* vs = left ? vsl : vsr;
@@ -648,10 +659,12 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             }
             if (left) { dn_lb += usb[0] / ssm; slsmb -= usb[0] * us[0] / ssm; }
             else { dn_rb += usb[0] / ssm; srsmb -= usb[0] * us[0] / ssm; }
-        }
+        };
+        side_part1(Side<true>{});
+        side_part1(Side<false>{});
         // vbs = (vs0*bs0 + vs1*bs1) + vs2*bs2, vs0 = sm, bs0 = b0
-        for (int side = 0; side < 2; ++side) {
-            const bool left = side == 0;
+        auto side_part2 = [&](auto sd) {
+            constexpr bool left = decltype(sd)::value;
             const double vbsb = left ? vbslb : vbsrb;
             const double* vs = left ? vsl : vsr;
             const double* bs = left ? bsl : bsr;
@@ -665,10 +678,12 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
                 bsb[c] += vbsb * vs[c];
             }
             smb += vsb[0];
-        }
+        };
+        side_part2(Side<true>{});
+        side_part2(Side<false>{});
         // vs[c] = u[1+c] + k*(b[c] - bs[c]),  k = b0/dn
-        for (int side = 0; side < 2; ++side) {
-            const bool left = side == 0;
+        auto side_part3 = [&](auto sd) {
+            constexpr bool left = decltype(sd)::value;
             const double* u = left ? ul : ur;
             const double* b = left ? bl : br;
             double* ub = left ? ulb : urb;
@@ -687,11 +702,13 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             }
             bb[0] += kb / dn;
             if (left) dn_lb -= kb * k / dn; else dn_rb -= kb * k / dn;
-        }
+        };
+        side_part3(Side<true>{});
+        side_part3(Side<false>{});
         // bs[1..2]: star formula or the HLL fallback (shared by both sides)
         double hll1b = 0.0, hll2b = 0.0;
-        for (int side = 0; side < 2; ++side) {
-            const bool left = side == 0;
+        auto side_part4 = [&](auto sd) {
+            constexpr bool left = decltype(sd)::value;
             const bool star = left ? starL : starR;
             double* bsb = left ? bslb : bsrb;
             if (star) {
@@ -719,7 +736,9 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
                 hll1b += bsb[1];
                 hll2b += bsb[2];
             }
-        }
+        };
+        side_part4(Side<true>{});
+        side_part4(Side<false>{});
         if (hll1b != 0.0 || hll2b != 0.0) {
             // hll_c = ((sr*br_c - sl*bl_c) - (bcrf_c - bclf_c))/srmsl
             const double hb[3] = {0.0, hll1b, hll2b};
@@ -791,28 +810,32 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
         if (cf > 0.0) {
             // cf = sqrt(0.5*cmax), c = (a + root)/u0, root = sqrt(a*a - 4*gp*b0^2), a = gp + bb, gp = g*p
             const double cmb = cfb * 0.25 / cf;
-            const bool right = cr > cl;
-            const double* u = right ? ur : ul;
-            const double* b = right ? br : bl;
-            double* ub = right ? urb : ulb;
-            double* bb = right ? brb : blb;
-            const double c = right ? cr : cl;
-            const double a = right ? ar : al;
-            const double root = right ? rootr : rootl;
-            const double gp = right ? gpr : gpl;
-            const double numb = cmb / u[0];
-            ub[0] -= cmb * c / u[0];
-            double abb = numb, rootb = numb;
-            double gpb = 0.0;
-            if (root > 0.0) {
-                const double rb = rootb * 0.5 / root;   // d(root^2)
-                abb += rb * 2.0 * a;
-                gpb += -rb * 4.0 * (b[0] * b[0]);
-                bb[0] += -rb * (4.0 * gp) * 2.0 * b[0];
-            }
-            gpb += abb;                                    // a = gp + bb
-            for (int k = 0; k < 3; ++k) bb[k] += abb * 2.0 * b[k];
-            ub[4] += gpb * gamma;
+            auto cf_adj = [&](auto sd) {
+                constexpr bool right = decltype(sd)::value;
+                const double* u = right ? ur : ul;
+                const double* b = right ? br : bl;
+                double* ub = right ? urb : ulb;
+                double* bb = right ? brb : blb;
+                const double c = right ? cr : cl;
+                const double a = right ? ar : al;
+                const double root = right ? rootr : rootl;
+                const double gp = right ? gpr : gpl;
+                const double numb = cmb / u[0];
+                ub[0] -= cmb * c / u[0];
+                double abb = numb, rootb = numb;
+                double gpb = 0.0;
+                if (root > 0.0) {
+                    const double rb = rootb * 0.5 / root;   // d(root^2)
+                    abb += rb * 2.0 * a;
+                    gpb += -rb * 4.0 * (b[0] * b[0]);
+                    bb[0] += -rb * (4.0 * gp) * 2.0 * b[0];
+                }
+                gpb += abb;                                    // a = gp + bb
+                for (int k = 0; k < 3; ++k) bb[k] += abb * 2.0 * b[k];
+                ub[4] += gpb * gamma;
+            };
+            if (cr > cl) cf_adj(Side<true>{});
+            else cf_adj(Side<false>{});
         }
         pr_en_adj(true, gamma, ul, bl, prlb, enlb, ulb, blb);
         pr_en_adj(true, gamma, ur, br, prrb, enrb, urb, brb);

@@ -7,9 +7,15 @@
 // returns dL/dU:
 //   mu2  = floors2^T (fac-scaled lam'')
 //   lam  = mu2 + floors1^T( c2 D'(U*)^T mu2 ) + c1 D'(U)^T floors1^T(...)
-// Each CTA recomputes both forward stages for its tile (8-cell halo read with
-// periodic wrap), recording which floors clipped, then runs the two
-// transposed divergences back to front.  D'(V)^T mu is assembled face by
+// The backward pass runs it as three kernels per sweep:
+//   k_sweep_fused_rec  the forward sweep again, also storing U* and which
+//                      floors clipped in either stage (2 bytes per cell);
+//   k_adj_stage2       mu2, rho = c2 D'(U*)^T mu2, mu1 = floors1^T rho:
+//                      writes lam_acc = mu2 + mu1 and m1 = c1 mu1;
+//   k_adj_stage1       lam = lam_acc + D'(U)^T m1.
+// Each adjoint kernel holds one transposed divergence (one Riemann adjoint per
+// face, no forward Riemann solve) over a tile with a 3-cell halo read with
+// periodic wrap.  D'(V)^T mu is assembled face by
 // face: g_{k+1/2} = mu_{k+1} - mu_k, the Riemann adjoint gives the adjoints of
 // the two face states, the slope adjoint spreads them over the 3-cell
 // stencil, and utoq's adjoint maps primitive adjoints to conservative ones.
@@ -118,22 +124,34 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active
     __syncthreads();
 }
 
-// Adjoint of one fused sweep (k_sweep_fused) of a periodic block:
-// lam_out = dL/d(sweep output) in, lam_in = dL/d(sweep input) out.
-// grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2;
-// each tile spans L + 16 cells (8-cell halo) along the sweep.
+// floor records of both stages of one cell, as stored by k_sweep_fused_rec:
+// bits 0-2 density floors of stage 1 (one per fluid), 3-5 its internal-energy
+// floors, 6-8 and 9-11 the same for stage 2
+PK_DEV unsigned short pack_floors(const FloorRec& r1, const FloorRec& r2)
+{
+    return (unsigned short)(r1.dn | (r1.en << 3) | (r2.dn << 6) | (r2.en << 9));
+}
+
+PK_DEV FloorRec unpack_floors(unsigned short f, int stage)
+{
+    const int sh = stage == 1 ? 0 : 6;
+    return FloorRec{(unsigned)(f >> sh) & 7u, (unsigned)(f >> (sh + 3)) & 7u};
+}
+
+// The fused forward sweep (k_sweep_fused) that also stores the stage-1 state
+// U* and the floor records of the owned cells: the backward pass's segment
+// recomputation.
 template <class PH, int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB) k_sweep_adj(Geom g, Tile tl, const double* __restrict__ uin,
-                                                         const double* __restrict__ lam_out,
-                                                         double* __restrict__ lam_in, PhysParams pp, double dl,
-                                                         const StepParams* __restrict__ sp, int apply_fac,
-                                                         unsigned* __restrict__ gstatus)
+__global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused_rec(Geom g, Tile tl, const double* __restrict__ uin,
+                                                               double* __restrict__ uout, double* __restrict__ ustar,
+                                                               unsigned short* __restrict__ flags, PhysParams pp,
+                                                               double dl, const StepParams* __restrict__ sp,
+                                                               int apply_fac, unsigned* __restrict__ gstatus)
 {
     extern __shared__ double smem[];
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
-    const Smem fsm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
-    const AdjSmem asm_{smem, smem + NV * PT, smem + 2 * NV * PT, smem + 3 * NV * PT, PT};
+    const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
     const int tid = threadIdx.x;
     int p, t;
     if (tl.xfast) { t = tid % T; p = tid / T; }
@@ -144,17 +162,16 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_adj(Geom g, Tile tl, const
     const int c0 = blockIdx.y * tl.L;
     const int i2 = blockIdx.z;
     const bool active = (tid < PT) && (i1 < g.n1);
-    const int s = c0 - 8 + t;
+    const int s = c0 - 4 + t;
     const long long off = (long long)(g.g_d + wrap(s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
                           (long long)(g.g2 + i2) * g.s2;
-    const double dt = sp->dt, ch = sp->ch, fac = apply_fac ? sp->psi_fac : 1.0;
+    const double dt = sp->dt;
     const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
     unsigned status = 0;
     double w[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) w[v] = 0.0;
     if (active) load_cell<PH>(uin, off, g, w);
-    // forward stage 1 on [0, T) -> U* on [2, T-2)
     FloorRec rec1{0, 0}, rec2{0, 0};
     Roles r;
     r.end = 0;
@@ -163,55 +180,131 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_adj(Geom g, Tile tl, const
     r.slope = active && t >= 1 && t < T - 1;
     r.flux = active && t >= 1 && t < T - 2;
     r.upd = active && t >= 2 && t < T - 2;
-    rk_stage<PH, true>(fsm, me, st, r, w, uin, uin, off, g, c1, ch, pp, status, &rec1);
-    double us[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) us[v] = w[v];
-    // forward stage 2 on [2, T-2) -> U'' on [4, T-4)
+    rk_stage<PH, true>(sm, me, st, r, w, uin, uin, off, g, c1, sp->ch, pp, status, &rec1);
+    const bool own = active && t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d;
+    if (own) store_cell<PH>(ustar, off, g, w);
     r.q = active && t >= 2 && t < T - 2;
     r.slope = active && t >= 3 && t < T - 3;
     r.flux = active && t >= 3 && t < T - 4;
     r.upd = active && t >= 4 && t < T - 4;
-    rk_stage<PH, true>(fsm, me, st, r, w, uin, uin, off, g, c2, ch, pp, status, &rec2);
-    // adjoint of the stage-2 floors (and of the psi damping folded into this sweep)
-    double lam[NV], mu[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) lam[v] = mu[v] = 0.0;
-    if (active && t >= 4 && t < T - 4) {
-        load_cell<PH>(lam_out, off, g, mu);
-        if (PH::MHD) mu[PH::IB + 3] = mu[PH::IB + 3] * fac;
-        floors_adj<PH>(w, rec2, mu);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            lam[v] = mu[v];
-            mu[v] = c2 * mu[v];
-        }
-    }
-    // c2 D'(U*)^T mu2 -> valid on [6, T-6)
-    double rho[NV];
-    adj_divergence<PH>(asm_, me, st, t, active, 2, T - 2, 4, T - 4, us, mu, ch, pp, rho);
-    // adjoint of the stage-1 floors
-#pragma unroll
-    for (int v = 0; v < NV; ++v) mu[v] = 0.0;
-    if (active && t >= 6 && t < T - 6) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) mu[v] = rho[v];
-        floors_adj<PH>(us, rec1, mu);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            lam[v] += mu[v];
-            mu[v] = c1 * mu[v];
-        }
-    }
-    // c1 D'(U)^T mu1 -> valid on [8, T-8)
-    if (active) load_cell<PH>(uin, off, g, w);
-    adj_divergence<PH>(asm_, me, st, t, active, 0, T, 6, T - 6, w, mu, ch, pp, rho);
-    if (active && t >= 8 && t < T - 8 && s < c0 + tl.L && s < g.n_d) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) lam[v] += rho[v];
-        store_cell<PH>(lam_in, off, g, lam);
+    rk_stage<PH, true>(sm, me, st, r, w, uin, uin, off, g, c2, sp->ch, pp, status, &rec2);
+    if (own) {
+        if (PH::MHD && apply_fac) w[PH::IB + 3] = w[PH::IB + 3] * sp->psi_fac;
+        store_cell<PH>(uout, off, g, w);
+        flags[off] = pack_floors(rec1, rec2);
     }
     flush_status(status, gstatus);
+}
+
+// Tile position shared by the two adjoint kernels: 3-cell halo.
+struct AdjPos {
+    int t, me, st, s;
+    bool active, own;
+    long long off;
+};
+
+PK_DEV AdjPos adj_pos(const Geom& g, const Tile& tl)
+{
+    AdjPos a;
+    const int P = tl.P, T = tl.T, PT = P * T;
+    const int tid = threadIdx.x;
+    int p;
+    if (tl.xfast) { a.t = tid % T; p = tid / T; }
+    else { p = tid % P; a.t = tid / P; }
+    const int spp = tl.xfast ? T : 1;
+    a.st = tl.xfast ? 1 : P;
+    a.me = p * spp + a.t * a.st;
+    const int i1 = blockIdx.x * P + p;
+    const int c0 = blockIdx.y * tl.L;
+    a.active = (tid < PT) && (i1 < g.n1);
+    a.s = c0 - 3 + a.t;
+    a.own = a.active && a.t >= 3 && a.t < T - 3 && a.s < c0 + tl.L && a.s < g.n_d;
+    a.off = (long long)(g.g_d + wrap(a.s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
+            (long long)(g.g2 + blockIdx.z) * g.s2;
+    return a;
+}
+
+// Stage-2 half of the sweep adjoint.  In: U* (ustar), the sweep output U''
+// (read only where an energy floor clipped), floor records, lam'' (lam_out).
+// Out on every interior cell: lam_acc = mu2 + mu1 and m1 = c1 mu1.
+template <class PH, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_adj_stage2(Geom g, Tile tl, const double* __restrict__ ustar,
+                                                          const double* __restrict__ uout,
+                                                          const unsigned short* __restrict__ flags,
+                                                          const double* __restrict__ lam_out,
+                                                          double* __restrict__ lam_acc, double* __restrict__ m1,
+                                                          PhysParams pp, double dl, const StepParams* __restrict__ sp,
+                                                          int apply_fac)
+{
+    extern __shared__ double smem[];
+    constexpr int NV = PH::NV;
+    const int PT = tl.P * tl.T;
+    const AdjSmem asm_{smem, smem + NV * PT, smem + 2 * NV * PT, smem + 3 * NV * PT, PT};
+    const AdjPos a = adj_pos(g, tl);
+    const double dt = sp->dt, ch = sp->ch, fac = apply_fac ? sp->psi_fac : 1.0;
+    const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
+    double V[NV], mu[NV], mu2[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) V[v] = mu[v] = 0.0;
+    unsigned short fl = 0;
+    if (a.active) {
+        load_cell<PH>(ustar, a.off, g, V);
+        load_cell<PH>(lam_out, a.off, g, mu);
+        fl = flags[a.off];
+        if (PH::MHD) mu[PH::IB + 3] = mu[PH::IB + 3] * fac;
+        const FloorRec r2 = unpack_floors(fl, 2);
+        if (r2.en || r2.dn) {
+            double w[NV];
+            load_cell<PH>(uout, a.off, g, w);
+            floors_adj<PH>(w, r2, mu);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        mu2[v] = mu[v];
+        mu[v] = c2 * mu[v];
+    }
+    double rho[NV];
+    adj_divergence<PH>(asm_, a.me, a.st, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, ch, pp, rho);
+    if (a.own) {
+        floors_adj<PH>(V, unpack_floors(fl, 1), rho);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            mu2[v] += rho[v];
+            rho[v] = c1 * rho[v];
+        }
+        store_cell<PH>(lam_acc, a.off, g, mu2);
+        store_cell<PH>(m1, a.off, g, rho);
+    }
+}
+
+// Stage-1 half: lam_io = lam_acc + D'(U)^T m1, in place.
+template <class PH, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_adj_stage1(Geom g, Tile tl, const double* __restrict__ uin,
+                                                          const double* __restrict__ m1, double* __restrict__ lam_io,
+                                                          PhysParams pp, const StepParams* __restrict__ sp)
+{
+    extern __shared__ double smem[];
+    constexpr int NV = PH::NV;
+    const int PT = tl.P * tl.T;
+    const AdjSmem asm_{smem, smem + NV * PT, smem + 2 * NV * PT, smem + 3 * NV * PT, PT};
+    const AdjPos a = adj_pos(g, tl);
+    double V[NV], mu[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) V[v] = mu[v] = 0.0;
+    if (a.active) {
+        load_cell<PH>(uin, a.off, g, V);
+        load_cell<PH>(m1, a.off, g, mu);
+    }
+    double rho[NV];
+    adj_divergence<PH>(asm_, a.me, a.st, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, sp->ch, pp, rho);
+    if (a.own) {
+        double l[NV];
+        load_cell<PH>(lam_io, a.off, g, l);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) l[v] += rho[v];
+        store_cell<PH>(lam_io, a.off, g, l);
+    }
 }
 
 }  // namespace pk

@@ -443,8 +443,11 @@ int pk_destroy(pk_handle h)
     for (int d = 0; d < 3; ++d) cudaFree(h->batch[d].dev);
     for (double* p : h->grad_ckpt) cudaFree(p);
     for (double* p : h->grad_pool) cudaFree(p);
+    for (double* p : h->grad_star) cudaFree(p);
+    for (unsigned short* p : h->grad_flags) cudaFree(p);
     cudaFree(h->lam);
     cudaFree(h->lam_tmp);
+    cudaFree(h->lam_m1);
     cudaFree(h->d_desc[0]);
     cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
@@ -892,8 +895,12 @@ void grad_release(pk_ctx* h)
     cudaStreamSynchronize(h->stream);
     for (double* p : h->grad_ckpt) cudaFree(p);
     for (double* p : h->grad_pool) cudaFree(p);
+    for (double* p : h->grad_star) cudaFree(p);
+    for (unsigned short* p : h->grad_flags) cudaFree(p);
     h->grad_ckpt.clear();
     h->grad_pool.clear();
+    h->grad_star.clear();
+    h->grad_flags.clear();
     h->grad_steps.clear();
 }
 
@@ -913,6 +920,26 @@ int alloc_state(pk_ctx* h, const Block& b, double** p)
     if (cudaMalloc(p, sizeof(double) * h->nplanes * b.plane) != cudaSuccess)
         return fail(h, PK_E_NOMEM, "cudaMalloc for the differentiable path failed");
     PK_CUDA(h, cudaMemsetAsync(*p, 0, sizeof(double) * h->nplanes * b.plane, h->stream));
+    return PK_OK;
+}
+
+// room for the recomputed sweeps of `need` sweeps (output, stage-1 state,
+// floor records) and the adjoint sweep's scratch state
+int ensure_pool(pk_ctx* h, const Block& b, int need)
+{
+    while ((int)h->grad_pool.size() < need) {
+        double *p, *q;
+        if (int rc = alloc_state(h, b, &p)) return rc;
+        h->grad_pool.push_back(p);
+        if (int rc = alloc_state(h, b, &q)) return rc;
+        h->grad_star.push_back(q);
+        unsigned short* f;
+        if (cudaMalloc(&f, sizeof(unsigned short) * b.plane) != cudaSuccess)
+            return fail(h, PK_E_NOMEM, "cudaMalloc for the differentiable path failed");
+        h->grad_flags.push_back(f);
+    }
+    if (!h->lam_m1)
+        if (int rc = alloc_state(h, b, &h->lam_m1)) return rc;
     return PK_OK;
 }
 
@@ -995,8 +1022,14 @@ int pk_adjoint_sweep(pk_handle h, int32_t cdim, double dt, double chspeed)
     if (int rc = grad_check(h)) return rc;
     if (!h->lam) return fail(h, PK_E_STATE, "set the adjoint first (pk_adjoint_set)");
     Block& b = h->blocks[0];
+    const PhysOps* ops = ops_of(h);
+    if (int rc = ensure_pool(h, b, 1)) return rc;
     if (int rc = put_step_params(h, dt, chspeed, 1.0)) return rc;
-    if (int rc = ops_of(h)->adj(h, b, cdim - 1, 0, state(h, b), h->lam, h->lam_tmp)) return rc;
+    const int d = cdim - 1;
+    if (int rc = ops->fused_rec(h, b, d, 0, state(h, b), h->grad_pool[0], h->grad_star[0], h->grad_flags[0])) return rc;
+    if (int rc = ops->adj(h, b, d, 0, state(h, b), h->grad_star[0], h->grad_pool[0], h->grad_flags[0], h->lam,
+                          h->lam_tmp, h->lam_m1))
+        return rc;
     std::swap(h->lam, h->lam_tmp);
     PK_CUDA(h, cudaStreamSynchronize(h->stream));
     return PK_OK;
@@ -1052,12 +1085,7 @@ int pk_grad_backward(pk_handle h)
     const int nsw = step_plan(h, dir, fac);
     const int K = (int)h->grad_steps.size(), C = h->grad_every;
     if (K == 0) return PK_OK;
-    const int need = C * nsw;
-    while ((int)h->grad_pool.size() < need) {
-        double* p;
-        if (int rc = alloc_state(h, b, &p)) return rc;
-        h->grad_pool.push_back(p);
-    }
+    if (int rc = ensure_pool(h, b, C * nsw)) return rc;
     const int nseg = (K + C - 1) / C;
     for (int seg = nseg - 1; seg >= 0; --seg) {
         const int s0 = seg * C, len = (K - s0 < C) ? K - s0 : C;
@@ -1067,9 +1095,10 @@ int pk_grad_backward(pk_handle h)
             const StepRec& r = h->grad_steps[s0 + j];
             if (int rc = put_step_params(h, r.dt, r.ch, r.fac)) return rc;
             for (int k = 0; k < nsw; ++k) {
-                double* out = h->grad_pool[j * nsw + k];
-                if (int rc = ops->fused_ptr(h, b, dir[k], fac[k], x, out)) return rc;
-                x = out;
+                const int i = j * nsw + k;
+                if (int rc = ops->fused_rec(h, b, dir[k], fac[k], x, h->grad_pool[i], h->grad_star[i], h->grad_flags[i]))
+                    return rc;
+                x = h->grad_pool[i];
             }
         }
         // adjoint sweeps back to the segment's start
@@ -1077,14 +1106,29 @@ int pk_grad_backward(pk_handle h)
             const StepRec& r = h->grad_steps[s0 + j];
             if (int rc = put_step_params(h, r.dt, r.ch, r.fac)) return rc;
             for (int k = nsw - 1; k >= 0; --k) {
-                const double* uin = k > 0 ? h->grad_pool[j * nsw + k - 1]
-                                          : (j > 0 ? h->grad_pool[(j - 1) * nsw + nsw - 1] : h->grad_ckpt[seg]);
-                if (int rc = ops->adj(h, b, dir[k], fac[k], uin, h->lam, h->lam_tmp)) return rc;
+                const int i = j * nsw + k;
+                const double* uin = i > 0 ? h->grad_pool[i - 1] : h->grad_ckpt[seg];
+                if (int rc = ops->adj(h, b, dir[k], fac[k], uin, h->grad_star[i], h->grad_pool[i], h->grad_flags[i],
+                                      h->lam, h->lam_tmp, h->lam_m1))
+                    return rc;
                 std::swap(h->lam, h->lam_tmp);
             }
         }
     }
     PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_set_adjoint_tile(pk_handle h, int32_t dir, int32_t length, int32_t variant)
+{
+    if (!h) return PK_E_ARG;
+    if (dir < -1 || dir > 2 || length < 0 || length > 250 || variant < -1 || variant > 4)
+        return fail(h, PK_E_ARG, "adjoint tile: dir -1..2, length 0..250, variant -1..4");
+    for (int d = 0; d < 3; ++d)
+        if (dir < 0 || dir == d) {
+            h->adjL[d] = length;
+            h->adjV[d] = variant;
+        }
     return PK_OK;
 }
 

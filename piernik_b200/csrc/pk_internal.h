@@ -80,13 +80,17 @@ struct pk_ctx {
     int use_graph = 0;
     long long graph_kernels = 0;        // kernel nodes of the captured step
     // differentiable path (single block, fused sweeps)
-    int adjL = 0;                       // chunk length of the adjoint tiles (0: default)
+    int adjL[3] = {0, 0, 0};            // owned cells per pencil of the adjoint tiles, per direction (0: default)
+    int adjV[3] = {-1, -1, -1};         // launch-bound variant of the adjoint kernels per direction (-1: default)
     std::vector<pk::StepRec> grad_steps;        // dt, chspeed, damping of each recorded step
     std::vector<double*> grad_ckpt;             // checkpointed states (every grad_every steps)
     int grad_every = 0;
     double* lam = nullptr;                      // adjoint of the state (structure of arrays)
     double* lam_tmp = nullptr;
-    std::vector<double*> grad_pool;             // states of a recomputed segment's sweeps
+    std::vector<double*> grad_pool;             // outputs of a recomputed segment's sweeps
+    std::vector<double*> grad_star;             // their stage-1 states
+    std::vector<unsigned short*> grad_flags;    // their floor records
+    double* lam_m1 = nullptr;                   // scratch state of the adjoint sweep
     pk_time_state grad_ts0;                     // time state at the start of the recording
 };
 
@@ -105,7 +109,10 @@ struct PhysOps {
     int (*stage)(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch);
     int (*batched)(pk_ctx* h, int dir, int apply_fac, unsigned* counter);
     int (*fused_ptr)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out);
-    int (*adj)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* lam_out, double* lam_in);
+    int (*fused_rec)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out, double* ustar,
+                     unsigned short* flags);
+    int (*adj)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* ustar,
+               const double* uout, const unsigned short* flags, const double* lam_out, double* lam_in, double* m1);
 };
 
 const PhysOps* ops_hd1();

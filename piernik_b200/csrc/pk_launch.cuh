@@ -99,40 +99,129 @@ int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
     return PK_OK;
 }
 
-// Adjoint of one fused sweep: lam_in = (d sweep / d uin)^T lam_out
+// Tile of the recording forward sweep: the forward sweep's tile along dir,
+// fitted into 256 threads.
+inline int rec_tile(pk_ctx* h, const Block& b, const Geom& g, int dir, Tile* tl)
+{
+    int L = h->tileL[dir] > 0 ? h->tileL[dir] : DEF_L[dir];
+    if (L > 248) L = 248;
+    if (L > b.n[dir]) L = b.n[dir];
+    int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
+    if (P > g.n1) P = g.n1;
+    const int T = L + 8;
+    while (P * T > 256 && P > 1) --P;
+    tl->P = P;
+    tl->T = T;
+    tl->L = L;
+    tl->halo = 4;
+    tl->xfast = dir == 0;
+    return PK_OK;
+}
+
+// The forward sweep of the backward pass's recomputation: also stores U* and
+// the floor records (k_sweep_fused_rec)
 template <class PH>
-int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* lam_out, double* lam_in)
+int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out, double* ustar,
+                     unsigned short* flags)
+{
+    if constexpr (PH::NFL != 1) {
+        return fail(h, PK_E_UNSUPPORTED, "the differentiable path is built for one-fluid HD and MHD");
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            PK_CUDA(h, cudaFuncSetAttribute(k_sweep_fused_rec<PH, 256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            220 * 1024));
+            attr = true;
+        }
+        Geom g = make_geom(b, dir);
+        Tile tl;
+        if (int rc = rec_tile(h, b, g, dir, &tl)) return rc;
+        dim3 grid((g.n1 + tl.P - 1) / tl.P, (b.n[dir] + tl.L - 1) / tl.L, g.n2);
+        const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+        std::pair<cudaEvent_t, cudaEvent_t> ev;
+        if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+        k_sweep_fused_rec<PH, 256, 1><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, ustar, flags, h->pp,
+                                                                            b.dl[dir], h->d_step, apply_fac,
+                                                                            h->d_status);
+        PK_CUDA(h, cudaGetLastError());
+        if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+        h->launches += 1;
+        return PK_OK;
+    }
+}
+
+// Launch-bound variants of the two adjoint kernels (threads per CTA, CTAs per SM)
+constexpr int NADJ_VARIANT = 5;
+constexpr int ADJ_T[NADJ_VARIANT] = {256, 256, 192, 128, 128};
+// defaults per sweep direction, measured on B200 at 128^3 (MHD and HD) over
+// variants x owned lengths 26..250: 8 pencils x 32 cells in 256 threads with
+// 128 registers (spilling) beat every longer tile and every variant with
+// more registers per thread
+constexpr int DEF_ADJ_V[3] = {1, 1, 1};
+constexpr int DEF_ADJ_L[3] = {26, 26, 26};
+
+template <class PH>
+struct AdjKernels {
+    decltype(&k_adj_stage2<PH, 256, 1>) s2;
+    decltype(&k_adj_stage1<PH, 256, 1>) s1;
+};
+
+template <class PH>
+AdjKernels<PH> adj_variant(int v)
+{
+    switch (v) {
+    case 0: return {k_adj_stage2<PH, 256, 1>, k_adj_stage1<PH, 256, 1>};
+    case 1: return {k_adj_stage2<PH, 256, 2>, k_adj_stage1<PH, 256, 2>};
+    case 2: return {k_adj_stage2<PH, 192, 2>, k_adj_stage1<PH, 192, 2>};
+    case 3: return {k_adj_stage2<PH, 128, 3>, k_adj_stage1<PH, 128, 3>};
+    default: return {k_adj_stage2<PH, 128, 4>, k_adj_stage1<PH, 128, 4>};
+    }
+}
+
+// Adjoint of one fused sweep: lam_in = (d sweep / d uin)^T lam_out, from the
+// sweep's input, its stage-1 state, its output and floor records; m1 is
+// scratch of one state.
+template <class PH>
+int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* ustar, const double* uout,
+               const unsigned short* flags, const double* lam_out, double* lam_in, double* m1)
 {
     if constexpr (PH::NFL != 1) {
         return fail(h, PK_E_UNSUPPORTED, "the adjoint sweep is built for one-fluid HD and MHD");
     } else {
         static bool attr = false;
         if (!attr) {
-            PK_CUDA(h, cudaFuncSetAttribute(k_sweep_adj<PH, 256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            for (int v = 0; v < NADJ_VARIANT; ++v) {
+                const AdjKernels<PH> k = adj_variant<PH>(v);
+                PK_CUDA(h, cudaFuncSetAttribute(k.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+                PK_CUDA(h, cudaFuncSetAttribute(k.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            }
             attr = true;
         }
+        const int var = (h->adjV[dir] >= 0 && h->adjV[dir] < NADJ_VARIANT) ? h->adjV[dir] : DEF_ADJ_V[dir];
         Geom g = make_geom(b, dir);
         Tile tl;
-        int L = h->adjL > 0 ? h->adjL : 48;
+        int L = h->adjL[dir] > 0 ? h->adjL[dir] : DEF_ADJ_L[dir];
+        if (L > ADJ_T[var] - 6) L = ADJ_T[var] - 6;
         if (L > b.n[dir]) L = b.n[dir];
-        const int T = L + 16;
-        int P = 256 / T;
-        if (P < 1) return fail(h, PK_E_ARG, "adjoint tile longer than 256");
-        if (P > g.n1) P = g.n1;
-        tl.P = P;
-        tl.T = T;
+        tl.T = L + 6;
+        tl.P = ADJ_T[var] / tl.T;
+        if (tl.P < 1) return fail(h, PK_E_ARG, "adjoint tile longer than the variant's CTA size");
+        if (tl.P > g.n1) tl.P = g.n1;
         tl.L = L;
-        tl.halo = 8;
+        tl.halo = 3;
         tl.xfast = dir == 0;
-        dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
-        const size_t smem = 4ull * PH::NV * P * T * sizeof(double);
+        dim3 grid((g.n1 + tl.P - 1) / tl.P, (b.n[dir] + tl.L - 1) / tl.L, g.n2);
+        const size_t smem = 4ull * PH::NV * tl.P * tl.T * sizeof(double);
+        const AdjKernels<PH> k = adj_variant<PH>(var);
         std::pair<cudaEvent_t, cudaEvent_t> ev;
         if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-        k_sweep_adj<PH, 256, 1><<<grid, P * T, smem, h->stream>>>(g, tl, uin, lam_out, lam_in, h->pp, b.dl[dir],
-                                                                h->d_step, apply_fac, h->d_status);
+        k.s2<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, ustar, uout, flags, lam_out, lam_in, m1, h->pp, b.dl[dir],
+                                                     h->d_step, apply_fac);
+        PK_CUDA(h, cudaGetLastError());
+        k.s1<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, uin, m1, lam_in, h->pp, h->d_step);
         PK_CUDA(h, cudaGetLastError());
         if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
-        h->launches += 1;
+        h->launches += 2;
         return PK_OK;
     }
 }
@@ -222,7 +311,7 @@ template <class PH>
 const PhysOps* make_ops()
 {
     static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_batched<PH>,
-                     launch_fused_ptr<PH>, launch_adj<PH>};
+                     launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>};
     return &o;
 }
 

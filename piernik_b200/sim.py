@@ -286,6 +286,11 @@ class Simulation:
     def grad_backward(self) -> None:
         self._chk(self.lib.pk_grad_backward(self.h), "pk_grad_backward")
 
+    def set_adjoint_tile(self, direction: int = -1, length: int = 0, variant: int = -1) -> None:
+        """Owned cells per pencil and launch-bound variant of the adjoint
+        kernels along ``direction`` (0..2, -1: all)."""
+        self._chk(self.lib.pk_set_adjoint_tile(self.h, direction, length, variant), "pk_set_adjoint_tile")
+
     def grad_release(self) -> None:
         self._chk(self.lib.pk_grad_release(self.h), "pk_grad_release")
 
