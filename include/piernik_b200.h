@@ -161,6 +161,18 @@ int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant);
  * device memory, so one capture serves every step. */
 int pk_use_graph(pk_handle h, int32_t enable);
 
+/* ---- Connected blocks of one level (cg_list_bnd.F90:251-324) ----
+ * pk_set_domain declares a level of ncells cells per direction (periodic or
+ * not per direction); pk_block_place puts a block's first interior cell at
+ * off on that grid.  From then on every guard refresh (pk_fill_guards, and
+ * the one after each RK stage of pk_sweep) copies the neighbours' interior
+ * cells into the guard cells that lie over them, after the blocks' own
+ * boundary rules (outflow / reflecting) have filled the rest; the sweep runs
+ * per RK stage (pk_solve_cg) for such a domain.  Overlapping blocks are
+ * rejected at the first refresh. */
+int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3]);
+int pk_block_place(pk_handle h, int32_t id, const int64_t off[3]);
+
 /* ---- Differentiable path (one periodic block, one fluid, RK2) ----
  * Not in the reference, which has no derivatives: the adjoint (reverse
  * mode) of the sweep path at a fixed sequence of time steps. */

@@ -30,7 +30,7 @@ EXPORTS = (
     "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_use_graph",
     "pk_upload_device", "pk_download_device", "pk_adjoint_set", "pk_adjoint_get", "pk_adjoint_sweep",
     "pk_grad_forward", "pk_grad_backward", "pk_grad_release",
-    "pk_timestep_raw_noalloc", "pk_set_adjoint_tile",
+    "pk_timestep_raw_noalloc", "pk_set_adjoint_tile", "pk_set_domain", "pk_block_place",
 )
 
 
@@ -126,6 +126,8 @@ def load(path: str = LIBPATH):
     L.pk_grad_backward.argtypes = [H]
     L.pk_grad_release.argtypes = [H]
     L.pk_set_adjoint_tile.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
+    L.pk_set_domain.argtypes = [H, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    L.pk_block_place.argtypes = [H, C.c_int32, C.POINTER(C.c_int64)]
     L.pk_timestep_raw_noalloc.argtypes = [C.POINTER(PkConfig), C.c_int32, C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.c_void_p,
                                           C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_char_p, C.c_int32]

@@ -13,9 +13,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["pk_api.cu", "pk_noalloc.cu", "pk_phys_hd1.cu", "pk_phys_hd2.cu", "pk_phys_mhd1.cu", "pk_phys_mhd2.cu", "pk_phys_mhd3.cu"]
+UNITS = ["pk_api.cu", "pk_noalloc.cu", "pk_exchange.cpp", "pk_phys_hd1.cu", "pk_phys_hd2.cu", "pk_phys_mhd1.cu", "pk_phys_mhd2.cu", "pk_phys_mhd3.cu"]
 HEADERS = ["pk_device.cuh", "pk_kernels.cuh", "pk_aux.cuh", "pk_internal.h", "pk_launch.cuh", "pk_adjoint.cuh",
-           "pk_adjoint_kernels.cuh"]
+           "pk_adjoint_kernels.cuh", "pk_exchange.h"]
 DEPS = [os.path.join(CSRC, f) for f in UNITS + HEADERS]
 INC = os.path.join(os.path.dirname(HERE), "include")
 OUT = os.path.join(HERE, "libpiernik_b200.so")
@@ -40,7 +40,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     procs = []
     objs = []
     for unit in UNITS:
-        obj = os.path.join(objdir, unit.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
         cmd = [NVCC] + FLAGS + (["-Xptxas=-v"] if verbose else []) + ["-I", INC, "-c", "-o", obj,
                                                                     os.path.join(CSRC, unit)]

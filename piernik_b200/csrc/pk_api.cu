@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "pk_aux.cuh"
+#include "pk_exchange.h"
 #include "pk_internal.h"
 
 using namespace pk;
@@ -127,9 +128,79 @@ int fill_guards_block(pk_ctx* h, Block& b)
     return PK_OK;
 }
 
+// Same-level exchange of all placed blocks' guard cells (update_boundaries'
+// internal part); blocks' own boundary rules were applied before.
+int exchange_guards(pk_ctx* h)
+{
+    if (!h->connected) return PK_OK;
+    const int nb = (int)h->blocks.size();
+    if (h->x_dirty) {
+        std::vector<XBlock> xb(nb);
+        for (int i = 0; i < nb; ++i) {
+            const Block& b = h->blocks[i];
+            if (!b.placed) return fail(h, PK_E_STATE, "every block of a connected domain must be placed (pk_block_place)");
+            for (int d = 0; d < 3; ++d) {
+                xb[i].n[d] = b.n[d];
+                xb[i].g[d] = b.g[d];
+                xb[i].off[d] = b.off[d];
+            }
+        }
+        std::vector<XSeg> segs;
+        std::string err;
+        if (!build_exchange(xb, h->dom, h->dom_periodic, segs, err)) return fail(h, PK_E_ARG, err);
+        std::vector<XSegDev> dev(segs.size());
+        long long total = 0;
+        for (size_t s = 0; s < segs.size(); ++s) {
+            XSegDev& d = dev[s];
+            d.dst = segs[s].dst;
+            d.src = segs[s].src;
+            long long cells = 1;
+            for (int k = 0; k < 3; ++k) {
+                d.lo[k] = segs[s].lo[k];
+                d.hi[k] = segs[s].hi[k];
+                d.shift[k] = segs[s].shift[k];
+                cells *= segs[s].hi[k] - segs[s].lo[k];
+            }
+            d.first = total;
+            total += cells;
+        }
+        PK_CUDA(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->d_xseg);
+        h->d_xseg = nullptr;
+        if (!dev.empty()) {
+            PK_CUDA(h, cudaMalloc(&h->d_xseg, sizeof(XSegDev) * dev.size()));
+            PK_CUDA(h, cudaMemcpy(h->d_xseg, dev.data(), sizeof(XSegDev) * dev.size(), cudaMemcpyHostToDevice));
+        }
+        h->nxseg = (int)dev.size();
+        h->xtotal = total;
+        h->x_dirty = false;
+        h->x_cur = -1;
+    }
+    if (h->x_cur != h->cur) {
+        std::vector<XPtr> ptr(nb);
+        for (int i = 0; i < nb; ++i) {
+            const Block& b = h->blocks[i];
+            ptr[i].u = b.buf[h->cur];
+            ptr[i].plane = b.plane;
+            for (int d = 0; d < 3; ++d) ptr[i].ext[d] = b.ext[d];
+        }
+        PK_CUDA(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->d_xptr);
+        h->d_xptr = nullptr;
+        PK_CUDA(h, cudaMalloc(&h->d_xptr, sizeof(XPtr) * (nb > 0 ? nb : 1)));
+        PK_CUDA(h, cudaMemcpy(h->d_xptr, ptr.data(), sizeof(XPtr) * nb, cudaMemcpyHostToDevice));
+        h->x_cur = h->cur;
+    }
+    if (h->xtotal == 0) return PK_OK;
+    k_exchange<<<grid1d(h->xtotal, 256), 256, 0, h->stream>>>(h->d_xseg, h->nxseg, h->xtotal, h->d_xptr, h->nplanes);
+    PK_CUDA(h, cudaGetLastError());
+    h->launches += 1;
+    return PK_OK;
+}
+
 bool fused_ok(pk_ctx* h)
 {
-    if (h->cfg.integration_order != 2) return false;
+    if (h->cfg.integration_order != 2 || h->connected) return false;
     for (auto& b : h->blocks)
         for (int d = 0; d < 3; ++d)
             if (b.n[d] > 1 && (b.bnd[d][0] != PK_BND_PER || b.bnd[d][1] != PK_BND_PER)) return false;
@@ -267,6 +338,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
         }
         for (auto& b : h->blocks)
             if (int rc = fill_guards_block(h, b)) return rc;
+        if (int rc = exchange_guards(h)) return rc;
     }
     if (h->cfg.magnetic && apply_fac) return glm_scale(h, fac);
     return PK_OK;
@@ -448,6 +520,8 @@ int pk_destroy(pk_handle h)
     cudaFree(h->lam);
     cudaFree(h->lam_tmp);
     cudaFree(h->lam_m1);
+    cudaFree(h->d_xseg);
+    cudaFree(h->d_xptr);
     cudaFree(h->d_desc[0]);
     cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
@@ -615,6 +689,33 @@ int pk_fill_guards(pk_handle h)
     if (!h) return PK_E_ARG;
     for (auto& b : h->blocks)
         if (int rc = fill_guards_block(h, b)) return rc;
+    return exchange_guards(h);
+}
+
+int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3])
+{
+    if (!h || !ncells || !periodic) return PK_E_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (ncells[d] < 1) return fail(h, PK_E_ARG, "domain extents must be positive");
+    for (int d = 0; d < 3; ++d) {
+        h->dom[d] = ncells[d];
+        h->dom_periodic[d] = periodic[d] ? 1 : 0;
+    }
+    h->connected = true;
+    h->x_dirty = true;
+    invalidate_graph(h);
+    return PK_OK;
+}
+
+int pk_block_place(pk_handle h, int32_t id, const int64_t off[3])
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!off) return fail(h, PK_E_ARG, "null offset");
+    for (int d = 0; d < 3; ++d) b->off[d] = off[d];
+    b->placed = true;
+    h->x_dirty = true;
+    invalidate_graph(h);
     return PK_OK;
 }
 

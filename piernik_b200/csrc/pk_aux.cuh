@@ -201,6 +201,46 @@ static __global__ void k_fill_guards(BoxGeom b, double* __restrict__ u, GuardArg
     }
 }
 
+// Same-level guard exchange between blocks (cg_list_bnd.F90:286-314): one
+// thread per guard cell of all segments; a segment is found by binary search
+// over the running cell counts.  Sources are interior cells, targets guard
+// cells, so the copies never race.
+struct XSegDev {
+    int dst, src;
+    int lo[3], hi[3], shift[3];
+    long long first;            // cells of all earlier segments
+};
+
+struct XPtr {
+    double* u;
+    long long plane;
+    int ext[3];
+};
+
+static __global__ void k_exchange(const XSegDev* __restrict__ segs, int nseg, long long total,
+                                  const XPtr* __restrict__ blk, int nplanes)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].first <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const XSegDev s = segs[lo];
+        long long r = c - s.first;
+        const int nx = s.hi[0] - s.lo[0], ny = s.hi[1] - s.lo[1];
+        const int i = s.lo[0] + (int)(r % nx);
+        r /= nx;
+        const int j = s.lo[1] + (int)(r % ny);
+        const int k = s.lo[2] + (int)(r / ny);
+        const XPtr d = blk[s.dst], q = blk[s.src];
+        const long long di = ((long long)k * d.ext[1] + j) * d.ext[0] + i;
+        const long long si = ((long long)(k + s.shift[2]) * q.ext[1] + (j + s.shift[1])) * q.ext[0] + (i + s.shift[0]);
+        for (int v = 0; v < nplanes; ++v) d.u[(long long)v * d.plane + di] = q.u[(long long)v * q.plane + si];
+    }
+}
+
 // zero every guard cell of all planes (adjoint states carry no guard values)
 static __global__ void k_zero_guards(BoxGeom b, double* __restrict__ u, int nplanes)
 {

@@ -1,0 +1,38 @@
+// pk_exchange.h -- guard-cell exchange between blocks of one refinement level
+// on one device (cg_list_bnd.F90:251-324, internal_boundaries_local): the plan
+// of box-to-box copies, built on the host.  Pure C++ so that the tests can
+// build it without CUDA.
+#pragma once
+#include <string>
+#include <vector>
+
+namespace pk {
+
+// One block as the exchange sees it: interior extent n, guard width g (0 in
+// directions without extent), offset of its first interior cell on the
+// level's global cell grid.
+struct XBlock {
+    int n[3];
+    int g[3];
+    long long off[3];
+};
+
+// One box of guard cells of block dst filled from the interior of block src:
+// dst cells lo..hi-1 (in dst's guard-inclusive coordinates) take src cell
+// (i + shift[0], j + shift[1], k + shift[2]) (in src's guard-inclusive
+// coordinates).
+struct XSeg {
+    int dst, src;
+    int lo[3], hi[3];
+    int shift[3];
+};
+
+// Every guard cell of every block whose position (wrapped into the domain
+// along periodic directions) lies in the interior of some block gets one
+// segment cell.  dom: cells of the level along each direction; periodic: wrap
+// flags.  Fails (returns false, err set) when two interiors overlap or a
+// block leaves a non-periodic domain.
+bool build_exchange(const std::vector<XBlock>& blocks, const long long dom[3], const int periodic[3],
+                    std::vector<XSeg>& segs, std::string& err);
+
+}  // namespace pk

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/piernik_b200.h"
+#include "pk_aux.cuh"
 #include "pk_kernels.cuh"
 
 namespace pk {
@@ -30,6 +31,8 @@ struct Block {
     double* uh = nullptr;                  // stage path: state at the start of the step (cg%w(uh))
     double* stage = nullptr;               // host-layout conversion buffer
     bool guards_stale = false;             // fused sweeps read periodic images and never store guards
+    long long off[3] = {0, 0, 0};          // first interior cell on the level's cell grid (connected domains)
+    bool placed = false;
 };
 
 struct pk_dir_tile { int P, L, V; };
@@ -79,6 +82,16 @@ struct pk_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int use_graph = 0;
     long long graph_kernels = 0;        // kernel nodes of the captured step
+    // same-level domain of connected blocks (pk_set_domain / pk_block_place)
+    bool connected = false;
+    long long dom[3] = {1, 1, 1};
+    int dom_periodic[3] = {0, 0, 0};
+    bool x_dirty = true;                // the exchange plan must be rebuilt
+    int x_cur = -1;                     // parity the pointer table was built for
+    pk::XSegDev* d_xseg = nullptr;
+    pk::XPtr* d_xptr = nullptr;
+    int nxseg = 0;
+    long long xtotal = 0;
     // differentiable path (single block, fused sweeps)
     int adjL[3] = {0, 0, 0};            // owned cells per pencil of the adjoint tiles, per direction (0: default)
     int adjV[3] = {-1, -1, -1};         // launch-bound variant of the adjoint kernels per direction (-1: default)

@@ -225,6 +225,18 @@ class Simulation:
         """Replay each step's sweeps as a captured CUDA graph."""
         self._chk(self.lib.pk_use_graph(self.h, int(enable)), "pk_use_graph")
 
+    # -- connected blocks of one level --------------------------------------
+    def set_domain(self, ncells, periodic=(True, True, True)) -> None:
+        """Declare the level's cell grid; placed blocks then exchange guards."""
+        n = (C.c_int64 * 3)(*[int(x) for x in ncells])
+        p = (C.c_int32 * 3)(*[int(bool(x)) for x in periodic])
+        self._chk(self.lib.pk_set_domain(self.h, n, p), "pk_set_domain")
+
+    def place_block(self, block: int, off) -> None:
+        """Put the block's first interior cell at ``off`` on the level's grid."""
+        o = (C.c_int64 * 3)(*[int(x) for x in off])
+        self._chk(self.lib.pk_block_place(self.h, block, o), "pk_block_place")
+
     # -- differentiable path (one periodic block, one fluid, RK2) -------------
     @property
     def nplanes(self) -> int:
