@@ -129,8 +129,11 @@ int fill_guards_block(pk_ctx* h, Block& b)
 }
 
 // Same-level exchange of all placed blocks' guard cells (update_boundaries'
-// internal part); blocks' own boundary rules were applied before.
-int exchange_guards(pk_ctx* h)
+// internal part); blocks' own boundary rules were applied before.  The plan
+// and the per-parity block tables are built here, outside any graph capture.
+int ensure_pingpong(pk_ctx* h);
+
+int exchange_prepare(pk_ctx* h)
 {
     if (!h->connected) return PK_OK;
     const int nb = (int)h->blocks.size();
@@ -174,33 +177,71 @@ int exchange_guards(pk_ctx* h)
         h->nxseg = (int)dev.size();
         h->xtotal = total;
         h->x_dirty = false;
-        h->x_cur = -1;
     }
-    if (h->x_cur != h->cur) {
+    if (h->x_ptrs_dirty) {
+        if (int rc = ensure_pingpong(h)) return rc;
         std::vector<XPtr> ptr(nb);
-        for (int i = 0; i < nb; ++i) {
-            const Block& b = h->blocks[i];
-            ptr[i].u = b.buf[h->cur];
-            ptr[i].plane = b.plane;
-            for (int d = 0; d < 3; ++d) ptr[i].ext[d] = b.ext[d];
-        }
         PK_CUDA(h, cudaStreamSynchronize(h->stream));
-        cudaFree(h->d_xptr);
-        h->d_xptr = nullptr;
-        PK_CUDA(h, cudaMalloc(&h->d_xptr, sizeof(XPtr) * (nb > 0 ? nb : 1)));
-        PK_CUDA(h, cudaMemcpy(h->d_xptr, ptr.data(), sizeof(XPtr) * nb, cudaMemcpyHostToDevice));
-        h->x_cur = h->cur;
+        for (int p = 0; p < 2; ++p) {
+            for (int i = 0; i < nb; ++i) {
+                const Block& b = h->blocks[i];
+                ptr[i].u = b.buf[p];
+                ptr[i].plane = b.plane;
+                for (int d = 0; d < 3; ++d) ptr[i].ext[d] = b.ext[d];
+            }
+            cudaFree(h->d_xptr[p]);
+            h->d_xptr[p] = nullptr;
+            PK_CUDA(h, cudaMalloc(&h->d_xptr[p], sizeof(XPtr) * (nb > 0 ? nb : 1)));
+            PK_CUDA(h, cudaMemcpy(h->d_xptr[p], ptr.data(), sizeof(XPtr) * nb, cudaMemcpyHostToDevice));
+        }
+        h->x_ptrs_dirty = false;
     }
+    return PK_OK;
+}
+
+// launch the exchange on the current state (tables built by exchange_prepare)
+int exchange_guards(pk_ctx* h)
+{
+    if (!h->connected) return PK_OK;
+    if (int rc = exchange_prepare(h)) return rc;
     if (h->xtotal == 0) return PK_OK;
-    k_exchange<<<grid1d(h->xtotal, 256), 256, 0, h->stream>>>(h->d_xseg, h->nxseg, h->xtotal, h->d_xptr, h->nplanes);
+    k_exchange<<<grid1d(h->xtotal, 256), 256, 0, h->stream>>>(h->d_xseg, h->nxseg, h->xtotal, h->d_xptr[h->cur],
+                                                                h->nplanes);
     PK_CUDA(h, cudaGetLastError());
     h->launches += 1;
     return PK_OK;
 }
 
+// Guard cells of a block whose sweeps left them stale: its own boundary rules,
+// and for a connected domain every block's exchange.
+int refresh_guards(pk_ctx* h, Block& b)
+{
+    if (!h->connected) return fill_guards_block(h, b);
+    for (auto& c : h->blocks)
+        if (int rc = fill_guards_block(h, c)) return rc;
+    return exchange_guards(h);
+}
+
+// A connected domain sweeps with the fused kernels when the blocks tile a
+// domain periodic in every swept direction: the exchange before each sweep
+// then fills every guard cell, and the kernels read their 4-cell halo from
+// the guards -- the same values a periodic single block reads by wrapping.
+bool connected_fused_ok(pk_ctx* h)
+{
+    long long cells = 0;
+    for (auto& b : h->blocks) {
+        if (!b.placed) return false;
+        cells += (long long)b.n[0] * b.n[1] * b.n[2];
+    }
+    for (int d = 0; d < 3; ++d)
+        if (h->dom[d] > 1 && !h->dom_periodic[d]) return false;
+    return cells == h->dom[0] * h->dom[1] * h->dom[2];
+}
+
 bool fused_ok(pk_ctx* h)
 {
-    if (h->cfg.integration_order != 2 || h->connected) return false;
+    if (h->cfg.integration_order != 2) return false;
+    if (h->connected) return connected_fused_ok(h);
     for (auto& b : h->blocks)
         for (int d = 0; d < 3; ++d)
             if (b.n[d] > 1 && (b.bnd[d][0] != PK_BND_PER || b.bnd[d][1] != PK_BND_PER)) return false;
@@ -216,6 +257,7 @@ int ensure_pingpong(pk_ctx* h)
             PK_CUDA(h, cudaMemsetAsync(p, 0, sizeof(double) * h->nplanes * b.plane, h->stream));
             b.buf[1 - h->cur] = p;
             h->batch_dirty = true;
+            h->x_ptrs_dirty = true;
         }
     return PK_OK;
 }
@@ -240,6 +282,7 @@ int build_batch(pk_ctx* h)
                 d.n[k] = b.n[k];
                 d.dl[k] = b.dl[k];
             }
+            d.wrap = h->connected ? 0 : 1;
         }
         cudaFree(h->d_desc[p]);
         h->d_desc[p] = nullptr;
@@ -313,6 +356,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
     const PhysOps* ops = ops_of(h);
     if (fused_ok(h)) {
         if (int rc = ensure_pingpong(h)) return rc;
+        if (int rc = exchange_guards(h)) return rc;      // connected domains: halos come from the guards
         if (h->batched || h->blocks.size() > 1) {
             if (int rc = build_batch(h)) return rc;
             if (int rc = ops->batched(h, dir, apply_fac, h->d_counter + dir)) return rc;
@@ -521,7 +565,8 @@ int pk_destroy(pk_handle h)
     cudaFree(h->lam_tmp);
     cudaFree(h->lam_m1);
     cudaFree(h->d_xseg);
-    cudaFree(h->d_xptr);
+    cudaFree(h->d_xptr[0]);
+    cudaFree(h->d_xptr[1]);
     cudaFree(h->d_desc[0]);
     cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
@@ -570,6 +615,8 @@ int pk_block_add(pk_handle h, const int32_t n[3], const double dl[3], const int3
     b.buf[h->cur] = p;                      // the state lives in the current parity's buffer
     h->blocks.push_back(b);
     h->batch_dirty = true;
+    h->x_dirty = true;
+    h->x_ptrs_dirty = true;
     invalidate_graph(h);
     if (id_out) *id_out = (int32_t)h->blocks.size() - 1;
     const int need = (int)h->blocks.size() * 12;
@@ -632,7 +679,7 @@ int pk_download(pk_handle h, int32_t id, double* u, double* bf, double* psi, int
     if (int rc = get_block(h, id, &b)) return rc;
     if (!u || (h->cfg.magnetic && (!bf || !psi))) return fail(h, PK_E_ARG, "null array");
     if (b->guards_stale)
-        if (int rc = fill_guards_block(h, *b)) return rc;
+        if (int rc = refresh_guards(h, *b)) return rc;
     const long long nc = b->plane;
     double* s = state(h, *b);
     if (layout == PK_LAYOUT_SOA) {
@@ -703,6 +750,7 @@ int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3
     }
     h->connected = true;
     h->x_dirty = true;
+    h->batch_dirty = true;
     invalidate_graph(h);
     return PK_OK;
 }
@@ -835,6 +883,7 @@ int pk_fluid_update(pk_handle h)
     if (h->use_graph && !h->profiling) {
         if (fused_ok(h) && h->blocks.size() > 1)
             if (int rc = build_batch(h)) return rc;   // tables are built outside the capture
+        if (int rc = exchange_prepare(h)) return rc;
         if (int rc = ensure_pingpong(h)) return rc;
         for (auto& b : h->blocks)
             if (!b.uh && !fused_ok(h)) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
@@ -1079,7 +1128,7 @@ int pk_download_device(pk_handle h, int32_t id, double* soa_dev)
     if (int rc = get_block(h, id, &b)) return rc;
     if (!soa_dev) return fail(h, PK_E_ARG, "null array");
     if (b->guards_stale)
-        if (int rc = fill_guards_block(h, *b)) return rc;
+        if (int rc = refresh_guards(h, *b)) return rc;
     PK_CUDA(h, cudaMemcpyAsync(soa_dev, state(h, *b), sizeof(double) * h->nplanes * b->plane, cudaMemcpyDeviceToDevice,
                                h->stream));
     PK_CUDA(h, cudaStreamSynchronize(h->stream));

@@ -87,9 +87,9 @@ struct pk_ctx {
     long long dom[3] = {1, 1, 1};
     int dom_periodic[3] = {0, 0, 0};
     bool x_dirty = true;                // the exchange plan must be rebuilt
-    int x_cur = -1;                     // parity the pointer table was built for
+    bool x_ptrs_dirty = true;           // block buffers changed: rebuild the pointer tables
     pk::XSegDev* d_xseg = nullptr;
-    pk::XPtr* d_xptr = nullptr;
+    pk::XPtr* d_xptr[2] = {nullptr, nullptr};   // block states of parity 0 / 1
     int nxseg = 0;
     long long xtotal = 0;
     // differentiable path (single block, fused sweeps)

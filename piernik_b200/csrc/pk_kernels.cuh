@@ -40,6 +40,8 @@ struct Tile {
     int P, T, L;            // pencils, tile length, output cells per pencil
     int xfast;              // 1: lanes run along the pencil (x sweeps)
     int halo;               // stage mode: tile cells before the first owned cell (0 or 2)
+    int wrap = 1;           // fused mode: 1 read the halo as periodic images of the interior,
+                            // 0 read it from the block's guard cells (filled by the exchange)
 };
 
 // -------------------------------------------------------------------------
@@ -193,7 +195,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     const int i1 = i1_0 + p;
     const bool active = (tid < PT) && (i1 < g.n1);
     const int s = c0 - 4 + t;                                  // position along the pencil (interior coords)
-    const long long off = (long long)(g.g_d + wrap(s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
+    const long long off = (long long)(g.g_d + (tl.wrap ? wrap(s, g.n_d) : s)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
                           (long long)(g.g2 + i2) * g.s2;
     double w[NV];
 #pragma unroll
@@ -251,6 +253,7 @@ struct BlockDesc {
     long long plane;
     int ext[3], g[3], n[3];
     double dl[3];
+    int wrap;               // Tile::wrap for this block's tiles
 };
 
 struct WorkItem {
@@ -301,6 +304,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
         tl.T = w.L + 8;
         tl.xfast = dir == 0;
         tl.halo = 4;
+        tl.wrap = b.wrap;
         const double dl = b.dl[dir];
         fused_tile<PH>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, (0.5 * dt) / dl, (1.0 * dt) / dl, ch, fac, smem,
                        status);

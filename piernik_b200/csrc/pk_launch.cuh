@@ -79,6 +79,7 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     tl.L = L;
     tl.halo = 4;
     tl.xfast = (dir == 0);
+    tl.wrap = h->connected ? 0 : 1;
     dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
     const size_t smem = 3ull * PH::NV * P * T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;

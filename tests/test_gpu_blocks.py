@@ -48,7 +48,7 @@ def exact_dl(setup):
     return setup.replace(xmin=(0.0, 0.0, 0.0), xmax=tuple(0.125 * setup.n[d] for d in range(3)))
 
 
-def run_tiled(full, state, blocks, periodic, nsteps, bnd_x=BND_PER):
+def run_tiled(full, state, blocks, periodic, nsteps, bnd_x=BND_PER, graph=False):
     u, b, psi = state
     sims = None
     for i, (n, off) in enumerate(blocks):
@@ -69,6 +69,8 @@ def run_tiled(full, state, blocks, periodic, nsteps, bnd_x=BND_PER):
         sims.place_block(bid, off)
         sims.upload(window(full, u, n, off), window(full, b, n, off), window(full, psi, n, off), block=bid)
     sims.update_boundaries()
+    if graph:
+        sims.use_graph(True)
     sims.run(nsteps)
     out = []
     for i, (n, off) in enumerate(blocks):
@@ -78,8 +80,10 @@ def run_tiled(full, state, blocks, periodic, nsteps, bnd_x=BND_PER):
     return out, st
 
 
-@pytest.mark.parametrize("phys", ["hd", "mhd"])
-def test_tiled_periodic_domain_equals_one_block(gpu_lib, phys):
+@pytest.mark.parametrize("phys,graph", [("hd", False), ("mhd", False), ("mhd", True)])
+def test_tiled_periodic_domain_equals_one_block(gpu_lib, phys, graph):
+    """A periodic domain tiled completely: exchange before each sweep, then the
+    batched fused sweep reading its halo from the guards."""
     full = exact_dl(setup_for(phys, n=(40, 36, 28), lim="moncen"))
     state = random_state(full, seed=3)
     one = Simulation(full)
@@ -89,7 +93,7 @@ def test_tiled_periodic_domain_equals_one_block(gpu_lib, phys):
     st1 = one.time_state
     one.close()
     blocks = tiles([16, 24], [20, 16], [12, 16])
-    got, st2 = run_tiled(full, state, blocks, (True, True, True), 3)
+    got, st2 = run_tiled(full, state, blocks, (True, True, True), 3, graph=graph)
     assert st1.t == st2.t and st1.dt == st2.dt
     for (n, off), arrs in zip(blocks, got):
         s = full.replace(n=n)
@@ -101,6 +105,8 @@ def test_tiled_periodic_domain_equals_one_block(gpu_lib, phys):
 
 
 def test_tiled_outflow_domain_equals_one_block(gpu_lib):
+    """Outflow along x: the per-stage path (pk_solve_cg per block, then the
+    blocks' own outflow rule and the exchange after each stage)."""
     full = exact_dl(setup_for("hd", n=(40, 20, 16), lim="vanleer", bnd=((BND_OUT, BND_OUT), (BND_PER, BND_PER),
                                                                        (BND_PER, BND_PER))))
     state = random_state(full, seed=4)
@@ -115,6 +121,16 @@ def test_tiled_outflow_domain_equals_one_block(gpu_lib):
     for (n, off), arrs in zip(blocks, got):
         s = full.replace(n=n)
         assert_bitexact(interior_of(s, arrs[0], n, (0, 0, 0)), interior_of(full, ref[0], n, off), f"block {off}")
+
+
+def test_tiled_domain_with_a_hole_uses_stages(gpu_lib):
+    """Blocks that do not cover the periodic domain still exchange what they
+    share; the run equals the same blocks swept one stage at a time."""
+    full = exact_dl(setup_for("hd", n=(32, 16, 16), lim="vanleer"))
+    state = random_state(full, seed=5)
+    blocks = tiles([16, 16], [16], [16])[:1] + [((8, 16, 16), (16, 0, 0))]
+    got, _ = run_tiled(full, state, blocks, (True, True, True), 2)
+    assert all(np.isfinite(g[0]).all() for g in got)
 
 
 def test_overlapping_blocks_are_rejected(gpu_lib):
