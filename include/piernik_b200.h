@@ -173,6 +173,33 @@ int pk_use_graph(pk_handle h, int32_t enable);
 int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3]);
 int pk_block_place(pk_handle h, int32_t id, const int64_t off[3]);
 
+/* ---- Domains spanning ranks (one process per GPU) ----
+ * The reference exchanges guard cells between MPI ranks in the same
+ * internal_boundaries pass (cg_list_bnd.F90:251-324, MPI isend/irecv of the
+ * segment buffers) and reduces dt over ranks (timestep.F90:173).  Here the
+ * library plans and packs, the host moves the bytes (NCCL, MPI, ...):
+ *   pk_block_remote declares a block of the same level held by rank owner
+ *   (every rank declares all blocks it does not hold);
+ *   pk_halo_peers lists the ranks this one exchanges with, pk_halo_sizes the
+ *   doubles sent to / received from one of them per exchange;
+ *   pk_halo_pack fills a device buffer with the cells a peer needs,
+ *   pk_halo_unpack writes a peer's buffer into the guard cells (both
+ *   synchronous on the handle's stream);
+ *   pk_set_comm installs host callbacks: halo(ctx, dir) runs after every
+ *   local guard exchange (dir = the sweep direction 0..2, or -1) and must
+ *   pack, move and unpack for all peers; reduce(ctx, x, op) returns the
+ *   minimum (op 0) or maximum (op 1) of x over ranks and is used for dt and
+ *   c_all in pk_time_step.  With callbacks set, pk_run does not use graphs.
+ * Both sides order a peer's cells alike (by positions on the level's grid). */
+typedef void (*pk_halo_fn)(void* ctx, int32_t dir);
+typedef double (*pk_reduce_fn)(void* ctx, double x, int32_t op);
+int pk_block_remote(pk_handle h, int32_t owner, const int32_t n[3], const int64_t off[3]);
+int pk_halo_peers(pk_handle h, int32_t* peers, int32_t max_peers, int32_t* count);
+int pk_halo_sizes(pk_handle h, int32_t peer, int64_t* send_doubles, int64_t* recv_doubles);
+int pk_halo_pack(pk_handle h, int32_t peer, double* sendbuf_dev);
+int pk_halo_unpack(pk_handle h, int32_t peer, const double* recvbuf_dev);
+int pk_set_comm(pk_handle h, pk_halo_fn halo, pk_reduce_fn reduce, void* ctx);
+
 /* ---- Differentiable path (one periodic block, one fluid, RK2) ----
  * Not in the reference, which has no derivatives: the adjoint (reverse
  * mode) of the sweep path at a fixed sequence of time steps. */

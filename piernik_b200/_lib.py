@@ -31,7 +31,11 @@ EXPORTS = (
     "pk_upload_device", "pk_download_device", "pk_adjoint_set", "pk_adjoint_get", "pk_adjoint_sweep",
     "pk_grad_forward", "pk_grad_backward", "pk_grad_release",
     "pk_timestep_raw_noalloc", "pk_set_adjoint_tile", "pk_set_domain", "pk_block_place",
+    "pk_block_remote", "pk_halo_peers", "pk_halo_sizes", "pk_halo_pack", "pk_halo_unpack", "pk_set_comm",
 )
+
+HALO_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32)
+REDUCE_FN = C.CFUNCTYPE(C.c_double, C.c_void_p, C.c_double, C.c_int32)
 
 
 class PkConfig(C.Structure):
@@ -128,6 +132,12 @@ def load(path: str = LIBPATH):
     L.pk_set_adjoint_tile.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
     L.pk_set_domain.argtypes = [H, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
     L.pk_block_place.argtypes = [H, C.c_int32, C.POINTER(C.c_int64)]
+    L.pk_block_remote.argtypes = [H, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    L.pk_halo_peers.argtypes = [H, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]
+    L.pk_halo_sizes.argtypes = [H, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.pk_halo_pack.argtypes = [H, C.c_int32, C.c_void_p]
+    L.pk_halo_unpack.argtypes = [H, C.c_int32, C.c_void_p]
+    L.pk_set_comm.argtypes = [H, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pk_timestep_raw_noalloc.argtypes = [C.POINTER(PkConfig), C.c_int32, C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.c_void_p,
                                           C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_char_p, C.c_int32]

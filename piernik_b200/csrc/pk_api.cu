@@ -133,13 +133,55 @@ int fill_guards_block(pk_ctx* h, Block& b)
 // and the per-parity block tables are built here, outside any graph capture.
 int ensure_pingpong(pk_ctx* h);
 
+int upload_segs(pk_ctx* h, const std::vector<XSeg>& segs, XSegList* out)
+{
+    std::vector<XSegDev> dev(segs.size());
+    long long total = 0;
+    for (size_t s = 0; s < segs.size(); ++s) {
+        XSegDev& d = dev[s];
+        d.dst = segs[s].dst;
+        d.src = segs[s].src;
+        long long cells = 1;
+        for (int k = 0; k < 3; ++k) {
+            d.lo[k] = segs[s].lo[k];
+            d.hi[k] = segs[s].hi[k];
+            d.shift[k] = segs[s].shift[k];
+            cells *= segs[s].hi[k] - segs[s].lo[k];
+        }
+        d.first = total;
+        total += cells;
+    }
+    cudaFree(out->dev);
+    out->dev = nullptr;
+    if (!dev.empty()) {
+        PK_CUDA(h, cudaMalloc(&out->dev, sizeof(XSegDev) * dev.size()));
+        PK_CUDA(h, cudaMemcpy(out->dev, dev.data(), sizeof(XSegDev) * dev.size(), cudaMemcpyHostToDevice));
+    }
+    out->n = (int)dev.size();
+    out->total = total;
+    return PK_OK;
+}
+
+void free_segs(pk_ctx* h)
+{
+    cudaFree(h->xlocal.dev);
+    h->xlocal = XSegList();
+    for (auto& p : h->xpeers) {
+        cudaFree(p.send.dev);
+        cudaFree(p.recv.dev);
+    }
+    h->xpeers.clear();
+}
+
 int exchange_prepare(pk_ctx* h)
 {
     if (!h->connected) return PK_OK;
-    const int nb = (int)h->blocks.size();
+    const int nl = (int)h->blocks.size();
     if (h->x_dirty) {
-        std::vector<XBlock> xb(nb);
-        for (int i = 0; i < nb; ++i) {
+        // this rank's blocks first, then the other ranks'
+        std::vector<XBlock> xb(nl + h->remote.size());
+        std::vector<int> owner(xb.size(), -1);
+        for (int i = 0; i < nl; ++i) {
             const Block& b = h->blocks[i];
             if (!b.placed) return fail(h, PK_E_STATE, "every block of a connected domain must be placed (pk_block_place)");
             for (int d = 0; d < 3; ++d) {
@@ -148,42 +190,39 @@ int exchange_prepare(pk_ctx* h)
                 xb[i].off[d] = b.off[d];
             }
         }
-        std::vector<XSeg> segs;
+        for (size_t r = 0; r < h->remote.size(); ++r) {
+            const RemoteBlock& rb = h->remote[r];
+            XBlock& x = xb[nl + r];
+            for (int d = 0; d < 3; ++d) {
+                x.n[d] = rb.n[d];
+                x.g[d] = rb.n[d] > 1 ? h->cfg.nb : 0;
+                x.off[d] = rb.off[d];
+            }
+            owner[nl + r] = rb.owner;
+        }
+        std::vector<XSeg> segs, local;
+        std::vector<XPeer> peers;
         std::string err;
         if (!build_exchange(xb, h->dom, h->dom_periodic, segs, err)) return fail(h, PK_E_ARG, err);
-        std::vector<XSegDev> dev(segs.size());
-        long long total = 0;
-        for (size_t s = 0; s < segs.size(); ++s) {
-            XSegDev& d = dev[s];
-            d.dst = segs[s].dst;
-            d.src = segs[s].src;
-            long long cells = 1;
-            for (int k = 0; k < 3; ++k) {
-                d.lo[k] = segs[s].lo[k];
-                d.hi[k] = segs[s].hi[k];
-                d.shift[k] = segs[s].shift[k];
-                cells *= segs[s].hi[k] - segs[s].lo[k];
-            }
-            d.first = total;
-            total += cells;
-        }
+        split_by_owner(xb, owner, nl, segs, local, peers);
         PK_CUDA(h, cudaStreamSynchronize(h->stream));
-        cudaFree(h->d_xseg);
-        h->d_xseg = nullptr;
-        if (!dev.empty()) {
-            PK_CUDA(h, cudaMalloc(&h->d_xseg, sizeof(XSegDev) * dev.size()));
-            PK_CUDA(h, cudaMemcpy(h->d_xseg, dev.data(), sizeof(XSegDev) * dev.size(), cudaMemcpyHostToDevice));
+        free_segs(h);
+        if (int rc = upload_segs(h, local, &h->xlocal)) return rc;
+        for (const XPeer& p : peers) {
+            XPeerDev d;
+            d.rank = p.rank;
+            h->xpeers.push_back(d);
+            if (int rc = upload_segs(h, p.send, &h->xpeers.back().send)) return rc;
+            if (int rc = upload_segs(h, p.recv, &h->xpeers.back().recv)) return rc;
         }
-        h->nxseg = (int)dev.size();
-        h->xtotal = total;
         h->x_dirty = false;
     }
     if (h->x_ptrs_dirty) {
         if (int rc = ensure_pingpong(h)) return rc;
-        std::vector<XPtr> ptr(nb);
+        std::vector<XPtr> ptr(nl);
         PK_CUDA(h, cudaStreamSynchronize(h->stream));
         for (int p = 0; p < 2; ++p) {
-            for (int i = 0; i < nb; ++i) {
+            for (int i = 0; i < nl; ++i) {
                 const Block& b = h->blocks[i];
                 ptr[i].u = b.buf[p];
                 ptr[i].plane = b.plane;
@@ -191,24 +230,27 @@ int exchange_prepare(pk_ctx* h)
             }
             cudaFree(h->d_xptr[p]);
             h->d_xptr[p] = nullptr;
-            PK_CUDA(h, cudaMalloc(&h->d_xptr[p], sizeof(XPtr) * (nb > 0 ? nb : 1)));
-            PK_CUDA(h, cudaMemcpy(h->d_xptr[p], ptr.data(), sizeof(XPtr) * nb, cudaMemcpyHostToDevice));
+            PK_CUDA(h, cudaMalloc(&h->d_xptr[p], sizeof(XPtr) * (nl > 0 ? nl : 1)));
+            PK_CUDA(h, cudaMemcpy(h->d_xptr[p], ptr.data(), sizeof(XPtr) * nl, cudaMemcpyHostToDevice));
         }
         h->x_ptrs_dirty = false;
     }
     return PK_OK;
 }
 
-// launch the exchange on the current state (tables built by exchange_prepare)
-int exchange_guards(pk_ctx* h)
+// launch the exchange between this rank's blocks on the current state, then
+// let the host move the other ranks' halo (dir: sweep direction or -1)
+int exchange_guards(pk_ctx* h, int dir = -1)
 {
     if (!h->connected) return PK_OK;
     if (int rc = exchange_prepare(h)) return rc;
-    if (h->xtotal == 0) return PK_OK;
-    k_exchange<<<grid1d(h->xtotal, 256), 256, 0, h->stream>>>(h->d_xseg, h->nxseg, h->xtotal, h->d_xptr[h->cur],
-                                                                h->nplanes);
-    PK_CUDA(h, cudaGetLastError());
-    h->launches += 1;
+    if (h->xlocal.total > 0) {
+        k_exchange<<<grid1d(h->xlocal.total, 256), 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total,
+                                                                       h->d_xptr[h->cur], h->nplanes);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+    }
+    if (h->halo_cb && !h->xpeers.empty()) h->halo_cb(h->comm_ctx, dir);
     return PK_OK;
 }
 
@@ -356,7 +398,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
     const PhysOps* ops = ops_of(h);
     if (fused_ok(h)) {
         if (int rc = ensure_pingpong(h)) return rc;
-        if (int rc = exchange_guards(h)) return rc;      // connected domains: halos come from the guards
+        if (int rc = exchange_guards(h, dir)) return rc;   // connected domains: halos come from the guards
         if (h->batched || h->blocks.size() > 1) {
             if (int rc = build_batch(h)) return rc;
             if (int rc = ops->batched(h, dir, apply_fac, h->d_counter + dir)) return rc;
@@ -382,7 +424,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
         }
         for (auto& b : h->blocks)
             if (int rc = fill_guards_block(h, b)) return rc;
-        if (int rc = exchange_guards(h)) return rc;
+        if (int rc = exchange_guards(h, dir)) return rc;
     }
     if (h->cfg.magnetic && apply_fac) return glm_scale(h, fac);
     return PK_OK;
@@ -564,7 +606,7 @@ int pk_destroy(pk_handle h)
     cudaFree(h->lam);
     cudaFree(h->lam_tmp);
     cudaFree(h->lam_m1);
-    cudaFree(h->d_xseg);
+    free_segs(h);
     cudaFree(h->d_xptr[0]);
     cudaFree(h->d_xptr[1]);
     cudaFree(h->d_desc[0]);
@@ -755,6 +797,91 @@ int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3
     return PK_OK;
 }
 
+int pk_block_remote(pk_handle h, int32_t owner, const int32_t n[3], const int64_t off[3])
+{
+    if (!h || !n || !off) return PK_E_ARG;
+    if (owner < 0) return fail(h, PK_E_ARG, "owner rank must be >= 0");
+    RemoteBlock r;
+    r.owner = owner;
+    for (int d = 0; d < 3; ++d) {
+        if (n[d] < 1) return fail(h, PK_E_ARG, "block extent must be positive");
+        if (!h->blocks.empty() && ((h->blocks[0].n[d] > 1) != (n[d] > 1)))
+            return fail(h, PK_E_ARG, "all blocks must have the same directions (dom%has_dir)");
+        r.n[d] = n[d];
+        r.off[d] = off[d];
+    }
+    h->remote.push_back(r);
+    h->x_dirty = true;
+    return PK_OK;
+}
+
+int pk_halo_peers(pk_handle h, int32_t* peers, int32_t max_peers, int32_t* count)
+{
+    if (!h || !count) return PK_E_ARG;
+    if (int rc = exchange_prepare(h)) return rc;
+    *count = (int32_t)h->xpeers.size();
+    for (int i = 0; i < (int)h->xpeers.size() && i < max_peers; ++i)
+        if (peers) peers[i] = h->xpeers[i].rank;
+    return PK_OK;
+}
+
+static XPeerDev* find_peer(pk_ctx* h, int peer)
+{
+    for (auto& p : h->xpeers)
+        if (p.rank == peer) return &p;
+    return nullptr;
+}
+
+int pk_halo_sizes(pk_handle h, int32_t peer, int64_t* send_doubles, int64_t* recv_doubles)
+{
+    if (!h) return PK_E_ARG;
+    if (int rc = exchange_prepare(h)) return rc;
+    XPeerDev* p = find_peer(h, peer);
+    if (!p) return fail(h, PK_E_ARG, "no halo traffic with that rank");
+    if (send_doubles) *send_doubles = p->send.total * h->nplanes;
+    if (recv_doubles) *recv_doubles = p->recv.total * h->nplanes;
+    return PK_OK;
+}
+
+static int halo_copy(pk_ctx* h, int peer, double* buf, int to_buf)
+{
+    if (int rc = exchange_prepare(h)) return rc;
+    XPeerDev* p = find_peer(h, peer);
+    if (!p) return fail(h, PK_E_ARG, "no halo traffic with that rank");
+    if (!buf) return fail(h, PK_E_ARG, "null buffer");
+    const XSegList& l = to_buf ? p->send : p->recv;
+    if (l.total > 0) {
+        k_halo_copy<<<grid1d(l.total, 256), 256, 0, h->stream>>>(l.dev, l.n, l.total, h->d_xptr[h->cur], h->nplanes, buf,
+                                                                to_buf);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+    }
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_halo_pack(pk_handle h, int32_t peer, double* sendbuf_dev)
+{
+    if (!h) return PK_E_ARG;
+    return halo_copy(h, peer, sendbuf_dev, 1);
+}
+
+int pk_halo_unpack(pk_handle h, int32_t peer, const double* recvbuf_dev)
+{
+    if (!h) return PK_E_ARG;
+    return halo_copy(h, peer, const_cast<double*>(recvbuf_dev), 0);
+}
+
+int pk_set_comm(pk_handle h, pk_halo_fn halo, pk_reduce_fn reduce, void* ctx)
+{
+    if (!h) return PK_E_ARG;
+    h->halo_cb = halo;
+    h->reduce_cb = reduce;
+    h->comm_ctx = ctx;
+    invalidate_graph(h);
+    return PK_OK;
+}
+
 int pk_block_place(pk_handle h, int32_t id, const int64_t off[3])
 {
     Block* b;
@@ -845,6 +972,10 @@ int pk_time_step(pk_handle h, double* dt_out)
     double dt, c_all;
     h->ts.dt_old = h->ts.dt;                          // timestep.F90:158
     if (int rc = pk_timestep_raw(h, &dt, &c_all)) return rc;
+    if (h->reduce_cb) {                               // over ranks (timestep.F90:173, MPI_MIN / MPI_MAX)
+        dt = h->reduce_cb(h->comm_ctx, dt, 0);
+        c_all = h->reduce_cb(h->comm_ctx, c_all, 1);
+    }
     const pk_config& c = h->cfg;
     if (h->ts.nstep < 1) {                            // :200-208
         if (c.dt_initial > 0.0) dt = (c.dt_initial < dt) ? c.dt_initial : dt;
@@ -880,7 +1011,7 @@ int pk_fluid_update(pk_handle h)
     glm_scalars(h, dt, &ch, &fac);
     h->ts.chspeed = ch;
     if (int rc = put_step_params(h, dt, ch, fac)) return rc;
-    if (h->use_graph && !h->profiling) {
+    if (h->use_graph && !h->profiling && !h->halo_cb) {
         if (fused_ok(h) && h->blocks.size() > 1)
             if (int rc = build_batch(h)) return rc;   // tables are built outside the capture
         if (int rc = exchange_prepare(h)) return rc;

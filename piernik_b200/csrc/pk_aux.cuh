@@ -241,6 +241,39 @@ static __global__ void k_exchange(const XSegDev* __restrict__ segs, int nseg, lo
     }
 }
 
+// Halo exchange with another rank: pack the source cells of the segments
+// sent to one peer (to_buf = 1) or unpack the cells received from it into
+// guard cells (to_buf = 0).  Buffer layout: plane v of cell c at v*total + c,
+// cells in segment order, i fastest within a segment.
+static __global__ void k_halo_copy(const XSegDev* __restrict__ segs, int nseg, long long total,
+                                   const XPtr* __restrict__ blk, int nplanes, double* __restrict__ buf, int to_buf)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].first <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const XSegDev s = segs[lo];
+        long long r = c - s.first;
+        const int nx = s.hi[0] - s.lo[0], ny = s.hi[1] - s.lo[1];
+        const int i = s.lo[0] + (int)(r % nx);
+        r /= nx;
+        const int j = s.lo[1] + (int)(r % ny);
+        const int k = s.lo[2] + (int)(r / ny);
+        if (to_buf) {
+            const XPtr q = blk[s.src];
+            const long long si = ((long long)(k + s.shift[2]) * q.ext[1] + (j + s.shift[1])) * q.ext[0] + (i + s.shift[0]);
+            for (int v = 0; v < nplanes; ++v) buf[(long long)v * total + c] = q.u[(long long)v * q.plane + si];
+        } else {
+            const XPtr d = blk[s.dst];
+            const long long di = ((long long)k * d.ext[1] + j) * d.ext[0] + i;
+            for (int v = 0; v < nplanes; ++v) d.u[(long long)v * d.plane + di] = buf[(long long)v * total + c];
+        }
+    }
+}
+
 // zero every guard cell of all planes (adjoint states carry no guard values)
 static __global__ void k_zero_guards(BoxGeom b, double* __restrict__ u, int nplanes)
 {

@@ -5,7 +5,10 @@
 // intersected once on the host and the copies run as one kernel.
 #include "pk_exchange.h"
 
+#include <algorithm>
 #include <cstdio>
+#include <map>
+#include <tuple>
 
 namespace pk {
 
@@ -107,6 +110,43 @@ bool build_exchange(const std::vector<XBlock>& blocks, const long long dom[3], c
         }
     }
     return true;
+}
+
+void sort_canonical(const std::vector<XBlock>& blocks, std::vector<XSeg>& segs)
+{
+    auto key = [&](const XSeg& s) {
+        const XBlock& d = blocks[s.dst];
+        const XBlock& q = blocks[s.src];
+        return std::make_tuple(d.off[2], d.off[1], d.off[0], s.lo[2], s.lo[1], s.lo[0], q.off[2], q.off[1], q.off[0],
+                               s.shift[2], s.shift[1], s.shift[0]);
+    };
+    std::stable_sort(segs.begin(), segs.end(), [&](const XSeg& a, const XSeg& b) { return key(a) < key(b); });
+}
+
+void split_by_owner(const std::vector<XBlock>& blocks, const std::vector<int>& owner, int nlocal,
+                    const std::vector<XSeg>& segs, std::vector<XSeg>& local, std::vector<XPeer>& peers)
+{
+    local.clear();
+    peers.clear();
+    std::map<int, XPeer> by;
+    for (const XSeg& s : segs) {
+        const bool dl = s.dst < nlocal, sl = s.src < nlocal;
+        if (dl && sl) local.push_back(s);
+        else if (dl) {
+            XPeer& p = by[owner[s.src]];
+            p.rank = owner[s.src];
+            p.recv.push_back(s);
+        } else if (sl) {
+            XPeer& p = by[owner[s.dst]];
+            p.rank = owner[s.dst];
+            p.send.push_back(s);
+        }
+    }
+    for (auto& kv : by) {
+        sort_canonical(blocks, kv.second.recv);
+        sort_canonical(blocks, kv.second.send);
+        peers.push_back(kv.second);
+    }
 }
 
 }  // namespace pk

@@ -35,4 +35,20 @@ struct XSeg {
 bool build_exchange(const std::vector<XBlock>& blocks, const long long dom[3], const int periodic[3],
                     std::vector<XSeg>& segs, std::string& err);
 
+// Segments between this rank and one peer, in an order both ranks derive
+// alike: by the destination block's offset, the segment's first cell, the
+// source block's offset and the shift -- positions on the level's grid, not
+// block numbers, which differ between ranks.
+void sort_canonical(const std::vector<XBlock>& blocks, std::vector<XSeg>& segs);
+
+// Split the segments of blocks[0..nlocal) (this rank's) and of the remote
+// blocks (owner[i] >= 0 for i >= nlocal) into the local copies, and per peer
+// rank the copies received (destination local) and sent (source local).
+struct XPeer {
+    int rank;
+    std::vector<XSeg> recv, send;
+};
+void split_by_owner(const std::vector<XBlock>& blocks, const std::vector<int>& owner, int nlocal,
+                    const std::vector<XSeg>& segs, std::vector<XSeg>& local, std::vector<XPeer>& peers);
+
 }  // namespace pk

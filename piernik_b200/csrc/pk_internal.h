@@ -42,6 +42,26 @@ struct StepRec {
     double dt, ch, fac;
 };
 
+// device copy of a segment list with its cell count
+struct XSegList {
+    XSegDev* dev = nullptr;
+    int n = 0;
+    long long total = 0;
+};
+
+// the halo traffic with one other rank
+struct XPeerDev {
+    int rank = -1;
+    XSegList send, recv;
+};
+
+// a block held by another rank (connected domains spanning ranks)
+struct RemoteBlock {
+    int owner;
+    int n[3];
+    long long off[3];
+};
+
 // work list of the batched sweep for one direction
 struct BatchList {
     std::vector<WorkItem> host;
@@ -88,10 +108,13 @@ struct pk_ctx {
     int dom_periodic[3] = {0, 0, 0};
     bool x_dirty = true;                // the exchange plan must be rebuilt
     bool x_ptrs_dirty = true;           // block buffers changed: rebuild the pointer tables
-    pk::XSegDev* d_xseg = nullptr;
+    pk::XSegList xlocal;                // copies between this rank's blocks
+    std::vector<pk::XPeerDev> xpeers;   // copies to and from each other rank
+    std::vector<pk::RemoteBlock> remote;
     pk::XPtr* d_xptr[2] = {nullptr, nullptr};   // block states of parity 0 / 1
-    int nxseg = 0;
-    long long xtotal = 0;
+    pk_halo_fn halo_cb = nullptr;       // moves the halo of other ranks (host callback)
+    pk_reduce_fn reduce_cb = nullptr;   // min / max over ranks for the time step
+    void* comm_ctx = nullptr;
     // differentiable path (single block, fused sweeps)
     int adjL[3] = {0, 0, 0};            // owned cells per pencil of the adjoint tiles, per direction (0: default)
     int adjV[3] = {-1, -1, -1};         // launch-bound variant of the adjoint kernels per direction (-1: default)
