@@ -275,6 +275,7 @@ bool connected_fused_ok(pk_ctx* h)
         if (!b.placed) return false;
         cells += (long long)b.n[0] * b.n[1] * b.n[2];
     }
+    for (auto& r : h->remote) cells += (long long)r.n[0] * r.n[1] * r.n[2];
     for (int d = 0; d < 3; ++d)
         if (h->dom[d] > 1 && !h->dom_periodic[d]) return false;
     return cells == h->dom[0] * h->dom[1] * h->dom[2];
@@ -1187,7 +1188,8 @@ void grad_release(pk_ctx* h)
 
 int grad_check(pk_ctx* h)
 {
-    if (h->blocks.size() != 1) return fail(h, PK_E_UNSUPPORTED, "the differentiable path runs on one block");
+    if (h->blocks.size() != 1 || !h->remote.empty())
+        return fail(h, PK_E_UNSUPPORTED, "the differentiable path runs on one block of one rank");
     if (!fused_ok(h)) return fail(h, PK_E_UNSUPPORTED, "the differentiable path needs RK2 and periodic boundaries");
     if (h->cfg.nfluids != 1) return fail(h, PK_E_UNSUPPORTED, "the differentiable path is built for one fluid");
     int dirs[3], nd;

@@ -163,8 +163,12 @@ class SlabRank:
         self.error = None
         self._halo_cb = L.HALO_FN(self._halo)
         self._reduce_cb = L.REDUCE_FN(self._reduce)
-        self.sim._chk(lib.pk_set_comm(h, C.cast(self._halo_cb, C.c_void_p), C.cast(self._reduce_cb, C.c_void_p),
-                                      None), "pk_set_comm")
+        self.attach()
+
+    def attach(self) -> None:
+        """Install the halo and reduce callbacks (done at construction)."""
+        self.sim._chk(self.sim.lib.pk_set_comm(self.sim.h, C.cast(self._halo_cb, C.c_void_p),
+                                               C.cast(self._reduce_cb, C.c_void_p), None), "pk_set_comm")
 
     # callbacks (called by the library on this rank's host thread); an error
     # cannot cross the C boundary, so it is kept and raised by check()
