@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PK_ABI_VERSION 1
+#define PK_ABI_VERSION 2
 
 enum {
     PK_OK = 0,
@@ -70,12 +70,27 @@ typedef struct pk_config {
     double dt_initial, dt_max_grow, dt_min, dt_max;
     double tend;                /* END_CONTROL: tend */
     int32_t skip_sweep[3];
+    /* step retry: cflcontrol (PK_CFL_*), cfl_max (sanitised as global.F90:304),
+     * dt_shrink, max_redostep_attempts (global.F90:218,233,245,258) */
+    int32_t cflcontrol;
+    double cfl_max, dt_shrink;
+    int32_t max_redostep_attempts;
 } pk_config;
+
+#define PK_CFL_NONE 0           /* no check */
+#define PK_CFL_WARN 1           /* stepcfl computed each step (timestep.F90:317-360), no retry */
+#define PK_CFL_REDO 2           /* a step whose effective CFL exceeds cfl_max, or that made
+                                   unwanted negatives, is redone with dt x dt_shrink^attempt
+                                   (timestep_retry.F90:repeat_fluidstep) -- the reference default */
 
 /* Time-integration state the reference keeps in module global (global.F90). */
 typedef struct pk_time_state {
     double t, dt, dt_old, c_all, chspeed;
     int32_t nstep;
+    /* step retry state (global.F90: dt_full, dt_cur_shrink, t_saved, nstep_saved,
+     * tstep_attempt; timestep_pub: c_all_old, stepcfl; repeatstep: repeat_step) */
+    double dt_full, c_all_old, dt_cur_shrink, stepcfl, t_saved;
+    int32_t nstep_saved, tstep_attempt, repeat_step, redone;
 } pk_time_state;
 
 typedef struct pk_ctx* pk_handle;

@@ -49,6 +49,10 @@ class OCfg(C.Structure):
         ("dt_max", C.c_double),
         ("tend", C.c_double),
         ("skip_sweep", C.c_int * 3),
+        ("cflcontrol", C.c_int),
+        ("cfl_max", C.c_double),
+        ("dt_shrink", C.c_double),
+        ("max_redostep_attempts", C.c_int),
     ]
 
 
@@ -66,6 +70,7 @@ class OBlock(C.Structure):
         ("psih", C.POINTER(C.c_double)),
         ("dn_negative", C.c_int),
         ("ei_negative", C.c_int),
+        ("uh_retry", C.POINTER(C.c_double)),
     ]
 
 
@@ -77,6 +82,15 @@ class OState(C.Structure):
         ("c_all", C.c_double),
         ("chspeed", C.c_double),
         ("nstep", C.c_int),
+        ("dt_full", C.c_double),
+        ("c_all_old", C.c_double),
+        ("dt_cur_shrink", C.c_double),
+        ("stepcfl", C.c_double),
+        ("t_saved", C.c_double),
+        ("nstep_saved", C.c_int),
+        ("tstep_attempt", C.c_int),
+        ("repeat", C.c_int),
+        ("redone", C.c_int),
     ]
 
 
@@ -114,6 +128,8 @@ def lib():
         L.o_nvar.argtypes = [P]
         L.o_run_multi.argtypes = [P, C.POINTER(B), C.c_int, S, C.c_int]
         L.o_set_threads.argtypes = [C.c_int]
+        L.o_cfl_max.argtypes = [P]
+        L.o_cfl_max.restype = C.c_double
         L.o_get_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -146,6 +162,10 @@ def make_cfg(setup) -> OCfg:
     c.tend = setup.tend
     for d in range(3):
         c.skip_sweep[d] = int(setup.skip_sweep[d])
+    c.cflcontrol = {"none": 0, "warn": 1, "redo": 2, "repeat": 2}[setup.cflcontrol]
+    c.cfl_max = setup.cfl_max
+    c.dt_shrink = setup.dt_shrink
+    c.max_redostep_attempts = setup.max_redostep_attempts
     return c
 
 
@@ -176,9 +196,13 @@ class OracleBlock:
         self.blk.u, self.blk.uh = _ptr(self.u), _ptr(self.uh)
         self.blk.b, self.blk.bh = _ptr(self.b), _ptr(self.bh)
         self.blk.psi, self.blk.psih = _ptr(self.psi), _ptr(self.psih)
+        ez, ey, ex = [setup.ext[d] for d in (2, 1, 0)]
+        self.retry = np.zeros((setup.nvar + 4) * ez * ey * ex)
+        self.blk.uh_retry = _ptr(self.retry)
         self.state = OState()
         self.state.dt = 0.0
         self.state.dt_old = -1.0
+        self.state.dt_cur_shrink = 1.0
 
     def fill_guards(self):
         lib().o_fill_guards(C.byref(self.cfg), C.byref(self.blk))
@@ -216,6 +240,7 @@ def run_multi(blocks, nsteps: int, state: OState = None) -> OState:
     if state is None:
         state = OState()
         state.dt_old = -1.0
+        state.dt_cur_shrink = 1.0
     arr = (C.POINTER(OBlock) * len(blocks))(*[C.pointer(b.blk) for b in blocks])
     rc = lib().o_run_multi(C.byref(blocks[0].cfg), arr, len(blocks), C.byref(state), nsteps)
     if rc:

@@ -929,15 +929,119 @@ int o_fluid_update(const o_cfg *cfg, o_block *blk, o_state *st)
     return 0;
 }
 
+/* cfl_max after the sanitising of init_global (global.F90:304) */
+double o_cfl_max(const o_cfg *cfg)
+{
+    const double c = cfg->cfl;
+    return f_min(f_max(cfg->cfl_max, f_min(f_min(c * 1.1, c + 0.05), (1.0 + c) / 2.0)), 1.0);
+}
+
+/* dt_shrink**n as an integer power: repeated squaring */
+static double o_powi(double x, int n)
+{
+    double r = 1.0;
+    while (n > 0) {
+        if (n & 1) r = r * x;
+        x = x * x;
+        n >>= 1;
+    }
+    return r;
+}
+
+/* stepcfl of cfl_warn (timestep.F90:329-330) */
+static double o_stepcfl(const o_cfg *cfg, const o_state *st, double c_all)
+{
+    double s = cfg->cfl * st->dt_cur_shrink;
+    if (st->c_all_old > 0.0) s = ((c_all / st->c_all_old) * cfg->cfl) * st->dt_cur_shrink;
+    return s;
+}
+
+/* check_cfl_violation (timestep.F90:247-310) with cfl_warn run from the
+   non-main time_step call (:211); decides st->repeat and dt_cur_shrink */
+static int o_check_cfl(const o_cfg *cfg, o_block *blk, o_state *st)
+{
+    int unwanted = 0;
+    if (blk->dn_negative) {
+        if (cfg->disallow_negatives) unwanted = 1;
+        blk->dn_negative = 0;
+    }
+    if (blk->ei_negative) {
+        if (cfg->disallow_negatives) unwanted = 1;
+        blk->ei_negative = 0;
+    }
+    double dt, c_all;                                     /* time_step(checkdt, flind, .false.) */
+    o_timestep_raw(cfg, blk, &dt, &c_all);
+    if (st->nstep < 1) {
+        if (cfg->dt_initial > 0.0) dt = f_min(dt, cfg->dt_initial);
+        else if (cfg->dt_initial < 0.0) dt = f_min(dt, -cfg->dt_initial * dt);
+    } else {
+        if (st->dt_old > 0.0) dt = f_min(dt, st->dt_old * cfg->dt_max_grow);
+    }
+    st->stepcfl = o_stepcfl(cfg, st, c_all);              /* cfl_warn */
+    int repeat = unwanted;
+    if (st->stepcfl > o_cfl_max(cfg)) repeat = 1;
+    st->dt_cur_shrink = repeat ? o_powi(cfg->dt_shrink, st->tstep_attempt + 1) : 1.0;
+    if (dt < cfg->dt_min) return 3;                       /* write_crashed */
+    st->repeat = repeat;                                  /* c_all keeps the main call's value */
+    return 0;
+}
+
+/* piernik.F90:125-167: the main loop body, nsteps times (a repeated step
+   counts as an iteration) */
 int o_run(const o_cfg *cfg, o_block *blk, o_state *st, int nsteps)
 {
+    const int redo = cfg->cflcontrol == O_CFL_REDO;
     for (int s = 0; s < nsteps; ++s) {
-        if (!(st->t < cfg->tend)) break;
-        int rc = o_time_step(cfg, blk, st);
-        if (rc) return rc;
+        if (!(st->t < cfg->tend) && !st->repeat) break;
+        int rc;
+        if (!st->repeat) {
+            const double c_old = st->c_all_old;
+            rc = o_time_step(cfg, blk, st);
+            if (cfg->cflcontrol == O_CFL_WARN) {          /* cfl_manager in the main call: a warning only */
+                o_state tmp = *st;
+                tmp.c_all_old = c_old;
+                st->stepcfl = o_stepcfl(cfg, &tmp, st->c_all);
+            }
+            st->c_all_old = st->c_all;
+            if (rc) return rc;
+            st->dt_full = st->dt;
+        }
+        if (redo) {                                       /* repeat_fluidstep (timestep_retry.F90:58-...) */
+            int ext[3], g[3];
+            o_extents(blk, ext, g);
+            const long long nc = (long long)ext[0] * ext[1] * ext[2];
+            const int nv = o_nvar(cfg);
+            if (!blk->uh_retry) return 5;
+            if (st->repeat) {
+                st->tstep_attempt += 1;
+                if (st->tstep_attempt > cfg->max_redostep_attempts) return 4;
+                st->t = st->t_saved;
+                st->nstep = st->nstep_saved;
+                st->dt = st->dt_full * st->dt_cur_shrink;
+                memcpy(blk->u, blk->uh_retry, sizeof(double) * nv * nc);
+                if (cfg->magnetic) {
+                    memcpy(blk->b, blk->uh_retry + nv * nc, sizeof(double) * 3 * nc);
+                    memcpy(blk->psi, blk->uh_retry + (nv + 3) * nc, sizeof(double) * nc);
+                }
+                st->redone += 1;
+            } else {
+                st->tstep_attempt = 0;
+                st->nstep_saved = st->nstep;
+                st->t_saved = st->t;
+                memcpy(blk->uh_retry, blk->u, sizeof(double) * nv * nc);
+                if (cfg->magnetic) {
+                    memcpy(blk->uh_retry + nv * nc, blk->b, sizeof(double) * 3 * nc);
+                    memcpy(blk->uh_retry + (nv + 3) * nc, blk->psi, sizeof(double) * nc);
+                }
+            }
+        }
         rc = o_fluid_update(cfg, blk, st);
         if (rc) return rc;
         st->nstep += 1;
+        if (redo) {
+            rc = o_check_cfl(cfg, blk, st);
+            if (rc) return rc;
+        }
     }
     return 0;
 }

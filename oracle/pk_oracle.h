@@ -47,7 +47,14 @@ typedef struct o_cfg {
     int integration_order;       /* 1 (EULER) or 2 (RK2) */
     double dt_initial, dt_max_grow, dt_min, dt_max, tend;
     int skip_sweep[3];
+    int cflcontrol;              /* O_CFL_NONE / O_CFL_WARN / O_CFL_REDO (global.F90:218, timestep.F90:73-90) */
+    double cfl_max, dt_shrink;   /* global.F90:233,245 (cfl_max sanitized as :304 on use) */
+    int max_redostep_attempts;   /* global.F90:258 */
 } o_cfg;
+
+#define O_CFL_NONE 0
+#define O_CFL_WARN 1
+#define O_CFL_REDO 2
 
 typedef struct o_block {
     int n[3];                    /* interior cells per direction */
@@ -58,14 +65,19 @@ typedef struct o_block {
     double *b, *bh;              /* 3 components (NULL when !magnetic) */
     double *psi, *psih;          /* (NULL when !magnetic) */
     int dn_negative, ei_negative;
+    double *uh_retry;            /* step-retry backup of u, b, psi (nvar+4 planes of the guard-inclusive block), or NULL */
 } o_block;
 
 typedef struct o_state {         /* the reference's global time-step state */
     double t, dt, dt_old, c_all, chspeed;
     int nstep;
+    /* step retry (timestep_retry.F90, timestep.F90:247-360) */
+    double dt_full, c_all_old, dt_cur_shrink, stepcfl, t_saved;
+    int nstep_saved, tstep_attempt, repeat, redone;
 } o_state;
 
 int    o_nvar(const o_cfg *cfg);
+double o_cfl_max(const o_cfg *cfg);
 void   o_extents(const o_block *blk, int ext[3], int g[3]);
 
 /* one stage of solve_cg_riemann on one block (solve_cg_riemann.F90:68-233,241-307) */

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libpiernik_b200.so")
 
 PK_OK = 0
+PK_CFL = {"none": 0, "warn": 1, "redo": 2, "repeat": 2}
 ERRORS = {-1: "PK_E_ARG", -2: "PK_E_CUDA", -3: "PK_E_NOMEM", -4: "PK_E_UNSUPPORTED", -5: "PK_E_STATE",
           -6: "PK_E_DTMIN"}
 PK_FLUID = {"ion": 0, "neu": 1, "dst": 2}
@@ -62,6 +63,10 @@ class PkConfig(C.Structure):
         ("dt_max", C.c_double),
         ("tend", C.c_double),
         ("skip_sweep", C.c_int32 * 3),
+        ("cflcontrol", C.c_int32),
+        ("cfl_max", C.c_double),
+        ("dt_shrink", C.c_double),
+        ("max_redostep_attempts", C.c_int32),
     ]
 
 
@@ -73,6 +78,15 @@ class PkTimeState(C.Structure):
         ("c_all", C.c_double),
         ("chspeed", C.c_double),
         ("nstep", C.c_int32),
+        ("dt_full", C.c_double),
+        ("c_all_old", C.c_double),
+        ("dt_cur_shrink", C.c_double),
+        ("stepcfl", C.c_double),
+        ("t_saved", C.c_double),
+        ("nstep_saved", C.c_int32),
+        ("tstep_attempt", C.c_int32),
+        ("repeat_step", C.c_int32),
+        ("redone", C.c_int32),
     ]
 
 

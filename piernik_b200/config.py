@@ -47,7 +47,10 @@ class Setup:
     dt_max_grow: float = 2.0
     dt_min: float = DBL_TINY
     dt_max: float = DBL_HUGE
-    cflcontrol: str = "none"
+    cflcontrol: str = "none"         # the reference defaults to 'redo' (:218); 'none' keeps parity runs unforked
+    cfl_max: float = 0.9             # :233
+    dt_shrink: float = 0.5           # :245
+    max_redostep_attempts: int = 10  # :258
     skip_sweep: Tuple[bool, bool, bool] = (False, False, False)
     # END_CONTROL
     tend: float = DBL_HUGE
@@ -80,6 +83,8 @@ class Setup:
             raise ValueError("CFL value should be >0. and <=1.")      # global.F90:303
         if self.integration_order not in (1, 2):
             raise ValueError("integration_order must be 1 or 2")
+        if self.cflcontrol not in ("none", "warn", "redo", "repeat"):
+            raise ValueError(f"cflcontrol {self.cflcontrol!r}: this library implements none, warn and redo")
         kinds = [k for k, _ in self.fluids]
         if kinds != sorted(kinds, key=("ion", "neu", "dst").index) or len(set(kinds)) != len(kinds):
             raise ValueError("fluids must be a subset of (ion, neu, dst) in that order")

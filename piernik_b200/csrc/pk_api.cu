@@ -528,10 +528,16 @@ void pk_config_default(pk_config* c)
     c->dt_min = DBL_MIN;
     c->dt_max = DBL_MAX;
     c->tend = DBL_MAX;
+    c->cflcontrol = PK_CFL_REDO;       // global.F90:218
+    c->cfl_max = 0.9;                  // :233
+    c->dt_shrink = 0.5;                // :245
+    c->max_redostep_attempts = 10;     // :258
 }
 
 int pk_create(const pk_config* cfg, pk_handle* out)
 {
+    if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_REDO || cfg->max_redostep_attempts < 0))
+        return PK_E_ARG;
     if (!cfg || !out) return PK_E_ARG;
     *out = nullptr;
     const pk_config& c = *cfg;
@@ -573,6 +579,7 @@ int pk_create(const pk_config* cfg, pk_handle* out)
     h->pp.limb = c.limiter_b;
     std::memset(&h->ts, 0, sizeof(h->ts));
     h->ts.dt_old = -1.0;
+    h->ts.dt_cur_shrink = 1.0;                        // global.F90:571
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&h->d_status, sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
@@ -610,6 +617,7 @@ int pk_destroy(pk_handle h)
     free_segs(h);
     cudaFree(h->d_xptr[0]);
     cudaFree(h->d_xptr[1]);
+    for (auto& b : h->blocks) cudaFree(b.retry);
     cudaFree(h->d_desc[0]);
     cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
@@ -1050,14 +1058,125 @@ int pk_fluid_update(pk_handle h)
     return PK_OK;
 }
 
+// cfl_max after the sanitising of init_global (global.F90:304)
+static double cfl_max_of(const pk_config& c)
+{
+    const double x = c.cfl;
+    double lo = (x * 1.1 < x + 0.05) ? x * 1.1 : x + 0.05;
+    lo = ((1.0 + x) / 2.0 < lo) ? (1.0 + x) / 2.0 : lo;
+    const double m = (lo > c.cfl_max) ? lo : c.cfl_max;
+    return (1.0 < m) ? 1.0 : m;
+}
+
+// dt_shrink**n as an integer power: repeated squaring
+static double powi(double x, int n)
+{
+    double r = 1.0;
+    while (n > 0) {
+        if (n & 1) r = r * x;
+        x = x * x;
+        n >>= 1;
+    }
+    return r;
+}
+
+// stepcfl of cfl_warn (timestep.F90:329-330)
+static double stepcfl_of(const pk_ctx* h, double c_all_old, double c_all)
+{
+    double s = h->cfg.cfl * h->ts.dt_cur_shrink;
+    if (c_all_old > 0.0) s = ((c_all / c_all_old) * h->cfg.cfl) * h->ts.dt_cur_shrink;
+    return s;
+}
+
+// the state copy of repeat_fluidstep: save (restore = 0) or restore (1)
+static int retry_copy(pk_ctx* h, int restore)
+{
+    for (auto& b : h->blocks) {
+        const size_t bytes = sizeof(double) * h->nplanes * b.plane;
+        if (!b.retry) {
+            if (cudaMalloc(&b.retry, bytes) != cudaSuccess) return fail(h, PK_E_NOMEM, "cudaMalloc of the retry copy failed");
+        }
+        if (b.guards_stale && !restore)
+            if (int rc = refresh_guards(h, b)) return rc;
+        if (restore) PK_CUDA(h, cudaMemcpyAsync(state(h, b), b.retry, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        else PK_CUDA(h, cudaMemcpyAsync(b.retry, state(h, b), bytes, cudaMemcpyDeviceToDevice, h->stream));
+        if (restore) b.guards_stale = false;
+    }
+    return PK_OK;
+}
+
+// check_cfl_violation (timestep.F90:247-310) with cfl_warn from the
+// non-main time_step call: sets repeat_step and dt_cur_shrink
+static int check_cfl(pk_ctx* h)
+{
+    uint32_t st = 0;
+    if (int rc = pk_status(h, &st)) return rc;
+    double neg = (st & (PK_ST_DN_NEGATIVE | PK_ST_EI_NEGATIVE)) ? 1.0 : 0.0;
+    if (h->reduce_cb) neg = h->reduce_cb(h->comm_ctx, neg, 1);        // pLOR
+    const int unwanted = (neg > 0.0 && h->cfg.disallow_negatives) ? 1 : 0;
+    double dt, c_all;                                                // time_step(checkdt, flind, .false.)
+    if (int rc = pk_timestep_raw(h, &dt, &c_all)) return rc;
+    if (h->reduce_cb) {
+        dt = h->reduce_cb(h->comm_ctx, dt, 0);
+        c_all = h->reduce_cb(h->comm_ctx, c_all, 1);
+    }
+    const pk_config& c = h->cfg;
+    if (h->ts.nstep < 1) {
+        if (c.dt_initial > 0.0) dt = (c.dt_initial < dt) ? c.dt_initial : dt;
+        else if (c.dt_initial < 0.0) {
+            const double x = -c.dt_initial * dt;
+            dt = (x < dt) ? x : dt;
+        }
+    } else if (h->ts.dt_old > 0.0) {
+        const double x = h->ts.dt_old * c.dt_max_grow;
+        dt = (x < dt) ? x : dt;
+    }
+    h->ts.stepcfl = stepcfl_of(h, h->ts.c_all_old, c_all);
+    int repeat = unwanted;
+    if (h->ts.stepcfl > cfl_max_of(c)) repeat = 1;
+    h->ts.dt_cur_shrink = repeat ? powi(c.dt_shrink, h->ts.tstep_attempt + 1) : 1.0;
+    if (dt < c.dt_min) return fail(h, PK_E_DTMIN, "dt < dt_min in the check after the step");
+    h->ts.repeat_step = repeat;
+    return PK_OK;
+}
+
+// piernik.F90:125-167: the main loop body nsteps times (a redone step counts
+// as one), with the retry machinery when cflcontrol = redo
 int pk_run(pk_handle h, int32_t nsteps)
 {
     if (!h) return PK_E_ARG;
+    const int redo = h->cfg.cflcontrol == PK_CFL_REDO;
     for (int s = 0; s < nsteps; ++s) {
-        if (!(h->ts.t < h->cfg.tend)) break;
-        if (int rc = pk_time_step(h, nullptr)) return rc;
+        if (!(h->ts.t < h->cfg.tend) && !h->ts.repeat_step) break;
+        if (!h->ts.repeat_step) {
+            const double c_old = h->ts.c_all_old;
+            const int rc = pk_time_step(h, nullptr);
+            if (h->cfg.cflcontrol == PK_CFL_WARN) h->ts.stepcfl = stepcfl_of(h, c_old, h->ts.c_all);
+            h->ts.c_all_old = h->ts.c_all;
+            if (rc) return rc;
+            h->ts.dt_full = h->ts.dt;
+        }
+        if (redo) {                                      // repeat_fluidstep
+            if (h->ts.repeat_step) {
+                h->ts.tstep_attempt += 1;
+                if (h->ts.tstep_attempt > h->cfg.max_redostep_attempts)
+                    return fail(h, PK_E_STATE, "tstep_attempt > max_redostep_attempts");
+                h->ts.t = h->ts.t_saved;
+                h->ts.nstep = h->ts.nstep_saved;
+                h->ts.dt = h->ts.dt_full * h->ts.dt_cur_shrink;
+                if (int rc = retry_copy(h, 1)) return rc;
+                h->ts.redone += 1;
+            } else {
+                h->ts.tstep_attempt = 0;
+                h->ts.nstep_saved = h->ts.nstep;
+                h->ts.t_saved = h->ts.t;
+                if (int rc = retry_copy(h, 0)) return rc;
+            }
+        }
         if (int rc = pk_fluid_update(h)) return rc;
         h->ts.nstep += 1;
+        if (redo)
+            if (int rc = check_cfl(h)) return rc;
     }
     return PK_OK;
 }

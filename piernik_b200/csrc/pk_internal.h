@@ -31,6 +31,7 @@ struct Block {
     double* uh = nullptr;                  // stage path: state at the start of the step (cg%w(uh))
     double* stage = nullptr;               // host-layout conversion buffer
     bool guards_stale = false;             // fused sweeps read periodic images and never store guards
+    double* retry = nullptr;               // copy of the state at the start of a step (cflcontrol = redo)
     long long off[3] = {0, 0, 0};          // first interior cell on the level's cell grid (connected domains)
     bool placed = false;
 };

@@ -155,7 +155,7 @@ def read_problem_par(text: str, cmdline: Optional[str] = None, setup: Optional[S
         kw["magnetic"] = bool(magnetic)
     ns = g.get("NUMERICAL_SETUP", {})
     for key in ("cfl", "cfl_glm", "glm_alpha", "smalld", "smallei", "dt_initial", "dt_max_grow", "dt_min",
-                "dt_max"):
+                "dt_max", "cfl_max", "dt_shrink"):
         if key in ns:
             kw[key] = float(ns[key])
     for key in ("use_smalld", "use_smallei", "disallow_negatives"):
@@ -171,6 +171,8 @@ def read_problem_par(text: str, cmdline: Optional[str] = None, setup: Optional[S
         kw["integration_order"] = int(ns["integration_order"])
     if "cflcontrol" in ns:
         kw["cflcontrol"] = str(ns["cflcontrol"]).strip().lower()
+    if "max_redostep_attempts" in ns:
+        kw["max_redostep_attempts"] = int(ns["max_redostep_attempts"])
     if "skip_sweep" in ns:
         v = ns["skip_sweep"]
         kw["skip_sweep"] = tuple(bool(x) for x in (v if isinstance(v, list) else [v] * 3))

@@ -64,6 +64,10 @@ def make_config(setup: Setup) -> L.PkConfig:
     c.tend = setup.tend
     for d in range(3):
         c.skip_sweep[d] = int(setup.skip_sweep[d])
+    c.cflcontrol = L.PK_CFL[setup.cflcontrol]
+    c.cfl_max = setup.cfl_max
+    c.dt_shrink = setup.dt_shrink
+    c.max_redostep_attempts = setup.max_redostep_attempts
     return c
 
 

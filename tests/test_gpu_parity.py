@@ -244,3 +244,24 @@ def test_single_block_graph_and_forced_batch(gpu_lib, oracle_lib):
     setup, u, b, psi = problems.mhd_turbulence(n=24, seed=4)
     _multi([(setup, u, b, psi)], 4, batched=False, graph=True)
     _multi([(setup, u, b, psi)], 3, batched=True, graph=False)
+
+
+@pytest.mark.parametrize("cfl", [0.7, 0.9])
+def test_cfl_redo_matches_oracle(gpu_lib, oracle_lib, cfl):
+    """cflcontrol = redo: steps whose effective CFL exceeds cfl_max are redone
+    from the saved state with a shrunk dt; the whole history (state, t, dt,
+    nstep, retries) equals the oracle's."""
+    s, u, b, psi = problems.sedov(n=24)
+    s = s.replace(cfl=cfl, cflcontrol="redo")
+    ob = oracle.OracleBlock(s, u, b, psi)
+    sim = Simulation(s)
+    sim.upload(u, b, psi)
+    assert ob.run(30) == 0
+    sim.run(30)
+    st, ost = sim.time_state, ob.state
+    for f in ("t", "dt", "dt_old", "c_all", "dt_full", "c_all_old", "dt_cur_shrink", "stepcfl", "t_saved"):
+        assert getattr(st, f) == getattr(ost, f), f
+    assert (st.nstep, st.redone, st.repeat_step, st.tstep_attempt) == (ost.nstep, ost.redone, ost.repeat, ost.tstep_attempt)
+    assert (st.redone > 0) == (cfl == 0.9)
+    compare(ob, sim, f"redo cfl={cfl}")
+    sim.close()

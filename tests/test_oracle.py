@@ -5,6 +5,7 @@ pinned by physics properties that hold bit-for-bit or to round-off:
 conservation on periodic boxes, exact symmetry under exchanging axes, GLM
 damping and CFL formulas restated independently in numpy.
 """
+import ctypes as C
 import math
 
 import numpy as np
@@ -190,3 +191,33 @@ def test_dust_in_hlld_diverging_flow_is_nan(oracle_lib):
     ob.solve_cg(0, 1, 0.001, 1.0)
     assert np.isnan(interior(s, ob.u)[..., 5:9]).any()
     assert not np.isnan(interior(s, ob.u)[..., 0:5]).any()
+
+
+def test_cfl_redo_without_violation_equals_none(oracle_lib):
+    """cflcontrol = redo changes nothing when no step violates cfl_max."""
+    from piernik_b200 import problems
+    s, u, b, psi = problems.sedov(n=16)
+    runs = []
+    for mode in ("none", "redo"):
+        ob = oracle.OracleBlock(s.replace(cfl=0.7, cflcontrol=mode), u, b, psi)
+        assert ob.run(12) == 0
+        runs.append(ob)
+    assert runs[1].state.redone == 0
+    assert np.array_equal(runs[0].u.view(np.uint64), runs[1].u.view(np.uint64))
+    assert runs[0].state.t == runs[1].state.t
+
+
+def test_cfl_redo_repeats_violating_steps(oracle_lib):
+    """At cfl = 0.9 the early Sedov blast speeds up faster than cfl_max allows
+    (stepcfl = c_new/c_old * cfl > 0.95): those steps are redone with half
+    the time step (timestep_retry.F90, timestep.F90:317-360)."""
+    from piernik_b200 import problems
+    s, u, b, psi = problems.sedov(n=24)
+    s = s.replace(cfl=0.9, cflcontrol="redo")
+    ob = oracle.OracleBlock(s, u, b, psi)
+    assert ob.run(30) == 0
+    st = ob.state
+    assert st.redone > 0
+    assert st.nstep == 30 - st.redone
+    assert st.stepcfl <= oracle.lib().o_cfl_max(C.byref(ob.cfg))
+    assert st.dt_cur_shrink == 1.0
