@@ -29,12 +29,12 @@ def variants() -> List[Tuple[int, int]]:
 
 
 def candidates(n_dir: int, n_ortho: int) -> Iterable[Tuple[int, int, int]]:
+    """(P, L, variant) tiles: chunks of L owned cells with a 4-cell halo, and the
+    whole pencil without halo (L = n_dir) where it fits the CTA."""
     for v, (maxt, _) in enumerate(variants()):
-        for Lc in LENGTHS:
-            if Lc > n_dir and Lc != LENGTHS[0]:
-                continue
-            Lc = min(Lc, n_dir)
-            T = Lc + 8
+        lengths = sorted(set(min(Lc, n_dir) for Lc in LENGTHS) | ({n_dir} if n_dir <= maxt else set()))
+        for Lc in lengths:
+            T = Lc if (Lc == n_dir and n_dir <= maxt) else Lc + 8
             for P in (1, 2, 3, 4, 6, 8, 12, 16):
                 if P > n_ortho:
                     continue

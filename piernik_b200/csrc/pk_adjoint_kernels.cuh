@@ -180,14 +180,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused_rec(Geom g, Tile tl,
     r.slope = active && t >= 1 && t < T - 1;
     r.flux = active && t >= 1 && t < T - 2;
     r.upd = active && t >= 2 && t < T - 2;
-    rk_stage<PH, true>(sm, me, st, r, w, uin, uin, off, g, c1, sp->ch, pp, status, &rec1);
+    rk_stage<PH, true>(sm, me, me - st, me + st, r, w, uin, uin, off, g, c1, sp->ch, pp, status, &rec1);
     const bool own = active && t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d;
     if (own) store_cell<PH>(ustar, off, g, w);
     r.q = active && t >= 2 && t < T - 2;
     r.slope = active && t >= 3 && t < T - 3;
     r.flux = active && t >= 3 && t < T - 4;
     r.upd = active && t >= 4 && t < T - 4;
-    rk_stage<PH, true>(sm, me, st, r, w, uin, uin, off, g, c2, sp->ch, pp, status, &rec2);
+    rk_stage<PH, true>(sm, me, me - st, me + st, r, w, uin, uin, off, g, c2, sp->ch, pp, status, &rec2);
     if (own) {
         if (PH::MHD && apply_fac) w[PH::IB + 3] = w[PH::IB + 3] * sp->psi_fac;
         store_cell<PH>(uout, off, g, w);

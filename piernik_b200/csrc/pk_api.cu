@@ -341,14 +341,16 @@ int build_batch(pk_ctx* h)
         for (int i = 0; i < nb; ++i) {
             const Block& b = h->blocks[i];
             if (b.n[dir] <= 1) continue;
-            const int L = b.n[dir] < h->batch_L ? b.n[dir] : h->batch_L;
-            const int T = L + 8;
+            // a periodic pencil that fits the CTA is swept whole, without halo
+            const int circ = (!h->connected && b.n[dir] <= threads && h->batch_circ) ? 1 : 0;
+            const int L = circ ? b.n[dir] : (b.n[dir] < h->batch_L ? b.n[dir] : h->batch_L);
+            const int T = circ ? L : L + 8;
             if (T > threads) return fail(h, PK_E_ARG, "batched tile longer than the CTA");
             int P = threads / T;
             if (P > b.n[o1]) P = b.n[o1];
             for (int i2 = 0; i2 < b.n[o2]; ++i2)
                 for (int c0 = 0; c0 < b.n[dir]; c0 += L)
-                    for (int i1 = 0; i1 < b.n[o1]; i1 += P) bl.host.push_back(WorkItem{i, i1, c0, i2, P, L});
+                    for (int i1 = 0; i1 < b.n[o1]; i1 += P) bl.host.push_back(WorkItem{i, i1, c0, i2, P, L, circ});
         }
         cudaFree(bl.dev);
         bl.dev = nullptr;
@@ -1217,7 +1219,9 @@ int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32
 {
     if (!h || dir < 0 || dir > 2 || pencils < 0 || length < 0 || variant < -1 || variant >= NVARIANT) return PK_E_ARG;
     const int maxt = VAR_T[variant >= 0 ? variant : 0];
-    if (length > 0 && length + 8 > maxt) return fail(h, PK_E_ARG, "length + 8 exceeds the variant's CTA size");
+    // a length of a whole periodic pencil runs without halo (up to the CTA size);
+    // any other length needs its 8 halo cells inside the CTA (checked at launch)
+    if (length > maxt) return fail(h, PK_E_ARG, "length exceeds the variant's CTA size");
     h->tileP[dir] = pencils;
     h->tileL[dir] = length;
     h->tileV[dir] = variant;

@@ -96,6 +96,7 @@ struct pk_ctx {
     int batched = 0;                    // 1: sweep all blocks in one persistent launch
     int batch_variant = 2;              // launch-bound variant of the batched kernel
     int batch_L = 56;                   // longest chunk of the batched tiles
+    int batch_circ = 1;                 // sweep pencils that fit the CTA whole (no halo)
     long long launches = 0;             // kernels of this library launched on the handle's stream
     bool profiling = false;             // bracket sweep kernels with CUDA events
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used, ev_free;

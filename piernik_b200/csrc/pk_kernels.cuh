@@ -42,6 +42,8 @@ struct Tile {
     int halo;               // stage mode: tile cells before the first owned cell (0 or 2)
     int wrap = 1;           // fused mode: 1 read the halo as periodic images of the interior,
                             // 0 read it from the block's guard cells (filled by the exchange)
+    int circ = 0;           // fused mode, periodic block: the tile is the whole pencil (T = L = n)
+                            // and cell t's neighbours are t -/+ 1 mod n -- no halo at all
 };
 
 // -------------------------------------------------------------------------
@@ -109,8 +111,11 @@ struct Smem {
 //   u0src  where u0 (uh / the sweep's input) is read for the update
 //   wsrc   where an unchanged end cell re-reads its state (r.keep)
 //   REC    record which floors clipped in *rec (the adjoint sweep's recomputation)
+//   me, mp, mn   this cell's slot in the shared planes and its previous / next
+//                neighbour's along the pencil (me -/+ the pencil stride, or the
+//                wrapped slot in a circular whole-pencil tile)
 template <class PH, bool REC = false>
-PK_DEV void rk_stage(const Smem& sm, int me, int st, const Roles& r, double (&w)[PH::NV], const double* u0src,
+PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, double (&w)[PH::NV], const double* u0src,
                      const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
                      const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr)
 {
@@ -129,22 +134,22 @@ PK_DEV void rk_stage(const Smem& sm, int me, int st, const Roles& r, double (&w)
             const int lim = (PH::MHD && v >= PH::IB) ? pp.limb : pp.lim;
             const double qc = sm.Q[v * PT + me];
             double s;
-            if (r.end < 0) s = slope_end(lim, sm.Q[v * PT + me + st] - qc);
-            else if (r.end > 0) s = slope_end(lim, qc - sm.Q[v * PT + me - st]);
-            else s = slope_interior(lim, qc - sm.Q[v * PT + me - st], sm.Q[v * PT + me + st] - qc);
+            if (r.end < 0) s = slope_end(lim, sm.Q[v * PT + mn] - qc);
+            else if (r.end > 0) s = slope_end(lim, qc - sm.Q[v * PT + mp]);
+            else s = slope_interior(lim, qc - sm.Q[v * PT + mp], sm.Q[v * PT + mn] - qc);
             const double dqh = 0.5 * s;                       // dq_interp = half * f_limiter(q)
             sm.L[v * PT + me] = qc + dqh;                     // left state of the right face
             sm.R[v * PT + me] = qc - dqh;                     // right state of the left face
         }
     }
     __syncthreads();
-    if (r.flux) riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, st, ch, pp);
+    if (r.flux) riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, pp);
     __syncthreads();
     if (r.upd) {
         double u0[NV];
         load_cell<PH>(u0src, off, g, u0);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) w[v] = u0[v] + dtodx * (sm.Q[v * PT + me - st] - sm.Q[v * PT + me]);
+        for (int v = 0; v < NV; ++v) w[v] = u0[v] + dtodx * (sm.Q[v * PT + mp] - sm.Q[v * PT + me]);
     } else if (r.keep) {
         load_cell<PH>(wsrc, off, g, w);
     }
@@ -194,9 +199,12 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     const int me = p * sp + t * st;
     const int i1 = i1_0 + p;
     const bool active = (tid < PT) && (i1 < g.n1);
-    const int s = c0 - 4 + t;                                  // position along the pencil (interior coords)
+    const bool circ = tl.circ;
+    const int s = circ ? t : c0 - 4 + t;                       // position along the pencil (interior coords)
     const long long off = (long long)(g.g_d + (tl.wrap ? wrap(s, g.n_d) : s)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
                           (long long)(g.g2 + i2) * g.s2;
+    const int mp = circ ? p * sp + (t == 0 ? T - 1 : t - 1) * st : me - st;
+    const int mn = circ ? p * sp + (t == T - 1 ? 0 : t + 1) * st : me + st;
     double w[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) w[v] = 0.0;
@@ -204,19 +212,19 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     Roles r;
     r.end = 0;
     r.keep = false;
-    // stage 1 (RK2_1) on tile cells [0, T)
+    // stage 1 (RK2_1) on tile cells [0, T) (circular: every cell)
     r.q = active;
-    r.slope = active && t >= 1 && t < T - 1;
-    r.flux = active && t >= 1 && t < T - 2;
-    r.upd = active && t >= 2 && t < T - 2;
-    rk_stage<PH>(sm, me, st, r, w, uin, uin, off, g, dtodx1, ch, pp, status);
+    r.slope = active && (circ || (t >= 1 && t < T - 1));
+    r.flux = active && (circ || (t >= 1 && t < T - 2));
+    r.upd = active && (circ || (t >= 2 && t < T - 2));
+    rk_stage<PH>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status);
     // stage 2 (RK2_2) on tile cells [2, T-2); u0 is again the sweep's input
-    r.q = active && t >= 2 && t < T - 2;
-    r.slope = active && t >= 3 && t < T - 3;
-    r.flux = active && t >= 3 && t < T - 4;
-    r.upd = active && t >= 4 && t < T - 4;
-    rk_stage<PH>(sm, me, st, r, w, uin, uin, off, g, dtodx2, ch, pp, status);
-    if (r.upd && s < c0 + tl.L && s < g.n_d) {
+    r.q = active && (circ || (t >= 2 && t < T - 2));
+    r.slope = active && (circ || (t >= 3 && t < T - 3));
+    r.flux = active && (circ || (t >= 3 && t < T - 4));
+    r.upd = active && (circ || (t >= 4 && t < T - 4));
+    rk_stage<PH>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status);
+    if (r.upd && (circ || (s < c0 + tl.L && s < g.n_d))) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);
     }
@@ -259,7 +267,8 @@ struct BlockDesc {
 struct WorkItem {
     int block;              // index into the block table
     int i1_0, c0, i2;       // first pencil, first output cell, ortho-2 index
-    int P, L;               // tile of this item (T = L + 8)
+    int P, L;               // tile of this item (T = L + 8, or T = L = n when circ)
+    int circ;               // whole periodic pencil without halo (Tile::circ)
 };
 
 template <class PH, int MAXT, int MINB>
@@ -301,10 +310,11 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
         Tile tl;
         tl.P = w.P;
         tl.L = w.L;
-        tl.T = w.L + 8;
+        tl.T = w.circ ? w.L : w.L + 8;
         tl.xfast = dir == 0;
         tl.halo = 4;
         tl.wrap = b.wrap;
+        tl.circ = w.circ;
         const double dl = b.dl[dir];
         fused_tile<PH>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, (0.5 * dt) / dl, (1.0 * dt) / dl, ch, fac, smem,
                        status);
@@ -363,7 +373,7 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     const bool prev_flux = (t >= 1) && (s >= 1) && ((s - 1 == 0) || (t - 1 >= 1));
     r.upd = valid && s >= 1 && s <= n - 2 && prev_flux && r.flux;
     r.keep = !r.upd && valid && (s == 0 || s == n - 1);        // u1 = u at the pencil ends, then floors
-    rk_stage<PH>(sm, me, st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status);
+    rk_stage<PH>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status);
     if (own) store_cell<PH>(uout, off, g, w);
     flush_status(status, gstatus);
 }

@@ -71,7 +71,10 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     if (P > g.n1) P = g.n1;
     const int var = h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir];
     const int maxt = VAR_T[var];
-    int T = L + 8;
+    tl.wrap = h->connected ? 0 : 1;
+    // a tile as long as a periodic pencil takes it whole, without halo, when it fits
+    tl.circ = (tl.wrap && L == b.n[dir] && b.n[dir] <= maxt) ? 1 : 0;
+    int T = tl.circ ? L : L + 8;
     while (P * T > maxt && P > 1) --P;
     if (P * T > maxt) return fail(h, PK_E_ARG, "fused sweep tile longer than the variant's CTA size");
     tl.P = P;
@@ -79,7 +82,6 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     tl.L = L;
     tl.halo = 4;
     tl.xfast = (dir == 0);
-    tl.wrap = h->connected ? 0 : 1;
     dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
     const size_t smem = 3ull * PH::NV * P * T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;

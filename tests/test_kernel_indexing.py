@@ -29,15 +29,16 @@ def fused_shape(n, d, P, L, maxt):
     G = geom(n, 4, d)
     L = min(L, n[d])
     P = min(P, G["n1"])
-    T = L + 8
+    circ = L == n[d] and n[d] <= maxt            # whole periodic pencil, no halo (Tile::circ)
+    T = L if circ else L + 8
     while P * T > maxt and P > 1:
         P -= 1
     assert P * T <= maxt
-    return G, P, L, T
+    return G, P, L, T, circ
 
 
 def check_fused(n, d, P, L, maxt):
-    G, P, L, T = fused_shape(n, d, P, L, maxt)
+    G, P, L, T, circ = fused_shape(n, d, P, L, maxt)
     PT = P * T
     xfast = d == 0
     covered = set()
@@ -52,10 +53,17 @@ def check_fused(n, d, P, L, maxt):
                     i1 = bx * P + p
                     if i1 >= G["n1"]:
                         continue
-                    s = by * L - 4 + t
+                    s = t if circ else by * L - 4 + t
                     w = s % G["n_d"]
                     off = (G["g_d"] + w) * G["sd"] + (G["g1"] + i1) * G["s1"] + (G["g2"] + bz) * G["s2"]
                     assert 0 <= off < G["plane"]
+                    if circ:
+                        mp = p * sp + ((t - 1) % T) * st
+                        mn = p * sp + ((t + 1) % T) * st
+                        assert 0 <= mp < PT and 0 <= mn < PT
+                        if bz == 0:
+                            covered.add((i1, s))
+                        continue
                     for lo, hi in ((0, T), (2, T - 2)):
                         if lo < t < hi - 1:
                             assert me - st >= 0 and me + st < PT
