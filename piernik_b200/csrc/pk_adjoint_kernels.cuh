@@ -124,14 +124,6 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active
     __syncthreads();
 }
 
-// floor records of both stages of one cell, as stored by k_sweep_fused_rec:
-// bits 0-2 density floors of stage 1 (one per fluid), 3-5 its internal-energy
-// floors, 6-8 and 9-11 the same for stage 2
-PK_DEV unsigned short pack_floors(const FloorRec& r1, const FloorRec& r2)
-{
-    return (unsigned short)(r1.dn | (r1.en << 3) | (r2.dn << 6) | (r2.en << 9));
-}
-
 PK_DEV FloorRec unpack_floors(unsigned short f, int stage)
 {
     const int sh = stage == 1 ? 0 : 6;
@@ -149,50 +141,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused_rec(Geom g, Tile tl,
                                                                int apply_fac, unsigned* __restrict__ gstatus)
 {
     extern __shared__ double smem[];
-    constexpr int NV = PH::NV;
-    const int P = tl.P, T = tl.T, PT = P * T;
-    const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
-    const int tid = threadIdx.x;
-    int p, t;
-    if (tl.xfast) { t = tid % T; p = tid / T; }
-    else { p = tid % P; t = tid / P; }
-    const int spp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
-    const int me = p * spp + t * st;
-    const int i1 = blockIdx.x * P + p;
-    const int c0 = blockIdx.y * tl.L;
-    const int i2 = blockIdx.z;
-    const bool active = (tid < PT) && (i1 < g.n1);
-    const int s = c0 - 4 + t;
-    const long long off = (long long)(g.g_d + wrap(s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
-                          (long long)(g.g2 + i2) * g.s2;
     const double dt = sp->dt;
-    const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
     unsigned status = 0;
-    double w[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) w[v] = 0.0;
-    if (active) load_cell<PH>(uin, off, g, w);
-    FloorRec rec1{0, 0}, rec2{0, 0};
-    Roles r;
-    r.end = 0;
-    r.keep = false;
-    r.q = active;
-    r.slope = active && t >= 1 && t < T - 1;
-    r.flux = active && t >= 1 && t < T - 2;
-    r.upd = active && t >= 2 && t < T - 2;
-    rk_stage<PH, true>(sm, me, me - st, me + st, r, w, uin, uin, off, g, c1, sp->ch, pp, status, &rec1);
-    const bool own = active && t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d;
-    if (own) store_cell<PH>(ustar, off, g, w);
-    r.q = active && t >= 2 && t < T - 2;
-    r.slope = active && t >= 3 && t < T - 3;
-    r.flux = active && t >= 3 && t < T - 4;
-    r.upd = active && t >= 4 && t < T - 4;
-    rk_stage<PH, true>(sm, me, me - st, me + st, r, w, uin, uin, off, g, c2, sp->ch, pp, status, &rec2);
-    if (own) {
-        if (PH::MHD && apply_fac) w[PH::IB + 3] = w[PH::IB + 3] * sp->psi_fac;
-        store_cell<PH>(uout, off, g, w);
-        flags[off] = pack_floors(rec1, rec2);
-    }
+    fused_tile<PH, true>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, (0.5 * dt) / dl,
+                         (1.0 * dt) / dl, sp->ch, apply_fac ? sp->psi_fac : 1.0, smem, status, ustar, flags);
     flush_status(status, gstatus);
 }
 

@@ -180,13 +180,24 @@ struct StepParams {
     double psi_fac;   // glmdamping factor, applied by the last sweep of each triple
 };
 
+// floor records of both stages of one cell, as the recording sweep stores
+// them: bits 0-2 density floors of stage 1 (one per fluid), 3-5 its
+// internal-energy floors, 6-8 and 9-11 the same for stage 2
+PK_DEV unsigned short pack_floors(const FloorRec& r1, const FloorRec& r2)
+{
+    return (unsigned short)(r1.dn | (r1.en << 3) | (r2.dn << 6) | (r2.en << 9));
+}
+
 // One tile of the fused two-stage sweep of a periodic block (uin -> uout):
 // P pencils starting at ortho-1 index i1_0, output cells [c0, c0+L) along the
-// sweep, ortho-2 index i2.  The tile reads a 4-cell halo with periodic wrap.
-template <class PH>
+// sweep, ortho-2 index i2.  The tile reads a 4-cell halo with periodic wrap
+// (or is the whole pencil, Tile::circ).  REC: also store the stage-1 state of
+// the owned cells in ustar and their floor records in flags (the backward
+// pass's recomputation).
+template <class PH, bool REC = false>
 PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
                        const PhysParams& pp, double dtodx1, double dtodx2, double ch, double psi_fac,
-                       double* smem, unsigned& status)
+                       double* smem, unsigned& status, double* ustar = nullptr, unsigned short* flags = nullptr)
 {
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
@@ -217,16 +228,20 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     r.slope = active && (circ || (t >= 1 && t < T - 1));
     r.flux = active && (circ || (t >= 1 && t < T - 2));
     r.upd = active && (circ || (t >= 2 && t < T - 2));
-    rk_stage<PH>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status);
+    FloorRec rec1{0, 0}, rec2{0, 0};
+    rk_stage<PH, REC>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status, &rec1);
+    const bool own = active && (circ || (t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d));
+    if (REC && own) store_cell<PH>(ustar, off, g, w);
     // stage 2 (RK2_2) on tile cells [2, T-2); u0 is again the sweep's input
     r.q = active && (circ || (t >= 2 && t < T - 2));
     r.slope = active && (circ || (t >= 3 && t < T - 3));
     r.flux = active && (circ || (t >= 3 && t < T - 4));
     r.upd = active && (circ || (t >= 4 && t < T - 4));
-    rk_stage<PH>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status);
-    if (r.upd && (circ || (s < c0 + tl.L && s < g.n_d))) {
+    rk_stage<PH, REC>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status, &rec2);
+    if (own) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);
+        if (REC) flags[off] = pack_floors(rec1, rec2);
     }
 }
 

@@ -59,35 +59,45 @@ constexpr int DEF_VARIANT[3] = {0, 0, 0};
 constexpr int DEF_P[3] = {2, 4, 4};
 constexpr int DEF_L[3] = {64, 64, 64};
 
-template <class PH>
-int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out)
+// Tile, grid and variant of the fused sweep along dir (the handle's tuned or
+// default settings; a whole periodic pencil runs without halo when it fits)
+inline int fused_geometry(pk_ctx* h, const Block& b, int dir, const Geom& g, Tile* tl, dim3* grid, int* var_out)
 {
-    if (int rc = set_smem_attr<PH>(h)) return rc;
-    Geom g = make_geom(b, dir);
-    Tile tl;
     int L = h->tileL[dir] > 0 ? h->tileL[dir] : DEF_L[dir];
     if (L > b.n[dir]) L = b.n[dir];
     int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
     if (P > g.n1) P = g.n1;
     const int var = h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir];
     const int maxt = VAR_T[var];
-    tl.wrap = h->connected ? 0 : 1;
-    // a tile as long as a periodic pencil takes it whole, without halo, when it fits
-    tl.circ = (tl.wrap && L == b.n[dir] && b.n[dir] <= maxt) ? 1 : 0;
-    int T = tl.circ ? L : L + 8;
+    tl->wrap = h->connected ? 0 : 1;
+    tl->circ = (tl->wrap && L == b.n[dir] && b.n[dir] <= maxt) ? 1 : 0;
+    const int T = tl->circ ? L : L + 8;
     while (P * T > maxt && P > 1) --P;
     if (P * T > maxt) return fail(h, PK_E_ARG, "fused sweep tile longer than the variant's CTA size");
-    tl.P = P;
-    tl.T = T;
-    tl.L = L;
-    tl.halo = 4;
-    tl.xfast = (dir == 0);
-    dim3 grid((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
-    const size_t smem = 3ull * PH::NV * P * T * sizeof(double);
+    tl->P = P;
+    tl->T = T;
+    tl->L = L;
+    tl->halo = 4;
+    tl->xfast = (dir == 0);
+    *grid = dim3((g.n1 + P - 1) / P, (b.n[dir] + L - 1) / L, g.n2);
+    *var_out = var;
+    return PK_OK;
+}
+
+template <class PH>
+int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out)
+{
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    Geom g = make_geom(b, dir);
+    Tile tl;
+    dim3 grid;
+    int var;
+    if (int rc = fused_geometry(h, b, dir, g, &tl, &grid, &var)) return rc;
+    const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    fused_variant<PH>(var)<<<grid, P * T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir], h->d_step, apply_fac,
-                                                            h->d_status);
+    fused_variant<PH>(var)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir], h->d_step,
+                                                                  apply_fac, h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
@@ -102,27 +112,25 @@ int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
     return PK_OK;
 }
 
-// Tile of the recording forward sweep: the forward sweep's tile along dir,
-// fitted into 256 threads.
-inline int rec_tile(pk_ctx* h, const Block& b, const Geom& g, int dir, Tile* tl)
+template <class PH>
+using RecFn = void (*)(Geom, Tile, const double*, double*, double*, unsigned short*, PhysParams, double,
+                       const StepParams*, int, unsigned*);
+
+template <class PH>
+RecFn<PH> rec_variant(int v)
 {
-    int L = h->tileL[dir] > 0 ? h->tileL[dir] : DEF_L[dir];
-    if (L > 248) L = 248;
-    if (L > b.n[dir]) L = b.n[dir];
-    int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
-    if (P > g.n1) P = g.n1;
-    const int T = L + 8;
-    while (P * T > 256 && P > 1) --P;
-    tl->P = P;
-    tl->T = T;
-    tl->L = L;
-    tl->halo = 4;
-    tl->xfast = dir == 0;
-    return PK_OK;
+    switch (v) {
+    case 0: return k_sweep_fused_rec<PH, 320, 1>;
+    case 1: return k_sweep_fused_rec<PH, 256, 1>;
+    case 2: return k_sweep_fused_rec<PH, 256, 2>;
+    case 3: return k_sweep_fused_rec<PH, 128, 3>;
+    case 4: return k_sweep_fused_rec<PH, 128, 4>;
+    default: return k_sweep_fused_rec<PH, 192, 2>;
+    }
 }
 
-// The forward sweep of the backward pass's recomputation: also stores U* and
-// the floor records (k_sweep_fused_rec)
+// The forward sweep of the backward pass's recomputation, in the forward
+// sweep's tile and variant: also stores U* and the floor records
 template <class PH>
 int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out, double* ustar,
                      unsigned short* flags)
@@ -132,20 +140,21 @@ int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     } else {
         static bool attr = false;
         if (!attr) {
-            PK_CUDA(h, cudaFuncSetAttribute(k_sweep_fused_rec<PH, 256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            220 * 1024));
+            for (int v = 0; v < NVARIANT; ++v)
+                PK_CUDA(h, cudaFuncSetAttribute(rec_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                220 * 1024));
             attr = true;
         }
         Geom g = make_geom(b, dir);
         Tile tl;
-        if (int rc = rec_tile(h, b, g, dir, &tl)) return rc;
-        dim3 grid((g.n1 + tl.P - 1) / tl.P, (b.n[dir] + tl.L - 1) / tl.L, g.n2);
+        dim3 grid;
+        int var;
+        if (int rc = fused_geometry(h, b, dir, g, &tl, &grid, &var)) return rc;
         const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
         std::pair<cudaEvent_t, cudaEvent_t> ev;
         if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-        k_sweep_fused_rec<PH, 256, 1><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, ustar, flags, h->pp,
-                                                                            b.dl[dir], h->d_step, apply_fac,
-                                                                            h->d_status);
+        rec_variant<PH>(var)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, ustar, flags, h->pp, b.dl[dir],
+                                                                    h->d_step, apply_fac, h->d_status);
         PK_CUDA(h, cudaGetLastError());
         if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
         h->launches += 1;
