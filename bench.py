@@ -60,8 +60,10 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--adj-steps", type=int, default=8)
     p.add_argument("--tune-log", default=None)
-    p.add_argument("--workload", default="mhd256", choices=["mhd256", "batched"],
-                   help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks")
+    p.add_argument("--workload", default="mhd256", choices=["mhd256", "batched", "adjoint", "ot-gradient"],
+                   help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks; "
+                        "adjoint: gradient of --steps steps of the MHD block at --n; ot-gradient: the "
+                        "differentiable Orszag-Tang workload (512^2, K = 100) with its FD check")
     p.add_argument("--nblocks", type=int, default=512)
     p.add_argument("--tiles", default=None,
                    help="fix fused-sweep tiles instead of autotuning, e.g. 'x:1,88,3;y:4,56,2;z:4,56,2' (P,L,variant)")
@@ -188,6 +190,12 @@ def adjoint_cost(sim, stream, args, fwd_ms_per_step, barrier, max_over_ranks):
     K = args.adj_steps
     every = max(1, int(round(np.sqrt(K))))
     st0 = sim.time_state
+    # untimed warm-up of the same shape: loads the kernels, allocates the
+    # checkpoints and the recomputation pool the timed gradient reuses
+    sim.grad_forward(K, every)
+    sim.adjoint_set(np.ones(sim.state_shape()))
+    sim.grad_backward()
+    sim.time_state = st0
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     barrier()
     ev[0].record(stream)
@@ -450,10 +458,138 @@ def batched_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def adjoint_arm(args):
+    """Gradient of --steps steps of the MHD turbulence block at --n: the
+    recorded forward, the backward pass and one adjoint sweep per direction,
+    each against the plain forward (also the command the adjoint kernels are
+    profiled with)."""
+    import torch
+    from piernik_b200 import build, problems
+    from piernik_b200.sim import Simulation
+    build.build()
+    setup, u, b, psi = problems.mhd_turbulence(n=args.n, seed=args.seed)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.run(args.warmup)
+    st0 = sim.time_state
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    fwd = e0.elapsed_time(e1) / args.steps
+    sim.time_state = st0
+
+    class _A:
+        adj_steps = args.steps
+    res = adjoint_cost(sim, stream, _A, fwd, torch.cuda.synchronize, lambda x: x)
+    out = {"workload": f"adjoint of {args.steps} MHD steps at {args.n}^3", "forward_ms_per_step": fwd,
+           "adjoint_cost_ratio": res}
+    print(json.dumps(out), flush=True)
+    sim.close()
+
+
+def ot_gradient_arm(args):
+    """C4: the differentiable Orszag-Tang vortex at 512^2 (--n), loss = magnetic
+    energy of the central 128^2 cells after K = --steps steps (default 100
+    when --steps is left at 10), gradient with respect to the relative density
+    perturbation (1e-3 x a seeded unit-rms Gaussian random field, correlation
+    8 cells) through torch.autograd with sqrt(K) checkpointing; checked
+    against central differences along 16 seeded directions at eps = 1e-6 and
+    1e-7 at the dt sequence of the unperturbed run."""
+    import numpy as np
+    import torch
+    from piernik_b200 import build, problems
+    from piernik_b200.autograd import advance, central_magnetic_energy, last_dts, orszag_tang_state
+    from piernik_b200.sim import Simulation
+    build.build()
+    n = args.n if args.n != 256 else 512
+    K = args.steps if args.steps != 10 else 100
+    s = problems.orszag_tang_fields(n)[0]
+    sim = Simulation(s)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    d0 = torch.tensor(1.0e-3 * problems.orszag_tang_perturbation(n, seed=1), device="cuda", requires_grad=True)
+    # plain forward of the same K steps for the cost ratio
+    st_init = sim.time_state
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    with torch.no_grad():
+        x0 = orszag_tang_state(sim, d0.detach())
+    full = torch.zeros(sim.state_shape(), dtype=torch.float64, device="cuda")
+    g = s.guards
+    full[:, :, g[1]:g[1] + n, g[0]:g[0] + n] = x0
+    torch.cuda.synchronize()
+    sim.upload_device(full.data_ptr())
+    e[0].record(stream)
+    sim.run(K)
+    e[1].record(stream)
+    e[1].synchronize()
+    fwd_ms = e[0].elapsed_time(e[1])
+    sim.time_state = st_init
+    # untimed warm-up gradient (loads the kernels, allocates the checkpoints and pool)
+    warm = advance(sim, orszag_tang_state(sim, d0), K)
+    central_magnetic_energy(sim, warm).backward()
+    d0.grad = None
+    sim.time_state = st_init
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t2 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record()
+    out = advance(sim, orszag_tang_state(sim, d0), K)
+    loss = central_magnetic_energy(sim, out)
+    t1.record()
+    loss.backward()
+    t2.record()
+    t2.synchronize()
+    dts = last_dts(out)
+    grad = d0.grad.detach().cpu().numpy()
+    nv, cy = s.nvar, n // 4
+    y0 = (n - cy) // 2
+    dV = float(np.prod(s.dl))
+
+    def central_b(d):
+        with torch.no_grad():
+            o = advance(sim, orszag_tang_state(sim, d), K, dts=dts)
+            return o[nv:nv + 3, 0, y0:y0 + cy, y0:y0 + cy].cpu().numpy()
+
+    rng = np.random.default_rng(21)
+    rows = []
+    for k in range(16):
+        v = problems.gaussian_random_field((n, n), 8.0, rng)
+        vt = torch.tensor(v, device="cuda")
+        ad = float(np.sum(grad * v))
+        row = {"adjoint": ad}
+        for eps in (1.0e-6, 1.0e-7):
+            bp, bm = central_b(d0.detach() + eps * vt), central_b(d0.detach() - eps * vt)
+            fd = float(0.5 * ((bp - bm) * (bp + bm)).sum() * dV / (2 * eps))
+            row[f"fd_{eps:g}"] = fd
+            row[f"rel_{eps:g}"] = abs(ad - fd) / max(abs(fd), 1e-300)
+        rows.append(row)
+    rel6 = [r["rel_1e-06"] for r in rows]
+    rel7 = [r["rel_1e-07"] for r in rows]
+    res = {"workload": f"differentiable Orszag-Tang {n}^2, K = {K}, loss = central {cy}^2 magnetic energy",
+           "forward_ms": fwd_ms, "recorded_forward_plus_loss_ms": t0.elapsed_time(t1),
+           "backward_ms": t1.elapsed_time(t2), "gradient_over_forward": t0.elapsed_time(t2) / fwd_ms,
+           "fd_rel_error_eps1e-6": {"median": float(np.median(rel6)), "max": float(np.max(rel6))},
+           "fd_rel_error_eps1e-7": {"median": float(np.median(rel7)), "max": float(np.max(rel7))},
+           "directions": rows}
+    print(json.dumps(res), flush=True)
+    sim.close()
+
+
 def main():
     args = parse()
     if args.workload == "batched":
         batched_arm(args)
+        return
+    if args.workload == "adjoint":
+        adjoint_arm(args)
+        return
+    if args.workload == "ot-gradient":
+        ot_gradient_arm(args)
         return
     if args.impl == "reference":
         reference_arm(args)

@@ -1445,16 +1445,19 @@ int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt
 {
     if (!h || nsteps < 0 || every < 1) return PK_E_ARG;
     if (int rc = grad_check(h)) return rc;
-    grad_release(h);
     Block& b = h->blocks[0];
+    h->grad_steps.clear();                            // checkpoint buffers of an earlier recording are reused
     h->grad_every = every;
     h->grad_ts0 = h->ts;
     for (int s = 0; s < nsteps; ++s) {
         if (s % every == 0) {
-            double* p;
-            if (int rc = alloc_state(h, b, &p)) return rc;
-            h->grad_ckpt.push_back(p);
-            PK_CUDA(h, cudaMemcpyAsync(p, state(h, b), sizeof(double) * h->nplanes * b.plane,
+            const size_t k = (size_t)(s / every);
+            if (k >= h->grad_ckpt.size()) {
+                double* p;
+                if (int rc = alloc_state(h, b, &p)) return rc;
+                h->grad_ckpt.push_back(p);
+            }
+            PK_CUDA(h, cudaMemcpyAsync(h->grad_ckpt[k], state(h, b), sizeof(double) * h->nplanes * b.plane,
                                        cudaMemcpyDeviceToDevice, h->stream));
         }
         double dt;
