@@ -36,3 +36,43 @@ extern "C" int xchg_plan(int nb, const int* n, const int* g, const long long* of
     }
     return (int)s.size();
 }
+
+// Per-rank split: blocks listed this rank's first (nlocal of them), owner[i]
+// for the rest.  Writes, for peer `peer`, the received (which = 0) or sent
+// (which = 1) segments in their canonical order as records of 12 ints:
+// dst offset (3), lo (3), hi (3) and 3 more: the source offset, folded
+// through the shift into the source's first guard-inclusive cell.
+extern "C" int xchg_peer(int nb, int nlocal, const int* owner, const int* n, const int* g, const long long* off,
+                         const long long* dom, const int* periodic, int peer, int which, long long* out, int max_out)
+{
+    std::vector<pk::XBlock> b(nb);
+    for (int i = 0; i < nb; ++i)
+        for (int d = 0; d < 3; ++d) {
+            b[i].n[d] = n[3 * i + d];
+            b[i].g[d] = g[3 * i + d];
+            b[i].off[d] = off[3 * i + d];
+        }
+    std::vector<pk::XSeg> s, local;
+    std::vector<pk::XPeer> peers;
+    std::string e;
+    if (!pk::build_exchange(b, dom, periodic, s, e)) return -1;
+    std::vector<int> own(owner, owner + nb);
+    pk::split_by_owner(b, own, nlocal, s, local, peers);
+    for (const auto& p : peers) {
+        if (p.rank != peer) continue;
+        const auto& l = which ? p.send : p.recv;
+        if ((int)l.size() > max_out) return -2;
+        for (size_t k = 0; k < l.size(); ++k) {
+            long long* r = out + 12 * k;
+            for (int d = 0; d < 3; ++d) {
+                r[d] = b[l[k].dst].off[d];
+                r[3 + d] = l[k].lo[d];
+                r[6 + d] = l[k].hi[d];
+                // global coordinate of the source cell under dst cell lo: dst base + lo - (dst base - src base - image)
+                r[9 + d] = (b[l[k].dst].off[d] - b[l[k].dst].g[d]) + l[k].lo[d] - l[k].shift[d];
+            }
+        }
+        return (int)l.size();
+    }
+    return 0;
+}

@@ -126,3 +126,37 @@ def test_plan_rejects_overlap_and_escape(lib):
         plan(lib, [((8, 8, 8), (0, 0, 0)), ((8, 8, 8), (4, 0, 0))], (16, 8, 8), (1, 1, 1))
     with pytest.raises(ValueError, match="leaves the domain"):
         plan(lib, [((8, 8, 8), (12, 0, 0))], (16, 8, 8), (1, 1, 1))
+
+
+def peer_lists(lib, blocks, owners, rank, peer, which, dom, periodic, g=4):
+    """Rank `rank`'s view: its blocks first, then the others with owners."""
+    order = [i for i in range(len(blocks)) if owners[i] == rank] + [i for i in range(len(blocks)) if owners[i] != rank]
+    nl = sum(1 for o in owners if o == rank)
+    bl = [blocks[i] for i in order]
+    own = [(-1 if owners[i] == rank else owners[i]) for i in order]
+    nb = len(bl)
+    n = (C.c_int * (3 * nb))(*[x for b in bl for x in b[0]])
+    gg = (C.c_int * (3 * nb))(*[(g if b[0][d] > 1 else 0) for b in bl for d in range(3)])
+    off = (C.c_longlong * (3 * nb))(*[x for b in bl for x in b[1]])
+    ow = (C.c_int * nb)(*own)
+    out = (C.c_longlong * (12 * 4096))()
+    k = lib.xchg_peer(nb, nl, ow, n, gg, off, (C.c_longlong * 3)(*dom), (C.c_int * 3)(*[int(p) for p in periodic]),
+                      peer, which, out, 4096)
+    assert k >= 0
+    return [tuple(out[12 * i:12 * i + 12]) for i in range(k)]
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_peer_order_agrees_between_ranks(lib, nranks):
+    """What rank s sends to rank r is what r receives from s, in the same
+    order, although each rank numbers the blocks differently."""
+    lib.xchg_peer.restype = C.c_int
+    blocks, dom = tiling([6, 9, 5], [5, 7], [8, 4])
+    owners = [i % nranks for i in range(len(blocks))]
+    for r in range(nranks):
+        for s in range(nranks):
+            if r == s:
+                continue
+            recv = peer_lists(lib, blocks, owners, r, s, 0, dom, (1, 1, 1))
+            send = peer_lists(lib, blocks, owners, s, r, 1, dom, (1, 1, 1))
+            assert recv == send and len(recv) > 0
