@@ -128,6 +128,7 @@ def lib():
         L.o_nvar.argtypes = [P]
         L.o_run_multi.argtypes = [P, C.POINTER(B), C.c_int, S, C.c_int]
         L.o_set_threads.argtypes = [C.c_int]
+        L.o_run_fixed.argtypes = [P, B, S, C.POINTER(C.c_double), C.c_int]
         L.o_cfl_max.argtypes = [P]
         L.o_cfl_max.restype = C.c_double
         L.o_get_threads.restype = C.c_int
@@ -226,6 +227,11 @@ class OracleBlock:
 
     def run(self, nsteps):
         return lib().o_run(C.byref(self.cfg), C.byref(self.blk), C.byref(self.state), nsteps)
+
+    def run_fixed(self, dts):
+        """fluid_update at the prescribed dt sequence (no CFL)."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        return lib().o_run_fixed(C.byref(self.cfg), C.byref(self.blk), C.byref(self.state), _ptr(d), len(d))
 
     def glm_fac(self, dt, ch):
         return lib().o_glm_fac(C.byref(self.cfg), C.byref(self.blk), dt, ch)

@@ -1046,6 +1046,20 @@ int o_run(const o_cfg *cfg, o_block *blk, o_state *st, int nsteps)
     return 0;
 }
 
+/* fluid_update_full at a prescribed dt sequence (nsteps values): the map the
+ * differentiable path takes the derivative of */
+int o_run_fixed(const o_cfg *cfg, o_block *blk, o_state *st, const double *dts, int nsteps)
+{
+    for (int s = 0; s < nsteps; ++s) {
+        st->dt_old = st->dt;
+        st->dt = dts[s];
+        int rc = o_fluid_update(cfg, blk, st);
+        if (rc) return rc;
+        st->nstep += 1;
+    }
+    return 0;
+}
+
 void o_set_threads(int n)
 {
 #ifdef _OPENMP

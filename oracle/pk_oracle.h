@@ -78,6 +78,7 @@ typedef struct o_state {         /* the reference's global time-step state */
 
 int    o_nvar(const o_cfg *cfg);
 double o_cfl_max(const o_cfg *cfg);
+int    o_run_fixed(const o_cfg *cfg, o_block *blk, o_state *st, const double *dts, int nsteps);
 void   o_extents(const o_block *blk, int ext[3], int g[3]);
 
 /* one stage of solve_cg_riemann on one block (solve_cg_riemann.F90:68-233,241-307) */
