@@ -75,7 +75,14 @@ typedef struct pk_config {
     int32_t cflcontrol;
     double cfl_max, dt_shrink;
     int32_t max_redostep_attempts;
+    /* interpol_str (global.F90:220): PK_INTERP_LINEAR or PK_INTERP_WENO3, and
+     * w_epsilon (:255) for WENO3 */
+    int32_t interpolation;
+    double w_epsilon;
 } pk_config;
+
+#define PK_INTERP_LINEAR 0
+#define PK_INTERP_WENO3  1
 
 #define PK_CFL_NONE 0           /* no check */
 #define PK_CFL_WARN 1           /* stepcfl computed each step (timestep.F90:317-360), no retry */

@@ -53,6 +53,8 @@ class OCfg(C.Structure):
         ("cfl_max", C.c_double),
         ("dt_shrink", C.c_double),
         ("max_redostep_attempts", C.c_int),
+        ("interpolation", C.c_int),
+        ("w_epsilon", C.c_double),
     ]
 
 
@@ -167,6 +169,8 @@ def make_cfg(setup) -> OCfg:
     c.cfl_max = setup.cfl_max
     c.dt_shrink = setup.dt_shrink
     c.max_redostep_attempts = setup.max_redostep_attempts
+    c.interpolation = {"linear": 0, "weno3": 1}[setup.interpolation]
+    c.w_epsilon = setup.w_epsilon
     return c
 
 

@@ -194,6 +194,40 @@ static void o_linear(int kind, int n, int ncol, const double *q, double *ql, dou
     }
 }
 
+/* interpolations.F90:210-337 (weno3) for ncol columns of length n; ql, qr are
+ * (n-1, ncol).  Yamaleev & Carpenter (2009), Eqs. 14-22, with constant
+ * w_epsilon; ql(1) = q(1) and qr(n-1) = q(n) at the pencil ends. */
+static void o_weno3(int n, int ncol, double weps, const double *q, double *ql, double *qr)
+{
+    const double d0 = 2.0 / 3.0, d1 = 1.0 / 3.0;            /* Eq. 19: twot, onet (constants.F90:65-66) */
+    for (int c = 0; c < ncol; ++c) {
+        const double *qc = q + (size_t)c * n;
+        double *l = ql + (size_t)c * (n - 1), *r = qr + (size_t)c * (n - 1);
+        for (int i = 1; i < n - 1; ++i) {
+            double beta0 = (qc[i + 1] - qc[i]) * (qc[i + 1] - qc[i]);                  /* Eq. 20 */
+            double beta1 = (qc[i] - qc[i - 1]) * (qc[i] - qc[i - 1]);
+            double t = (qc[i + 1] - 2.0 * qc[i]) + qc[i - 1];                         /* Eq. 22 */
+            double tau = t * t;
+            double alpha0 = d0 * (1.0 + tau / (weps + beta0));                         /* Eq. 21 */
+            double alpha1 = d1 * (1.0 + tau / (weps + beta1));
+            double w0 = alpha0 / (alpha0 + alpha1);                                    /* Eq. 18 */
+            double w1 = alpha1 / (alpha0 + alpha1);
+            double flux0 = 0.5 * (qc[i] + qc[i + 1]);                                  /* Eq. 15 */
+            double flux1 = 0.5 * (-qc[i - 1] + 3.0 * qc[i]);
+            l[i] = w0 * flux0 + w1 * flux1;                                            /* Eq. 14 */
+            alpha0 = d0 * (1.0 + tau / (weps + beta1));
+            alpha1 = d1 * (1.0 + tau / (weps + beta0));
+            w0 = alpha0 / (alpha0 + alpha1);
+            w1 = alpha1 / (alpha0 + alpha1);
+            flux0 = 0.5 * (qc[i] + qc[i - 1]);
+            flux1 = 0.5 * (-qc[i + 1] + 3.0 * qc[i]);
+            r[i - 1] = w0 * flux0 + w1 * flux1;
+        }
+        l[0] = qc[0];                                                                  /* "Q&D: fix for FPE" */
+        r[n - 2] = qc[n - 1];
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Riemann solvers                                                     */
 /* ------------------------------------------------------------------ */
@@ -541,8 +575,13 @@ static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx
 
     /* interpol (interpolations.F90:112-132) */
     o_utoq(L, n, w->u1, mag ? w->b1 : NULL, w->q);
-    o_linear(cfg->limiter, n, nv, w->q, w->ql, w->qr, w->dq);
-    if (mag) o_linear(cfg->limiter_b, n, 4, w->b1, w->bl, w->br, w->dq);
+    if (cfg->interpolation == 1) {
+        o_weno3(n, nv, cfg->w_epsilon, w->q, w->ql, w->qr);
+        if (mag) o_weno3(n, 4, cfg->w_epsilon, w->b1, w->bl, w->br);
+    } else {
+        o_linear(cfg->limiter, n, nv, w->q, w->ql, w->qr, w->dq);
+        if (mag) o_linear(cfg->limiter_b, n, 4, w->b1, w->bl, w->br, w->dq);
+    }
 
     /* riemann_wrap / riemann_wrap_u (hlld.F90:62-155) */
     if (mag) {

@@ -50,6 +50,8 @@ typedef struct o_cfg {
     int cflcontrol;              /* O_CFL_NONE / O_CFL_WARN / O_CFL_REDO (global.F90:218, timestep.F90:73-90) */
     double cfl_max, dt_shrink;   /* global.F90:233,245 (cfl_max sanitized as :304 on use) */
     int max_redostep_attempts;   /* global.F90:258 */
+    int interpolation;           /* 0 linear, 1 weno3 (interpol_str, global.F90:220) */
+    double w_epsilon;            /* global.F90:255 */
 } o_cfg;
 
 #define O_CFL_NONE 0

@@ -67,6 +67,8 @@ class PkConfig(C.Structure):
         ("cfl_max", C.c_double),
         ("dt_shrink", C.c_double),
         ("max_redostep_attempts", C.c_int32),
+        ("interpolation", C.c_int32),
+        ("w_epsilon", C.c_double),
     ]
 
 

@@ -51,6 +51,8 @@ class Setup:
     cfl_max: float = 0.9             # :233
     dt_shrink: float = 0.5           # :245
     max_redostep_attempts: int = 10  # :258
+    interpolation: str = "linear"    # interpol_str (:220): linear or weno3
+    w_epsilon: float = 1.0e-10       # :255
     skip_sweep: Tuple[bool, bool, bool] = (False, False, False)
     # END_CONTROL
     tend: float = DBL_HUGE
@@ -83,6 +85,8 @@ class Setup:
             raise ValueError("CFL value should be >0. and <=1.")      # global.F90:303
         if self.integration_order not in (1, 2):
             raise ValueError("integration_order must be 1 or 2")
+        if self.interpolation not in ("linear", "weno3"):
+            raise ValueError(f"interpol_str {self.interpolation!r}: this library implements linear and weno3")
         if self.cflcontrol not in ("none", "warn", "redo", "repeat"):
             raise ValueError(f"cflcontrol {self.cflcontrol!r}: this library implements none, warn and redo")
         kinds = [k for k, _ in self.fluids]

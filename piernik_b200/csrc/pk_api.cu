@@ -534,11 +534,14 @@ void pk_config_default(pk_config* c)
     c->cfl_max = 0.9;                  // :233
     c->dt_shrink = 0.5;                // :245
     c->max_redostep_attempts = 10;     // :258
+    c->interpolation = PK_INTERP_LINEAR;   // :220
+    c->w_epsilon = 1.0e-10;            // :255
 }
 
 int pk_create(const pk_config* cfg, pk_handle* out)
 {
-    if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_REDO || cfg->max_redostep_attempts < 0))
+    if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_REDO || cfg->max_redostep_attempts < 0 ||
+                cfg->interpolation < PK_INTERP_LINEAR || cfg->interpolation > PK_INTERP_WENO3))
         return PK_E_ARG;
     if (!cfg || !out) return PK_E_ARG;
     *out = nullptr;
@@ -579,6 +582,8 @@ int pk_create(const pk_config* cfg, pk_handle* out)
     h->pp.disallow_negatives = c.disallow_negatives;
     h->pp.lim = c.limiter;
     h->pp.limb = c.limiter_b;
+    h->pp.weno3 = c.interpolation == PK_INTERP_WENO3;
+    h->pp.w_epsilon = c.w_epsilon;
     std::memset(&h->ts, 0, sizeof(h->ts));
     h->ts.dt_old = -1.0;
     h->ts.dt_cur_shrink = 1.0;                        // global.F90:571
@@ -1315,6 +1320,8 @@ int grad_check(pk_ctx* h)
         return fail(h, PK_E_UNSUPPORTED, "the differentiable path runs on one block of one rank");
     if (!fused_ok(h)) return fail(h, PK_E_UNSUPPORTED, "the differentiable path needs RK2 and periodic boundaries");
     if (h->cfg.nfluids != 1) return fail(h, PK_E_UNSUPPORTED, "the differentiable path is built for one fluid");
+    if (h->cfg.interpolation != PK_INTERP_LINEAR)
+        return fail(h, PK_E_UNSUPPORTED, "the differentiable path differentiates the linear (limited) reconstruction");
     int dirs[3], nd;
     step_dirs(h, dirs, &nd);
     if (nd == 0) return fail(h, PK_E_UNSUPPORTED, "the differentiable path needs at least one swept direction");

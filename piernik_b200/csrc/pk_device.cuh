@@ -95,6 +95,8 @@ struct PhysParams {
     double smalld, smallei;
     int use_smalld, use_smallei, disallow_negatives;
     int lim, limb;      // flimiter, blimiter
+    int weno3;          // interpol_str = 'weno3': WENO3 face states instead of limited linear ones
+    double w_epsilon;   // WENO3 weight regulariser (global.F90:255)
 };
 
 // status bits written by kernels (never traps)
@@ -148,6 +150,30 @@ PK_PHYS double slope_interior(int lim, double dl, double dr)
     if (lim == L_MONCEN) return (s * f_min(f_min(2.0 * fabs(dl), 2.0 * fabs(dr)), 0.5 * fabs(dl + dr))) * 0.5;  // :185
     const double m = (fabs(dl) > fabs(dr)) ? f_min(fabs(dl), fabs(2.0 * dr)) : f_min(fabs(2.0 * dl), fabs(dr)); // :211-212
     return (s * 0.5) * m;
+}
+
+// WENO3 face states of cell c from q(c-1), q(c), q(c+1) (interpolations.F90:
+// 210-337, Yamaleev & Carpenter 2009): ql = the left state of the right face,
+// qr = the right state of the left face, in the reference's operation order.
+PK_PHYS void weno3_faces(double qm, double qc, double qp, double weps, double& ql, double& qr)
+{
+    const double d0 = 2.0 / 3.0, d1 = 1.0 / 3.0;                              // Eq. 19 (twot, onet)
+    const double b0 = (qp - qc) * (qp - qc);                                    // Eq. 20
+    const double b1 = (qc - qm) * (qc - qm);
+    const double tt = ((qp - 2.0 * qc) + qm);                                   // Eq. 22
+    const double tau = tt * tt;
+    double a0 = d0 * (1.0 + tau / (weps + b0));                                 // Eq. 21
+    double a1 = d1 * (1.0 + tau / (weps + b1));
+    double w0 = a0 / (a0 + a1), w1 = a1 / (a0 + a1);                            // Eq. 18
+    double f0 = 0.5 * (qc + qp), f1 = 0.5 * (-qm + 3.0 * qc);                   // Eq. 15
+    ql = w0 * f0 + w1 * f1;                                                     // Eq. 14
+    a0 = d0 * (1.0 + tau / (weps + b1));                                        // the mirrored stencil
+    a1 = d1 * (1.0 + tau / (weps + b0));
+    w0 = a0 / (a0 + a1);
+    w1 = a1 / (a0 + a1);
+    f0 = 0.5 * (qc + qm);
+    f1 = 0.5 * (-qp + 3.0 * qc);
+    qr = w0 * f0 + w1 * f1;
 }
 
 PK_PHYS double slope_end(int lim, double d)

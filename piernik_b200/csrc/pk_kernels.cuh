@@ -128,7 +128,16 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
         for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = q[v];
     }
     __syncthreads();
-    if (r.slope) {
+    if (r.slope && pp.weno3) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const double qc = sm.Q[v * PT + me];
+            double l = qc, rr = qc;                           // pencil ends: ql(1) = q(1), qr(n-1) = q(n)
+            if (r.end == 0) weno3_faces(sm.Q[v * PT + mp], qc, sm.Q[v * PT + mn], pp.w_epsilon, l, rr);
+            sm.L[v * PT + me] = l;
+            sm.R[v * PT + me] = rr;
+        }
+    } else if (r.slope) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             const int lim = (PH::MHD && v >= PH::IB) ? pp.limb : pp.lim;

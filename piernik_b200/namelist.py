@@ -176,10 +176,18 @@ def read_problem_par(text: str, cmdline: Optional[str] = None, setup: Optional[S
     if "skip_sweep" in ns:
         v = ns["skip_sweep"]
         kw["skip_sweep"] = tuple(bool(x) for x in (v if isinstance(v, list) else [v] * 3))
-    for key in ("solver_str", "interpol_str", "divb_0"):
+    if "interpol_str" in ns:
+        val = str(ns["interpol_str"]).strip().lower()
+        names = {"linear": "linear", "lin": "linear", "1": "linear", "weno3": "weno3", "wo3": "weno3", "2": "weno3"}
+        if val not in names:
+            raise ValueError(f"interpol_str={val!r} is outside the sweep path this library implements")
+        kw["interpolation"] = names[val]                  # interpolations.F90:set_interpolations
+    if "w_epsilon" in ns:
+        kw["w_epsilon"] = float(ns["w_epsilon"])
+    for key in ("solver_str", "divb_0"):
         if key in ns:
             val = str(ns[key]).strip().lower()
-            ok = {"solver_str": ("", "riemann", "riemann_split"), "interpol_str": ("linear", "lin", "1"),
+            ok = {"solver_str": ("", "riemann", "riemann_split"),
                   "divb_0": ("hdc", "glm", "divergence cleaning")}[key]
             if val not in ok:
                 raise ValueError(f"{key}={val!r} is outside the sweep path this library implements")

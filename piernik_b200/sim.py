@@ -68,6 +68,8 @@ def make_config(setup: Setup) -> L.PkConfig:
     c.cfl_max = setup.cfl_max
     c.dt_shrink = setup.dt_shrink
     c.max_redostep_attempts = setup.max_redostep_attempts
+    c.interpolation = {"linear": 0, "weno3": 1}[setup.interpolation]
+    c.w_epsilon = setup.w_epsilon
     return c
 
 

@@ -6,7 +6,13 @@ from piernik_b200 import problems
 
 
 def setup_for(phys: str, n=(12, 10, 8), lim="vanleer", limb=None, bnd=None, **kw) -> Setup:
+    """lim = 'weno3' selects interpol_str = 'weno3' (the limiters then play no part)."""
     mag = phys == "mhd"
+    if lim == "weno3":
+        kw.setdefault("interpolation", "weno3")
+        lim = "vanleer"
+    if limb == "weno3":
+        limb = None
     s = Setup(n=tuple(n), fluids=[("ion", 5.0 / 3.0)] if mag else [("neu", 1.4)], magnetic=mag,
               limiter=lim, limiter_b=limb or lim, xmin=(0.0, 0.0, 0.0),
               xmax=(n[0] * 0.1, n[1] * 0.1, n[2] * 0.1), **kw)

@@ -15,7 +15,7 @@ from piernik_b200.sim import Simulation
 
 pytestmark = pytest.mark.gpu
 
-LIMS = ["vanleer", "minmod", "moncen", "superbee"]
+LIMS = ["vanleer", "minmod", "moncen", "superbee", "weno3"]   # weno3: interpol_str = weno3
 
 
 def both(setup, seed=0):
@@ -265,3 +265,28 @@ def test_cfl_redo_matches_oracle(gpu_lib, oracle_lib, cfl):
     assert (st.redone > 0) == (cfl == 0.9)
     compare(ob, sim, f"redo cfl={cfl}")
     sim.close()
+
+
+@pytest.mark.parametrize("recipe", ["mhd", "ot", "batched", "sedov"])
+def test_weno3_runs_bitexact(gpu_lib, oracle_lib, recipe):
+    """interpol_str = 'weno3' (interpolations.F90:210-337) on whole runs:
+    fused single block (MHD turbulence, 2D Orszag-Tang), the batched sweep
+    over uneven 3-fluid blocks, and the Sedov blast with outflow boundaries
+    (per-stage path with pencil ends)."""
+    if recipe == "batched":
+        data = problems.batched_blocks(nblocks=5, seed=9, sizes=(8, 12, 16), n0=16)
+        data = [(s.replace(interpolation="weno3"), u, b, psi) for s, u, b, psi in data]
+        _multi(data, 3)
+        return
+    if recipe == "mhd":
+        setup, u, b, psi = problems.mhd_turbulence(n=20, seed=5)
+    elif recipe == "ot":
+        setup, u, b, psi = problems.orszag_tang(n=32, seed=2)
+    else:
+        setup, u, b, psi = problems.sedov(n=20)
+        setup = setup.replace(bnd=((BND_OUT, BND_OUT),) * 3)
+    setup = setup.replace(interpolation="weno3")
+    ob, sim = run_pair(setup, u, b, psi, 6)
+    st = sim.time_state
+    assert st.t == ob.state.t and st.dt == ob.state.dt
+    compare(ob, sim, f"weno3 {recipe}")

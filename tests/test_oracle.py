@@ -15,7 +15,7 @@ import oracle
 from helpers import assert_bitexact, interior, random_state, setup_for
 from piernik_b200 import problems
 
-LIMS = ["vanleer", "minmod", "moncen", "superbee"]
+LIMS = ["vanleer", "minmod", "moncen", "superbee", "weno3"]   # weno3: interpol_str = weno3
 
 
 def totals(setup, ob):
