@@ -333,7 +333,7 @@ int build_batch(pk_ctx* h)
         PK_CUDA(h, cudaMemcpyAsync(h->d_desc[p], desc.data(), sizeof(BlockDesc) * nb, cudaMemcpyHostToDevice, h->stream));
         PK_CUDA(h, cudaStreamSynchronize(h->stream));   // desc is reused for the other parity
     }
-    const int threads = VAR_T[h->batch_variant];
+    const int threads = VAR_T[h->pp.weno3 ? W3_VARIANT : h->batch_variant];
     for (int dir = 0; dir < 3; ++dir) {
         BatchList& bl = h->batch[dir];
         bl.host.clear();

@@ -17,10 +17,11 @@ namespace pk {
 // the register budget the compiler may use is 65536 / (threads * CTAs);
 // tighter budgets trade spills for resident warps.  The autotuner picks one
 // per direction.
-constexpr int NVARIANT = 6;
-constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192};
-constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2};
-constexpr int STAGE_MAXT = 320;        // threads per CTA of the stage kernel
+constexpr int NVARIANT = 7;
+constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512};
+constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1};
+constexpr int STAGE_MAXT = 320;
+constexpr int W3_VARIANT = 2;          // interpol_str = 'weno3' runs this launch-bound variant only        // threads per CTA of the stage kernel
 
 struct Block {
     int n[3], g[3], ext[3];

@@ -114,7 +114,9 @@ struct Smem {
 //   me, mp, mn   this cell's slot in the shared planes and its previous / next
 //                neighbour's along the pencil (me -/+ the pencil stride, or the
 //                wrapped slot in a circular whole-pencil tile)
-template <class PH, bool REC = false>
+//   W3     interpol_str = 'weno3' face states (a compile-time choice, so that the
+//          limited-linear kernels carry no WENO3 code)
+template <class PH, bool REC = false, bool W3 = false>
 PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, double (&w)[PH::NV], const double* u0src,
                      const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
                      const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr)
@@ -128,7 +130,8 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
         for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = q[v];
     }
     __syncthreads();
-    if (r.slope && pp.weno3) {
+    if constexpr (W3) {
+        if (r.slope) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             const double qc = sm.Q[v * PT + me];
@@ -136,6 +139,7 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
             if (r.end == 0) weno3_faces(sm.Q[v * PT + mp], qc, sm.Q[v * PT + mn], pp.w_epsilon, l, rr);
             sm.L[v * PT + me] = l;
             sm.R[v * PT + me] = rr;
+        }
         }
     } else if (r.slope) {
 #pragma unroll
@@ -203,7 +207,7 @@ PK_DEV unsigned short pack_floors(const FloorRec& r1, const FloorRec& r2)
 // (or is the whole pencil, Tile::circ).  REC: also store the stage-1 state of
 // the owned cells in ustar and their floor records in flags (the backward
 // pass's recomputation).
-template <class PH, bool REC = false>
+template <class PH, bool REC = false, bool W3 = false>
 PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
                        const PhysParams& pp, double dtodx1, double dtodx2, double ch, double psi_fac,
                        double* smem, unsigned& status, double* ustar = nullptr, unsigned short* flags = nullptr)
@@ -238,7 +242,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     r.flux = active && (circ || (t >= 1 && t < T - 2));
     r.upd = active && (circ || (t >= 2 && t < T - 2));
     FloorRec rec1{0, 0}, rec2{0, 0};
-    rk_stage<PH, REC>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status, &rec1);
+    rk_stage<PH, REC, W3>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status, &rec1);
     const bool own = active && (circ || (t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d));
     if (REC && own) store_cell<PH>(ustar, off, g, w);
     // stage 2 (RK2_2) on tile cells [2, T-2); u0 is again the sweep's input
@@ -246,7 +250,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     r.slope = active && (circ || (t >= 3 && t < T - 3));
     r.flux = active && (circ || (t >= 3 && t < T - 4));
     r.upd = active && (circ || (t >= 4 && t < T - 4));
-    rk_stage<PH, REC>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status, &rec2);
+    rk_stage<PH, REC, W3>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status, &rec2);
     if (own) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);
@@ -258,7 +262,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
 // Fused two-stage sweep of one periodic block.
 // grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2.
 // -------------------------------------------------------------------------
-template <class PH, int MAXT, int MINB>
+template <class PH, int MAXT, int MINB, bool W3 = false>
 __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
                                                            double* __restrict__ uout, PhysParams pp, double dl,
                                                            const StepParams* __restrict__ sp, int apply_fac,
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, con
     const double dtodx1 = (0.5 * dt) / dl;        // rk_coef(RK2_1) * dt / cg%dl(ddim)
     const double dtodx2 = (1.0 * dt) / dl;        // rk_coef(RK2_2) * dt / cg%dl(ddim)
     unsigned status = 0;
-    fused_tile<PH>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, dtodx1, dtodx2, sp->ch,
+    fused_tile<PH, false, W3>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, dtodx1, dtodx2, sp->ch,
                    apply_fac ? sp->psi_fac : 1.0, smem, status);
     flush_status(status, gstatus);
 }
@@ -295,7 +299,7 @@ struct WorkItem {
     int circ;               // whole periodic pencil without halo (Tile::circ)
 };
 
-template <class PH, int MAXT, int MINB>
+template <class PH, int MAXT, int MINB, bool W3 = false>
 __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* __restrict__ blocks,
                                                              const WorkItem* __restrict__ items, int nitems, int dir,
                                                              PhysParams pp, const StepParams* __restrict__ sp,
@@ -340,7 +344,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
         tl.wrap = b.wrap;
         tl.circ = w.circ;
         const double dl = b.dl[dir];
-        fused_tile<PH>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, (0.5 * dt) / dl, (1.0 * dt) / dl, ch, fac, smem,
+        fused_tile<PH, false, W3>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, (0.5 * dt) / dl, (1.0 * dt) / dl, ch, fac, smem,
                        status);
     }
     flush_status(status, gstatus);
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
 // uin and uout may alias only when one chunk covers the whole pencil (every
 // load of a pencil then precedes every store of it, within one CTA).
 // -------------------------------------------------------------------------
-template <class PH, int MAXT>
+template <class PH, int MAXT, bool W3 = false>
 __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* uin, double* uout,
                                                double* uh, PhysParams pp, int first, double dtodx, double ch,
                                                unsigned* __restrict__ gstatus)
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     const bool prev_flux = (t >= 1) && (s >= 1) && ((s - 1 == 0) || (t - 1 >= 1));
     r.upd = valid && s >= 1 && s <= n - 2 && prev_flux && r.flux;
     r.keep = !r.upd && valid && (s == 0 || s == n - 1);        // u1 = u at the pencil ends, then floors
-    rk_stage<PH>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status);
+    rk_stage<PH, false, W3>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status);
     if (own) store_cell<PH>(uout, off, g, w);
     flush_status(status, gstatus);
 }

@@ -15,28 +15,32 @@ using BatchedFn = void (*)(const BlockDesc*, const WorkItem*, int, int, PhysPara
                            unsigned*);
 
 template <class PH>
-FusedFn<PH> fused_variant(int v)
+FusedFn<PH> fused_variant(int v, bool w3 = false)
 {
+    if (w3) return k_sweep_fused<PH, 256, 2, true>;
     switch (v) {
     case 0: return k_sweep_fused<PH, 320, 1>;
     case 1: return k_sweep_fused<PH, 256, 1>;
     case 2: return k_sweep_fused<PH, 256, 2>;
     case 3: return k_sweep_fused<PH, 128, 3>;
     case 4: return k_sweep_fused<PH, 128, 4>;
-    default: return k_sweep_fused<PH, 192, 2>;
+    case 5: return k_sweep_fused<PH, 192, 2>;
+    default: return k_sweep_fused<PH, 512, 1>;
     }
 }
 
 template <class PH>
-BatchedFn<PH> batched_variant(int v)
+BatchedFn<PH> batched_variant(int v, bool w3 = false)
 {
+    if (w3) return k_sweep_batched<PH, 256, 2, true>;
     switch (v) {
     case 0: return k_sweep_batched<PH, 320, 1>;
     case 1: return k_sweep_batched<PH, 256, 1>;
     case 2: return k_sweep_batched<PH, 256, 2>;
     case 3: return k_sweep_batched<PH, 128, 3>;
     case 4: return k_sweep_batched<PH, 128, 4>;
-    default: return k_sweep_batched<PH, 192, 2>;
+    case 5: return k_sweep_batched<PH, 192, 2>;
+    default: return k_sweep_batched<PH, 512, 1>;
     }
 }
 
@@ -50,6 +54,12 @@ int set_smem_attr(pk_ctx* h)
             PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         }
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
         done = true;
     }
     return PK_OK;
@@ -67,7 +77,7 @@ inline int fused_geometry(pk_ctx* h, const Block& b, int dir, const Geom& g, Til
     if (L > b.n[dir]) L = b.n[dir];
     int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
     if (P > g.n1) P = g.n1;
-    const int var = h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir];
+    const int var = h->pp.weno3 ? W3_VARIANT : (h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir]);
     const int maxt = VAR_T[var];
     tl->wrap = h->connected ? 0 : 1;
     tl->circ = (tl->wrap && L == b.n[dir] && b.n[dir] <= maxt) ? 1 : 0;
@@ -96,8 +106,8 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    fused_variant<PH>(var)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir], h->d_step,
-                                                                  apply_fac, h->d_status);
+    fused_variant<PH>(var, h->pp.weno3)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir],
+                                                                               h->d_step, apply_fac, h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
@@ -125,7 +135,8 @@ RecFn<PH> rec_variant(int v)
     case 2: return k_sweep_fused_rec<PH, 256, 2>;
     case 3: return k_sweep_fused_rec<PH, 128, 3>;
     case 4: return k_sweep_fused_rec<PH, 128, 4>;
-    default: return k_sweep_fused_rec<PH, 192, 2>;
+    case 5: return k_sweep_fused_rec<PH, 192, 2>;
+    default: return k_sweep_fused_rec<PH, 512, 1>;
     }
 }
 
@@ -244,7 +255,7 @@ int launch_batched(pk_ctx* h, int dir, int apply_fac, unsigned* counter)
     if (int rc = set_smem_attr<PH>(h)) return rc;
     BatchList& bl = h->batch[dir];
     if (bl.n == 0) return PK_OK;
-    const int var = h->batch_variant;
+    const int var = h->pp.weno3 ? W3_VARIANT : h->batch_variant;
     int maxP = 1;
     for (const auto& w : bl.host) maxP = (w.P * (w.L + 8) > maxP) ? w.P * (w.L + 8) : maxP;
     const int threads = VAR_T[var];
@@ -252,14 +263,15 @@ int launch_batched(pk_ctx* h, int dir, int apply_fac, unsigned* counter)
     int dev = 0, nsm = 0, per_sm = 0;
     PK_CUDA(h, cudaGetDevice(&dev));
     PK_CUDA(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_variant<PH>(var), threads, smem));
+    PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_variant<PH>(var, h->pp.weno3), threads,
+                                                             smem));
     if (per_sm < 1) return fail(h, PK_E_ARG, "batched sweep tile does not fit on an SM");
     int grid = nsm * per_sm;
     if (grid > bl.n) grid = bl.n;
     PK_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream));
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    batched_variant<PH>(var)<<<grid, threads, smem, h->stream>>>(h->d_desc[h->cur], bl.dev, bl.n, dir, h->pp,
+    batched_variant<PH>(var, h->pp.weno3)<<<grid, threads, smem, h->stream>>>(h->d_desc[h->cur], bl.dev, bl.n, dir, h->pp,
                                                                  h->d_step, apply_fac, counter, h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
@@ -297,8 +309,12 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double c
     const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    k_stage<PH, STAGE_MAXT><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx, ch,
-                                                                   h->d_status);
+    if (h->pp.weno3)
+        k_stage<PH, STAGE_MAXT, true><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx,
+                                                                         ch, h->d_status);
+    else
+        k_stage<PH, STAGE_MAXT><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx, ch,
+                                                                       h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;

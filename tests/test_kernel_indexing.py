@@ -13,7 +13,7 @@ import pytest
 ORTHO1 = [1, 0, 0]
 ORTHO2 = [2, 2, 1]
 STAGE_MAXT = 320
-VARIANT_T = [320, 256, 256, 128, 128, 192]
+VARIANT_T = [320, 256, 256, 128, 128, 192, 512]
 
 
 def geom(n, nb, d):
