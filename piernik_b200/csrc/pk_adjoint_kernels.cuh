@@ -35,17 +35,19 @@ struct AdjSmem {
 
 // out = D'(V)^T mu for the tile: V valid on tile cells [va, vb), mu valid on
 // [ma, mb); out is exact where every face whose stencil holds the cell was
-// computed (cells [max(va+3, ma+2), min(vb-3, mb-2)) ).
+// computed (cells [max(va+3, ma+2), min(vb-3, mb-2)) ).  mp / mn: the slots
+// of the previous / next cell along the pencil; circ: the tile is a whole
+// periodic pencil (every cell valid, neighbours wrap).
 template <class PH>
-PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active, int va, int vb, int ma, int mb,
-                           const double (&V)[PH::NV], const double (&mu)[PH::NV], double ch, const PhysParams& pp,
-                           double (&out)[PH::NV])
+PK_DEV void adj_divergence(const AdjSmem& sm, int me, int mp, int mn, bool circ, int t, bool active, int va, int vb,
+                           int ma, int mb, const double (&V)[PH::NV], const double (&mu)[PH::NV], double ch,
+                           const PhysParams& pp, double (&out)[PH::NV])
 {
     constexpr int NV = PH::NV;
     const int PT = sm.PT;
-    auto qv = [&](int x) { return active && x >= va && x < vb; };
-    auto sv = [&](int x) { return active && x > va && x < vb - 1; };
-    auto mv = [&](int x) { return active && x >= ma && x < mb; };
+    auto qv = [&](int x) { return active && (circ || (x >= va && x < vb)); };
+    auto sv = [&](int x) { return active && (circ || (x > va && x < vb - 1)); };
+    auto mv = [&](int x) { return active && (circ || (x >= ma && x < mb)); };
     auto fv = [&](int x) { return sv(x) && sv(x + 1) && mv(x) && mv(x + 1); };   // face x+1/2
     // A: primitives and mu
     if (qv(t)) {
@@ -65,7 +67,7 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active
         for (int v = 0; v < NV; ++v) {
             const int lim = (PH::MHD && v >= PH::IB) ? pp.limb : pp.lim;
             const double qc = sm.Q[v * PT + me];
-            const double s = slope_interior(lim, qc - sm.Q[v * PT + me - st], sm.Q[v * PT + me + st] - qc);
+            const double s = slope_interior(lim, qc - sm.Q[v * PT + mp], sm.Q[v * PT + mn] - qc);
             const double dqh = 0.5 * s;
             sm.L[v * PT + me] = qc + dqh;
             sm.R[v * PT + me] = qc - dqh;
@@ -81,12 +83,12 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             ql[v] = sm.L[v * PT + me];
-            qr[v] = sm.R[v * PT + me + st];
-            fb[v] = sm.M[v * PT + me + st] - sm.M[v * PT + me];
+            qr[v] = sm.R[v * PT + mn];
+            fb[v] = sm.M[v * PT + mn] - sm.M[v * PT + me];
         }
         riemann_adj<PH>(ql, qr, ch, pp, fb, gl, gr);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sm.R[v * PT + me + st] = gr[v];
+        for (int v = 0; v < NV; ++v) sm.R[v * PT + mn] = gr[v];
     }
     __syncthreads();
     // D: primitive adjoint of the cell itself and the slope adjoint
@@ -100,7 +102,7 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active
             const int lim = (PH::MHD && v >= PH::IB) ? pp.limb : pp.lim;
             const double qc = sm.Q[v * PT + me];
             double dlb, drb;
-            slope_adj(lim, qc - sm.Q[v * PT + me - st], sm.Q[v * PT + me + st] - qc, 0.5 * gl[v] - 0.5 * grr, dlb, drb);
+            slope_adj(lim, qc - sm.Q[v * PT + mp], sm.Q[v * PT + mn] - qc, 0.5 * gl[v] - 0.5 * grr, dlb, drb);
             sm.L[v * PT + me] = dlb;
             sm.M[v * PT + me] = drb;
         }
@@ -115,8 +117,8 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int st, int t, bool active
         for (int v = 0; v < NV; ++v) {
             double x = qb[v];
             if (s0) x += sm.L[v * PT + me] - sm.M[v * PT + me];
-            if (sp) x -= sm.L[v * PT + me + st];
-            if (sn) x += sm.M[v * PT + me - st];
+            if (sp) x -= sm.L[v * PT + mn];
+            if (sn) x += sm.M[v * PT + mp];
             qb[v] = x;
         }
         utoq_adj<PH>(V, qb, out, pp);
@@ -150,8 +152,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused_rec(Geom g, Tile tl,
 
 // Tile position shared by the two adjoint kernels: 3-cell halo.
 struct AdjPos {
-    int t, me, st, s;
-    bool active, own;
+    int t, me, mp, mn, s;
+    bool active, own, circ;
     long long off;
 };
 
@@ -164,13 +166,16 @@ PK_DEV AdjPos adj_pos(const Geom& g, const Tile& tl)
     if (tl.xfast) { a.t = tid % T; p = tid / T; }
     else { p = tid % P; a.t = tid / P; }
     const int spp = tl.xfast ? T : 1;
-    a.st = tl.xfast ? 1 : P;
-    a.me = p * spp + a.t * a.st;
+    const int st = tl.xfast ? 1 : P;
+    a.me = p * spp + a.t * st;
+    a.circ = tl.circ;
+    a.mp = a.circ ? p * spp + (a.t == 0 ? T - 1 : a.t - 1) * st : a.me - st;
+    a.mn = a.circ ? p * spp + (a.t == T - 1 ? 0 : a.t + 1) * st : a.me + st;
     const int i1 = blockIdx.x * P + p;
     const int c0 = blockIdx.y * tl.L;
     a.active = (tid < PT) && (i1 < g.n1);
-    a.s = c0 - 3 + a.t;
-    a.own = a.active && a.t >= 3 && a.t < T - 3 && a.s < c0 + tl.L && a.s < g.n_d;
+    a.s = a.circ ? a.t : c0 - 3 + a.t;
+    a.own = a.active && (a.circ || (a.t >= 3 && a.t < T - 3 && a.s < c0 + tl.L && a.s < g.n_d));
     a.off = (long long)(g.g_d + wrap(a.s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
             (long long)(g.g2 + blockIdx.z) * g.s2;
     return a;
@@ -217,7 +222,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage2(Geom g, Tile tl, cons
         mu[v] = c2 * mu[v];
     }
     double rho[NV];
-    adj_divergence<PH>(asm_, a.me, a.st, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, ch, pp, rho);
+    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, ch, pp, rho);
     if (a.own) {
         floors_adj<PH>(V, unpack_floors(fl, 1), rho);
 #pragma unroll
@@ -249,7 +254,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage1(Geom g, Tile tl, cons
         load_cell<PH>(m1, a.off, g, mu);
     }
     double rho[NV];
-    adj_divergence<PH>(asm_, a.me, a.st, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, sp->ch, pp, rho);
+    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, sp->ch, pp, rho);
     if (a.own) {
         double l[NV];
         load_cell<PH>(lam_io, a.off, g, l);

@@ -176,12 +176,20 @@ int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
 // Launch-bound variants of the two adjoint kernels (threads per CTA, CTAs per SM)
 constexpr int NADJ_VARIANT = 5;
 constexpr int ADJ_T[NADJ_VARIANT] = {256, 256, 192, 128, 128};
-// defaults per sweep direction, measured on B200 at 128^3 (MHD and HD) over
-// variants x owned lengths 26..250: 8 pencils x 32 cells in 256 threads with
-// 128 registers (spilling) beat every longer tile and every variant with
-// more registers per thread
+// defaults, measured on B200 (MHD, 128^3 and 256^3) over variants x owned
+// lengths: the 128-register variant (spilling) beats every variant with more
+// registers; the whole periodic pencil without halo beats 8 pencils x 26 + 6
+// halo cells along x always (256^3: 29.9 vs 35.3 ms per adjoint sweep) and
+// along y and z while at least two pencils share the CTA (128^3: 3.97 vs
+// 4.23 ms), but not with one pencil per CTA (256^3 y: 34.7 vs 31.8 ms)
 constexpr int DEF_ADJ_V[3] = {1, 1, 1};
-constexpr int DEF_ADJ_L[3] = {26, 26, 26};
+constexpr int DEF_ADJ_CHUNK = 26;
+
+inline int default_adj_length(int dir, int n, int threads)
+{
+    if (n <= threads && (dir == 0 || 2 * n <= threads)) return n;
+    return DEF_ADJ_CHUNK;
+}
 
 template <class PH>
 struct AdjKernels {
@@ -223,10 +231,11 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
         const int var = (h->adjV[dir] >= 0 && h->adjV[dir] < NADJ_VARIANT) ? h->adjV[dir] : DEF_ADJ_V[dir];
         Geom g = make_geom(b, dir);
         Tile tl;
-        int L = h->adjL[dir] > 0 ? h->adjL[dir] : DEF_ADJ_L[dir];
-        if (L > ADJ_T[var] - 6) L = ADJ_T[var] - 6;
+        int L = h->adjL[dir] > 0 ? h->adjL[dir] : default_adj_length(dir, b.n[dir], ADJ_T[var]);
         if (L > b.n[dir]) L = b.n[dir];
-        tl.T = L + 6;
+        tl.circ = (L == b.n[dir] && b.n[dir] <= ADJ_T[var]) ? 1 : 0;
+        if (!tl.circ && L > ADJ_T[var] - 6) L = ADJ_T[var] - 6;
+        tl.T = tl.circ ? L : L + 6;
         tl.P = ADJ_T[var] / tl.T;
         if (tl.P < 1) return fail(h, PK_E_ARG, "adjoint tile longer than the variant's CTA size");
         if (tl.P > g.n1) tl.P = g.n1;
