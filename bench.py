@@ -60,10 +60,15 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--adj-steps", type=int, default=8)
     p.add_argument("--tune-log", default=None)
-    p.add_argument("--workload", default="mhd256", choices=["mhd256", "batched", "adjoint", "ot-gradient"],
+    p.add_argument("--workload", default="mhd256",
+                   choices=["mhd256", "batched", "adjoint", "ot-gradient", "batched-adjoint"],
                    help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks; "
                         "adjoint: gradient of --steps steps of the MHD block at --n; ot-gradient: the "
-                        "differentiable Orszag-Tang workload (512^2, K = 100) with its FD check")
+                        "differentiable Orszag-Tang workload (512^2, K = 100) with its FD check; "
+                        "batched-adjoint: gradients of 64 stacked 128^3 turbulence instances (K = 50)")
+    p.add_argument("--instances", type=int, default=64)
+    p.add_argument("--group", type=int, default=8, help="instances stacked per handle (batched-adjoint)")
+    p.add_argument("--k", type=int, default=50, help="time steps differentiated (batched-adjoint)")
     p.add_argument("--nblocks", type=int, default=512)
     p.add_argument("--tiles", default=None,
                    help="fix fused-sweep tiles instead of autotuning, e.g. 'x:1,88,3;y:4,56,2;z:4,56,2' (P,L,variant)")
@@ -580,8 +585,132 @@ def ot_gradient_arm(args):
     sim.close()
 
 
+def batched_adjoint_arm(args):
+    """Batched adjoint: --instances independent 128^3 ideal-MHD turbulence
+    instances (the 256^3 recipe with rms Mach log-uniform in [0.5, 5] and B0
+    uniform in [0.05, 0.5], seeded), loss = sum over instances of the
+    kinetic-energy spectrum power in 8 <= |k| <= 16 after K = --k steps,
+    gradient with respect to every instance's initial velocity field.
+
+    --group instances are stacked along z in one handle (pk_set_instances):
+    each sweep and each adjoint sweep is one launch over the group, every
+    instance with its own CFL time step.  The gradient goes through
+    torch.autograd (turbulence_state -> advance -> spectrum_power) with
+    checkpoints every 2 steps (the memory optimum for 6 stored sweeps per
+    step).  A "step" of this workload is the gradient of one group; the
+    timed steps cycle over the groups, so --steps = instances / group covers
+    the whole ensemble once.  Beside it: K plain forward steps of a group,
+    and the gradient of one instance in a handle of its own."""
+    import torch
+    from piernik_b200 import build, problems
+    from piernik_b200._lib import PkTimeState
+    from piernik_b200.autograd import advance, spectrum_power, turbulence_state
+    from piernik_b200.sim import Simulation
+    build.build()
+    torch.cuda.set_device(0)
+    n = args.n if args.n != 256 else 128
+    G, K = args.group, args.k
+    ngroups = max(1, args.instances // G)
+    steps = args.steps if args.steps != 10 else ngroups
+    every = 2
+    params = problems.turbulence_ensemble(ngroups * G, n, args.seed)
+    groups = []
+    p0 = None
+    for j in range(ngroups):
+        f = [problems.mhd_turbulence_fields(n, sd, mach, b0) for sd, mach, b0 in params[j * G:(j + 1) * G]]
+        p0 = f[0][3]
+        cat = lambda i, ax: torch.tensor(np.concatenate([x[i] for x in f], axis=ax), device="cuda")
+        groups.append((cat(0, 0), cat(1, 1), cat(2, 1)))
+    setup = problems.turbulence_setup(n, nz=G * n)
+    sim = Simulation(setup)
+    sim.set_instances(G)
+    stream = torch.cuda.ExternalStream(sim.stream)
+
+    def gradient(s, grp, inst):
+        rho, v0, b = grp
+        v = v0.clone().requires_grad_(True)
+        s.time_state = PkTimeState()
+        out = advance(s, turbulence_state(s, rho, v, b, p0), K, every=every)
+        loss = spectrum_power(s, out, 8.0, 16.0, instances=inst).sum()
+        loss.backward()
+        return v.grad, loss.detach()
+
+    for w in range(args.warmup):
+        gradient(sim, groups[w % ngroups], G)
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    l0, _, _ = sim.profile_read()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = []
+    for i in range(steps):
+        g, loss = gradient(sim, groups[i % ngroups], G)
+        losses.append(loss)
+    e1.record()
+    e1.synchronize()
+    l1, _, _ = sim.profile_read()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    gnorm = float(torch.linalg.vector_norm(g))
+    # K plain forward steps of the last group, for the gradient / forward ratio
+    rho, v0, b = groups[(steps - 1) % ngroups]
+    x0 = turbulence_state(sim, rho, v0, b, p0)
+    full = torch.zeros(sim.state_shape(), dtype=torch.float64, device="cuda")
+    gd = setup.guards
+    full[:, gd[2]:gd[2] + G * n, gd[1]:gd[1] + n, gd[0]:gd[0] + n] = x0
+    torch.cuda.synchronize()
+    sim.upload_device(full.data_ptr())
+    sim.time_state = PkTimeState()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    sim.run(K)
+    f1.record(stream)
+    f1.synchronize()
+    fwd_ms = f0.elapsed_time(f1)
+    dts = [sim.instance_state(i).dt for i in range(G)]
+    del full
+    sim.close()
+    # one instance alone, same K and checkpointing
+    one = Simulation(problems.turbulence_setup(n))
+    single = (groups[0][0][:n], groups[0][1][:, :n], groups[0][2][:, :n])
+    gradient(one, single, 1)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    gradient(one, single, 1)
+    s1.record()
+    s1.synchronize()
+    single_ms = s0.elapsed_time(s1)
+    one.close()
+    cells = G * n ** 3
+    value = 2.0 * cells * K * steps / (ms / 1e3)
+    out = {"metric": "FP64 MHD cell-updates/s differentiated (forward + adjoint), stacked 128^3 instances",
+           "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+           "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"batched adjoint: {ngroups * G} independent {n}^3 ideal-MHD turbulence "
+                                  f"instances (Mach log-uniform 0.5..5, B0 0.05..0.5), HLLD + GLM, moncen, "
+                                  f"CFL 0.5, loss = kinetic-energy shell power 8 <= |k| <= 16 after K = {K} "
+                                  f"steps, gradient wrt initial velocity", "instances": ngroups * G,
+                      "group": G, "K": K, "checkpoint_every": every,
+                      "step": f"gradient of one group of {G} stacked instances",
+                      "l2": "group state %.2f GB > 126 MB L2" % (9 * 8 * (n + 8) ** 2 * (G * n + 8) / 1e9)},
+           "instance_gradients_per_s": G * steps / (ms / 1e3),
+           "gradient_ms_per_instance": ms / (steps * G),
+           "forward_ms_per_group": fwd_ms, "gradient_over_forward": (ms / steps) / fwd_ms,
+           "single_instance_gradient_ms": single_ms,
+           "batched_per_instance_over_single": (ms / (steps * G)) / single_ms,
+           "instance_dt_spread": [min(dts), max(dts)],
+           "loss_last_group": float(losses[-1]), "grad_norm_last_group": gnorm,
+           "gpu_launches": l1 - l0, "clocks": ck}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "batched-adjoint":
+        batched_adjoint_arm(args)
+        return
     if args.workload == "batched":
         batched_arm(args)
         return

@@ -183,6 +183,25 @@ int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant);
  * device memory, so one capture serves every step. */
 int pk_use_graph(pk_handle h, int32_t enable);
 
+/* ---- Independent instances in one launch ----
+ * count independent, fully periodic problems of n[0] x n[1] x (n[2]/count)
+ * cells stacked along z in the handle's single block (instance i owns the
+ * interior z planes [i*n[2]/count, (i+1)*n[2]/count)).  Every sweep is one
+ * launch over all instances; each instance wraps periodically inside its own
+ * z range and advances with its own time state: its own CFL time step
+ * (timestep.F90:158-228, reduction over its cells only), chspeed and
+ * glmdamping factor.  The result of each instance is bit for bit that of a
+ * handle holding that instance alone.  Needs RK2, every direction periodic,
+ * no step retry, and n[2]/count in [nb, 256].  count = 1 returns to one
+ * problem.  The reference runs such an ensemble as separate runs: no
+ * counterpart in its code.  pk_time_step, pk_fluid_update, pk_run and the
+ * pk_grad_* calls then act on all instances (the grad calls' dt arrays hold
+ * count values per step, step-major); pk_get_time_state reports instance
+ * 0 and pk_set_time_state sets every instance. */
+int pk_set_instances(pk_handle h, int32_t count);
+int pk_get_instance_state(pk_handle h, int32_t instance, pk_time_state* st);
+int pk_set_instance_state(pk_handle h, int32_t instance, const pk_time_state* st);
+
 /* ---- Connected blocks of one level (cg_list_bnd.F90:251-324) ----
  * pk_set_domain declares a level of ncells cells per direction (periodic or
  * not per direction); pk_block_place puts a block's first interior cell at

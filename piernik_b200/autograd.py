@@ -99,6 +99,45 @@ def central_magnetic_energy(sim: Simulation, state: torch.Tensor, frac: float = 
     return 0.5 * (b * b).sum() * float(np.prod(s.dl))
 
 
+def turbulence_state(sim: Simulation, rho: torch.Tensor, v: torch.Tensor, b: torch.Tensor,
+                     p0: float) -> torch.Tensor:
+    """Interior MHD state (nplanes, nz, ny, nx) from density, velocity and
+    magnetic field (each component-first), pressure p0 and psi = 0: a
+    differentiable function of the fields (the conversion of the turbulence
+    recipe: m = rho v, e = p0/(gamma-1) + rho |v|^2 / 2 + |B|^2 / 2)."""
+    gam = sim.setup.fluids[0][1]
+    emag = 0.5 * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2])
+    ene = ((p0 / (gam - 1.0)) + 0.5 * rho * ((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])) + emag
+    planes = [rho, rho * v[0], rho * v[1], rho * v[2], ene, b[0], b[1], b[2], torch.zeros_like(rho)]
+    return torch.stack(planes, 0)
+
+
+def spectrum_power(sim: Simulation, state: torch.Tensor, kmin: float = 8.0, kmax: float = 16.0,
+                   instances: int = 1) -> torch.Tensor:
+    """Kinetic-energy spectrum power in the shell kmin <= |k| <= kmax of each
+    of ``instances`` cubes stacked along z in ``state`` (interior,
+    (nplanes, nz, ny, nx)): P = sum over the shell of |v_hat(k)|^2 / 2 with
+    v = m / rho and v_hat the unitary-mean DFT (sum_k |v_hat|^2 = mean |v|^2).
+    Returns a tensor of ``instances`` powers."""
+    nz, ny, nx = state.shape[1:]
+    seg = nz // instances
+    rho = state[0].reshape(instances, seg, ny, nx)
+    v = state[1:4].reshape(3, instances, seg, ny, nx) / rho
+    vh = torch.fft.rfftn(v, dim=(-3, -2, -1)) / float(seg * ny * nx)
+    kz = torch.fft.fftfreq(seg, 1.0 / seg, dtype=torch.float64, device=state.device)[:, None, None]
+    ky = torch.fft.fftfreq(ny, 1.0 / ny, dtype=torch.float64, device=state.device)[None, :, None]
+    kx = torch.fft.rfftfreq(nx, 1.0 / nx, dtype=torch.float64, device=state.device)[None, None, :]
+    kk = torch.sqrt(kx * kx + ky * ky + kz * kz)
+    # the half spectrum holds each pair (k, -k) once except the kx = 0 and Nyquist planes
+    wgt = torch.full(kk.shape, 2.0, dtype=torch.float64, device=state.device)
+    wgt[..., 0] = 1.0
+    if nx % 2 == 0:
+        wgt[..., -1] = 1.0
+    wgt = torch.where((kk >= kmin) & (kk <= kmax), wgt, torch.zeros_like(wgt))
+    pw = (vh.real * vh.real + vh.imag * vh.imag) * wgt
+    return 0.5 * pw.sum(dim=(0, 2, 3, 4))
+
+
 def last_dts(out: torch.Tensor):
     """The dt sequence recorded by the ``advance`` call that produced ``out``."""
     fn = out.grad_fn

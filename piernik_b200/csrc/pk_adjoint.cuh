@@ -684,7 +684,6 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
         // vs[c] = u[1+c] + k*(b[c] - bs[c]),  k = b0/dn
         auto side_part3 = [&](auto sd) {
             constexpr bool left = decltype(sd)::value;
-            const double* u = left ? ul : ur;
             const double* b = left ? bl : br;
             double* ub = left ? ulb : urb;
             double* bb = left ? blb : brb;

@@ -143,16 +143,16 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused_rec(Geom g, Tile tl,
                                                                int apply_fac, unsigned* __restrict__ gstatus)
 {
     extern __shared__ double smem[];
-    const double dt = sp->dt;
     unsigned status = 0;
-    fused_tile<PH, true>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, (0.5 * dt) / dl,
-                         (1.0 * dt) / dl, sp->ch, apply_fac ? sp->psi_fac : 1.0, smem, status, ustar, flags);
+    fused_tile<PH, true>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, sp, dl, apply_fac, smem,
+                         status, ustar, flags);
     flush_status(status, gstatus);
 }
 
 // Tile position shared by the two adjoint kernels: 3-cell halo.
 struct AdjPos {
     int t, me, mp, mn, s;
+    int seg;                // instance of the tile (cells stacked along z), for the step scalars
     bool active, own, circ;
     long long off;
 };
@@ -174,7 +174,8 @@ PK_DEV AdjPos adj_pos(const Geom& g, const Tile& tl)
     const int i1 = blockIdx.x * P + p;
     const int c0 = blockIdx.y * tl.L;
     a.active = (tid < PT) && (i1 < g.n1);
-    a.s = a.circ ? a.t : c0 - 3 + a.t;
+    a.s = a.circ ? c0 + a.t : c0 - 3 + a.t;
+    a.seg = g.seg_len ? ((g.seg_along ? c0 : (int)blockIdx.z) / g.seg_len) : 0;
     a.own = a.active && (a.circ || (a.t >= 3 && a.t < T - 3 && a.s < c0 + tl.L && a.s < g.n_d));
     a.off = (long long)(g.g_d + wrap(a.s, g.n_d)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
             (long long)(g.g2 + blockIdx.z) * g.s2;
@@ -198,7 +199,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage2(Geom g, Tile tl, cons
     const int PT = tl.P * tl.T;
     const AdjSmem asm_{smem, smem + NV * PT, smem + 2 * NV * PT, smem + 3 * NV * PT, PT};
     const AdjPos a = adj_pos(g, tl);
-    const double dt = sp->dt, ch = sp->ch, fac = apply_fac ? sp->psi_fac : 1.0;
+    const StepParams stp = sp[a.seg];
+    const double dt = stp.dt, ch = stp.ch, fac = apply_fac ? stp.psi_fac : 1.0;
     const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
     double V[NV], mu[NV], mu2[NV];
 #pragma unroll
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage1(Geom g, Tile tl, cons
         load_cell<PH>(m1, a.off, g, mu);
     }
     double rho[NV];
-    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, sp->ch, pp, rho);
+    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, sp[a.seg].ch, pp, rho);
     if (a.own) {
         double l[NV];
         load_cell<PH>(lam_io, a.off, g, l);

@@ -68,6 +68,8 @@ Geom make_geom(const Block& b, int dir)
     g.n2 = b.n[o2];
     g.g2 = b.g[o2];
     for (int j = 0; j < 3; ++j) g.perm[j] = PERM3[dir][j];
+    g.seg_len = b.seg_len;
+    g.seg_along = dir == 2;
     return g;
 }
 
@@ -376,10 +378,25 @@ void invalidate_graph(pk_ctx* h)
 int put_step_params(pk_ctx* h, double dt, double ch, double fac)
 {
     PK_CUDA(h, cudaStreamSynchronize(h->stream));   // the previous copy out of h_step has completed
-    h->h_step->dt = dt;
-    h->h_step->ch = ch;
-    h->h_step->psi_fac = fac;
-    PK_CUDA(h, cudaMemcpyAsync(h->d_step, h->h_step, sizeof(StepParams), cudaMemcpyHostToDevice, h->stream));
+    for (int i = 0; i < h->ninst; ++i) {
+        h->h_step[i].dt = dt;
+        h->h_step[i].ch = ch;
+        h->h_step[i].psi_fac = fac;
+    }
+    PK_CUDA(h, cudaMemcpyAsync(h->d_step, h->h_step, sizeof(StepParams) * h->ninst, cudaMemcpyHostToDevice, h->stream));
+    return PK_OK;
+}
+
+// one set of step scalars per instance
+int put_step_array(pk_ctx* h, const StepRec* r)
+{
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < h->ninst; ++i) {
+        h->h_step[i].dt = r[i].dt;
+        h->h_step[i].ch = r[i].ch;
+        h->h_step[i].psi_fac = r[i].fac;
+    }
+    PK_CUDA(h, cudaMemcpyAsync(h->d_step, h->h_step, sizeof(StepParams) * h->ninst, cudaMemcpyHostToDevice, h->stream));
     return PK_OK;
 }
 
@@ -402,7 +419,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
     if (fused_ok(h)) {
         if (int rc = ensure_pingpong(h)) return rc;
         if (int rc = exchange_guards(h, dir)) return rc;   // connected domains: halos come from the guards
-        if (h->batched || h->blocks.size() > 1) {
+        if ((h->batched && h->ninst < 2) || h->blocks.size() > 1) {
             if (int rc = build_batch(h)) return rc;
             if (int rc = ops->batched(h, dir, apply_fac, h->d_counter + dir)) return rc;
             for (auto& b : h->blocks) b.guards_stale = true;
@@ -475,11 +492,11 @@ int step_sweeps(pk_ctx* h, double dt, double ch, double fac)
 }
 
 // update_chspeed and the glmdamping factor for dt (hdc.F90:112-119, 310-330)
-void glm_scalars(pk_ctx* h, double dt, double* ch, double* fac)
+void glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fac)
 {
     int eff;
     const double mdl = min_dl(h, &eff);
-    *ch = h->ts.chspeed;
+    *ch = ch_now;
     *fac = 1.0;
     if (!h->cfg.magnetic) return;
     double c = DBL_MAX;
@@ -495,6 +512,8 @@ void glm_scalars(pk_ctx* h, double dt, double* ch, double* fac)
     *ch = c;
     *fac = std::exp(-f);
 }
+
+void glm_scalars(pk_ctx* h, double dt, double* ch, double* fac) { glm_scalars_for(h, dt, h->ts.chspeed, ch, fac); }
 
 }  // namespace
 
@@ -625,6 +644,8 @@ int pk_destroy(pk_handle h)
     cudaFree(h->d_xptr[0]);
     cudaFree(h->d_xptr[1]);
     for (auto& b : h->blocks) cudaFree(b.retry);
+    cudaFree(h->d_inst[0]);
+    cudaFree(h->d_inst[1]);
     cudaFree(h->d_desc[0]);
     cudaFree(h->d_desc[1]);
     cudaFree(h->d_status);
@@ -645,6 +666,7 @@ void* pk_stream(pk_handle h) { return h ? (void*)h->stream : nullptr; }
 int pk_block_add(pk_handle h, const int32_t n[3], const double dl[3], const int32_t bnd[6], int32_t* id_out)
 {
     if (!h || !n || !dl || !bnd) return PK_E_ARG;
+    if (h->ninst > 1) return fail(h, PK_E_STATE, "stacked instances live in one block");
     Block b;
     for (int d = 0; d < 3; ++d) {
         if (n[d] < 1 || !(dl[d] > 0.0)) return fail(h, PK_E_ARG, "block extent and cell size must be positive");
@@ -795,6 +817,83 @@ int pk_fill_guards(pk_handle h)
     for (auto& b : h->blocks)
         if (int rc = fill_guards_block(h, b)) return rc;
     return exchange_guards(h);
+}
+
+int pk_set_instances(pk_handle h, int32_t count)
+{
+    if (!h || count < 1) return PK_E_ARG;
+    if (h->blocks.size() != 1) return fail(h, PK_E_UNSUPPORTED, "instances are stacked in one block");
+    Block& b = h->blocks[0];
+    if (count > 1) {
+        if (b.n[2] % count) return fail(h, PK_E_ARG, "the z extent must be a multiple of the instance count");
+        const int seg = b.n[2] / count;
+        if (seg < h->cfg.nb || seg > 256) return fail(h, PK_E_ARG, "instances need nb..256 cells along z");
+        for (int d = 0; d < 3; ++d)
+            if (b.n[d] > 1 && (b.bnd[d][0] != PK_BND_PER || b.bnd[d][1] != PK_BND_PER))
+                return fail(h, PK_E_UNSUPPORTED, "stacked instances are periodic in every direction");
+        if (h->cfg.integration_order != 2 || h->connected || h->cfg.cflcontrol == PK_CFL_REDO)
+            return fail(h, PK_E_UNSUPPORTED, "stacked instances need RK2, one unconnected block and no step retry");
+        b.seg_len = seg;
+    } else {
+        b.seg_len = 0;
+    }
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_step);
+    cudaFreeHost(h->h_step);
+    h->d_step = nullptr;
+    h->h_step = nullptr;
+    PK_CUDA(h, cudaMalloc(&h->d_step, sizeof(StepParams) * count));
+    PK_CUDA(h, cudaMallocHost(&h->h_step, sizeof(StepParams) * count));
+    h->ninst = count;
+    h->its.assign(count, h->ts);
+    if (count * 12 > h->red_cap) {
+        cudaFree(h->d_red);
+        cudaFreeHost(h->h_red);
+        h->red_cap = count * 12 + 1200;
+        PK_CUDA(h, cudaMalloc(&h->d_red, sizeof(unsigned long long) * h->red_cap));
+        PK_CUDA(h, cudaMallocHost(&h->h_red, sizeof(unsigned long long) * h->red_cap));
+    }
+    // the instances as blocks for the CFL reduction, one table per parity
+    if (int rc = ensure_pingpong(h)) return rc;
+    for (int p = 0; p < 2; ++p) {
+        cudaFree(h->d_inst[p]);
+        h->d_inst[p] = nullptr;
+        if (count < 2) continue;
+        std::vector<BlockDesc> t(count);
+        for (int i = 0; i < count; ++i) {
+            BlockDesc& d = t[i];
+            d.in = b.buf[p] + (long long)i * b.seg_len * b.ext[0] * b.ext[1];
+            d.out = nullptr;
+            d.plane = b.plane;
+            for (int k = 0; k < 3; ++k) {
+                d.ext[k] = b.ext[k];
+                d.g[k] = b.g[k];
+                d.n[k] = b.n[k];
+                d.dl[k] = b.dl[k];
+            }
+            d.n[2] = b.seg_len;
+            d.wrap = 1;
+        }
+        PK_CUDA(h, cudaMalloc(&h->d_inst[p], sizeof(BlockDesc) * count));
+        PK_CUDA(h, cudaMemcpy(h->d_inst[p], t.data(), sizeof(BlockDesc) * count, cudaMemcpyHostToDevice));
+    }
+    invalidate_graph(h);
+    return PK_OK;
+}
+
+int pk_get_instance_state(pk_handle h, int32_t i, pk_time_state* st)
+{
+    if (!h || !st || i < 0 || i >= h->ninst) return PK_E_ARG;
+    *st = h->ninst > 1 ? h->its[i] : h->ts;
+    return PK_OK;
+}
+
+int pk_set_instance_state(pk_handle h, int32_t i, const pk_time_state* st)
+{
+    if (!h || !st || i < 0 || i >= h->ninst) return PK_E_ARG;
+    if (h->ninst > 1) h->its[i] = *st;
+    if (i == 0) h->ts = *st;
+    return PK_OK;
 }
 
 int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3])
@@ -982,51 +1081,37 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out)
     return PK_OK;
 }
 
-int pk_time_step(pk_handle h, double* dt_out)
+// the sanity factors of time_step (timestep.F90:200-228) on a raw dt for one
+// time state; returns PK_E_DTMIN when dt < dt_min
+static int clamp_dt(const pk_config& c, pk_time_state& ts, double dt, double c_all)
 {
-    if (!h) return PK_E_ARG;
-    double dt, c_all;
-    h->ts.dt_old = h->ts.dt;                          // timestep.F90:158
-    if (int rc = pk_timestep_raw(h, &dt, &c_all)) return rc;
-    if (h->reduce_cb) {                               // over ranks (timestep.F90:173, MPI_MIN / MPI_MAX)
-        dt = h->reduce_cb(h->comm_ctx, dt, 0);
-        c_all = h->reduce_cb(h->comm_ctx, c_all, 1);
-    }
-    const pk_config& c = h->cfg;
-    if (h->ts.nstep < 1) {                            // :200-208
+    if (ts.nstep < 1) {                               // :200-208
         if (c.dt_initial > 0.0) dt = (c.dt_initial < dt) ? c.dt_initial : dt;
         else if (c.dt_initial < 0.0) {
             const double x = -c.dt_initial * dt;
             dt = (x < dt) ? x : dt;
         }
-    } else if (h->ts.dt_old > 0.0) {
-        const double x = h->ts.dt_old * c.dt_max_grow;
+    } else if (ts.dt_old > 0.0) {
+        const double x = ts.dt_old * c.dt_max_grow;
         dt = (x < dt) ? x : dt;
     }
-    h->ts.c_all = c_all;
+    ts.c_all = c_all;
     if (dt < c.dt_min) {                              // :213-219
-        h->ts.dt = dt;
-        if (dt_out) *dt_out = dt;
-        return fail(h, PK_E_DTMIN, "dt < dt_min");
+        ts.dt = dt;
+        return PK_E_DTMIN;
     }
-    const double rem = c.tend - h->ts.t;              // :224
+    const double rem = c.tend - ts.t;                 // :224
     const double cap = (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem);
     dt = (c.dt_max < dt) ? c.dt_max : dt;
     dt = (cap < dt) ? cap : dt;
-    h->ts.dt = dt;
-    if (dt_out) *dt_out = dt;
+    ts.dt = dt;
     return PK_OK;
 }
 
-int pk_fluid_update(pk_handle h)
+// the sweeps of one step, the step scalars already in d_step: replayed from a
+// CUDA graph captured once (use_graph) or launched one by one
+static int run_step_sweeps(pk_ctx* h, double dt, double ch, double fac)
 {
-    if (!h) return PK_E_ARG;
-    if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
-    const double dt = h->ts.dt;
-    double ch, fac;
-    glm_scalars(h, dt, &ch, &fac);
-    h->ts.chspeed = ch;
-    if (int rc = put_step_params(h, dt, ch, fac)) return rc;
     if (h->use_graph && !h->profiling && !h->halo_cb) {
         if (fused_ok(h) && h->blocks.size() > 1)
             if (int rc = build_batch(h)) return rc;   // tables are built outside the capture
@@ -1057,9 +1142,114 @@ int pk_fluid_update(pk_handle h)
         h->launches += h->graph_kernels;
         if (fused_ok(h))
             for (auto& b : h->blocks) b.guards_stale = true;
-    } else {
-        if (int rc = step_sweeps(h, dt, ch, fac)) return rc;
+        return PK_OK;
     }
+    return step_sweeps(h, dt, ch, fac);
+}
+
+// time_step of every stacked instance: its own CFL reduction and clamps
+static int inst_time_step(pk_ctx* h)
+{
+    Block& b = h->blocks[0];
+    const int ni = h->ninst;
+    if (ni > h->red_cap / 12) return fail(h, PK_E_STATE, "reduction slots too few for the instances");
+    PK_CUDA(h, cudaMemsetAsync(h->d_red, 0, sizeof(unsigned long long) * 12 * ni, h->stream));
+    CflArgs a;
+    a.nfl = h->cfg.nfluids;
+    int beg = 0;
+    for (int f = 0; f < 3; ++f) {
+        a.fl[f].kind = f < a.nfl ? h->cfg.fluid_kind[f] : K_NONE;
+        a.fl[f].beg = beg;
+        a.fl[f].gam = h->pp.gam[f];
+        a.fl[f].gam_1 = h->pp.gam_1[f];
+        if (f < a.nfl) beg += (h->cfg.fluid_kind[f] == PK_FLUID_DST) ? 4 : 5;
+    }
+    a.magnetic = h->cfg.magnetic;
+    a.ib = h->ib;
+    k_cfl_blocks<<<dim3(64, ni), 256, 0, h->stream>>>(h->d_inst[h->cur], a, h->d_red);
+    PK_CUDA(h, cudaGetLastError());
+    h->launches += 1;
+    PK_CUDA(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(unsigned long long) * 12 * ni, cudaMemcpyDeviceToHost,
+                               h->stream));
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < ni; ++i) {
+        double dt = DBL_MAX, c_all = 0.0;
+        for (int f = 0; f < h->cfg.nfluids; ++f) {
+            double cm[4];
+            for (int d = 0; d < 4; ++d) std::memcpy(&cm[d], &h->h_red[12 * i + 4 * f + d], sizeof(double));
+            double dtp[3];
+            for (int d = 0; d < 3; ++d) dtp[d] = (b.n[d] > 1 && cm[d] > 0.0) ? b.dl[d] / cm[d] : DBL_MAX;
+            double m = dtp[0];
+            m = (dtp[1] < m) ? dtp[1] : m;
+            m = (dtp[2] < m) ? dtp[2] : m;
+            const double dtf = h->cfg.cfl * m;
+            dt = (dtf < dt) ? dtf : dt;
+            c_all = (cm[3] > c_all) ? cm[3] : c_all;
+        }
+        pk_time_state& ts = h->its[i];
+        ts.dt_old = ts.dt;
+        if (clamp_dt(h->cfg, ts, dt, c_all)) return fail(h, PK_E_DTMIN, "dt < dt_min in an instance");
+    }
+    h->ts = h->its[0];
+    return PK_OK;
+}
+
+// fluid_update_full of every stacked instance with its own dt (one launch per sweep)
+static int inst_fluid_update(pk_ctx* h, std::vector<StepRec>* record)
+{
+    const int ni = h->ninst;
+    std::vector<StepRec> r(ni);
+    for (int i = 0; i < ni; ++i) {
+        pk_time_state& ts = h->its[i];
+        double ch, fac;
+        glm_scalars_for(h, ts.dt, ts.chspeed, &ch, &fac);
+        ts.chspeed = ch;
+        r[i] = StepRec{ts.dt, ch, fac};
+    }
+    if (int rc = put_step_array(h, r.data())) return rc;
+    if (int rc = run_step_sweeps(h, r[0].dt, r[0].ch, r[0].fac)) return rc;
+    for (int i = 0; i < ni; ++i) {
+        pk_time_state& ts = h->its[i];
+        ts.t = ts.t + ts.dt;                          // fluidupdate.F90:116, :126
+        ts.t = ts.t + ts.dt;
+    }
+    if (record) record->insert(record->end(), r.begin(), r.end());
+    h->ts = h->its[0];
+    return PK_OK;
+}
+
+int pk_time_step(pk_handle h, double* dt_out)
+{
+    if (!h) return PK_E_ARG;
+    if (h->ninst > 1) {
+        const int rc = inst_time_step(h);
+        if (dt_out) *dt_out = h->its[0].dt;
+        return rc;
+    }
+    double dt, c_all;
+    h->ts.dt_old = h->ts.dt;                          // timestep.F90:158
+    if (int rc = pk_timestep_raw(h, &dt, &c_all)) return rc;
+    if (h->reduce_cb) {                               // over ranks (timestep.F90:173, MPI_MIN / MPI_MAX)
+        dt = h->reduce_cb(h->comm_ctx, dt, 0);
+        c_all = h->reduce_cb(h->comm_ctx, c_all, 1);
+    }
+    const int rc = clamp_dt(h->cfg, h->ts, dt, c_all);
+    if (dt_out) *dt_out = h->ts.dt;
+    if (rc) return fail(h, PK_E_DTMIN, "dt < dt_min");
+    return PK_OK;
+}
+
+int pk_fluid_update(pk_handle h)
+{
+    if (!h) return PK_E_ARG;
+    if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
+    if (h->ninst > 1) return inst_fluid_update(h, nullptr);
+    const double dt = h->ts.dt;
+    double ch, fac;
+    glm_scalars(h, dt, &ch, &fac);
+    h->ts.chspeed = ch;
+    if (int rc = put_step_params(h, dt, ch, fac)) return rc;
+    if (int rc = run_step_sweeps(h, dt, ch, fac)) return rc;
     h->ts.t = h->ts.t + dt;                            // fluidupdate.F90:116
     h->ts.t = h->ts.t + dt;                            // :126
     return PK_OK;
@@ -1152,6 +1342,15 @@ static int check_cfl(pk_ctx* h)
 int pk_run(pk_handle h, int32_t nsteps)
 {
     if (!h) return PK_E_ARG;
+    if (h->ninst > 1) {                                // stacked instances: each its own dt
+        for (int s = 0; s < nsteps; ++s) {
+            if (int rc = inst_time_step(h)) return rc;
+            if (int rc = inst_fluid_update(h, nullptr)) return rc;
+            for (auto& ts : h->its) ts.nstep += 1;
+            h->ts = h->its[0];
+        }
+        return PK_OK;
+    }
     const int redo = h->cfg.cflcontrol == PK_CFL_REDO;
     for (int s = 0; s < nsteps; ++s) {
         if (!(h->ts.t < h->cfg.tend) && !h->ts.repeat_step) break;
@@ -1199,6 +1398,7 @@ int pk_set_time_state(pk_handle h, const pk_time_state* st)
 {
     if (!h || !st) return PK_E_ARG;
     h->ts = *st;
+    if (h->ninst > 1) h->its.assign(h->ninst, *st);   // stacked instances: every one
     return PK_OK;
 }
 
@@ -1467,6 +1667,23 @@ int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt
             PK_CUDA(h, cudaMemcpyAsync(h->grad_ckpt[k], state(h, b), sizeof(double) * h->nplanes * b.plane,
                                        cudaMemcpyDeviceToDevice, h->stream));
         }
+        if (h->ninst > 1) {                            // stacked instances: ninst step records per step
+            const int ni = h->ninst;
+            if (dt_in) {
+                for (int i = 0; i < ni; ++i) {
+                    h->its[i].dt_old = h->its[i].dt;
+                    h->its[i].dt = dt_in[(size_t)s * ni + i];
+                }
+            } else {
+                if (int rc = inst_time_step(h)) return rc;
+            }
+            if (int rc = inst_fluid_update(h, &h->grad_steps)) return rc;
+            for (auto& ts : h->its) ts.nstep += 1;
+            h->ts = h->its[0];
+            if (dt_out)
+                for (int i = 0; i < ni; ++i) dt_out[(size_t)s * ni + i] = h->its[i].dt;
+            continue;
+        }
         double dt;
         if (dt_in) {
             h->ts.dt_old = h->ts.dt;
@@ -1499,7 +1716,8 @@ int pk_grad_backward(pk_handle h)
     const PhysOps* ops = ops_of(h);
     int dir[6], fac[6];
     const int nsw = step_plan(h, dir, fac);
-    const int K = (int)h->grad_steps.size(), C = h->grad_every;
+    const int ni = h->ninst;
+    const int K = (int)h->grad_steps.size() / ni, C = h->grad_every;
     if (K == 0) return PK_OK;
     if (int rc = ensure_pool(h, b, C * nsw)) return rc;
     const int nseg = (K + C - 1) / C;
@@ -1508,8 +1726,7 @@ int pk_grad_backward(pk_handle h)
         // recompute the segment, keeping every sweep's output
         const double* x = h->grad_ckpt[seg];
         for (int j = 0; j < len; ++j) {
-            const StepRec& r = h->grad_steps[s0 + j];
-            if (int rc = put_step_params(h, r.dt, r.ch, r.fac)) return rc;
+            if (int rc = put_step_array(h, &h->grad_steps[(size_t)(s0 + j) * ni])) return rc;
             for (int k = 0; k < nsw; ++k) {
                 const int i = j * nsw + k;
                 if (int rc = ops->fused_rec(h, b, dir[k], fac[k], x, h->grad_pool[i], h->grad_star[i], h->grad_flags[i]))
@@ -1519,8 +1736,7 @@ int pk_grad_backward(pk_handle h)
         }
         // adjoint sweeps back to the segment's start
         for (int j = len - 1; j >= 0; --j) {
-            const StepRec& r = h->grad_steps[s0 + j];
-            if (int rc = put_step_params(h, r.dt, r.ch, r.fac)) return rc;
+            if (int rc = put_step_array(h, &h->grad_steps[(size_t)(s0 + j) * ni])) return rc;
             for (int k = nsw - 1; k >= 0; --k) {
                 const int i = j * nsw + k;
                 const double* uin = i > 0 ? h->grad_pool[i - 1] : h->grad_ckpt[seg];

@@ -33,6 +33,7 @@ struct Block {
     double* stage = nullptr;               // host-layout conversion buffer
     bool guards_stale = false;             // fused sweeps read periodic images and never store guards
     double* retry = nullptr;               // copy of the state at the start of a step (cflcontrol = redo)
+    int seg_len = 0;                       // independent instances stacked along z: cells per instance
     long long off[3] = {0, 0, 0};          // first interior cell on the level's cell grid (connected domains)
     bool placed = false;
 };
@@ -86,8 +87,11 @@ struct pk_ctx {
     unsigned long long* d_red = nullptr;
     unsigned long long* h_red = nullptr;
     int red_cap = 0;
-    pk::StepParams* d_step = nullptr;   // device copy of the step scalars
+    pk::StepParams* d_step = nullptr;   // device copy of the step scalars (one per instance)
     pk::StepParams* h_step = nullptr;   // pinned host copy
+    int ninst = 1;                      // independent instances stacked along z in the one block
+    std::vector<pk_time_state> its;     // their time states (ninst > 1)
+    pk::BlockDesc* d_inst[2] = {nullptr, nullptr};   // the instances as CFL blocks, per parity
     pk::BlockDesc* d_desc[2] = {nullptr, nullptr};   // block tables for cur = 0 / 1
     bool batch_dirty = true;
     pk::BatchList batch[3];

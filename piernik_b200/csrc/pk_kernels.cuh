@@ -34,6 +34,8 @@ struct Geom {
     int n_d, g_d;           // interior length / guard offset along the sweep direction
     int n1, g1, n2, g2;     // interior extent / guard offset of the ortho directions
     int perm[3];            // slot b+1+j of a swept cell holds plane b+1+perm[j]
+    int seg_len = 0;        // independent instances stacked along z: cells per instance (0: one)
+    int seg_along = 0;      // 1: this sweep runs along z (the stacking axis)
 };
 
 struct Tile {
@@ -209,9 +211,14 @@ PK_DEV unsigned short pack_floors(const FloorRec& r1, const FloorRec& r2)
 // pass's recomputation).
 template <class PH, bool REC = false, bool W3 = false>
 PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
-                       const PhysParams& pp, double dtodx1, double dtodx2, double ch, double psi_fac,
+                       const PhysParams& pp, const StepParams* __restrict__ sp, double dl, int apply_fac,
                        double* smem, unsigned& status, double* ustar = nullptr, unsigned short* flags = nullptr)
 {
+    // the step scalars of this tile's instance (one instance unless stacked along z)
+    const StepParams stp = sp[g.seg_len ? ((g.seg_along ? c0 : i2) / g.seg_len) : 0];
+    const double dtodx1 = (0.5 * stp.dt) / dl;        // rk_coef(RK2_1) * dt / cg%dl(ddim)
+    const double dtodx2 = (1.0 * stp.dt) / dl;        // rk_coef(RK2_2) * dt / cg%dl(ddim)
+    const double ch = stp.ch, psi_fac = apply_fac ? stp.psi_fac : 1.0;
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
     const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
@@ -219,16 +226,16 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     int p, t;
     if (tl.xfast) { t = tid % T; p = tid / T; }
     else { p = tid % P; t = tid / P; }
-    const int sp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
-    const int me = p * sp + t * st;
+    const int pstride = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
+    const int me = p * pstride + t * st;
     const int i1 = i1_0 + p;
     const bool active = (tid < PT) && (i1 < g.n1);
     const bool circ = tl.circ;
-    const int s = circ ? t : c0 - 4 + t;                       // position along the pencil (interior coords)
+    const int s = circ ? c0 + t : c0 - 4 + t;                  // position along the pencil (interior coords)
     const long long off = (long long)(g.g_d + (tl.wrap ? wrap(s, g.n_d) : s)) * g.sd + (long long)(g.g1 + i1) * g.s1 +
                           (long long)(g.g2 + i2) * g.s2;
-    const int mp = circ ? p * sp + (t == 0 ? T - 1 : t - 1) * st : me - st;
-    const int mn = circ ? p * sp + (t == T - 1 ? 0 : t + 1) * st : me + st;
+    const int mp = circ ? p * pstride + (t == 0 ? T - 1 : t - 1) * st : me - st;
+    const int mn = circ ? p * pstride + (t == T - 1 ? 0 : t + 1) * st : me + st;
     double w[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) w[v] = 0.0;
@@ -269,12 +276,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, con
                                                            unsigned* __restrict__ gstatus)
 {
     extern __shared__ double smem[];
-    const double dt = sp->dt;
-    const double dtodx1 = (0.5 * dt) / dl;        // rk_coef(RK2_1) * dt / cg%dl(ddim)
-    const double dtodx2 = (1.0 * dt) / dl;        // rk_coef(RK2_2) * dt / cg%dl(ddim)
     unsigned status = 0;
-    fused_tile<PH, false, W3>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, dtodx1, dtodx2, sp->ch,
-                   apply_fac ? sp->psi_fac : 1.0, smem, status);
+    fused_tile<PH, false, W3>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, sp, dl, apply_fac,
+                              smem, status);
     flush_status(status, gstatus);
 }
 
@@ -309,7 +313,6 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
     extern __shared__ double smem[];
     __shared__ int next;
     const int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;
-    const double dt = sp->dt, ch = sp->ch, fac = apply_fac ? sp->psi_fac : 1.0;
     unsigned status = 0;
     for (;;) {
         if (threadIdx.x == 0) next = (int)atomicAdd(counter, 1u);
@@ -343,9 +346,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
         tl.halo = 4;
         tl.wrap = b.wrap;
         tl.circ = w.circ;
-        const double dl = b.dl[dir];
-        fused_tile<PH, false, W3>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, (0.5 * dt) / dl, (1.0 * dt) / dl, ch, fac, smem,
-                       status);
+        fused_tile<PH, false, W3>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, sp, b.dl[dir], apply_fac, smem, status);
     }
     flush_status(status, gstatus);
 }

@@ -81,6 +81,11 @@ inline int fused_geometry(pk_ctx* h, const Block& b, int dir, const Geom& g, Til
     const int maxt = VAR_T[var];
     tl->wrap = h->connected ? 0 : 1;
     tl->circ = (tl->wrap && L == b.n[dir] && b.n[dir] <= maxt) ? 1 : 0;
+    if (g.seg_len && g.seg_along) {                   // stacked instances: one whole segment per tile
+        L = g.seg_len;
+        tl->circ = 1;
+        if (L > maxt) return fail(h, PK_E_ARG, "instance segment longer than the variant's CTA size");
+    }
     const int T = tl->circ ? L : L + 8;
     while (P * T > maxt && P > 1) --P;
     if (P * T > maxt) return fail(h, PK_E_ARG, "fused sweep tile longer than the variant's CTA size");
@@ -234,6 +239,11 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
         int L = h->adjL[dir] > 0 ? h->adjL[dir] : default_adj_length(dir, b.n[dir], ADJ_T[var]);
         if (L > b.n[dir]) L = b.n[dir];
         tl.circ = (L == b.n[dir] && b.n[dir] <= ADJ_T[var]) ? 1 : 0;
+        if (g.seg_len && g.seg_along) {               // stacked instances: one whole segment per tile
+            L = g.seg_len;
+            tl.circ = 1;
+            if (L > ADJ_T[var]) return fail(h, PK_E_ARG, "instance segment longer than the adjoint variant's CTA size");
+        }
         if (!tl.circ && L > ADJ_T[var] - 6) L = ADJ_T[var] - 6;
         tl.T = tl.circ ? L : L + 6;
         tl.P = ADJ_T[var] / tl.T;

@@ -127,22 +127,15 @@ def _fourier_field(n: Tuple[int, int, int], kmin: float, kmax: float, slope: flo
     return out, (kx, ky, kz, mask)
 
 
-def mhd_turbulence(n: int = 256, seed: int = 1, mach: float = 1.0, b0: float = 0.2,
-                   db_frac: float = 0.1, gamma: float = 5.0 / 3.0, limiter: str = "moncen",
-                   cfl: float = 0.5):
-    """3D ideal-MHD decaying turbulence on one periodic block.
-
-    rho = 1 + 1% white noise (seed); v from random-phase Fourier modes with
-    1 <= |k| <= 4, amplitude ~ k^-2 (seed+1), scaled to rms Mach ``mach`` for the
-    sound speed of p0 = 1/gamma (c_s = 1); B = (b0, 0, 0) + curl of a random
-    vector potential (seed+2) scaled to rms ``db_frac * b0``; psi = 0.
-    """
-    setup = Setup(n=(n, n, n), xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0),
-                  fluids=[("ion", gamma)], magnetic=True, limiter=limiter, limiter_b=limiter,
-                  cfl=cfl, cfl_glm=0.7, smalld=1.0e-3)
+def mhd_turbulence_fields(n: int = 256, seed: int = 1, mach: float = 1.0, b0: float = 0.2,
+                          db_frac: float = 0.1, gamma: float = 5.0 / 3.0):
+    """Interior fields (rho, v[3], B[3]; each (n, n, n) as [k, j, i]) and the
+    uniform pressure p0 of the decaying-turbulence recipe: rho = 1 + 1% white
+    noise (seed); v from random-phase Fourier modes with 1 <= |k| <= 4,
+    amplitude ~ k^-2 (seed+1), scaled to rms Mach ``mach`` for the sound speed
+    of p0 = 1/gamma (c_s = 1); B = (b0, 0, 0) + curl of a random vector
+    potential (seed+2) scaled to rms ``db_frac * b0``."""
     p0 = 1.0 / gamma
-    g = setup.guards
-    u, b, psi = _empty(setup)
     shp = (n, n, n)
     rho = 1.0 + 0.01 * _rng(seed).standard_normal((n, n, n))
     v, _ = _fourier_field(shp, 1.0, 4.0, -2.0, _rng(seed + 1))
@@ -155,17 +148,50 @@ def mhd_turbulence(n: int = 256, seed: int = 1, mach: float = 1.0, b0: float = 0
     db = np.stack([np.fft.irfftn(bh[c], s=shp, axes=(0, 1, 2)) for c in range(3)])
     dbrms = math.sqrt(float(np.mean(db[0] ** 2 + db[1] ** 2 + db[2] ** 2)))
     db *= db_frac * b0 / dbrms
-    bx, by, bz = b0 + db[0], db[1], db[2]
-    emag = 0.5 * (bx * bx + by * by + bz * bz)
+    bf = np.stack([b0 + db[0], db[1], db[2]])
+    return rho, v, bf, p0
+
+
+def turbulence_setup(n: int, nz: Optional[int] = None, gamma: float = 5.0 / 3.0, limiter: str = "moncen",
+                     cfl: float = 0.5) -> Setup:
+    """The decaying-turbulence run on [0,1]^3 cells of 1/n (nz cells along z,
+    default n: nz = count * n stacks count instances along z)."""
+    nz = n if nz is None else nz
+    return Setup(n=(n, n, nz), xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, nz / n),
+                 fluids=[("ion", gamma)], magnetic=True, limiter=limiter, limiter_b=limiter,
+                 cfl=cfl, cfl_glm=0.7, smalld=1.0e-3)
+
+
+def mhd_turbulence(n: int = 256, seed: int = 1, mach: float = 1.0, b0: float = 0.2,
+                   db_frac: float = 0.1, gamma: float = 5.0 / 3.0, limiter: str = "moncen",
+                   cfl: float = 0.5):
+    """3D ideal-MHD decaying turbulence on one periodic block (the fields of
+    mhd_turbulence_fields, psi = 0)."""
+    setup = turbulence_setup(n, gamma=gamma, limiter=limiter, cfl=cfl)
+    rho, v, bf, p0 = mhd_turbulence_fields(n, seed, mach, b0, db_frac, gamma)
+    g = setup.guards
+    u, b, psi = _empty(setup)
+    emag = 0.5 * (bf[0] * bf[0] + bf[1] * bf[1] + bf[2] * bf[2])
     sl = (slice(g[2], g[2] + n), slice(g[1], g[1] + n), slice(g[0], g[0] + n))
     ui = u[sl]
     _set_fluid(setup, ui, 0, rho, v[0], v[1], v[2], p0, emag)
-    b[sl + (0,)] = bx
-    b[sl + (1,)] = by
-    b[sl + (2,)] = bz
+    b[sl + (0,)] = bf[0]
+    b[sl + (1,)] = bf[1]
+    b[sl + (2,)] = bf[2]
     fill_periodic(setup, u)
     fill_periodic(setup, b)
     return setup, u, b, psi
+
+
+def turbulence_ensemble(count: int = 64, n: int = 128, seed: int = 1):
+    """Parameters of the batched-adjoint ensemble: instance i is the
+    decaying-turbulence recipe at n^3 with seed seed + 10 i, rms Mach drawn
+    log-uniform in [0.5, 5] and B0 uniform in [0.05, 0.5] (one generator
+    seeded with ``seed``).  Returns a list of (seed, mach, b0)."""
+    rng = _rng(seed + 7919)
+    mach = np.exp(rng.uniform(math.log(0.5), math.log(5.0), size=count))
+    b0 = rng.uniform(0.05, 0.5, size=count)
+    return [(seed + 10 * i, float(mach[i]), float(b0[i])) for i in range(count)]
 
 
 def orszag_tang(n: int = 512, seed: int = 1, amp: float = 1.0e-3, corr_cells: float = 8.0,

@@ -231,6 +231,21 @@ class Simulation:
         """Replay each step's sweeps as a captured CUDA graph."""
         self._chk(self.lib.pk_use_graph(self.h, int(enable)), "pk_use_graph")
 
+    # -- independent instances stacked along z -------------------------------
+    def set_instances(self, count: int) -> None:
+        """Run ``count`` independent periodic problems, stacked along z in the
+        single block, with one launch per sweep and a time step each."""
+        self._chk(self.lib.pk_set_instances(self.h, count), "pk_set_instances")
+        self.instances = count
+
+    def instance_state(self, i: int) -> L.PkTimeState:
+        st = L.PkTimeState()
+        self._chk(self.lib.pk_get_instance_state(self.h, i, C.byref(st)), "pk_get_instance_state")
+        return st
+
+    def set_instance_state(self, i: int, st: L.PkTimeState) -> None:
+        self._chk(self.lib.pk_set_instance_state(self.h, i, C.byref(st)), "pk_set_instance_state")
+
     # -- connected blocks of one level --------------------------------------
     def set_domain(self, ncells, periodic=(True, True, True)) -> None:
         """Declare the level's cell grid; placed blocks then exchange guards."""
@@ -288,18 +303,22 @@ class Simulation:
     def grad_forward(self, nsteps: int, every: int = 0, dts=None) -> np.ndarray:
         """Advance ``nsteps`` steps recording what the adjoint needs; checkpoint
         every ``every`` steps (0: about sqrt(nsteps)).  ``dts`` replays a
-        prescribed dt sequence.  Returns the dt of each step."""
+        prescribed dt sequence.  Returns the dt of each step
+        (with stacked instances: an array [step, instance], and ``dts`` holds
+        that many values)."""
         if every <= 0:
             every = max(1, int(round(np.sqrt(max(nsteps, 1)))))
-        out = np.empty(max(nsteps, 1))
+        ni = getattr(self, "instances", 1)
+        out = np.empty(max(nsteps, 1) * ni)
         dp = None
         if dts is not None:
             dts = np.ascontiguousarray(dts, dtype=np.float64)
-            if dts.size < nsteps:
-                raise ValueError("dts has fewer than nsteps values")
+            if dts.size < nsteps * ni:
+                raise ValueError("dts has fewer than nsteps values (per instance)")
             dp = dts.ctypes.data
         self._chk(self.lib.pk_grad_forward(self.h, nsteps, every, dp, out.ctypes.data), "pk_grad_forward")
-        return out[:nsteps]
+        out = out[:nsteps * ni]
+        return out.reshape(nsteps, ni) if ni > 1 else out
 
     def grad_backward(self) -> None:
         self._chk(self.lib.pk_grad_backward(self.h), "pk_grad_backward")
