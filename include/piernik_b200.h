@@ -214,6 +214,24 @@ int pk_set_instance_state(pk_handle h, int32_t instance, const pk_time_state* st
 int pk_set_domain(pk_handle h, const int64_t ncells[3], const int32_t periodic[3]);
 int pk_block_place(pk_handle h, int32_t id, const int64_t off[3]);
 
+/* ---- Refined domains (several levels, refinement factor 2) ----
+ * pk_block_place_level puts a block on level `level`, whose grid is the
+ * base grid (pk_set_domain) refined `level` times, at offset off; the
+ * block's cell size must be the base cell size / 2**level.  With blocks on
+ * more than one level the domain must be periodic in every direction with
+ * extent, level 0 must cover it, blocks of level >= 1 need even offsets and
+ * extents and must lie two coarse cells inside their coarser level.  The
+ * sweeps then run stage by stage as the reference's sweep does
+ * (sweeps.F90:214-272): finest level first, each fine block's boundary
+ * fluxes restricted (2 x 2 mean) into the coarser block's update through the
+ * same face (fc_fluxes.F90:55-233, solve_cg_riemann.F90:353-362); after each
+ * stage the guard cells of each level are copied from its own blocks, then
+ * those over the coarser level only are prolonged from it, coarsest first:
+ * fluids by injection, B and psi by the O_I2 interpolation
+ * (cg_level_connected.F90:1150-1359, grid_container_prolong.F90:180-453).
+ * pk_timestep_raw reduces over leaf cells only (timestep.F90:463). */
+int pk_block_place_level(pk_handle h, int32_t id, int32_t level, const int64_t off[3]);
+
 /* ---- Domains spanning ranks (one process per GPU) ----
  * The reference exchanges guard cells between MPI ranks in the same
  * internal_boundaries pass (cg_list_bnd.F90:251-324, MPI isend/irecv of the

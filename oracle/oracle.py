@@ -73,6 +73,8 @@ class OBlock(C.Structure):
         ("dn_negative", C.c_int),
         ("ei_negative", C.c_int),
         ("uh_retry", C.POINTER(C.c_double)),
+        ("leaf", C.c_void_p),
+        ("eflx", C.c_void_p * 3),
     ]
 
 
@@ -129,6 +131,7 @@ def lib():
         L.o_run.argtypes = [P, B, S, C.c_int]
         L.o_nvar.argtypes = [P]
         L.o_run_multi.argtypes = [P, C.POINTER(B), C.c_int, S, C.c_int]
+        L.o_time_step_multi.argtypes = [P, C.POINTER(B), C.c_int, S]
         L.o_set_threads.argtypes = [C.c_int]
         L.o_run_fixed.argtypes = [P, B, S, C.POINTER(C.c_double), C.c_int]
         L.o_cfl_max.argtypes = [P]

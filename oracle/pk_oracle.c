@@ -568,7 +568,30 @@ static void o_work_free(o_work *w)
 /* solve (solve_cg_riemann.F90:318-376) or solve_u (:378-414) on one pencil of
  * length n: u1/b1 enter as the current state and leave as the Euler update of
  * u0/b0 by dtodx.  No f/c flux substitution (single-level blocks). */
-static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx, double ch, o_work *w)
+/* the ext_fluxes of one pencil: faces replaced (li, ri; -1 none) and faces
+ * recorded (lo, ro; -1 none) with their flux vectors */
+typedef struct o_pfc {
+    int li, ri, lo, ro;
+    const double *fli, *fri;
+    double *flo, *fro;
+} o_pfc;
+
+static void o_pfc_face(const o_lay *L, int mag, int m, o_work *w, int face, const double *in, double *out)
+{
+    const int nv = L->nv;
+    for (int c = 0; c < nv; ++c) {
+        if (in) w->flx[(size_t)c * m + face] = in[c];
+        if (out) out[c] = w->flx[(size_t)c * m + face];
+    }
+    if (mag)
+        for (int c = 0; c < 4; ++c) {
+            if (in) w->mflx[(size_t)c * m + face] = in[nv + c];
+            if (out) out[nv + c] = w->mflx[(size_t)c * m + face];
+        }
+}
+
+static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx, double ch, o_work *w,
+                           const o_pfc *pf)
 {
     const int nv = L->nv, m = n - 1;
     const int mag = cfg->magnetic;
@@ -618,6 +641,14 @@ static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx
             }
             for (int c = 0; c < nc; ++c) w->flx[(size_t)(L->beg[f] + c) * m + i] = fx[c];
         }
+    }
+
+    /* external fluxes (solve_cg_riemann.F90:353-362): li, ri replace, then lo, ro record */
+    if (pf) {
+        if (pf->li >= 0) o_pfc_face(L, mag, m, w, pf->li, pf->fli, NULL);
+        if (pf->ri >= 0) o_pfc_face(L, mag, m, w, pf->ri, pf->fri, NULL);
+        if (pf->lo >= 0) o_pfc_face(L, mag, m, w, pf->lo, NULL, pf->flo);
+        if (pf->ro >= 0) o_pfc_face(L, mag, m, w, pf->ro, NULL, pf->fro);
     }
 
     /* u1(2:nx-1,:) = u0(2:nx-1,:) + dtodx * (flx(:nx-2,:) - flx(2:,:))  (:365-374) */
@@ -734,7 +765,29 @@ int o_solve_cg(const o_cfg *cfg, o_block *blk, int ddim, int istep, double dt, d
                         w.b1[3 * (size_t)n + i] = blk->psi[cell];
                     }
                 }
-                o_pencil_solve(cfg, &L, n, dtodx, ch, &w);
+                o_pfc pf = {-1, -1, -1, -1, NULL, NULL, NULL, NULL};
+                const o_eflx *ef = blk->eflx[ddim];
+                if (ef) {
+                    const size_t pen = (size_t)(i1 - g[o1]) + (size_t)blk->n[o1] * (size_t)(i2 - g[o2]);
+                    const size_t fw = (size_t)nv + (mag ? 4 : 0);
+                    if (ef->in_face[0] && ef->in_face[0][pen] >= 0) {
+                        pf.li = ef->in_face[0][pen];
+                        pf.fli = ef->in_flx[0] + pen * fw;
+                    }
+                    if (ef->in_face[1] && ef->in_face[1][pen] >= 0) {
+                        pf.ri = ef->in_face[1][pen];
+                        pf.fri = ef->in_flx[1] + pen * fw;
+                    }
+                    if (ef->out_on[0] && ef->out_on[0][pen]) {
+                        pf.lo = g[ddim] - 1;
+                        pf.flo = ef->out_flx[0] + pen * fw;
+                    }
+                    if (ef->out_on[1] && ef->out_on[1][pen]) {
+                        pf.ro = g[ddim] + blk->n[ddim] - 1;
+                        pf.fro = ef->out_flx[1] + pen * fw;
+                    }
+                }
+                o_pencil_solve(cfg, &L, n, dtodx, ch, &w, ef ? &pf : NULL);
                 o_internal_sources(&L, n, &w);
                 o_care_for_positives(cfg, &L, n, &w, &dnneg, &eineg);
                 /* transpose back (:225-227) */
@@ -898,6 +951,9 @@ void o_timestep_raw(const o_cfg *cfg, const o_block *blk, double *dt_out, double
             for (int k = g[2]; k < g[2] + blk->n[2]; ++k)
                 for (int j = g[1]; j < g[1] + blk->n[1]; ++j)
                     for (int i = g[0]; i < g[0] + blk->n[0]; ++i) {
+                        if (blk->leaf &&
+                            !blk->leaf[((size_t)(k - g[2]) * blk->n[1] + (j - g[1])) * blk->n[0] + (i - g[0])])
+                            continue;                                      /* cg%leafmap (:463) */
                         size_t cell = ((size_t)k * ext[1] + j) * ext[0] + i;
                         const double *u = blk->u + cell * nv;
                         const double *b = cfg->magnetic ? blk->b + cell * 3 : NULL;

@@ -58,6 +58,21 @@ typedef struct o_cfg {
 #define O_CFL_WARN 1
 #define O_CFL_REDO 2
 
+/* Fine/coarse flux hooks of one block along one direction (fluxtypes.F90
+ * ext_fluxes, set by grid_container_fcflx.F90:148-259).  Pencils are
+ * numbered (i1 - g[o1]) + n[o1] * (i2 - g[o2]) with (o1, o2) the reference's
+ * ORTHO1 / ORTHO2 of the direction.  A flux vector is the pencil's nvar flux
+ * columns (in the pencil's column order) followed, when magnetic, by the 4
+ * mag_flx columns. */
+typedef struct o_eflx {
+    int *in_face[2];             /* per pencil: 0-based face (between pencil cells k and k+1) whose
+                                    flux is replaced, -1 none; [0] li, [1] ri */
+    double *in_flx[2];           /* per pencil: the replacing flux vector */
+    int *out_on[2];              /* per pencil: record the face before the first ([0], lo) or
+                                    after the last ([1], ro) interior cell */
+    double *out_flx[2];          /* per pencil: the recorded flux vector */
+} o_eflx;
+
 typedef struct o_block {
     int n[3];                    /* interior cells per direction */
     int nb;                      /* guard cells (dom%nb) */
@@ -68,6 +83,8 @@ typedef struct o_block {
     double *psi, *psih;          /* (NULL when !magnetic) */
     int dn_negative, ei_negative;
     double *uh_retry;            /* step-retry backup of u, b, psi (nvar+4 planes of the guard-inclusive block), or NULL */
+    const unsigned char *leaf;   /* interior cells not covered by a finer block (i fastest), or NULL: all */
+    const o_eflx *eflx[3];       /* fine/coarse flux hooks per direction, or NULL */
 } o_block;
 
 typedef struct o_state {         /* the reference's global time-step state */

@@ -3,6 +3,7 @@
 // PIERNIK's main loop for the split Riemann path.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -175,10 +176,198 @@ void free_segs(pk_ctx* h)
     h->xpeers.clear();
 }
 
+void free_levels(pk_ctx* h)
+{
+    cudaFree(h->d_runs);
+    cudaFree(h->d_run_start);
+    h->d_runs = nullptr;
+    h->d_run_start = nullptr;
+    h->run_beg.clear();
+    h->run_cells.clear();
+    for (int d = 0; d < 3; ++d) {
+        cudaFree(h->d_fc_int[d]);
+        cudaFree(h->d_in_flux[d]);
+        cudaFree(h->d_out_flux[d]);
+        h->d_fc_int[d] = nullptr;
+        h->d_in_flux[d] = nullptr;
+        h->d_out_flux[d] = nullptr;
+        h->d_src[d] = nullptr;
+        h->in_level_beg[d].clear();
+    }
+    for (auto& b : h->blocks) {
+        for (int d = 0; d < 3; ++d) b.fc[d] = FcArgs{};
+        cudaFree(b.leaf);
+        b.leaf = nullptr;
+        b.leaf_cells = -1;
+    }
+}
+
+template <class T>
+int upload_vec(pk_ctx* h, const std::vector<T>& v, T** dev)
+{
+    *dev = nullptr;
+    if (v.empty()) return PK_OK;
+    PK_CUDA(h, cudaMalloc(dev, sizeof(T) * v.size()));
+    PK_CUDA(h, cudaMemcpy(*dev, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return PK_OK;
+}
+
+// the fine/coarse couplings of a refined domain (build_levels) on the device
+int levels_prepare(pk_ctx* h)
+{
+    const int nl = (int)h->blocks.size();
+    std::vector<LBlock> lb(nl);
+    double dl0[3] = {0, 0, 0};
+    for (int i = 0; i < nl; ++i)
+        if (h->blocks[i].level == 0)
+            for (int d = 0; d < 3; ++d) dl0[d] = h->blocks[i].dl[d];
+    for (int i = 0; i < nl; ++i) {
+        const Block& b = h->blocks[i];
+        lb[i].level = b.level;
+        for (int d = 0; d < 3; ++d) {
+            lb[i].n[d] = b.n[d];
+            lb[i].g[d] = b.g[d];
+            lb[i].off[d] = b.off[d];
+            if (h->dom[d] > 1 && b.dl[d] != std::ldexp(dl0[d], -b.level))
+                return fail(h, PK_E_ARG, "a block's cell size must be the base cell size / 2**level");
+        }
+    }
+    for (int d = 0; d < 3; ++d)
+        if (h->dom[d] > 1 && !h->dom_periodic[d])
+            return fail(h, PK_E_UNSUPPORTED, "refined domains are periodic in every direction");
+    LevelPlan plan;
+    std::string err;
+    if (!build_levels(lb, h->dom, plan, err)) return fail(h, PK_E_ARG, err);
+    free_levels(h);
+    const int NV = h->nplanes;
+    // prolongation rows, start counts relative to each level's first row
+    std::vector<PRunDev> runs(plan.runs.size());
+    std::vector<long long> start(plan.runs.size());
+    h->run_beg.assign(plan.run_level_beg.begin(), plan.run_level_beg.end());
+    h->run_cells.assign(plan.max_level + 1, 0);
+    for (int L = 1; L <= plan.max_level; ++L) {
+        long long acc = 0;
+        for (long long r = plan.run_level_beg[L]; r < plan.run_level_beg[L + 1]; ++r) {
+            const PRun& s = plan.runs[r];
+            runs[r] = PRunDev{s.fb, s.cb, s.fx, s.fy, s.fz, s.len, s.cx, s.cy, s.cz, s.px, s.py, s.pz};
+            start[r] = acc;
+            acc += s.len;
+        }
+        h->run_cells[L] = acc;
+    }
+    if (int rc = upload_vec(h, runs, &h->d_runs)) return rc;
+    if (int rc = upload_vec(h, start, &h->d_run_start)) return rc;
+    // per direction: the blocks' slot tables, then in faces, then flux sources
+    for (int d = 0; d < 3; ++d) {
+        const FcDir& F = plan.fc[d];
+        h->in_level_beg[d] = F.in_level_beg;
+        std::vector<int> ints;
+        std::vector<long long> in_off(nl, -1), out_off(nl, -1);
+        for (int i = 0; i < nl; ++i) {
+            if (!F.in_slot[i].empty()) {
+                in_off[i] = (long long)ints.size();
+                ints.insert(ints.end(), F.in_slot[i].begin(), F.in_slot[i].end());
+            }
+            if (!F.out_slot[i].empty()) {
+                out_off[i] = (long long)ints.size();
+                ints.insert(ints.end(), F.out_slot[i].begin(), F.out_slot[i].end());
+            }
+        }
+        const long long face_off = (long long)ints.size();
+        ints.insert(ints.end(), F.in_face.begin(), F.in_face.end());
+        const long long src_off = (long long)ints.size();
+        ints.insert(ints.end(), F.src.begin(), F.src.end());
+        if (int rc = upload_vec(h, ints, &h->d_fc_int[d])) return rc;
+        const size_t nin = F.in_face.size();
+        if (nin) PK_CUDA(h, cudaMalloc(&h->d_in_flux[d], sizeof(double) * NV * nin));
+        if (F.n_out) PK_CUDA(h, cudaMalloc(&h->d_out_flux[d], sizeof(double) * NV * F.n_out));
+        h->d_src[d] = nin ? h->d_fc_int[d] + src_off : nullptr;
+        for (int i = 0; i < nl; ++i) {
+            FcArgs& f = h->blocks[i].fc[d];
+            f.in_slot = in_off[i] >= 0 ? h->d_fc_int[d] + in_off[i] : nullptr;
+            f.in_face = nin ? h->d_fc_int[d] + face_off : nullptr;
+            f.in_flux = h->d_in_flux[d];
+            f.out_slot = out_off[i] >= 0 ? h->d_fc_int[d] + out_off[i] : nullptr;
+            f.out_flux = h->d_out_flux[d];
+        }
+    }
+    for (int i = 0; i < nl; ++i) {
+        Block& b = h->blocks[i];
+        b.leaf_cells = plan.leaf_cells[i];
+        if (!plan.leaf[i].empty())
+            if (int rc = upload_vec(h, plan.leaf[i], &b.leaf)) return rc;
+    }
+    h->fc_scale = 1.0 / std::ldexp(1.0, plan.eff_dim - 1);
+    h->max_level = plan.max_level;
+    h->batch_dirty = true;
+    return PK_OK;
+}
+
+// prolong_bnd_from_coarser of every refined level, coarsest first
+int prolong_guards(pk_ctx* h)
+{
+    for (int L = 1; L <= h->max_level; ++L) {
+        const long long cells = h->run_cells[L];
+        if (!cells) continue;
+        const long long r0 = h->run_beg[L];
+        const int nr = (int)(h->run_beg[L + 1] - r0);
+        k_prolong<<<grid1d(cells, 256), 256, 0, h->stream>>>(h->d_runs + r0, h->d_run_start + r0, nr, cells,
+                                                             h->d_xptr[h->cur], h->nvf, h->cfg.magnetic ? 4 : 0,
+                                                             h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+    }
+    return PK_OK;
+}
+
 int exchange_prepare(pk_ctx* h)
 {
     if (!h->connected) return PK_OK;
     const int nl = (int)h->blocks.size();
+    int maxl = 0;
+    for (auto& b : h->blocks) maxl = std::max(maxl, b.level);
+    if (h->x_dirty && maxl > 0) {
+        // one exchange plan per level, on that level's grid
+        if (!h->remote.empty()) return fail(h, PK_E_UNSUPPORTED, "refined domains run on one rank");
+        std::vector<XSeg> all;
+        for (int L = 0; L <= maxl; ++L) {
+            std::vector<int> ids;
+            std::vector<XBlock> xb;
+            for (int i = 0; i < nl; ++i) {
+                const Block& b = h->blocks[i];
+                if (!b.placed) return fail(h, PK_E_STATE, "every block of a connected domain must be placed (pk_block_place)");
+                if (b.level != L) continue;
+                XBlock x;
+                for (int d = 0; d < 3; ++d) {
+                    x.n[d] = b.n[d];
+                    x.g[d] = b.g[d];
+                    x.off[d] = b.off[d];
+                }
+                ids.push_back(i);
+                xb.push_back(x);
+            }
+            long long dom[3];
+            for (int d = 0; d < 3; ++d) dom[d] = h->dom[d] > 1 ? h->dom[d] << L : 1;
+            std::vector<XSeg> segs;
+            std::string err;
+            if (!build_exchange(xb, dom, h->dom_periodic, segs, err)) return fail(h, PK_E_ARG, err);
+            for (XSeg s : segs) {
+                s.dst = ids[s.dst];
+                s.src = ids[s.src];
+                all.push_back(s);
+            }
+        }
+        if (int rc = levels_prepare(h)) return rc;
+        PK_CUDA(h, cudaStreamSynchronize(h->stream));
+        free_segs(h);
+        if (int rc = upload_segs(h, all, &h->xlocal)) return rc;
+        h->x_dirty = false;
+    }
+    if (h->x_dirty && h->max_level > 0) {              // no longer refined
+        free_levels(h);
+        h->max_level = 0;
+        h->batch_dirty = true;
+    }
     if (h->x_dirty) {
         // this rank's blocks first, then the other ranks'
         std::vector<XBlock> xb(nl + h->remote.size());
@@ -253,6 +442,7 @@ int exchange_guards(pk_ctx* h, int dir = -1)
         h->launches += 1;
     }
     if (h->halo_cb && !h->xpeers.empty()) h->halo_cb(h->comm_ctx, dir);
+    if (h->max_level > 0) return prolong_guards(h);
     return PK_OK;
 }
 
@@ -286,6 +476,8 @@ bool connected_fused_ok(pk_ctx* h)
 bool fused_ok(pk_ctx* h)
 {
     if (h->cfg.integration_order != 2) return false;
+    for (auto& b : h->blocks)
+        if (b.level > 0) return false;                 // refined domains sweep stage by stage
     if (h->connected) return connected_fused_ok(h);
     for (auto& b : h->blocks)
         for (int d = 0; d < 3; ++d)
@@ -328,6 +520,7 @@ int build_batch(pk_ctx* h)
                 d.dl[k] = b.dl[k];
             }
             d.wrap = h->connected ? 0 : 1;
+            d.leaf = b.leaf;
         }
         cudaFree(h->d_desc[p]);
         h->d_desc[p] = nullptr;
@@ -432,15 +625,30 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
         return PK_OK;
     }
     const int nst = h->cfg.integration_order == 1 ? 1 : 2;
+    if (int rc = exchange_prepare(h)) return rc;       // a refined domain's couplings
     for (int s = 1; s <= nst; ++s) {
         const double rk = (h->cfg.integration_order == 1) ? 1.0 : (s == 1 ? 0.5 : 1.0);
-        for (auto& b : h->blocks) {
-            if (b.n[dir] <= 1) continue;
-            if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
-            if (b.ext[dir] > STAGE_MAXT)
-                if (int rc = ensure_pingpong(h)) return rc;
-            const double dtodx = (rk * dt) / b.dl[dir];
-            if (int rc = ops->stage(h, b, dir, s == 1, dtodx, ch)) return rc;
+        // finest level first: its boundary fluxes replace the coarser level's (sweeps.F90:218-262)
+        for (int L = h->max_level; L >= 0; --L) {
+            for (auto& b : h->blocks) {
+                if (b.n[dir] <= 1 || b.level != L) continue;
+                if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+                if (b.ext[dir] > STAGE_MAXT)
+                    if (int rc = ensure_pingpong(h)) return rc;
+                const double dtodx = (rk * dt) / b.dl[dir];
+                if (int rc = ops->stage(h, b, dir, s == 1, dtodx, ch)) return rc;
+            }
+            if (L > 0 && h->d_src[dir]) {
+                const int beg = h->in_level_beg[dir][L - 1], end = h->in_level_beg[dir][L];
+                if (end > beg) {
+                    const long long n = (long long)(end - beg) * h->nplanes;
+                    k_restrict_flux<<<grid1d(n, 256), 256, 0, h->stream>>>(h->d_src[dir], beg, end, h->nplanes,
+                                                                           h->d_out_flux[dir], h->d_in_flux[dir],
+                                                                           h->fc_scale);
+                    PK_CUDA(h, cudaGetLastError());
+                    h->launches += 1;
+                }
+            }
         }
         for (auto& b : h->blocks)
             if (int rc = fill_guards_block(h, b)) return rc;
@@ -641,6 +849,7 @@ int pk_destroy(pk_handle h)
     cudaFree(h->lam_tmp);
     cudaFree(h->lam_m1);
     free_segs(h);
+    free_levels(h);
     cudaFree(h->d_xptr[0]);
     cudaFree(h->d_xptr[1]);
     for (auto& b : h->blocks) cudaFree(b.retry);
@@ -999,12 +1208,21 @@ int pk_set_comm(pk_handle h, pk_halo_fn halo, pk_reduce_fn reduce, void* ctx)
 
 int pk_block_place(pk_handle h, int32_t id, const int64_t off[3])
 {
+    return pk_block_place_level(h, id, 0, off);
+}
+
+int pk_block_place_level(pk_handle h, int32_t id, int32_t level, const int64_t off[3])
+{
     Block* b;
     if (int rc = get_block(h, id, &b)) return rc;
     if (!off) return fail(h, PK_E_ARG, "null offset");
+    if (level < 0 || level > 8) return fail(h, PK_E_ARG, "level must lie in 0..8");
+    if (level > 0 && h->ninst > 1) return fail(h, PK_E_STATE, "stacked instances are not refined");
     for (int d = 0; d < 3; ++d) b->off[d] = off[d];
+    b->level = level;
     b->placed = true;
     h->x_dirty = true;
+    h->batch_dirty = true;
     invalidate_graph(h);
     return PK_OK;
 }
@@ -1028,6 +1246,7 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out)
 {
     if (!h) return PK_E_ARG;
     if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
+    if (int rc = exchange_prepare(h)) return rc;       // a refined domain's leaf masks
     const int nb = (int)h->blocks.size();
     PK_CUDA(h, cudaMemsetAsync(h->d_red, 0, sizeof(unsigned long long) * 12 * nb, h->stream));
     CflArgs a;
@@ -1060,6 +1279,7 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out)
     double dt = DBL_MAX, c_all = 0.0;                  // timestep.F90:161-162
     for (int i = 0; i < nb; ++i) {
         const Block& b = h->blocks[i];
+        if (b.leaf_cells == 0) continue;               // wholly covered by finer blocks
         for (int f = 0; f < h->cfg.nfluids; ++f) {
             double cm[4];
             for (int d = 0; d < 4; ++d) {

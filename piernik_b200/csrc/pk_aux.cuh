@@ -36,8 +36,10 @@ struct CflArgs {
 // reduction with one division per direction.  Maxima of positive doubles are
 // reduced as their bit patterns (order-independent, deterministic).
 // out[f*4 + d] (d < 3) and out[f*4 + 3] hold the bit patterns.
+// leaf (or null: every cell) marks the interior cells that no finer block
+// covers (cg%leafmap, timestep.F90:463); the others are skipped.
 PK_DEV void cfl_block(const BoxGeom& b, const double* __restrict__ u, const CflArgs& a, unsigned long long* __restrict__ out,
-                      long long first, long long stride)
+                      long long first, long long stride, const unsigned char* __restrict__ leaf = nullptr)
 {
     const double small = 1.1754943508222875e-38;   // tiny(real(1.0,4)), constants.F90:104
     const long long ncell = (long long)b.n[0] * b.n[1] * b.n[2];
@@ -47,6 +49,7 @@ PK_DEV void cfl_block(const BoxGeom& b, const double* __restrict__ u, const CflA
 #pragma unroll
         for (int d = 0; d < 4; ++d) cm[f][d] = small;
     for (long long c = first; c < ncell; c += stride) {
+        if (leaf && !leaf[c]) continue;
         const int i = (int)(c % b.n[0]);
         const long long r = c / b.n[0];
         const int j = (int)(r % b.n[1]);
@@ -135,8 +138,9 @@ static __global__ void k_cfl_blocks(const BlockDesc* __restrict__ blocks, CflArg
     }
     b.plane = d.plane;
     cfl_block(b, d.in, a, out + 12 * blockIdx.y, (long long)blockIdx.x * blockDim.x + threadIdx.x,
-              (long long)gridDim.x * blockDim.x);
+              (long long)gridDim.x * blockDim.x, d.leaf);
 }
+
 
 // psi *= fac over the whole plane, guard cells included (hdc.F90:338)
 static __global__ void k_scale(double* __restrict__ p, long long n, double fac)
@@ -323,6 +327,88 @@ static __global__ void k_copy_pencils(BoxGeom b, int dir, const double* __restri
         const int k = lo[2] + (int)(r / ny);
         const long long o = cell_index(b, i, j, k);
         for (int v = 0; v < nplanes; ++v) dst[(long long)v * b.plane + o] = src[(long long)v * b.plane + o];
+    }
+}
+
+// ---- refined domains -------------------------------------------------------
+
+// The fine->coarse flux sum of send_cg_coarsebnd (fc_fluxes.F90:213-225): each
+// coarse face takes 0 + the fine faces' fluxes in the reference's loop order
+// (ORTHO1 outer, ORTHO2 inner), times 1 / 2**(eff_dim - 1).
+static __global__ void k_restrict_flux(const int* __restrict__ src, int beg, int end, int nv,
+                                       const double* __restrict__ out_flux, double* __restrict__ in_flux, double scale)
+{
+    const long long n = (long long)(end - beg) * nv;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int slot = beg + (int)(t / nv);
+        const int v = (int)(t % nv);
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int s = src[4 * slot + q];
+            if (s >= 0) acc = acc + out_flux[(long long)s * nv + v];
+        }
+        in_flux[(long long)slot * nv + v] = scale * acc;
+    }
+}
+
+struct PRunDev {
+    int fb, cb;
+    int fx, fy, fz, len;
+    int cx, cy, cz;
+    int px, py, pz;
+};
+
+// one centred O_I2 interpolation along a direction (grid_container_prolong.F90,
+// O_I2 coefficients P_1 = -1/8, P0 = 1, P1 = 1/8): the left child takes
+// P1 c(-1) + P0 c(0) + P_1 c(+1), the right child P_1 c(-1) + P0 c(0) + P1 c(+1),
+// summed left to right
+PK_DEV double prolong_i2(double cm, double c0, double cp, int par)
+{
+    const double P1 = 1.0 / 8.0, P0 = 1.0, P_1 = -1.0 / 8.0;
+    return par == 0 ? (P1 * cm + P0 * c0) + P_1 * cp : (P_1 * cm + P0 * c0) + P1 * cp;
+}
+
+// prolong_bnd_from_coarser (cg_level_connected.F90:1150-1359) for the guard
+// cells of one level: u by injection (ord_fluid_prolong = O_INJ), B and psi by
+// the directionally split O_I2 interpolation (ord_mag_prolong, x then y then
+// z over the 3 x 3 x 3 coarse neighbourhood, as prolong() does).  runs has
+// nruns rows; start[r] is the running cell count before run r.
+static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long long* __restrict__ start, int nruns,
+                                 long long total, const XPtr* __restrict__ blocks, int nu, int nmag, int has_x,
+                                 int has_y, int has_z)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nruns - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const PRunDev r = runs[lo];
+        const int i = (int)(t - start[lo]);
+        const XPtr F = blocks[r.fb], C = blocks[r.cb];
+        const int px = (r.px + i) & 1;
+        const int cx = r.cx + ((r.px + i) >> 1);
+        const long long fo = ((long long)r.fz * F.ext[1] + r.fy) * F.ext[0] + (r.fx + i);
+        const long long co = ((long long)r.cz * C.ext[1] + r.cy) * C.ext[0] + cx;
+        for (int v = 0; v < nu; ++v) F.u[(long long)v * F.plane + fo] = C.u[(long long)v * C.plane + co];
+        const long long sx = has_x, sy = has_y ? C.ext[0] : 0, sz = has_z ? (long long)C.ext[0] * C.ext[1] : 0;
+        for (int v = nu; v < nu + nmag; ++v) {
+            const double* c = C.u + (long long)v * C.plane + co;
+            double Y[3];
+            for (int kz = -1; kz <= 1; ++kz) {
+                if (!has_z && kz != 0) continue;
+                double X[3];
+                for (int ky = -1; ky <= 1; ++ky) {
+                    if (!has_y && ky != 0) continue;
+                    const double* row = c + ky * sy + kz * sz;
+                    X[ky + 1] = has_x ? prolong_i2(row[-sx], row[0], row[sx], px) : row[0];
+                }
+                Y[kz + 1] = has_y ? prolong_i2(X[0], X[1], X[2], r.py) : X[1];
+            }
+            F.u[(long long)v * F.plane + fo] = has_z ? prolong_i2(Y[0], Y[1], Y[2], r.pz) : Y[1];
+        }
     }
 }
 

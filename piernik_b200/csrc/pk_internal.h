@@ -10,6 +10,7 @@
 #include "../../include/piernik_b200.h"
 #include "pk_aux.cuh"
 #include "pk_kernels.cuh"
+#include "pk_levels.h"
 
 namespace pk {
 
@@ -20,8 +21,8 @@ namespace pk {
 constexpr int NVARIANT = 7;
 constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512};
 constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1};
-constexpr int STAGE_MAXT = 320;
-constexpr int W3_VARIANT = 2;          // interpol_str = 'weno3' runs this launch-bound variant only        // threads per CTA of the stage kernel
+constexpr int STAGE_MAXT = 320;       // threads per CTA of the stage kernel
+constexpr int W3_VARIANT = 2;          // interpol_str = 'weno3' runs this launch-bound variant only
 
 struct Block {
     int n[3], g[3], ext[3];
@@ -36,6 +37,10 @@ struct Block {
     int seg_len = 0;                       // independent instances stacked along z: cells per instance
     long long off[3] = {0, 0, 0};          // first interior cell on the level's cell grid (connected domains)
     bool placed = false;
+    int level = 0;                         // refinement level (0: base)
+    FcArgs fc[3] = {};                     // fine/coarse flux couplings per sweep direction (device)
+    unsigned char* leaf = nullptr;         // device interior leaf mask (null: every cell is a leaf)
+    long long leaf_cells = -1;             // cells of the mask set (-1: all)
 };
 
 struct pk_dir_tile { int P, L, V; };
@@ -119,6 +124,18 @@ struct pk_ctx {
     std::vector<pk::XPeerDev> xpeers;   // copies to and from each other rank
     std::vector<pk::RemoteBlock> remote;
     pk::XPtr* d_xptr[2] = {nullptr, nullptr};   // block states of parity 0 / 1
+    // refined domains (pk_block_place_level): the fine/coarse couplings on the device
+    int max_level = 0;
+    pk::PRunDev* d_runs = nullptr;              // prolongation rows, by fine level
+    long long* d_run_start = nullptr;           // running cell count of each row within its level
+    std::vector<long long> run_beg;             // rows of fine level L: [run_beg[L], run_beg[L+1])
+    std::vector<long long> run_cells;           // guard cells prolonged into level L
+    int* d_fc_int[3] = {nullptr, nullptr, nullptr};          // per-pencil slot tables, in faces, flux sources
+    double* d_in_flux[3] = {nullptr, nullptr, nullptr};      // restricted fluxes per in slot
+    double* d_out_flux[3] = {nullptr, nullptr, nullptr};     // fine boundary fluxes per out slot
+    const int* d_src[3] = {nullptr, nullptr, nullptr};
+    std::vector<int> in_level_beg[3];           // in slots of coarse level L: [in_level_beg[L], in_level_beg[L+1])
+    double fc_scale = 1.0;                      // 1 / 2**(eff_dim - 1)
     pk_halo_fn halo_cb = nullptr;       // moves the halo of other ranks (host callback)
     pk_reduce_fn reduce_cb = nullptr;   // min / max over ranks for the time step
     void* comm_ctx = nullptr;

@@ -118,10 +118,15 @@ struct Smem {
 //                wrapped slot in a circular whole-pencil tile)
 //   W3     interpol_str = 'weno3' face states (a compile-time choice, so that the
 //          limited-linear kernels carry no WENO3 code)
-template <class PH, bool REC = false, bool W3 = false>
+//   FC     fine/coarse flux hooks (ext_fluxes, solve_cg_riemann.F90:353-362): where
+//          fc_in is set, the flux through this cell's right face is replaced by
+//          the NV values there (li / ri); where fc_out is set, it is stored there
+//          (lo / ro), before the update
+template <class PH, bool REC = false, bool W3 = false, bool FC = false>
 PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, double (&w)[PH::NV], const double* u0src,
                      const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
-                     const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr)
+                     const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr,
+                     const double* fc_in = nullptr, double* fc_out = nullptr)
 {
     constexpr int NV = PH::NV;
     const int PT = sm.PT;
@@ -160,6 +165,17 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
     __syncthreads();
     if (r.flux) riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, pp);
     __syncthreads();
+    if constexpr (FC) {
+        if (r.flux && fc_in) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = fc_in[v];
+        }
+        if (r.flux && fc_out) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fc_out[v] = sm.Q[v * PT + me];
+        }
+        __syncthreads();
+    }
     if (r.upd) {
         double u0[NV];
         load_cell<PH>(u0src, off, g, u0);
@@ -294,6 +310,7 @@ struct BlockDesc {
     int ext[3], g[3], n[3];
     double dl[3];
     int wrap;               // Tile::wrap for this block's tiles
+    const unsigned char* leaf = nullptr;   // interior leaf mask for the CFL reduction (null: every cell)
 };
 
 struct WorkItem {
@@ -362,10 +379,21 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
 // uin and uout may alias only when one chunk covers the whole pencil (every
 // load of a pencil then precedes every store of it, within one CTA).
 // -------------------------------------------------------------------------
-template <class PH, int MAXT, bool W3 = false>
+// The fine/coarse flux couplings of one block along one sweep direction.
+// Pencils are numbered i1 + n1 * i2; slots index the per-direction arrays
+// shared by all blocks.
+struct FcArgs {
+    const int* in_slot;      // [2][pencils]: slot of the coarse-side override, -1 none
+    const int* in_face;      // per in slot: storage index of the cell whose right face takes it
+    const double* in_flux;   // per in slot: NV restricted fine fluxes
+    const int* out_slot;     // [2][pencils]: slot of the block's own LO / HI boundary face, -1 none
+    double* out_flux;        // per out slot: NV fluxes
+};
+
+template <class PH, int MAXT, bool W3 = false, bool FC = false>
 __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* uin, double* uout,
                                                double* uh, PhysParams pp, int first, double dtodx, double ch,
-                                               unsigned* __restrict__ gstatus)
+                                               unsigned* __restrict__ gstatus, FcArgs fc = FcArgs{})
 {
     extern __shared__ double smem[];
     constexpr int NV = PH::NV;
@@ -402,7 +430,28 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     const bool prev_flux = (t >= 1) && (s >= 1) && ((s - 1 == 0) || (t - 1 >= 1));
     r.upd = valid && s >= 1 && s <= n - 2 && prev_flux && r.flux;
     r.keep = !r.upd && valid && (s == 0 || s == n - 1);        // u1 = u at the pencil ends, then floors
-    rk_stage<PH, false, W3>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status);
+    const double* fc_in = nullptr;
+    double* fc_out = nullptr;
+    if constexpr (FC) {
+        if (valid) {
+            const long long np = (long long)g.n1 * g.n2;
+            const long long pen = i1 + (long long)g.n1 * i2;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                if (fc.in_slot) {
+                    const int sl = fc.in_slot[side * np + pen];
+                    if (sl >= 0 && fc.in_face[sl] == s) fc_in = fc.in_flux + (long long)sl * PH::NV;
+                }
+                if (fc.out_slot) {
+                    const int sl = fc.out_slot[side * np + pen];
+                    if (sl >= 0 && s == (side == 0 ? g.g_d - 1 : g.g_d + g.n_d - 1))
+                        fc_out = fc.out_flux + (long long)sl * PH::NV;
+                }
+            }
+        }
+    }
+    rk_stage<PH, false, W3, FC>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status,
+                                nullptr, fc_in, fc_out);
     if (own) store_cell<PH>(uout, off, g, w);
     flush_status(status, gstatus);
 }

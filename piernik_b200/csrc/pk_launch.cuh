@@ -56,6 +56,10 @@ int set_smem_attr(pk_ctx* h)
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -328,12 +332,11 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double c
     const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    if (h->pp.weno3)
-        k_stage<PH, STAGE_MAXT, true><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx,
-                                                                         ch, h->d_status);
-    else
-        k_stage<PH, STAGE_MAXT><<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx, ch,
-                                                                       h->d_status);
+    const FcArgs& fc = b.fc[dir];
+    const bool hooks = fc.in_slot || fc.out_slot;      // a fine/coarse boundary crosses this block's pencils
+    auto* kern = h->pp.weno3 ? (hooks ? k_stage<PH, STAGE_MAXT, true, true> : k_stage<PH, STAGE_MAXT, true, false>)
+                             : (hooks ? k_stage<PH, STAGE_MAXT, false, true> : k_stage<PH, STAGE_MAXT, false, false>);
+    kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx, ch, h->d_status, fc);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;

@@ -331,3 +331,119 @@ def batched_blocks(nblocks: int = 512, seed: int = 1, sizes=(16, 24, 32, 48, 64)
         fill_periodic(setup, u)
         out.append((setup, u, b, psi))
     return out
+
+
+def _composition(total: int, sizes, rng: np.random.Generator):
+    """Split total cells into consecutive pieces with sizes from ``sizes``."""
+    for _ in range(1000):
+        parts, left = [], total
+        while left > 0:
+            fit = [s for s in sizes if s <= left]
+            if not fit:
+                break
+            s = int(rng.choice(fit))
+            parts.append(s)
+            left -= s
+        if left == 0:
+            return parts
+    raise ValueError(f"{total} cells cannot be split into pieces from {sizes}")
+
+
+def refined_layout(dom, regions, sizes=(16, 24, 32, 48, 64), seed: int = 1):
+    """Blocks of a refined periodic domain.  dom: base cells per direction;
+    regions[L-1] = (lo, hi): the box of level L >= 1 on the level-L grid
+    (even bounds, two coarse cells inside level L-1).  Every level is cut
+    into blocks by per-axis compositions drawn from ``sizes`` (seeded).
+    Returns a list of (level, off, n)."""
+    rng = _rng(seed)
+    boxes = [((0, 0, 0), tuple(dom))] + [tuple(r) for r in regions]
+    out = []
+    for L, (lo, hi) in enumerate(boxes):
+        cuts = []
+        for d in range(3):
+            ext = hi[d] - lo[d]
+            if dom[d] == 1:
+                cuts.append([(0, 1)])
+                continue
+            parts = _composition(ext, [s for s in sizes if L == 0 or s % 2 == 0], rng)
+            edges = np.concatenate([[0], np.cumsum(parts)]) + lo[d]
+            cuts.append([(int(edges[k]), int(parts[k])) for k in range(len(parts))])
+        for oz, nz in cuts[2]:
+            for oy, ny in cuts[1]:
+                for ox, nx in cuts[0]:
+                    out.append((L, (ox, oy, oz), (nx, ny, nz)))
+    return out
+
+
+def refined_blocks(dom, layout, setup: Setup, fields, dl0: float = 0.125):
+    """Setups and states of the blocks of ``refined_layout``: block cells of
+    level L have size dl0 / 2**L (dl0 a power of two keeps every cell size
+    exact); ``fields(setup, X, Y, Z)`` returns (u, b, psi) at cell centres
+    (guard cells included), with X, Y, Z in base-cell units.  Returns a list
+    of (setup, level, off, u, b, psi)."""
+    out = []
+    for L, off, n in layout:
+        dl = dl0 / 2 ** L
+        s = setup.replace(n=tuple(n), xmin=tuple(off[d] * dl if dom[d] > 1 else -0.5 * dl0 for d in range(3)),
+                          xmax=tuple((off[d] + n[d]) * dl if dom[d] > 1 else 0.5 * dl0 for d in range(3)))
+        X, Y, Z = (_centres(s, d) / dl0 for d in range(3))
+        Zg, Yg, Xg = np.meshgrid(Z, Y, X, indexing="ij")
+        u, b, psi = fields(s, Xg, Yg, Zg)
+        out.append((s, L, tuple(off), u, b, psi))
+    return out
+
+
+def blast_fields(centre, radius: float, e_in: float = 10.0, p0: float = 1.0e-5, b0=(0.1, 0.05, 0.0),
+                 dust_rho: float = 0.01):
+    """(u, b, psi) at cell centres: every fluid at rest with density 1 (dust
+    ``dust_rho``) and pressure p0, the gaseous fluids with thermal energy
+    density e_in inside ``radius`` base cells of ``centre``; uniform B = b0,
+    psi = 0 when magnetised."""
+    def f(setup, X, Y, Z):
+        u, b, psi = _empty(setup)
+        r = np.sqrt((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2)
+        hot = np.where(r < radius, e_in, 0.0)
+        emag = None
+        if setup.magnetic:
+            for c in range(3):
+                b[..., c] = b0[c]
+            emag = 0.5 * (b0[0] ** 2 + b0[1] ** 2 + b0[2] ** 2)
+        for fl, (kind, gam) in enumerate(setup.fluids):
+            rho = dust_rho if kind == "dst" else 1.0
+            _set_fluid(setup, u, fl, rho, 0.0, 0.0, 0.0, p0, emag if kind == "ion" else None)
+            if kind != "dst":
+                beg = sum(4 if k == "dst" else 5 for k, _ in setup.fluids[:fl])
+                u[..., beg + 4] += hot
+        return u, b, psi
+    return f
+
+
+def wave_fields(dom, seed: int = 1, amp: float = 0.2):
+    """Smooth periodic (u, b, psi) at cell centres: a few seeded sinusoids
+    with the period of the base domain (``dom`` base cells) per field, a
+    function of position only, so that every level samples the same state."""
+    rng = _rng(seed)
+    per = [float(max(n, 1)) for n in dom]
+
+    def f(setup, X, Y, Z):
+        u, b, psi = _empty(setup)
+
+        def wave(a):
+            k = rng.integers(1, 3, size=3)
+            ph = rng.uniform(0, 2 * np.pi, size=3)
+            return a * (np.sin(2 * np.pi * k[0] * X / per[0] + ph[0]) * np.cos(2 * np.pi * k[1] * Y / per[1] + ph[1])
+                        + np.sin(2 * np.pi * k[2] * Z / per[2] + ph[2]))
+        state = rng.bit_generator.state
+        emag = None
+        if setup.magnetic:
+            for c in range(3):
+                b[..., c] = (0.5 if c == 0 else 0.2) + wave(0.15)
+            psi[...] = wave(0.02)
+            emag = 0.5 * (b ** 2).sum(-1)
+        for fl, (kind, gam) in enumerate(setup.fluids):
+            rho = 1.0 + wave(amp)
+            p = 0.8 + wave(0.15)
+            _set_fluid(setup, u, fl, rho, wave(0.3), wave(0.3), wave(0.3), p, emag if kind == "ion" else None)
+        rng.bit_generator.state = state
+        return u, b, psi
+    return f

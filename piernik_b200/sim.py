@@ -253,10 +253,11 @@ class Simulation:
         p = (C.c_int32 * 3)(*[int(bool(x)) for x in periodic])
         self._chk(self.lib.pk_set_domain(self.h, n, p), "pk_set_domain")
 
-    def place_block(self, block: int, off) -> None:
-        """Put the block's first interior cell at ``off`` on the level's grid."""
+    def place_block(self, block: int, off, level: int = 0) -> None:
+        """Put the block's first interior cell at ``off`` on the grid of its
+        refinement level (the base grid refined ``level`` times)."""
         o = (C.c_int64 * 3)(*[int(x) for x in off])
-        self._chk(self.lib.pk_block_place(self.h, block, o), "pk_block_place")
+        self._chk(self.lib.pk_block_place_level(self.h, block, level, o), "pk_block_place_level")
 
     # -- differentiable path (one periodic block, one fluid, RK2) -------------
     @property

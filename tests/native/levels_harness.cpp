@@ -1,0 +1,74 @@
+// Host harness of the refined-domain planner (pk_levels.cpp) for the CPU
+// tests: builds a plan and hands its tables out through plain C calls.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../piernik_b200/csrc/pk_levels.h"
+
+static pk::LevelPlan g_plan;
+
+extern "C" {
+
+int lv_build(int nb, const int* level, const int* n, const int* g, const long long* off, const long long* dom,
+             char* err, int errlen)
+{
+    std::vector<pk::LBlock> b(nb);
+    for (int i = 0; i < nb; ++i) {
+        b[i].level = level[i];
+        for (int d = 0; d < 3; ++d) {
+            b[i].n[d] = n[3 * i + d];
+            b[i].g[d] = g[3 * i + d];
+            b[i].off[d] = off[3 * i + d];
+        }
+    }
+    std::string e;
+    if (!pk::build_levels(b, dom, g_plan, e)) {
+        if (err && errlen > 0) {
+            std::strncpy(err, e.c_str(), errlen - 1);
+            err[errlen - 1] = 0;
+        }
+        return -1;
+    }
+    return 0;
+}
+
+long long lv_nruns() { return (long long)g_plan.runs.size(); }
+
+void lv_run(long long i, int* out)
+{
+    const pk::PRun& r = g_plan.runs[i];
+    const int v[12] = {r.fb, r.cb, r.fx, r.fy, r.fz, r.len, r.cx, r.cy, r.cz, r.px, r.py, r.pz};
+    std::memcpy(out, v, sizeof(v));
+}
+
+long long lv_run_level_beg(int L) { return g_plan.run_level_beg[L]; }
+
+int lv_fc_nin(int d) { return (int)g_plan.fc[d].in_face.size(); }
+
+// face, then the 4 out slots summed into in slot s
+void lv_fc_in(int d, int s, int* out)
+{
+    out[0] = g_plan.fc[d].in_face[s];
+    for (int q = 0; q < 4; ++q) out[1 + q] = g_plan.fc[d].src[4 * s + q];
+}
+
+int lv_fc_in_level_beg(int d, int L) { return g_plan.fc[d].in_level_beg[L]; }
+
+// slot of block b's pencil pen on side (kind 0: in, 1: out); -2 when the block has no table
+int lv_fc_slot(int d, int b, int kind, int side, long long pen)
+{
+    const std::vector<int>& t = kind == 0 ? g_plan.fc[d].in_slot[b] : g_plan.fc[d].out_slot[b];
+    if (t.empty()) return -2;
+    return t[(size_t)side * (t.size() / 2) + pen];
+}
+
+long long lv_leaf_cells(int b) { return g_plan.leaf_cells[b]; }
+
+int lv_leaf(int b, long long c)
+{
+    if (g_plan.leaf[b].empty()) return 1;
+    return g_plan.leaf[b][c];
+}
+
+}  // extern "C"

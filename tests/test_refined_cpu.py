@@ -1,0 +1,174 @@
+"""Refined (multi-level) domains on the CPU.
+
+The oracle's multi-level driver (oracle/amr.py) is pinned by conservation:
+with the fine->coarse flux correction every conserved quantity summed over
+leaf cells (times the cell volume) is constant to round-off on a periodic
+domain.  The library's planner (pk_levels.cpp, through a host harness) must
+produce exactly the couplings the oracle derives independently from cell
+positions: the prolonged guard cells with their coarse sources and
+parities, the restricted coarse faces with their fine faces in summation
+order, and the leaf cells.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import setup_for
+import amr
+from piernik_b200 import problems
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "native", "levels_harness.cpp")
+PLAN = os.path.join(HERE, "..", "piernik_b200", "csrc", "pk_levels.cpp")
+HDR = os.path.join(HERE, "..", "piernik_b200", "csrc", "pk_levels.h")
+LIB = os.path.join(HERE, "native", "liblevels_harness.so")
+
+DOM3 = (16, 16, 16)
+REG3 = [((8, 8, 8), (24, 24, 24)), ((24, 24, 24), (40, 40, 40))]
+DOM2 = (16, 16, 1)
+REG2 = [((8, 6, 0), (24, 22, 1)), ((22, 18, 0), (38, 34, 1))]
+GO1, GO2 = (1, 0, 0), (2, 2, 1)
+RO1, RO2 = (1, 2, 0), (2, 0, 1)
+
+
+def case(phys, dom=DOM3, regions=REG3, lim="vanleer", seed=3):
+    layout = problems.refined_layout(dom, regions, sizes=(8, 16), seed=seed)
+    setup = setup_for(phys, n=tuple(8 if d > 1 else 1 for d in dom), lim=lim)
+    return problems.refined_blocks(dom, layout, setup, problems.wave_fields(dom, seed=5))
+
+
+@pytest.fixture(scope="module")
+def hlib():
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in (SRC, PLAN, HDR)):
+        subprocess.check_call(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", LIB, SRC, PLAN])
+    L = C.CDLL(LIB)
+    L.lv_nruns.restype = C.c_longlong
+    L.lv_run.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
+    L.lv_fc_slot.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_longlong]
+    L.lv_leaf_cells.restype = C.c_longlong
+    return L
+
+
+def build(hlib, blocks, dom):
+    nb = len(blocks)
+    lev = (C.c_int * nb)(*[b[1] for b in blocks])
+    n = (C.c_int * (3 * nb))(*[x for b in blocks for x in b[0].n])
+    g = (C.c_int * (3 * nb))(*[x for b in blocks for x in b[0].guards])
+    off = (C.c_longlong * (3 * nb))(*[x for b in blocks for x in b[2]])
+    dm = (C.c_longlong * 3)(*dom)
+    err = C.create_string_buffer(256)
+    if hlib.lv_build(nb, lev, n, g, off, dm, err, 256) != 0:
+        raise ValueError(err.value.decode())
+
+
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_refined_oracle_conserves(oracle_lib, phys, dim):
+    dom, reg = (DOM3, REG3) if dim == 3 else (DOM2, REG2)
+    a = amr.AmrOracle(dom, case(phys, dom, reg))
+    a.fill_guards()
+    t0 = amr.leaf_totals(a)
+    scale = amr.leaf_totals(a, absolute=True)
+    a.run(2)
+    t1 = amr.leaf_totals(a)
+    assert a.state.nstep == 2 and a.state.t > 0
+    assert np.all(np.abs(t1 - t0) <= 1e-12 * scale), (t1 - t0) / scale
+
+
+def test_refined_oracle_without_correction_does_not_conserve(oracle_lib):
+    """The check above has teeth: with the fine fluxes never passed to the
+    coarse blocks the leaf totals drift far beyond round-off."""
+    a = amr.AmrOracle(DOM3, case("hd"))
+    a.restr = [[[] for _ in lv] for lv in a.restr]
+    a.fill_guards()
+    t0 = amr.leaf_totals(a)
+    scale = amr.leaf_totals(a, absolute=True)
+    a.run(1)
+    assert np.max(np.abs(amr.leaf_totals(a) - t0) / scale) > 1e-8
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_planner_matches_oracle(hlib, oracle_lib, dim):
+    dom, reg = (DOM3, REG3) if dim == 3 else (DOM2, REG2)
+    blocks = case("mhd", dom, reg)
+    build(hlib, blocks, dom)
+    a = amr.AmrOracle(dom, blocks)
+    # prolonged guard cells: (fine block, x, y, z) -> (coarse block, cx, cy, cz, px, py, pz)
+    got = {}
+    r = (C.c_int * 12)()
+    for k in range(hlib.lv_nruns()):
+        hlib.lv_run(k, r)
+        fb, cb, fx, fy, fz, ln, cx, cy, cz, px, py, pz = list(r)
+        for i in range(ln):
+            got[(fb, fx + i, fy, fz)] = (cb, cx + ((px + i) >> 1), cy, cz, (px + i) & 1, py, pz)
+    want = {}
+    for L, i, dst, j, cs, par in a.prolong:
+        z, y, x = dst
+        for k in range(len(x)):
+            want[(i, int(x[k]), int(y[k]), int(z[k]))] = (j, int(cs[0][k]), int(cs[1][k]), int(cs[2][k]),
+                                                          int(par[0][k]), int(par[1][k]), int(par[2][k]))
+    assert got == want
+    # restricted faces: (coarse block, d, side, pencil position) -> (face, [fine (block, side, position)])
+    for d in range(3):
+        if dom[d] == 1:
+            continue
+        slots_in, slots_out = {}, {}
+        for b, blk in enumerate(blocks):
+            n = blk[0].n
+            for kind, tab in ((0, slots_in), (1, slots_out)):
+                for side in range(2):
+                    if hlib.lv_fc_slot(d, b, kind, side, 0) == -2:
+                        continue
+                    for i2 in range(n[GO2[d]]):
+                        for i1 in range(n[GO1[d]]):
+                            s = hlib.lv_fc_slot(d, b, kind, side, i1 + n[GO1[d]] * i2)
+                            if s >= 0:
+                                pos = [0, 0, 0]
+                                pos[GO1[d]], pos[GO2[d]] = i1, i2
+                                tab[s] = (b, side, tuple(pos))
+        got = {}
+        rec = (C.c_int * 5)()
+        beg = [hlib.lv_fc_in_level_beg(d, L) for L in range(a.maxl + 1)]
+        assert beg == sorted(beg) and beg[-1] == hlib.lv_fc_nin(d)
+        for s in range(hlib.lv_fc_nin(d)):
+            lc = max(L for L in range(a.maxl) if beg[L] <= s)
+            assert beg[lc] <= s < beg[lc + 1] and a.level[slots_in[s][0]] == lc, "in slots grouped by coarse level"
+            hlib.lv_fc_in(d, s, rec)
+            face, src = rec[0], [x for x in list(rec)[1:] if x >= 0]
+            got[slots_in[s]] = (face, [slots_out[x] for x in src])
+        want = {}
+        for Lc in range(a.maxl + 1):
+            for j, side, cpen, order in a.restr[d][Lc]:
+                nj = blocks[j][0].n
+
+                def coords(pen, nn):
+                    pos = [0, 0, 0]
+                    pos[RO1[d]], pos[RO2[d]] = pen % nn[RO1[d]], pen // nn[RO1[d]]
+                    return tuple(pos)
+                face = int(a._tabs[(j, d)]["in_face"][side][cpen])
+                want[(j, side, coords(cpen, nj))] = (face, [(i, s, coords(p, blocks[i][0].n)) for i, s, p in order])
+        assert got == want, d
+    # leaf cells
+    for b in range(len(blocks)):
+        n = blocks[b][0].n
+        cells = n[0] * n[1] * n[2] if a.leaf[b] is None else int(a.leaf[b].sum())
+        assert hlib.lv_leaf_cells(b) == cells
+
+
+def test_planner_rejects(hlib):
+    s = setup_for("hd", n=(8, 8, 8))
+    base = [(s.replace(n=(16, 16, 16)), 0, (0, 0, 0))]
+    odd = base + [(s.replace(n=(8, 8, 8)), 1, (9, 8, 8))]
+    with pytest.raises(ValueError, match="even"):
+        build(hlib, odd, (16, 16, 16))
+    edge = base + [(s.replace(n=(8, 8, 8)), 1, (0, 8, 8))]       # touches the level boundary: fine,
+    build(hlib, edge, (16, 16, 16))                              # level 0 covers the periodic domain
+    deep = edge + [(s.replace(n=(8, 8, 8)), 2, (0, 18, 18))]     # level 2 beyond its level 1 block
+    with pytest.raises(ValueError, match="nested"):
+        build(hlib, deep, (16, 16, 16))
+    hole = [(s.replace(n=(16, 16, 8)), 0, (0, 0, 0))]
+    with pytest.raises(ValueError, match="cover"):
+        build(hlib, hole, (16, 16, 16))
