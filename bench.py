@@ -61,7 +61,8 @@ def parse():
     p.add_argument("--adj-steps", type=int, default=8)
     p.add_argument("--tune-log", default=None)
     p.add_argument("--workload", default="mhd256",
-                   choices=["mhd256", "batched", "adjoint", "ot-gradient", "batched-adjoint"],
+                   choices=["mhd256", "batched", "batched-independent", "adjoint", "ot-gradient",
+                            "batched-adjoint"],
                    help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks; "
                         "adjoint: gradient of --steps steps of the MHD block at --n; ot-gradient: the "
                         "differentiable Orszag-Tang workload (512^2, K = 100) with its FD check; "
@@ -388,6 +389,81 @@ def our_arm(args):
 
 
 def batched_arm(args):
+    """The uneven-blocks workload on a three-level refinement
+    (problems.refined_blast, seed 4): 515 blocks with edges from
+    {16,24,32,48,64} (64 on the base level, 128^3 cells; a level-1 box of
+    208^3 and a level-2 box of 240^3 cells around an off-centre blast), ion MHD
+    + neutral + dust, vanleer, CFL 0.7.  Each RK stage sweeps every block of a
+    level in one launch, finest level first, with the fine->coarse flux
+    correction, then copies and prolongs the guard cells; a step's launches
+    are replayed from one CUDA graph.  A cell-update is one cell of any block
+    (covered ones included: the reference sweeps them too) advanced by one
+    dt.  Timed beside one block of the same physics and a similar cell count
+    through the single-block fused path."""
+    import torch
+    from piernik_b200 import build, problems
+    from piernik_b200.autotune import autotune
+    from piernik_b200.sim import Simulation
+    build.build()
+    torch.cuda.set_device(0)
+    dom, blocks = problems.refined_blast()
+    cells = sum(int(np.prod(s.n)) for s, *_ in blocks)
+    sim = Simulation(blocks[0][0])
+    for s, *_ in blocks[1:]:
+        sim.add_block(s)
+    sim.set_domain(dom, (True, True, True))
+    for i, (s, L, off, u, b, psi) in enumerate(blocks):
+        sim.place_block(i, off, L)
+        sim.upload(u, b, psi, block=i)
+    levels = [sum(1 for x in blocks if x[1] == L) for L in range(3)]
+    del blocks
+    sim.update_boundaries()
+    sim.use_graph(True)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.run(args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(0)
+    l0, _, _ = sim.profile_read()
+    e0.record(stream)
+    sim.run(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    l1, _, _ = sim.profile_read()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    refined = 2.0 * cells * args.steps / (ms / 1e3)
+    st = sim.time_state
+    sim.close()
+    # one block of the same physics and a similar number of cells
+    side = int(round(cells ** (1.0 / 3.0) / 8.0)) * 8
+    one = problems.batched_blocks(nblocks=1, seed=args.seed, sizes=(side,), levels=1)[0]
+    s1 = Simulation(one[0])
+    s1.upload(*one[1:])
+    autotune(s1, reps=1)
+    s1.run(args.warmup)
+    st1 = torch.cuda.ExternalStream(s1.stream)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(st1)
+    s1.run(args.steps)
+    e3.record(st1)
+    e3.synchronize()
+    single = 2.0 * side ** 3 * args.steps / (e2.elapsed_time(e3) / 1e3)
+    s1.close()
+    out = {"metric": "FP64 3-fluid MHD cell-updates/s, %d blocks on 3 refinement levels" % sum(levels),
+           "value": refined, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "refined blast: uneven blocks (edges 16..64) on 3 levels of a periodic 128^3 "
+                                  "base domain, ion MHD + neutral + dust, vanleer, CFL 0.7, fine->coarse flux "
+                                  "correction, guard prolongation, one launch per level per RK stage, CUDA graph "
+                                  "per step", "blocks_per_level": levels, "cells": cells},
+           "single_block": {"n": side, "value": single, "ratio_refined_to_single": refined / single},
+           "t_end": st.t, "gpu_launches": l1 - l0, "clocks": ck}
+    print(json.dumps(out), flush=True)
+
+
+def batched_independent_arm(args):
     """512 independent periodic blocks with edges from {16,24,32,48,64}, three
     fluids (ion MHD 5/3, neutral 7/5, dust), one persistent launch per sweep,
     each step's sweeps replayed from a CUDA graph; timed beside one block of
@@ -713,6 +789,9 @@ def main():
         return
     if args.workload == "batched":
         batched_arm(args)
+        return
+    if args.workload == "batched-independent":
+        batched_independent_arm(args)
         return
     if args.workload == "adjoint":
         adjoint_arm(args)

@@ -193,6 +193,8 @@ void free_levels(pk_ctx* h)
         h->d_out_flux[d] = nullptr;
         h->d_src[d] = nullptr;
         h->in_level_beg[d].clear();
+        cudaFree(h->d_fcargs[d]);
+        h->d_fcargs[d] = nullptr;
     }
     for (auto& b : h->blocks) {
         for (int d = 0; d < 3; ++d) b.fc[d] = FcArgs{};
@@ -282,6 +284,7 @@ int levels_prepare(pk_ctx* h)
         if (nin) PK_CUDA(h, cudaMalloc(&h->d_in_flux[d], sizeof(double) * NV * nin));
         if (F.n_out) PK_CUDA(h, cudaMalloc(&h->d_out_flux[d], sizeof(double) * NV * F.n_out));
         h->d_src[d] = nin ? h->d_fc_int[d] + src_off : nullptr;
+        std::vector<FcArgs> tab(nl);
         for (int i = 0; i < nl; ++i) {
             FcArgs& f = h->blocks[i].fc[d];
             f.in_slot = in_off[i] >= 0 ? h->d_fc_int[d] + in_off[i] : nullptr;
@@ -289,7 +292,10 @@ int levels_prepare(pk_ctx* h)
             f.in_flux = h->d_in_flux[d];
             f.out_slot = out_off[i] >= 0 ? h->d_fc_int[d] + out_off[i] : nullptr;
             f.out_flux = h->d_out_flux[d];
+            tab[i] = f;
         }
+        if (nin || F.n_out)
+            if (int rc = upload_vec(h, tab, &h->d_fcargs[d])) return rc;
     }
     for (int i = 0; i < nl; ++i) {
         Block& b = h->blocks[i];
@@ -505,6 +511,9 @@ int build_batch(pk_ctx* h)
     if (int rc = ensure_pingpong(h)) return rc;
     if (!h->batch_dirty) return PK_OK;
     const int nb = (int)h->blocks.size();
+    if (!fused_ok(h))                                  // the stage path keeps cg%w(uh) per block
+        for (auto& b : h->blocks)
+            if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
     std::vector<BlockDesc> desc(nb);
     for (int p = 0; p < 2; ++p) {
         for (int i = 0; i < nb; ++i) {
@@ -521,6 +530,7 @@ int build_batch(pk_ctx* h)
             }
             d.wrap = h->connected ? 0 : 1;
             d.leaf = b.leaf;
+            d.uh = b.uh;
         }
         cudaFree(h->d_desc[p]);
         h->d_desc[p] = nullptr;
@@ -553,6 +563,43 @@ int build_batch(pk_ctx* h)
         if (bl.n) {
             PK_CUDA(h, cudaMalloc(&bl.dev, sizeof(WorkItem) * bl.n));
             PK_CUDA(h, cudaMemcpyAsync(bl.dev, bl.host.data(), sizeof(WorkItem) * bl.n, cudaMemcpyHostToDevice, h->stream));
+        }
+    }
+    // the batched stage: per direction and level, items of whole pencils
+    int maxl = 0;
+    bool fits = true;
+    for (auto& b : h->blocks) {
+        maxl = std::max(maxl, b.level);
+        for (int d = 0; d < 3; ++d) fits = fits && (b.n[d] <= 1 || b.ext[d] <= STAGE_MAXT);
+    }
+    h->stage_batched = fits && nb > 1;
+    std::vector<std::vector<StageItem>> items;
+    for (int dir = 0; dir < 3; ++dir) {
+        for (StageList& s : h->sbatch[dir]) cudaFree(s.dev);
+        h->sbatch[dir].assign(maxl + 1, StageList());
+        if (!h->stage_batched) continue;
+        items.assign(maxl + 1, {});
+        const int o1 = ORTHO1[dir], o2 = ORTHO2[dir];
+        for (int i = 0; i < nb; ++i) {
+            const Block& b = h->blocks[i];
+            if (b.n[dir] <= 1) continue;
+            const int T = b.ext[dir];
+            int P = STAGE_MAXT / T;
+            if (P >= 4) P -= P % 4;
+            if (P > b.n[o1]) P = b.n[o1];
+            StageList& sl = h->sbatch[dir][b.level];
+            sl.smem = std::max(sl.smem, (size_t)3 * h->nplanes * P * T * sizeof(double));
+            for (int i2 = 0; i2 < b.n[o2]; ++i2)
+                for (int i1 = 0; i1 < b.n[o1]; i1 += P) items[b.level].push_back(StageItem{i, i1, i2, P});
+        }
+        for (int L = 0; L <= maxl; ++L) {
+            StageList& sl = h->sbatch[dir][L];
+            sl.n = (int)items[L].size();
+            if (!sl.n) continue;
+            PK_CUDA(h, cudaMalloc(&sl.dev, sizeof(StageItem) * sl.n));
+            PK_CUDA(h, cudaMemcpyAsync(sl.dev, items[L].data(), sizeof(StageItem) * sl.n, cudaMemcpyHostToDevice,
+                                       h->stream));
+            PK_CUDA(h, cudaStreamSynchronize(h->stream));
         }
     }
     PK_CUDA(h, cudaStreamSynchronize(h->stream));   // host vectors of the tables may change after return
@@ -593,6 +640,30 @@ int put_step_array(pk_ctx* h, const StepRec* r)
     return PK_OK;
 }
 
+// glmdamping with the step's factor read from d_step (graph-safe)
+int glm_scale_dev(pk_ctx* h)
+{
+    if (h->blocks.size() > 1) {
+        if (int rc = build_batch(h)) return rc;
+        long long mp = 0;
+        for (auto& b : h->blocks) mp = std::max(mp, b.plane);
+        long long gx = (mp + 255) / 256;
+        if (gx > 64) gx = 64;
+        k_scale_blocks<<<dim3((unsigned)gx, (unsigned)h->blocks.size()), 256, 0, h->stream>>>(h->d_desc[h->cur], h->ib + 3,
+                                                                                         h->d_step);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+        return PK_OK;
+    }
+    for (auto& b : h->blocks) {
+        k_scale_dev<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(state(h, b) + (long long)(h->ib + 3) * b.plane, b.plane,
+                                                                 h->d_step);
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
+    }
+    return PK_OK;
+}
+
 int glm_scale(pk_ctx* h, double fac)
 {
     for (auto& b : h->blocks) {
@@ -626,17 +697,22 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
     }
     const int nst = h->cfg.integration_order == 1 ? 1 : 2;
     if (int rc = exchange_prepare(h)) return rc;       // a refined domain's couplings
+    if (h->blocks.size() > 1)
+        if (int rc = build_batch(h)) return rc;
     for (int s = 1; s <= nst; ++s) {
         const double rk = (h->cfg.integration_order == 1) ? 1.0 : (s == 1 ? 0.5 : 1.0);
         // finest level first: its boundary fluxes replace the coarser level's (sweeps.F90:218-262)
         for (int L = h->max_level; L >= 0; --L) {
-            for (auto& b : h->blocks) {
-                if (b.n[dir] <= 1 || b.level != L) continue;
-                if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
-                if (b.ext[dir] > STAGE_MAXT)
-                    if (int rc = ensure_pingpong(h)) return rc;
-                const double dtodx = (rk * dt) / b.dl[dir];
-                if (int rc = ops->stage(h, b, dir, s == 1, dtodx, ch)) return rc;
+            if (h->stage_batched) {
+                if (int rc = ops->stage_batched(h, dir, L, s == 1, rk)) return rc;
+            } else {
+                for (auto& b : h->blocks) {
+                    if (b.n[dir] <= 1 || b.level != L) continue;
+                    if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+                    if (b.ext[dir] > STAGE_MAXT)
+                        if (int rc = ensure_pingpong(h)) return rc;
+                    if (int rc = ops->stage(h, b, dir, s == 1, rk)) return rc;
+                }
             }
             if (L > 0 && h->d_src[dir]) {
                 const int beg = h->in_level_beg[dir][L - 1], end = h->in_level_beg[dir][L];
@@ -650,11 +726,12 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
                 }
             }
         }
-        for (auto& b : h->blocks)
-            if (int rc = fill_guards_block(h, b)) return rc;
+        if (h->max_level == 0)                        // refined domains overwrite every guard cell below
+            for (auto& b : h->blocks)
+                if (int rc = fill_guards_block(h, b)) return rc;
         if (int rc = exchange_guards(h, dir)) return rc;
     }
-    if (h->cfg.magnetic && apply_fac) return glm_scale(h, fac);
+    if (h->cfg.magnetic && apply_fac) return glm_scale_dev(h);
     return PK_OK;
 }
 
@@ -840,7 +917,10 @@ int pk_destroy(pk_handle h)
     }
     for (auto& p : h->ev_used) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
     for (auto& p : h->ev_free) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
-    for (int d = 0; d < 3; ++d) cudaFree(h->batch[d].dev);
+    for (int d = 0; d < 3; ++d) {
+        cudaFree(h->batch[d].dev);
+        for (StageList& s : h->sbatch[d]) cudaFree(s.dev);
+    }
     for (double* p : h->grad_ckpt) cudaFree(p);
     for (double* p : h->grad_pool) cudaFree(p);
     for (double* p : h->grad_star) cudaFree(p);
@@ -1016,8 +1096,8 @@ int pk_solve_cg(pk_handle h, int32_t id, int32_t ddim, int32_t istep, double dt,
     if (!b->uh) PK_CUDA(h, cudaMalloc(&b->uh, sizeof(double) * h->nplanes * b->plane));
     if (b->ext[dir] > STAGE_MAXT)
         if (int rc = ensure_pingpong(h)) return rc;
-    const double dtodx = (rk * dt) / b->dl[dir];   // rk_coef(istep) * dt / cg%dl(ddim)
-    return ops_of(h)->stage(h, *b, dir, first, dtodx, chspeed);
+    if (int rc = put_step_params(h, dt, chspeed, 1.0)) return rc;   // rk_coef(istep) * dt / cg%dl(ddim) on the device
+    return ops_of(h)->stage(h, *b, dir, first, rk);
 }
 
 int pk_fill_guards(pk_handle h)
@@ -1333,9 +1413,9 @@ static int clamp_dt(const pk_config& c, pk_time_state& ts, double dt, double c_a
 static int run_step_sweeps(pk_ctx* h, double dt, double ch, double fac)
 {
     if (h->use_graph && !h->profiling && !h->halo_cb) {
-        if (fused_ok(h) && h->blocks.size() > 1)
-            if (int rc = build_batch(h)) return rc;   // tables are built outside the capture
         if (int rc = exchange_prepare(h)) return rc;
+        if (h->blocks.size() > 1)
+            if (int rc = build_batch(h)) return rc;   // tables are built outside the capture
         if (int rc = ensure_pingpong(h)) return rc;
         for (auto& b : h->blocks)
             if (!b.uh && !fused_ok(h)) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));

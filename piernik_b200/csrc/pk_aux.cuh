@@ -149,6 +149,25 @@ static __global__ void k_scale(double* __restrict__ p, long long n, double fac)
         p[i] = p[i] * fac;
 }
 
+// the same for the step's factor in device memory (sp->psi_fac), over the
+// psi plane (plane index ipsi) of every block of a table: blockIdx.y picks the block
+static __global__ void k_scale_blocks(const BlockDesc* __restrict__ blocks, int ipsi,
+                                      const StepParams* __restrict__ sp)
+{
+    const BlockDesc b = blocks[blockIdx.y];
+    double* p = const_cast<double*>(b.in) + (long long)ipsi * b.plane;
+    const double fac = sp->psi_fac;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < b.plane; i += (long long)gridDim.x * blockDim.x)
+        p[i] = p[i] * fac;
+}
+
+static __global__ void k_scale_dev(double* __restrict__ p, long long n, const StepParams* __restrict__ sp)
+{
+    const double fac = sp->psi_fac;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = p[i] * fac;
+}
+
 struct GuardArgs {
     int bnd[3][2];      // 0 per, 1 out, 2 ref
     int nplanes;

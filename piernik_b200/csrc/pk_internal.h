@@ -77,6 +77,13 @@ struct BatchList {
     int n = 0;
 };
 
+// work list of the batched stage for one direction and level
+struct StageList {
+    StageItem* dev = nullptr;
+    int n = 0;
+    size_t smem = 0;
+};
+
 }  // namespace pk
 
 struct pk_ctx {
@@ -100,6 +107,9 @@ struct pk_ctx {
     pk::BlockDesc* d_desc[2] = {nullptr, nullptr};   // block tables for cur = 0 / 1
     bool batch_dirty = true;
     pk::BatchList batch[3];
+    std::vector<pk::StageList> sbatch[3];       // batched stage per direction, per level
+    bool stage_batched = false;                 // every block's pencils fit one stage CTA
+    pk::FcArgs* d_fcargs[3] = {nullptr, nullptr, nullptr};   // per block flux couplings (refined domains)
     pk_time_state ts;
     std::string err;
     int tileP[3] = {0, 0, 0}, tileL[3] = {0, 0, 0}, tileV[3] = {-1, -1, -1};
@@ -166,7 +176,8 @@ struct PhysOps {
     int nv;
     int (*prepare)(pk_ctx* h);      // kernel attributes; called before any launch or graph capture
     int (*fused)(pk_ctx* h, Block& b, int dir, int apply_fac);
-    int (*stage)(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch);
+    int (*stage)(pk_ctx* h, Block& b, int dir, int first, double rk);           // dt, ch from d_step
+    int (*stage_batched)(pk_ctx* h, int dir, int level, int first, double rk);  // all blocks of a level
     int (*batched)(pk_ctx* h, int dir, int apply_fac, unsigned* counter);
     int (*fused_ptr)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out);
     int (*fused_rec)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out, double* ustar,

@@ -311,6 +311,7 @@ struct BlockDesc {
     double dl[3];
     int wrap;               // Tile::wrap for this block's tiles
     const unsigned char* leaf = nullptr;   // interior leaf mask for the CFL reduction (null: every cell)
+    double* uh = nullptr;   // stage path: the state at the start of the stage pair (cg%w(uh))
 };
 
 struct WorkItem {
@@ -368,17 +369,6 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
     flush_status(status, gstatus);
 }
 
-// -------------------------------------------------------------------------
-// One RK stage of solve_cg on a block with guard cells.
-// grid: x = ortho-1 tiles, y = chunks of L cells of the full pencil, z = ortho-2.
-// The tile spans [c0-halo, c0-halo+T) of the pencil: the whole pencil
-// (halo 0, T = L = ext) or a chunk with a 2-cell halo; pencil ends (storage index 0
-// and ext-1) follow the reference's one-sided limiter rules and get floors
-// without an update, exactly like cells 1 and n of solve().
-// first != 0: u0 = u and the owned cells are copied to uh (pu0 = pu).
-// uin and uout may alias only when one chunk covers the whole pencil (every
-// load of a pencil then precedes every store of it, within one CTA).
-// -------------------------------------------------------------------------
 // The fine/coarse flux couplings of one block along one sweep direction.
 // Pencils are numbered i1 + n1 * i2; slots index the per-direction arrays
 // shared by all blocks.
@@ -390,12 +380,24 @@ struct FcArgs {
     double* out_flux;        // per out slot: NV fluxes
 };
 
-template <class PH, int MAXT, bool W3 = false, bool FC = false>
-__global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* uin, double* uout,
-                                               double* uh, PhysParams pp, int first, double dtodx, double ch,
-                                               unsigned* __restrict__ gstatus, FcArgs fc = FcArgs{})
+// -------------------------------------------------------------------------
+// One RK stage of solve_cg on a tile of a block with guard cells: P pencils
+// from ortho-1 index i1_0 at ortho-2 index i2.  The tile spans
+// [c0-halo, c0-halo+T) of the pencil: the whole pencil (halo 0, T = L = ext)
+// or a chunk with a 2-cell halo; pencil ends (storage index 0 and ext-1)
+// follow the reference's one-sided limiter rules and get floors without an
+// update, exactly like cells 1 and n of solve().
+// first != 0: u0 = u and the owned cells are copied to uh (pu0 = pu).
+// uin and uout may alias only when one chunk covers the whole pencil (every
+// load of a pencil then precedes every store of it, within one CTA).
+// dtodx = rk_coef * dt / dl and ch come from the step scalars in device
+// memory, so that a captured CUDA graph serves every step.
+// -------------------------------------------------------------------------
+template <class PH, bool W3, bool FC>
+PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
+                       double* uh, const PhysParams& pp, int first, double dtodx, double ch, const FcArgs& fc,
+                       double* smem, unsigned& status)
 {
-    extern __shared__ double smem[];
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
     const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
@@ -405,9 +407,7 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     else { p = tid % P; t = tid / P; }
     const int sp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
     const int me = p * sp + t * st;
-    const int i1 = blockIdx.x * P + p;
-    const int c0 = blockIdx.y * tl.L;
-    const int i2 = blockIdx.z;
+    const int i1 = i1_0 + p;
     const int n = g.ext_d;
     const int s = c0 - tl.halo + t;                            // storage index along the pencil
     const bool valid = (tid < PT) && (i1 < g.n1) && s >= 0 && s < n;
@@ -418,7 +418,6 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     for (int v = 0; v < NV; ++v) w[v] = 0.0;
     if (valid) load_cell<PH>(uin, off, g, w);
     if (first && own) store_cell<PH>(uh, off, g, w);           // pu0 = pu (solve_cg_riemann.F90:176)
-    unsigned status = 0;
     Roles r;
     r.q = valid;
     r.end = (s == 0) ? -1 : ((s == n - 1) ? 1 : 0);
@@ -453,6 +452,69 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     rk_stage<PH, false, W3, FC>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status,
                                 nullptr, fc_in, fc_out);
     if (own) store_cell<PH>(uout, off, g, w);
+}
+
+// One stage of one block.  grid: x = ortho-1 tiles, y = chunks of L cells of
+// the full pencil, z = ortho-2.
+template <class PH, int MAXT, bool W3 = false, bool FC = false>
+__global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* uin, double* uout, double* uh,
+                                               PhysParams pp, int first, double rk, double dl,
+                                               const StepParams* __restrict__ spar, unsigned* __restrict__ gstatus,
+                                               FcArgs fc = FcArgs{})
+{
+    extern __shared__ double smem[];
+    unsigned status = 0;
+    const double dtodx = (rk * spar->dt) / dl;                 // rk_coef(istep) * dt / cg%dl(ddim)
+    stage_tile<PH, W3, FC>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, uh, pp, first, dtodx,
+                           spar->ch, fc, smem, status);
+    flush_status(status, gstatus);
+}
+
+// One stage of many blocks in one launch: one CTA per work item of P whole
+// pencils (in place, T = ext along the sweep).  blocks[b].in is the state,
+// blocks[b].uh its stage-1 copy; fcs (or null) the blocks' flux couplings
+// along dir.
+struct StageItem {
+    int block, i1_0, i2, P;
+};
+
+template <class PH, int MAXT, bool W3 = false, bool FC = false>
+__global__ void __launch_bounds__(MAXT) k_stage_batched(const BlockDesc* __restrict__ blocks,
+                                                       const StageItem* __restrict__ items, int dir, PhysParams pp,
+                                                       int first, double rk, const StepParams* __restrict__ spar,
+                                                       const FcArgs* __restrict__ fcs, unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    unsigned status = 0;
+    const StageItem w = items[blockIdx.x];
+    const BlockDesc b = blocks[w.block];
+    const int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;
+    Geom g;
+    const long long st3[3] = {1, b.ext[0], (long long)b.ext[0] * b.ext[1]};
+    g.plane = b.plane;
+    g.sd = st3[dir];
+    g.s1 = st3[o1];
+    g.s2 = st3[o2];
+    g.ext_d = b.ext[dir];
+    g.n_d = b.n[dir];
+    g.g_d = b.g[dir];
+    g.n1 = b.n[o1];
+    g.g1 = b.g[o1];
+    g.n2 = b.n[o2];
+    g.g2 = b.g[o2];
+    g.perm[0] = dir;                              // iarr_swp: (x,y,z) (y,x,z) (z,y,x)
+    g.perm[1] = dir == 1 ? 0 : 1;
+    g.perm[2] = dir == 2 ? 0 : 2;
+    Tile tl;
+    tl.P = w.P;
+    tl.T = b.ext[dir];
+    tl.L = b.ext[dir];
+    tl.halo = 0;
+    tl.xfast = dir == 0;
+    const double dtodx = (rk * spar->dt) / b.dl[dir];
+    const FcArgs fc = fcs ? fcs[w.block] : FcArgs{};
+    double* u = const_cast<double*>(b.in);
+    stage_tile<PH, W3, FC>(g, tl, w.i1_0, 0, w.i2, u, u, b.uh, pp, first, dtodx, spar->ch, fc, smem, status);
     flush_status(status, gstatus);
 }
 

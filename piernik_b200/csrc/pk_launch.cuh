@@ -60,6 +60,14 @@ int set_smem_attr(pk_ctx* h)
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, false, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, false, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, true, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, true, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -304,7 +312,7 @@ int launch_batched(pk_ctx* h, int dir, int apply_fac, unsigned* counter)
 }
 
 template <class PH>
-int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double ch)
+int launch_stage(pk_ctx* h, Block& b, int dir, int first, double rk)
 {
     if (int rc = set_smem_attr<PH>(h)) return rc;
     Geom g = make_geom(b, dir);
@@ -336,7 +344,8 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double c
     const bool hooks = fc.in_slot || fc.out_slot;      // a fine/coarse boundary crosses this block's pencils
     auto* kern = h->pp.weno3 ? (hooks ? k_stage<PH, STAGE_MAXT, true, true> : k_stage<PH, STAGE_MAXT, true, false>)
                              : (hooks ? k_stage<PH, STAGE_MAXT, false, true> : k_stage<PH, STAGE_MAXT, false, false>);
-    kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, dtodx, ch, h->d_status, fc);
+    kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, u, uout, b.uh, h->pp, first, rk, b.dl[dir], h->d_step,
+                                                 h->d_status, fc);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
@@ -357,11 +366,33 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double dtodx, double c
     return PK_OK;
 }
 
+// one stage of every block of a level in one launch (k_stage_batched); the
+// work list and the block table were built by build_batch
+template <class PH>
+int launch_stage_batched(pk_ctx* h, int dir, int level, int first, double rk)
+{
+    if (level >= (int)h->sbatch[dir].size()) return PK_OK;
+    const StageList& sl = h->sbatch[dir][level];
+    if (!sl.n) return PK_OK;
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    const bool hooks = h->d_fcargs[dir] != nullptr;
+    auto* kern = h->pp.weno3 ? (hooks ? k_stage_batched<PH, STAGE_MAXT, true, true> : k_stage_batched<PH, STAGE_MAXT, true, false>)
+                             : (hooks ? k_stage_batched<PH, STAGE_MAXT, false, true> : k_stage_batched<PH, STAGE_MAXT, false, false>);
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+    kern<<<sl.n, STAGE_MAXT, sl.smem, h->stream>>>(h->d_desc[h->cur], sl.dev, dir, h->pp, first, rk, h->d_step,
+                                                  h->d_fcargs[dir], h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+    h->launches += 1;
+    return PK_OK;
+}
+
 template <class PH>
 const PhysOps* make_ops()
 {
-    static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_batched<PH>,
-                     launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>};
+    static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_stage_batched<PH>,
+                     launch_batched<PH>, launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>};
     return &o;
 }
 

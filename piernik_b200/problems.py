@@ -447,3 +447,24 @@ def wave_fields(dom, seed: int = 1, amp: float = 0.2):
         rng.bit_generator.state = state
         return u, b, psi
     return f
+
+
+def refined_blast(seed: int = 4, base: int = 128, centre=(70, 58, 66), r1: int = 104, r2: int = 120,
+                  sizes=(16, 24, 32, 48, 64), radius: float = 4.0, dl0: float = 2.0 ** -6,
+                  fluids=(("ion", 5.0 / 3.0), ("neu", 7.0 / 5.0), ("dst", -1.0)), magnetic: bool = True):
+    """The uneven-blocks workload on a real three-level refinement: a
+    periodic base^3 domain cut into blocks with edges from ``sizes`` (seeded),
+    a level-1 box of (2 r1)^3 level-1 cells and a level-2 box of (2 r2)^3
+    level-2 cells centred on the blast at ``centre`` (base cells), each cut the
+    same way; ion MHD + neutral + dust at rest, thermal energy density 10
+    inside ``radius`` base cells of the centre, uniform B = (0.1, 0.05, 0).
+    Returns (dom, blocks) for refined_blocks' block list."""
+    dom = (base, base, base)
+    c1 = [2 * c for c in centre]
+    c2 = [4 * c for c in centre]
+    regions = [(tuple(c - r1 for c in c1), tuple(c + r1 for c in c1)),
+               (tuple(c - r2 for c in c2), tuple(c + r2 for c in c2))]
+    layout = refined_layout(dom, regions, sizes=sizes, seed=seed)
+    setup = Setup(n=(16, 16, 16), fluids=list(fluids), magnetic=magnetic, limiter="vanleer", limiter_b="vanleer",
+                  cfl=0.7, cfl_glm=0.7, smalld=1.0e-4)
+    return dom, refined_blocks(dom, layout, setup, blast_fields(centre, radius), dl0=dl0)

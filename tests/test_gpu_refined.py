@@ -27,7 +27,7 @@ def case(phys, dom, regions, lim="vanleer", fluids=None, fields=None, **kw):
     return problems.refined_blocks(dom, layout, setup, fields or problems.wave_fields(dom, seed=5))
 
 
-def library(dom, blocks):
+def library(dom, blocks, graph=False):
     sim = Simulation(blocks[0][0])
     for s, *_ in blocks[1:]:
         sim.add_block(s)
@@ -36,6 +36,8 @@ def library(dom, blocks):
         sim.place_block(i, off, L)
         sim.upload(u, b, psi, block=i)
     sim.update_boundaries()
+    if graph:
+        sim.use_graph(True)
     return sim
 
 
@@ -70,13 +72,14 @@ def test_refined_single_sweeps(gpu_lib, phys):
     sim.close()
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", sorted(CASES) + ["mhd-3d-moncen+graph"])
 def test_refined_matches_oracle(gpu_lib, name):
-    c = CASES[name]
+    graph = name.endswith("+graph")
+    c = CASES[name.split("+")[0]]
     blocks = case(**c)
     a = amr.AmrOracle(c["dom"], blocks)
     a.fill_guards()
-    sim = library(c["dom"], blocks)
+    sim = library(c["dom"], blocks, graph=graph)
     compare(sim, a, "after the first boundary update")
     a.run(3)
     sim.run(3)
