@@ -570,7 +570,7 @@ int build_batch(pk_ctx* h)
     bool fits = true;
     for (auto& b : h->blocks) {
         maxl = std::max(maxl, b.level);
-        for (int d = 0; d < 3; ++d) fits = fits && (b.n[d] <= 1 || b.ext[d] <= STAGE_MAXT);
+        for (int d = 0; d < 3; ++d) fits = fits && (b.n[d] <= 1 || (b.n[d] + 4 <= STAGE_MAXT && b.g[d] >= 3));
     }
     h->stage_batched = fits && nb > 1;
     std::vector<std::vector<StageItem>> items;
@@ -583,9 +583,8 @@ int build_batch(pk_ctx* h)
         for (int i = 0; i < nb; ++i) {
             const Block& b = h->blocks[i];
             if (b.n[dir] <= 1) continue;
-            const int T = b.ext[dir];
+            const int T = b.n[dir] + 4;                 // the trimmed tile of k_stage_batched
             int P = STAGE_MAXT / T;
-            if (P >= 4) P -= P % 4;
             if (P > b.n[o1]) P = b.n[o1];
             StageList& sl = h->sbatch[dir][b.level];
             sl.smem = std::max(sl.smem, (size_t)3 * h->nplanes * P * T * sizeof(double));

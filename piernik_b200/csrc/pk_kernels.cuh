@@ -392,11 +392,15 @@ struct FcArgs {
 // load of a pencil then precedes every store of it, within one CTA).
 // dtodx = rk_coef * dt / dl and ch come from the step scalars in device
 // memory, so that a captured CUDA graph serves every step.
+// trim: the caller overwrites every guard cell after the stage (the sweeps'
+// boundary update), so only the interior cells are updated and stored: the
+// tile is then [g-2, g+n+2) of the pencil (c0 = g-2, T = L = n+4), which holds
+// every cell the interior updates read.
 // -------------------------------------------------------------------------
 template <class PH, bool W3, bool FC>
 PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
                        double* uh, const PhysParams& pp, int first, double dtodx, double ch, const FcArgs& fc,
-                       double* smem, unsigned& status)
+                       double* smem, unsigned& status, bool trim = false)
 {
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
@@ -417,7 +421,8 @@ PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
 #pragma unroll
     for (int v = 0; v < NV; ++v) w[v] = 0.0;
     if (valid) load_cell<PH>(uin, off, g, w);
-    if (first && own) store_cell<PH>(uh, off, g, w);           // pu0 = pu (solve_cg_riemann.F90:176)
+    const bool inner = s >= g.g_d && s < g.g_d + g.n_d;
+    if (first && own && (!trim || inner)) store_cell<PH>(uh, off, g, w);   // pu0 = pu (solve_cg_riemann.F90:176)
     Roles r;
     r.q = valid;
     r.end = (s == 0) ? -1 : ((s == n - 1) ? 1 : 0);
@@ -451,7 +456,7 @@ PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     }
     rk_stage<PH, false, W3, FC>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status,
                                 nullptr, fc_in, fc_out);
-    if (own) store_cell<PH>(uout, off, g, w);
+    if (own && (!trim || inner)) store_cell<PH>(uout, off, g, w);
 }
 
 // One stage of one block.  grid: x = ortho-1 tiles, y = chunks of L cells of
@@ -470,10 +475,10 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
     flush_status(status, gstatus);
 }
 
-// One stage of many blocks in one launch: one CTA per work item of P whole
-// pencils (in place, T = ext along the sweep).  blocks[b].in is the state,
-// blocks[b].uh its stage-1 copy; fcs (or null) the blocks' flux couplings
-// along dir.
+// One stage of many blocks in one launch: one CTA per work item of P
+// pencils (in place, the trimmed tile: every guard cell is refreshed after
+// the stage).  blocks[b].in is the state, blocks[b].uh its stage-1 copy; fcs
+// (or null) the blocks' flux couplings along dir.
 struct StageItem {
     int block, i1_0, i2, P;
 };
@@ -507,14 +512,15 @@ __global__ void __launch_bounds__(MAXT) k_stage_batched(const BlockDesc* __restr
     g.perm[2] = dir == 2 ? 0 : 2;
     Tile tl;
     tl.P = w.P;
-    tl.T = b.ext[dir];
-    tl.L = b.ext[dir];
+    tl.T = b.n[dir] + 4;                          // [g-2, g+n+2): the interior updates' stencil
+    tl.L = tl.T;
     tl.halo = 0;
     tl.xfast = dir == 0;
     const double dtodx = (rk * spar->dt) / b.dl[dir];
     const FcArgs fc = fcs ? fcs[w.block] : FcArgs{};
     double* u = const_cast<double*>(b.in);
-    stage_tile<PH, W3, FC>(g, tl, w.i1_0, 0, w.i2, u, u, b.uh, pp, first, dtodx, spar->ch, fc, smem, status);
+    stage_tile<PH, W3, FC>(g, tl, w.i1_0, b.g[dir] - 2, w.i2, u, u, b.uh, pp, first, dtodx, spar->ch, fc, smem, status,
+                           true);
     flush_status(status, gstatus);
 }
 
