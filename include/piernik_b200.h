@@ -183,6 +183,12 @@ int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant);
  * device memory, so one capture serves every step. */
 int pk_use_graph(pk_handle h, int32_t enable);
 
+/* Launch-bound variant of the batched stage kernel that sweeps many blocks
+ * stage by stage (refined or non-periodic connected domains): 0 = 320
+ * threads x 1 CTA per SM (default), 1 = 128 x 3, 2 = 192 x 2.  Used by the
+ * tuning of the refined workload; WENO3 always runs variant 0. */
+int pk_set_stage_variant(pk_handle h, int32_t variant);
+
 /* ---- Independent instances in one launch ----
  * count independent, fully periodic problems of n[0] x n[1] x (n[2]/count)
  * cells stacked along z in the handle's single block (instance i owns the

@@ -442,8 +442,9 @@ int exchange_guards(pk_ctx* h, int dir = -1)
     if (!h->connected) return PK_OK;
     if (int rc = exchange_prepare(h)) return rc;
     if (h->xlocal.total > 0) {
-        k_exchange<<<grid1d(h->xlocal.total, 256), 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total,
-                                                                       h->d_xptr[h->cur], h->nplanes);
+        const int nblk = h->xlocal.n < 148 * 16 ? h->xlocal.n : 148 * 16;   // CTAs take whole segments
+        k_exchange<<<nblk, 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total, h->d_xptr[h->cur],
+                                                h->nplanes);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
@@ -565,12 +566,13 @@ int build_batch(pk_ctx* h)
             PK_CUDA(h, cudaMemcpyAsync(bl.dev, bl.host.data(), sizeof(WorkItem) * bl.n, cudaMemcpyHostToDevice, h->stream));
         }
     }
-    // the batched stage: per direction and level, items of whole pencils
+    // the batched stage: per direction and level, items of P pencils
+    const int sv = h->pp.weno3 ? 0 : h->stage_variant;
     int maxl = 0;
     bool fits = true;
     for (auto& b : h->blocks) {
         maxl = std::max(maxl, b.level);
-        for (int d = 0; d < 3; ++d) fits = fits && (b.n[d] <= 1 || (b.n[d] + 4 <= STAGE_MAXT && b.g[d] >= 3));
+        for (int d = 0; d < 3; ++d) fits = fits && (b.n[d] <= 1 || (b.n[d] + 4 <= SV_T[sv] && b.g[d] >= 3));
     }
     h->stage_batched = fits && nb > 1;
     std::vector<std::vector<StageItem>> items;
@@ -584,7 +586,7 @@ int build_batch(pk_ctx* h)
             const Block& b = h->blocks[i];
             if (b.n[dir] <= 1) continue;
             const int T = b.n[dir] + 4;                 // the trimmed tile of k_stage_batched
-            int P = STAGE_MAXT / T;
+            int P = SV_T[sv] / T;
             if (P > b.n[o1]) P = b.n[o1];
             StageList& sl = h->sbatch[dir][b.level];
             sl.smem = std::max(sl.smem, (size_t)3 * h->nplanes * P * T * sizeof(double));
@@ -2047,6 +2049,16 @@ int pk_grad_backward(pk_handle h)
         }
     }
     PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_set_stage_variant(pk_handle h, int32_t variant)
+{
+    if (!h) return PK_E_ARG;
+    if (variant < 0 || variant >= NSTAGE_VARIANT) return fail(h, PK_E_ARG, "stage variant out of range");
+    h->stage_variant = variant;
+    h->batch_dirty = true;
+    invalidate_graph(h);
     return PK_OK;
 }
 

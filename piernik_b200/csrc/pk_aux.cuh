@@ -240,27 +240,43 @@ struct XPtr {
     int ext[3];
 };
 
+// nplanes values from src (plane stride ss) to dst (stride ds), eight loads
+// in flight before their stores (the two may alias as far as the compiler
+// knows, which would otherwise serialise every load behind the last store)
+PK_DEV void copy_planes(double* dst, long long ds, const double* src, long long ss, int nplanes)
+{
+    for (int v0 = 0; v0 < nplanes; v0 += 8) {
+        double r[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (v0 + k < nplanes) r[k] = src[(long long)(v0 + k) * ss];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (v0 + k < nplanes) dst[(long long)(v0 + k) * ds] = r[k];
+    }
+}
+
+// Same-level guard copies: each CTA takes whole segments (blockIdx.x, then
+// every gridDim.x-th), its threads walk the segment's cells, i fastest.
 static __global__ void k_exchange(const XSegDev* __restrict__ segs, int nseg, long long total,
                                   const XPtr* __restrict__ blk, int nplanes)
 {
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = nseg - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (segs[mid].first <= c) lo = mid;
-            else hi = mid - 1;
-        }
-        const XSegDev s = segs[lo];
-        long long r = c - s.first;
-        const int nx = s.hi[0] - s.lo[0], ny = s.hi[1] - s.lo[1];
-        const int i = s.lo[0] + (int)(r % nx);
-        r /= nx;
-        const int j = s.lo[1] + (int)(r % ny);
-        const int k = s.lo[2] + (int)(r / ny);
+    (void)total;
+    for (int sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+        const XSegDev s = segs[sg];
+        const int nx = s.hi[0] - s.lo[0], ny = s.hi[1] - s.lo[1], nz = s.hi[2] - s.lo[2];
+        const long long cells = (long long)nx * ny * nz;
         const XPtr d = blk[s.dst], q = blk[s.src];
-        const long long di = ((long long)k * d.ext[1] + j) * d.ext[0] + i;
-        const long long si = ((long long)(k + s.shift[2]) * q.ext[1] + (j + s.shift[1])) * q.ext[0] + (i + s.shift[0]);
-        for (int v = 0; v < nplanes; ++v) d.u[(long long)v * d.plane + di] = q.u[(long long)v * q.plane + si];
+        for (long long r = threadIdx.x; r < cells; r += blockDim.x) {
+            const int i = s.lo[0] + (int)(r % nx);
+            const long long rr = r / nx;
+            const int j = s.lo[1] + (int)(rr % ny);
+            const int k = s.lo[2] + (int)(rr / ny);
+            const long long di = ((long long)k * d.ext[1] + j) * d.ext[0] + i;
+            const long long si =
+                ((long long)(k + s.shift[2]) * q.ext[1] + (j + s.shift[1])) * q.ext[0] + (i + s.shift[0]);
+            copy_planes(d.u + di, d.plane, q.u + si, q.plane, nplanes);
+        }
     }
 }
 
@@ -288,11 +304,11 @@ static __global__ void k_halo_copy(const XSegDev* __restrict__ segs, int nseg, l
         if (to_buf) {
             const XPtr q = blk[s.src];
             const long long si = ((long long)(k + s.shift[2]) * q.ext[1] + (j + s.shift[1])) * q.ext[0] + (i + s.shift[0]);
-            for (int v = 0; v < nplanes; ++v) buf[(long long)v * total + c] = q.u[(long long)v * q.plane + si];
+            copy_planes(buf + c, total, q.u + si, q.plane, nplanes);
         } else {
             const XPtr d = blk[s.dst];
             const long long di = ((long long)k * d.ext[1] + j) * d.ext[0] + i;
-            for (int v = 0; v < nplanes; ++v) d.u[(long long)v * d.plane + di] = buf[(long long)v * total + c];
+            copy_planes(d.u + di, d.plane, buf + c, total, nplanes);
         }
     }
 }
@@ -411,7 +427,7 @@ static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long lo
         const int cx = r.cx + ((r.px + i) >> 1);
         const long long fo = ((long long)r.fz * F.ext[1] + r.fy) * F.ext[0] + (r.fx + i);
         const long long co = ((long long)r.cz * C.ext[1] + r.cy) * C.ext[0] + cx;
-        for (int v = 0; v < nu; ++v) F.u[(long long)v * F.plane + fo] = C.u[(long long)v * C.plane + co];
+        copy_planes(F.u + fo, F.plane, C.u + co, C.plane, nu);
         const long long sx = has_x, sy = has_y ? C.ext[0] : 0, sz = has_z ? (long long)C.ext[0] * C.ext[1] : 0;
         for (int v = nu; v < nu + nmag; ++v) {
             const double* c = C.u + (long long)v * C.plane + co;

@@ -22,6 +22,10 @@ constexpr int NVARIANT = 7;
 constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512};
 constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1};
 constexpr int STAGE_MAXT = 320;       // threads per CTA of the stage kernel
+// launch-bound variants of the batched stage kernel (threads per CTA, CTAs per SM)
+constexpr int NSTAGE_VARIANT = 3;
+constexpr int SV_T[NSTAGE_VARIANT] = {320, 128, 192};
+constexpr int SV_B[NSTAGE_VARIANT] = {1, 3, 2};
 constexpr int W3_VARIANT = 2;          // interpol_str = 'weno3' runs this launch-bound variant only
 
 struct Block {
@@ -109,6 +113,7 @@ struct pk_ctx {
     pk::BatchList batch[3];
     std::vector<pk::StageList> sbatch[3];       // batched stage per direction, per level
     bool stage_batched = false;                 // every block's pencils fit one stage CTA
+    int stage_variant = 0;                      // launch-bound variant of k_stage_batched (SV_T / SV_B)
     pk::FcArgs* d_fcargs[3] = {nullptr, nullptr, nullptr};   // per block flux couplings (refined domains)
     pk_time_state ts;
     std::string err;

@@ -483,8 +483,8 @@ struct StageItem {
     int block, i1_0, i2, P;
 };
 
-template <class PH, int MAXT, bool W3 = false, bool FC = false>
-__global__ void __launch_bounds__(MAXT) k_stage_batched(const BlockDesc* __restrict__ blocks,
+template <class PH, int MAXT, int MINB, bool W3 = false, bool FC = false>
+__global__ void __launch_bounds__(MAXT, MINB) k_stage_batched(const BlockDesc* __restrict__ blocks,
                                                        const StageItem* __restrict__ items, int dir, PhysParams pp,
                                                        int first, double rk, const StepParams* __restrict__ spar,
                                                        const FcArgs* __restrict__ fcs, unsigned* __restrict__ gstatus)

@@ -44,6 +44,19 @@ BatchedFn<PH> batched_variant(int v, bool w3 = false)
     }
 }
 
+// the batched stage kernel of launch-bound variant v (SV_T / SV_B); WENO3
+// runs variant 0 only
+template <class PH>
+auto stage_batched_variant(int v, bool w3, bool fc) -> decltype(&k_stage_batched<PH, 320, 1, false, false>)
+{
+    if (w3) return fc ? k_stage_batched<PH, 320, 1, true, true> : k_stage_batched<PH, 320, 1, true, false>;
+    switch (v) {
+    case 1: return fc ? k_stage_batched<PH, 128, 3, false, true> : k_stage_batched<PH, 128, 3, false, false>;
+    case 2: return fc ? k_stage_batched<PH, 192, 2, false, true> : k_stage_batched<PH, 192, 2, false, false>;
+    default: return fc ? k_stage_batched<PH, 320, 1, false, true> : k_stage_batched<PH, 320, 1, false, false>;
+    }
+}
+
 template <class PH>
 int set_smem_attr(pk_ctx* h)
 {
@@ -60,14 +73,11 @@ int set_smem_attr(pk_ctx* h)
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, false, false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, false, true>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, true, false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_stage_batched<PH, STAGE_MAXT, true, true>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        for (int v = 0; v < NSTAGE_VARIANT; ++v)
+            for (int w3 = 0; w3 < 2; ++w3)
+                for (int fc = 0; fc < 2; ++fc)
+                    PK_CUDA(h, cudaFuncSetAttribute(stage_batched_variant<PH>(v, w3, fc),
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -376,12 +386,12 @@ int launch_stage_batched(pk_ctx* h, int dir, int level, int first, double rk)
     if (!sl.n) return PK_OK;
     if (int rc = set_smem_attr<PH>(h)) return rc;
     const bool hooks = h->d_fcargs[dir] != nullptr;
-    auto* kern = h->pp.weno3 ? (hooks ? k_stage_batched<PH, STAGE_MAXT, true, true> : k_stage_batched<PH, STAGE_MAXT, true, false>)
-                             : (hooks ? k_stage_batched<PH, STAGE_MAXT, false, true> : k_stage_batched<PH, STAGE_MAXT, false, false>);
+    const int v = h->pp.weno3 ? 0 : h->stage_variant;
+    auto* kern = stage_batched_variant<PH>(v, h->pp.weno3, hooks);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    kern<<<sl.n, STAGE_MAXT, sl.smem, h->stream>>>(h->d_desc[h->cur], sl.dev, dir, h->pp, first, rk, h->d_step,
-                                                  h->d_fcargs[dir], h->d_status);
+    kern<<<sl.n, SV_T[v], sl.smem, h->stream>>>(h->d_desc[h->cur], sl.dev, dir, h->pp, first, rk, h->d_step,
+                                               h->d_fcargs[dir], h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;

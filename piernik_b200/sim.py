@@ -227,6 +227,11 @@ class Simulation:
         """Sweep all blocks in one persistent launch over a tile work list."""
         self._chk(self.lib.pk_set_batch(self.h, int(enable), length, variant), "pk_set_batch")
 
+    def set_stage_variant(self, variant: int) -> None:
+        """Launch-bound variant of the batched stage kernel (0: 320 x 1,
+        1: 128 x 3, 2: 192 x 2 threads x CTAs per SM)."""
+        self._chk(self.lib.pk_set_stage_variant(self.h, variant), "pk_set_stage_variant")
+
     def use_graph(self, enable: bool = True) -> None:
         """Replay each step's sweeps as a captured CUDA graph."""
         self._chk(self.lib.pk_use_graph(self.h, int(enable)), "pk_use_graph")

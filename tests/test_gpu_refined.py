@@ -72,7 +72,7 @@ def test_refined_single_sweeps(gpu_lib, phys):
     sim.close()
 
 
-@pytest.mark.parametrize("name", sorted(CASES) + ["mhd-3d-moncen+graph"])
+@pytest.mark.parametrize("name", sorted(CASES) + ["mhd-3d-moncen+graph", "hd-3d+v1", "mhd-3d-moncen+v2"])
 def test_refined_matches_oracle(gpu_lib, name):
     graph = name.endswith("+graph")
     c = CASES[name.split("+")[0]]
@@ -80,6 +80,8 @@ def test_refined_matches_oracle(gpu_lib, name):
     a = amr.AmrOracle(c["dom"], blocks)
     a.fill_guards()
     sim = library(c["dom"], blocks, graph=graph)
+    if "+v" in name:
+        sim.set_stage_variant(int(name[-1]))               # another launch shape, the same arithmetic
     compare(sim, a, "after the first boundary update")
     a.run(3)
     sim.run(3)
