@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--tune-log", default=None)
     p.add_argument("--workload", default="mhd256",
                    choices=["mhd256", "batched", "batched-independent", "adjoint", "ot-gradient",
-                            "batched-adjoint"],
+                            "batched-adjoint", "unsplit"],
                    help="mhd256: the headline 256^3 MHD block; batched: 512 uneven 3-fluid blocks; "
                         "adjoint: gradient of --steps steps of the MHD block at --n; ot-gradient: the "
                         "differentiable Orszag-Tang workload (512^2, K = 100) with its FD check; "
@@ -796,8 +796,49 @@ def batched_adjoint_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def unsplit_arm(args):
+    """The 256^3 MHD turbulence block through the unsplit scheme
+    (solver_str = 'unsplit'): one dt per step, every stage the face fluxes of
+    x, y and z from the same state, CFL 0.3 and cfl_glm 0.3 (the values the
+    reference recommends for this solver, global.F90:525-533)."""
+    import torch
+    from piernik_b200 import build, problems
+    from piernik_b200.sim import Simulation
+    build.build()
+    torch.cuda.set_device(0)
+    setup, u, b, psi = problems.mhd_turbulence(n=args.n, seed=args.seed, cfl=0.3)
+    setup = setup.replace(solver="unsplit", cfl_glm=0.3)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.run(args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(0)
+    l0, _, _ = sim.profile_read()
+    e0.record(stream)
+    sim.run(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    l1, _, _ = sim.profile_read()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    n = args.n
+    out = {"metric": "FP64 MHD cell-updates/s at %d^3, unsplit scheme" % n, "value": n ** 3 * args.steps / (ms / 1e3),
+           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"3D ideal-MHD decaying turbulence, one periodic {n}^3 block, unsplit HLLD + GLM, "
+                                  f"moncen, RK2, CFL 0.3", "step": "time_step + fluid_update_unsplit (1 dt)"},
+           "gpu_launches": l1 - l0, "clocks": ck}
+    print(json.dumps(out), flush=True)
+    sim.close()
+
+
 def main():
     args = parse()
+    if args.workload == "unsplit":
+        unsplit_arm(args)
+        return
     if args.workload == "batched-adjoint":
         batched_adjoint_arm(args)
         return

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PK_ABI_VERSION 2
+#define PK_ABI_VERSION 3
 
 enum {
     PK_OK = 0,
@@ -79,7 +79,13 @@ typedef struct pk_config {
      * w_epsilon (:255) for WENO3 */
     int32_t interpolation;
     double w_epsilon;
+    /* solver_str (global.F90:423-437): PK_SOLVER_SPLIT (RIEMANN_SPLIT) or
+     * PK_SOLVER_UNSPLIT (RIEMANN_UNSPLIT, src/scheme/unsplit_schemes) */
+    int32_t solver;
 } pk_config;
+
+#define PK_SOLVER_SPLIT   0
+#define PK_SOLVER_UNSPLIT 1
 
 #define PK_INTERP_LINEAR 0
 #define PK_INTERP_WENO3  1
@@ -150,7 +156,13 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out);
 int pk_time_step(pk_handle h, double* dt_out);
 
 /* fluid_update_full (src/scheme/fluidupdate.F90:99-136): update_chspeed,
- * X->Y->Z sweeps, glmdamping, Z->Y->X sweeps, glmdamping; t += 2 dt. */
+ * X->Y->Z sweeps, glmdamping, Z->Y->X sweeps, glmdamping; t += 2 dt.
+ * With PK_SOLVER_UNSPLIT: fluid_update_unsplit (unsplit_fluidupdate.F90:
+ * 45-126): update_chspeed, glmdamping over dt/2, t += dt, one unsplit sweep
+ * (every stage: the face fluxes of all directions from the same state, the
+ * x, y, z flux differences applied in turn, sources and floors;
+ * unsplit_sweeps.F90:104-189), glmdamping over dt/2.  The unsplit scheme
+ * runs on single or independent (unconnected) blocks. */
 int pk_fluid_update(pk_handle h);
 
 /* nsteps iterations of the reference main loop body (time_step +

@@ -55,6 +55,7 @@ class OCfg(C.Structure):
         ("max_redostep_attempts", C.c_int),
         ("interpolation", C.c_int),
         ("w_epsilon", C.c_double),
+        ("solver", C.c_int),
     ]
 
 
@@ -174,6 +175,7 @@ def make_cfg(setup) -> OCfg:
     c.max_redostep_attempts = setup.max_redostep_attempts
     c.interpolation = {"linear": 0, "weno3": 1}[setup.interpolation]
     c.w_epsilon = setup.w_epsilon
+    c.solver = {"split": 0, "unsplit": 1}[setup.solver]
     return c
 
 

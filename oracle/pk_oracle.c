@@ -565,9 +565,6 @@ static void o_work_free(o_work *w)
     free(w->qr); free(w->bl); free(w->br); free(w->flx); free(w->mflx); free(w->dq);
 }
 
-/* solve (solve_cg_riemann.F90:318-376) or solve_u (:378-414) on one pencil of
- * length n: u1/b1 enter as the current state and leave as the Euler update of
- * u0/b0 by dtodx.  No f/c flux substitution (single-level blocks). */
 /* the ext_fluxes of one pencil: faces replaced (li, ri; -1 none) and faces
  * recorded (lo, ro; -1 none) with their flux vectors */
 typedef struct o_pfc {
@@ -590,8 +587,10 @@ static void o_pfc_face(const o_lay *L, int mag, int m, o_work *w, int face, cons
         }
 }
 
-static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx, double ch, o_work *w,
-                           const o_pfc *pf)
+/* interpol + riemann_wrap (solve_cg_riemann.F90:346-351): the face fluxes
+ * flx (nv columns) and mflx (Bx, By, Bz, psi in sweep order) of the pencil
+ * state u1 / b1 of length n */
+static void o_pencil_fluxes(const o_cfg *cfg, const o_lay *L, int n, double ch, o_work *w)
 {
     const int nv = L->nv, m = n - 1;
     const int mag = cfg->magnetic;
@@ -642,6 +641,17 @@ static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx
             for (int c = 0; c < nc; ++c) w->flx[(size_t)(L->beg[f] + c) * m + i] = fx[c];
         }
     }
+}
+
+/* solve (solve_cg_riemann.F90:318-376) or solve_u (:378-414) on one pencil of
+ * length n: u1/b1 enter as the current state and leave as the Euler update of
+ * u0/b0 by dtodx, with the pencil's ext_fluxes pf (or NULL) */
+static void o_pencil_solve(const o_cfg *cfg, const o_lay *L, int n, double dtodx, double ch, o_work *w,
+                           const o_pfc *pf)
+{
+    const int nv = L->nv, m = n - 1;
+    const int mag = cfg->magnetic;
+    o_pencil_fluxes(cfg, L, n, ch, w);
 
     /* external fluxes (solve_cg_riemann.F90:353-362): li, ri replace, then lo, ro record */
     if (pf) {
@@ -1001,14 +1011,18 @@ int o_time_step(const o_cfg *cfg, const o_block *blk, o_state *st)
         st->dt = dt;
         return 3;
     }
-    double rem = cfg->tend - st->t;                       /* :224 */
-    dt = f_min(f_min(dt, cfg->dt_max), (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem));
+    double rem = cfg->tend - st->t;                       /* :221-225 */
+    if (cfg->solver == 1) dt = f_min(f_min(dt, cfg->dt_max), rem + ((2.0 * DBL_EPSILON) * rem));
+    else dt = f_min(f_min(dt, cfg->dt_max), (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem));
     st->dt = dt;
     return 0;
 }
 
+int o_fluid_update_unsplit(const o_cfg *cfg, o_block *blk, o_state *st);
+
 int o_fluid_update(const o_cfg *cfg, o_block *blk, o_state *st)
 {
+    if (cfg->solver == 1) return o_fluid_update_unsplit(cfg, blk, st);
     const double dt = st->dt;
     int rc;
     if (cfg->magnetic) st->chspeed = o_chspeed(cfg, blk, dt);   /* update_chspeed (fluidupdate.F90:113) */
@@ -1255,5 +1269,207 @@ int o_run_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st, int
         if (rc) return rc;
         st->nstep += 1;
     }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* The unsplit scheme (RIEMANN_UNSPLIT, src/scheme/unsplit_schemes)    */
+/* ------------------------------------------------------------------ */
+
+/* pencil of direction ddim at (i1, i2) of arrays u / b / psi into w->u1 / w->b1
+ * in sweep order (solve_cg_unsplit.F90:120-131, unsplit_mag_modules.F90:109-114) */
+static void o_load_pencil(const o_lay *L, int mag, const size_t cst[3], int n, int ddim, size_t base,
+                          const double *u, const double *b, const double *psi, o_work *w)
+{
+    const int *pm = PERM3[ddim];
+    const int nv = L->nv;
+    for (int i = 0; i < n; ++i) {
+        const size_t cell = base + (size_t)i * cst[ddim];
+        const double *pu = u + cell * nv;
+        for (int f = 0; f < L->nfl; ++f) {
+            const int bb = L->beg[f];
+            const int cols[5] = {L->idn[f], L->imx[f] + pm[0], L->imx[f] + pm[1], L->imx[f] + pm[2], L->ien[f]};
+            for (int c = 0; c < (L->has_en[f] ? 5 : 4); ++c) w->u1[(size_t)cols[c] * n + i] = pu[bb + c];
+        }
+        if (mag) {
+            for (int c = 0; c < 3; ++c) w->b1[(size_t)pm[c] * n + i] = b[cell * 3 + c];
+            w->b1[3 * (size_t)n + i] = psi ? psi[cell] : 0.0;
+        }
+    }
+}
+
+static void o_store_pencil_u(const o_lay *L, const size_t cst[3], int n, int ddim, size_t base, double *u,
+                             const o_work *w)
+{
+    const int *pm = PERM3[ddim];
+    const int nv = L->nv;
+    for (int i = 0; i < n; ++i) {
+        double *pu = u + (base + (size_t)i * cst[ddim]) * nv;
+        for (int f = 0; f < L->nfl; ++f) {
+            const int bb = L->beg[f];
+            const int cols[5] = {L->idn[f], L->imx[f] + pm[0], L->imx[f] + pm[1], L->imx[f] + pm[2], L->ien[f]};
+            for (int c = 0; c < (L->has_en[f] ? 5 : 4); ++c) pu[bb + c] = w->u1[(size_t)cols[c] * n + i];
+        }
+    }
+}
+
+/* one stage of solve_cg_unsplit (solve_cg_unsplit.F90:52-93 and :95-165,
+ * unsplit_mag_modules.F90:56-154): the face fluxes of every direction from
+ * the stage's input state, then T = T + dt/dl(d) * rk_coef * (F(i) - F(i+1))
+ * for d = x, y, z over bounds_for_flux (all but the outermost guard layer
+ * along d, the interior across), for B, u and psi, then apply_source
+ * (unsplit_source.F90:36-132): per direction with extent, the pencils through
+ * the interior get internal_sources and, at the last stage,
+ * care_for_positives.  istep 1 is the first stage (EULER or RK2_1). */
+int o_unsplit_stage(const o_cfg *cfg, o_block *blk, int istep, double dt, double ch)
+{
+    o_lay L;
+    o_layout(cfg, &L);
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    const int nv = L.nv, mag = cfg->magnetic, fw = nv + 4;
+    const size_t cst[3] = {1, (size_t)ext[0], (size_t)ext[0] * ext[1]};
+    const size_t ncell = (size_t)ext[0] * ext[1] * ext[2];
+    const int order = cfg->integration_order;
+    const int first = (istep == 1), last = (order == 1) || (istep == 2);
+    const double rk = (order == 1) ? 1.0 : (first ? 0.5 : 1.0);
+    const double *su = (first || order < 2) ? blk->u : blk->uh;
+    const double *sb = mag ? ((first || order < 2) ? blk->b : blk->bh) : NULL;
+    const double *sp = mag ? ((first || order < 2) ? blk->psi : blk->psih) : NULL;
+    double *F = calloc((size_t)3 * ncell * fw, sizeof(double));
+    if (!F) return 1;
+
+    for (int ddim = 0; ddim < 3; ++ddim) {
+        if (blk->n[ddim] <= 1) continue;
+        const int n = ext[ddim], o1 = ORTHO[ddim][0], o2 = ORTHO[ddim][1];
+        const int *pm = PERM3[ddim];
+#pragma omp parallel
+        {
+            o_work w;
+            o_work_init(&w, n, nv);
+#pragma omp for collapse(2) schedule(static)
+            for (int i2 = g[o2]; i2 < g[o2] + blk->n[o2]; ++i2)
+                for (int i1 = g[o1]; i1 < g[o1] + blk->n[o1]; ++i1) {
+                    const size_t base = (size_t)i1 * cst[o1] + (size_t)i2 * cst[o2];
+                    o_load_pencil(&L, mag, cst, n, ddim, base, su, sb, sp, &w);
+                    o_pencil_fluxes(cfg, &L, n, ch, &w);
+                    /* pflux(:, 1) = 0, pflux(:, i) = flux(i-1): the flux through the left face of cell i */
+                    for (int i = 1; i < n; ++i) {
+                        double *fc = F + ((size_t)ddim * ncell + base + (size_t)i * cst[ddim]) * fw;
+                        for (int f = 0; f < L.nfl; ++f) {
+                            const int bb = L.beg[f];
+                            const int cols[5] = {L.idn[f], L.imx[f] + pm[0], L.imx[f] + pm[1], L.imx[f] + pm[2], L.ien[f]};
+                            for (int c = 0; c < (L.has_en[f] ? 5 : 4); ++c)
+                                fc[bb + c] = w.flx[(size_t)cols[c] * (n - 1) + i - 1];
+                        }
+                        if (mag) {
+                            for (int c = 0; c < 3; ++c) fc[nv + c] = w.mflx[(size_t)pm[c] * (n - 1) + i - 1];
+                            fc[nv + 3] = w.mflx[3 * (size_t)(n - 1) + i - 1];
+                        }
+                    }
+                }
+            o_work_free(&w);
+        }
+    }
+
+    /* apply_flux (mag first, then u) and update_psi */
+    double *Tu = blk->u, *Tb = blk->b, *Tp = blk->psi;
+    if (order == 2 && first) {
+        memcpy(blk->uh, blk->u, ncell * nv * sizeof(double));
+        if (mag) {
+            memcpy(blk->bh, blk->b, ncell * 3 * sizeof(double));
+            memcpy(blk->psih, blk->psi, ncell * sizeof(double));
+        }
+        Tu = blk->uh;
+        Tb = blk->bh;
+        Tp = blk->psih;
+    }
+    for (int part = 0; part < 3; ++part) {               /* 0: B, 1: u, 2: psi */
+        if (part != 1 && !mag) continue;
+        for (int af = 0; af < 3; ++af) {
+            if (blk->n[af] <= 1) continue;
+            const double coef = (dt / blk->dl[af]) * rk;
+            int lo[3], hi[3];
+            for (int d = 0; d < 3; ++d) {
+                if (blk->n[d] <= 1) lo[d] = hi[d] = 0;
+                else if (d == af) { lo[d] = 1; hi[d] = ext[d] - 2; }
+                else { lo[d] = g[d]; hi[d] = g[d] + blk->n[d] - 1; }
+            }
+            for (int k = lo[2]; k <= hi[2]; ++k)
+                for (int j = lo[1]; j <= hi[1]; ++j)
+                    for (int i = lo[0]; i <= hi[0]; ++i) {
+                        const size_t cell = (size_t)i * cst[0] + (size_t)j * cst[1] + (size_t)k * cst[2];
+                        const double *f0 = F + ((size_t)af * ncell + cell) * fw;
+                        const double *f1 = F + ((size_t)af * ncell + cell + cst[af]) * fw;
+                        if (part == 1)
+                            for (int c = 0; c < nv; ++c) Tu[cell * nv + c] = Tu[cell * nv + c] + coef * (f0[c] - f1[c]);
+                        else if (part == 0)
+                            for (int c = 0; c < 3; ++c)
+                                Tb[cell * 3 + c] = Tb[cell * 3 + c] + coef * (f0[nv + c] - f1[nv + c]);
+                        else
+                            Tp[cell] = Tp[cell] + coef * (f0[nv + 3] - f1[nv + 3]);
+                    }
+        }
+    }
+    free(F);
+
+    /* apply_source */
+    int dnneg = 0, eineg = 0;
+    for (int ddim = 0; ddim < 3; ++ddim) {
+        if (blk->n[ddim] <= 1) continue;
+        const int n = ext[ddim], o1 = ORTHO[ddim][0], o2 = ORTHO[ddim][1];
+        o_work w;
+        o_work_init(&w, n, nv);
+        for (int i2 = g[o2]; i2 < g[o2] + blk->n[o2]; ++i2)
+            for (int i1 = g[o1]; i1 < g[o1] + blk->n[o1]; ++i1) {
+                const size_t base = (size_t)i1 * cst[o1] + (size_t)i2 * cst[o2];
+                o_load_pencil(&L, mag, cst, n, ddim, base, Tu, Tb, NULL, &w);
+                o_internal_sources(&L, n, &w);
+                if (last) o_care_for_positives(cfg, &L, n, &w, &dnneg, &eineg);
+                o_store_pencil_u(&L, cst, n, ddim, base, Tu, &w);
+            }
+        o_work_free(&w);
+    }
+    blk->dn_negative |= dnneg;
+    blk->ei_negative |= eineg;
+    return 0;
+}
+
+/* unsplit_sweep (unsplit_sweeps.F90:104-189): the stages, each followed by
+ * the boundary update of the array it wrote (uh / bh / psih after RK2_1) */
+int o_unsplit_sweep(const o_cfg *cfg, o_block *blk, double dt, double ch)
+{
+    const int nst = cfg->integration_order == 1 ? 1 : 2;
+    for (int s = 1; s <= nst; ++s) {
+        int rc = o_unsplit_stage(cfg, blk, s, dt, ch);
+        if (rc) return rc;
+        if (nst == 2 && s == 1) {
+            o_block h = *blk;
+            h.u = blk->uh;
+            h.b = blk->bh;
+            h.psi = blk->psih;
+            o_fill_guards(cfg, &h);
+        } else {
+            o_fill_guards(cfg, blk);
+        }
+    }
+    return 0;
+}
+
+/* fluid_update_unsplit (unsplit_fluidupdate.F90:45-126): update_chspeed,
+ * glmdamping over dt/2, t += dt, one unsplit sweep, glmdamping over dt/2 */
+int o_fluid_update_unsplit(const o_cfg *cfg, o_block *blk, o_state *st)
+{
+    const double dt = st->dt;
+    double fac = 1.0;
+    if (cfg->magnetic) {
+        st->chspeed = o_chspeed(cfg, blk, dt);
+        fac = o_glm_fac(cfg, blk, dt / 2.0, st->chspeed);          /* glmdamping(half = .true.) */
+        o_glm_apply(cfg, blk, fac);
+    }
+    st->t = st->t + dt;
+    int rc = o_unsplit_sweep(cfg, blk, dt, st->chspeed);
+    if (rc) return rc;
+    if (cfg->magnetic) o_glm_apply(cfg, blk, fac);
     return 0;
 }

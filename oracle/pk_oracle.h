@@ -52,6 +52,7 @@ typedef struct o_cfg {
     int max_redostep_attempts;   /* global.F90:258 */
     int interpolation;           /* 0 linear, 1 weno3 (interpol_str, global.F90:220) */
     double w_epsilon;            /* global.F90:255 */
+    int solver;                  /* 0 RIEMANN_SPLIT, 1 RIEMANN_UNSPLIT (solver_str, global.F90:423-437) */
 } o_cfg;
 
 #define O_CFL_NONE 0
@@ -108,6 +109,11 @@ void   o_fill_guards(const o_cfg *cfg, o_block *blk);
 int    o_sweep(const o_cfg *cfg, o_block *blk, int cdim, double dt, double ch);
 /* glmdamping factor and application (hdc.F90:289-349) */
 double o_glm_fac(const o_cfg *cfg, const o_block *blk, double dt, double ch);
+/* the unsplit scheme (src/scheme/unsplit_schemes): one stage (istep 1: first),
+ * the sweep of all stages with boundary updates, fluid_update_unsplit */
+int    o_unsplit_stage(const o_cfg *cfg, o_block *blk, int istep, double dt, double ch);
+int    o_unsplit_sweep(const o_cfg *cfg, o_block *blk, double dt, double ch);
+int    o_fluid_update_unsplit(const o_cfg *cfg, o_block *blk, o_state *st);
 void   o_glm_apply(const o_cfg *cfg, o_block *blk, double fac);
 /* update_chspeed with ch_grid (hdc.F90:90-140) */
 double o_chspeed(const o_cfg *cfg, const o_block *blk, double dt);

@@ -71,6 +71,7 @@ class PkConfig(C.Structure):
         ("max_redostep_attempts", C.c_int32),
         ("interpolation", C.c_int32),
         ("w_epsilon", C.c_double),
+        ("solver", C.c_int32),
     ]
 
 

@@ -53,6 +53,7 @@ class Setup:
     max_redostep_attempts: int = 10  # :258
     interpolation: str = "linear"    # interpol_str (:220): linear or weno3
     w_epsilon: float = 1.0e-10       # :255
+    solver: str = "split"            # solver_str (:423-437): split (RIEMANN_SPLIT) or unsplit (RIEMANN_UNSPLIT)
     skip_sweep: Tuple[bool, bool, bool] = (False, False, False)
     # END_CONTROL
     tend: float = DBL_HUGE
@@ -85,6 +86,8 @@ class Setup:
             raise ValueError("CFL value should be >0. and <=1.")      # global.F90:303
         if self.integration_order not in (1, 2):
             raise ValueError("integration_order must be 1 or 2")
+        if self.solver not in ("split", "unsplit"):
+            raise ValueError(f"solver {self.solver!r}: this library implements split and unsplit")
         if self.interpolation not in ("linear", "weno3"):
             raise ValueError(f"interpol_str {self.interpolation!r}: this library implements linear and weno3")
         if self.cflcontrol not in ("none", "warn", "redo", "repeat"):

@@ -110,7 +110,17 @@ BoxGeom box_of(const Block& b)
 
 double* state(pk_ctx* h, Block& b) { return b.buf[h->cur]; }
 
+int fill_guards_ptr(pk_ctx* h, Block& b, double* u);
+
 int fill_guards_block(pk_ctx* h, Block& b)
+{
+    if (int rc = fill_guards_ptr(h, b, state(h, b))) return rc;
+    b.guards_stale = false;
+    return PK_OK;
+}
+
+// update_boundaries of one block's own boundary rules on the array u
+int fill_guards_ptr(pk_ctx* h, Block& b, double* u)
 {
     GuardArgs a;
     int beg = 0;
@@ -124,10 +134,9 @@ int fill_guards_block(pk_ctx* h, Block& b)
     }
     a.nfl = h->cfg.nfluids;
     a.nplanes = h->nplanes;
-    k_fill_guards<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(box_of(b), state(h, b), a);
+    k_fill_guards<<<grid1d(b.plane, 256), 256, 0, h->stream>>>(box_of(b), u, a);
     PK_CUDA(h, cudaGetLastError());
     h->launches += 1;
-    b.guards_stale = false;
     return PK_OK;
 }
 
@@ -801,6 +810,19 @@ void glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fa
 
 void glm_scalars(pk_ctx* h, double dt, double* ch, double* fac) { glm_scalars_for(h, dt, h->ts.chspeed, ch, fac); }
 
+// the glmdamping factor for chspeed ch over dt_eff (hdc.F90:310-332)
+double glm_fac_for(pk_ctx* h, double dt_eff, double ch)
+{
+    int eff;
+    const double mdl = min_dl(h, &eff);
+    double f = 0.0;
+    if (eff) {
+        const double x = (h->cfg.glm_alpha * ch) / (mdl / dt_eff);
+        f = (x > f) ? x : f;
+    }
+    return std::exp(-f);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -840,13 +862,15 @@ void pk_config_default(pk_config* c)
     c->dt_shrink = 0.5;                // :245
     c->max_redostep_attempts = 10;     // :258
     c->interpolation = PK_INTERP_LINEAR;   // :220
+    c->solver = PK_SOLVER_SPLIT;          // :423-437
     c->w_epsilon = 1.0e-10;            // :255
 }
 
 int pk_create(const pk_config* cfg, pk_handle* out)
 {
     if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_REDO || cfg->max_redostep_attempts < 0 ||
-                cfg->interpolation < PK_INTERP_LINEAR || cfg->interpolation > PK_INTERP_WENO3))
+                cfg->interpolation < PK_INTERP_LINEAR || cfg->interpolation > PK_INTERP_WENO3 ||
+                cfg->solver < PK_SOLVER_SPLIT || cfg->solver > PK_SOLVER_UNSPLIT))
         return PK_E_ARG;
     if (!cfg || !out) return PK_E_ARG;
     *out = nullptr;
@@ -915,6 +939,7 @@ int pk_destroy(pk_handle h)
         cudaFree(b.buf[1]);
         cudaFree(b.uh);
         cudaFree(b.stage);
+        for (int d = 0; d < 3; ++d) cudaFree(b.flux[d]);
     }
     for (auto& p : h->ev_used) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
     for (auto& p : h->ev_free) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
@@ -1401,8 +1426,9 @@ static int clamp_dt(const pk_config& c, pk_time_state& ts, double dt, double c_a
         ts.dt = dt;
         return PK_E_DTMIN;
     }
-    const double rem = c.tend - ts.t;                 // :224
-    const double cap = (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem);
+    const double rem = c.tend - ts.t;                 // :221-225
+    const double cap = c.solver == PK_SOLVER_UNSPLIT ? rem + ((2.0 * DBL_EPSILON) * rem)
+                                                     : (0.5 * rem) + ((2.0 * DBL_EPSILON) * rem);
     dt = (c.dt_max < dt) ? c.dt_max : dt;
     dt = (cap < dt) ? cap : dt;
     ts.dt = dt;
@@ -1446,6 +1472,61 @@ static int run_step_sweeps(pk_ctx* h, double dt, double ch, double fac)
         return PK_OK;
     }
     return step_sweeps(h, dt, ch, fac);
+}
+
+// unsplit_sweep (unsplit_sweeps.F90:104-189) of every block: per stage the
+// face fluxes of all directions from the stage's input (u, or uh at RK2_2),
+// their application to T (uh = u + ... at RK2_1, u itself otherwise) with
+// sources and floors, then the boundary update of T.  dt and chspeed come
+// from d_step.
+static int unsplit_sweep(pk_ctx* h)
+{
+    if (h->connected) return fail(h, PK_E_UNSUPPORTED, "the unsplit scheme runs on single or independent blocks");
+    const PhysOps* ops = ops_of(h);
+    const int order = h->cfg.integration_order, nst = order == 1 ? 1 : 2;
+    for (auto& b : h->blocks) {
+        if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+        for (int d = 0; d < 3; ++d)
+            if (b.n[d] > 1 && !b.flux[d]) PK_CUDA(h, cudaMalloc(&b.flux[d], sizeof(double) * h->nplanes * b.plane));
+    }
+    for (int s = 1; s <= nst; ++s) {
+        const bool first = s == 1;
+        const int last = (order == 1) || (s == 2);
+        const double rk = order == 1 ? 1.0 : (first ? 0.5 : 1.0);
+        for (auto& b : h->blocks) {
+            double* u = state(h, b);
+            const double* in = (first || order < 2) ? u : b.uh;
+            double* T = (order == 2 && first) ? b.uh : u;
+            for (int d = 0; d < 3; ++d)
+                if (b.n[d] > 1)
+                    if (int rc = ops->unsplit_flux(h, b, d, in, b.flux[d])) return rc;
+            if (int rc = ops->unsplit_apply(h, b, u, T, rk, last)) return rc;
+            if (int rc = fill_guards_ptr(h, b, T)) return rc;
+            b.guards_stale = false;
+        }
+    }
+    return PK_OK;
+}
+
+// fluid_update_unsplit (unsplit_fluidupdate.F90:45-126)
+static int unsplit_fluid_update(pk_ctx* h)
+{
+    const double dt = h->ts.dt;
+    double ch = h->ts.chspeed, fac = 1.0;
+    if (h->cfg.magnetic) {
+        double fac_full;
+        glm_scalars_for(h, dt, h->ts.chspeed, &ch, &fac_full);   // update_chspeed
+        fac = glm_fac_for(h, dt / 2.0, ch);                      // glmdamping(half = .true.): dt_eff = dt/2
+        h->ts.chspeed = ch;
+    }
+    if (int rc = put_step_params(h, dt, ch, fac)) return rc;
+    if (h->cfg.magnetic)
+        if (int rc = glm_scale(h, fac)) return rc;
+    h->ts.t = h->ts.t + dt;                           // unsplit_fluidupdate.F90:98
+    if (int rc = unsplit_sweep(h)) return rc;
+    if (h->cfg.magnetic)
+        if (int rc = glm_scale(h, fac)) return rc;
+    return PK_OK;
 }
 
 // time_step of every stacked instance: its own CFL reduction and clamps
@@ -1544,6 +1625,7 @@ int pk_fluid_update(pk_handle h)
 {
     if (!h) return PK_E_ARG;
     if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
+    if (h->cfg.solver == PK_SOLVER_UNSPLIT) return unsplit_fluid_update(h);
     if (h->ninst > 1) return inst_fluid_update(h, nullptr);
     const double dt = h->ts.dt;
     double ch, fac;

@@ -447,4 +447,80 @@ static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long lo
     }
 }
 
+// apply_flux, update_psi and apply_source of one stage (solve_cg_unsplit.F90:
+// 167-229, unsplit_mag_modules.F90:195-350, unsplit_source.F90:36-132), one
+// thread per cell of the guard-inclusive block.  T starts as S (the first
+// RK2 stage writes the copy uh = u: S = u, T = uh; otherwise S = T = u) and
+// gains, for d = x, y, z over
+// bounds_for_flux(d) (every cell but the outermost layer along d, interior
+// across), (dt / dl(d)) * rk * (F_d(i) - F_d(i+1)); every plane, B and psi
+// included.  Then each cell on an interior pencil of direction d (d = x, y,
+// z with extent) gets internal_sources (+0) and, at the last stage,
+// care_for_positives in d's swept component order, once per such d.
+template <class PH>
+__global__ void k_unsplit_apply(BoxGeom b, const double* S, double* T,
+                                const double* __restrict__ Fx, const double* __restrict__ Fy,
+                                const double* __restrict__ Fz, PhysParams pp, const StepParams* __restrict__ spar,
+                                double rk, double dlx, double dly, double dlz, int last, unsigned* __restrict__ gstatus)
+{
+    constexpr int NV = PH::NV;
+    unsigned status = 0;
+    const long long ncell = (long long)b.ext[0] * b.ext[1] * b.ext[2];
+    const double* Fd[3] = {Fx, Fy, Fz};
+    const double dl[3] = {dlx, dly, dlz};
+    const long long stride[3] = {1, b.ext[0], (long long)b.ext[0] * b.ext[1]};
+    const double dt = spar->dt;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        int x[3];
+        x[0] = (int)(c % b.ext[0]);
+        const long long rr = c / b.ext[0];
+        x[1] = (int)(rr % b.ext[1]);
+        x[2] = (int)(rr / b.ext[1]);
+        bool in[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) in[d] = b.n[d] <= 1 || (x[d] >= b.g[d] && x[d] < b.g[d] + b.n[d]);
+        double nat[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) nat[v] = S[(long long)v * b.plane + c];
+#pragma unroll
+        for (int af = 0; af < 3; ++af) {
+            if (b.n[af] <= 1) continue;
+            bool reg = x[af] >= 1 && x[af] <= b.ext[af] - 2;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (d != af) reg = reg && in[d];
+            if (!reg) continue;
+            const double coef = (dt / dl[af]) * rk;
+            const double* F = Fd[af];
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+                nat[v] = nat[v] + coef * (F[(long long)v * b.plane + c] - F[(long long)v * b.plane + c + stride[af]]);
+        }
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+            if (b.n[dd] <= 1) continue;
+            bool pencil = true;                       // on a pencil of dd through the interior
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (d != dd) pencil = pencil && in[d];
+            if (!pencil) continue;
+            if (!last) {
+#pragma unroll
+                for (int v = 0; v < PH::NVF; ++v) nat[v] = nat[v] + 0.0;
+                continue;
+            }
+            const int perm[3] = {dd, dd == 1 ? 0 : 1, dd == 2 ? 0 : 2};   // iarr_swp of dd
+            double w[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) w[v] = nat[plane_of<PH>(v, perm)];
+            sources_and_floors<PH>(w, pp, status);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) nat[plane_of<PH>(v, perm)] = w[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) T[(long long)v * b.plane + c] = nat[v];
+    }
+    flush_status(status, gstatus);
+}
+
 }  // namespace pk

@@ -45,6 +45,7 @@ struct Block {
     FcArgs fc[3] = {};                     // fine/coarse flux couplings per sweep direction (device)
     unsigned char* leaf = nullptr;         // device interior leaf mask (null: every cell is a leaf)
     long long leaf_cells = -1;             // cells of the mask set (-1: all)
+    double* flux[3] = {nullptr, nullptr, nullptr};   // unsplit scheme: face fluxes per direction
 };
 
 struct pk_dir_tile { int P, L, V; };
@@ -189,6 +190,8 @@ struct PhysOps {
                      unsigned short* flags);
     int (*adj)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, const double* ustar,
                const double* uout, const unsigned short* flags, const double* lam_out, double* lam_in, double* m1);
+    int (*unsplit_flux)(pk_ctx* h, Block& b, int dir, const double* in, double* F);
+    int (*unsplit_apply)(pk_ctx* h, Block& b, const double* S, double* T, double rk, int last);
 };
 
 const PhysOps* ops_hd1();

@@ -524,4 +524,59 @@ __global__ void __launch_bounds__(MAXT, MINB) k_stage_batched(const BlockDesc* _
     flush_status(status, gstatus);
 }
 
+// -------------------------------------------------------------------------
+// The unsplit scheme (RIEMANN_UNSPLIT, src/scheme/unsplit_schemes).
+// -------------------------------------------------------------------------
+
+// Face fluxes of one direction (solve_cg_unsplit.F90:95-138,
+// unsplit_mag_modules.F90:56-128): the pencils through the interior, whole or
+// in chunks with a 2-cell halo as k_stage; the flux through the face between
+// storage cells s and s+1 goes to F at cell s+1 (pflux(:, i) is the flux
+// through cell i's left face), in the state's own plane order.
+template <class PH, int MAXT, bool W3 = false>
+__global__ void __launch_bounds__(MAXT) k_unsplit_flux(Geom g, Tile tl, const double* __restrict__ uin,
+                                                      double* __restrict__ F, PhysParams pp,
+                                                      const StepParams* __restrict__ spar,
+                                                      unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    constexpr int NV = PH::NV;
+    const int P = tl.P, T = tl.T, PT = P * T;
+    const Smem sm{smem, smem + NV * PT, smem + 2 * NV * PT, PT};
+    const int tid = threadIdx.x;
+    int p, t;
+    if (tl.xfast) { t = tid % T; p = tid / T; }
+    else { p = tid % P; t = tid / P; }
+    const int spp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
+    const int me = p * spp + t * st;
+    const int i1 = blockIdx.x * P + p;
+    const int c0 = blockIdx.y * tl.L;
+    const int i2 = blockIdx.z;
+    const int n = g.ext_d;
+    const int s = c0 - tl.halo + t;
+    const bool valid = (tid < PT) && (i1 < g.n1) && s >= 0 && s < n;
+    const bool own = valid && s >= c0 && s < c0 + tl.L;
+    const long long off = (long long)s * g.sd + (long long)(g.g1 + i1) * g.s1 + (long long)(g.g2 + i2) * g.s2;
+    double w[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) w[v] = 0.0;
+    if (valid) load_cell<PH>(uin, off, g, w);
+    Roles r;
+    r.q = valid;
+    r.end = (s == 0) ? -1 : ((s == n - 1) ? 1 : 0);
+    r.slope = valid && (r.end != 0 || (t >= 1 && t <= T - 2));
+    const bool next_slope = (s + 1 < n) && (t + 1 <= T - 1) && ((s + 1 == n - 1) || (t + 1 <= T - 2));
+    r.flux = r.slope && next_slope;
+    r.upd = false;
+    r.keep = false;
+    unsigned status = 0;
+    rk_stage<PH, false, W3>(sm, me, me - st, me + st, r, w, uin, uin, off, g, 0.0, spar->ch, pp, status);
+    if (own && r.flux) {
+        double f[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sm.Q[v * PT + me];
+        store_cell<PH>(F, off + g.sd, g, f);
+    }
+}
+
 }  // namespace pk

@@ -73,6 +73,10 @@ int set_smem_attr(pk_ctx* h)
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_unsplit_flux<PH, STAGE_MAXT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_unsplit_flux<PH, STAGE_MAXT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
         for (int v = 0; v < NSTAGE_VARIANT; ++v)
             for (int w3 = 0; w3 < 2; ++w3)
                 for (int fc = 0; fc < 2; ++fc)
@@ -398,11 +402,67 @@ int launch_stage_batched(pk_ctx* h, int dir, int level, int first, double rk)
     return PK_OK;
 }
 
+// the face fluxes of one direction for the unsplit scheme (k_unsplit_flux),
+// tiles as the stage kernel's
+template <class PH>
+int launch_unsplit_flux(pk_ctx* h, Block& b, int dir, const double* in, double* F)
+{
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    Geom g = make_geom(b, dir);
+    Tile tl;
+    const int ext = b.ext[dir];
+    if (ext <= STAGE_MAXT) {
+        int P = STAGE_MAXT / ext;
+        if (P >= 4) P -= P % 4;
+        if (P > g.n1) P = g.n1;
+        tl.P = P;
+        tl.T = ext;
+        tl.L = ext;
+        tl.halo = 0;
+    } else {
+        tl.P = 4;
+        tl.L = 64;
+        tl.T = tl.L + 4;
+        tl.halo = 2;
+    }
+    tl.xfast = (dir == 0);
+    dim3 grid((g.n1 + tl.P - 1) / tl.P, (ext + tl.L - 1) / tl.L, g.n2);
+    const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+    auto* kern = h->pp.weno3 ? k_unsplit_flux<PH, STAGE_MAXT, true> : k_unsplit_flux<PH, STAGE_MAXT, false>;
+    kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, F, h->pp, h->d_step, h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+    h->launches += 1;
+    return PK_OK;
+}
+
+template <class PH>
+int launch_unsplit_apply(pk_ctx* h, Block& b, const double* S, double* T, double rk, int last)
+{
+    BoxGeom bg;
+    for (int d = 0; d < 3; ++d) {
+        bg.ext[d] = b.ext[d];
+        bg.g[d] = b.g[d];
+        bg.n[d] = b.n[d];
+    }
+    bg.plane = b.plane;
+    long long nblk = (b.plane + 255) / 256;
+    if (nblk > 148LL * 16) nblk = 148LL * 16;
+    k_unsplit_apply<PH><<<(int)nblk, 256, 0, h->stream>>>(bg, S, T, b.flux[0], b.flux[1], b.flux[2], h->pp, h->d_step,
+                                                          rk, b.dl[0], b.dl[1], b.dl[2], last, h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    h->launches += 1;
+    return PK_OK;
+}
+
 template <class PH>
 const PhysOps* make_ops()
 {
     static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_stage_batched<PH>,
-                     launch_batched<PH>, launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>};
+                     launch_batched<PH>, launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>,
+                     launch_unsplit_flux<PH>, launch_unsplit_apply<PH>};
     return &o;
 }
 

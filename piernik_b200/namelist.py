@@ -184,13 +184,18 @@ def read_problem_par(text: str, cmdline: Optional[str] = None, setup: Optional[S
         kw["interpolation"] = names[val]                  # interpolations.F90:set_interpolations
     if "w_epsilon" in ns:
         kw["w_epsilon"] = float(ns["w_epsilon"])
-    for key in ("solver_str", "divb_0"):
-        if key in ns:
-            val = str(ns[key]).strip().lower()
-            ok = {"solver_str": ("", "riemann", "riemann_split"),
-                  "divb_0": ("hdc", "glm", "divergence cleaning")}[key]
-            if val not in ok:
-                raise ValueError(f"{key}={val!r} is outside the sweep path this library implements")
+    if "solver_str" in ns:                               # global.F90:423-437
+        val = str(ns["solver_str"]).strip().lower()
+        if val in ("", "riemann", "riemann_split"):
+            kw["solver"] = "split"
+        elif val in ("unsplit", "van_leer", "riemann_unsplit"):
+            kw["solver"] = "unsplit"
+        else:
+            raise ValueError(f"solver_str={val!r} is outside the sweep path this library implements")
+    if "divb_0" in ns:
+        val = str(ns["divb_0"]).strip().lower()
+        if val not in ("hdc", "glm", "divergence cleaning"):
+            raise ValueError(f"divB_0={val!r} is outside the sweep path this library implements")
     end = g.get("END_CONTROL", {})
     if "tend" in end:
         kw["tend"] = float(end["tend"])

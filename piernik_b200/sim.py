@@ -70,6 +70,7 @@ def make_config(setup: Setup) -> L.PkConfig:
     c.max_redostep_attempts = setup.max_redostep_attempts
     c.interpolation = {"linear": 0, "weno3": 1}[setup.interpolation]
     c.w_epsilon = setup.w_epsilon
+    c.solver = {"split": 0, "unsplit": 1}[setup.solver]
     return c
 
 
