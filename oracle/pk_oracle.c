@@ -1,10 +1,14 @@
 /*
  * pk_oracle.c -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
  *
- * A CPU restatement of PIERNIK's RIEMANN_SPLIT fluid update, written to be the
- * checker for the CUDA library (see pk_oracle.h for the parity status: the
- * restatement is UNPINNED because the Fortran reference cannot be built here
- * and holds no golden vectors for this path).
+ * A CPU restatement of PIERNIK's RIEMANN_SPLIT fluid update (and of
+ * RIEMANN_UNSPLIT, which shares its reconstruction, Riemann solvers, floors,
+ * CFL and GLM code), written to be the checker for the CUDA library.  Parity
+ * is pinned by the reference's own known answers: run through the unsplit
+ * scheme, the CPAW test (problems/cpaw, Makefile CPAW target) reproduces the
+ * reference's L2 errors at every tabulated resolution to the 8 printed
+ * decimals (tests/test_cpaw.py); the split-only parts are pinned by exact
+ * physical properties (tests/test_oracle.py).
  *
  * Every routine cites the reference routine it restates, by path within the
  * PIERNIK source tree.  Floating-point expressions keep the reference's

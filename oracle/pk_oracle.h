@@ -5,13 +5,19 @@
  * used only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
  * leg, as the checker the CUDA library is compared against.
  *
- * Parity status: UNPINNED.  The reference is Fortran 2008 and no Fortran
- * compiler exists in this environment, and the reference tree holds no golden
- * vectors for this path (its gold tests regenerate outputs from upstream git).
- * The restatement follows the reference sources operation by operation
- * (evaluation order, Fortran intrinsics spacing/sign/min/max, the -0.0
- * normalisation done by internal_sources) and is cross-checked by physics
- * properties in tests/ (conservation, axis-permutation symmetry).
+ * Parity status: pinned by the reference's known answers.  The reference is
+ * Fortran 2008 and no Fortran compiler exists in this environment; its gold
+ * tests regenerate outputs from upstream git.  Its CPAW artifact test
+ * (Makefile CPAW target, problems/cpaw/problem.par:1-13) tabulates the L2
+ * error of B after one wave period at eight resolutions; the restatement,
+ * run through the unsplit scheme (which shares utoq, the limiters, HLLD with
+ * GLM, the floors, the CFL reduction and the GLM scalars with the split
+ * sweep), reproduces every one to the 8 printed decimals (tests/test_cpaw.py).
+ * The split-only structure (sweep order, per-sweep RK stages) follows the
+ * reference sources operation by operation (evaluation order, Fortran
+ * intrinsics spacing/sign/min/max, the -0.0 normalisation done by
+ * internal_sources) and is cross-checked by physics properties in tests/
+ * (conservation, axis-permutation symmetry).
  *
  * Layout mirrors the reference's named arrays with guard cells:
  *   u  (nvar, i, j, k)  -> u[((k*NY + j)*NX + i)*nvar + v]   (cg%u, cg%w(uh))

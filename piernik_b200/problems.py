@@ -468,3 +468,60 @@ def refined_blast(seed: int = 4, base: int = 128, centre=(70, 58, 66), r1: int =
     setup = Setup(n=(16, 16, 16), fluids=list(fluids), magnetic=magnetic, limiter="vanleer", limiter_b="vanleer",
                   cfl=0.7, cfl_glm=0.7, smalld=1.0e-4)
     return dom, refined_blocks(dom, layout, setup, blast_fields(centre, radius), dl0=dl0)
+
+
+def cpaw(nx: int = 128, ny: int = 64, A: float = 0.1, d0: float = 1.0, p0: float = 0.1, vA: float = 1.0,
+         kx: float = 6.283185307, ky: float = 12.566370614, gamma: float = 5.0 / 3.0):
+    """Circularly polarised Alfvén wave (problems/cpaw/initproblem.F90:
+    problem_initial_conditions, problem.par): [0,1] x [0,0.5] periodic, one
+    ionised fluid, the wave rotated by atan(ky/kx) in the x-y plane, run with
+    the unsplit solver, vanleer, CFL 0.3, cfl_glm 0.3, smalld = smallei = 1e-5
+    to tend = 0.447213595 (one period).  Returns (setup, u, b, psi, ini_b)
+    with ini_b the initial field (the reference compares B with it)."""
+    setup = Setup(n=(nx, ny, 1), xmin=(0.0, 0.0, 0.0), xmax=(1.0, 0.5, 1.0), fluids=[("ion", gamma)],
+                  magnetic=True, limiter="vanleer", limiter_b="vanleer", cfl=0.3, cfl_glm=0.3, smalld=1.0e-5,
+                  smallei=1.0e-5, solver="unsplit", cflcontrol="redo", tend=0.447213595)
+    u, b, psi = _empty(setup)
+    g = setup.guards
+    # cell centres: fbnd + dl * (i - is + 1/2) over the guard-inclusive range (grid_container_base.F90:377)
+    x = setup.xmin[0] + setup.dl[0] * (np.arange(setup.ext[0]) - g[0] + 0.5)
+    y = setup.xmin[1] + setup.dl[1] * (np.arange(setup.ext[1]) - g[1] + 0.5)
+    z = 0.5 * (setup.xmin[2] + setup.xmax[2])
+    aa = math.atan(ky / kx)
+    gg = math.atan(math.cos(aa) * (0.0 / kx))
+    kp = math.sqrt(kx ** 2 + ky ** 2)
+    rot = np.array([[math.cos(aa) * math.cos(gg), -math.sin(aa), -math.cos(aa) * math.sin(gg)],
+                    [math.sin(aa) * math.cos(gg), math.cos(aa), -math.sin(aa) * math.sin(gg)],
+                    [math.sin(gg), 0.0, math.cos(gg)]])
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    xp = (rot[0, 0] * X + rot[1, 0] * Y) + rot[2, 0] * z       # first row of rot^T . (x, y, z)
+    phi = kp * xp
+    s, c = np.sin(phi), np.cos(phi)
+    vp = [np.zeros_like(phi), A * s, A * c]
+    bp = [np.full_like(phi, vA * math.sqrt(d0)), -math.sqrt(d0) * A * s, -math.sqrt(d0) * A * c]
+    v = [(rot[i, 0] * vp[0] + rot[i, 1] * vp[1]) + rot[i, 2] * vp[2] for i in range(3)]
+    bf = [(rot[i, 0] * bp[0] + rot[i, 1] * bp[1]) + rot[i, 2] * bp[2] for i in range(3)]
+    ek = (0.5 * ((v[0] ** 2 + v[1] ** 2) + v[2] ** 2)) / d0
+    em = 0.5 * ((bf[0] ** 2 + bf[1] ** 2) + bf[2] ** 2)
+    gam_1 = gamma - 1.0
+    for k in range(setup.ext[2]):
+        u[k, :, :, 0] = d0
+        for dd in range(3):
+            u[k, :, :, 1 + dd] = v[dd]
+            b[k, :, :, dd] = bf[dd]
+        u[k, :, :, 4] = (p0 / gam_1 + ek) + em
+    return setup, u, b, psi, b.copy()
+
+
+def cpaw_error(setup, b, ini_b):
+    """verify_test (problems/cpaw/initproblem.F90): sqrt of the summed squared
+    deviation of B from its initial field over the interior, directions with
+    extent only, over the summed squares of the initial field."""
+    g, n = setup.guards, setup.n
+    sl = (slice(g[2], g[2] + n[2]), slice(g[1], g[1] + n[1]), slice(g[0], g[0] + n[0]))
+    num = den = 0.0
+    for d in range(3):
+        if n[d] > 1:
+            num += float(((ini_b[sl + (d,)] - b[sl + (d,)]) ** 2).sum())
+            den += float((ini_b[sl + (d,)] ** 2).sum())
+    return math.sqrt(num / den)
