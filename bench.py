@@ -44,6 +44,11 @@ NVAR = 9                         # dn, mx, my, mz, en, Bx, By, Bz, psi
 # 125.97 MB written over 128^3 cells); traffic grows with the cell count, so the
 # full-size figure is this times n^3.
 TRAFFIC_BYTES_PER_CELL = (161.756672e6 + 125.965568e6) / 128 ** 3
+# FP64 flops per cell of one fused sweep (both RK2 stages) without halo
+# recomputation, i.e. the algorithmic FP64 work: 2 DFMA + DMUL + DADD thread
+# instructions of the whole-pencil x sweep at 128^3 over its 128^3 cells
+# (profiles/k_sweep_fused_fp64_128cube.md)
+FP64_FLOP_PER_CELL_SWEEP = 3.589298377e9 / 128 ** 3
 
 
 def parse():
@@ -332,6 +337,17 @@ def our_arm(args):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": "k_sweep_fused<MHD> (one sweep direction, both RK2 stages)",
                 "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms, "peak_source": src}
+    # the bound that limits it: FP64 issue, against the device's measured DFMA rate
+    import ctypes
+    from piernik_b200 import _lib
+    peak64 = ctypes.c_double(0.0)
+    roofline_fp64 = None
+    if _lib.load().pk_fp64_peak(ctypes.byref(peak64)) == 0 and peak64.value > 0:
+        flops = FP64_FLOP_PER_CELL_SWEEP * n ** 3
+        got = flops / (launch_ms / 1e3) / 1e12
+        roofline_fp64 = {"bound": "fp64", "achieved": got, "peak": peak64.value, "unit": "TFLOP/s",
+                         "frac": got / peak64.value, "flop_per_launch": flops,
+                         "peak_source": "measured (pk_fp64_peak: independent DFMA chains)"}
 
     # end to end through the C ABI with host buffers in the reference's layout
     e2e = None
@@ -379,7 +395,7 @@ def our_arm(args):
                "config": dict(workload_config(n), parallelism=("one block" if world == 1 else
                                                                f"{world} z-slabs of {n}^3, NCCL halo exchange"),
                               tiles_P_L_variant_ms=tiles),
-               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+               "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": launches1 - launches0, "clocks": ck,
                "adjoint_cost_ratio": adjoint}
         print(json.dumps(out), flush=True)

@@ -310,6 +310,13 @@ int pk_grad_release(pk_handle h);
  * per pencil (0: default) and launch-bound variant (-1: default). */
 int pk_set_adjoint_tile(pk_handle h, int32_t dir, int32_t length, int32_t variant);
 
+/* ---- Measurement utility ----
+ * No counterpart in the reference.  The FP64 fused-multiply-add throughput
+ * of the current device in TFLOP/s (2 flops per DFMA), measured with a
+ * latency-free DFMA kernel: the denominator of the sweep kernels' FP64
+ * roofline.  Allocates 2 KiB of device memory for the call's duration. */
+int pk_fp64_peak(double* tflops);
+
 /* ---- Raw CFL time step without allocation ----
  * No counterpart in the reference.  For host codes that cannot let this
  * library allocate device memory (all of it is reserved for their own pool,

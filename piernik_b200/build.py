@@ -13,7 +13,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["pk_api.cu", "pk_noalloc.cu", "pk_exchange.cpp", "pk_levels.cpp", "pk_phys_hd1.cu", "pk_phys_hd2.cu", "pk_phys_mhd1.cu", "pk_phys_mhd2.cu", "pk_phys_mhd3.cu"]
+UNITS = ["pk_api.cu", "pk_noalloc.cu", "pk_peak.cu", "pk_exchange.cpp", "pk_levels.cpp", "pk_phys_hd1.cu", "pk_phys_hd2.cu", "pk_phys_mhd1.cu", "pk_phys_mhd2.cu", "pk_phys_mhd3.cu"]
 HEADERS = ["pk_device.cuh", "pk_kernels.cuh", "pk_aux.cuh", "pk_internal.h", "pk_launch.cuh", "pk_adjoint.cuh", "pk_levels.h",
            "pk_adjoint_kernels.cuh", "pk_exchange.h"]
 DEPS = [os.path.join(CSRC, f) for f in UNITS + HEADERS]

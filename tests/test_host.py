@@ -108,7 +108,7 @@ def test_orszag_tang_ic():
 
 def _header_symbols():
     text = open(os.path.join(ROOT, "include", "piernik_b200.h")).read()
-    return sorted(set(re.findall(r"\b(pk_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(pk_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_header_symbols_listed():
