@@ -30,12 +30,15 @@ def variants() -> List[Tuple[int, int]]:
 
 def candidates(n_dir: int, n_ortho: int) -> Iterable[Tuple[int, int, int]]:
     """(P, L, variant) tiles: chunks of L owned cells with a 4-cell halo, and the
-    whole pencil without halo (L = n_dir) where it fits the CTA."""
+    whole pencil without halo (L = n_dir) where it fits the CTA.  Besides the
+    fixed lengths, the balanced ones ceil(n_dir / k) split the pencil into k
+    nearly equal chunks, so that no short last chunk runs a full tile."""
+    balanced = {-(-n_dir // k) for k in range(2, 13) if -(-n_dir // k) >= 16}
     for v, (maxt, _) in enumerate(variants()):
-        lengths = sorted(set(min(Lc, n_dir) for Lc in LENGTHS) | ({n_dir} if n_dir <= maxt else set()))
+        lengths = sorted(set(min(Lc, n_dir) for Lc in LENGTHS) | balanced | ({n_dir} if n_dir <= maxt else set()))
         for Lc in lengths:
             T = Lc if (Lc == n_dir and n_dir <= maxt) else Lc + 8
-            for P in (1, 2, 3, 4, 6, 8, 12, 16):
+            for P in (1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16):
                 if P > n_ortho:
                     continue
                 if P * T <= maxt and 2 * P * T > maxt:

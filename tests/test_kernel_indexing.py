@@ -141,8 +141,9 @@ def test_fused_kernel_indexing(n):
     for d in range(3):
         if n[d] <= 1:
             continue
+        balanced = tuple(sorted({-(-n[d] // k) for k in (2, 3, 5, 7) if -(-n[d] // k) >= 8}))
         for maxt in sorted(set(VARIANT_T)):
-            for L in LENGTHS[:6] + (8, 16):
-                for P in (1, 2, 3, 4, 8):
+            for L in LENGTHS[:6] + (8, 16) + balanced:
+                for P in (1, 2, 3, 4, 5, 7, 8):
                     if L + 8 <= maxt:
                         check_fused(n, d, P, L, maxt)
