@@ -250,6 +250,13 @@ int pk_block_place(pk_handle h, int32_t id, const int64_t off[3]);
  * pk_timestep_raw reduces over leaf cells only (timestep.F90:463). */
 int pk_block_place_level(pk_handle h, int32_t id, int32_t level, const int64_t off[3]);
 
+/* restrict_to_base (cg_level_connected.F90:1395-1409, restrict_1var
+ * :1480-1721): every cell covered by a finer block takes the mean of its
+ * 2**eff_dim children (u, B and psi), finest level first, as the reference
+ * does before writing output or regridding; guard cells are not touched.
+ * Synchronous.  No effect on a domain with one level. */
+int pk_restrict(pk_handle h);
+
 /* ---- Domains spanning ranks (one process per GPU) ----
  * The reference exchanges guard cells between MPI ranks in the same
  * internal_boundaries pass (cg_list_bnd.F90:251-324, MPI isend/irecv of the

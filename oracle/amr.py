@@ -272,6 +272,56 @@ class AmrOracle:
                         Y[kz] = i2(X[-1], X[0], X[1], par[1]) if self.has[1] else X[0]
                     fa[dst] = i2(Y[-1], Y[0], Y[1], par[2]) if self.has[2] else Y[0]
 
+    # ---- restriction (restrict_to_base) ---------------------------------
+    def restrict(self):
+        """Every coarse cell covered by a finer block takes the mean of its
+        children, finest level first (cg_level_connected.F90:1395-1409,
+        1480-1721): in 3D the eight children summed x fastest, then scaled
+        once; otherwise each child scaled and accumulated from 0 in z, y, x
+        order; the coarse cell becomes 0 + that."""
+        norm = 1.0 / 2.0 ** self.eff_dim
+        full3 = self.eff_dim == 3
+        for L in range(self.maxl, 0, -1):
+            for fi, lf in enumerate(self.level):
+                if lf != L:
+                    continue
+                F = self.blocks[fi]
+                sf = F.setup
+                lo = [self.off[fi][d] // 2 if self.has[d] else 0 for d in range(3)]
+                hi = [(self.off[fi][d] + sf.n[d]) // 2 if self.has[d] else 1 for d in range(3)]
+                for ci, lc in enumerate(self.level):
+                    if lc != L - 1:
+                        continue
+                    Cb = self.blocks[ci]
+                    sc = Cb.setup
+                    a = [max(lo[d], self.off[ci][d]) for d in range(3)]
+                    e = [min(hi[d], self.off[ci][d] + sc.n[d]) for d in range(3)]
+                    if any(a[d] >= e[d] for d in range(3)):
+                        continue
+                    cs = tuple(slice(a[d] - self.off[ci][d] + sc.guards[d], e[d] - self.off[ci][d] + sc.guards[d])
+                               for d in (2, 1, 0))
+                    f0 = [2 * a[d] - self.off[fi][d] + sf.guards[d] if self.has[d] else 0 for d in range(3)]
+                    cnt = [e[d] - a[d] for d in range(3)]
+
+                    def child(arr, dx, dy, dz):
+                        return arr[f0[2] + dz:f0[2] + dz + 2 * cnt[2]:2 if self.has[2] else 1,
+                                   f0[1] + dy:f0[1] + dy + 2 * cnt[1]:2 if self.has[1] else 1,
+                                   f0[0] + dx:f0[0] + dx + 2 * cnt[0]:2 if self.has[0] else 1]
+
+                    pairs = [(Cb.u, F.u)] + ([(Cb.b, F.b), (Cb.psi, F.psi)] if self.mag else [])
+                    for cA, fA in pairs:
+                        if full3:
+                            val = (((((((child(fA, 0, 0, 0) + child(fA, 1, 0, 0)) + child(fA, 0, 1, 0))
+                                      + child(fA, 1, 1, 0)) + child(fA, 0, 0, 1)) + child(fA, 1, 0, 1))
+                                    + child(fA, 0, 1, 1)) + child(fA, 1, 1, 1)) * norm
+                        else:
+                            val = np.zeros_like(cA[cs])
+                            for dz in range(2 if self.has[2] else 1):
+                                for dy in range(2 if self.has[1] else 1):
+                                    for dx in range(2 if self.has[0] else 1):
+                                        val = val + child(fA, dx, dy, dz) * norm
+                        cA[cs] = 0.0 + val
+
     # ---- the main loop ---------------------------------------------------
     def sweep(self, d, dt, ch):
         lib = O.lib()

@@ -187,6 +187,12 @@ void free_segs(pk_ctx* h)
 
 void free_levels(pk_ctx* h)
 {
+    cudaFree(h->d_rbox);
+    cudaFree(h->d_rbox_start);
+    h->d_rbox = nullptr;
+    h->d_rbox_start = nullptr;
+    h->rbox_beg.clear();
+    h->rbox_cells.clear();
     cudaFree(h->d_runs);
     cudaFree(h->d_run_start);
     h->d_runs = nullptr;
@@ -312,6 +318,33 @@ int levels_prepare(pk_ctx* h)
         if (!plan.leaf[i].empty())
             if (int rc = upload_vec(h, plan.leaf[i], &b.leaf)) return rc;
     }
+    // restriction targets, start counts relative to each fine level's first box
+    std::vector<RBoxDev> rb(plan.rboxes.size());
+    std::vector<long long> rstart(plan.rboxes.size());
+    h->rbox_beg.assign(plan.rbox_level_beg.begin(), plan.rbox_level_beg.end());
+    h->rbox_cells.assign(plan.max_level + 1, 0);
+    for (int L = 1; L <= plan.max_level; ++L) {
+        long long acc = 0;
+        for (int r = plan.rbox_level_beg[L]; r < plan.rbox_level_beg[L + 1]; ++r) {
+            const RBox& s = plan.rboxes[r];
+            RBoxDev& d = rb[r];
+            d.fb = s.fb;
+            d.cb = s.cb;
+            long long cells = 1;
+            for (int k = 0; k < 3; ++k) {
+                d.lo[k] = s.lo[k];
+                d.hi[k] = s.hi[k];
+                d.flo[k] = s.flo[k];
+                cells *= s.hi[k] - s.lo[k];
+            }
+            rstart[r] = acc;
+            acc += cells;
+        }
+        h->rbox_cells[L] = acc;
+    }
+    if (int rc = upload_vec(h, rb, &h->d_rbox)) return rc;
+    if (int rc = upload_vec(h, rstart, &h->d_rbox_start)) return rc;
+    h->eff_dim = plan.eff_dim;
     h->fc_scale = 1.0 / std::ldexp(1.0, plan.eff_dim - 1);
     h->max_level = plan.max_level;
     h->batch_dirty = true;
@@ -2129,6 +2162,25 @@ int pk_grad_backward(pk_handle h)
                 std::swap(h->lam, h->lam_tmp);
             }
         }
+    }
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_restrict(pk_handle h)
+{
+    if (!h) return PK_E_ARG;
+    if (int rc = exchange_prepare(h)) return rc;
+    for (int L = h->max_level; L >= 1; --L) {         // restrict_to_base: finest level first
+        const long long cells = h->rbox_cells[L];
+        if (!cells) continue;
+        const int r0 = h->rbox_beg[L], nr = h->rbox_beg[L + 1] - r0;
+        k_restrict<<<grid1d(cells, 256), 256, 0, h->stream>>>(h->d_rbox + r0, h->d_rbox_start + r0, nr, cells,
+                                                               h->d_xptr[h->cur], h->nplanes, h->dom[0] > 1,
+                                                               h->dom[1] > 1, h->dom[2] > 1,
+                                                               1.0 / std::ldexp(1.0, h->eff_dim));
+        PK_CUDA(h, cudaGetLastError());
+        h->launches += 1;
     }
     PK_CUDA(h, cudaStreamSynchronize(h->stream));
     return PK_OK;

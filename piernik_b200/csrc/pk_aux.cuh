@@ -523,4 +523,58 @@ __global__ void k_unsplit_apply(BoxGeom b, const double* S, double* T,
     flush_status(status, gstatus);
 }
 
+struct RBoxDev {
+    int fb, cb;
+    int lo[3], hi[3], flo[3];
+};
+
+// restrict (cg_level_connected.F90:1480-1721) of one level into the next
+// coarser one: each covered coarse cell takes the mean of its children, every
+// plane.  With three directions the eight children are summed x fastest and
+// scaled once (the even-offset array form, :1566-1590); with fewer, each
+// child is scaled and accumulated from 0 in z, y, x loop order (:1613-1631).
+// The coarse cell then becomes 0 + that (:1654-1680).
+static __global__ void k_restrict(const RBoxDev* __restrict__ boxes, const long long* __restrict__ start, int nbox,
+                                  long long total, const XPtr* __restrict__ blocks, int nplanes, int has_x, int has_y,
+                                  int has_z, double norm)
+{
+    const bool full3 = has_x && has_y && has_z;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nbox - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const RBoxDev bx = boxes[lo];
+        long long r = t - start[lo];
+        const int nx = bx.hi[0] - bx.lo[0], ny = bx.hi[1] - bx.lo[1];
+        const int i = (int)(r % nx);
+        r /= nx;
+        const int j = (int)(r % ny);
+        const int k = (int)(r / ny);
+        const XPtr C = blocks[bx.cb], F = blocks[bx.fb];
+        const long long co = ((long long)(bx.lo[2] + k) * C.ext[1] + (bx.lo[1] + j)) * C.ext[0] + (bx.lo[0] + i);
+        const int fx = bx.flo[0] + (has_x ? 2 * i : 0), fy = bx.flo[1] + (has_y ? 2 * j : 0),
+                  fz = bx.flo[2] + (has_z ? 2 * k : 0);
+        const long long sx = 1, sy = F.ext[0], sz = (long long)F.ext[0] * F.ext[1];
+        const long long fo = fz * sz + fy * sy + fx;
+        for (int v = 0; v < nplanes; ++v) {
+            const double* f = F.u + (long long)v * F.plane + fo;
+            double val;
+            if (full3) {
+                val = (((((((f[0] + f[sx]) + f[sy]) + f[sx + sy]) + f[sz]) + f[sx + sz]) + f[sy + sz]) + f[sx + sy + sz]) *
+                      norm;
+            } else {
+                double acc = 0.0;
+                for (int kz = 0; kz <= has_z; ++kz)
+                    for (int jy = 0; jy <= has_y; ++jy)
+                        for (int ix = 0; ix <= has_x; ++ix) acc = acc + f[kz * sz + jy * sy + ix * sx] * norm;
+                val = acc;
+            }
+            C.u[(long long)v * C.plane + co] = 0.0 + val;
+        }
+    }
+}
+
 }  // namespace pk

@@ -292,10 +292,13 @@ bool build_levels(const std::vector<LBlock>& blocks, const long long dom[3], Lev
     }
 
     // leaf cells: paint each refined block's coarse shadow into the next coarser level
+    // (the same intersections are the restriction targets)
     plan.leaf.assign(nb, {});
     plan.leaf_cells.assign(nb, 0);
+    plan.rbox_level_beg.assign(maxl + 2, 0);
     for (int i = 0; i < nb; ++i) plan.leaf_cells[i] = (long long)blocks[i].n[0] * blocks[i].n[1] * blocks[i].n[2];
-    for (int L = 1; L <= maxl; ++L)
+    for (int L = 1; L <= maxl; ++L) {
+        plan.rbox_level_beg[L] = (int)plan.rboxes.size();
         for (int fi : of_level[L]) {
             const LBlock& f = blocks[fi];
             long long lo[3], hi[3];
@@ -313,6 +316,15 @@ bool build_levels(const std::vector<LBlock>& blocks, const long long dom[3], Lev
                     ov = ov && a[d] < e[d];
                 }
                 if (!ov) continue;
+                RBox rb;
+                rb.fb = fi;
+                rb.cb = ci;
+                for (int d = 0; d < 3; ++d) {
+                    rb.lo[d] = (int)(a[d] - c.off[d]) + c.g[d];
+                    rb.hi[d] = (int)(e[d] - c.off[d]) + c.g[d];
+                    rb.flo[d] = has[d] ? (int)(2 * a[d] - f.off[d]) + f.g[d] : 0;
+                }
+                plan.rboxes.push_back(rb);
                 std::vector<unsigned char>& m = plan.leaf[ci];
                 if (m.empty()) m.assign((size_t)c.n[0] * c.n[1] * c.n[2], 1);
                 for (long long z = a[2]; z < e[2]; ++z)
@@ -326,6 +338,8 @@ bool build_levels(const std::vector<LBlock>& blocks, const long long dom[3], Lev
                         }
             }
         }
+    }
+    plan.rbox_level_beg[maxl + 1] = (int)plan.rboxes.size();
     return true;
 }
 

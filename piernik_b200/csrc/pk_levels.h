@@ -56,6 +56,14 @@ struct FcDir {
     int n_out = 0;
 };
 
+// Coarse cells [lo, hi) (coarse block cb's storage coordinates) covered by
+// fine block fb: the targets of restriction (cg_level_connected.F90:1480-1721)
+struct RBox {
+    int fb, cb;
+    int lo[3], hi[3];
+    int flo[3];          // fine block fb's storage cell of the first child of lo
+};
+
 struct LevelPlan {
     int max_level = 0;
     int eff_dim = 0;
@@ -64,6 +72,8 @@ struct LevelPlan {
     FcDir fc[3];
     std::vector<std::vector<unsigned char>> leaf;   // per block: interior leaf mask (1 = leaf) or empty (all leaf)
     std::vector<long long> leaf_cells;              // per block: number of leaf cells
+    std::vector<RBox> rboxes;                       // restriction targets, by the fine block's level
+    std::vector<int> rbox_level_beg;                // boxes of fine level L: [rbox_level_beg[L], rbox_level_beg[L+1])
 };
 
 // dom: base-level cells per direction (1 where the domain has no extent);

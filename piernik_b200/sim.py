@@ -259,6 +259,11 @@ class Simulation:
         p = (C.c_int32 * 3)(*[int(bool(x)) for x in periodic])
         self._chk(self.lib.pk_set_domain(self.h, n, p), "pk_set_domain")
 
+    def restrict(self) -> None:
+        """Covered coarse cells take the mean of their children, finest level
+        first (restrict_to_base)."""
+        self._chk(self.lib.pk_restrict(self.h), "pk_restrict")
+
     def place_block(self, block: int, off, level: int = 0) -> None:
         """Put the block's first interior cell at ``off`` on the grid of its
         refinement level (the base grid refined ``level`` times)."""

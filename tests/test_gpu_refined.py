@@ -118,3 +118,17 @@ def test_refined_conserves_on_gpu(gpu_lib):
         ob.u[...], ob.b[...], ob.psi[...] = sim.download(block=i)
     assert np.all(np.abs(amr.leaf_totals(a) - t0) <= 1e-12 * scale)
     sim.close()
+
+
+@pytest.mark.parametrize("dom,reg", [(DOM3, REG3), (DOM2, REG2)])
+def test_refined_restriction_matches_oracle(gpu_lib, dom, reg):
+    blocks = case("mhd", dom, reg)
+    a = amr.AmrOracle(dom, blocks)
+    a.fill_guards()
+    sim = library(dom, blocks)
+    a.run(2)
+    sim.run(2)
+    a.restrict()
+    sim.restrict()
+    compare(sim, a, "after restriction")
+    sim.close()

@@ -172,3 +172,32 @@ def test_planner_rejects(hlib):
     hole = [(s.replace(n=(16, 16, 8)), 0, (0, 0, 0))]
     with pytest.raises(ValueError, match="cover"):
         build(hlib, hole, (16, 16, 16))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_refined_oracle_restriction_matches_leaves(oracle_lib, dim):
+    """After restriction every covered coarse cell is the mean of its
+    children, so the base level alone holds the leaf totals (to round-off),
+    after steps that made the levels drift apart."""
+    dom, reg = (DOM3, REG3) if dim == 3 else (DOM2, REG2)
+    a = amr.AmrOracle(dom, case("mhd", dom, reg))
+    a.fill_guards()
+    a.run(2)
+    leaf = amr.leaf_totals(a)
+    scale = amr.leaf_totals(a, absolute=True)
+
+    def base_totals():
+        t = None
+        for i, ob in enumerate(a.blocks):
+            if a.level[i]:
+                continue
+            s = ob.setup
+            g, n = s.guards, s.n
+            sl = (slice(g[2], g[2] + n[2]), slice(g[1], g[1] + n[1]), slice(g[0], g[0] + n[0]))
+            vol = float(np.prod([s.dl[d] for d in range(3) if a.has[d]]))
+            x = np.concatenate([ob.u[sl].reshape(-1, s.nvar).sum(0), ob.b[sl].reshape(-1, 3).sum(0)]) * vol
+            t = x if t is None else t + x
+        return t
+    assert np.max(np.abs(base_totals() - leaf) / scale) > 1e-10      # drifted before
+    a.restrict()
+    assert np.all(np.abs(base_totals() - leaf) <= 1e-12 * scale)
