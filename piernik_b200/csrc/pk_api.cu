@@ -752,7 +752,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
                 for (auto& b : h->blocks) {
                     if (b.n[dir] <= 1 || b.level != L) continue;
                     if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
-                    if (b.ext[dir] > STAGE_MAXT)
+                    if (stage_chunked(b, dir))
                         if (int rc = ensure_pingpong(h)) return rc;
                     if (int rc = ops->stage(h, b, dir, s == 1, rk)) return rc;
                 }
@@ -1153,7 +1153,7 @@ int pk_solve_cg(pk_handle h, int32_t id, int32_t ddim, int32_t istep, double dt,
     if (b->guards_stale)
         if (int rc = fill_guards_block(h, *b)) return rc;
     if (!b->uh) PK_CUDA(h, cudaMalloc(&b->uh, sizeof(double) * h->nplanes * b->plane));
-    if (b->ext[dir] > STAGE_MAXT)
+    if (stage_chunked(*b, dir))
         if (int rc = ensure_pingpong(h)) return rc;
     if (int rc = put_step_params(h, dt, chspeed, 1.0)) return rc;   // rk_coef(istep) * dt / cg%dl(ddim) on the device
     return ops_of(h)->stage(h, *b, dir, first, rk);

@@ -48,6 +48,16 @@ struct Block {
     double* flux[3] = {nullptr, nullptr, nullptr};   // unsplit scheme: face fluxes per direction
 };
 
+// the per-block stage kernel sweeps whole pencils in place where they fit
+// the CTA (for y and z sweeps only when four or more neighbouring pencils
+// share it, so that the loads stay coalesced), else chunks with a 2-cell halo
+// out of place into the ping-pong buffer
+inline bool stage_chunked(const Block& b, int dir)
+{
+    const int ext = b.ext[dir], n1 = b.n[dir == 0 ? 1 : 0];
+    return !(ext <= STAGE_MAXT && (dir == 0 || STAGE_MAXT / ext >= 4 || n1 < 4));
+}
+
 struct pk_dir_tile { int P, L, V; };
 
 // scalars of one recorded step of the differentiable path

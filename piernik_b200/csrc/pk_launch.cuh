@@ -334,7 +334,7 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double rk)
     const int ext = b.ext[dir];
     double* u = b.buf[h->cur];
     double* uout = u;
-    if (ext <= STAGE_MAXT) {                 // whole pencil per tile: in place
+    if (!stage_chunked(b, dir)) {            // whole pencils per tile: in place
         int P = STAGE_MAXT / ext;
         if (P >= 4) P -= P % 4;
         if (P > g.n1) P = g.n1;
@@ -411,7 +411,10 @@ int launch_unsplit_flux(pk_ctx* h, Block& b, int dir, const double* in, double* 
     Geom g = make_geom(b, dir);
     Tile tl;
     const int ext = b.ext[dir];
-    if (ext <= STAGE_MAXT) {
+    // whole pencils where they fit; across x (y and z sweeps) only when four or
+    // more neighbouring pencils share the CTA, so that the loads stay coalesced,
+    // else chunks of 64 cells with a 2-cell halo
+    if (ext <= STAGE_MAXT && (dir == 0 || STAGE_MAXT / ext >= 4 || g.n1 < 4)) {
         int P = STAGE_MAXT / ext;
         if (P >= 4) P -= P % 4;
         if (P > g.n1) P = g.n1;

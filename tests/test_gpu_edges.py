@@ -54,3 +54,13 @@ def test_two_fluids_weno3(gpu_lib, oracle_lib):
     differ between host and device)."""
     s = setup_for("mhd", n=(12, 10, 8), lim="weno3").replace(fluids=[("ion", 5.0 / 3.0), ("neu", 1.4)])
     run_both(s, 3, seed=1, smooth=True)
+
+
+@pytest.mark.parametrize("n", [(8, 100, 6), (6, 8, 90)])
+def test_stage_path_chunked_y_z(gpu_lib, oracle_lib, n):
+    """Outflow boundaries take the stage path; y and z pencils longer than 80
+    cells run there in chunks with a 2-cell halo (fewer than four whole
+    pencils would fit a CTA)."""
+    from piernik_b200.config import BND_OUT
+    s = setup_for("hd", n=n, lim="moncen").replace(bnd=((BND_OUT, BND_OUT),) * 3)
+    run_both(s, 2, seed=8, smooth=True)

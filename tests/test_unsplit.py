@@ -61,7 +61,8 @@ def test_unsplit_one_dt_per_step_and_end_clamp(oracle_lib):
 
 # ---- GPU parity --------------------------------------------------------------
 CASES = [("hd", (16, 12, 10), "vanleer"), ("mhd", (16, 12, 10), "moncen"), ("mhd", (16, 12, 1), "vanleer"),
-         ("mhd", (16, 12, 10), "weno3"), ("hd", (12, 10, 8), "minmod")]
+         ("mhd", (16, 12, 10), "weno3"), ("hd", (12, 10, 8), "minmod"),
+         ("mhd", (8, 100, 6), "vanleer")]          # y pencils in chunks (fewer than 4 whole ones fit a CTA)
 
 
 @pytest.mark.gpu
