@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PK_ABI_VERSION 3
+#define PK_ABI_VERSION 4
 
 enum {
     PK_OK = 0,
@@ -82,6 +82,13 @@ typedef struct pk_config {
     /* solver_str (global.F90:423-437): PK_SOLVER_SPLIT (RIEMANN_SPLIT) or
      * PK_SOLVER_UNSPLIT (RIEMANN_UNSPLIT, src/scheme/unsplit_schemes) */
     int32_t solver;
+    /* ord_fluid_prolong, ord_mag_prolong (global.F90:113-114, defaults O_INJ
+     * and O_I2 :259-260): the reference's prolongation orders of refined
+     * domains' guard cells, PK_O_* (0 injection, 1 linear, 2..6 integral,
+     * -2..-6 direct); fluids accept injection or linear only (others degrade
+     * to injection, global.F90:561-566); 2 x the stencil range (0 for
+     * injection, 1 for orders +-1..2, 2 for 3..4, 3 for 5..6) must not exceed nb */
+    int32_t ord_fluid_prolong, ord_mag_prolong;
 } pk_config;
 
 #define PK_SOLVER_SPLIT   0

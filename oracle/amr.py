@@ -32,6 +32,23 @@ import numpy as np
 
 import oracle as O
 
+# the directional prolongation stencils (grid_container_prolong.F90:223-287):
+# order -> ([P_3, P_2, P_1, P0, P1, P2, P3], stencil range)
+PROLONG = {
+    -6: ([-231 / 65536, 2002 / 65536, -9009 / 65536, 60060 / 65536, 15015 / 65536, -2574 / 65536, 273 / 65536], 3),
+    -5: ([0.0, 77 / 8192, -693 / 8192, 6930 / 8192, 2310 / 8192, -495 / 8192, 63 / 8192], 3),
+    -4: ([0.0, 35 / 2048, -252 / 2048, 1890 / 2048, 420 / 2048, -45 / 2048, 0.0], 2),
+    -3: ([0.0, 0.0, -7 / 128, 105 / 128, 35 / 128, -5 / 128, 0.0], 2),
+    -2: ([0.0, 0.0, -3 / 32, 30 / 32, 5 / 32, 0.0, 0.0], 1),
+    1: ([0.0, 0.0, 0.0, 3 / 4, 1 / 4, 0.0, 0.0], 1),
+    0: ([0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0], 0),
+    2: ([0.0, 0.0, -1 / 8, 1.0, 1 / 8, 0.0, 0.0], 1),
+    3: ([0.0, 0.0, -5 / 64, 55 / 64, 17 / 64, -3 / 64, 0.0], 2),
+    4: ([0.0, 3 / 128, -11 / 64, 1.0, 11 / 64, -3 / 128, 0.0], 2),
+    5: ([0.0, 7 / 512, -63 / 512, 462 / 512, 138 / 512, -37 / 512, 5 / 512], 3),
+    6: ([-5 / 1024, 44 / 1024, -201 / 1024, 1.0, 201 / 1024, -44 / 1024, 5 / 1024], 3),
+}
+
 RO1 = (1, 2, 0)     # pdims ORTHO1 of x, y, z (constants.F90:127-128)
 RO2 = (2, 0, 1)
 
@@ -244,33 +261,49 @@ class AmrOracle:
             if self.mag:
                 A.b[dst] = B.b[src]
                 A.psi[dst] = B.psi[src]
-        P1, P0, P_1 = 1.0 / 8.0, 1.0, -1.0 / 8.0
+        s0 = self.setup0
+        ofl = s0.ord_fluid_prolong if s0.ord_fluid_prolong in (0, 1) else 0
+        ku, kb = PROLONG[ofl], PROLONG[s0.ord_mag_prolong]
 
-        def i2(cm, c0, cp, par):
-            return np.where(par == 0, (P1 * cm + P0 * c0) + P_1 * cp, (P_1 * cm + P0 * c0) + P1 * cp)
+        def pro1(k, get, par):
+            """sum over m = -r..r of P(-m) c(m) (left child) or P(m) c(m), left to right"""
+            P, r = k
+            if r == 0:
+                return get(0)
+            acc = None
+            for m in range(-r, r + 1):
+                t = np.where(par == 0, P[3 - m], P[3 + m]) * get(m)
+                acc = t if acc is None else acc + t
+            return acc
+
+        def pro3(k, fb, cs, par):
+            r = k[1]
+            ry = r if self.has[1] else 0
+            rz = r if self.has[2] else 0
+            Y = {}
+            for kz in range(-rz, rz + 1):
+                X = {}
+                for ky in range(-ry, ry + 1):
+                    row = lambda kx, ky=ky, kz=kz: fb[cs[2] + kz, cs[1] + ky, cs[0] + kx]
+                    X[ky] = pro1(k, row, par[0]) if self.has[0] else row(0)
+                Y[kz] = pro1(k, lambda m: X[m], par[1]) if self.has[1] else X[0]
+            return pro1(k, lambda m: Y[m], par[2]) if self.has[2] else Y[0]
 
         for L in range(1, self.maxl + 1):
             for lev, i, dst, j, cs, par in self.prolong:
                 if lev != L:
                     continue
                 A, B = self.blocks[i], self.blocks[j]
-                A.u[dst] = B.u[cs[2], cs[1], cs[0]]
+                if ku[1] == 0:
+                    A.u[dst] = B.u[cs[2], cs[1], cs[0]]
+                else:
+                    for v in range(A.u.shape[-1]):
+                        A.u[dst + (v,)] = pro3(ku, B.u[..., v], cs, par)
                 if not self.mag:
                     continue
                 fields = [(A.b[..., c], B.b[..., c]) for c in range(3)] + [(A.psi, B.psi)]
                 for fa, fb in fields:
-                    Y = {}
-                    for kz in (-1, 0, 1):
-                        if not self.has[2] and kz:
-                            continue
-                        X = {}
-                        for ky in (-1, 0, 1):
-                            if not self.has[1] and ky:
-                                continue
-                            row = lambda kx: fb[cs[2] + kz, cs[1] + ky, cs[0] + kx]
-                            X[ky] = i2(row(-1), row(0), row(1), par[0]) if self.has[0] else row(0)
-                        Y[kz] = i2(X[-1], X[0], X[1], par[1]) if self.has[1] else X[0]
-                    fa[dst] = i2(Y[-1], Y[0], Y[1], par[2]) if self.has[2] else Y[0]
+                    fa[dst] = pro3(kb, fb, cs, par)
 
     # ---- restriction (restrict_to_base) ---------------------------------
     def restrict(self):

@@ -72,6 +72,8 @@ class PkConfig(C.Structure):
         ("interpolation", C.c_int32),
         ("w_epsilon", C.c_double),
         ("solver", C.c_int32),
+        ("ord_fluid_prolong", C.c_int32),
+        ("ord_mag_prolong", C.c_int32),
     ]
 
 

@@ -54,6 +54,8 @@ class Setup:
     interpolation: str = "linear"    # interpol_str (:220): linear or weno3
     w_epsilon: float = 1.0e-10       # :255
     solver: str = "split"            # solver_str (:423-437): split (RIEMANN_SPLIT) or unsplit (RIEMANN_UNSPLIT)
+    ord_fluid_prolong: int = 0       # :260 O_INJ (refined domains' guard cells; 0 or 1, others degrade to 0)
+    ord_mag_prolong: int = 2         # :259 O_I2 (-6..6 but -1: the orders of grid_container_prolong.F90)
     skip_sweep: Tuple[bool, bool, bool] = (False, False, False)
     # END_CONTROL
     tend: float = DBL_HUGE
@@ -86,6 +88,8 @@ class Setup:
             raise ValueError("CFL value should be >0. and <=1.")      # global.F90:303
         if self.integration_order not in (1, 2):
             raise ValueError("integration_order must be 1 or 2")
+        if self.ord_mag_prolong not in (-6, -5, -4, -3, -2, 0, 1, 2, 3, 4, 5, 6):
+            raise ValueError(f"ord_mag_prolong {self.ord_mag_prolong}: unknown prolongation order")
         if self.solver not in ("split", "unsplit"):
             raise ValueError(f"solver {self.solver!r}: this library implements split and unsplit")
         if self.interpolation not in ("linear", "weno3"):

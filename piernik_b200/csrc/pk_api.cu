@@ -351,6 +351,38 @@ int levels_prepare(pk_ctx* h)
     return PK_OK;
 }
 
+// The directional stencil of a prolongation order (grid_container_prolong.F90:
+// 223-287 select case (ord_prolong)): P_3..P3 and the stencil range; every
+// coefficient is a dyadic fraction, exact in binary64.  false: unknown order.
+bool prolong_coef(int order, ProlongCoef* k)
+{
+    double P[7] = {0, 0, 0, 0, 0, 0, 0};      // P_3, P_2, P_1, P0, P1, P2, P3
+    int r;
+    switch (order) {
+    case -6: P[0] = -231.0 / 65536; P[1] = 2002.0 / 65536; P[2] = -9009.0 / 65536; P[3] = 60060.0 / 65536;
+             P[4] = 15015.0 / 65536; P[5] = -2574.0 / 65536; P[6] = 273.0 / 65536; r = 3; break;
+    case -5: P[1] = 77.0 / 8192; P[2] = -693.0 / 8192; P[3] = 6930.0 / 8192; P[4] = 2310.0 / 8192;
+             P[5] = -495.0 / 8192; P[6] = 63.0 / 8192; r = 3; break;
+    case -4: P[1] = 35.0 / 2048; P[2] = -252.0 / 2048; P[3] = 1890.0 / 2048; P[4] = 420.0 / 2048;
+             P[5] = -45.0 / 2048; r = 2; break;
+    case -3: P[2] = -7.0 / 128; P[3] = 105.0 / 128; P[4] = 35.0 / 128; P[5] = -5.0 / 128; r = 2; break;
+    case -2: P[2] = -3.0 / 32; P[3] = 30.0 / 32; P[4] = 5.0 / 32; r = 1; break;
+    case 1: P[3] = 3.0 / 4; P[4] = 1.0 / 4; r = 1; break;                      // O_LIN
+    case 0: P[3] = 1.0; r = 0; break;                                         // O_INJ
+    case 2: P[2] = -1.0 / 8; P[3] = 1.0; P[4] = 1.0 / 8; r = 1; break;
+    case 3: P[2] = -5.0 / 64; P[3] = 55.0 / 64; P[4] = 17.0 / 64; P[5] = -3.0 / 64; r = 2; break;
+    case 4: P[1] = 3.0 / 128; P[2] = -11.0 / 64; P[3] = 1.0; P[4] = 11.0 / 64; P[5] = -3.0 / 128; r = 2; break;
+    case 5: P[1] = 7.0 / 512; P[2] = -63.0 / 512; P[3] = 462.0 / 512; P[4] = 138.0 / 512; P[5] = -37.0 / 512;
+            P[6] = 5.0 / 512; r = 3; break;
+    case 6: P[0] = -5.0 / 1024; P[1] = 44.0 / 1024; P[2] = -201.0 / 1024; P[3] = 1.0; P[4] = 201.0 / 1024;
+            P[5] = -44.0 / 1024; P[6] = 5.0 / 1024; r = 3; break;
+    default: return false;
+    }
+    for (int i = 0; i < 7; ++i) k->p[i] = P[i];
+    k->r = r;
+    return true;
+}
+
 // prolong_bnd_from_coarser of every refined level, coarsest first
 int prolong_guards(pk_ctx* h)
 {
@@ -361,7 +393,8 @@ int prolong_guards(pk_ctx* h)
         const int nr = (int)(h->run_beg[L + 1] - r0);
         k_prolong<<<grid1d(cells, 256), 256, 0, h->stream>>>(h->d_runs + r0, h->d_run_start + r0, nr, cells,
                                                              h->d_xptr[h->cur], h->nvf, h->cfg.magnetic ? 4 : 0,
-                                                             h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1);
+                                                             h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1, h->pro_u,
+                                                             h->pro_b);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
@@ -896,6 +929,8 @@ void pk_config_default(pk_config* c)
     c->max_redostep_attempts = 10;     // :258
     c->interpolation = PK_INTERP_LINEAR;   // :220
     c->solver = PK_SOLVER_SPLIT;          // :423-437
+    c->ord_fluid_prolong = 0;             // O_INJ (:260)
+    c->ord_mag_prolong = 2;               // O_I2 (:259)
     c->w_epsilon = 1.0e-10;            // :255
 }
 
@@ -924,9 +959,18 @@ int pk_create(const pk_config* cfg, pk_handle* out)
     else if (c.magnetic && c.fluid_kind[0] == PK_FLUID_ION && nen == 2 && ndst == 0) phys = 3;
     else if (c.magnetic && c.fluid_kind[0] == PK_FLUID_ION && nen == 2 && ndst == 1) phys = 4;
     else return PK_E_UNSUPPORTED;
+    // prolongation orders of refined domains (cg_list_global.F90:195-207,
+    // global.F90:561-566: fluids other than injection / linear degrade to injection)
+    ProlongCoef pro_u, pro_b;
+    const int ofl = (c.ord_fluid_prolong == 0 || c.ord_fluid_prolong == 1) ? c.ord_fluid_prolong : 0;
+    if (!prolong_coef(ofl, &pro_u) || !prolong_coef(c.ord_mag_prolong, &pro_b)) return PK_E_ARG;
+    if (2 * pro_u.r > c.nb || (c.magnetic && 2 * pro_b.r > c.nb)) return PK_E_ARG;
 
     pk_ctx* h = new pk_ctx();
     h->cfg = c;
+    h->cfg.ord_fluid_prolong = ofl;
+    h->pro_u = pro_u;
+    h->pro_b = pro_b;
     h->phys = phys;
     int nvf = 0;
     for (int f = 0; f < c.nfluids; ++f) {

@@ -394,24 +394,52 @@ struct PRunDev {
     int px, py, pz;
 };
 
-// one centred O_I2 interpolation along a direction (grid_container_prolong.F90,
-// O_I2 coefficients P_1 = -1/8, P0 = 1, P1 = 1/8): the left child takes
-// P1 c(-1) + P0 c(0) + P_1 c(+1), the right child P_1 c(-1) + P0 c(0) + P1 c(+1),
-// summed left to right
-PK_DEV double prolong_i2(double cm, double c0, double cp, int par)
+// The directional stencil of one prolongation order
+// (grid_container_prolong.F90:180-453): coefficients P_3..P3 in p[0..6] and
+// the stencil range r (0: injection).
+struct ProlongCoef {
+    double p[7];
+    int r;
+};
+
+// one centred interpolation along a direction: the left child (par 0) takes
+// sum over m = -r..r of P(-m) c(m), the right child sum of P(m) c(m), added
+// left to right in increasing m; c points at the parent, s is the stride
+PK_DEV double prolong_1d(const ProlongCoef& k, const double* c, long long s, int par)
 {
-    const double P1 = 1.0 / 8.0, P0 = 1.0, P_1 = -1.0 / 8.0;
-    return par == 0 ? (P1 * cm + P0 * c0) + P_1 * cp : (P_1 * cm + P0 * c0) + P1 * cp;
+    if (k.r == 0) return c[0];
+    double acc = 0.0;
+    for (int m = -k.r; m <= k.r; ++m) {
+        const double t = k.p[3 + (par == 0 ? -m : m)] * c[m * s];
+        acc = (m == -k.r) ? t : acc + t;
+    }
+    return acc;
 }
 
 // prolong_bnd_from_coarser (cg_level_connected.F90:1150-1359) for the guard
-// cells of one level: u by injection (ord_fluid_prolong = O_INJ), B and psi by
-// the directionally split O_I2 interpolation (ord_mag_prolong, x then y then
-// z over the 3 x 3 x 3 coarse neighbourhood, as prolong() does).  runs has
-// nruns rows; start[r] is the running cell count before run r.
+// cells of one level: the fluid planes with the stencil ku (ord_fluid_prolong),
+// B and psi with kb (ord_mag_prolong), each split by direction as prolong()
+// does: x over the (2r+1)^2 coarse rows around the parent, then y, then z.
+// runs has nruns rows; start[r] is the running cell count before run r.
+PK_DEV double prolong_cell(const ProlongCoef& k, const double* c, long long sx, long long sy, long long sz, int px,
+                           int py, int pz, bool hx, bool hy, bool hz)
+{
+    const int ry = hy ? k.r : 0, rz = hz ? k.r : 0;
+    double Y[7];
+    for (int kz = -rz; kz <= rz; ++kz) {
+        double X[7];
+        for (int ky = -ry; ky <= ry; ++ky) {
+            const double* row = c + ky * sy + kz * sz;
+            X[ky + 3] = hx ? prolong_1d(k, row, sx, px) : row[0];
+        }
+        Y[kz + 3] = hy ? prolong_1d(k, X + 3, 1, py) : X[3];
+    }
+    return hz ? prolong_1d(k, Y + 3, 1, pz) : Y[3];
+}
+
 static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long long* __restrict__ start, int nruns,
                                  long long total, const XPtr* __restrict__ blocks, int nu, int nmag, int has_x,
-                                 int has_y, int has_z)
+                                 int has_y, int has_z, ProlongCoef ku, ProlongCoef kb)
 {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         int lo = 0, hi = nruns - 1;
@@ -427,23 +455,17 @@ static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long lo
         const int cx = r.cx + ((r.px + i) >> 1);
         const long long fo = ((long long)r.fz * F.ext[1] + r.fy) * F.ext[0] + (r.fx + i);
         const long long co = ((long long)r.cz * C.ext[1] + r.cy) * C.ext[0] + cx;
-        copy_planes(F.u + fo, F.plane, C.u + co, C.plane, nu);
         const long long sx = has_x, sy = has_y ? C.ext[0] : 0, sz = has_z ? (long long)C.ext[0] * C.ext[1] : 0;
-        for (int v = nu; v < nu + nmag; ++v) {
-            const double* c = C.u + (long long)v * C.plane + co;
-            double Y[3];
-            for (int kz = -1; kz <= 1; ++kz) {
-                if (!has_z && kz != 0) continue;
-                double X[3];
-                for (int ky = -1; ky <= 1; ++ky) {
-                    if (!has_y && ky != 0) continue;
-                    const double* row = c + ky * sy + kz * sz;
-                    X[ky + 1] = has_x ? prolong_i2(row[-sx], row[0], row[sx], px) : row[0];
-                }
-                Y[kz + 1] = has_y ? prolong_i2(X[0], X[1], X[2], r.py) : X[1];
-            }
-            F.u[(long long)v * F.plane + fo] = has_z ? prolong_i2(Y[0], Y[1], Y[2], r.pz) : Y[1];
+        if (ku.r == 0) {
+            copy_planes(F.u + fo, F.plane, C.u + co, C.plane, nu);   // O_INJ
+        } else {
+            for (int v = 0; v < nu; ++v)
+                F.u[(long long)v * F.plane + fo] = prolong_cell(ku, C.u + (long long)v * C.plane + co, sx, sy, sz, px,
+                                                                r.py, r.pz, has_x, has_y, has_z);
         }
+        for (int v = nu; v < nu + nmag; ++v)
+            F.u[(long long)v * F.plane + fo] = prolong_cell(kb, C.u + (long long)v * C.plane + co, sx, sy, sz, px,
+                                                            r.py, r.pz, has_x, has_y, has_z);
     }
 }
 

@@ -162,6 +162,7 @@ struct pk_ctx {
     const int* d_src[3] = {nullptr, nullptr, nullptr};
     std::vector<int> in_level_beg[3];           // in slots of coarse level L: [in_level_beg[L], in_level_beg[L+1])
     double fc_scale = 1.0;                      // 1 / 2**(eff_dim - 1)
+    pk::ProlongCoef pro_u{}, pro_b{};           // prolongation stencils of the fluids and of B / psi
     pk::RBoxDev* d_rbox = nullptr;              // restriction targets, by fine level
     long long* d_rbox_start = nullptr;          // running cell count of each box within its level
     std::vector<int> rbox_beg;                  // boxes of fine level L: [rbox_beg[L], rbox_beg[L+1])

@@ -184,6 +184,9 @@ def read_problem_par(text: str, cmdline: Optional[str] = None, setup: Optional[S
         kw["interpolation"] = names[val]                  # interpolations.F90:set_interpolations
     if "w_epsilon" in ns:
         kw["w_epsilon"] = float(ns["w_epsilon"])
+    for key in ("ord_fluid_prolong", "ord_mag_prolong"):
+        if key in ns:
+            kw[key] = int(ns[key])
     if "solver_str" in ns:                               # global.F90:423-437
         val = str(ns["solver_str"]).strip().lower()
         if val in ("", "riemann", "riemann_split"):

@@ -71,6 +71,8 @@ def make_config(setup: Setup) -> L.PkConfig:
     c.interpolation = {"linear": 0, "weno3": 1}[setup.interpolation]
     c.w_epsilon = setup.w_epsilon
     c.solver = {"split": 0, "unsplit": 1}[setup.solver]
+    c.ord_fluid_prolong = setup.ord_fluid_prolong
+    c.ord_mag_prolong = setup.ord_mag_prolong
     return c
 
 

@@ -132,3 +132,19 @@ def test_refined_restriction_matches_oracle(gpu_lib, dom, reg):
     sim.restrict()
     compare(sim, a, "after restriction")
     sim.close()
+
+
+@pytest.mark.parametrize("orders,nb", [((0, -2), 4), ((0, 3), 4), ((1, 4), 4), ((0, -3), 4), ((1, -4), 4),
+                                        ((0, 5), 6), ((1, -5), 6), ((0, 6), 6), ((0, -6), 6), ((1, 1), 4)])
+def test_refined_prolongation_orders(gpu_lib, orders, nb):
+    """Every prolongation order of the reference (ord_fluid_prolong,
+    ord_mag_prolong; stencil ranges up to 3 need nb = 6), bit for bit."""
+    blocks = case("mhd", DOM3, REG3, nb=nb, ord_fluid_prolong=orders[0], ord_mag_prolong=orders[1])
+    a = amr.AmrOracle(DOM3, blocks)
+    a.fill_guards()
+    sim = library(DOM3, blocks)
+    compare(sim, a, "after the first boundary update")
+    a.run(2)
+    sim.run(2)
+    compare(sim, a, "after 2 steps")
+    sim.close()
