@@ -129,6 +129,12 @@ int pk_abi_version(void);
  * boundaries are swept by the fused two-stage kernel. */
 int pk_block_add(pk_handle h, const int32_t n[3], const double dl[3], const int32_t bnd[6], int32_t* id_out);
 
+/* Free block id; the ids above it move down by one.  With pk_block_add,
+ * pk_block_place_level, pk_restrict and pk_prolong_block a host regrids a
+ * refined domain (the cg removal of refinement_update.F90 derefinement).
+ * Refused while the differentiable path holds checkpoints. */
+int pk_block_remove(pk_handle h, int32_t id);
+
 /* Copy a block's u (all fluids), b and psi between host and device.
  * b/psi are ignored when the run is not magnetised.  Guard cells come back as
  * the last stage left them; after fused sweeps (which read periodic images and
@@ -263,6 +269,17 @@ int pk_block_place_level(pk_handle h, int32_t id, int32_t level, const int64_t o
  * does before writing output or regridding; guard cells are not touched.
  * Synchronous.  No effect on a domain with one level. */
 int pk_restrict(pk_handle h);
+
+/* Fill the interior of block id (a refined level's) from the next coarser
+ * level, as the reference's refinement update fills a new fine block
+ * (cg_level_connected.F90:870-920 prolong, 1059-1093 prolong_1var): u and B
+ * by injection (rank-4 arrays are prolonged at order 0 whatever their
+ * registered order), psi at ord_mag_prolong.  With pk_restrict this lets a
+ * host regrid: restrict, place the blocks of the new layout, fill the new
+ * ones with pk_prolong_block, then pk_fill_guards.  The coarser level's guard
+ * cells must be current (pk_fill_guards before the new blocks were placed).
+ * Synchronous. */
+int pk_prolong_block(pk_handle h, int32_t id);
 
 /* ---- Domains spanning ranks (one process per GPU) ----
  * The reference exchanges guard cells between MPI ranks in the same

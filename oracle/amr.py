@@ -264,30 +264,7 @@ class AmrOracle:
         s0 = self.setup0
         ofl = s0.ord_fluid_prolong if s0.ord_fluid_prolong in (0, 1) else 0
         ku, kb = PROLONG[ofl], PROLONG[s0.ord_mag_prolong]
-
-        def pro1(k, get, par):
-            """sum over m = -r..r of P(-m) c(m) (left child) or P(m) c(m), left to right"""
-            P, r = k
-            if r == 0:
-                return get(0)
-            acc = None
-            for m in range(-r, r + 1):
-                t = np.where(par == 0, P[3 - m], P[3 + m]) * get(m)
-                acc = t if acc is None else acc + t
-            return acc
-
-        def pro3(k, fb, cs, par):
-            r = k[1]
-            ry = r if self.has[1] else 0
-            rz = r if self.has[2] else 0
-            Y = {}
-            for kz in range(-rz, rz + 1):
-                X = {}
-                for ky in range(-ry, ry + 1):
-                    row = lambda kx, ky=ky, kz=kz: fb[cs[2] + kz, cs[1] + ky, cs[0] + kx]
-                    X[ky] = pro1(k, row, par[0]) if self.has[0] else row(0)
-                Y[kz] = pro1(k, lambda m: X[m], par[1]) if self.has[1] else X[0]
-            return pro1(k, lambda m: Y[m], par[2]) if self.has[2] else Y[0]
+        pro3 = self._pro3
 
         for L in range(1, self.maxl + 1):
             for lev, i, dst, j, cs, par in self.prolong:
@@ -304,6 +281,81 @@ class AmrOracle:
                 fields = [(A.b[..., c], B.b[..., c]) for c in range(3)] + [(A.psi, B.psi)]
                 for fa, fb in fields:
                     fa[dst] = pro3(kb, fb, cs, par)
+
+    @staticmethod
+    def _pro1(k, get, par):
+        """sum over m = -r..r of P(-m) c(m) (left child) or P(m) c(m), left to right"""
+        P, r = k
+        if r == 0:
+            return get(0)
+        acc = None
+        for m in range(-r, r + 1):
+            t = np.where(par == 0, P[3 - m], P[3 + m]) * get(m)
+            acc = t if acc is None else acc + t
+        return acc
+
+    def _pro3(self, k, fb, cs, par):
+        """directional prolongation x, then y, then z (grid_container_prolong.F90:290-453)"""
+        pro1 = self._pro1
+        r = k[1]
+        ry = r if self.has[1] else 0
+        rz = r if self.has[2] else 0
+        Y = {}
+        for kz in range(-rz, rz + 1):
+            X = {}
+            for ky in range(-ry, ry + 1):
+                row = lambda kx, ky=ky, kz=kz: fb[cs[2] + kz, cs[1] + ky, cs[0] + kx]
+                X[ky] = pro1(k, row, par[0]) if self.has[0] else row(0)
+            Y[kz] = pro1(k, lambda m: X[m], par[1]) if self.has[1] else X[0]
+        return pro1(k, lambda m: Y[m], par[2]) if self.has[2] else Y[0]
+
+    def relayout(self, add=(), remove=()):
+        """A new driver over this one's blocks minus ``remove`` (ids), plus
+        ``add`` = [(setup, level, off)] appended with zero state, carrying
+        every remaining block's whole array and the time state."""
+        keep = [i for i in range(len(self.blocks)) if i not in set(remove)]
+        blocks = []
+        for i in keep:
+            ob = self.blocks[i]
+            blocks.append((ob.setup, self.level[i], self.off[i], ob.u, ob.b, ob.psi))
+        for s, lev, off in add:
+            ext = (s.ext[2], s.ext[1], s.ext[0])
+            blocks.append((s, lev, off, np.zeros(ext + (s.nvar,)), np.zeros(ext + (3,)) if self.mag else None,
+                           np.zeros(ext) if self.mag else None))
+        new = AmrOracle(self.dom, blocks)
+        C.memmove(C.byref(new.state), C.byref(self.state), C.sizeof(O.OState))
+        return new
+
+    # ---- filling a new block (refinement update) ----------------------------
+    def prolong_block(self, i):
+        """Every interior cell of block i (a refined level's) from the level
+        below, as cg_level_connected.F90:870-920 / 1059-1093 fill the blocks a
+        refinement update creates: u and B (rank-4 arrays) by injection, psi
+        at ord_mag_prolong, read from the coarse blocks' storage (guard cells
+        included, which must be current)."""
+        L = self.level[i]
+        assert L >= 1
+        A = self.blocks[i]
+        s = A.setup
+        g, n = s.guards, s.n
+        z, y, x = [a.ravel() for a in np.meshgrid(*[np.arange(g[d], g[d] + n[d]) for d in (2, 1, 0)], indexing="ij")]
+        F = [x - g[0] + self.off[i][0], y - g[1] + self.off[i][1], z - g[2] + self.off[i][2]]
+        P = [np.where(self.has[d], _floor2(F[d]), 0) for d in range(3)]
+        par = [np.where(self.has[d], F[d] - 2 * _floor2(F[d]), 0) for d in range(3)]
+        cown = self._owner(L - 1, P)
+        assert (cown >= 0).all(), "a refined block is not nested in the coarser level"
+        Pw = self._wrap(L - 1, P)
+        kb = PROLONG[self.setup0.ord_mag_prolong]
+        for j in np.unique(cown):
+            m = cown == j
+            B = self.blocks[int(j)]
+            sj = B.setup
+            cs = tuple(Pw[d][m] - self.off[j][d] + sj.guards[d] for d in range(3))
+            dst = (z[m], y[m], x[m])
+            A.u[dst] = B.u[cs[2], cs[1], cs[0]]
+            if self.mag:
+                A.b[dst] = B.b[cs[2], cs[1], cs[0]]
+                A.psi[dst] = self._pro3(kb, B.psi, cs, tuple(par[d][m] for d in range(3)))
 
     # ---- restriction (restrict_to_base) ---------------------------------
     def restrict(self):

@@ -35,6 +35,8 @@ EXPORTS = (
     "pk_block_remote", "pk_halo_peers", "pk_halo_sizes", "pk_halo_pack", "pk_halo_unpack", "pk_set_comm",
     "pk_set_instances", "pk_get_instance_state", "pk_set_instance_state", "pk_block_place_level",
     "pk_set_stage_variant", "pk_fp64_peak", "pk_restrict",
+    "pk_prolong_block",
+    "pk_block_remove",
 )
 
 HALO_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32)
@@ -147,6 +149,8 @@ def load(path: str = LIBPATH):
     L.pk_set_stage_variant.argtypes = [H, C.c_int32]
     L.pk_fp64_peak.argtypes = [C.POINTER(C.c_double)]
     L.pk_restrict.argtypes = [H]
+    L.pk_prolong_block.argtypes = [H, C.c_int32]
+    L.pk_block_remove.argtypes = [H, C.c_int32]
     L.pk_get_instance_state.argtypes = [H, C.c_int32, C.POINTER(PkTimeState)]
     L.pk_set_instance_state.argtypes = [H, C.c_int32, C.POINTER(PkTimeState)]
     L.pk_upload_device.argtypes = [H, C.c_int32, C.c_void_p]

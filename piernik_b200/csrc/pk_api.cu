@@ -394,7 +394,7 @@ int prolong_guards(pk_ctx* h)
         k_prolong<<<grid1d(cells, 256), 256, 0, h->stream>>>(h->d_runs + r0, h->d_run_start + r0, nr, cells,
                                                              h->d_xptr[h->cur], h->nvf, h->cfg.magnetic ? 4 : 0,
                                                              h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1, h->pro_u,
-                                                             h->pro_b);
+                                                             h->pro_b, h->pro_b);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
@@ -1100,6 +1100,29 @@ int pk_block_add(pk_handle h, const int32_t n[3], const double dl[3], const int3
         PK_CUDA(h, cudaMalloc(&h->d_red, sizeof(unsigned long long) * h->red_cap));
         PK_CUDA(h, cudaMallocHost(&h->h_red, sizeof(unsigned long long) * h->red_cap));
     }
+    return PK_OK;
+}
+
+int pk_block_remove(pk_handle h, int32_t id)
+{
+    if (!h) return PK_E_ARG;
+    if (id < 0 || id >= (int)h->blocks.size()) return fail(h, PK_E_ARG, "unknown block id");
+    if (h->ninst > 1) return fail(h, PK_E_STATE, "stacked instances live in one block");
+    if (!h->grad_ckpt.empty() || h->lam) return fail(h, PK_E_STATE, "release the differentiable path first (pk_grad_release)");
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    invalidate_graph(h);
+    Block& b = h->blocks[id];
+    cudaFree(b.buf[0]);
+    cudaFree(b.buf[1]);
+    cudaFree(b.uh);
+    cudaFree(b.stage);
+    cudaFree(b.retry);
+    cudaFree(b.leaf);
+    for (int d = 0; d < 3; ++d) cudaFree(b.flux[d]);
+    h->blocks.erase(h->blocks.begin() + id);
+    h->batch_dirty = true;
+    h->x_dirty = true;
+    h->x_ptrs_dirty = true;
     return PK_OK;
 }
 
@@ -2228,6 +2251,58 @@ int pk_restrict(pk_handle h)
     }
     PK_CUDA(h, cudaStreamSynchronize(h->stream));
     return PK_OK;
+}
+
+int pk_prolong_block(pk_handle h, int32_t id)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (int rc = exchange_prepare(h)) return rc;
+    if (h->max_level < 1 || b->level < 1) return fail(h, PK_E_ARG, "only a block of a refined level can be prolonged");
+    const int nl = (int)h->blocks.size();
+    std::vector<LBlock> lb(nl);
+    for (int i = 0; i < nl; ++i) {
+        const Block& x = h->blocks[i];
+        lb[i].level = x.level;
+        for (int d = 0; d < 3; ++d) {
+            lb[i].n[d] = x.n[d];
+            lb[i].g[d] = x.g[d];
+            lb[i].off[d] = x.off[d];
+        }
+    }
+    std::vector<PRun> runs;
+    std::string err;
+    if (!build_fill_runs(lb, h->dom, id, runs, err)) return fail(h, PK_E_ARG, err);
+    std::vector<PRunDev> dev(runs.size());
+    std::vector<long long> start(runs.size());
+    long long total = 0;
+    for (size_t r = 0; r < runs.size(); ++r) {
+        const PRun& s = runs[r];
+        dev[r] = PRunDev{s.fb, s.cb, s.fx, s.fy, s.fz, s.len, s.cx, s.cy, s.cz, s.px, s.py, s.pz};
+        start[r] = total;
+        total += s.len;
+    }
+    PRunDev* d_runs = nullptr;
+    long long* d_start = nullptr;
+    int rc = upload_vec(h, dev, &d_runs);
+    if (rc == PK_OK) rc = upload_vec(h, start, &d_start);
+    // u and B are rank-4 arrays, prolonged by injection whatever their order
+    // (cg_level_connected.F90:1063, the QUIRKY ord_prolong = 0); psi with its
+    // own order, ord_mag_prolong
+    ProlongCoef inj{};
+    prolong_coef(0, &inj);
+    if (rc == PK_OK && total > 0) {
+        k_prolong<<<grid1d(total, 256), 256, 0, h->stream>>>(d_runs, d_start, (int)runs.size(), total,
+                                                             h->d_xptr[h->cur], h->nvf, h->cfg.magnetic ? 4 : 0,
+                                                             h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1, inj, inj,
+                                                             h->pro_b);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess)
+            rc = fail(h, PK_E_CUDA, "prolongation of a block failed");
+        h->launches += 1;
+    }
+    cudaFree(d_runs);
+    cudaFree(d_start);
+    return rc;
 }
 
 int pk_set_stage_variant(pk_handle h, int32_t variant)

@@ -439,7 +439,7 @@ PK_DEV double prolong_cell(const ProlongCoef& k, const double* c, long long sx, 
 
 static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long long* __restrict__ start, int nruns,
                                  long long total, const XPtr* __restrict__ blocks, int nu, int nmag, int has_x,
-                                 int has_y, int has_z, ProlongCoef ku, ProlongCoef kb)
+                                 int has_y, int has_z, ProlongCoef ku, ProlongCoef kb, ProlongCoef kpsi)
 {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         int lo = 0, hi = nruns - 1;
@@ -464,8 +464,8 @@ static __global__ void k_prolong(const PRunDev* __restrict__ runs, const long lo
                                                                 r.py, r.pz, has_x, has_y, has_z);
         }
         for (int v = nu; v < nu + nmag; ++v)
-            F.u[(long long)v * F.plane + fo] = prolong_cell(kb, C.u + (long long)v * C.plane + co, sx, sy, sz, px,
-                                                            r.py, r.pz, has_x, has_y, has_z);
+            F.u[(long long)v * F.plane + fo] = prolong_cell(v < nu + 3 ? kb : kpsi, C.u + (long long)v * C.plane + co, sx,
+                                                            sy, sz, px, r.py, r.pz, has_x, has_y, has_z);
     }
 }
 

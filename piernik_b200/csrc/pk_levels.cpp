@@ -343,4 +343,59 @@ bool build_levels(const std::vector<LBlock>& blocks, const long long dom[3], Lev
     return true;
 }
 
+bool build_fill_runs(const std::vector<LBlock>& blocks, const long long dom[3], int target, std::vector<PRun>& runs,
+                     std::string& err)
+{
+    runs.clear();
+    if (target < 0 || target >= (int)blocks.size()) {
+        err = "no such block";
+        return false;
+    }
+    const LBlock& b = blocks[target];
+    const int L = b.level;
+    if (L < 1) {
+        err = "a base-level block has no coarser level to be filled from";
+        return false;
+    }
+    bool has[3];
+    for (int d = 0; d < 3; ++d) has[d] = dom[d] > 1;
+    LevelIndex coarse;
+    coarse.init(blocks, dom, L - 1);
+    for (int i = 0; i < (int)blocks.size(); ++i)
+        if (blocks[i].level == L - 1) coarse.add(i);
+    for (int z = b.g[2]; z < b.g[2] + b.n[2]; ++z)
+        for (int y = b.g[1]; y < b.g[1] + b.n[1]; ++y) {
+            PRun run{};
+            run.len = 0;
+            for (int x = b.g[0]; x < b.g[0] + b.n[0]; ++x) {
+                const int s[3] = {x, y, z};
+                long long p[3];
+                int par[3], cs[3];
+                for (int d = 0; d < 3; ++d) {
+                    const long long f = s[d] - b.g[d] + b.off[d];
+                    p[d] = has[d] ? floordiv2(f) : 0;
+                    par[d] = has[d] ? (int)(f - 2 * floordiv2(f)) : 0;
+                }
+                const int cb = coarse.owner(p);
+                if (cb < 0) {
+                    err = where(target, b) + " reaches outside its coarser level";
+                    return false;
+                }
+                const LBlock& c = blocks[cb];
+                for (int d = 0; d < 3; ++d) cs[d] = (int)(p[d] - c.off[d]) + c.g[d];
+                const bool cont = run.len > 0 && cb == run.cb && cs[1] == run.cy && cs[2] == run.cz &&
+                                  par[1] == run.py && par[2] == run.pz &&
+                                  cs[0] == run.cx + ((run.px + run.len) >> 1) && par[0] == ((run.px + run.len) & 1);
+                if (cont) {
+                    ++run.len;
+                    continue;
+                }
+                if (run.len > 0) runs.push_back(run);
+                run = PRun{target, cb, x, y, z, 1, cs[0], cs[1], cs[2], par[0], par[1], par[2]};
+            }
+            if (run.len > 0) runs.push_back(run);
+        }
+    return true;
+}
+
 }  // namespace pk

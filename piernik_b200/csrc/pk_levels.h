@@ -84,4 +84,11 @@ struct LevelPlan {
 // regions on the same side.
 bool build_levels(const std::vector<LBlock>& blocks, const long long dom[3], LevelPlan& plan, std::string& err);
 
+// Rows prolonging every interior cell of block `target` from the next coarser
+// level, as the refinement update fills a new block (cg_level_connected.F90:
+// 870-920 prolong, 1059-1093 the fine block's ijkse): fails if a parent lies
+// in no interior of that level.
+bool build_fill_runs(const std::vector<LBlock>& blocks, const long long dom[3], int target, std::vector<PRun>& runs,
+                     std::string& err);
+
 }  // namespace pk

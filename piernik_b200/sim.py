@@ -266,6 +266,15 @@ class Simulation:
         first (restrict_to_base)."""
         self._chk(self.lib.pk_restrict(self.h), "pk_restrict")
 
+    def remove_block(self, block: int) -> None:
+        """Free ``block``; the ids above it move down by one."""
+        self._chk(self.lib.pk_block_remove(self.h, block), "pk_block_remove")
+        self.blocks = {(k if k < block else k - 1): v for k, v in self.blocks.items() if k != block}
+
+    def prolong_block(self, block: int) -> None:
+        """Fill every cell of ``block`` (a refined level's) from the coarser level."""
+        self._chk(self.lib.pk_prolong_block(self.h, block), "pk_prolong_block")
+
     def place_block(self, block: int, off, level: int = 0) -> None:
         """Put the block's first interior cell at ``off`` on the grid of its
         refinement level (the base grid refined ``level`` times)."""

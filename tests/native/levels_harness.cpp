@@ -7,11 +7,9 @@
 #include "../../piernik_b200/csrc/pk_levels.h"
 
 static pk::LevelPlan g_plan;
+static std::vector<pk::PRun> g_fill;
 
-extern "C" {
-
-int lv_build(int nb, const int* level, const int* n, const int* g, const long long* off, const long long* dom,
-             char* err, int errlen)
+static std::vector<pk::LBlock> blocks_of(int nb, const int* level, const int* n, const int* g, const long long* off)
 {
     std::vector<pk::LBlock> b(nb);
     for (int i = 0; i < nb; ++i) {
@@ -22,6 +20,37 @@ int lv_build(int nb, const int* level, const int* n, const int* g, const long lo
             b[i].off[d] = off[3 * i + d];
         }
     }
+    return b;
+}
+
+extern "C" {
+
+// rows filling the interior of block target from the coarser level; -1 on error
+long long lv_fill(int nb, const int* level, const int* n, const int* g, const long long* off, const long long* dom,
+                  int target, char* err, int errlen)
+{
+    std::string e;
+    if (!pk::build_fill_runs(blocks_of(nb, level, n, g, off), dom, target, g_fill, e)) {
+        if (err && errlen > 0) {
+            std::strncpy(err, e.c_str(), errlen - 1);
+            err[errlen - 1] = 0;
+        }
+        return -1;
+    }
+    return (long long)g_fill.size();
+}
+
+void lv_fill_run(long long i, int* out)
+{
+    const pk::PRun& r = g_fill[i];
+    const int v[12] = {r.fb, r.cb, r.fx, r.fy, r.fz, r.len, r.cx, r.cy, r.cz, r.px, r.py, r.pz};
+    std::memcpy(out, v, sizeof(v));
+}
+
+int lv_build(int nb, const int* level, const int* n, const int* g, const long long* off, const long long* dom,
+             char* err, int errlen)
+{
+    std::vector<pk::LBlock> b = blocks_of(nb, level, n, g, off);
     std::string e;
     if (!pk::build_levels(b, dom, g_plan, e)) {
         if (err && errlen > 0) {

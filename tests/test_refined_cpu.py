@@ -201,3 +201,91 @@ def test_refined_oracle_restriction_matches_leaves(oracle_lib, dim):
     assert np.max(np.abs(base_totals() - leaf) / scale) > 1e-10      # drifted before
     a.restrict()
     assert np.all(np.abs(base_totals() - leaf) <= 1e-12 * scale)
+
+
+# level-2 blocks of a refinement update inside the level-1 box of REG3[0]
+NEW2 = [((24, 24, 24), (8, 8, 8)), ((32, 24, 24), (8, 8, 8))]
+
+
+def new_blocks(blocks, placements, dom=DOM3, level=2):
+    made = problems.refined_blocks(dom, [(level, off, n) for off, n in placements], blocks[0][0],
+                                   problems.wave_fields(dom, seed=5))
+    return [(s, L, off) for s, L, off, *_ in made]
+
+
+def fill_runs(hlib, blocks, dom, target):
+    nb = len(blocks)
+    lev = (C.c_int * nb)(*[b[1] for b in blocks])
+    n = (C.c_int * (3 * nb))(*[x for b in blocks for x in b[0].n])
+    g = (C.c_int * (3 * nb))(*[x for b in blocks for x in b[0].guards])
+    off = (C.c_longlong * (3 * nb))(*[x for b in blocks for x in b[2]])
+    dm = (C.c_longlong * 3)(*dom)
+    err = C.create_string_buffer(256)
+    hlib.lv_fill.restype = C.c_longlong
+    cnt = hlib.lv_fill(nb, lev, n, g, off, dm, target, err, 256)
+    if cnt < 0:
+        raise ValueError(err.value.decode())
+    out = []
+    r = (C.c_int * 12)()
+    hlib.lv_fill_run.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
+    for i in range(cnt):
+        hlib.lv_fill_run(i, r)
+        out.append(tuple(r))
+    return out
+
+
+def test_planner_fill_runs(hlib, oracle_lib):
+    """The rows filling a new block cover its interior once, each cell with
+    the parent and parity the oracle's ownership maps give."""
+    base = case("hd", DOM3, REG3[:1])
+    a = amr.AmrOracle(DOM3, base).relayout(add=new_blocks(base, NEW2))
+    blocks = [(ob.setup, a.level[i], a.off[i]) for i, ob in enumerate(a.blocks)]
+    for target in (len(blocks) - 2, len(blocks) - 1):
+        s = blocks[target][0]
+        g, n, off = s.guards, s.n, blocks[target][2]
+        seen = {}
+        for fb, cb, fx, fy, fz, ln, cx, cy, cz, px, py, pz in fill_runs(hlib, blocks, DOM3, target):
+            assert fb == target
+            for i in range(ln):
+                key = (fx + i, fy, fz)
+                assert key not in seen
+                seen[key] = (cb, cx + ((px + i) >> 1), cy, cz, (px + i) & 1, py, pz)
+        assert len(seen) == n[0] * n[1] * n[2]
+        for (x, y, z), got in seen.items():
+            F = [x - g[0] + off[0], y - g[1] + off[1], z - g[2] + off[2]]
+            P = [f // 2 for f in F]
+            j = int(a._owner(1, [np.array(p) for p in P]))
+            sj = a.blocks[j].setup
+            want = (j,) + tuple(P[d] - a.off[j][d] + sj.guards[d] for d in range(3)) + tuple(f & 1 for f in F)
+            assert got == want
+    with pytest.raises(ValueError, match="outside"):
+        fill_runs(hlib, blocks[:-2] + [(blocks[-1][0], 2, (0, 0, 0))], DOM3, len(blocks) - 2)
+    with pytest.raises(ValueError, match="base-level"):
+        fill_runs(hlib, blocks, DOM3, 0)
+
+
+def test_regrid_oracle_restores_by_restriction(oracle_lib):
+    """A block filled by the refinement update (u and B injected) restricts
+    back to the coarse cells it came from: the eight equal children summed
+    one by one round at most in the last bits; cells not covered stay as
+    they were."""
+    base = case("mhd", DOM3, REG3[:1])
+    a = amr.AmrOracle(DOM3, base)
+    a.fill_guards()
+    a.run(1)
+    r = a.relayout(add=new_blocks(base, NEW2))
+    r.fill_guards()
+    before = [(ob.u.copy(), ob.b.copy()) for ob in r.blocks]
+    for k in (len(r.blocks) - 2, len(r.blocks) - 1):
+        r.prolong_block(k)
+        ob = r.blocks[k]
+        g, n = ob.setup.guards, ob.setup.n
+        inner = ob.u[g[2]:g[2] + n[2], g[1]:g[1] + n[1], g[0]:g[0] + n[0]]
+        assert np.all(np.isfinite(inner)) and np.any(inner != 0.0)
+    r.restrict()
+    for i, ob in enumerate(r.blocks):
+        if r.level[i] == 1:
+            for now, was in ((ob.u, before[i][0]), (ob.b, before[i][1])):
+                assert np.all(np.abs(now - was) <= 4e-16 * np.abs(was)), i
+            changed = np.any(ob.u != before[i][0], axis=-1)
+            assert changed.sum() <= 8 * 8 * 8 // 8 * 2, i      # only the cells under the two new blocks
