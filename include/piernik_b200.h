@@ -281,6 +281,58 @@ int pk_restrict(pk_handle h);
  * Synchronous. */
 int pk_prolong_block(pk_handle h, int32_t id);
 
+/* ---- Refinement criteria (unified_ref_crit_var, URC_var.F90) ----
+ * One criterion examines one plane of the block state (field: the plane
+ * index, fluid components first in the reference's order, then B, then psi;
+ * the reference's "dens" / "velx" / "ener" name every fluid's component of
+ * that kind, i.e. one criterion per fluid).  A cell is flagged when any
+ * criterion fires (cg%flag%set):
+ *   PK_URC_THRESHOLD  field >= thr over the interior; none on levels >= aux
+ *                     when aux > 0 (refine_on_threshold :297-330);
+ *   PK_URC_GRAD       sum over directions of (p(+1) - p(-1))^2 >= thr^2
+ *                     over the interior (refine_on_gradient :512-582);
+ *   PK_URC_RELGRAD    the (+)-sum of |a - b| / (|a| + |b|) over the six
+ *                     neighbours, squared, >= thr^2 (refine_on_relative_gradient
+ *                     :589-708);
+ *   PK_URC_LOECHNER   Loechner's second-derivative estimator with noise
+ *                     filter aux >= thr, over the interior widened by two
+ *                     cells along each direction (refine_on_second_derivative
+ *                     :348-505; needs nb >= 4). */
+#define PK_URC_THRESHOLD 0
+#define PK_URC_GRAD 1
+#define PK_URC_RELGRAD 2
+#define PK_URC_LOECHNER 3
+
+typedef struct pk_urc {
+    int32_t method;     /* PK_URC_* */
+    int32_t field;      /* plane of the block state */
+    double thr;         /* ref_thr */
+    double aux;         /* Loechner noise filter; threshold: first level left unmarked (> 0) */
+} pk_urc;
+
+/* scan_for_refinements' marking pass (refinement_update.F90:57-120): refresh
+ * the guard cells (all_bnd), clear every block's flag map (flag%init) and
+ * apply the criteria on every block with a leaf cell (urc_list%all_mark over
+ * leaves).  flagged (host, one per block, may be null) receives 1 where a
+ * leaf interior cell is flagged: the block may not be derefined
+ * (sanitize_ref_flags :222-249).  The maps stay on the device for
+ * pk_refine_map and pk_refine_candidates.  Synchronous. */
+int pk_mark_refinement(pk_handle h, const pk_urc* crit, int32_t ncrit, int32_t* flagged);
+
+/* Block id's flag map after pk_mark_refinement: one byte per guard-inclusive
+ * cell, x fastest (cg%flag%map). */
+int pk_refine_map(pk_handle h, int32_t id, uint8_t* map);
+
+/* refinemap2SFC_list (grid_container_ref.F90:96-142) of block id: flags on
+ * covered interior cells are dropped, then every bsize-sized block of the
+ * next finer level whose parent cells inside this block's interior hold a
+ * flag is listed by its offset on that level's grid (3 per candidate, x
+ * outermost as the reference loops).  count receives the number found;
+ * at most cap are written.  No candidates when bsize <= 0 along a direction
+ * with extent (blocky AMR only). */
+int pk_refine_candidates(pk_handle h, int32_t id, const int32_t bsize[3], int64_t* offsets, int32_t cap,
+                         int32_t* count);
+
 /* ---- Domains spanning ranks (one process per GPU) ----
  * The reference exchanges guard cells between MPI ranks in the same
  * internal_boundaries pass (cg_list_bnd.F90:251-324, MPI isend/irecv of the

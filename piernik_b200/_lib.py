@@ -37,6 +37,9 @@ EXPORTS = (
     "pk_set_stage_variant", "pk_fp64_peak", "pk_restrict",
     "pk_prolong_block",
     "pk_block_remove",
+    "pk_mark_refinement",
+    "pk_refine_map",
+    "pk_refine_candidates",
 )
 
 HALO_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32)
@@ -77,6 +80,15 @@ class PkConfig(C.Structure):
         ("ord_fluid_prolong", C.c_int32),
         ("ord_mag_prolong", C.c_int32),
     ]
+
+
+URC_THRESHOLD, URC_GRAD, URC_RELGRAD, URC_LOECHNER = 0, 1, 2, 3
+URC_METHODS = {"threshold": URC_THRESHOLD, "grad": URC_GRAD, "relgrad": URC_RELGRAD, "Loechner": URC_LOECHNER,
+               "second_order": URC_LOECHNER, "d2": URC_LOECHNER}
+
+
+class PkUrc(C.Structure):
+    _fields_ = [("method", C.c_int32), ("field", C.c_int32), ("thr", C.c_double), ("aux", C.c_double)]
 
 
 class PkTimeState(C.Structure):
@@ -151,6 +163,10 @@ def load(path: str = LIBPATH):
     L.pk_restrict.argtypes = [H]
     L.pk_prolong_block.argtypes = [H, C.c_int32]
     L.pk_block_remove.argtypes = [H, C.c_int32]
+    L.pk_mark_refinement.argtypes = [H, C.POINTER(PkUrc), C.c_int32, C.POINTER(C.c_int32)]
+    L.pk_refine_map.argtypes = [H, C.c_int32, C.c_void_p]
+    L.pk_refine_candidates.argtypes = [H, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.c_int32,
+                                       C.POINTER(C.c_int32)]
     L.pk_get_instance_state.argtypes = [H, C.c_int32, C.POINTER(PkTimeState)]
     L.pk_set_instance_state.argtypes = [H, C.c_int32, C.POINTER(PkTimeState)]
     L.pk_upload_device.argtypes = [H, C.c_int32, C.c_void_p]

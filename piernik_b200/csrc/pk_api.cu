@@ -1017,6 +1017,7 @@ int pk_destroy(pk_handle h)
         cudaFree(b.uh);
         cudaFree(b.stage);
         for (int d = 0; d < 3; ++d) cudaFree(b.flux[d]);
+        cudaFree(b.flag);
     }
     for (auto& p : h->ev_used) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
     for (auto& p : h->ev_free) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
@@ -1118,6 +1119,7 @@ int pk_block_remove(pk_handle h, int32_t id)
     cudaFree(b.stage);
     cudaFree(b.retry);
     cudaFree(b.leaf);
+    cudaFree(b.flag);
     for (int d = 0; d < 3; ++d) cudaFree(b.flux[d]);
     h->blocks.erase(h->blocks.begin() + id);
     h->batch_dirty = true;
@@ -2303,6 +2305,150 @@ int pk_prolong_block(pk_handle h, int32_t id)
     cudaFree(d_runs);
     cudaFree(d_start);
     return rc;
+}
+
+int pk_mark_refinement(pk_handle h, const pk_urc* crit, int32_t ncrit, int32_t* flagged)
+{
+    if (!h || (ncrit > 0 && !crit) || ncrit < 0) return PK_E_ARG;
+    if (h->ninst > 1) return fail(h, PK_E_STATE, "stacked instances are not refined");
+    std::vector<UrcDev> cr(ncrit);
+    for (int c = 0; c < ncrit; ++c) {
+        if (crit[c].method < PK_URC_THRESHOLD || crit[c].method > PK_URC_LOECHNER)
+            return fail(h, PK_E_ARG, "unknown refinement criterion");
+        if (crit[c].field < 0 || crit[c].field >= h->nplanes) return fail(h, PK_E_ARG, "criterion field out of range");
+        cr[c] = UrcDev{crit[c].method, crit[c].field, crit[c].thr, crit[c].aux};
+        if (crit[c].method == PK_URC_LOECHNER && h->cfg.nb < 4)
+            return fail(h, PK_E_ARG, "the Loechner criterion needs nb >= 4");
+    }
+    if (int rc = pk_fill_guards(h)) return rc;          // all_bnd: up-to-date guard cells
+    if (int rc = exchange_prepare(h)) return rc;
+    const int nb = (int)h->blocks.size();
+    std::vector<MarkBlk> mb;
+    std::vector<long long> start;
+    std::vector<int> owner;
+    long long total = 0;
+    for (int i = 0; i < nb; ++i) {
+        Block& b = h->blocks[i];
+        const long long ncell = b.plane;
+        if (!b.flag) PK_CUDA(h, cudaMalloc(&b.flag, ncell));
+        PK_CUDA(h, cudaMemsetAsync(b.flag, 0, ncell, h->stream));      // flag%init
+        if (b.leaf_cells == 0) continue;                                  // not a leaf block
+        MarkBlk m;
+        m.u = b.buf[h->cur];
+        m.plane = b.plane;
+        for (int d = 0; d < 3; ++d) {
+            m.ext[d] = b.ext[d];
+            m.g[d] = b.g[d];
+            m.n[d] = b.n[d];
+            m.idl[d] = 1.0 / b.dl[d];
+        }
+        m.level = b.level;
+        m.map = b.flag;
+        m.leaf = b.leaf;
+        mb.push_back(m);
+        start.push_back(total);
+        owner.push_back(i);
+        total += ncell;
+    }
+    MarkBlk* d_mb = nullptr;
+    long long* d_start = nullptr;
+    UrcDev* d_cr = nullptr;
+    int* d_flagged = nullptr;
+    int rc = upload_vec(h, mb, &d_mb);
+    if (rc == PK_OK) rc = upload_vec(h, start, &d_start);
+    if (rc == PK_OK) rc = upload_vec(h, cr, &d_cr);
+    if (rc == PK_OK && !mb.empty() && cudaMalloc(&d_flagged, sizeof(int) * mb.size()) != cudaSuccess)
+        rc = fail(h, PK_E_NOMEM, "cudaMalloc failed");
+    std::vector<int> got(mb.size(), 0);
+    if (rc == PK_OK && total > 0 && ncrit > 0) {
+        cudaMemsetAsync(d_flagged, 0, sizeof(int) * mb.size(), h->stream);
+        k_mark<<<grid1d(total, 256), 256, 0, h->stream>>>(d_mb, d_start, (int)mb.size(), total, d_cr, ncrit,
+                                                          h->blocks[0].n[0] > 1, h->blocks[0].n[1] > 1,
+                                                          h->blocks[0].n[2] > 1, d_flagged);
+        h->launches += 1;
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(got.data(), d_flagged, sizeof(int) * got.size(), cudaMemcpyDeviceToHost, h->stream) !=
+                cudaSuccess)
+            rc = fail(h, PK_E_CUDA, "refinement marking failed");
+    }
+    if (rc == PK_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = fail(h, PK_E_CUDA, "refinement marking failed");
+    cudaFree(d_mb);
+    cudaFree(d_start);
+    cudaFree(d_cr);
+    cudaFree(d_flagged);
+    if (rc == PK_OK && flagged) {
+        for (int i = 0; i < nb; ++i) flagged[i] = 0;
+        for (size_t k = 0; k < owner.size(); ++k) flagged[owner[k]] = got[k];
+    }
+    return rc;
+}
+
+int pk_refine_map(pk_handle h, int32_t id, uint8_t* map)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!map) return fail(h, PK_E_ARG, "null map");
+    if (!b->flag) return fail(h, PK_E_STATE, "no flags: call pk_mark_refinement first");
+    PK_CUDA(h, cudaMemcpyAsync(map, b->flag, b->plane, cudaMemcpyDeviceToHost, h->stream));
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_refine_candidates(pk_handle h, int32_t id, const int32_t bsize[3], int64_t* offsets, int32_t cap,
+                         int32_t* count)
+{
+    Block* b;
+    if (int rc = get_block(h, id, &b)) return rc;
+    if (!bsize || !count || (cap > 0 && !offsets)) return fail(h, PK_E_ARG, "null argument");
+    *count = 0;
+    std::vector<uint8_t> map((size_t)b->plane);
+    if (int rc = pk_refine_map(h, id, map.data())) return rc;
+    std::vector<unsigned char> leaf;
+    if (b->leaf) {
+        leaf.resize((size_t)b->n[0] * b->n[1] * b->n[2]);
+        PK_CUDA(h, cudaMemcpy(leaf.data(), b->leaf, leaf.size(), cudaMemcpyDeviceToHost));
+    }
+    bool has[3];
+    long long bs[3], is[3], ie[3];
+    for (int d = 0; d < 3; ++d) {
+        has[d] = b->n[d] > 1;
+        if (has[d] && bsize[d] <= 0) return PK_OK;          // blocky AMR only
+        bs[d] = has[d] ? bsize[d] : (1LL << 40);             // huge along directions without extent
+        is[d] = b->off[d];
+        ie[d] = b->off[d] + b->n[d] - 1;
+    }
+    // flag%clear(leafmap): drop the flags of covered interior cells
+    auto flag_at = [&](long long x, long long y, long long z) -> bool {
+        const long long lx = x - b->off[0], ly = y - b->off[1], lz = z - b->off[2];
+        const long long c = ((lz + b->g[2]) * b->ext[1] + (ly + b->g[1])) * b->ext[0] + (lx + b->g[0]);
+        if (!map[(size_t)c]) return false;
+        return leaf.empty() || leaf[(size_t)((lz * b->n[1] + ly) * b->n[0] + lx)];
+    };
+    const long long rf = 2;
+    int found = 0;
+    for (long long i = ((is[0]) * rf) / bs[0]; i <= ((ie[0]) * rf + 1) / bs[0]; ++i) {
+        const long long ifs = std::max(is[0], (i * bs[0]) / rf), ife = std::min(ie[0], ((i + 1) * bs[0] - 1) / rf);
+        for (long long j = ((is[1]) * rf) / bs[1]; j <= ((ie[1]) * rf + 1) / bs[1]; ++j) {
+            const long long jfs = std::max(is[1], (j * bs[1]) / rf), jfe = std::min(ie[1], ((j + 1) * bs[1] - 1) / rf);
+            for (long long k = ((is[2]) * rf) / bs[2]; k <= ((ie[2]) * rf + 1) / bs[2]; ++k) {
+                const long long kfs = std::max(is[2], (k * bs[2]) / rf),
+                                kfe = std::min(ie[2], ((k + 1) * bs[2] - 1) / rf);
+                bool any = false;
+                for (long long z = kfs; z <= kfe && !any; ++z)
+                    for (long long y = jfs; y <= jfe && !any; ++y)
+                        for (long long x = ifs; x <= ife && !any; ++x) any = flag_at(x, y, z);
+                if (!any) continue;
+                if (found < cap) {
+                    offsets[3 * found + 0] = has[0] ? i * bs[0] : 0;
+                    offsets[3 * found + 1] = has[1] ? j * bs[1] : 0;
+                    offsets[3 * found + 2] = has[2] ? k * bs[2] : 0;
+                }
+                ++found;
+            }
+        }
+    }
+    *count = found;
+    return PK_OK;
 }
 
 int pk_set_stage_variant(pk_handle h, int32_t variant)

@@ -1,6 +1,7 @@
 // pk_aux.cuh -- bandwidth kernels around the sweep: CFL reduction, psi
 // damping, guard-cell refresh, host-layout conversion.
 #pragma once
+#include "../../include/piernik_b200.h"
 #include "pk_device.cuh"
 #include "pk_kernels.cuh"
 
@@ -596,6 +597,151 @@ static __global__ void k_restrict(const RBoxDev* __restrict__ boxes, const long 
             }
             C.u[(long long)v * C.plane + co] = 0.0 + val;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Refinement criteria (URC_var.F90): one thread per guard-inclusive cell of
+// each marked block sets the cell's flag when any criterion fires there.
+// ---------------------------------------------------------------------------
+struct UrcDev {
+    int method, field;
+    double thr, aux;
+};
+
+struct MarkBlk {
+    const double* u;
+    long long plane;
+    int ext[3], g[3], n[3];
+    int level;
+    double idl[3];                  // 1 / dl (cg%idl)
+    unsigned char* map;             // ext cells, x fastest
+    const unsigned char* leaf;      // interior leaf mask or null (all leaf)
+};
+
+// first differences of refine_on_second_derivative (URC_var.F90:447-505):
+// du = (p(+1) - p(-1)) * idl, dau = (|p(+1)| + |p(-1)|) * idl along stride s
+PK_DEV double urc_du(const double* p, long long s, double id) { return (p[s] - p[-s]) * id; }
+PK_DEV double urc_dau(const double* p, long long s, double id) { return (fabs(p[s]) + fabs(p[-s])) * id; }
+
+// one cross term of the Loechner denominator: ((|du(+t)| + |du(-t)|) + aux (dau(+t) + dau(-t))) * id_t,
+// du and dau taken along s and evaluated at the neighbours along t
+PK_DEV double urc_den(const double* p, long long s, double ids, long long t, double idt, double aux)
+{
+    return ((fabs(urc_du(p + t, s, ids)) + fabs(urc_du(p - t, s, ids))) +
+            aux * (urc_dau(p + t, s, ids) + urc_dau(p - t, s, ids))) * idt;
+}
+
+// Loechner's estimator (refine_on_second_derivative, URC_var.F90:348-437)
+PK_DEV double urc_loechner(const double* p, const long long st[3], const double id[3], const bool has[3], double aux)
+{
+    double sn = 0.0, sd = 0.0;
+    if (has[0]) {
+        double t = (urc_du(p + st[0], st[0], id[0]) - urc_du(p - st[0], st[0], id[0])) * id[0];
+        double a = urc_den(p, st[0], id[0], st[0], id[0], aux);
+        sn = sn + t * t;
+        sd = sd + a * a;
+        if (has[1]) {
+            t = (urc_du(p + st[1], st[0], id[0]) - urc_du(p - st[1], st[0], id[0])) * id[1];
+            sn = sn + 2.0 * (t * t);
+            a = urc_den(p, st[0], id[0], st[1], id[1], aux);
+            const double b = urc_den(p, st[1], id[1], st[0], id[0], aux);
+            sd = (sd + a * a) + b * b;
+        }
+        if (has[2]) {
+            t = (urc_du(p + st[2], st[0], id[0]) - urc_du(p - st[2], st[0], id[0])) * id[2];
+            sn = sn + 2.0 * (t * t);
+            a = urc_den(p, st[0], id[0], st[2], id[2], aux);
+            const double b = urc_den(p, st[2], id[2], st[0], id[0], aux);
+            sd = (sd + a * a) + b * b;
+        }
+    }
+    if (has[1]) {
+        double t = (urc_du(p + st[1], st[1], id[1]) - urc_du(p - st[1], st[1], id[1])) * id[1];
+        double a = urc_den(p, st[1], id[1], st[1], id[1], aux);
+        sn = sn + t * t;
+        sd = sd + a * a;
+        if (has[2]) {
+            t = (urc_du(p + st[2], st[1], id[1]) - urc_du(p - st[2], st[1], id[1])) * id[2];
+            sn = sn + 2.0 * (t * t);
+            a = urc_den(p, st[1], id[1], st[2], id[2], aux);
+            const double b = urc_den(p, st[2], id[2], st[1], id[1], aux);
+            sd = (sd + a * a) + b * b;
+        }
+    }
+    if (has[2]) {
+        const double t = (urc_du(p + st[2], st[2], id[2]) - urc_du(p - st[2], st[2], id[2])) * id[2];
+        const double a = urc_den(p, st[2], id[2], st[2], id[2], aux);
+        sn = sn + t * t;
+        sd = sd + a * a;
+    }
+    if (sd > 0.0) return sn / sd;
+    return sn > 0.0 ? 1.0 : 0.0;
+}
+
+// |a - b| / (|a| + |b|), 0 when either is 0 (rel_grad_1pair, URC_var.F90:674-688)
+PK_DEV double urc_rel1(double a, double b)
+{
+    if (fabs(a) != 0.0 && fabs(b) != 0.0) return fabs(a - b) / (fabs(a) + fabs(b));
+    return 0.0;
+}
+
+// a (+) b squared (sumsq01, URC_var.F90:690-706)
+PK_DEV double urc_sumsq01(double a, double b) { return (a * a) * (1.0 - b * b) + b * b; }
+
+static __global__ void k_mark(const MarkBlk* __restrict__ blks, const long long* __restrict__ start, int nblk,
+                              long long total, const UrcDev* __restrict__ crit, int ncrit, int hx, int hy, int hz,
+                              int* __restrict__ flagged)
+{
+    const bool has[3] = {hx != 0, hy != 0, hz != 0};
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nblk - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const MarkBlk B = blks[lo];
+        long long r = t - start[lo];
+        const int x = (int)(r % B.ext[0]);
+        r /= B.ext[0];
+        const int y = (int)(r % B.ext[1]);
+        const int z = (int)(r / B.ext[1]);
+        const int ic[3] = {x - B.g[0], y - B.g[1], z - B.g[2]};
+        bool inside = true, near = true;          // interior; interior widened by 2 along each direction with extent
+        for (int d = 0; d < 3; ++d) {
+            inside = inside && ic[d] >= 0 && ic[d] < B.n[d];
+            const int w = has[d] ? 2 : 0;
+            near = near && ic[d] >= -w && ic[d] < B.n[d] + w;
+        }
+        const long long cell = ((long long)z * B.ext[1] + y) * B.ext[0] + x;
+        const long long st[3] = {has[0] ? 1 : 0, has[1] ? (long long)B.ext[0] : 0,
+                                 has[2] ? (long long)B.ext[0] * B.ext[1] : 0};
+        unsigned char f = 0;
+        for (int c = 0; c < ncrit; ++c) {
+            const UrcDev C = crit[c];
+            const double* p = B.u + (long long)C.field * B.plane + cell;
+            if (C.method == PK_URC_LOECHNER) {
+                if (near && urc_loechner(p, st, B.idl, has, C.aux) >= C.thr) f = 1;
+                continue;
+            }
+            if (!inside) continue;
+            if (C.method == PK_URC_THRESHOLD) {
+                if (C.aux > 0.0 && (double)B.level >= C.aux) continue;
+                if (p[0] >= C.thr) f = 1;
+            } else if (C.method == PK_URC_GRAD) {
+                const double a = p[st[0]] - p[-st[0]], b = p[st[1]] - p[-st[1]], e = p[st[2]] - p[-st[2]];
+                if ((a * a + b * b) + e * e >= C.thr * C.thr) f = 1;
+            } else if (C.method == PK_URC_RELGRAD) {
+                double g2 = 0.0;
+                if (has[0]) g2 = urc_sumsq01(urc_rel1(p[0], p[st[0]]), urc_rel1(p[0], p[-st[0]]));
+                if (has[1]) g2 = urc_sumsq01(g2, urc_sumsq01(urc_rel1(p[0], p[st[1]]), urc_rel1(p[0], p[-st[1]])));
+                if (has[2]) g2 = urc_sumsq01(g2, urc_sumsq01(urc_rel1(p[0], p[st[2]]), urc_rel1(p[0], p[-st[2]])));
+                if (g2 >= C.thr * C.thr) f = 1;
+            }
+        }
+        B.map[cell] = f;
+        if (f && inside && (!B.leaf || B.leaf[((long long)ic[2] * B.n[1] + ic[1]) * B.n[0] + ic[0]])) flagged[lo] = 1;
     }
 }
 

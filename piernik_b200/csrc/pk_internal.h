@@ -46,6 +46,7 @@ struct Block {
     unsigned char* leaf = nullptr;         // device interior leaf mask (null: every cell is a leaf)
     long long leaf_cells = -1;             // cells of the mask set (-1: all)
     double* flux[3] = {nullptr, nullptr, nullptr};   // unsplit scheme: face fluxes per direction
+    unsigned char* flag = nullptr;         // refinement flag map (ext cells), pk_mark_refinement
 };
 
 // the per-block stage kernel sweeps whole pencils in place where they fit

@@ -266,6 +266,35 @@ class Simulation:
         first (restrict_to_base)."""
         self._chk(self.lib.pk_restrict(self.h), "pk_restrict")
 
+    def mark_refinement(self, criteria) -> np.ndarray:
+        """Flag cells by the refinement criteria (URC_var.F90) on every leaf
+        block; ``criteria`` = [(method, field, thr, aux)], method one of
+        ``_lib.URC_METHODS`` (or its number), field a plane of the state.
+        Returns, per block, 1 where a leaf interior cell is flagged."""
+        arr = (L.PkUrc * max(len(criteria), 1))()
+        for k, (m, f, thr, aux) in enumerate(criteria):
+            arr[k] = L.PkUrc(L.URC_METHODS[m] if isinstance(m, str) else int(m), int(f), float(thr), float(aux))
+        out = (C.c_int32 * len(self.blocks))()
+        self._chk(self.lib.pk_mark_refinement(self.h, arr, len(criteria), out), "pk_mark_refinement")
+        return np.array(out[:], dtype=np.int32)
+
+    def refine_map(self, block: int = 0) -> np.ndarray:
+        """The flag map of ``block`` after mark_refinement, [z, y, x] with guard cells."""
+        s = self.blocks.get(block, self.setup)
+        m = np.zeros((s.ext[2], s.ext[1], s.ext[0]), dtype=np.uint8)
+        self._chk(self.lib.pk_refine_map(self.h, block, m.ctypes.data), "pk_refine_map")
+        return m
+
+    def refine_candidates(self, block: int, bsize) -> list:
+        """Offsets (level + 1 grid) of the bsize blocks refinemap2SFC_list would create."""
+        bs = (C.c_int32 * 3)(*bsize)
+        cnt = C.c_int32()
+        self._chk(self.lib.pk_refine_candidates(self.h, block, bs, None, 0, C.byref(cnt)), "pk_refine_candidates")
+        offs = (C.c_int64 * (3 * max(cnt.value, 1)))()
+        self._chk(self.lib.pk_refine_candidates(self.h, block, bs, offs, cnt.value, C.byref(cnt)),
+                  "pk_refine_candidates")
+        return [tuple(offs[3 * k:3 * k + 3]) for k in range(cnt.value)]
+
     def remove_block(self, block: int) -> None:
         """Free ``block``; the ids above it move down by one."""
         self._chk(self.lib.pk_block_remove(self.h, block), "pk_block_remove")
