@@ -1583,11 +1583,18 @@ static int run_step_sweeps(pk_ctx* h, double dt, double ch, double fac)
 // from d_step.
 static int unsplit_sweep(pk_ctx* h)
 {
-    if (h->connected) return fail(h, PK_E_UNSUPPORTED, "the unsplit scheme runs on single or independent blocks");
     const PhysOps* ops = ops_of(h);
     const int order = h->cfg.integration_order, nst = order == 1 ? 1 : 2;
+    if (h->connected) {
+        // blocks of one level on this device: the stage array uh lives in the
+        // other parity's buffer so that the same-level exchange tables serve it
+        if (!h->remote.empty()) return fail(h, PK_E_UNSUPPORTED, "the unsplit scheme runs on one rank");
+        for (auto& b : h->blocks)
+            if (b.level > 0) return fail(h, PK_E_UNSUPPORTED, "refined domains use the split scheme");
+        if (int rc = exchange_prepare(h)) return rc;
+    }
     for (auto& b : h->blocks) {
-        if (!b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+        if (!h->connected && !b.uh) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
         for (int d = 0; d < 3; ++d)
             if (b.n[d] > 1 && !b.flux[d]) PK_CUDA(h, cudaMalloc(&b.flux[d], sizeof(double) * h->nplanes * b.plane));
     }
@@ -1595,16 +1602,26 @@ static int unsplit_sweep(pk_ctx* h)
         const bool first = s == 1;
         const int last = (order == 1) || (s == 2);
         const double rk = order == 1 ? 1.0 : (first ? 0.5 : 1.0);
+        const bool to_uh = order == 2 && first;
         for (auto& b : h->blocks) {
             double* u = state(h, b);
-            const double* in = (first || order < 2) ? u : b.uh;
-            double* T = (order == 2 && first) ? b.uh : u;
+            double* uh = h->connected ? b.buf[1 - h->cur] : b.uh;
+            const double* in = (first || order < 2) ? u : uh;
+            double* T = to_uh ? uh : u;
             for (int d = 0; d < 3; ++d)
                 if (b.n[d] > 1)
                     if (int rc = ops->unsplit_flux(h, b, d, in, b.flux[d])) return rc;
             if (int rc = ops->unsplit_apply(h, b, u, T, rk, last)) return rc;
             if (int rc = fill_guards_ptr(h, b, T)) return rc;
             b.guards_stale = false;
+        }
+        // update_boundaries(istep) between the blocks (unsplit_sweeps.F90:182)
+        if (h->connected && h->xlocal.total > 0) {
+            const int nblk = h->xlocal.n < 148 * 16 ? h->xlocal.n : 148 * 16;
+            k_exchange<<<nblk, 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total,
+                                                    h->d_xptr[to_uh ? 1 - h->cur : h->cur], h->nplanes);
+            PK_CUDA(h, cudaGetLastError());
+            h->launches += 1;
         }
     }
     return PK_OK;

@@ -101,3 +101,34 @@ def test_unsplit_euler_and_outflow(gpu_lib):
     ob.run(3)
     assert_bitexact(sim.download()[0], ob.u, "u")
     sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("phys,lim,order,periodic", [("mhd", "moncen", 2, True), ("hd", "vanleer", 2, False),
+                                                     ("hd", "minmod", 1, True), ("mhd", "weno3", 2, True)])
+def test_unsplit_tiled_domain_equals_one_block(gpu_lib, phys, lim, order, periodic):
+    """Blocks of one level tiling the domain (the uh stage array exchanged
+    after the first stage, u after the second, unsplit_sweeps.F90:182)
+    evolve exactly like the oracle's single block."""
+    from test_gpu_blocks import exact_dl, interior_of, run_tiled, tiles
+    from piernik_b200.config import BND_OUT, BND_PER
+    bnd = ((BND_PER, BND_PER),) * 3 if periodic else ((BND_OUT, BND_OUT), (BND_PER, BND_PER), (BND_PER, BND_PER))
+    n = (40, 36, 28) if phys == "mhd" else (40, 20, 16)
+    full = exact_dl(useup(phys, n=n, lim=lim, integration_order=order).replace(bnd=bnd))
+    state = random_state(full, seed=3)
+    ob = oracle.OracleBlock(full, *state)
+    ob.fill_guards()
+    ob.run(3)
+    blocks = tiles([16, 24], [20, 16], [12, 16]) if phys == "mhd" else tiles([12, 16, 12], [20], [8, 8])
+    st0 = tuple(x.copy() if x is not None else None for x in (ob.u, ob.b, ob.psi))
+    fresh = oracle.OracleBlock(full, *state)
+    fresh.fill_guards()
+    got, st = run_tiled(full, (fresh.u, fresh.b, fresh.psi), blocks, (periodic, True, True), 3, bnd_x=BND_OUT)
+    assert (st.t, st.dt, st.nstep) == (ob.state.t, ob.state.dt, ob.state.nstep)
+    for (nn, off), arrs in zip(blocks, got):
+        s = full.replace(n=nn)
+        for k, name in enumerate(("u", "b", "psi")):
+            if arrs[k] is None:
+                continue
+            assert_bitexact(interior_of(s, arrs[k], nn, (0, 0, 0)), interior_of(full, st0[k], nn, off),
+                            f"{phys} block {off} {name}")
