@@ -187,6 +187,12 @@ void free_segs(pk_ctx* h)
 
 void free_levels(pk_ctx* h)
 {
+    for (auto& q : h->part) {
+        cudaFree(q.segs.dev);
+        cudaFree(q.runs);
+        cudaFree(q.run_start);
+        q = pk_ctx::Partial();
+    }
     cudaFree(h->d_rbox);
     cudaFree(h->d_rbox_start);
     h->d_rbox = nullptr;
@@ -230,7 +236,31 @@ int upload_vec(pk_ctx* h, const std::vector<T>& v, T** dev)
 }
 
 // the fine/coarse couplings of a refined domain (build_levels) on the device
-int levels_prepare(pk_ctx* h)
+int upload_segs(pk_ctx* h, const std::vector<XSeg>& segs, XSegList* out);
+
+// rows of each fine level on the device, start counts relative to the level's first row
+static int upload_runs(pk_ctx* h, int maxl, const std::vector<PRun>& pr, const std::vector<long long>& level_beg,
+                       PRunDev** d_runs, long long** d_start, std::vector<long long>& beg, std::vector<long long>& cells)
+{
+    std::vector<PRunDev> runs(pr.size());
+    std::vector<long long> start(pr.size());
+    beg.assign(level_beg.begin(), level_beg.end());
+    cells.assign(maxl + 1, 0);
+    for (int L = 1; L <= maxl; ++L) {
+        long long acc = 0;
+        for (long long r = level_beg[L]; r < level_beg[L + 1]; ++r) {
+            const PRun& s = pr[r];
+            runs[r] = PRunDev{s.fb, s.cb, s.fx, s.fy, s.fz, s.len, s.cx, s.cy, s.cz, s.px, s.py, s.pz};
+            start[r] = acc;
+            acc += s.len;
+        }
+        cells[L] = acc;
+    }
+    if (int rc = upload_vec(h, runs, d_runs)) return rc;
+    return upload_vec(h, start, d_start);
+}
+
+int levels_prepare(pk_ctx* h, const std::vector<XSeg>& segs)
 {
     const int nl = (int)h->blocks.size();
     std::vector<LBlock> lb(nl);
@@ -257,23 +287,22 @@ int levels_prepare(pk_ctx* h)
     if (!build_levels(lb, h->dom, plan, err)) return fail(h, PK_E_ARG, err);
     free_levels(h);
     const int NV = h->nplanes;
-    // prolongation rows, start counts relative to each level's first row
-    std::vector<PRunDev> runs(plan.runs.size());
-    std::vector<long long> start(plan.runs.size());
-    h->run_beg.assign(plan.run_level_beg.begin(), plan.run_level_beg.end());
-    h->run_cells.assign(plan.max_level + 1, 0);
-    for (int L = 1; L <= plan.max_level; ++L) {
-        long long acc = 0;
-        for (long long r = plan.run_level_beg[L]; r < plan.run_level_beg[L + 1]; ++r) {
-            const PRun& s = plan.runs[r];
-            runs[r] = PRunDev{s.fb, s.cb, s.fx, s.fy, s.fz, s.len, s.cx, s.cy, s.cz, s.px, s.py, s.pz};
-            start[r] = acc;
-            acc += s.len;
-        }
-        h->run_cells[L] = acc;
+    if (int rc = upload_runs(h, plan.max_level, plan.runs, plan.run_level_beg, &h->d_runs, &h->d_run_start, h->run_beg,
+                             h->run_cells))
+        return rc;
+    // the partial refreshes of the batched stage path, one per swept direction
+    const int rmax = std::max(h->pro_u.r, h->pro_b.r);
+    for (int d = 0; d < 3; ++d) {
+        if (h->dom[d] <= 1) continue;
+        PartialRefresh pr;
+        build_partial_refresh(lb, plan, segs, d, rmax, pr);
+        pk_ctx::Partial& q = h->part[d];
+        if (int rc = upload_segs(h, pr.segs, &q.segs)) return rc;
+        if (int rc = upload_runs(h, plan.max_level, pr.runs, pr.run_level_beg, &q.runs, &q.run_start, q.run_beg,
+                                 q.run_cells))
+            return rc;
+        q.ok = true;
     }
-    if (int rc = upload_vec(h, runs, &h->d_runs)) return rc;
-    if (int rc = upload_vec(h, start, &h->d_run_start)) return rc;
     // per direction: the blocks' slot tables, then in faces, then flux sources
     for (int d = 0; d < 3; ++d) {
         const FcDir& F = plan.fc[d];
@@ -384,14 +413,19 @@ bool prolong_coef(int order, ProlongCoef* k)
 }
 
 // prolong_bnd_from_coarser of every refined level, coarsest first
-int prolong_guards(pk_ctx* h)
+int prolong_guards(pk_ctx* h, int need = -1)
 {
+    const bool part = need >= 0 && h->part[need].ok;
+    const std::vector<long long>& beg = part ? h->part[need].run_beg : h->run_beg;
+    const std::vector<long long>& cnt = part ? h->part[need].run_cells : h->run_cells;
+    const PRunDev* rows = part ? h->part[need].runs : h->d_runs;
+    const long long* rstart = part ? h->part[need].run_start : h->d_run_start;
     for (int L = 1; L <= h->max_level; ++L) {
-        const long long cells = h->run_cells[L];
+        const long long cells = cnt[L];
         if (!cells) continue;
-        const long long r0 = h->run_beg[L];
-        const int nr = (int)(h->run_beg[L + 1] - r0);
-        k_prolong<<<grid1d(cells, 256), 256, 0, h->stream>>>(h->d_runs + r0, h->d_run_start + r0, nr, cells,
+        const long long r0 = beg[L];
+        const int nr = (int)(beg[L + 1] - r0);
+        k_prolong<<<grid1d(cells, 256), 256, 0, h->stream>>>(rows + r0, rstart + r0, nr, cells,
                                                              h->d_xptr[h->cur], h->nvf, h->cfg.magnetic ? 4 : 0,
                                                              h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1, h->pro_u,
                                                              h->pro_b, h->pro_b);
@@ -438,7 +472,7 @@ int exchange_prepare(pk_ctx* h)
                 all.push_back(s);
             }
         }
-        if (int rc = levels_prepare(h)) return rc;
+        if (int rc = levels_prepare(h, all)) return rc;
         PK_CUDA(h, cudaStreamSynchronize(h->stream));
         free_segs(h);
         if (int rc = upload_segs(h, all, &h->xlocal)) return rc;
@@ -512,19 +546,23 @@ int exchange_prepare(pk_ctx* h)
 
 // launch the exchange between this rank's blocks on the current state, then
 // let the host move the other ranks' halo (dir: sweep direction or -1)
-int exchange_guards(pk_ctx* h, int dir = -1)
+// need >= 0: only the guard cells the interior-trimmed stage kernel reads
+// when it next sweeps direction need (refined domains; every other guard cell
+// may stay stale until a full refresh)
+int exchange_guards(pk_ctx* h, int dir = -1, int need = -1)
 {
     if (!h->connected) return PK_OK;
     if (int rc = exchange_prepare(h)) return rc;
-    if (h->xlocal.total > 0) {
-        const int nblk = h->xlocal.n < 148 * 16 ? h->xlocal.n : 148 * 16;   // CTAs take whole segments
-        k_exchange<<<nblk, 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total, h->d_xptr[h->cur],
-                                                h->nplanes);
+    if (need >= 0 && !(h->max_level > 0 && h->part[need].ok)) need = -1;
+    const XSegList& xs = need >= 0 ? h->part[need].segs : h->xlocal;
+    if (xs.total > 0) {
+        const int nblk = xs.n < 148 * 16 ? xs.n : 148 * 16;   // CTAs take whole segments
+        k_exchange<<<nblk, 256, 0, h->stream>>>(xs.dev, xs.n, xs.total, h->d_xptr[h->cur], h->nplanes);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
     if (h->halo_cb && !h->xpeers.empty()) h->halo_cb(h->comm_ctx, dir);
-    if (h->max_level > 0) return prolong_guards(h);
+    if (h->max_level > 0) return prolong_guards(h, need);
     return PK_OK;
 }
 
@@ -752,7 +790,9 @@ int glm_scale(pk_ctx* h, double fac)
 
 // sweep(cdim) of all blocks; the step scalars are already in d_step.
 // apply_fac: the psi damping of glmdamping is folded into this sweep.
-int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double fac)
+// next_dir: the direction the following sweep of the same step takes (-1:
+// none, so the last guard refresh is complete)
+int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double fac, int next_dir = -1)
 {
     if (h->blocks.empty()) return fail(h, PK_E_STATE, "no block registered");
     const PhysOps* ops = ops_of(h);
@@ -805,7 +845,9 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
         if (h->max_level == 0)                        // refined domains overwrite every guard cell below
             for (auto& b : h->blocks)
                 if (int rc = fill_guards_block(h, b)) return rc;
-        if (int rc = exchange_guards(h, dir)) return rc;
+        // the batched stage reads two guard layers along the next stage's direction only
+        const int need = !h->stage_batched ? -1 : (s < nst ? dir : next_dir);
+        if (int rc = exchange_guards(h, dir, need)) return rc;
     }
     if (h->cfg.magnetic && apply_fac) return glm_scale_dev(h);
     return PK_OK;
@@ -844,7 +886,10 @@ int step_sweeps(pk_ctx* h, double dt, double ch, double fac)
         for (int s = 0; s < nd; ++s) {
             const int d = half == 0 ? dirs[s] : dirs[nd - 1 - s];
             const int last = h->cfg.magnetic && s == nd - 1;
-            if (int rc = sweep_impl(h, d, dt, ch, last, fac)) return rc;
+            int next = -1;                                // the sweep after this one in the same step
+            if (half == 0) next = s + 1 < nd ? dirs[s + 1] : dirs[nd - 1];
+            else if (s + 1 < nd) next = dirs[nd - 2 - s];
+            if (int rc = sweep_impl(h, d, dt, ch, last, fac, next)) return rc;
         }
         if (h->cfg.magnetic && nd == 0)
             if (int rc = glm_scale(h, fac)) return rc;

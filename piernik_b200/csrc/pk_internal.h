@@ -169,6 +169,15 @@ struct pk_ctx {
     std::vector<int> rbox_beg;                  // boxes of fine level L: [rbox_beg[L], rbox_beg[L+1])
     std::vector<long long> rbox_cells;          // coarse cells restricted from level L
     int eff_dim = 3;
+    // guard refresh before a stage of the interior-trimmed stage kernel along
+    // direction d: only the cells it reads (build_partial_refresh)
+    struct Partial {
+        pk::XSegList segs;
+        pk::PRunDev* runs = nullptr;
+        long long* run_start = nullptr;
+        std::vector<long long> run_beg, run_cells;
+        bool ok = false;
+    } part[3];
     pk_halo_fn halo_cb = nullptr;       // moves the halo of other ranks (host callback)
     pk_reduce_fn reduce_cb = nullptr;   // min / max over ranks for the time step
     void* comm_ctx = nullptr;

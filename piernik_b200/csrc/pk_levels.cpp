@@ -398,4 +398,120 @@ bool build_fill_runs(const std::vector<LBlock>& blocks, const long long dom[3], 
     return true;
 }
 
+void build_partial_refresh(const std::vector<LBlock>& blocks, const LevelPlan& plan, const std::vector<XSeg>& segs,
+                           int dir, int r, PartialRefresh& out)
+{
+    const int nb = (int)blocks.size();
+    bool has[3];
+    for (int d = 0; d < 3; ++d) has[d] = blocks[0].n[d] > 1;
+    // per block: 0 not needed, 1 in a slab, 2 needed by a prolongation stencil only
+    std::vector<std::vector<unsigned char>> need(nb);
+    std::vector<int> ext(3 * nb);
+    std::vector<char> extra(nb, 0);
+    auto at = [&](int b, int x, int y, int z) -> unsigned char& {
+        return need[b][((size_t)z * ext[3 * b + 1] + y) * ext[3 * b] + x];
+    };
+    for (int b = 0; b < nb; ++b) {
+        const LBlock& B = blocks[b];
+        for (int d = 0; d < 3; ++d) ext[3 * b + d] = B.n[d] + 2 * B.g[d];
+        need[b].assign((size_t)ext[3 * b] * ext[3 * b + 1] * ext[3 * b + 2], 0);
+        for (int side = 0; side < 2; ++side) {
+            int lo[3], hi[3];
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = B.g[d];
+                hi[d] = B.g[d] + B.n[d];
+            }
+            lo[dir] = side == 0 ? B.g[dir] - 2 : B.g[dir] + B.n[dir];
+            hi[dir] = lo[dir] + 2;
+            for (int z = lo[2]; z < hi[2]; ++z)
+                for (int y = lo[1]; y < hi[1]; ++y)
+                    for (int x = lo[0]; x < hi[0]; ++x) at(b, x, y, z) = 1;
+        }
+    }
+    // prolongation rows, finest level first: keep the needed pieces, mark their stencils' coarse cells
+    out.runs.clear();
+    out.run_level_beg.assign(plan.max_level + 2, 0);
+    std::vector<std::vector<PRun>> by_level(plan.max_level + 1);
+    for (int L = plan.max_level; L >= 1; --L) {
+        for (long long q = plan.run_level_beg[L]; q < plan.run_level_beg[L + 1]; ++q) {
+            const PRun& R = plan.runs[q];
+            int i = 0;
+            while (i < R.len) {
+                if (!at(R.fb, R.fx + i, R.fy, R.fz)) {
+                    ++i;
+                    continue;
+                }
+                int e = i;
+                while (e < R.len && at(R.fb, R.fx + e, R.fy, R.fz)) ++e;
+                PRun p = R;
+                p.fx = R.fx + i;
+                p.len = e - i;
+                p.px = (R.px + i) & 1;
+                p.cx = R.cx + ((R.px + i) >> 1);
+                by_level[L].push_back(p);
+                const int rx = has[0] ? r : 0, ry = has[1] ? r : 0, rz = has[2] ? r : 0;
+                const int x0 = p.cx - rx, x1 = R.cx + ((R.px + e - 1) >> 1) + rx;
+                const int c = R.cb;
+                for (int z = std::max(0, R.cz - rz); z <= std::min(ext[3 * c + 2] - 1, R.cz + rz); ++z)
+                    for (int y = std::max(0, R.cy - ry); y <= std::min(ext[3 * c + 1] - 1, R.cy + ry); ++y)
+                        for (int x = std::max(0, x0); x <= std::min(ext[3 * c] - 1, x1); ++x) {
+                            unsigned char& m = at(c, x, y, z);
+                            if (!m) {
+                                m = 2;
+                                extra[c] = 1;
+                            }
+                        }
+                i = e;
+            }
+        }
+    }
+    for (int L = 1; L <= plan.max_level; ++L) {
+        out.run_level_beg[L] = (long long)out.runs.size();
+        out.runs.insert(out.runs.end(), by_level[L].begin(), by_level[L].end());
+    }
+    out.run_level_beg[plan.max_level + 1] = (long long)out.runs.size();
+    // same-level segments: slab pieces as boxes, other needed cells as rows
+    out.segs.clear();
+    for (const XSeg& s : segs) {
+        const LBlock& B = blocks[s.dst];
+        for (int side = 0; side < 2; ++side) {
+            XSeg p = s;
+            bool ok = true;
+            for (int d = 0; d < 3; ++d) {
+                int lo = B.g[d], hi = B.g[d] + B.n[d];
+                if (d == dir) {
+                    lo = side == 0 ? B.g[d] - 2 : B.g[d] + B.n[d];
+                    hi = lo + 2;
+                }
+                p.lo[d] = std::max(s.lo[d], lo);
+                p.hi[d] = std::min(s.hi[d], hi);
+                ok = ok && p.lo[d] < p.hi[d];
+            }
+            if (ok) out.segs.push_back(p);
+        }
+        if (!extra[s.dst]) continue;
+        for (int z = s.lo[2]; z < s.hi[2]; ++z)
+            for (int y = s.lo[1]; y < s.hi[1]; ++y) {
+                int x = s.lo[0];
+                while (x < s.hi[0]) {
+                    if (at(s.dst, x, y, z) != 2) {
+                        ++x;
+                        continue;
+                    }
+                    int e = x;
+                    while (e < s.hi[0] && at(s.dst, e, y, z) == 2) ++e;
+                    XSeg p = s;
+                    p.lo[0] = x;
+                    p.hi[0] = e;
+                    p.lo[1] = y;
+                    p.hi[1] = y + 1;
+                    p.lo[2] = z;
+                    p.hi[2] = z + 1;
+                    out.segs.push_back(p);
+                    x = e;
+                }
+            }
+    }
+}
+
 }  // namespace pk

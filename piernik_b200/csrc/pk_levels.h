@@ -22,6 +22,8 @@
 #include <string>
 #include <vector>
 
+#include "pk_exchange.h"
+
 namespace pk {
 
 struct LBlock {
@@ -90,5 +92,23 @@ bool build_levels(const std::vector<LBlock>& blocks, const long long dom[3], Lev
 // in no interior of that level.
 bool build_fill_runs(const std::vector<LBlock>& blocks, const long long dom[3], int target, std::vector<PRun>& runs,
                      std::string& err);
+
+// The guard refresh one RK stage of the interior-trimmed stage kernel needs
+// before it sweeps direction dir: that kernel reads, of each block, only the
+// two guard layers on either side of the interior along dir, across the
+// interior (the slabs), and a prolonged slab cell reads the coarser block's
+// cells within the stencil range r of its parent, guard cells included,
+// which must be refreshed too (closed downwards level by level).  Every
+// other guard cell may stay stale until a full refresh.  From the full
+// plan (same-level segments segs, prolongation rows plan.runs) keeps the
+// segment pieces and row pieces that write needed cells: slab pieces as
+// boxes, the few other needed cells as rows.
+struct PartialRefresh {
+    std::vector<XSeg> segs;
+    std::vector<PRun> runs;                 // by the fine block's level
+    std::vector<long long> run_level_beg;   // as LevelPlan::run_level_beg
+};
+void build_partial_refresh(const std::vector<LBlock>& blocks, const LevelPlan& plan, const std::vector<XSeg>& segs,
+                           int dir, int r, PartialRefresh& out);
 
 }  // namespace pk
