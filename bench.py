@@ -438,7 +438,7 @@ def batched_arm(args):
     stream = torch.cuda.ExternalStream(sim.stream)
     # launch shape of the batched stage kernel: one captured step each, then the fastest
     tune = {}
-    for v in (0, 1, 2):
+    for v in range(4):
         sim.set_stage_variant(v)
         sim.run(1)
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -210,7 +210,7 @@ int pk_use_graph(pk_handle h, int32_t enable);
 
 /* Launch-bound variant of the batched stage kernel that sweeps many blocks
  * stage by stage (refined or non-periodic connected domains): 0 = 320
- * threads x 1 CTA per SM (default), 1 = 128 x 3, 2 = 192 x 2.  Used by the
+ * threads x 1 CTA per SM (default), 1 = 128 x 3, 2 = 192 x 2, 3 = 384 x 1.  Used by the
  * tuning of the refined workload; WENO3 always runs variant 0. */
 int pk_set_stage_variant(pk_handle h, int32_t variant);
 

@@ -1516,7 +1516,9 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out)
     a.ib = h->ib;
     if (nb > 1) {
         if (int rc = build_batch(h)) return rc;
-        dim3 grid(64, nb);
+        long long most = 1;                               // about four cells per thread in the largest block
+        for (auto& b : h->blocks) most = std::max(most, ((long long)b.n[0] * b.n[1] * b.n[2] + 1023) / 1024);
+        dim3 grid((unsigned)std::min<long long>(most, 1024), nb);
         k_cfl_blocks<<<grid, 256, 0, h->stream>>>(h->d_desc[h->cur], a, h->d_red);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;

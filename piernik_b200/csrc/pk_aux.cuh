@@ -49,12 +49,21 @@ PK_DEV void cfl_block(const BoxGeom& b, const double* __restrict__ u, const CflA
     for (int f = 0; f < 3; ++f)
 #pragma unroll
         for (int d = 0; d < 4; ++d) cm[f][d] = small;
+    const bool small_block = ncell <= 0x7fffffffLL;            // 32-bit index arithmetic suffices
     for (long long c = first; c < ncell; c += stride) {
         if (leaf && !leaf[c]) continue;
-        const int i = (int)(c % b.n[0]);
-        const long long r = c / b.n[0];
-        const int j = (int)(r % b.n[1]);
-        const int k = (int)(r / b.n[1]);
+        int i, j, k;
+        if (small_block) {
+            const int ci = (int)c, r = ci / b.n[0];
+            i = ci - r * b.n[0];
+            j = r % b.n[1];
+            k = r / b.n[1];
+        } else {
+            i = (int)(c % b.n[0]);
+            const long long r = c / b.n[0];
+            j = (int)(r % b.n[1]);
+            k = (int)(r / b.n[1]);
+        }
         const long long off = cell_index(b, i + b.g[0], j + b.g[1], k + b.g[2]);
         double pmag = 0.0;
         if (a.magnetic) {
@@ -131,6 +140,7 @@ static __global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a,
 static __global__ void k_cfl_blocks(const BlockDesc* __restrict__ blocks, CflArgs a, unsigned long long* __restrict__ out)
 {
     const BlockDesc d = blocks[blockIdx.y];
+    if ((long long)blockIdx.x * blockDim.x >= (long long)d.n[0] * d.n[1] * d.n[2]) return;   // CTAs a smaller block does not need
     BoxGeom b;
     for (int k = 0; k < 3; ++k) {
         b.ext[k] = d.ext[k];

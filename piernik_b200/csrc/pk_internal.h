@@ -23,9 +23,9 @@ constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512};
 constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1};
 constexpr int STAGE_MAXT = 320;       // threads per CTA of the stage kernel
 // launch-bound variants of the batched stage kernel (threads per CTA, CTAs per SM)
-constexpr int NSTAGE_VARIANT = 3;
-constexpr int SV_T[NSTAGE_VARIANT] = {320, 128, 192};
-constexpr int SV_B[NSTAGE_VARIANT] = {1, 3, 2};
+constexpr int NSTAGE_VARIANT = 4;
+constexpr int SV_T[NSTAGE_VARIANT] = {320, 128, 192, 384};
+constexpr int SV_B[NSTAGE_VARIANT] = {1, 3, 2, 1};
 constexpr int W3_VARIANT = 2;          // interpol_str = 'weno3' runs this launch-bound variant only
 
 struct Block {

@@ -53,6 +53,7 @@ auto stage_batched_variant(int v, bool w3, bool fc) -> decltype(&k_stage_batched
     switch (v) {
     case 1: return fc ? k_stage_batched<PH, 128, 3, false, true> : k_stage_batched<PH, 128, 3, false, false>;
     case 2: return fc ? k_stage_batched<PH, 192, 2, false, true> : k_stage_batched<PH, 192, 2, false, false>;
+    case 3: return fc ? k_stage_batched<PH, 384, 1, false, true> : k_stage_batched<PH, 384, 1, false, false>;
     default: return fc ? k_stage_batched<PH, 320, 1, false, true> : k_stage_batched<PH, 320, 1, false, false>;
     }
 }

@@ -470,36 +470,57 @@ void build_partial_refresh(const std::vector<LBlock>& blocks, const LevelPlan& p
         out.runs.insert(out.runs.end(), by_level[L].begin(), by_level[L].end());
     }
     out.run_level_beg[plan.max_level + 1] = (long long)out.runs.size();
-    // same-level segments: slab pieces as boxes, other needed cells as rows
+    // same-level segments: slab pieces as boxes, other needed cells as rows.
+    // Along x the slab pieces take the whole guard depth: two-cell rows would
+    // leave every memory sector half used, and the extra cells receive the
+    // values a complete refresh gives them.
+    auto slab = [&](int b, int side, int lo[3], int hi[3]) {
+        const LBlock& B = blocks[b];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = B.g[d];
+            hi[d] = B.g[d] + B.n[d];
+        }
+        const int w = dir == 0 ? B.g[0] : 2;
+        lo[dir] = side == 0 ? B.g[dir] - w : B.g[dir] + B.n[dir];
+        hi[dir] = lo[dir] + w;
+    };
+    auto in_slab = [&](int b, int x, int y, int z) {
+        const int c[3] = {x, y, z};
+        for (int side = 0; side < 2; ++side) {
+            int lo[3], hi[3];
+            slab(b, side, lo, hi);
+            bool in = true;
+            for (int d = 0; d < 3; ++d) in = in && c[d] >= lo[d] && c[d] < hi[d];
+            if (in) return true;
+        }
+        return false;
+    };
     out.segs.clear();
     for (const XSeg& s : segs) {
-        const LBlock& B = blocks[s.dst];
         for (int side = 0; side < 2; ++side) {
             XSeg p = s;
+            int lo[3], hi[3];
+            slab(s.dst, side, lo, hi);
             bool ok = true;
             for (int d = 0; d < 3; ++d) {
-                int lo = B.g[d], hi = B.g[d] + B.n[d];
-                if (d == dir) {
-                    lo = side == 0 ? B.g[d] - 2 : B.g[d] + B.n[d];
-                    hi = lo + 2;
-                }
-                p.lo[d] = std::max(s.lo[d], lo);
-                p.hi[d] = std::min(s.hi[d], hi);
+                p.lo[d] = std::max(s.lo[d], lo[d]);
+                p.hi[d] = std::min(s.hi[d], hi[d]);
                 ok = ok && p.lo[d] < p.hi[d];
             }
             if (ok) out.segs.push_back(p);
         }
         if (!extra[s.dst]) continue;
+        auto closure_only = [&](int x, int y, int z) { return at(s.dst, x, y, z) == 2 && !in_slab(s.dst, x, y, z); };
         for (int z = s.lo[2]; z < s.hi[2]; ++z)
             for (int y = s.lo[1]; y < s.hi[1]; ++y) {
                 int x = s.lo[0];
                 while (x < s.hi[0]) {
-                    if (at(s.dst, x, y, z) != 2) {
+                    if (!closure_only(x, y, z)) {
                         ++x;
                         continue;
                     }
                     int e = x;
-                    while (e < s.hi[0] && at(s.dst, e, y, z) == 2) ++e;
+                    while (e < s.hi[0] && closure_only(e, y, z)) ++e;
                     XSeg p = s;
                     p.lo[0] = x;
                     p.hi[0] = e;

@@ -232,7 +232,7 @@ class Simulation:
 
     def set_stage_variant(self, variant: int) -> None:
         """Launch-bound variant of the batched stage kernel (0: 320 x 1,
-        1: 128 x 3, 2: 192 x 2 threads x CTAs per SM)."""
+        1: 128 x 3, 2: 192 x 2, 3: 384 x 1 threads x CTAs per SM)."""
         self._chk(self.lib.pk_set_stage_variant(self.h, variant), "pk_set_stage_variant")
 
     def use_graph(self, enable: bool = True) -> None:

@@ -72,7 +72,7 @@ def test_refined_single_sweeps(gpu_lib, phys):
     sim.close()
 
 
-@pytest.mark.parametrize("name", sorted(CASES) + ["mhd-3d-moncen+graph", "hd-3d+v1", "mhd-3d-moncen+v2"])
+@pytest.mark.parametrize("name", sorted(CASES) + ["mhd-3d-moncen+graph", "hd-3d+v1", "mhd-3d-moncen+v2", "mhd-3d-moncen+v3"])
 def test_refined_matches_oracle(gpu_lib, name):
     graph = name.endswith("+graph")
     c = CASES[name.split("+")[0]]
