@@ -1,5 +1,6 @@
 // Host harness of the refined-domain planner (pk_levels.cpp) for the CPU
 // tests: builds a plan and hands its tables out through plain C calls.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -8,6 +9,8 @@
 
 static pk::LevelPlan g_plan;
 static std::vector<pk::PRun> g_fill;
+static pk::PartialRefresh g_part;
+static std::vector<pk::LBlock> g_blocks;
 
 static std::vector<pk::LBlock> blocks_of(int nb, const int* level, const int* n, const int* g, const long long* off)
 {
@@ -51,6 +54,7 @@ int lv_build(int nb, const int* level, const int* n, const int* g, const long lo
              char* err, int errlen)
 {
     std::vector<pk::LBlock> b = blocks_of(nb, level, n, g, off);
+    g_blocks = b;
     std::string e;
     if (!pk::build_levels(b, dom, g_plan, e)) {
         if (err && errlen > 0) {
@@ -63,6 +67,74 @@ int lv_build(int nb, const int* level, const int* n, const int* g, const long lo
 }
 
 long long lv_nruns() { return (long long)g_plan.runs.size(); }
+
+static std::vector<pk::XSeg> g_segs;
+
+// same-level segments of every level of the blocks of the last lv_build
+// (periodic in every direction with extent), as the library plans them
+long long lv_segs(const long long* dom)
+{
+    g_segs.clear();
+    int maxl = 0;
+    for (const pk::LBlock& b : g_blocks) maxl = std::max(maxl, b.level);
+    const int per[3] = {1, 1, 1};
+    for (int L = 0; L <= maxl; ++L) {
+        std::vector<int> ids;
+        std::vector<pk::XBlock> xb;
+        for (int i = 0; i < (int)g_blocks.size(); ++i) {
+            if (g_blocks[i].level != L) continue;
+            pk::XBlock x;
+            for (int d = 0; d < 3; ++d) {
+                x.n[d] = g_blocks[i].n[d];
+                x.g[d] = g_blocks[i].g[d];
+                x.off[d] = g_blocks[i].off[d];
+            }
+            ids.push_back(i);
+            xb.push_back(x);
+        }
+        long long dl[3];
+        for (int d = 0; d < 3; ++d) dl[d] = dom[d] > 1 ? dom[d] << L : 1;
+        std::vector<pk::XSeg> segs;
+        std::string err;
+        if (!pk::build_exchange(xb, dl, per, segs, err)) return -1;
+        for (pk::XSeg s : segs) {
+            s.dst = ids[s.dst];
+            s.src = ids[s.src];
+            g_segs.push_back(s);
+        }
+    }
+    return (long long)g_segs.size();
+}
+
+void lv_seg(long long i, int* out)
+{
+    const pk::XSeg& s = g_segs[i];
+    const int v[11] = {s.dst, s.src, s.lo[0], s.lo[1], s.lo[2], s.hi[0], s.hi[1], s.hi[2], s.shift[0], s.shift[1], s.shift[2]};
+    std::memcpy(out, v, sizeof(v));
+}
+
+// the partial refresh of direction dir over the plan and segments built last
+long long lv_partial(int dir, int r)
+{
+    pk::build_partial_refresh(g_blocks, g_plan, g_segs, dir, r, g_part);
+    return (long long)g_part.segs.size();
+}
+
+long long lv_partial_nruns() { return (long long)g_part.runs.size(); }
+
+void lv_partial_seg(long long i, int* out)
+{
+    const pk::XSeg& s = g_part.segs[i];
+    const int v[11] = {s.dst, s.src, s.lo[0], s.lo[1], s.lo[2], s.hi[0], s.hi[1], s.hi[2], s.shift[0], s.shift[1], s.shift[2]};
+    std::memcpy(out, v, sizeof(v));
+}
+
+void lv_partial_run(long long i, int* out)
+{
+    const pk::PRun& r = g_part.runs[i];
+    const int v[12] = {r.fb, r.cb, r.fx, r.fy, r.fz, r.len, r.cx, r.cy, r.cz, r.px, r.py, r.pz};
+    std::memcpy(out, v, sizeof(v));
+}
 
 void lv_run(long long i, int* out)
 {

@@ -25,6 +25,7 @@ SRC = os.path.join(HERE, "native", "levels_harness.cpp")
 PLAN = os.path.join(HERE, "..", "piernik_b200", "csrc", "pk_levels.cpp")
 HDR = os.path.join(HERE, "..", "piernik_b200", "csrc", "pk_levels.h")
 LIB = os.path.join(HERE, "native", "liblevels_harness.so")
+XPLAN = os.path.join(HERE, "..", "piernik_b200", "csrc", "pk_exchange.cpp")
 
 DOM3 = (16, 16, 16)
 REG3 = [((8, 8, 8), (24, 24, 24)), ((24, 24, 24), (40, 40, 40))]
@@ -42,8 +43,8 @@ def case(phys, dom=DOM3, regions=REG3, lim="vanleer", seed=3):
 
 @pytest.fixture(scope="module")
 def hlib():
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in (SRC, PLAN, HDR)):
-        subprocess.check_call(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", LIB, SRC, PLAN])
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in (SRC, PLAN, HDR, XPLAN)):
+        subprocess.check_call(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", LIB, SRC, PLAN, XPLAN])
     L = C.CDLL(LIB)
     L.lv_nruns.restype = C.c_longlong
     L.lv_run.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
@@ -289,3 +290,92 @@ def test_regrid_oracle_restores_by_restriction(oracle_lib):
                 assert np.all(np.abs(now - was) <= 4e-16 * np.abs(was)), i
             changed = np.any(ob.u != before[i][0], axis=-1)
             assert changed.sum() <= 8 * 8 * 8 // 8 * 2, i      # only the cells under the two new blocks
+
+
+def _cells_of_segs(rows):
+    """(block, x, y, z) -> (src block, sx, sy, sz) of copy rows (dst, src, lo, hi, shift)"""
+    out = {}
+    for dst, src, lx, ly, lz, hx, hy, hz, sx, sy, sz in rows:
+        for z in range(lz, hz):
+            for y in range(ly, hy):
+                for x in range(lx, hx):
+                    out[(dst, x, y, z)] = ("copy", src, x + sx, y + sy, z + sz)
+    return out
+
+
+def _cells_of_runs(rows):
+    out = {}
+    for fb, cb, fx, fy, fz, ln, cx, cy, cz, px, py, pz in rows:
+        for i in range(ln):
+            out[(fb, fx + i, fy, fz)] = ("prolong", cb, cx + ((px + i) >> 1), cy, cz, (px + i) & 1, py, pz)
+    return out
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("r", [1, 2])
+def test_partial_refresh_plan(hlib, oracle_lib, dim, r):
+    """The guard refresh before a stage along dir writes, with the sources the
+    complete refresh uses, every guard cell the stage reads (two layers along
+    dir, across the interior) and every coarse guard cell within r of a
+    prolonged cell's parent; nothing else is written differently."""
+    dom, reg = (DOM3, REG3) if dim == 3 else (DOM2, REG2)
+    blocks = case("mhd", dom, reg)
+    build(hlib, blocks, dom)
+    dm = (C.c_longlong * 3)(*dom)
+    ns = hlib.lv_segs(dm)
+    assert ns > 0
+    row = (C.c_int * 12)()
+    hlib.lv_seg.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
+    full = {}
+    for i in range(ns):
+        hlib.lv_seg(i, row)
+        full.update(_cells_of_segs([tuple(row[:11])]))
+    runs = []
+    for i in range(hlib.lv_nruns()):
+        hlib.lv_run(i, row)
+        runs.append(tuple(row[:12]))
+    full.update(_cells_of_runs(runs))
+    hlib.lv_partial.restype = C.c_longlong
+    hlib.lv_partial_nruns.restype = C.c_longlong
+    hlib.lv_partial_seg.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
+    hlib.lv_partial_run.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
+    has = [d > 1 for d in dom]
+    for dr in [d for d in range(3) if has[d]]:
+        nps = hlib.lv_partial(dr, r)
+        part = {}
+        for i in range(nps):
+            hlib.lv_partial_seg(i, row)
+            part.update(_cells_of_segs([tuple(row[:11])]))
+        pruns = []
+        for i in range(hlib.lv_partial_nruns()):
+            hlib.lv_partial_run(i, row)
+            pruns.append(tuple(row[:12]))
+        part.update(_cells_of_runs(pruns))
+        assert len(part) < len(full)
+        for key, src in part.items():                       # the same source as the complete refresh
+            assert full[key] == src, key
+        for b, (s, L, off, *_) in enumerate(blocks):        # every slab cell
+            g, n = s.guards, s.n
+            for side in (0, 1):
+                lo = [g[d] for d in range(3)]
+                hi = [g[d] + n[d] for d in range(3)]
+                lo[dr] = g[dr] - 2 if side == 0 else g[dr] + n[dr]
+                hi[dr] = lo[dr] + 2
+                for z in range(lo[2], hi[2]):
+                    for y in range(lo[1], hi[1]):
+                        for x in range(lo[0], hi[0]):
+                            if (b, x, y, z) in full:
+                                assert (b, x, y, z) in part, (dr, b, x, y, z)
+        for key, src in part.items():                       # the prolongation stencils' coarse guard cells
+            if src[0] != "prolong":
+                continue
+            _, cb, cx, cy, cz = src[:5]
+            sc = blocks[cb][0]
+            rr = [r if has[d] else 0 for d in range(3)]
+            for z in range(cz - rr[2], cz + rr[2] + 1):
+                for y in range(cy - rr[1], cy + rr[1] + 1):
+                    for x in range(cx - rr[0], cx + rr[0] + 1):
+                        c = (x, y, z)
+                        inner = all(sc.guards[d] <= c[d] < sc.guards[d] + sc.n[d] for d in range(3))
+                        if not inner and (cb, x, y, z) in full:
+                            assert (cb, x, y, z) in part, (dr, key, cb, c)
