@@ -131,13 +131,17 @@ PK_DEV void cfl_block(const BoxGeom& b, const double* __restrict__ u, const CflA
     }
 }
 
-static __global__ void k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsigned long long* __restrict__ out)
+// three CTAs of 256 threads per SM: the reduction is latency-bound (dependent
+// division and square-root chains), so resident warps matter more than registers
+static __global__ void __launch_bounds__(256, 3)
+k_cfl(BoxGeom b, const double* __restrict__ u, CflArgs a, unsigned long long* __restrict__ out)
 {
     cfl_block(b, u, a, out, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
 // the same over a table of blocks: blockIdx.y picks the block, out has 12 slots per block
-static __global__ void k_cfl_blocks(const BlockDesc* __restrict__ blocks, CflArgs a, unsigned long long* __restrict__ out)
+static __global__ void __launch_bounds__(256, 3)
+k_cfl_blocks(const BlockDesc* __restrict__ blocks, CflArgs a, unsigned long long* __restrict__ out)
 {
     const BlockDesc d = blocks[blockIdx.y];
     if ((long long)blockIdx.x * blockDim.x >= (long long)d.n[0] * d.n[1] * d.n[2]) return;   // CTAs a smaller block does not need
