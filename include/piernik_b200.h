@@ -175,7 +175,9 @@ int pk_time_step(pk_handle h, double* dt_out);
  * (every stage: the face fluxes of all directions from the same state, the
  * x, y, z flux differences applied in turn, sources and floors;
  * unsplit_sweeps.F90:104-189), glmdamping over dt/2.  The unsplit scheme
- * runs on single or independent (unconnected) blocks. */
+ * runs on single, independent, connected and refined blocks of one rank
+ * (refined: the fine/coarse flux replacement of fc_fluxes_unsplit.F90 and
+ * the guard update of each stage's array, levels as the split scheme). */
 int pk_fluid_update(pk_handle h);
 
 /* nsteps iterations of the reference main loop body (time_step +

@@ -254,13 +254,16 @@ class AmrOracle:
                 acc = acc + self._tabs[(i, d)]["out_flx"][s][pen]
             self._tabs[(j, d)]["in_flx"][side][cpen] = scale * acc
 
-    def fill_guards(self):
+    def fill_guards(self, half=False):
+        """update_boundaries of u, b, psi (of uh, bh, psih when ``half``: the
+        unsplit scheme's first-stage arrays)"""
+        nu, nb, npsi = ("uh", "bh", "psih") if half else ("u", "b", "psi")
         for i, dst, j, src in self.copies:
             A, B = self.blocks[i], self.blocks[j]
-            A.u[dst] = B.u[src]
+            getattr(A, nu)[dst] = getattr(B, nu)[src]
             if self.mag:
-                A.b[dst] = B.b[src]
-                A.psi[dst] = B.psi[src]
+                getattr(A, nb)[dst] = getattr(B, nb)[src]
+                getattr(A, npsi)[dst] = getattr(B, npsi)[src]
         s0 = self.setup0
         ofl = s0.ord_fluid_prolong if s0.ord_fluid_prolong in (0, 1) else 0
         ku, kb = PROLONG[ofl], PROLONG[s0.ord_mag_prolong]
@@ -271,14 +274,16 @@ class AmrOracle:
                 if lev != L:
                     continue
                 A, B = self.blocks[i], self.blocks[j]
+                Au, Bu = getattr(A, nu), getattr(B, nu)
                 if ku[1] == 0:
-                    A.u[dst] = B.u[cs[2], cs[1], cs[0]]
+                    Au[dst] = Bu[cs[2], cs[1], cs[0]]
                 else:
-                    for v in range(A.u.shape[-1]):
-                        A.u[dst + (v,)] = pro3(ku, B.u[..., v], cs, par)
+                    for v in range(Au.shape[-1]):
+                        Au[dst + (v,)] = pro3(ku, Bu[..., v], cs, par)
                 if not self.mag:
                     continue
-                fields = [(A.b[..., c], B.b[..., c]) for c in range(3)] + [(A.psi, B.psi)]
+                Ab, Bb = getattr(A, nb), getattr(B, nb)
+                fields = [(Ab[..., c], Bb[..., c]) for c in range(3)] + [(getattr(A, npsi), getattr(B, npsi))]
                 for fa, fb in fields:
                     fa[dst] = pro3(kb, fb, cs, par)
 
@@ -424,6 +429,29 @@ class AmrOracle:
                     self._restrict(d, L - 1)
             self.fill_guards()
 
+    def unsplit_sweep(self, dt, ch):
+        """unsplit_sweep (unsplit_sweeps.F90:104-189) over the levels: each
+        stage solves the finest level first -- every block's face fluxes of
+        all directions with the ext_fluxes hooks, their application and
+        sources -- restricting a level's boundary fluxes into the next coarser
+        level before it, then updates the boundaries of the array the stage
+        wrote (uh, bh, psih after RK2_1)."""
+        lib = O.lib()
+        nst = 1 if self.setup0.integration_order == 1 else 2
+        for st in range(1, nst + 1):
+            for L in range(self.maxl, -1, -1):
+                for i, ob in enumerate(self.blocks):
+                    if self.level[i] != L:
+                        continue
+                    rc = lib.o_unsplit_stage(C.byref(ob.cfg), C.byref(ob.blk), st, dt, ch)
+                    if rc:
+                        raise RuntimeError(f"o_unsplit_stage failed: {rc}")
+                if L > 0:
+                    for d in range(3):
+                        if self.has[d]:
+                            self._restrict(d, L - 1)
+            self.fill_guards(half=(nst == 2 and st == 1))
+
     def time_step(self):
         lib = O.lib()
         arr = (C.POINTER(O.OBlock) * len(self.blocks))(*[C.pointer(b.blk) for b in self.blocks])
@@ -431,11 +459,40 @@ class AmrOracle:
         if rc:
             raise RuntimeError(f"o_time_step_multi failed: {rc}")
 
+    def _glm_fac(self, dt):
+        cfg = self.blocks[0].cfg
+        f = 0.0
+        for b in self.blocks:
+            dl = [b.setup.dl[e] for e in range(3) if b.setup.n[e] > 1]
+            if dl:
+                f = max(f, (cfg.glm_alpha * self.state.chspeed) / (min(dl) / dt))
+        return math.exp(-f)
+
+    def fluid_update_unsplit(self):
+        """fluid_update_unsplit (unsplit_fluidupdate.F90:45-126) over all blocks"""
+        st = self.state
+        dt = st.dt
+        cfg = self.blocks[0].cfg
+        lib = O.lib()
+        fac = 1.0
+        if self.mag:
+            st.chspeed = min(lib.o_chspeed(C.byref(cfg), C.byref(b.blk), dt) for b in self.blocks)
+            fac = self._glm_fac(dt / 2.0)
+            for b in self.blocks:
+                lib.o_glm_apply(C.byref(cfg), C.byref(b.blk), fac)
+        st.t = st.t + dt
+        self.unsplit_sweep(dt, st.chspeed)
+        if self.mag:
+            for b in self.blocks:
+                lib.o_glm_apply(C.byref(cfg), C.byref(b.blk), fac)
+
     def fluid_update(self):
         st = self.state
         dt = st.dt
         cfg = self.blocks[0].cfg
         lib = O.lib()
+        if self.setup0.solver == "unsplit":
+            return self.fluid_update_unsplit()
         if self.mag:
             st.chspeed = min(lib.o_chspeed(C.byref(cfg), C.byref(b.blk), dt) for b in self.blocks)
             f = 0.0

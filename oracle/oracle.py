@@ -133,6 +133,7 @@ def lib():
         L.o_nvar.argtypes = [P]
         L.o_run_multi.argtypes = [P, C.POINTER(B), C.c_int, S, C.c_int]
         L.o_time_step_multi.argtypes = [P, C.POINTER(B), C.c_int, S]
+        L.o_unsplit_stage.argtypes = [P, B, C.c_int, C.c_double, C.c_double]
         L.o_set_threads.argtypes = [C.c_int]
         L.o_run_fixed.argtypes = [P, B, S, C.POINTER(C.c_double), C.c_int]
         L.o_cfl_max.argtypes = [P]

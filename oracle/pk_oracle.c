@@ -569,6 +569,9 @@ static void o_work_free(o_work *w)
     free(w->qr); free(w->bl); free(w->br); free(w->flx); free(w->mflx); free(w->dq);
 }
 
+/* pdims (constants.F90:127-128): ORTHO1/ORTHO2 for each sweep direction */
+static const int ORTHO[3][2] = { {1, 2}, {2, 0}, {0, 1} };
+
 /* the ext_fluxes of one pencil: faces replaced (li, ri; -1 none) and faces
  * recorded (lo, ro; -1 none) with their flux vectors */
 typedef struct o_pfc {
@@ -589,6 +592,36 @@ static void o_pfc_face(const o_lay *L, int mag, int m, o_work *w, int face, cons
             if (in) w->mflx[(size_t)c * m + face] = in[nv + c];
             if (out) out[nv + c] = w->mflx[(size_t)c * m + face];
         }
+}
+
+/* the ext_fluxes of pencil (i1, i2) (guard-inclusive ortho indices) along
+ * ddim from the block's hook tables (cg%set_fluxpointers); 0 when the block
+ * has none along ddim */
+static int o_pfc_for(const o_block *blk, int ddim, int i1, int i2, const int g[3], int nv, int mag, o_pfc *pf)
+{
+    const int o1 = ORTHO[ddim][0], o2 = ORTHO[ddim][1];
+    const o_eflx *ef = blk->eflx[ddim];
+    *pf = (o_pfc){-1, -1, -1, -1, NULL, NULL, NULL, NULL};
+    if (!ef) return 0;
+    const size_t pen = (size_t)(i1 - g[o1]) + (size_t)blk->n[o1] * (size_t)(i2 - g[o2]);
+    const size_t fw = (size_t)nv + (mag ? 4 : 0);
+    if (ef->in_face[0] && ef->in_face[0][pen] >= 0) {
+        pf->li = ef->in_face[0][pen];
+        pf->fli = ef->in_flx[0] + pen * fw;
+    }
+    if (ef->in_face[1] && ef->in_face[1][pen] >= 0) {
+        pf->ri = ef->in_face[1][pen];
+        pf->fri = ef->in_flx[1] + pen * fw;
+    }
+    if (ef->out_on[0] && ef->out_on[0][pen]) {
+        pf->lo = g[ddim] - 1;
+        pf->flo = ef->out_flx[0] + pen * fw;
+    }
+    if (ef->out_on[1] && ef->out_on[1][pen]) {
+        pf->ro = g[ddim] + blk->n[ddim] - 1;
+        pf->fro = ef->out_flx[1] + pen * fw;
+    }
+    return 1;
 }
 
 /* interpol + riemann_wrap (solve_cg_riemann.F90:346-351): the face fluxes
@@ -723,8 +756,6 @@ static void o_care_for_positives(const o_cfg *cfg, const o_lay *L, int n, o_work
 /* Block-level stage: solve_cg_ub / solve_cg_u                         */
 /* ------------------------------------------------------------------ */
 
-/* pdims (constants.F90:127-128): ORTHO1/ORTHO2 for each sweep direction */
-static const int ORTHO[3][2] = { {1, 2}, {2, 0}, {0, 1} };
 
 int o_solve_cg(const o_cfg *cfg, o_block *blk, int ddim, int istep, double dt, double ch)
 {
@@ -779,29 +810,9 @@ int o_solve_cg(const o_cfg *cfg, o_block *blk, int ddim, int istep, double dt, d
                         w.b1[3 * (size_t)n + i] = blk->psi[cell];
                     }
                 }
-                o_pfc pf = {-1, -1, -1, -1, NULL, NULL, NULL, NULL};
-                const o_eflx *ef = blk->eflx[ddim];
-                if (ef) {
-                    const size_t pen = (size_t)(i1 - g[o1]) + (size_t)blk->n[o1] * (size_t)(i2 - g[o2]);
-                    const size_t fw = (size_t)nv + (mag ? 4 : 0);
-                    if (ef->in_face[0] && ef->in_face[0][pen] >= 0) {
-                        pf.li = ef->in_face[0][pen];
-                        pf.fli = ef->in_flx[0] + pen * fw;
-                    }
-                    if (ef->in_face[1] && ef->in_face[1][pen] >= 0) {
-                        pf.ri = ef->in_face[1][pen];
-                        pf.fri = ef->in_flx[1] + pen * fw;
-                    }
-                    if (ef->out_on[0] && ef->out_on[0][pen]) {
-                        pf.lo = g[ddim] - 1;
-                        pf.flo = ef->out_flx[0] + pen * fw;
-                    }
-                    if (ef->out_on[1] && ef->out_on[1][pen]) {
-                        pf.ro = g[ddim] + blk->n[ddim] - 1;
-                        pf.fro = ef->out_flx[1] + pen * fw;
-                    }
-                }
-                o_pencil_solve(cfg, &L, n, dtodx, ch, &w, ef ? &pf : NULL);
+                o_pfc pf;
+                const int has_ef = o_pfc_for(blk, ddim, i1, i2, g, nv, mag, &pf);
+                o_pencil_solve(cfg, &L, n, dtodx, ch, &w, has_ef ? &pf : NULL);
                 o_internal_sources(&L, n, &w);
                 o_care_for_positives(cfg, &L, n, &w, &dnneg, &eineg);
                 /* transpose back (:225-227) */
@@ -1357,6 +1368,16 @@ int o_unsplit_stage(const o_cfg *cfg, o_block *blk, int istep, double dt, double
                     const size_t base = (size_t)i1 * cst[o1] + (size_t)i2 * cst[o2];
                     o_load_pencil(&L, mag, cst, n, ddim, base, su, sb, sp, &w);
                     o_pencil_fluxes(cfg, &L, n, ch, &w);
+                    /* ext_fluxes (unsplit_mag_modules.F90:195-204, solve_cg_unsplit.F90:182-183):
+                     * li, ri replace, then lo, ro record */
+                    o_pfc pf;
+                    if (o_pfc_for(blk, ddim, i1, i2, g, nv, mag, &pf)) {
+                        const int m = n - 1;
+                        if (pf.li >= 0) o_pfc_face(&L, mag, m, &w, pf.li, pf.fli, NULL);
+                        if (pf.ri >= 0) o_pfc_face(&L, mag, m, &w, pf.ri, pf.fri, NULL);
+                        if (pf.lo >= 0) o_pfc_face(&L, mag, m, &w, pf.lo, NULL, pf.flo);
+                        if (pf.ro >= 0) o_pfc_face(&L, mag, m, &w, pf.ro, NULL, pf.fro);
+                    }
                     /* pflux(:, 1) = 0, pflux(:, i) = flux(i-1): the flux through the left face of cell i */
                     for (int i = 1; i < n; ++i) {
                         double *fc = F + ((size_t)ddim * ncell + base + (size_t)i * cst[ddim]) * fw;

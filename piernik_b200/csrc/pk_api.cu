@@ -413,7 +413,7 @@ bool prolong_coef(int order, ProlongCoef* k)
 }
 
 // prolong_bnd_from_coarser of every refined level, coarsest first
-int prolong_guards(pk_ctx* h, int need = -1)
+int prolong_guards(pk_ctx* h, int need = -1, int parity = -1)
 {
     const bool part = need >= 0 && h->part[need].ok;
     const std::vector<long long>& beg = part ? h->part[need].run_beg : h->run_beg;
@@ -426,7 +426,8 @@ int prolong_guards(pk_ctx* h, int need = -1)
         const long long r0 = beg[L];
         const int nr = (int)(beg[L + 1] - r0);
         k_prolong<<<grid1d(cells, 256), 256, 0, h->stream>>>(rows + r0, rstart + r0, nr, cells,
-                                                             h->d_xptr[h->cur], h->nvf, h->cfg.magnetic ? 4 : 0,
+                                                             h->d_xptr[parity < 0 ? h->cur : parity], h->nvf,
+                                                             h->cfg.magnetic ? 4 : 0,
                                                              h->dom[0] > 1, h->dom[1] > 1, h->dom[2] > 1, h->pro_u,
                                                              h->pro_b, h->pro_b);
         PK_CUDA(h, cudaGetLastError());
@@ -1633,11 +1634,9 @@ static int unsplit_sweep(pk_ctx* h)
     const PhysOps* ops = ops_of(h);
     const int order = h->cfg.integration_order, nst = order == 1 ? 1 : 2;
     if (h->connected) {
-        // blocks of one level on this device: the stage array uh lives in the
-        // other parity's buffer so that the same-level exchange tables serve it
+        // blocks on this device: the stage array uh lives in the other
+        // parity's buffer so that the exchange and prolongation tables serve it
         if (!h->remote.empty()) return fail(h, PK_E_UNSUPPORTED, "the unsplit scheme runs on one rank");
-        for (auto& b : h->blocks)
-            if (b.level > 0) return fail(h, PK_E_UNSUPPORTED, "refined domains use the split scheme");
         if (int rc = exchange_prepare(h)) return rc;
     }
     for (auto& b : h->blocks) {
@@ -1650,25 +1649,55 @@ static int unsplit_sweep(pk_ctx* h)
         const int last = (order == 1) || (s == 2);
         const double rk = order == 1 ? 1.0 : (first ? 0.5 : 1.0);
         const bool to_uh = order == 2 && first;
+        // the face fluxes, finest level first: a refined block's fluxes through
+        // faces bordering the coarser level are restricted into that level's
+        // flux through the same face before its blocks compute theirs
+        // (unsplit_sweeps.F90:132-177 with fc_fluxes_unsplit.F90)
+        for (int L = h->max_level; L >= 0; --L) {
+            for (auto& b : h->blocks) {
+                if (b.level != L) continue;
+                double* u = state(h, b);
+                double* uh = h->connected ? b.buf[1 - h->cur] : b.uh;
+                const double* in = (first || order < 2) ? u : uh;
+                for (int d = 0; d < 3; ++d)
+                    if (b.n[d] > 1)
+                        if (int rc = ops->unsplit_flux(h, b, d, in, b.flux[d])) return rc;
+            }
+            if (L > 0)
+                for (int d = 0; d < 3; ++d) {
+                    if (!h->d_src[d]) continue;
+                    const int beg = h->in_level_beg[d][L - 1], end = h->in_level_beg[d][L];
+                    if (end <= beg) continue;
+                    const long long n = (long long)(end - beg) * h->nplanes;
+                    k_restrict_flux<<<grid1d(n, 256), 256, 0, h->stream>>>(h->d_src[d], beg, end, h->nplanes,
+                                                                           h->d_out_flux[d], h->d_in_flux[d],
+                                                                           h->fc_scale);
+                    PK_CUDA(h, cudaGetLastError());
+                    h->launches += 1;
+                }
+        }
         for (auto& b : h->blocks) {
             double* u = state(h, b);
             double* uh = h->connected ? b.buf[1 - h->cur] : b.uh;
-            const double* in = (first || order < 2) ? u : uh;
             double* T = to_uh ? uh : u;
-            for (int d = 0; d < 3; ++d)
-                if (b.n[d] > 1)
-                    if (int rc = ops->unsplit_flux(h, b, d, in, b.flux[d])) return rc;
             if (int rc = ops->unsplit_apply(h, b, u, T, rk, last)) return rc;
-            if (int rc = fill_guards_ptr(h, b, T)) return rc;
+            if (h->max_level == 0)                     // refined domains overwrite every guard cell below
+                if (int rc = fill_guards_ptr(h, b, T)) return rc;
             b.guards_stale = false;
         }
-        // update_boundaries(istep) between the blocks (unsplit_sweeps.F90:182)
-        if (h->connected && h->xlocal.total > 0) {
-            const int nblk = h->xlocal.n < 148 * 16 ? h->xlocal.n : 148 * 16;
-            k_exchange<<<nblk, 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total,
-                                                    h->d_xptr[to_uh ? 1 - h->cur : h->cur], h->nplanes);
-            PK_CUDA(h, cudaGetLastError());
-            h->launches += 1;
+        // update_boundaries(istep) between the blocks (unsplit_sweeps.F90:182):
+        // same-level copies, then prolongation coarsest level first
+        if (h->connected) {
+            const int par = to_uh ? 1 - h->cur : h->cur;
+            if (h->xlocal.total > 0) {
+                const int nblk = h->xlocal.n < 148 * 16 ? h->xlocal.n : 148 * 16;
+                k_exchange<<<nblk, 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total, h->d_xptr[par],
+                                                        h->nplanes);
+                PK_CUDA(h, cudaGetLastError());
+                h->launches += 1;
+            }
+            if (h->max_level > 0)
+                if (int rc = prolong_guards(h, -1, par)) return rc;
         }
     }
     return PK_OK;

@@ -397,6 +397,28 @@ struct FcArgs {
 // tile is then [g-2, g+n+2) of the pencil (c0 = g-2, T = L = n+4), which holds
 // every cell the interior updates read.
 // -------------------------------------------------------------------------
+// The ext_fluxes of storage cell s of pencil (i1, i2): the restricted fine
+// flux replacing the flux through its right face (li / ri) and the slot
+// recording the flux through it (lo / ro: the faces just outside the interior)
+template <class PH>
+PK_DEV void fc_slots(const FcArgs& fc, const Geom& g, int i1, int i2, int s, const double*& fc_in, double*& fc_out)
+{
+    const long long np = (long long)g.n1 * g.n2;
+    const long long pen = i1 + (long long)g.n1 * i2;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        if (fc.in_slot) {
+            const int sl = fc.in_slot[side * np + pen];
+            if (sl >= 0 && fc.in_face[sl] == s) fc_in = fc.in_flux + (long long)sl * PH::NV;
+        }
+        if (fc.out_slot) {
+            const int sl = fc.out_slot[side * np + pen];
+            if (sl >= 0 && s == (side == 0 ? g.g_d - 1 : g.g_d + g.n_d - 1))
+                fc_out = fc.out_flux + (long long)sl * PH::NV;
+        }
+    }
+}
+
 template <class PH, bool W3, bool FC>
 PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
                        double* uh, const PhysParams& pp, int first, double dtodx, double ch, const FcArgs& fc,
@@ -436,24 +458,8 @@ PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     r.keep = !r.upd && valid && (s == 0 || s == n - 1);        // u1 = u at the pencil ends, then floors
     const double* fc_in = nullptr;
     double* fc_out = nullptr;
-    if constexpr (FC) {
-        if (valid) {
-            const long long np = (long long)g.n1 * g.n2;
-            const long long pen = i1 + (long long)g.n1 * i2;
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                if (fc.in_slot) {
-                    const int sl = fc.in_slot[side * np + pen];
-                    if (sl >= 0 && fc.in_face[sl] == s) fc_in = fc.in_flux + (long long)sl * PH::NV;
-                }
-                if (fc.out_slot) {
-                    const int sl = fc.out_slot[side * np + pen];
-                    if (sl >= 0 && s == (side == 0 ? g.g_d - 1 : g.g_d + g.n_d - 1))
-                        fc_out = fc.out_flux + (long long)sl * PH::NV;
-                }
-            }
-        }
-    }
+    if constexpr (FC)
+        if (valid) fc_slots<PH>(fc, g, i1, i2, s, fc_in, fc_out);
     rk_stage<PH, false, W3, FC>(sm, me, me - st, me + st, r, w, first ? uin : uh, uin, off, g, dtodx, ch, pp, status,
                                 nullptr, fc_in, fc_out);
     if (own && (!trim || inner)) store_cell<PH>(uout, off, g, w);
@@ -533,11 +539,11 @@ __global__ void __launch_bounds__(MAXT, MINB) k_stage_batched(const BlockDesc* _
 // in chunks with a 2-cell halo as k_stage; the flux through the face between
 // storage cells s and s+1 goes to F at cell s+1 (pflux(:, i) is the flux
 // through cell i's left face), in the state's own plane order.
-template <class PH, int MAXT, bool W3 = false>
+template <class PH, int MAXT, bool W3 = false, bool FC = false>
 __global__ void __launch_bounds__(MAXT) k_unsplit_flux(Geom g, Tile tl, const double* __restrict__ uin,
                                                       double* __restrict__ F, PhysParams pp,
                                                       const StepParams* __restrict__ spar,
-                                                      unsigned* __restrict__ gstatus)
+                                                      unsigned* __restrict__ gstatus, FcArgs fc = FcArgs{})
 {
     extern __shared__ double smem[];
     constexpr int NV = PH::NV;
@@ -570,7 +576,12 @@ __global__ void __launch_bounds__(MAXT) k_unsplit_flux(Geom g, Tile tl, const do
     r.upd = false;
     r.keep = false;
     unsigned status = 0;
-    rk_stage<PH, false, W3>(sm, me, me - st, me + st, r, w, uin, uin, off, g, 0.0, spar->ch, pp, status);
+    const double* fc_in = nullptr;
+    double* fc_out = nullptr;
+    if constexpr (FC)
+        if (valid) fc_slots<PH>(fc, g, i1, i2, s, fc_in, fc_out);
+    rk_stage<PH, false, W3, FC>(sm, me, me - st, me + st, r, w, uin, uin, off, g, 0.0, spar->ch, pp, status, nullptr,
+                                fc_in, fc_out);
     if (own && r.flux) {
         double f[NV];
 #pragma unroll

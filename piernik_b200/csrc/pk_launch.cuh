@@ -74,10 +74,9 @@ int set_smem_attr(pk_ctx* h)
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_unsplit_flux<PH, STAGE_MAXT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(k_unsplit_flux<PH, STAGE_MAXT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        220 * 1024));
+        for (auto* kf : {k_unsplit_flux<PH, STAGE_MAXT, false, false>, k_unsplit_flux<PH, STAGE_MAXT, true, false>,
+                         k_unsplit_flux<PH, STAGE_MAXT, false, true>, k_unsplit_flux<PH, STAGE_MAXT, true, true>})
+            PK_CUDA(h, cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         for (int v = 0; v < NSTAGE_VARIANT; ++v)
             for (int w3 = 0; w3 < 2; ++w3)
                 for (int fc = 0; fc < 2; ++fc)
@@ -434,8 +433,12 @@ int launch_unsplit_flux(pk_ctx* h, Block& b, int dir, const double* in, double* 
     const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    auto* kern = h->pp.weno3 ? k_unsplit_flux<PH, STAGE_MAXT, true> : k_unsplit_flux<PH, STAGE_MAXT, false>;
-    kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, F, h->pp, h->d_step, h->d_status);
+    // a refined block's fine/coarse flux couplings along dir (ext_fluxes, unsplit_mag_modules.F90:195-204)
+    const FcArgs fc = b.fc[dir];
+    const bool hooks = fc.in_slot || fc.out_slot;
+    auto* kern = h->pp.weno3 ? (hooks ? k_unsplit_flux<PH, STAGE_MAXT, true, true> : k_unsplit_flux<PH, STAGE_MAXT, true, false>)
+                             : (hooks ? k_unsplit_flux<PH, STAGE_MAXT, false, true> : k_unsplit_flux<PH, STAGE_MAXT, false, false>);
+    kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, F, h->pp, h->d_step, h->d_status, fc);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;

@@ -148,3 +148,21 @@ def test_refined_prolongation_orders(gpu_lib, orders, nb):
     sim.run(2)
     compare(sim, a, "after 2 steps")
     sim.close()
+
+
+@pytest.mark.parametrize("phys,dom,reg,lim", [("hd", DOM3, REG3, "vanleer"), ("mhd", DOM3, REG3, "moncen"),
+                                              ("mhd", DOM2, REG2, "vanleer"), ("mhd", DOM3, REG3, "weno3")])
+def test_refined_unsplit_matches_oracle(gpu_lib, phys, dom, reg, lim):
+    """The unsplit scheme on a refined domain: per stage every level's face
+    fluxes finest first with the fine/coarse flux replacement, their
+    application, then the guard update of uh (first stage) or u."""
+    blocks = case(phys, dom, reg, lim=lim, solver="unsplit", cfl=0.3, cfl_glm=0.3)
+    a = amr.AmrOracle(dom, blocks)
+    a.fill_guards()
+    sim = library(dom, blocks)
+    a.run(3)
+    sim.run(3)
+    compare(sim, a, "unsplit, 3 steps")
+    st = sim.time_state
+    assert (st.t, st.dt, st.nstep) == (a.state.t, a.state.dt, a.state.nstep)
+    sim.close()

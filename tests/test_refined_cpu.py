@@ -79,6 +79,29 @@ def test_refined_oracle_conserves(oracle_lib, phys, dim):
     assert np.all(np.abs(t1 - t0) <= 1e-12 * scale), (t1 - t0) / scale
 
 
+@pytest.mark.parametrize("phys", ["hd", "mhd"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_refined_oracle_unsplit_conserves(oracle_lib, phys, dim):
+    """The unsplit scheme over the levels (fc_fluxes_unsplit: the coarse
+    face flux replaced by the restricted fine ones) conserves the leaf
+    totals to round-off, and without the replacement it does not."""
+    dom, reg = (DOM3, REG3) if dim == 3 else (DOM2, REG2)
+    layout = problems.refined_layout(dom, reg, sizes=(8, 16), seed=3)
+    setup = setup_for(phys, n=tuple(8 if d > 1 else 1 for d in dom), solver="unsplit", cfl=0.3, cfl_glm=0.3)
+    blocks = problems.refined_blocks(dom, layout, setup, problems.wave_fields(dom, seed=5))
+    for teeth in (False, True):
+        a = amr.AmrOracle(dom, blocks)
+        if teeth:
+            a.restr = [[[] for _ in lv] for lv in a.restr]
+        a.fill_guards()
+        t0 = amr.leaf_totals(a)
+        scale = amr.leaf_totals(a, absolute=True)
+        a.run(2)
+        err = np.max(np.abs(amr.leaf_totals(a) - t0) / scale)
+        assert a.state.nstep == 2 and a.state.t > 0
+        assert (err > 1e-8) if teeth else (err <= 1e-12), (teeth, err)
+
+
 def test_refined_oracle_without_correction_does_not_conserve(oracle_lib):
     """The check above has teeth: with the fine fluxes never passed to the
     coarse blocks the leaf totals drift far beyond round-off."""
