@@ -22,6 +22,7 @@ constexpr int NVARIANT = 7;
 constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512};
 constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1};
 constexpr int STAGE_MAXT = 320;       // threads per CTA of the stage kernel
+constexpr int UNSPLIT_MAXT = 256;     // threads per CTA of the unsplit flux kernel (two CTAs per SM)
 // launch-bound variants of the batched stage kernel (threads per CTA, CTAs per SM)
 constexpr int NSTAGE_VARIANT = 4;
 constexpr int SV_T[NSTAGE_VARIANT] = {320, 128, 192, 384};

@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_stage_batched(const BlockDesc* _
 // storage cells s and s+1 goes to F at cell s+1 (pflux(:, i) is the flux
 // through cell i's left face), in the state's own plane order.
 template <class PH, int MAXT, bool W3 = false, bool FC = false>
-__global__ void __launch_bounds__(MAXT) k_unsplit_flux(Geom g, Tile tl, const double* __restrict__ uin,
+__global__ void __launch_bounds__(MAXT, 2) k_unsplit_flux(Geom g, Tile tl, const double* __restrict__ uin,
                                                       double* __restrict__ F, PhysParams pp,
                                                       const StepParams* __restrict__ spar,
                                                       unsigned* __restrict__ gstatus, FcArgs fc = FcArgs{})

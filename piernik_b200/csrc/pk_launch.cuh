@@ -74,8 +74,8 @@ int set_smem_attr(pk_ctx* h)
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
-        for (auto* kf : {k_unsplit_flux<PH, STAGE_MAXT, false, false>, k_unsplit_flux<PH, STAGE_MAXT, true, false>,
-                         k_unsplit_flux<PH, STAGE_MAXT, false, true>, k_unsplit_flux<PH, STAGE_MAXT, true, true>})
+        for (auto* kf : {k_unsplit_flux<PH, UNSPLIT_MAXT, false, false>, k_unsplit_flux<PH, UNSPLIT_MAXT, true, false>,
+                         k_unsplit_flux<PH, UNSPLIT_MAXT, false, true>, k_unsplit_flux<PH, UNSPLIT_MAXT, true, true>})
             PK_CUDA(h, cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         for (int v = 0; v < NSTAGE_VARIANT; ++v)
             for (int w3 = 0; w3 < 2; ++w3)
@@ -414,8 +414,8 @@ int launch_unsplit_flux(pk_ctx* h, Block& b, int dir, const double* in, double* 
     // whole pencils where they fit; across x (y and z sweeps) only when four or
     // more neighbouring pencils share the CTA, so that the loads stay coalesced,
     // else chunks of 64 cells with a 2-cell halo
-    if (ext <= STAGE_MAXT && (dir == 0 || STAGE_MAXT / ext >= 4 || g.n1 < 4)) {
-        int P = STAGE_MAXT / ext;
+    if (ext <= UNSPLIT_MAXT && (dir == 0 || UNSPLIT_MAXT / ext >= 4 || g.n1 < 4)) {
+        int P = UNSPLIT_MAXT / ext;
         if (P >= 4) P -= P % 4;
         if (P > g.n1) P = g.n1;
         tl.P = P;
@@ -424,7 +424,7 @@ int launch_unsplit_flux(pk_ctx* h, Block& b, int dir, const double* in, double* 
         tl.halo = 0;
     } else {
         tl.P = 4;
-        tl.L = 64;
+        tl.L = UNSPLIT_MAXT / 4 - 4;
         tl.T = tl.L + 4;
         tl.halo = 2;
     }
@@ -436,8 +436,8 @@ int launch_unsplit_flux(pk_ctx* h, Block& b, int dir, const double* in, double* 
     // a refined block's fine/coarse flux couplings along dir (ext_fluxes, unsplit_mag_modules.F90:195-204)
     const FcArgs fc = b.fc[dir];
     const bool hooks = fc.in_slot || fc.out_slot;
-    auto* kern = h->pp.weno3 ? (hooks ? k_unsplit_flux<PH, STAGE_MAXT, true, true> : k_unsplit_flux<PH, STAGE_MAXT, true, false>)
-                             : (hooks ? k_unsplit_flux<PH, STAGE_MAXT, false, true> : k_unsplit_flux<PH, STAGE_MAXT, false, false>);
+    auto* kern = h->pp.weno3 ? (hooks ? k_unsplit_flux<PH, UNSPLIT_MAXT, true, true> : k_unsplit_flux<PH, UNSPLIT_MAXT, true, false>)
+                             : (hooks ? k_unsplit_flux<PH, UNSPLIT_MAXT, false, true> : k_unsplit_flux<PH, UNSPLIT_MAXT, false, false>);
     kern<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, F, h->pp, h->d_step, h->d_status, fc);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
