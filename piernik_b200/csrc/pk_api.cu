@@ -700,12 +700,12 @@ int build_batch(pk_ctx* h)
             const Block& b = h->blocks[i];
             if (b.n[dir] <= 1) continue;
             const int T = b.n[dir] + 4;                 // the trimmed tile of k_stage_batched
+            const int face = b.n[o1] * b.n[o2];         // pencils, taken in i1-fastest order across i2 rows
             int P = SV_T[sv] / T;
-            if (P > b.n[o1]) P = b.n[o1];
+            if (P > face) P = face;
             StageList& sl = h->sbatch[dir][b.level];
             sl.smem = std::max(sl.smem, (size_t)3 * h->nplanes * P * T * sizeof(double));
-            for (int i2 = 0; i2 < b.n[o2]; ++i2)
-                for (int i1 = 0; i1 < b.n[o1]; i1 += P) items[b.level].push_back(StageItem{i, i1, i2, P});
+            for (int q = 0; q < face; q += P) items[b.level].push_back(StageItem{i, q, 0, P});
         }
         for (int L = 0; L <= maxl; ++L) {
             StageList& sl = h->sbatch[dir][L];

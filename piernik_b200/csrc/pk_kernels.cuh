@@ -422,7 +422,7 @@ PK_DEV void fc_slots(const FcArgs& fc, const Geom& g, int i1, int i2, int s, con
 template <class PH, bool W3, bool FC>
 PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
                        double* uh, const PhysParams& pp, int first, double dtodx, double ch, const FcArgs& fc,
-                       double* smem, unsigned& status, bool trim = false)
+                       double* smem, unsigned& status, bool trim = false, bool flat = false)
 {
     constexpr int NV = PH::NV;
     const int P = tl.P, T = tl.T, PT = P * T;
@@ -433,10 +433,18 @@ PK_DEV void stage_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     else { p = tid % P; t = tid / P; }
     const int sp = tl.xfast ? T : 1, st = tl.xfast ? 1 : P;
     const int me = p * sp + t * st;
-    const int i1 = i1_0 + p;
+    // flat: the tile's pencils are i1_0 + p in i1-fastest order over the whole
+    // block face, so that a CTA may take pencils of consecutive i2 rows
+    int i1 = i1_0 + p;
+    bool in_face = i1 < g.n1;
+    if (flat) {
+        in_face = i1 < g.n1 * g.n2;
+        i2 = i1 / g.n1;
+        i1 -= i2 * g.n1;
+    }
     const int n = g.ext_d;
     const int s = c0 - tl.halo + t;                            // storage index along the pencil
-    const bool valid = (tid < PT) && (i1 < g.n1) && s >= 0 && s < n;
+    const bool valid = (tid < PT) && in_face && s >= 0 && s < n;
     const bool own = valid && s >= c0 && s < c0 + tl.L;
     const long long off = (long long)s * g.sd + (long long)(g.g1 + i1) * g.s1 + (long long)(g.g2 + i2) * g.s2;
     double w[NV];
@@ -486,7 +494,7 @@ __global__ void __launch_bounds__(MAXT) k_stage(Geom g, Tile tl, const double* u
 // the stage).  blocks[b].in is the state, blocks[b].uh its stage-1 copy; fcs
 // (or null) the blocks' flux couplings along dir.
 struct StageItem {
-    int block, i1_0, i2, P;
+    int block, i1_0, i2, P;     // i1_0: first pencil in i1-fastest order over the face (i2 unused)
 };
 
 template <class PH, int MAXT, int MINB, bool W3 = false, bool FC = false>
@@ -526,7 +534,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_stage_batched(const BlockDesc* _
     const FcArgs fc = fcs ? fcs[w.block] : FcArgs{};
     double* u = const_cast<double*>(b.in);
     stage_tile<PH, W3, FC>(g, tl, w.i1_0, b.g[dir] - 2, w.i2, u, u, b.uh, pp, first, dtodx, spar->ch, fc, smem, status,
-                           true);
+                           true, true);
     flush_status(status, gstatus);
 }
 
