@@ -5,14 +5,17 @@ For every launch shape the library can produce for the given block sizes
 chunked stage tiles), each thread's global offset and every shared-memory
 slot it reads are computed exactly as the kernels do and checked to be in
 bounds; owned cells must be updated.  This runs before any GPU sees a new
-tile shape.  Mirrors k_sweep_fused / k_stage in piernik_b200/csrc/pk_kernels.cuh
-and launch_fused / launch_stage in pk_api.cu.
+tile shape.  Mirrors k_sweep_fused / k_stage / k_stage_batched / k_unsplit_flux in
+piernik_b200/csrc/pk_kernels.cuh and launch_fused / launch_stage /
+launch_unsplit_flux / build_batch in pk_launch.cuh and pk_api.cu.
 """
 import pytest
 
 ORTHO1 = [1, 0, 0]
 ORTHO2 = [2, 2, 1]
 STAGE_MAXT = 320
+UNSPLIT_MAXT = 256
+SV_T = [320, 128, 192, 384]             # launch shapes of the batched stage kernel
 VARIANT_T = [320, 256, 256, 128, 128, 192, 512]
 
 
@@ -124,6 +127,99 @@ def check_stage(n, d):
                         assert upd
 
 
+def roles_ok(ext, T, t, s, me, st, PT):
+    """the neighbour slots rk_stage reads for a tile cell are inside the tile"""
+    end = -1 if s == 0 else (1 if s == ext - 1 else 0)
+    slope = end != 0 or (1 <= t <= T - 2)
+    next_slope = s + 1 < ext and t + 1 <= T - 1 and (s + 1 == ext - 1 or t + 1 <= T - 2)
+    flux = slope and next_slope
+    prev_flux = t >= 1 and s >= 1 and (s - 1 == 0 or t - 1 >= 1)
+    upd = 1 <= s <= ext - 2 and prev_flux and flux
+    if slope:
+        if end < 0:
+            assert me + st < PT
+        elif end > 0:
+            assert me - st >= 0
+        else:
+            assert me - st >= 0 and me + st < PT
+    if flux:
+        assert me + st < PT
+    if upd:
+        assert me - st >= 0
+    return flux, upd
+
+
+def check_stage_batched(n, d, maxt):
+    """k_stage_batched: tiles [g-2, g+n+2) of P pencils taken in i1-fastest
+    order across the rows of the block face; every interior cell updated"""
+    G = geom(n, 4, d)
+    ext, T = G["ext_d"], n[d] + 4
+    face = G["n1"] * G["n2"]
+    P = min(maxt // T, face)
+    PT = P * T
+    assert PT <= maxt and 3 * 18 * PT * 8 <= 220 * 1024
+    xfast = d == 0
+    updated = set()
+    for q0 in range(0, face, P):
+        for tid in range(PT):
+            t, p = (tid % T, tid // T) if xfast else (tid // P, tid % P)
+            sp, st = (T, 1) if xfast else (1, P)
+            me = p * sp + t * st
+            assert 0 <= me < PT
+            q = q0 + p
+            if q >= face:
+                continue
+            i2, i1 = divmod(q, G["n1"])
+            s = G["g_d"] - 2 + t
+            if not 0 <= s < ext:
+                continue
+            off = s * G["sd"] + (G["g1"] + i1) * G["s1"] + (G["g2"] + i2) * G["s2"]
+            assert 0 <= off < G["plane"]
+            _, upd = roles_ok(ext, T, t, s, me, st, PT)
+            if upd and G["g_d"] <= s < G["g_d"] + n[d]:
+                updated.add((i1, i2, s))
+    assert len(updated) == face * n[d]
+
+
+def check_unsplit(n, d):
+    """k_unsplit_flux: whole pencils where they fit, else 4 x (60 + 4) chunks;
+    the flux through every face between two cells of the pencil is stored once"""
+    G = geom(n, 4, d)
+    ext = G["ext_d"]
+    if ext <= UNSPLIT_MAXT and (d == 0 or UNSPLIT_MAXT // ext >= 4 or G["n1"] < 4):
+        P = UNSPLIT_MAXT // ext
+        if P >= 4:
+            P -= P % 4
+        P = min(P, G["n1"])
+        T, L, halo = ext, ext, 0
+    else:
+        P, L, halo = 4, UNSPLIT_MAXT // 4 - 4, 2
+        T = L + 4
+    PT = P * T
+    assert PT <= UNSPLIT_MAXT
+    xfast = d == 0
+    stored = {}
+    for bx in range((G["n1"] + P - 1) // P):
+        for by in range((ext + L - 1) // L):
+            for tid in range(PT):
+                t, p = (tid % T, tid // T) if xfast else (tid // P, tid % P)
+                sp, st = (T, 1) if xfast else (1, P)
+                me = p * sp + t * st
+                i1 = bx * P + p
+                c0 = by * L
+                s = c0 - halo + t
+                if not (i1 < G["n1"] and 0 <= s < ext):
+                    continue
+                off = s * G["sd"] + (G["g1"] + i1) * G["s1"] + G["g2"] * G["s2"]
+                assert 0 <= off < G["plane"]
+                flux, _ = roles_ok(ext, T, t, s, me, st, PT)
+                if flux and c0 <= s < c0 + L:
+                    assert 0 <= off + G["sd"] < G["plane"]
+                    stored[(i1, s)] = stored.get((i1, s), 0) + 1
+    assert all(v == 1 for v in stored.values())
+    assert len(stored) == G["n1"] * (ext - 1)
+
+
 CASES = [(12, 10, 8), (20, 14, 11), (50, 37, 29), (400, 6, 5), (24, 17, 9), (32, 32, 1), (9, 8, 7),
          (64, 64, 64), (16, 24, 48)]
 
@@ -147,3 +243,22 @@ def test_fused_kernel_indexing(n):
                 for P in (1, 2, 3, 4, 5, 7, 8):
                     if L + 8 <= maxt:
                         check_fused(n, d, P, L, maxt)
+
+
+BATCH_CASES = [(16, 16, 16), (24, 64, 48), (64, 64, 64), (48, 16, 32), (40, 36, 28), (8, 8, 8), (16, 24, 1)]
+
+
+@pytest.mark.parametrize("n", BATCH_CASES)
+def test_stage_batched_kernel_indexing(n):
+    for d in range(3):
+        if n[d] > 1:
+            for maxt in SV_T:
+                if n[d] + 4 <= maxt:
+                    check_stage_batched(n, d, maxt)
+
+
+@pytest.mark.parametrize("n", [(12, 10, 8), (50, 37, 29), (264, 6, 5), (64, 64, 64), (16, 300, 6), (32, 32, 1)])
+def test_unsplit_flux_kernel_indexing(n):
+    for d in range(3):
+        if n[d] > 1:
+            check_unsplit(n, d)
