@@ -92,6 +92,9 @@ class Simulation:
         dl = (C.c_double * 3)(*setup.dl)
         bnd = (C.c_int32 * 6)(*[setup.bnd[d][s] for d in range(3) for s in range(2)])
         self.blocks = {}
+        self.instances = 1
+        self.domain = None          # (cells of the base grid, periodic flags) after set_domain
+        self.placement = {}         # block -> (offset, level) after place_block
         self.block = self.add_block(setup)
 
     def add_block(self, setup: Setup) -> int:
@@ -260,6 +263,7 @@ class Simulation:
         n = (C.c_int64 * 3)(*[int(x) for x in ncells])
         p = (C.c_int32 * 3)(*[int(bool(x)) for x in periodic])
         self._chk(self.lib.pk_set_domain(self.h, n, p), "pk_set_domain")
+        self.domain = (tuple(int(x) for x in ncells), tuple(bool(x) for x in periodic))
 
     def restrict(self) -> None:
         """Covered coarse cells take the mean of their children, finest level
@@ -299,6 +303,7 @@ class Simulation:
         """Free ``block``; the ids above it move down by one."""
         self._chk(self.lib.pk_block_remove(self.h, block), "pk_block_remove")
         self.blocks = {(k if k < block else k - 1): v for k, v in self.blocks.items() if k != block}
+        self.placement = {(k if k < block else k - 1): v for k, v in self.placement.items() if k != block}
 
     def prolong_block(self, block: int) -> None:
         """Fill every cell of ``block`` (a refined level's) from the coarser level."""
@@ -309,6 +314,7 @@ class Simulation:
         refinement level (the base grid refined ``level`` times)."""
         o = (C.c_int64 * 3)(*[int(x) for x in off])
         self._chk(self.lib.pk_block_place_level(self.h, block, level, o), "pk_block_place_level")
+        self.placement[block] = (tuple(int(x) for x in off), int(level))
 
     # -- differentiable path (one periodic block, one fluid, RK2) -------------
     @property
