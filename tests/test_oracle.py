@@ -221,3 +221,32 @@ def test_cfl_redo_repeats_violating_steps(oracle_lib):
     assert st.nstep == 30 - st.redone
     assert st.stepcfl <= oracle.lib().o_cfl_max(C.byref(ob.cfg))
     assert st.dt_cur_shrink == 1.0
+
+
+def test_sedov_shock_follows_similarity_solution(oracle_lib):
+    """Sedov-Taylor: the blast front (peak of the spherically averaged
+    density) sits at R = xi0 (E t^2 / rho)^(1/5), xi0 = 1.1517 for gamma =
+    5/3 in 3D, within 10 % at 48^3, and R grows as t^(2/5) between t = 0.05
+    and 0.1 within 5 % (the physics check of the restated split solver)."""
+    radii = []
+    for tend in (0.05, 0.1):
+        setup, u, b, psi = problems.sedov(n=48)
+        setup = setup.replace(tend=tend)
+        ob = oracle.OracleBlock(setup, u, b, psi)
+        ob.run(5000)
+        assert abs(ob.state.t - tend) <= 1e-12
+        rho = interior(setup, ob.u)[..., 0]
+        n, dx = setup.n[0], setup.dl[0]
+        c = (np.arange(n) + 0.5) * dx - 1.0
+        Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+        R = np.sqrt(X ** 2 + Y ** 2 + Z ** 2).ravel()
+        edges = np.arange(0.0, 1.0, dx / 2)
+        k = np.digitize(R, edges)
+        cnt = np.bincount(k, minlength=len(edges) + 1)[1:len(edges)]
+        tot = np.bincount(k, weights=rho.ravel(), minlength=len(edges) + 1)[1:len(edges)]
+        prof = np.where(cnt > 0, tot / np.maximum(cnt, 1), 0.0)
+        r_shock = 0.5 * (edges[1:] + edges[:-1])[np.argmax(prof)]
+        r_theory = 1.15167 * (1.0 * tend ** 2 / 1.0) ** 0.2
+        assert 0.9 < r_shock / r_theory < 1.1, (tend, r_shock, r_theory)
+        radii.append(r_shock)
+    assert abs(radii[1] / radii[0] / 2.0 ** 0.4 - 1.0) < 0.05, radii
