@@ -14,7 +14,8 @@ Arms:
   default            the CUDA library through Simulation.run (state resident in HBM)
   --impl reference   the reference's CPU algorithm (the oracle port in oracle/,
                      the Fortran reference cannot be compiled here) on all host
-                     threads, each step a bounded 128^3 sample of the workload
+                     threads, on the same 256^3 workload (each step one main-loop
+                     iteration of it, a few seconds of CPU work)
 
 Multi-GPU (torchrun): every rank advances its own 256^3 replica (weak scaling);
 timing is the max over ranks of CUDA-event time on the library's stream.
@@ -39,15 +40,17 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 MHD cell-updates/s at 256^3 on 1 B200; adjoint-gradient cost ÷ forward step"
 UNIT = "cell-updates/s"
 NVAR = 9                         # dn, mx, my, mz, en, Bx, By, Bz, psi
-# DRAM bytes per cell of one fused-sweep launch from the ncu capture in
-# profiles/k_sweep_fused_mhd_128cube.md (y sweep, 128^3: 161.76 MB read +
-# 125.97 MB written over 128^3 cells); traffic grows with the cell count, so the
+# DRAM bytes per cell of one fused-sweep launch, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the y sweep of a 128^3
+# block (181 MB with guards, above the 126 MB L2): 161.76 MB read + 125.97 MB
+# written over 128^3 cells.  Traffic grows with the cell count, so the
 # full-size figure is this times n^3.
 TRAFFIC_BYTES_PER_CELL = (161.756672e6 + 125.965568e6) / 128 ** 3
 # FP64 flops per cell of one fused sweep (both RK2 stages) without halo
-# recomputation, i.e. the algorithmic FP64 work: 2 DFMA + DMUL + DADD thread
-# instructions of the whole-pencil x sweep at 128^3 over its 128^3 cells
-# (profiles/k_sweep_fused_fp64_128cube.md)
+# recomputation, i.e. the algorithmic FP64 work: 2 x DFMA + DMUL + DADD
+# thread instructions (ncu sm__sass_thread_inst_executed_op_{dfma,dmul,dadd}
+# _pred_on.sum) of the whole-pencil x sweep of a 128^3 block over its 128^3
+# cells, in the bit-exact build
 FP64_FLOP_PER_CELL_SWEEP = 3.589298377e9 / 128 ** 3
 
 
@@ -169,17 +172,20 @@ def reference_arm(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from piernik_b200 import problems
-    ns = 128 if args.n >= 128 else args.n
+    ns = args.n
     setup, u, b, psi = problems.mhd_turbulence(n=ns, seed=args.seed)
     ob = oracle.OracleBlock(setup, u, b, psi)
-    ob.run(args.warmup)
+    # one warm-up step at most: the CPU path has no caches or kernels to load
+    # beyond the first touch of its arrays
+    ob.run(min(args.warmup, 1))
     t0 = time.perf_counter()
     ob.run(args.steps)
     el = time.perf_counter() - t0
     value = 2.0 * ns ** 3 * args.steps / el
     threads = oracle.get_threads()
-    sample = (f"{args.steps} steps of the workload recipe at {ns}^3 (oracle/pk_oracle.c, OpenMP over pencils, "
-              f"{threads} threads); the Fortran reference has no compiler here")
+    sample = (f"{args.steps} steps of the workload at {ns}^3 ({2 * ns ** 3 * args.steps} cell-updates, {el:.1f} s; "
+              f"oracle/pk_oracle.c, OpenMP over pencils, {threads} threads); the Fortran reference has no "
+              f"compiler here")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",

@@ -411,13 +411,17 @@ int pk_fp64_peak(double* tflops);
  * handle's layout (component planes u, then bx, by, bz, psi when magnetic;
  * each plane ext_x*ext_y*ext_z doubles with ext = n + 2*nb where n > 1,
  * else 1).  n and dl hold 3 values per block; states holds nblocks device
- * pointers; stream may be NULL (the legacy default stream).  The call is
- * synchronous and allocates nothing: its reduction slots are a fixed 6 KiB
- * device array, kept by every GPU that loads the library until exit and
- * shared by all calls, so calls that overlap on one GPU race.  At most
- * PK_NOALLOC_MAX_BLOCKS blocks per call (PK_E_ARG beyond).  The first call
- * on a device looks up the array's address there: make it before any stream
- * capture.  err (errlen bytes, or NULL) receives a message. */
+ * pointers of the current device; stream may be NULL (the legacy default
+ * stream) or a stream of the current device.  The call is synchronous (it
+ * reads the result back and waits for the stream) and allocates nothing: its
+ * reduction slots are a fixed 6 KiB device array, kept by every GPU that
+ * loads the library until exit and shared by all calls, so calls that
+ * overlap on one GPU race.  At most PK_NOALLOC_MAX_BLOCKS blocks per call
+ * (PK_E_ARG beyond).  A state that is not device memory of the current
+ * device, or a stream of another device, gives PK_E_ARG before anything is
+ * launched; a call while the stream is capturing gives PK_E_STATE.  The first
+ * call on a device looks up the array's address there.  err (errlen bytes,
+ * or NULL) receives a message. */
 #define PK_NOALLOC_MAX_BLOCKS 64
 int pk_timestep_raw_noalloc(const pk_config* cfg, int32_t nblocks, const int32_t* n, const double* dl,
                             const double* const* states, void* stream, double* dt_out, double* c_all_out,

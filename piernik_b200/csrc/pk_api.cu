@@ -81,7 +81,7 @@ namespace {
 int grid1d(long long n, int threads)
 {
     long long b = (n + threads - 1) / threads;
-    if (b > 148LL * 16) b = 148LL * 16;
+    if (b > grid_cap()) b = grid_cap();
     return (int)(b < 1 ? 1 : b);
 }
 
@@ -557,7 +557,7 @@ int exchange_guards(pk_ctx* h, int dir = -1, int need = -1)
     if (need >= 0 && !(h->max_level > 0 && h->part[need].ok)) need = -1;
     const XSegList& xs = need >= 0 ? h->part[need].segs : h->xlocal;
     if (xs.total > 0) {
-        const int nblk = xs.n < 148 * 16 ? xs.n : 148 * 16;   // CTAs take whole segments
+        const int nblk = (int)(xs.n < grid_cap() ? xs.n : grid_cap());   // CTAs take whole segments
         k_exchange<<<nblk, 256, 0, h->stream>>>(xs.dev, xs.n, xs.total, h->d_xptr[h->cur], h->nplanes);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
@@ -1690,7 +1690,7 @@ static int unsplit_sweep(pk_ctx* h)
         if (h->connected) {
             const int par = to_uh ? 1 - h->cur : h->cur;
             if (h->xlocal.total > 0) {
-                const int nblk = h->xlocal.n < 148 * 16 ? h->xlocal.n : 148 * 16;
+                const int nblk = (int)(h->xlocal.n < grid_cap() ? h->xlocal.n : grid_cap());
                 k_exchange<<<nblk, 256, 0, h->stream>>>(h->xlocal.dev, h->xlocal.n, h->xlocal.total, h->d_xptr[par],
                                                         h->nplanes);
                 PK_CUDA(h, cudaGetLastError());

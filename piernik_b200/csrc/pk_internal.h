@@ -199,6 +199,23 @@ struct pk_ctx {
 
 namespace pk {
 
+// multiprocessors of the current device (looked up once per device); 1-D
+// grid-stride kernels launch at most 16 CTAs of 256 threads per SM
+inline int sm_count()
+{
+    static int cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+inline long long grid_cap() { return (long long)sm_count() * 16; }
+
 int fail(pk_ctx* h, int code, const std::string& msg);
 int ev_begin(pk_ctx* h, std::pair<cudaEvent_t, cudaEvent_t>* p);
 int ev_end(pk_ctx* h, const std::pair<cudaEvent_t, cudaEvent_t>& p);

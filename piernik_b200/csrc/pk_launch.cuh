@@ -372,7 +372,7 @@ int launch_stage(pk_ctx* h, Block& b, int dir, int first, double rk)
         }
         bg.plane = b.plane;
         long long nb = (b.plane + 255) / 256;
-        if (nb > 148LL * 16) nb = 148LL * 16;
+        if (nb > grid_cap()) nb = grid_cap();
         k_copy_pencils<<<(int)nb, 256, 0, h->stream>>>(bg, dir, uout, u, h->nplanes);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
@@ -456,7 +456,7 @@ int launch_unsplit_apply(pk_ctx* h, Block& b, const double* S, double* T, double
     }
     bg.plane = b.plane;
     long long nblk = (b.plane + 255) / 256;
-    if (nblk > 148LL * 16) nblk = 148LL * 16;
+    if (nblk > grid_cap()) nblk = grid_cap();
     k_unsplit_apply<PH><<<(int)nblk, 256, 0, h->stream>>>(bg, S, T, b.flux[0], b.flux[1], b.flux[2], h->pp, h->d_step,
                                                           rk, b.dl[0], b.dl[1], b.dl[2], last, h->d_status);
     PK_CUDA(h, cudaGetLastError());

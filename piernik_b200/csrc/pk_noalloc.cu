@@ -16,8 +16,11 @@
 // overlap on a GPU (other streams, other host threads) race on it and give
 // wrong results.  Each call clears the slots it uses before the reduction.
 // The first call on a device looks up the array's device address with that
-// device current (cudaGetSymbolAddress); make that first call before any
-// stream capture.
+// device current (cudaGetSymbolAddress).  The call is synchronous (it reads
+// the reduction back and waits for its stream), so it is never made while
+// its stream is capturing: it checks that and returns PK_E_STATE.  The
+// stream and every state must belong to the current device (PK_E_ARG
+// otherwise, before anything is launched).
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -112,9 +115,42 @@ extern "C" int pk_timestep_raw_noalloc(const pk_config* cfg, int32_t nblocks, co
                 return say(err, errlen, PK_E_ARG, "block extent and cell size must be positive");
     }
 
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return say(err, errlen, PK_E_CUDA, "cudaGetDevice failed");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the stream must not be capturing (the call reads its result back and
+    // synchronises) and must be one of the current device's
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        (void)cudaGetLastError();
+        return say(err, errlen, PK_E_STATE, "the stream is capturing: this call synchronises and cannot be captured");
+    }
+    if (s) {
+        int sdev = -1;
+        if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return say(err, errlen, PK_E_ARG, "invalid stream");
+        }
+        if (sdev != dev) return say(err, errlen, PK_E_ARG, "stream belongs to another device than the current one");
+    }
+    // every state must be device (or managed) memory of the current device
+    for (int i = 0; i < nblocks; ++i) {
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, states[i]) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return say(err, errlen, PK_E_ARG, "block state is not a CUDA pointer");
+        }
+        if (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged)
+            return say(err, errlen, PK_E_ARG, "block state is not device memory");
+        if (pa.type == cudaMemoryTypeDevice && pa.device != dev)
+            return say(err, errlen, PK_E_ARG, "block state lives on another device than the current one");
+    }
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1)
+        return say(err, errlen, PK_E_CUDA, "cudaDeviceGetAttribute failed");
+
     unsigned long long* slots = nullptr;
     if (int rc = slots_of_current_device(&slots, err, errlen)) return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t bytes = sizeof(unsigned long long) * SLOTS * (size_t)nblocks;
     // the maxima start from zero bits (below every positive double)
     if (cudaMemsetAsync(slots, 0, bytes, s) != cudaSuccess) return say(err, errlen, PK_E_CUDA, "cudaMemsetAsync failed");
@@ -128,7 +164,7 @@ extern "C" int pk_timestep_raw_noalloc(const pk_config* cfg, int32_t nblocks, co
         bg.plane = (long long)bg.ext[0] * bg.ext[1] * bg.ext[2];
         const long long ncell = (long long)bg.n[0] * bg.n[1] * bg.n[2];
         long long grid = (ncell + 255) / 256;
-        if (grid > 148LL * 16) grid = 148LL * 16;
+        if (grid > (long long)nsm * 16) grid = (long long)nsm * 16;
         k_cfl<<<(int)grid, 256, 0, s>>>(bg, states[i], a, slots + SLOTS * i);
     }
     if (cudaGetLastError() != cudaSuccess) return say(err, errlen, PK_E_CUDA, "k_cfl launch failed");

@@ -81,7 +81,14 @@ def load(path: str) -> Simulation:
             raise ValueError(f"{path}: restart format {meta.get('format')} (this library reads {FORMAT})")
         arrays = {k: z[k] for k in z.files if k != "meta"}
     setups = [_setup_from(b["setup"]) for b in meta["blocks"]]
-    sim = Simulation(_setup_from(meta["setup"]))      # block 0 is the run's own Setup
+    phys = _setup_from(meta["setup"])
+    # block 0 takes its own extent, cell size and boundaries (after a
+    # remove_block(0) it is not the block the run was created with); the
+    # physics comes from the run's Setup, which the Simulation keeps
+    s0 = setups[0]
+    sim = Simulation(phys.replace(n=s0.n, nb=s0.nb, xmin=s0.xmin, xmax=s0.xmax, bnd=s0.bnd))
+    sim.setup = phys
+    sim.blocks[0] = s0
     for s in setups[1:]:
         sim.add_block(s)
     if meta["domain"] is not None:

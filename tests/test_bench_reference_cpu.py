@@ -20,6 +20,7 @@ def test_reference_arm_json_line(oracle_lib):
     d = json.loads(lines[0])
     assert KEYS <= set(d), KEYS - set(d)
     assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["config"]["n"] == 32          # the arm runs the configuration its line names
     assert d["value"] > 0 and d["higher_is_better"] is True and d["dtype"] == "f64"
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]

@@ -78,7 +78,8 @@ def test_fused_sweep_bitexact(gpu_lib, oracle_lib, phys, lim):
     compare(ob, sim, "fused sweeps")
 
 
-@pytest.mark.parametrize("tile", [(1, 8, 3), (3, 16, 4), (4, 40, 1), (2, 64, 0), (8, 24, 2), (2, 56, 5)])
+@pytest.mark.parametrize("tile", [(1, 8, 3), (3, 16, 4), (4, 40, 1), (2, 64, 0), (8, 24, 2), (2, 56, 5), (7, 24, 6),
+                                  (1, 50, 6)])
 def test_fused_tiles_agree(gpu_lib, oracle_lib, tile):
     """Tile shapes (pencils per CTA, cells per chunk, launch-bound variant) do
     not change any bit."""

@@ -76,3 +76,33 @@ def test_restart_instances(gpu_lib, tmp_path):
         assert (a.t, a.dt, a.nstep) == (b.t, b.dt, b.nstep)
     back.close()
     sim.close()
+
+
+def test_restart_after_removing_block0(gpu_lib, tmp_path):
+    """Block 0 removed (derefined) before the save: the new block 0 is a base
+    block with another cell size and level than the Setup the run was made
+    with, and the resumed run must still continue bit for bit."""
+    layout = problems.refined_layout(DOM3, REG3[:1], sizes=(8, 16), seed=3)
+    setup = setup_for("mhd", n=(8, 8, 8))
+    blocks = problems.refined_blocks(DOM3, layout, setup, problems.wave_fields(DOM3, seed=5))
+    fine = [i for i, x in enumerate(blocks) if x[1] == 1]
+    assert fine
+    order = [fine[0]] + [i for i in range(len(blocks)) if i != fine[0]]
+    blocks = [blocks[i] for i in order]            # a level-1 block is block 0
+    sim = Simulation(blocks[0][0])
+    for s, *_ in blocks[1:]:
+        sim.add_block(s)
+    sim.set_domain(DOM3, (True, True, True))
+    for i, (s, L, off, u, b, psi) in enumerate(blocks):
+        sim.place_block(i, off, L)
+        sim.upload(u, b, psi, block=i)
+    sim.update_boundaries()
+    sim.run(1)
+    sim.restrict()
+    sim.remove_block(0)
+    sim.update_boundaries()
+    assert sim.placement[0][1] == 0 and sim.blocks[0].dl != sim.setup.dl
+    back = resume_equals(sim, str(tmp_path / "removed0.npz"), before=1, after=2)
+    assert back.placement == sim.placement
+    back.close()
+    sim.close()

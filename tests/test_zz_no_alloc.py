@@ -21,8 +21,12 @@ from piernik_b200.sim import Simulation, make_config
 PK_E_ARG = -1            # include/piernik_b200.h
 
 
-def call_noalloc(lib, setup, blocks, err_len=256):
-    """blocks: list of (n, dl, device pointer); returns (rc, dt, c_all, message)."""
+PK_E_STATE = -5
+
+
+def call_noalloc(lib, setup, blocks, err_len=256, stream=None):
+    """blocks: list of (n, dl, device pointer); stream: a cudaStream_t handle
+    (int) or None; returns (rc, dt, c_all, message)."""
     cfg = make_config(setup)
     nb = len(blocks)
     n = (C.c_int32 * (3 * nb))(*[x for b in blocks for x in b[0]])
@@ -30,7 +34,8 @@ def call_noalloc(lib, setup, blocks, err_len=256):
     ptrs = (C.c_void_p * nb)(*[b[2] for b in blocks])
     dt, c_all = C.c_double(-1.0), C.c_double(-1.0)
     err = C.create_string_buffer(err_len)
-    rc = lib.pk_timestep_raw_noalloc(C.byref(cfg), nb, n, dl, ptrs, None, C.byref(dt), C.byref(c_all), err, err_len)
+    rc = lib.pk_timestep_raw_noalloc(C.byref(cfg), nb, n, dl, ptrs, C.c_void_p(stream), C.byref(dt),
+                                     C.byref(c_all), err, err_len)
     return rc, dt.value, c_all.value, err.value.decode()
 
 
@@ -45,12 +50,19 @@ def test_noalloc_rejects_too_many_blocks():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("phys", ["hd", "mhd"])
-def test_noalloc_matches_timestep_raw(gpu_lib, phys):
+@pytest.mark.parametrize("phys,shape,on_stream", [
+    ("hd", "3d", False), ("mhd", "3d", False), ("mhd", "3d", True),
+    ("hd", "2d", False), ("mhd", "2d", True)])
+def test_noalloc_matches_timestep_raw(gpu_lib, phys, shape, on_stream):
+    """Blocks of 3D and 2D (n_z = 1: no z guard cells) extents, on the legacy
+    default stream and on a stream of the caller's."""
     import torch
 
-    s1 = setup_for(phys, n=(20, 14, 11), lim="moncen")
-    s2 = setup_for(phys, n=(9, 16, 12), lim="moncen")
+    n1, n2 = ((20, 14, 11), (9, 16, 12)) if shape == "3d" else ((16, 12, 1), (10, 18, 1))
+    s1 = setup_for(phys, n=n1, lim="moncen")
+    s2 = setup_for(phys, n=n2, lim="moncen")
+    stream = torch.cuda.Stream() if on_stream else None
+    handle = stream.cuda_stream if on_stream else None
     slow = [random_state(s1, seed=1), random_state(s2, seed=2)]
     fast = []
     for (u, b, psi), s in zip(slow, (s1, s2)):
@@ -76,7 +88,7 @@ def test_noalloc_matches_timestep_raw(gpu_lib, phys):
         dt_ref, c_ref, dev = on_handle(states)
         torch.cuda.synchronize()
         blocks = [(s1.n, s1.dl, dev[0].data_ptr()), (s2.n, s2.dl, dev[1].data_ptr())]
-        rc, dt, c_all, msg = call_noalloc(gpu_lib, s1, blocks)
+        rc, dt, c_all, msg = call_noalloc(gpu_lib, s1, blocks, stream=handle)
         assert rc == L.PK_OK, msg
         assert np.float64(dt).view(np.uint64) == np.float64(dt_ref).view(np.uint64), (dt, dt_ref)
         assert np.float64(c_all).view(np.uint64) == np.float64(c_ref).view(np.uint64), (c_all, c_ref)
@@ -85,6 +97,38 @@ def test_noalloc_matches_timestep_raw(gpu_lib, phys):
         sim.upload(*states[0])
         dt1, c1 = sim.timestep_raw()
         sim.close()
-        rc, dt, c_all, msg = call_noalloc(gpu_lib, s1, blocks[:1])
+        rc, dt, c_all, msg = call_noalloc(gpu_lib, s1, blocks[:1], stream=handle)
         assert rc == L.PK_OK, msg
         assert (dt, c_all) == (dt1, c1)
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_host_memory(gpu_lib):
+    """A state in host memory is refused before any launch (a kernel given it
+    would fault or read the wrong memory)."""
+    s = setup_for("hd", n=(8, 8, 8))
+    host = np.zeros(s.nvar * 16 ** 3)
+    rc, _, _, msg = call_noalloc(gpu_lib, s, [(s.n, s.dl, host.ctypes.data)])
+    assert rc == PK_E_ARG and "device memory" in msg
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_capture(gpu_lib):
+    """The call synchronises its stream, so it refuses to run while that
+    stream is capturing (the caller's graph stays valid)."""
+    import torch
+
+    s = setup_for("hd", n=(8, 8, 8))
+    x = torch.zeros(s.nvar * 16 ** 3, dtype=torch.float64, device="cuda")
+    # first call outside any capture
+    rc, _, _, msg = call_noalloc(gpu_lib, s, [(s.n, s.dl, x.data_ptr())])
+    assert rc == L.PK_OK, msg
+    stream = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        x.add_(1.0)
+        rc, _, _, msg = call_noalloc(gpu_lib, s, [(s.n, s.dl, x.data_ptr())], stream=stream.cuda_stream)
+    assert rc == PK_E_STATE and "capturing" in msg
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(x[0]) == 1.0
