@@ -52,6 +52,13 @@ TRAFFIC_BYTES_PER_CELL = (161.756672e6 + 125.965568e6) / 128 ** 3
 # _pred_on.sum) of the whole-pencil x sweep of a 128^3 block over its 128^3
 # cells, in the bit-exact build
 FP64_FLOP_PER_CELL_SWEEP = 3.589298377e9 / 128 ** 3
+# the same count for the tolerance-mode (fma) sweep; None until measured
+FP64_FLOP_PER_CELL_SWEEP_FMA = None
+ARITH_NOTE = {
+    "fma": "fma: multiply-add contraction and hoisted reciprocals in the fused sweep; agrees with the "
+           "reference's arithmetic to <= 1e-12 relative per step and <= 1e-9 after 100 steps (tests/test_gpu_fma.py)",
+    "bitexact": "bitexact: the reference's operation order and rounding, equal to the oracle bit for bit",
+}
 
 
 def parse():
@@ -79,6 +86,10 @@ def parse():
     p.add_argument("--group", type=int, default=8, help="instances stacked per handle (batched-adjoint)")
     p.add_argument("--k", type=int, default=50, help="time steps differentiated (batched-adjoint)")
     p.add_argument("--nblocks", type=int, default=512)
+    p.add_argument("--arith", default="both", choices=["both", "fma", "bitexact"],
+                   help="arithmetic of the fused sweep; both: the headline in fma, bitexact beside it")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the bounded C3 / C4 / C5 measurements appended to the headline line")
     p.add_argument("--tiles", default=None,
                    help="fix fused-sweep tiles instead of autotuning, e.g. 'x:1,88,3;y:4,56,2;z:4,56,2' (P,L,variant)")
     return p.parse_args()
@@ -247,7 +258,36 @@ def adjoint_cost(sim, stream, args, fwd_ms_per_step, barrier, max_over_ranks):
             "adjoint_sweep_ms": adj_sweep, "fused_sweep_ms": fwd_ms_per_step / 6}
 
 
+def tune_tiles(sim, args, slab, rank):
+    """Fused-sweep tiles: --tiles as given, else the autotuner's picks (on a
+    multi-rank run rank 0 tunes alone and every rank takes its choice)."""
+    import torch
+    if args.tiles:
+        tiles = {}
+        for item in args.tiles.split(";"):
+            ax, vals = item.split(":")
+            P, Lc, V = (int(x) for x in vals.split(","))
+            sim.set_tile("xyz".index(ax), P, Lc, V)
+            tiles[ax] = [P, Lc, V]
+        return tiles
+    if args.no_autotune:
+        return None
+    from piernik_b200.autotune import autotune
+    if slab is not None:
+        slab.detach()
+    best = autotune(sim, reps=2, verbose=False)
+    if slab is not None:
+        pick = [best]
+        torch.distributed.broadcast_object_list(pick, src=0)
+        best = pick[0]
+        for d, v in best.items():
+            sim.set_tile(d, v["P"], v["L"], v["V"])
+        slab.attach()
+    return {"xyz"[d]: [v["P"], v["L"], v["V"], round(v["ms"], 4)] for d, v in best.items()}
+
+
 def our_arm(args):
+    import ctypes
     import numpy as np
     import torch
     world, rank, local = dist_env()
@@ -256,8 +296,8 @@ def our_arm(args):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    from piernik_b200 import build, problems
-    from piernik_b200._lib import PK_LAYOUT_FORTRAN
+    from piernik_b200 import _lib, build, problems
+    from piernik_b200._lib import PK_LAYOUT_FORTRAN, PkTimeState
     from piernik_b200.sim import Simulation
     build.build()
     n = args.n
@@ -265,7 +305,7 @@ def our_arm(args):
     slab = None
     if world > 1:
         # weak scaling: the level is n x n x (n * world), one n^3 slab per rank,
-        # z halos moved by NCCL before every sweep, dt reduced over ranks
+        # z halos moved by NCCL before every z sweep, dt reduced over ranks
         from piernik_b200.slabs import SlabRank, TorchTransport
         gsetup = setup.replace(n=(n, n, n * world),
                                xmax=(setup.xmax[0], setup.xmax[1],
@@ -276,31 +316,6 @@ def our_arm(args):
         sim = Simulation(setup)
     sim.upload(u, b, psi)
     stream = torch.cuda.ExternalStream(sim.stream)
-    tiles = None
-    if args.tiles:
-        tiles = {}
-        for item in args.tiles.split(";"):
-            ax, vals = item.split(":")
-            P, Lc, V = (int(x) for x in vals.split(","))
-            sim.set_tile("xyz".index(ax), P, Lc, V)
-            tiles[ax] = [P, Lc, V]
-    elif not args.no_autotune:
-        from piernik_b200.autotune import autotune
-        log = open(args.tune_log, "w") if (args.tune_log and rank == 0) else None
-        if slab is not None:
-            slab.detach()                 # tune on this rank alone; every rank then takes rank 0's choice
-        best = autotune(sim, reps=2, verbose=False)
-        if slab is not None:
-            pick = [best]
-            torch.distributed.broadcast_object_list(pick, src=0)
-            best = pick[0]
-            for d, v in best.items():
-                sim.set_tile(d, v["P"], v["L"], v["V"])
-            slab.attach()
-        tiles = {"xyz"[d]: [v["P"], v["L"], v["V"], round(v["ms"], 4)] for d, v in best.items()}
-        if log:
-            json.dump(best, log, indent=1)
-            log.close()
 
     def barrier():
         torch.cuda.synchronize()
@@ -315,45 +330,61 @@ def our_arm(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (also compiles nothing: the library is prebuilt)
-    sim.run(args.warmup)
-    barrier()
-    clocks = Clocks(local)
-    sim.profile(True)
-    launches0, _, _ = sim.profile_read()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    sim.run(args.steps)
-    e1.record(stream)
-    e1.synchronize()
-    launches1, nsweep, sweep_ms = sim.profile_read()
-    sim.profile(False)
-    ck = clocks.stop()
-    barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    cell_updates = 2.0 * n ** 3 * args.steps * world
-    value = cell_updates / (ms / 1e3)
-
-    # roofline of the fused sweep kernel (algorithmic bytes: read + write 9 planes of n^3)
     hbm, src = peaks()
-    bytes_per_launch = 2.0 * NVAR * 8 * n ** 3
-    launch_ms = sweep_ms / max(nsweep, 1)
-    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
-    traffic = TRAFFIC_BYTES_PER_CELL * n ** 3
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "kernel": "k_sweep_fused<MHD> (one sweep direction, both RK2 stages)",
-                "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms, "peak_source": src}
-    # the bound that limits it: FP64 issue, against the device's measured DFMA rate
-    import ctypes
-    from piernik_b200 import _lib
     peak64 = ctypes.c_double(0.0)
-    roofline_fp64 = None
-    if _lib.load().pk_fp64_peak(ctypes.byref(peak64)) == 0 and peak64.value > 0:
-        flops = FP64_FLOP_PER_CELL_SWEEP * n ** 3
-        got = flops / (launch_ms / 1e3) / 1e12
-        roofline_fp64 = {"bound": "fp64", "achieved": got, "peak": peak64.value, "unit": "TFLOP/s",
-                         "frac": got / peak64.value, "flop_per_launch": flops,
-                         "peak_source": "measured (pk_fp64_peak: independent DFMA chains)"}
+    have64 = _lib.load().pk_fp64_peak(ctypes.byref(peak64)) == 0 and peak64.value > 0
+    modes = ["fma", "bitexact"] if args.arith == "both" else [args.arith]
+    cell_updates = 2.0 * n ** 3 * args.steps * world
+    res = {}
+    for mode in modes:
+        # every mode starts from the same initial state and time
+        sim.upload(u, b, psi)
+        sim.time_state = PkTimeState()
+        sim.set_arithmetic(mode)
+        tiles = tune_tiles(sim, args, slab, rank)
+        sim.run(args.warmup)
+        barrier()
+        clocks = Clocks(local)
+        sim.profile(True)
+        launches0, _, _ = sim.profile_read()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.run(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        launches1, nsweep, sweep_ms = sim.profile_read()
+        sim.profile(False)
+        ck = clocks.stop()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        # roofline of the fused sweep kernel (algorithmic bytes: read + write 9 planes of n^3)
+        bytes_per_launch = 2.0 * NVAR * 8 * n ** 3
+        launch_ms = sweep_ms / max(nsweep, 1)
+        achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "traffic": TRAFFIC_BYTES_PER_CELL * n ** 3,
+                    "kernel": f"k_sweep_fused<MHD> ({mode} arithmetic; one sweep direction, both RK2 stages)",
+                    "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms, "peak_source": src}
+        # the bound that limits it: FP64 issue, against the device's measured DFMA rate
+        roofline_fp64 = None
+        fpc = FP64_FLOP_PER_CELL_SWEEP if mode == "bitexact" else FP64_FLOP_PER_CELL_SWEEP_FMA
+        if have64 and fpc:
+            flops = fpc * n ** 3
+            got = flops / (launch_ms / 1e3) / 1e12
+            roofline_fp64 = {"bound": "fp64", "achieved": got, "peak": peak64.value, "unit": "TFLOP/s",
+                             "frac": got / peak64.value, "flop_per_launch": flops,
+                             "flop_count": f"FP64 flops executed per cell by the {mode} whole-pencil sweep (ncu)",
+                             "peak_source": "measured (pk_fp64_peak: independent DFMA chains)"}
+        res[mode] = {"value": cell_updates / (ms / 1e3), "ms_per_step": ms / args.steps, "roofline": roofline,
+                     "roofline_fp64": roofline_fp64, "gpu_launches": launches1 - launches0, "clocks": ck,
+                     "tiles_P_L_variant_ms": tiles}
+    head = modes[0]
+    sim.upload(u, b, psi)
+    sim.time_state = PkTimeState()
+    sim.set_arithmetic(head)
+    if res[head]["tiles_P_L_variant_ms"]:
+        for ax, t in res[head]["tiles_P_L_variant_ms"].items():
+            sim.set_tile("xyz".index(ax), t[0], t[1], t[2])
 
     # end to end through the C ABI with host buffers in the reference's layout
     e2e = None
@@ -378,13 +409,19 @@ def our_arm(args):
         ms2 = max_over_ranks(e2.elapsed_time(e3))
         nbytes = (pu.nbytes + pb.nbytes + pp.nbytes)
         e2e = {"value": cell_updates / (ms2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes, "ms_per_step": ms2 / args.steps,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": ms2 / args.steps, "arithmetic": head,
                "path": "pk_upload(Fortran layout, pinned) + pk_run(1) + pk_download per step"}
         sim.time_state = st0
 
     adjoint = None
     if not args.no_adjoint and world == 1:
-        adjoint = adjoint_cost(sim, stream, args, ms / args.steps, barrier, max_over_ranks)
+        # the adjoint kernels and the recomputation run in the bit-exact
+        # arithmetic: compare with forward steps in that arithmetic
+        ref = "bitexact" if "bitexact" in res else head
+        sim.set_arithmetic(ref)
+        adjoint = adjoint_cost(sim, stream, args, res[ref]["ms_per_step"], barrier, max_over_ranks)
+        adjoint["forward_arithmetic"] = ref
+        sim.set_arithmetic(head)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -393,24 +430,40 @@ def our_arm(args):
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
                "sample": f"1 step of the workload at {cn}^3 ({2 * cn ** 3} cell-updates, {el:.1f} s) with "
                          f"oracle/pk_oracle.c on {thr} OpenMP threads"}
+    sim.close()
+
+    extras = {}
+    if world == 1 and not args.no_extras:
+        for name, fn in (("c3_refined", lambda: c3_refined(args, steps=2, warmup=1, arith=head)),
+                         ("c4_ot_gradient", lambda: c4_ot_gradient(args, ndirs=4, n=512, K=100)),
+                         ("c5_batched_adjoint", lambda: c5_batched_adjoint(args, K=10, ngroups=1, warmup=1,
+                                                                           steps=1))):
+            try:
+                extras[name] = fn()
+            except Exception as e:        # an extra never costs the headline line
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        r = res[head]
+        out = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "arithmetic": ARITH_NOTE[head],
                "config": dict(workload_config(n), parallelism=("one block" if world == 1 else
                                                                f"{world} z-slabs of {n}^3, NCCL halo exchange"),
-                              tiles_P_L_variant_ms=tiles),
-               "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
-               "gpu_launches": launches1 - launches0, "clocks": ck,
+                              tiles_P_L_variant_ms=r["tiles_P_L_variant_ms"]),
+               "roofline": r["roofline"], "roofline_fp64": r["roofline_fp64"], "cpu_baseline": cpu, "e2e": e2e,
+               "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
                "adjoint_cost_ratio": adjoint}
+        for mode in modes[1:]:
+            out[mode] = dict(res[mode], arithmetic=ARITH_NOTE[mode])
+        out.update(extras)
         print(json.dumps(out), flush=True)
-    sim.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
-def batched_arm(args):
+def c3_refined(args, steps=None, warmup=None):
     """The uneven-blocks workload on a three-level refinement
     (problems.refined_blast, seed 4): 515 blocks with edges from
     {16,24,32,48,64} (64 on the base level, 128^3 cells; a level-1 box of
@@ -421,7 +474,10 @@ def batched_arm(args):
     are replayed from one CUDA graph.  A cell-update is one cell of any block
     (covered ones included: the reference sweeps them too) advanced by one
     dt.  Timed beside one block of the same physics and a similar cell count
-    through the single-block fused path."""
+    through the single-block fused path, both in the bit-exact arithmetic (the
+    stage kernels of refined domains have no other).  Returns the JSON record."""
+    steps = steps or args.steps
+    warmup = args.warmup if warmup is None else warmup
     import torch
     from piernik_b200 import build, problems
     from piernik_b200.autotune import autotune
@@ -455,19 +511,19 @@ def batched_arm(args):
         tune[v] = t0.elapsed_time(t1)
     best_v = min(tune, key=tune.get)
     sim.set_stage_variant(best_v)
-    sim.run(args.warmup)
+    sim.run(warmup)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = Clocks(0)
     l0, _, _ = sim.profile_read()
     e0.record(stream)
-    sim.run(args.steps)
+    sim.run(steps)
     e1.record(stream)
     e1.synchronize()
     l1, _, _ = sim.profile_read()
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
-    refined = 2.0 * cells * args.steps / (ms / 1e3)
+    refined = 2.0 * cells * steps / (ms / 1e3)
     st = sim.time_state
     sim.close()
     # one block of the same physics and a similar number of cells
@@ -476,18 +532,18 @@ def batched_arm(args):
     s1 = Simulation(one[0])
     s1.upload(*one[1:])
     autotune(s1, reps=1)
-    s1.run(args.warmup)
+    s1.run(warmup)
     st1 = torch.cuda.ExternalStream(s1.stream)
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(st1)
-    s1.run(args.steps)
+    s1.run(steps)
     e3.record(st1)
     e3.synchronize()
-    single = 2.0 * side ** 3 * args.steps / (e2.elapsed_time(e3) / 1e3)
+    single = 2.0 * side ** 3 * steps / (e2.elapsed_time(e3) / 1e3)
     s1.close()
     out = {"metric": "FP64 3-fluid MHD cell-updates/s, %d blocks on 3 refinement levels" % sum(levels),
-           "value": refined, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "value": refined, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warmup,
+           "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic",
            "config": {"workload": "refined blast: uneven blocks (edges 16..64) on 3 levels of a periodic 128^3 "
                                   "base domain, ion MHD + neutral + dust, vanleer, CFL 0.7, fine->coarse flux "
@@ -496,7 +552,11 @@ def batched_arm(args):
                       "stage_variant": best_v, "stage_variant_ms_per_step": tune},
            "single_block": {"n": side, "value": single, "ratio_refined_to_single": refined / single},
            "t_end": st.t, "gpu_launches": l1 - l0, "clocks": ck}
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def batched_arm(args):
+    print(json.dumps(c3_refined(args)), flush=True)
 
 
 def batched_independent_arm(args):
@@ -607,22 +667,22 @@ def adjoint_arm(args):
     sim.close()
 
 
-def ot_gradient_arm(args):
+def c4_ot_gradient(args, ndirs=16, n=None, K=None):
     """C4: the differentiable Orszag-Tang vortex at 512^2 (--n), loss = magnetic
     energy of the central 128^2 cells after K = --steps steps (default 100
     when --steps is left at 10), gradient with respect to the relative density
     perturbation (1e-3 x a seeded unit-rms Gaussian random field, correlation
     8 cells) through torch.autograd with sqrt(K) checkpointing; checked
     against central differences along 16 seeded directions at eps = 1e-6 and
-    1e-7 at the dt sequence of the unperturbed run."""
+    1e-7 at the dt sequence of the unperturbed run.  Returns the record."""
     import numpy as np
     import torch
     from piernik_b200 import build, problems
     from piernik_b200.autograd import advance, central_magnetic_energy, last_dts, orszag_tang_state
     from piernik_b200.sim import Simulation
     build.build()
-    n = args.n if args.n != 256 else 512
-    K = args.steps if args.steps != 10 else 100
+    n = n or (args.n if args.n != 256 else 512)
+    K = K or (args.steps if args.steps != 10 else 100)
     s = problems.orszag_tang_fields(n)[0]
     sim = Simulation(s)
     stream = torch.cuda.ExternalStream(sim.stream)
@@ -674,7 +734,7 @@ def ot_gradient_arm(args):
 
     rng = np.random.default_rng(21)
     rows = []
-    for k in range(16):
+    for k in range(ndirs):
         v = problems.gaussian_random_field((n, n), 8.0, rng)
         vt = torch.tensor(v, device="cuda")
         ad = float(np.sum(grad * v))
@@ -687,17 +747,22 @@ def ot_gradient_arm(args):
         rows.append(row)
     rel6 = [r["rel_1e-06"] for r in rows]
     rel7 = [r["rel_1e-07"] for r in rows]
-    res = {"workload": f"differentiable Orszag-Tang {n}^2, K = {K}, loss = central {cy}^2 magnetic energy",
+    res = {"workload": f"differentiable Orszag-Tang {n}^2, K = {K}, loss = central {cy}^2 magnetic energy, "
+                       f"{ndirs} FD directions", "arithmetic": "bitexact",
            "forward_ms": fwd_ms, "recorded_forward_plus_loss_ms": t0.elapsed_time(t1),
            "backward_ms": t1.elapsed_time(t2), "gradient_over_forward": t0.elapsed_time(t2) / fwd_ms,
            "fd_rel_error_eps1e-6": {"median": float(np.median(rel6)), "max": float(np.max(rel6))},
            "fd_rel_error_eps1e-7": {"median": float(np.median(rel7)), "max": float(np.max(rel7))},
            "directions": rows}
-    print(json.dumps(res), flush=True)
     sim.close()
+    return res
 
 
-def batched_adjoint_arm(args):
+def ot_gradient_arm(args):
+    print(json.dumps(c4_ot_gradient(args)), flush=True)
+
+
+def c5_batched_adjoint(args, K=None, ngroups=None, warmup=None, steps=None):
     """Batched adjoint: --instances independent 128^3 ideal-MHD turbulence
     instances (the 256^3 recipe with rms Mach log-uniform in [0.5, 5] and B0
     uniform in [0.05, 0.5], seeded), loss = sum over instances of the
@@ -712,7 +777,9 @@ def batched_adjoint_arm(args):
     step).  A "step" of this workload is the gradient of one group; the
     timed steps cycle over the groups, so --steps = instances / group covers
     the whole ensemble once.  Beside it: K plain forward steps of a group,
-    and the gradient of one instance in a handle of its own."""
+    and the gradient of one instance in a handle of its own.  Returns the
+    record (K, the number of groups, warm-up and timed steps default to the
+    command line's)."""
     import torch
     from piernik_b200 import build, problems
     from piernik_b200._lib import PkTimeState
@@ -721,9 +788,10 @@ def batched_adjoint_arm(args):
     build.build()
     torch.cuda.set_device(0)
     n = args.n if args.n != 256 else 128
-    G, K = args.group, args.k
-    ngroups = max(1, args.instances // G)
-    steps = args.steps if args.steps != 10 else ngroups
+    G, K = args.group, (K or args.k)
+    ngroups = ngroups or max(1, args.instances // G)
+    steps = steps or (args.steps if args.steps != 10 else ngroups)
+    warmup = args.warmup if warmup is None else warmup
     every = 2
     params = problems.turbulence_ensemble(ngroups * G, n, args.seed)
     groups = []
@@ -747,7 +815,7 @@ def batched_adjoint_arm(args):
         loss.backward()
         return v.grad, loss.detach()
 
-    for w in range(args.warmup):
+    for w in range(warmup):
         gradient(sim, groups[w % ngroups], G)
     torch.cuda.synchronize()
     clocks = Clocks(0)
@@ -797,7 +865,7 @@ def batched_adjoint_arm(args):
     cells = G * n ** 3
     value = 2.0 * cells * K * steps / (ms / 1e3)
     out = {"metric": "FP64 MHD cell-updates/s differentiated (forward + adjoint), stacked 128^3 instances",
-           "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+           "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warmup,
            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic",
            "config": {"workload": f"batched adjoint: {ngroups * G} independent {n}^3 ideal-MHD turbulence "
@@ -815,7 +883,11 @@ def batched_adjoint_arm(args):
            "instance_dt_spread": [min(dts), max(dts)],
            "loss_last_group": float(losses[-1]), "grad_norm_last_group": gnorm,
            "gpu_launches": l1 - l0, "clocks": ck}
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def batched_adjoint_arm(args):
+    print(json.dumps(c5_batched_adjoint(args)), flush=True)
 
 
 def unsplit_arm(args):

@@ -199,6 +199,21 @@ int pk_sync(pk_handle h);
  * default.  Used by the autotuner; 0 keeps the built-in P / L. */
 int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32_t variant);
 
+/* Arithmetic of the fused and batched sweeps (no counterpart in the
+ * reference, whose arithmetic is gfortran -O2 SSE2 without FMA):
+ *   PK_ARITH_BITEXACT (default): every operation in the reference's order and
+ *     rounding; results equal the reference's bit for bit.
+ *   PK_ARITH_FMA: multiply-add contraction and divisions by a common
+ *     denominator replaced by one reciprocal (1/rho, 1/(gamma-1), 1/gamma,
+ *     1/(S-S_M) and the other HLLD denominators, 1/ch); same branches and
+ *     algorithm, rounding differs by a few units in the last place per
+ *     operation, so a time step agrees with the bit-exact one to ~1e-15
+ *     relative (tested to 1e-12 per step and 1e-9 after 100 steps).
+ * The per-block stage path, the unsplit scheme and the adjoint kernels
+ * always use the bit-exact arithmetic. */
+enum { PK_ARITH_BITEXACT = 0, PK_ARITH_FMA = 1 };
+int pk_set_arithmetic(pk_handle h, int32_t mode);
+
 /* Sweep all blocks in one persistent launch over a work list of tiles (the
  * default whenever more than one block is registered; enable = 1 forces it for
  * a single block), with chunks of at most `length` cells and the given

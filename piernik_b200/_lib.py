@@ -21,6 +21,7 @@ PK_LIM = {"vanleer": 0, "minmod": 1, "moncen": 2, "superbee": 3}
 PK_LAYOUT_FORTRAN, PK_LAYOUT_SOA = 0, 1
 PK_EULER, PK_RK2_1, PK_RK2_2 = 10000, 10001, 10002
 PK_ST_DN_NEGATIVE, PK_ST_EI_NEGATIVE = 1, 2
+PK_ARITH = {"bitexact": 0, "fma": 1}
 
 # every symbol include/piernik_b200.h declares
 EXPORTS = (
@@ -28,7 +29,7 @@ EXPORTS = (
     "pk_upload", "pk_download", "pk_solve_cg", "pk_fill_guards", "pk_sweep", "pk_glm_damp",
     "pk_timestep_raw", "pk_time_step", "pk_fluid_update", "pk_run", "pk_get_time_state",
     "pk_set_time_state", "pk_status", "pk_sync", "pk_set_tile", "pk_stream", "pk_profile_enable",
-    "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_use_graph",
+    "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_use_graph", "pk_set_arithmetic",
     "pk_upload_device", "pk_download_device", "pk_adjoint_set", "pk_adjoint_get", "pk_adjoint_sweep",
     "pk_grad_forward", "pk_grad_backward", "pk_grad_release",
     "pk_timestep_raw_noalloc", "pk_set_adjoint_tile", "pk_set_domain", "pk_block_place",
@@ -156,6 +157,7 @@ def load(path: str = LIBPATH):
     L.pk_tile_variants.argtypes = [C.POINTER(C.c_int32)] * 3
     L.pk_set_batch.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
     L.pk_use_graph.argtypes = [H, C.c_int32]
+    L.pk_set_arithmetic.argtypes = [H, C.c_int32]
     L.pk_set_instances.argtypes = [H, C.c_int32]
     L.pk_block_place_level.argtypes = [H, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]
     L.pk_set_stage_variant.argtypes = [H, C.c_int32]

@@ -3,7 +3,9 @@
 ``--fmad=false`` keeps every multiply and add separately rounded, the IEEE
 double division and square root are the defaults, and nothing is compiled
 with fast-math: this is what makes the kernels reproduce the reference's
-gfortran -O2 (SSE2, no FMA) arithmetic bit for bit.
+gfortran -O2 (SSE2, no FMA) arithmetic bit for bit.  The pk_fast_*.cu units
+(the tolerance-mode sweeps) are the exception: they are compiled with
+``--fmad=true`` and instantiate only their own kernels.
 """
 from __future__ import annotations
 
@@ -13,9 +15,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["pk_api.cu", "pk_noalloc.cu", "pk_peak.cu", "pk_exchange.cpp", "pk_levels.cpp", "pk_phys_hd1.cu", "pk_phys_hd2.cu", "pk_phys_mhd1.cu", "pk_phys_mhd2.cu", "pk_phys_mhd3.cu"]
+PHYS = ["hd1", "hd2", "mhd1", "mhd2", "mhd3"]
+# the tolerance-mode units (pk_set_arithmetic(PK_ARITH_FMA)) are the only ones
+# compiled with multiply-add contraction
+FAST_UNITS = [f"pk_fast_{p}.cu" for p in PHYS]
+UNITS = (["pk_api.cu", "pk_noalloc.cu", "pk_peak.cu", "pk_exchange.cpp", "pk_levels.cpp"]
+         + [f"pk_phys_{p}.cu" for p in PHYS] + FAST_UNITS)
 HEADERS = ["pk_device.cuh", "pk_kernels.cuh", "pk_aux.cuh", "pk_internal.h", "pk_launch.cuh", "pk_adjoint.cuh", "pk_levels.h",
-           "pk_adjoint_kernels.cuh", "pk_exchange.h"]
+           "pk_adjoint_kernels.cuh", "pk_exchange.h", "pk_fast.cuh"]
 DEPS = [os.path.join(CSRC, f) for f in UNITS + HEADERS]
 INC = os.path.join(os.path.dirname(HERE), "include")
 OUT = os.path.join(HERE, "libpiernik_b200.so")
@@ -42,7 +49,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for unit in UNITS:
         obj = os.path.join(objdir, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
-        cmd = [NVCC] + FLAGS + (["-Xptxas=-v"] if verbose else []) + ["-I", INC, "-c", "-o", obj,
+        flags = [("--fmad=true" if f == "--fmad=false" else f) for f in FLAGS] if unit in FAST_UNITS else FLAGS
+        cmd = [NVCC] + flags + (["-Xptxas=-v"] if verbose else []) + ["-I", INC, "-c", "-o", obj,
                                                                     os.path.join(CSRC, unit)]
         procs.append((unit, subprocess.Popen(cmd)))
     bad = [u for u, p in procs if p.wait() != 0]

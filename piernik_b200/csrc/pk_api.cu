@@ -85,6 +85,17 @@ int grid1d(long long n, int threads)
     return (int)(b < 1 ? 1 : b);
 }
 
+const FastOps* fast_ops_of(pk_ctx* h)
+{
+    switch (h->phys) {
+    case 0: return fast_ops_hd1();
+    case 1: return fast_ops_hd2();
+    case 2: return fast_ops_mhd1();
+    case 3: return fast_ops_mhd2();
+    default: return fast_ops_mhd3();
+    }
+}
+
 const PhysOps* ops_of(pk_ctx* h)
 {
     switch (h->phys) {
@@ -800,14 +811,17 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
     if (fused_ok(h)) {
         if (int rc = ensure_pingpong(h)) return rc;
         if (int rc = exchange_guards(h, dir)) return rc;   // connected domains: halos come from the guards
+        const FastOps* fo = h->arith == PK_ARITH_FMA ? fast_ops_of(h) : nullptr;
         if ((h->batched && h->ninst < 2) || h->blocks.size() > 1) {
             if (int rc = build_batch(h)) return rc;
-            if (int rc = ops->batched(h, dir, apply_fac, h->d_counter + dir)) return rc;
+            if (int rc = fo ? fo->batched(h, dir, apply_fac, h->d_counter + dir)
+                            : ops->batched(h, dir, apply_fac, h->d_counter + dir))
+                return rc;
             for (auto& b : h->blocks) b.guards_stale = true;
         } else {
             for (auto& b : h->blocks)
                 if (b.n[dir] > 1)
-                    if (int rc = ops->fused(h, b, dir, apply_fac)) return rc;
+                    if (int rc = fo ? fo->fused(h, b, dir, apply_fac) : ops->fused(h, b, dir, apply_fac)) return rc;
         }
         h->cur ^= 1;
         return PK_OK;
@@ -1023,6 +1037,8 @@ int pk_create(const pk_config* cfg, pk_handle* out)
         nvf += (c.fluid_kind[f] == PK_FLUID_DST) ? 4 : 5;
         h->pp.gam[f] = (c.fluid_kind[f] == PK_FLUID_DST) ? -1.0 : c.gamma[f];
         h->pp.gam_1[f] = h->pp.gam[f] - 1.0;
+        h->pp.rgam_1[f] = 1.0 / h->pp.gam_1[f];
+        h->pp.rgam[f] = 1.0 / h->pp.gam[f];
     }
     h->nvf = nvf;
     h->ib = nvf;
@@ -1995,6 +2011,17 @@ int pk_sync(pk_handle h)
 {
     if (!h) return PK_E_ARG;
     PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PK_OK;
+}
+
+int pk_set_arithmetic(pk_handle h, int32_t mode)
+{
+    if (!h) return PK_E_ARG;
+    if (mode != PK_ARITH_BITEXACT && mode != PK_ARITH_FMA) return fail(h, PK_E_ARG, "unknown arithmetic mode");
+    if (mode == PK_ARITH_FMA)
+        if (int rc = fast_ops_of(h)->prepare(h)) return rc;   // kernel attributes, before any capture
+    if (mode != h->arith) invalidate_graph(h);
+    h->arith = mode;
     return PK_OK;
 }
 

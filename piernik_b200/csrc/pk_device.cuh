@@ -92,6 +92,8 @@ struct Phys {
 struct PhysParams {
     double gam[3];      // adiabatic index per fluid (dust: -1)
     double gam_1[3];    // gam - 1
+    double rgam_1[3];   // 1 / (gam - 1), 1 / gam: the tolerance-mode kernels multiply by these
+    double rgam[3];
     double smalld, smallei;
     int use_smalld, use_smallei, disallow_negatives;
     int lim, limb;      // flimiter, blimiter

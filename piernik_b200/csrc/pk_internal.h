@@ -131,6 +131,7 @@ struct pk_ctx {
     pk_time_state ts;
     std::string err;
     int tileP[3] = {0, 0, 0}, tileL[3] = {0, 0, 0}, tileV[3] = {-1, -1, -1};
+    int arith = 0;                      // PK_ARITH_*: the fused / batched sweeps' arithmetic
     int batched = 0;                    // 1: sweep all blocks in one persistent launch
     int batch_variant = 2;              // launch-bound variant of the batched kernel
     int batch_L = 56;                   // longest chunk of the batched tiles
@@ -237,6 +238,20 @@ struct PhysOps {
     int (*unsplit_flux)(pk_ctx* h, Block& b, int dir, const double* in, double* F);
     int (*unsplit_apply)(pk_ctx* h, Block& b, const double* S, double* T, double rk, int last);
 };
+
+// the fused and batched sweeps in the tolerance-mode arithmetic (pk_fast_*.cu,
+// compiled with multiply-add contraction; pk_set_arithmetic)
+struct FastOps {
+    int (*prepare)(pk_ctx* h);
+    int (*fused)(pk_ctx* h, Block& b, int dir, int apply_fac);
+    int (*batched)(pk_ctx* h, int dir, int apply_fac, unsigned* counter);
+};
+
+const FastOps* fast_ops_hd1();
+const FastOps* fast_ops_hd2();
+const FastOps* fast_ops_mhd1();
+const FastOps* fast_ops_mhd2();
+const FastOps* fast_ops_mhd3();
 
 const PhysOps* ops_hd1();
 const PhysOps* ops_hd2();

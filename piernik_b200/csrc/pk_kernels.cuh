@@ -23,7 +23,7 @@
 //     2-cell halo, pencil ends (the outermost guard cells) handled with the
 //     reference's one-sided rules, written back in place.
 #pragma once
-#include "pk_device.cuh"
+#include "pk_fast.cuh"
 
 namespace pk {
 
@@ -122,7 +122,9 @@ struct Smem {
 //          fc_in is set, the flux through this cell's right face is replaced by
 //          the NV values there (li / ri); where fc_out is set, it is stored there
 //          (lo / ro), before the update
-template <class PH, bool REC = false, bool W3 = false, bool FC = false>
+//   FAST   tolerance-mode arithmetic (pk_fast.cuh): kernels instantiated with it
+//          are compiled in their own translation units with contraction on
+template <class PH, bool REC = false, bool W3 = false, bool FC = false, bool FAST = false>
 PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, double (&w)[PH::NV], const double* u0src,
                      const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
                      const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr,
@@ -132,7 +134,8 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
     const int PT = sm.PT;
     if (r.q) {
         double q[NV];
-        utoq<PH>(w, q, pp);
+        if constexpr (FAST) utoq_fast<PH>(w, q, pp);
+        else utoq<PH>(w, q, pp);
 #pragma unroll
         for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = q[v];
     }
@@ -163,7 +166,10 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
         }
     }
     __syncthreads();
-    if (r.flux) riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, pp);
+    if (r.flux) {
+        if constexpr (FAST) riemann_tile_fast<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, 1.0 / ch, pp);
+        else riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, pp);
+    }
     __syncthreads();
     if constexpr (FC) {
         if (r.flux && fc_in) {
@@ -225,7 +231,7 @@ PK_DEV unsigned short pack_floors(const FloorRec& r1, const FloorRec& r2)
 // (or is the whole pencil, Tile::circ).  REC: also store the stage-1 state of
 // the owned cells in ustar and their floor records in flags (the backward
 // pass's recomputation).
-template <class PH, bool REC = false, bool W3 = false>
+template <class PH, bool REC = false, bool W3 = false, bool FAST = false>
 PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, const double* uin, double* uout,
                        const PhysParams& pp, const StepParams* __restrict__ sp, double dl, int apply_fac,
                        double* smem, unsigned& status, double* ustar = nullptr, unsigned short* flags = nullptr)
@@ -265,7 +271,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     r.flux = active && (circ || (t >= 1 && t < T - 2));
     r.upd = active && (circ || (t >= 2 && t < T - 2));
     FloorRec rec1{0, 0}, rec2{0, 0};
-    rk_stage<PH, REC, W3>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status, &rec1);
+    rk_stage<PH, REC, W3, false, FAST>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status, &rec1);
     const bool own = active && (circ || (t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d));
     if (REC && own) store_cell<PH>(ustar, off, g, w);
     // stage 2 (RK2_2) on tile cells [2, T-2); u0 is again the sweep's input
@@ -273,7 +279,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     r.slope = active && (circ || (t >= 3 && t < T - 3));
     r.flux = active && (circ || (t >= 3 && t < T - 4));
     r.upd = active && (circ || (t >= 4 && t < T - 4));
-    rk_stage<PH, REC, W3>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status, &rec2);
+    rk_stage<PH, REC, W3, false, FAST>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status, &rec2);
     if (own) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);
@@ -285,7 +291,7 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
 // Fused two-stage sweep of one periodic block.
 // grid: x = ortho-1 tiles of P pencils, y = chunks of L cells, z = ortho-2.
 // -------------------------------------------------------------------------
-template <class PH, int MAXT, int MINB, bool W3 = false>
+template <class PH, int MAXT, int MINB, bool W3 = false, bool FAST = false>
 __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, const double* __restrict__ uin,
                                                            double* __restrict__ uout, PhysParams pp, double dl,
                                                            const StepParams* __restrict__ sp, int apply_fac,
@@ -293,7 +299,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_fused(Geom g, Tile tl, con
 {
     extern __shared__ double smem[];
     unsigned status = 0;
-    fused_tile<PH, false, W3>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, sp, dl, apply_fac,
+    fused_tile<PH, false, W3, FAST>(g, tl, blockIdx.x * tl.P, blockIdx.y * tl.L, blockIdx.z, uin, uout, pp, sp, dl, apply_fac,
                               smem, status);
     flush_status(status, gstatus);
 }
@@ -321,7 +327,7 @@ struct WorkItem {
     int circ;               // whole periodic pencil without halo (Tile::circ)
 };
 
-template <class PH, int MAXT, int MINB, bool W3 = false>
+template <class PH, int MAXT, int MINB, bool W3 = false, bool FAST = false>
 __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* __restrict__ blocks,
                                                              const WorkItem* __restrict__ items, int nitems, int dir,
                                                              PhysParams pp, const StepParams* __restrict__ sp,
@@ -364,7 +370,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sweep_batched(const BlockDesc* _
         tl.halo = 4;
         tl.wrap = b.wrap;
         tl.circ = w.circ;
-        fused_tile<PH, false, W3>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, sp, b.dl[dir], apply_fac, smem, status);
+        fused_tile<PH, false, W3, FAST>(g, tl, w.i1_0, w.c0, w.i2, b.in, b.out, pp, sp, b.dl[dir], apply_fac, smem,
+                                        status);
     }
     flush_status(status, gstatus);
 }

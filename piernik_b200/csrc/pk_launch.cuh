@@ -14,34 +14,59 @@ template <class PH>
 using BatchedFn = void (*)(const BlockDesc*, const WorkItem*, int, int, PhysParams, const StepParams*, int, unsigned*,
                            unsigned*);
 
-template <class PH>
+// FAST: the tolerance-mode instantiations (pk_fast.cuh arithmetic), which only
+// the pk_fast_*.cu units (compiled with contraction) may instantiate; every
+// other unit instantiates FAST = false only, so that no kernel is compiled
+// twice with different arithmetic
+template <class PH, bool FAST = false>
 FusedFn<PH> fused_variant(int v, bool w3 = false)
 {
-    if (w3) return k_sweep_fused<PH, 256, 2, true>;
+    if (w3) return k_sweep_fused<PH, 256, 2, true, FAST>;
     switch (v) {
-    case 0: return k_sweep_fused<PH, 320, 1>;
-    case 1: return k_sweep_fused<PH, 256, 1>;
-    case 2: return k_sweep_fused<PH, 256, 2>;
-    case 3: return k_sweep_fused<PH, 128, 3>;
-    case 4: return k_sweep_fused<PH, 128, 4>;
-    case 5: return k_sweep_fused<PH, 192, 2>;
-    default: return k_sweep_fused<PH, 512, 1>;
+    case 0: return k_sweep_fused<PH, 320, 1, false, FAST>;
+    case 1: return k_sweep_fused<PH, 256, 1, false, FAST>;
+    case 2: return k_sweep_fused<PH, 256, 2, false, FAST>;
+    case 3: return k_sweep_fused<PH, 128, 3, false, FAST>;
+    case 4: return k_sweep_fused<PH, 128, 4, false, FAST>;
+    case 5: return k_sweep_fused<PH, 192, 2, false, FAST>;
+    default: return k_sweep_fused<PH, 512, 1, false, FAST>;
     }
 }
 
-template <class PH>
+template <class PH, bool FAST = false>
 BatchedFn<PH> batched_variant(int v, bool w3 = false)
 {
-    if (w3) return k_sweep_batched<PH, 256, 2, true>;
+    if (w3) return k_sweep_batched<PH, 256, 2, true, FAST>;
     switch (v) {
-    case 0: return k_sweep_batched<PH, 320, 1>;
-    case 1: return k_sweep_batched<PH, 256, 1>;
-    case 2: return k_sweep_batched<PH, 256, 2>;
-    case 3: return k_sweep_batched<PH, 128, 3>;
-    case 4: return k_sweep_batched<PH, 128, 4>;
-    case 5: return k_sweep_batched<PH, 192, 2>;
-    default: return k_sweep_batched<PH, 512, 1>;
+    case 0: return k_sweep_batched<PH, 320, 1, false, FAST>;
+    case 1: return k_sweep_batched<PH, 256, 1, false, FAST>;
+    case 2: return k_sweep_batched<PH, 256, 2, false, FAST>;
+    case 3: return k_sweep_batched<PH, 128, 3, false, FAST>;
+    case 4: return k_sweep_batched<PH, 128, 4, false, FAST>;
+    case 5: return k_sweep_batched<PH, 192, 2, false, FAST>;
+    default: return k_sweep_batched<PH, 512, 1, false, FAST>;
     }
+}
+
+// dynamic shared memory limits of the fused and batched sweep kernels
+template <class PH, bool FAST>
+int set_fused_attr(pk_ctx* h)
+{
+    static bool done = false;
+    if (!done) {
+        for (int v = 0; v < NVARIANT; ++v) {
+            PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH, FAST>(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            220 * 1024));
+            PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH, FAST>(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            220 * 1024));
+        }
+        PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH, FAST>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH, FAST>(0, true),
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        done = true;
+    }
+    return PK_OK;
 }
 
 // the batched stage kernel of launch-bound variant v (SV_T / SV_B); WENO3
@@ -63,10 +88,7 @@ int set_smem_attr(pk_ctx* h)
 {
     static bool done = false;
     if (!done) {
-        for (int v = 0; v < NVARIANT; ++v) {
-            PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-            PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-        }
+        if (int rc = set_fused_attr<PH, false>(h)) return rc;
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(k_stage<PH, STAGE_MAXT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         220 * 1024));
@@ -82,10 +104,6 @@ int set_smem_attr(pk_ctx* h)
                 for (int fc = 0; fc < 2; ++fc)
                     PK_CUDA(h, cudaFuncSetAttribute(stage_batched_variant<PH>(v, w3, fc),
                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(fused_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        220 * 1024));
-        PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH>(0, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        220 * 1024));
         done = true;
     }
     return PK_OK;
@@ -125,10 +143,10 @@ inline int fused_geometry(pk_ctx* h, const Block& b, int dir, const Geom& g, Til
     return PK_OK;
 }
 
-template <class PH>
+template <class PH, bool FAST = false>
 int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out)
 {
-    if (int rc = set_smem_attr<PH>(h)) return rc;
+    if (int rc = set_fused_attr<PH, FAST>(h)) return rc;
     Geom g = make_geom(b, dir);
     Tile tl;
     dim3 grid;
@@ -137,18 +155,19 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    fused_variant<PH>(var, h->pp.weno3)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp, b.dl[dir],
-                                                                               h->d_step, apply_fac, h->d_status);
+    fused_variant<PH, FAST>(var, h->pp.weno3)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp,
+                                                                                     b.dl[dir], h->d_step, apply_fac,
+                                                                                     h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
     return PK_OK;
 }
 
-template <class PH>
+template <class PH, bool FAST = false>
 int launch_fused(pk_ctx* h, Block& b, int dir, int apply_fac)
 {
-    if (int rc = launch_fused_ptr<PH>(h, b, dir, apply_fac, b.buf[h->cur], b.buf[1 - h->cur])) return rc;
+    if (int rc = launch_fused_ptr<PH, FAST>(h, b, dir, apply_fac, b.buf[h->cur], b.buf[1 - h->cur])) return rc;
     b.guards_stale = true;
     return PK_OK;
 }
@@ -294,10 +313,10 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
     }
 }
 
-template <class PH>
+template <class PH, bool FAST = false>
 int launch_batched(pk_ctx* h, int dir, int apply_fac, unsigned* counter)
 {
-    if (int rc = set_smem_attr<PH>(h)) return rc;
+    if (int rc = set_fused_attr<PH, FAST>(h)) return rc;
     BatchList& bl = h->batch[dir];
     if (bl.n == 0) return PK_OK;
     const int var = h->pp.weno3 ? W3_VARIANT : h->batch_variant;
@@ -308,16 +327,16 @@ int launch_batched(pk_ctx* h, int dir, int apply_fac, unsigned* counter)
     int dev = 0, nsm = 0, per_sm = 0;
     PK_CUDA(h, cudaGetDevice(&dev));
     PK_CUDA(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_variant<PH>(var, h->pp.weno3), threads,
-                                                             smem));
+    PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_variant<PH, FAST>(var, h->pp.weno3),
+                                                             threads, smem));
     if (per_sm < 1) return fail(h, PK_E_ARG, "batched sweep tile does not fit on an SM");
     int grid = nsm * per_sm;
     if (grid > bl.n) grid = bl.n;
     PK_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream));
     std::pair<cudaEvent_t, cudaEvent_t> ev;
     if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    batched_variant<PH>(var, h->pp.weno3)<<<grid, threads, smem, h->stream>>>(h->d_desc[h->cur], bl.dev, bl.n, dir, h->pp,
-                                                                 h->d_step, apply_fac, counter, h->d_status);
+    batched_variant<PH, FAST>(var, h->pp.weno3)<<<grid, threads, smem, h->stream>>>(
+        h->d_desc[h->cur], bl.dev, bl.n, dir, h->pp, h->d_step, apply_fac, counter, h->d_status);
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
@@ -462,6 +481,14 @@ int launch_unsplit_apply(pk_ctx* h, Block& b, const double* S, double* T, double
     PK_CUDA(h, cudaGetLastError());
     h->launches += 1;
     return PK_OK;
+}
+
+// the tolerance-mode sweeps of PH (instantiated by the pk_fast_*.cu units only)
+template <class PH>
+const FastOps* make_fast_ops()
+{
+    static FastOps o{set_fused_attr<PH, true>, launch_fused<PH, true>, launch_batched<PH, true>};
+    return &o;
 }
 
 template <class PH>

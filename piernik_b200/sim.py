@@ -389,6 +389,12 @@ class Simulation:
     def grad_release(self) -> None:
         self._chk(self.lib.pk_grad_release(self.h), "pk_grad_release")
 
+    def set_arithmetic(self, mode: str = "bitexact") -> None:
+        """Arithmetic of the fused / batched sweeps: 'bitexact' (the
+        reference's rounding, the default) or 'fma' (contracted multiply-adds
+        and hoisted reciprocals; agrees to ~1e-15 relative per step)."""
+        self._chk(self.lib.pk_set_arithmetic(self.h, L.PK_ARITH[mode]), "pk_set_arithmetic")
+
     def set_tile(self, direction: int, pencils: int, length: int, variant: int = -1) -> None:
         """Tile of the fused sweep along ``direction`` (0..2): pencils per CTA,
         output cells per pencil, launch-bound variant (-1: default)."""

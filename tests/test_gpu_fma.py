@@ -1,0 +1,113 @@
+"""The tolerance-mode arithmetic (pk_set_arithmetic(PK_ARITH_FMA)) against the
+oracle.
+
+In this mode the fused and batched sweeps contract multiply-adds and replace
+divisions by a common denominator with one reciprocal, so results are no
+longer the reference's bit for bit; the path's specified bound applies:
+the conserved state agrees with the reference's to 1e-12 relative after one
+step and to 1e-9 after 100 steps.  Relative means, per component plane,
+max |a - b| over max |b| (a plane-wise norm: momenta and psi cross zero, so a
+cell-wise ratio has no meaning there).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import random_state, setup_for
+from piernik_b200 import problems
+from piernik_b200.sim import Simulation
+from test_gpu_configs import plane_rel
+
+pytestmark = pytest.mark.gpu
+
+REL_STEP = 1.0e-12
+REL_100 = 1.0e-9
+
+
+def rel_to_oracle(sim, ob, block=0):
+    gu, gb, gp = sim.download(block=block)
+    r = plane_rel(gu, ob.u)
+    if ob.setup.magnetic:
+        r = max(r, plane_rel(gb, ob.b), plane_rel(gp, ob.psi))
+    return r
+
+
+def pair(setup, u, b, psi, nsteps, tiles=None):
+    sim = Simulation(setup)
+    sim.set_arithmetic("fma")
+    sim.upload(u, b, psi)
+    if tiles:
+        for d, t in tiles.items():
+            sim.set_tile(d, *t)
+    sim.run(nsteps)
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    ob.run(nsteps)
+    return sim, ob
+
+
+@pytest.mark.parametrize("case", ["mhd-turb-64", "sedov-48", "ot-128", "mhd-moncen-random", "hd-weno3"])
+def test_fma_one_step(gpu_lib, oracle_lib, case):
+    if case == "mhd-turb-64":
+        s, u, b, psi = problems.mhd_turbulence(n=64, seed=5)
+    elif case == "sedov-48":
+        s, u, b, psi = problems.sedov(n=48)
+    elif case == "ot-128":
+        s, u, b, psi = problems.orszag_tang(n=128, seed=2)
+    elif case == "mhd-moncen-random":
+        s = setup_for("mhd", n=(40, 33, 27), lim="moncen")
+        u, b, psi = random_state(s, seed=6)
+    else:
+        s = setup_for("hd", n=(36, 30, 22), lim="weno3")
+        u, b, psi = random_state(s, seed=7)
+    sim, ob = pair(s, u, b, psi, 1)
+    rel = rel_to_oracle(sim, ob)
+    assert rel <= REL_STEP, f"{case}: relative difference {rel:.3e} after one step"
+    st = sim.time_state
+    assert abs(st.t - ob.state.t) <= REL_STEP * abs(ob.state.t)
+    sim.close()
+
+
+def test_fma_differs_from_bitexact(gpu_lib, oracle_lib):
+    """The mode is really switched: some value differs from the bit-exact run
+    (and switching back restores bit equality)."""
+    s, u, b, psi = problems.mhd_turbulence(n=32, seed=3)
+    sim, ob = pair(s, u, b, psi, 1)
+    gu, _, _ = sim.download()
+    assert not np.array_equal(gu.view(np.uint64), ob.u.view(np.uint64))
+    sim.set_arithmetic("bitexact")
+    sim.upload(u, b, psi)
+    sim.time_state = type(sim.time_state)()
+    sim.run(1)
+    gu, _, _ = sim.download()
+    assert np.array_equal(gu.view(np.uint64), ob.u.view(np.uint64))
+    sim.close()
+
+
+def test_fma_100_steps(gpu_lib, oracle_lib):
+    """The headline recipe at 128^3 with the benchmark's tiles: 100 steps."""
+    from test_gpu_configs import BENCH_TILES_128
+    s, u, b, psi = problems.mhd_turbulence(n=128, seed=2)
+    sim, ob = pair(s, u, b, psi, 100, BENCH_TILES_128)
+    rel = rel_to_oracle(sim, ob)
+    assert rel <= REL_100, f"relative difference {rel:.3e} after 100 steps"
+    sim.close()
+
+
+def test_fma_batched_three_fluids(gpu_lib, oracle_lib):
+    """Uneven independent blocks with ion MHD + neutral + dust through the
+    batched kernel: every block within the one-step bound of its own oracle
+    run (the blocks share one dt, as in the reference's leaf loop)."""
+    data = problems.batched_blocks(nblocks=12, seed=3, sizes=(16, 24, 32))
+    sim = Simulation(data[0][0])
+    for s, *_ in data[1:]:
+        sim.add_block(s)
+    sim.set_arithmetic("fma")
+    for i, (s, u, b, psi) in enumerate(data):
+        sim.upload(u, b, psi, block=i)
+    sim.use_graph(True)
+    sim.run(1)
+    obs = [oracle.OracleBlock(s, u, b, psi) for s, u, b, psi in data]
+    oracle.run_multi(obs, 1)
+    worst = max(rel_to_oracle(sim, ob, block=i) for i, ob in enumerate(obs))
+    assert worst <= REL_STEP, f"relative difference {worst:.3e} after one step"
+    sim.close()
