@@ -48,7 +48,8 @@ enum { PK_FLUID_ION = 0, PK_FLUID_NEU = 1, PK_FLUID_DST = 2 };
 enum { PK_LIM_VANLEER = 0, PK_LIM_MINMOD = 1, PK_LIM_MONCEN = 2, PK_LIM_SUPERBEE = 3 };
 enum { PK_BND_PER = 0, PK_BND_OUT = 1, PK_BND_REF = 2 };
 enum { PK_LAYOUT_FORTRAN = 0, PK_LAYOUT_SOA = 1 };
-enum { PK_ST_DN_NEGATIVE = 1, PK_ST_EI_NEGATIVE = 2 };
+enum { PK_ST_DN_NEGATIVE = 1, PK_ST_EI_NEGATIVE = 2,
+       PK_ST_TIMEOUT = 4 /* a kernel's bounded wait on an asynchronous copy gave up (its tile was not swept) */ };
 /* RK stage identifiers, numerically equal to the reference's istep enumerators
  * (src/base/constants.F90:230-238) */
 enum { PK_EULER = 10000, PK_RK2_1 = 10001, PK_RK2_2 = 10002 };
@@ -196,7 +197,12 @@ int pk_sync(pk_handle h);
 /* Tile shape of the fused sweep for direction d (0..2): P pencils per CTA,
  * L output cells per pencil (the CTA also computes a 4-cell halo each side),
  * and the launch-bound variant (register budget) of the kernel, -1 for the
- * default.  Used by the autotuner; 0 keeps the built-in P / L. */
+ * default.  Used by the autotuner; 0 keeps the built-in P / L.  Variant
+ * PK_VARIANT_STAGED sweeps whole pencils (n <= 256) two per CTA, staged in
+ * shared memory by TMA bulk-tensor copies (P and L are then ignored); where
+ * it cannot run (connected domains, stacked instances, WENO3, odd x extent or
+ * guard width) the whole-pencil tile of variant 2 runs instead. */
+#define PK_VARIANT_STAGED 7
 int pk_set_tile(pk_handle h, int32_t dir, int32_t pencils, int32_t length, int32_t variant);
 
 /* Arithmetic of the fused and batched sweeps (no counterpart in the

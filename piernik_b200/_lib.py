@@ -20,7 +20,8 @@ PK_FLUID = {"ion": 0, "neu": 1, "dst": 2}
 PK_LIM = {"vanleer": 0, "minmod": 1, "moncen": 2, "superbee": 3}
 PK_LAYOUT_FORTRAN, PK_LAYOUT_SOA = 0, 1
 PK_EULER, PK_RK2_1, PK_RK2_2 = 10000, 10001, 10002
-PK_ST_DN_NEGATIVE, PK_ST_EI_NEGATIVE = 1, 2
+PK_ST_DN_NEGATIVE, PK_ST_EI_NEGATIVE, PK_ST_TIMEOUT = 1, 2, 4
+PK_VARIANT_STAGED = 7
 PK_ARITH = {"bitexact": 0, "fma": 1}
 
 # every symbol include/piernik_b200.h declares

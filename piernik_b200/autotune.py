@@ -30,11 +30,17 @@ def variants() -> List[Tuple[int, int]]:
 
 def candidates(n_dir: int, n_ortho: int) -> Iterable[Tuple[int, int, int]]:
     """(P, L, variant) tiles: chunks of L owned cells with a 4-cell halo, and the
-    whole pencil without halo (L = n_dir) where it fits the CTA.  Besides the
+    whole pencil without halo (L = n_dir) where it fits the CTA, and the
+    TMA-staged whole-pencil kernel (two pencils per CTA) for pencils of up to
+    256 cells.  Besides the
     fixed lengths, the balanced ones ceil(n_dir / k) split the pencil into k
     nearly equal chunks, so that no short last chunk runs a full tile."""
     balanced = {-(-n_dir // k) for k in range(2, 13) if -(-n_dir // k) >= 16}
     for v, (maxt, _) in enumerate(variants()):
+        if v == L.PK_VARIANT_STAGED:             # whole pencils, two per CTA, staged by TMA
+            if n_dir <= 256:
+                yield 2, n_dir, v
+            continue
         lengths = sorted(set(min(Lc, n_dir) for Lc in LENGTHS) | balanced | ({n_dir} if n_dir <= maxt else set()))
         for Lc in lengths:
             T = Lc if (Lc == n_dir and n_dir <= maxt) else Lc + 8

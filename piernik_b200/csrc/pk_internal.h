@@ -18,9 +18,12 @@ namespace pk {
 // the register budget the compiler may use is 65536 / (threads * CTAs);
 // tighter budgets trade spills for resident warps.  The autotuner picks one
 // per direction.
-constexpr int NVARIANT = 7;
-constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512};
-constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1};
+// Variant VAR_STAGED is the TMA-staged whole-pencil kernel (pk_staged.cuh:
+// two pencils per 256-thread CTA, two CTAs per SM).
+constexpr int NVARIANT = 8;
+constexpr int VAR_T[NVARIANT] = {320, 256, 256, 128, 128, 192, 512, 256};
+constexpr int VAR_B[NVARIANT] = {1, 1, 2, 3, 4, 2, 1, 2};
+constexpr int VAR_STAGED = 7;
 constexpr int STAGE_MAXT = 320;       // threads per CTA of the stage kernel
 constexpr int UNSPLIT_MAXT = 256;     // threads per CTA of the unsplit flux kernel (two CTAs per SM)
 // launch-bound variants of the batched stage kernel (threads per CTA, CTAs per SM)

@@ -124,11 +124,14 @@ struct Smem {
 //          (lo / ro), before the update
 //   FAST   tolerance-mode arithmetic (pk_fast.cuh): kernels instantiated with it
 //          are compiled in their own translation units with contraction on
-template <class PH, bool REC = false, bool W3 = false, bool FC = false, bool FAST = false>
+//   U0S    u0 comes from shared memory (a staged tile): component plane j of
+//          this cell at u0sm[j * u0st] instead of u0src in global memory
+template <class PH, bool REC = false, bool W3 = false, bool FC = false, bool FAST = false, bool U0S = false>
 PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, double (&w)[PH::NV], const double* u0src,
                      const double* wsrc, long long off, const Geom& g, double dtodx, double ch,
                      const PhysParams& pp, unsigned& status, FloorRec* rec = nullptr,
-                     const double* fc_in = nullptr, double* fc_out = nullptr)
+                     const double* fc_in = nullptr, double* fc_out = nullptr, const double* u0sm = nullptr,
+                     int u0st = 0)
 {
     constexpr int NV = PH::NV;
     const int PT = sm.PT;
@@ -184,7 +187,13 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
     }
     if (r.upd) {
         double u0[NV];
-        load_cell<PH>(u0src, off, g, u0);
+        if constexpr (U0S) {
+            const int perm[3] = {g.perm[0], g.perm[1], g.perm[2]};
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u0[v] = u0sm[plane_of<PH>(v, perm) * u0st];
+        } else {
+            load_cell<PH>(u0src, off, g, u0);
+        }
 #pragma unroll
         for (int v = 0; v < NV; ++v) w[v] = u0[v] + dtodx * (sm.Q[v * PT + mp] - sm.Q[v * PT + me]);
     } else if (r.keep) {

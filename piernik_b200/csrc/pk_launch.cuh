@@ -5,6 +5,7 @@
 #include "pk_adjoint_kernels.cuh"
 #include "pk_aux.cuh"
 #include "pk_internal.h"
+#include "pk_staged.cuh"
 
 namespace pk {
 
@@ -29,7 +30,8 @@ FusedFn<PH> fused_variant(int v, bool w3 = false)
     case 3: return k_sweep_fused<PH, 128, 3, false, FAST>;
     case 4: return k_sweep_fused<PH, 128, 4, false, FAST>;
     case 5: return k_sweep_fused<PH, 192, 2, false, FAST>;
-    default: return k_sweep_fused<PH, 512, 1, false, FAST>;
+    case 6: return k_sweep_fused<PH, 512, 1, false, FAST>;
+    default: return k_sweep_fused<PH, 256, 2, false, FAST>;   // VAR_STAGED where the staged kernel cannot run
     }
 }
 
@@ -44,7 +46,8 @@ BatchedFn<PH> batched_variant(int v, bool w3 = false)
     case 3: return k_sweep_batched<PH, 128, 3, false, FAST>;
     case 4: return k_sweep_batched<PH, 128, 4, false, FAST>;
     case 5: return k_sweep_batched<PH, 192, 2, false, FAST>;
-    default: return k_sweep_batched<PH, 512, 1, false, FAST>;
+    case 6: return k_sweep_batched<PH, 512, 1, false, FAST>;
+    default: return k_sweep_batched<PH, 256, 2, false, FAST>;
     }
 }
 
@@ -64,6 +67,8 @@ int set_fused_attr(pk_ctx* h)
                                         220 * 1024));
         PK_CUDA(h, cudaFuncSetAttribute(batched_variant<PH, FAST>(0, true),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        PK_CUDA(h, cudaFuncSetAttribute(k_sweep_staged<PH, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        220 * 1024));
         done = true;
     }
     return PK_OK;
@@ -114,16 +119,35 @@ constexpr int DEF_P[3] = {2, 4, 4};
 constexpr int DEF_L[3] = {64, 64, 64};
 
 // Tile, grid and variant of the fused sweep along dir (the handle's tuned or
-// default settings; a whole periodic pencil runs without halo when it fits)
-inline int fused_geometry(pk_ctx* h, const Block& b, int dir, const Geom& g, Tile* tl, dim3* grid, int* var_out)
+// default settings; a whole periodic pencil runs without halo when it fits).
+// VAR_STAGED: the TMA-staged kernel where it can run (staged != 0 and
+// staged_ok), otherwise the whole-pencil tile of the 256 x 2 variant.
+inline int fused_geometry(pk_ctx* h, const Block& b, int dir, const Geom& g, Tile* tl, dim3* grid, int* var_out,
+                          bool staged = false)
 {
     int L = h->tileL[dir] > 0 ? h->tileL[dir] : DEF_L[dir];
     if (L > b.n[dir]) L = b.n[dir];
     int P = h->tileP[dir] > 0 ? h->tileP[dir] : DEF_P[dir];
     if (P > g.n1) P = g.n1;
-    const int var = h->pp.weno3 ? W3_VARIANT : (h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir]);
-    const int maxt = VAR_T[var];
+    int var = h->pp.weno3 ? W3_VARIANT : (h->tileV[dir] >= 0 ? h->tileV[dir] : DEF_VARIANT[dir]);
     tl->wrap = h->connected ? 0 : 1;
+    if (var == VAR_STAGED) {
+        if (staged && tl->wrap && staged_ok(b.n, b.g, b.ext, h->nplanes, dir, g.seg_len)) {
+            tl->P = 2;
+            tl->T = b.n[dir];
+            tl->L = b.n[dir];
+            tl->circ = 1;
+            tl->halo = 0;
+            tl->xfast = (dir == 0);
+            *grid = dim3((g.n1 + 1) / 2, 1, g.n2);
+            *var_out = VAR_STAGED;
+            return PK_OK;
+        }
+        var = 2;
+        L = b.n[dir] <= VAR_T[2] ? b.n[dir] : VAR_T[2] - 8;
+        P = 1;
+    }
+    const int maxt = VAR_T[var];
     tl->circ = (tl->wrap && L == b.n[dir] && b.n[dir] <= maxt) ? 1 : 0;
     if (g.seg_len && g.seg_along) {                   // stacked instances: one whole segment per tile
         L = g.seg_len;
@@ -151,13 +175,24 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     Tile tl;
     dim3 grid;
     int var;
-    if (int rc = fused_geometry(h, b, dir, g, &tl, &grid, &var)) return rc;
-    const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+    if (int rc = fused_geometry(h, b, dir, g, &tl, &grid, &var, !h->pp.weno3)) return rc;
     std::pair<cudaEvent_t, cudaEvent_t> ev;
-    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-    fused_variant<PH, FAST>(var, h->pp.weno3)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp,
-                                                                                     b.dl[dir], h->d_step, apply_fac,
-                                                                                     h->d_status);
+    if (var == VAR_STAGED) {
+        CUtensorMap tin, tout;
+        if (!encode_state_map(&tin, in, b.n, b.ext, b.plane, PH::NV, dir) ||
+            !encode_state_map(&tout, out, b.n, b.ext, b.plane, PH::NV, dir))
+            return fail(h, PK_E_CUDA, "cuTensorMapEncodeTiled failed for the staged sweep");
+        const int threads = (b.n[dir] + 31) / 32 * 32;
+        if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+        k_sweep_staged<PH, FAST><<<grid, threads, staged_smem(PH::NV, b.n[dir]), h->stream>>>(
+            tin, tout, g, h->pp, b.dl[dir], h->d_step, apply_fac, dir, h->d_status);
+    } else {
+        const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+        if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+        fused_variant<PH, FAST>(var, h->pp.weno3)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, h->pp,
+                                                                                         b.dl[dir], h->d_step,
+                                                                                         apply_fac, h->d_status);
+    }
     PK_CUDA(h, cudaGetLastError());
     if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
     h->launches += 1;
@@ -186,7 +221,8 @@ RecFn<PH> rec_variant(int v)
     case 3: return k_sweep_fused_rec<PH, 128, 3>;
     case 4: return k_sweep_fused_rec<PH, 128, 4>;
     case 5: return k_sweep_fused_rec<PH, 192, 2>;
-    default: return k_sweep_fused_rec<PH, 512, 1>;
+    case 6: return k_sweep_fused_rec<PH, 512, 1>;
+    default: return k_sweep_fused_rec<PH, 256, 2>;
     }
 }
 

@@ -84,6 +84,16 @@ def test_mhd_turbulence_256_bench_tiles(gpu_lib, oracle_lib):
     sim.close()
 
 
+def test_mhd_turbulence_256_staged_tiles(gpu_lib, oracle_lib):
+    """The headline block with the TMA-staged whole-pencil kernel along y and z."""
+    from piernik_b200._lib import PK_VARIANT_STAGED
+    setup, u, b, psi = problems.mhd_turbulence(n=256, seed=1)
+    tiles = {0: (1, 256, 2), 1: (2, 256, PK_VARIANT_STAGED), 2: (2, 256, PK_VARIANT_STAGED)}
+    sim, ob = run_both(setup, u, b, psi, 2, tiles)
+    check_same(sim, ob, "mhd 256^3 x 2, staged y/z")
+    sim.close()
+
+
 def test_mhd_turbulence_128_100_steps(gpu_lib, oracle_lib):
     """100 main-loop steps (200 time steps) of the turbulence recipe at 128^3:
     bit for bit, and so within the 1e-9 relative bound after 100 steps."""

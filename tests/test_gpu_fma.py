@@ -6,8 +6,11 @@ divisions by a common denominator with one reciprocal, so results are no
 longer the reference's bit for bit; the path's specified bound applies:
 the conserved state agrees with the reference's to 1e-12 relative after one
 step and to 1e-9 after 100 steps.  Relative means, per component plane,
-max |a - b| over max |b| (a plane-wise norm: momenta and psi cross zero, so a
-cell-wise ratio has no meaning there).
+max |a - b| over max |b| (a plane-wise norm: momenta cross zero, so a
+cell-wise ratio has no meaning there).  The GLM field psi is not a conserved
+quantity and starts at zero; it is carried in the units of B and its fluxes
+are differences of O(|B| ch) terms, so its difference is measured against
+max |B| instead of its own (still small) maximum.
 """
 import numpy as np
 import pytest
@@ -24,11 +27,22 @@ REL_STEP = 1.0e-12
 REL_100 = 1.0e-9
 
 
+class Rel(float):
+    """The largest relative difference, with the per-plane values for messages."""
+    detail = None
+
+    def __format__(self, spec):
+        return f"{float(self):{spec}} (per plane {self.detail})"
+
+
 def rel_to_oracle(sim, ob, block=0):
     gu, gb, gp = sim.download(block=block)
-    r = plane_rel(gu, ob.u)
+    per = {f"u{v}": plane_rel(gu[..., v], ob.u[..., v]) for v in range(gu.shape[-1])}
     if ob.setup.magnetic:
-        r = max(r, plane_rel(gb, ob.b), plane_rel(gp, ob.psi))
+        per.update({f"b{d}": plane_rel(gb[..., d], ob.b[..., d]) for d in range(3)})
+        per["psi/|B|"] = float(np.abs(gp - ob.psi).max() / max(np.abs(ob.b).max(), 1e-300))
+    r = Rel(max(per.values()))
+    r.detail = {k: f"{v:.1e}" for k, v in per.items()}
     return r
 
 
@@ -45,10 +59,15 @@ def pair(setup, u, b, psi, nsteps, tiles=None):
     return sim, ob
 
 
-@pytest.mark.parametrize("case", ["mhd-turb-64", "sedov-48", "ot-128", "mhd-moncen-random", "hd-weno3"])
+@pytest.mark.parametrize("case", ["mhd-turb-64", "sedov-48", "ot-128", "mhd-moncen-random", "hd-weno3",
+                                  "mhd-turb-64-staged"])
 def test_fma_one_step(gpu_lib, oracle_lib, case):
-    if case == "mhd-turb-64":
+    tiles = None
+    if case.startswith("mhd-turb-64"):
         s, u, b, psi = problems.mhd_turbulence(n=64, seed=5)
+        if case.endswith("staged"):
+            from piernik_b200._lib import PK_VARIANT_STAGED
+            tiles = {d: (2, 0, PK_VARIANT_STAGED) for d in range(3)}
     elif case == "sedov-48":
         s, u, b, psi = problems.sedov(n=48)
     elif case == "ot-128":
@@ -59,7 +78,7 @@ def test_fma_one_step(gpu_lib, oracle_lib, case):
     else:
         s = setup_for("hd", n=(36, 30, 22), lim="weno3")
         u, b, psi = random_state(s, seed=7)
-    sim, ob = pair(s, u, b, psi, 1)
+    sim, ob = pair(s, u, b, psi, 1, tiles)
     rel = rel_to_oracle(sim, ob)
     assert rel <= REL_STEP, f"{case}: relative difference {rel:.3e} after one step"
     st = sim.time_state

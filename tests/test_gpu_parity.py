@@ -9,7 +9,7 @@ import pytest
 import oracle
 from helpers import assert_bitexact, interior, random_state, setup_for
 from piernik_b200 import problems
-from piernik_b200._lib import PK_EULER, PK_RK2_1, PK_RK2_2, PK_ST_DN_NEGATIVE
+from piernik_b200._lib import PK_EULER, PK_RK2_1, PK_RK2_2, PK_ST_DN_NEGATIVE, PK_ST_TIMEOUT, PK_VARIANT_STAGED
 from piernik_b200.config import BND_OUT, BND_PER, BND_REF
 from piernik_b200.sim import Simulation
 
@@ -92,6 +92,41 @@ def test_fused_tiles_agree(gpu_lib, oracle_lib, tile):
         sim.sweep(d + 1, dt, ch)
         ob.sweep(d, dt, ch)
     compare(ob, sim, f"tile {tile}")
+
+
+@pytest.mark.parametrize("phys,n,lim", [("mhd", (50, 37, 29), "moncen"), ("hd", (48, 31, 20), "vanleer"),
+                                         ("mhd", (64, 48, 1), "moncen"), ("mhd", (36, 30, 22), "superbee"),
+                                         ("hd", (8, 8, 8), "minmod")])
+def test_staged_sweeps_bitexact(gpu_lib, oracle_lib, phys, n, lim):
+    """The TMA-staged whole-pencil kernel (PK_VARIANT_STAGED: two pencils per
+    CTA, the box loaded and stored by bulk-tensor copies) along every
+    direction, with an odd number of pencils across (the last CTA sweeps one)
+    and pencils shorter than a warp multiple, equals the oracle bit for bit."""
+    s = setup_for(phys, n=n, lim=lim)
+    ob, sim = both(s, seed=13)
+    for d in range(3):
+        sim.set_tile(d, 2, 0, PK_VARIANT_STAGED)
+    dt, ch = 0.009, 1.2
+    for d in (0, 1, 2, 2, 1, 0):
+        if n[d] > 1:
+            sim.sweep(d + 1, dt, ch)
+            ob.sweep(d, dt, ch)
+    compare(ob, sim, "staged sweeps")
+    assert not (sim.status() & PK_ST_TIMEOUT)
+
+
+def test_staged_run_with_graph(gpu_lib, oracle_lib):
+    """Whole main-loop steps with the staged kernel on y and z, replayed from a CUDA graph."""
+    setup, u, b, psi = problems.mhd_turbulence(n=32, seed=6)
+    ob = oracle.OracleBlock(setup, u, b, psi)
+    sim = Simulation(setup)
+    sim.upload(u, b, psi)
+    sim.set_tile(1, 2, 0, PK_VARIANT_STAGED)
+    sim.set_tile(2, 2, 0, PK_VARIANT_STAGED)
+    sim.use_graph(True)
+    sim.run(3)
+    ob.run(3)
+    compare(ob, sim, "staged run")
 
 
 def test_stage_path_long_pencil(gpu_lib, oracle_lib):

@@ -262,3 +262,88 @@ def test_unsplit_flux_kernel_indexing(n):
     for d in range(3):
         if n[d] > 1:
             check_unsplit(n, d)
+
+
+# ---------------------------------------------------------------------------
+# k_sweep_staged (pk_staged.cuh): TMA box per CTA and the shared-memory slots
+# ---------------------------------------------------------------------------
+def staged_ok(n, g, ext, nplanes, d):
+    """staged_ok in pk_staged.cuh"""
+    if n[d] > 256 or n[d] < 2 or nplanes > 256:
+        return False
+    if ext[0] % 2 or g[0] % 2:
+        return False
+    if d == 0 and n[0] % 2:
+        return False
+    return True
+
+
+def check_staged(n, nb, d, nv):
+    g = [nb if x > 1 else 0 for x in n]
+    ext = [n[k] + 2 * g[k] for k in range(3)]
+    if not staged_ok(n, g, ext, nv, d):
+        return False
+    o1, o2 = ORTHO1[d], ORTHO2[d]
+    nd, n1, n2 = n[d], n[o1], n[o2]
+    box = [0, 0, 0, nv]
+    box[d], box[o1], box[o2] = nd, 2, 1
+    # the tensor map: strides multiples of 16 bytes, the inner box row a multiple of 16 bytes
+    assert (ext[0] * 8) % 16 == 0 and (ext[0] * ext[1] * 8) % 16 == 0
+    assert (box[0] * 8) % 16 == 0 and all(1 <= b <= 256 for b in box)
+    threads = (nd + 31) // 32 * 32
+    assert threads <= 256
+    smem_doubles = 5 * nv * nd
+    bar_off = 5 * nv * nd * 8
+    assert bar_off % 8 == 0 and bar_off + 8 <= smem_doubles * 8 + 16
+    st_t, st_p = (1, nd) if d == 0 else (2, 1)
+    stored = set()
+    nbx = (n1 + 1) // 2
+    full = n[0] * n[1] * n[2] <= 200000          # larger blocks: the edge CTAs only
+    for bx in (range(nbx) if full else sorted({0, 1, nbx - 1})):
+        for bz in (range(n2) if full else sorted({0, n2 - 1})):
+            c = [0, 0, 0, 0]
+            c[d], c[o1], c[o2] = g[d], g[o1] + 2 * bx, g[o2] + bz
+            assert (c[0] * 8) % 16 == 0                      # TMA: x coordinate on a 16-byte boundary
+            for k in range(3):                               # the box lies inside the array (guards included)
+                assert 0 <= c[k] and c[k] + box[k] <= ext[k], (c, box, ext)
+            for p in range(2):
+                if 2 * bx + p >= n1:
+                    break
+                for t in range(threads):
+                    if t >= nd:
+                        continue
+                    for v in range(nv):
+                        idx = v * 2 * nd + t * st_t + p * st_p
+                        assert 0 <= idx < 2 * nv * nd
+                        # the box element order (x fastest, then y, z, plane) holds this cell there
+                        e = [0, 0, 0, v]
+                        e[d], e[o1], e[o2] = t, p, 0
+                        assert idx == ((e[3] * box[2] + e[2]) * box[1] + e[1]) * box[0] + e[0]
+                    for nb_ in ((t - 1) % nd, (t + 1) % nd):          # circular neighbours in the Q/L/R planes
+                        assert 0 <= nb_ < nd
+                    cell = [0, 0, 0]
+                    cell[d], cell[o1], cell[o2] = t, 2 * bx + p, bz
+                    assert tuple(cell) not in stored
+                    stored.add(tuple(cell))
+    if full:
+        assert len(stored) == n[0] * n[1] * n[2]
+    return True
+
+
+@pytest.mark.parametrize("n", [(256, 256, 256), (50, 37, 29), (48, 31, 20), (64, 48, 1), (36, 30, 22), (8, 8, 8)])
+@pytest.mark.parametrize("d", [0, 1, 2])
+@pytest.mark.parametrize("nv", [5, 9, 18])
+def test_staged_indexing(n, d, nv):
+    if n[d] == 1:
+        return
+    if n == (256, 256, 256) and nv != 9:
+        return
+    ok = check_staged(n, 4, d, nv)
+    assert ok == staged_ok(n, [4 if x > 1 else 0 for x in n], [x + 8 if x > 1 else 1 for x in n], nv, d)
+
+
+def test_staged_refused_for_odd_x():
+    """An odd x extent or guard width would put a TMA row off a 16-byte boundary."""
+    assert not staged_ok((51, 40, 40), (4, 4, 4), (59, 48, 48), 9, 1)
+    assert not staged_ok((50, 40, 40), (3, 3, 3), (56, 46, 46), 9, 2)
+    assert not staged_ok((300, 40, 40), (4, 4, 4), (308, 48, 48), 9, 0)
