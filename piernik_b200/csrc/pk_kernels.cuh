@@ -274,21 +274,29 @@ PK_DEV void fused_tile(const Geom& g, const Tile& tl, int i1_0, int c0, int i2, 
     Roles r;
     r.end = 0;
     r.keep = false;
-    // stage 1 (RK2_1) on tile cells [0, T) (circular: every cell)
-    r.q = active;
-    r.slope = active && (circ || (t >= 1 && t < T - 1));
-    r.flux = active && (circ || (t >= 1 && t < T - 2));
-    r.upd = active && (circ || (t >= 2 && t < T - 2));
-    FloorRec rec1{0, 0}, rec2{0, 0};
-    rk_stage<PH, REC, W3, false, FAST>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx1, ch, pp, status, &rec1);
     const bool own = active && (circ || (t >= 4 && t < T - 4 && s < c0 + tl.L && s < g.n_d));
-    if (REC && own) store_cell<PH>(ustar, off, g, w);
-    // stage 2 (RK2_2) on tile cells [2, T-2); u0 is again the sweep's input
-    r.q = active && (circ || (t >= 2 && t < T - 2));
-    r.slope = active && (circ || (t >= 3 && t < T - 3));
-    r.flux = active && (circ || (t >= 3 && t < T - 4));
-    r.upd = active && (circ || (t >= 4 && t < T - 4));
-    rk_stage<PH, REC, W3, false, FAST>(sm, me, mp, mn, r, w, uin, uin, off, g, dtodx2, ch, pp, status, &rec2);
+    FloorRec rec1{0, 0}, rec2{0, 0};
+    // both RK2 stages through one copy of the stage code (the solver inlined
+    // twice crowds the instruction cache)
+#pragma unroll 1
+    for (int stage = 0; stage < 2; ++stage) {
+        // stage 1 (RK2_1) on tile cells [0, T) (circular: every cell); stage 2
+        // (RK2_2) on tile cells [2, T-2), u0 again the sweep's input
+        const int a = 2 * stage;
+        r.q = active && (circ || (t >= a && t < T - a));
+        r.slope = active && (circ || (t >= a + 1 && t < T - a - 1));
+        r.flux = active && (circ || (t >= a + 1 && t < T - a - 2));
+        r.upd = active && (circ || (t >= a + 2 && t < T - a - 2));
+        FloorRec rec{0, 0};
+        rk_stage<PH, REC, W3, false, FAST>(sm, me, mp, mn, r, w, uin, uin, off, g, stage == 0 ? dtodx1 : dtodx2, ch,
+                                           pp, status, &rec);
+        if (stage == 0) {
+            rec1 = rec;
+            if (REC && own) store_cell<PH>(ustar, off, g, w);
+        } else {
+            rec2 = rec;
+        }
+    }
     if (own) {
         if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
         store_cell<PH>(uout, off, g, w);

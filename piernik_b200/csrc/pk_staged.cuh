@@ -129,6 +129,9 @@ __global__ void __launch_bounds__(256, 2) k_sweep_staged(const __grid_constant__
     const int t = tid;
     const int mp = t == 0 ? n - 1 : t - 1, mn = t == n - 1 ? 0 : t + 1;
     unsigned status = 0;
+    // one copy of the stage code for both pencils and both RK2 stages (the
+    // solver inlined four times overflows the instruction cache)
+#pragma unroll 1
     for (int p = 0; p < 2; ++p) {
         if (i1_0 + p >= g.n1) break;                     // the same for the whole CTA
         const bool active = t < n;
@@ -140,10 +143,11 @@ __global__ void __launch_bounds__(256, 2) k_sweep_staged(const __grid_constant__
         r.end = 0;
         r.keep = false;
         r.q = r.slope = r.flux = r.upd = active;
-        rk_stage<PH, false, false, false, FAST, true>(sm, t, mp, mn, r, w, nullptr, nullptr, 0, g, dtodx1, ch, pp,
-                                                      status, nullptr, nullptr, nullptr, mine, 2 * n);
-        rk_stage<PH, false, false, false, FAST, true>(sm, t, mp, mn, r, w, nullptr, nullptr, 0, g, dtodx2, ch, pp,
-                                                      status, nullptr, nullptr, nullptr, mine, 2 * n);
+#pragma unroll 1
+        for (int s = 0; s < 2; ++s)
+            rk_stage<PH, false, false, false, FAST, true>(sm, t, mp, mn, r, w, nullptr, nullptr, 0, g,
+                                                          s == 0 ? dtodx1 : dtodx2, ch, pp, status, nullptr, nullptr,
+                                                          nullptr, mine, 2 * n);
         if (active) {
             if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
 #pragma unroll
