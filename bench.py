@@ -40,20 +40,20 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 MHD cell-updates/s at 256^3 on 1 B200; adjoint-gradient cost ÷ forward step"
 UNIT = "cell-updates/s"
 NVAR = 9                         # dn, mx, my, mz, en, Bx, By, Bz, psi
-# DRAM bytes per cell of one fused-sweep launch, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) of the y sweep of a 128^3
-# block (181 MB with guards, above the 126 MB L2): 161.76 MB read + 125.97 MB
-# written over 128^3 cells.  Traffic grows with the cell count, so the
-# full-size figure is this times n^3.
-TRAFFIC_BYTES_PER_CELL = (161.756672e6 + 125.965568e6) / 128 ** 3
-# FP64 flops per cell of one fused sweep (both RK2 stages) without halo
-# recomputation, i.e. the algorithmic FP64 work: 2 x DFMA + DMUL + DADD
-# thread instructions (ncu sm__sass_thread_inst_executed_op_{dfma,dmul,dadd}
-# _pred_on.sum) of the whole-pencil x sweep of a 128^3 block over its 128^3
-# cells, in the bit-exact build
-FP64_FLOP_PER_CELL_SWEEP = 3.589298377e9 / 128 ** 3
-# the same count for the tolerance-mode (fma) sweep; None until measured
-FP64_FLOP_PER_CELL_SWEEP_FMA = None
+# DRAM bytes per cell of one sweep launch, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the TMA-staged y sweep of a
+# 128^3 block (181 MB with guards, above the 126 MB L2) in the tolerance
+# arithmetic: 163.45 MB read + 112.46 MB written over 128^3 cells.  Traffic
+# grows with the cell count, so the full-size figure is this times n^3.
+TRAFFIC_BYTES_PER_CELL = (163.454976e6 + 112.455424e6) / 128 ** 3
+# FP64 flops per cell of one sweep (both RK2 stages) without halo
+# recomputation: 2 x DFMA + DMUL + DADD thread instructions (ncu
+# sm__sass_thread_inst_executed_op_{dfma,dmul,dadd}_pred_on.sum) of the
+# TMA-staged whole-pencil x sweep of a 128^3 block over its 128^3 cells, in
+# the bit-exact arithmetic (0.8408 G DFMA, 0.9312 G DMUL, 0.9150 G DADD) and in
+# the tolerance arithmetic (0.8082 G DFMA, 0.5069 G DMUL, 0.4459 G DADD)
+FP64_FLOP_PER_CELL_SWEEP = (2 * 840755524 + 931189733 + 915036464) / 128 ** 3
+FP64_FLOP_PER_CELL_SWEEP_FMA = (2 * 808225550 + 506923602 + 445894955) / 128 ** 3
 ARITH_NOTE = {
     "fma": "fma: multiply-add contraction and hoisted reciprocals in the fused sweep; agrees with the "
            "reference's arithmetic to <= 1e-12 relative per step and <= 1e-9 after 100 steps (tests/test_gpu_fma.py)",
@@ -363,7 +363,8 @@ def our_arm(args):
         achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
         roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                     "traffic": TRAFFIC_BYTES_PER_CELL * n ** 3,
-                    "kernel": f"k_sweep_fused<MHD> ({mode} arithmetic; one sweep direction, both RK2 stages)",
+                    "kernel": f"k_sweep_staged / k_sweep_fused<MHD> as tuned ({mode} arithmetic; one sweep direction, "
+                              "both RK2 stages)",
                     "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms, "peak_source": src}
         # the bound that limits it: FP64 issue, against the device's measured DFMA rate
         roofline_fp64 = None
@@ -434,7 +435,7 @@ def our_arm(args):
 
     extras = {}
     if world == 1 and not args.no_extras:
-        for name, fn in (("c3_refined", lambda: c3_refined(args, steps=2, warmup=1, arith=head)),
+        for name, fn in (("c3_refined", lambda: c3_refined(args, steps=2, warmup=1)),
                          ("c4_ot_gradient", lambda: c4_ot_gradient(args, ndirs=4, n=512, K=100)),
                          ("c5_batched_adjoint", lambda: c5_batched_adjoint(args, K=10, ngroups=1, warmup=1,
                                                                            steps=1))):
