@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PK_ABI_VERSION 4
+#define PK_ABI_VERSION 5
 
 enum {
     PK_OK = 0,
@@ -90,6 +90,11 @@ typedef struct pk_config {
      * to injection, global.F90:561-566); 2 x the stencil range (0 for
      * injection, 1 for orders +-1..2, 2 for 3..4, 3 for 5..6) must not exceed nb */
     int32_t ord_fluid_prolong, ord_mag_prolong;
+    /* ch_grid (global.F90:111, default .true. :254): 1 = chspeed from the
+     * grid, cfl_glm * min(dl) / dt; 0 = from the gas, the maximum over leaf
+     * cells of point_chspeed (hdc.F90:118-131,197-268), reduced over ranks
+     * with MAX (one device reduction per step) */
+    int32_t ch_grid;
 } pk_config;
 
 #define PK_SOLVER_SPLIT   0
@@ -103,6 +108,11 @@ typedef struct pk_config {
 #define PK_CFL_REDO 2           /* a step whose effective CFL exceeds cfl_max, or that made
                                    unwanted negatives, is redone with dt x dt_shrink^attempt
                                    (timestep_retry.F90:repeat_fluidstep) -- the reference default */
+#define PK_CFL_FLEX 3           /* 'flex': redone as REDO, with dt x cfl_max / stepcfl (x dt_shrink
+                                   from the second attempt on) (timestep.F90:81-84,347-351) */
+#define PK_CFL_AUTO 4           /* 'auto': cfl_auto in the main time step, dt x cfl_c with
+                                   cfl_c = min(1, (cfl_c + min(1, stepcfl_old / stepcfl * dt /
+                                   dt_old)) / 2) (timestep.F90:85-86,368-405), no retry */
 
 /* Time-integration state the reference keeps in module global (global.F90). */
 typedef struct pk_time_state {
@@ -112,6 +122,8 @@ typedef struct pk_time_state {
      * tstep_attempt; timestep_pub: c_all_old, stepcfl; repeatstep: repeat_step) */
     double dt_full, c_all_old, dt_cur_shrink, stepcfl, t_saved;
     int32_t nstep_saved, tstep_attempt, repeat_step, redone;
+    /* cfl_c of cfl_auto (timestep_pub, initially one; a 0 here is read as one) */
+    double cfl_c;
 } pk_time_state;
 
 typedef struct pk_ctx* pk_handle;

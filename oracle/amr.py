@@ -86,6 +86,7 @@ class AmrOracle:
         self.state = O.OState()
         self.state.dt_old = -1.0
         self.state.dt_cur_shrink = 1.0
+        self.state.cfl_c = 1.0
 
     # ---- layout ---------------------------------------------------------
     def grid(self, L):
@@ -253,6 +254,14 @@ class AmrOracle:
             for (i, s, pen) in order:
                 acc = acc + self._tabs[(i, d)]["out_flx"][s][pen]
             self._tabs[(j, d)]["in_flx"][side][cpen] = scale * acc
+
+    def _chspeed(self, dt):
+        """update_chspeed over the leaves (hdc.F90:90-140): the grid bound's
+        minimum over blocks, or with ch_grid = .false. the maximum of the
+        blocks' leaf-cell point_chspeed maxima"""
+        lib, cfg = O.lib(), self.blocks[0].cfg
+        vals = [lib.o_chspeed(C.byref(cfg), C.byref(b.blk), dt) for b in self.blocks]
+        return min(vals) if cfg.ch_grid else max(vals)
 
     def fill_guards(self, half=False):
         """update_boundaries of u, b, psi (of uh, bh, psih when ``half``: the
@@ -476,7 +485,7 @@ class AmrOracle:
         lib = O.lib()
         fac = 1.0
         if self.mag:
-            st.chspeed = min(lib.o_chspeed(C.byref(cfg), C.byref(b.blk), dt) for b in self.blocks)
+            st.chspeed = self._chspeed(dt)
             fac = self._glm_fac(dt / 2.0)
             for b in self.blocks:
                 lib.o_glm_apply(C.byref(cfg), C.byref(b.blk), fac)
@@ -494,7 +503,7 @@ class AmrOracle:
         if self.setup0.solver == "unsplit":
             return self.fluid_update_unsplit()
         if self.mag:
-            st.chspeed = min(lib.o_chspeed(C.byref(cfg), C.byref(b.blk), dt) for b in self.blocks)
+            st.chspeed = self._chspeed(dt)
             f = 0.0
             for b in self.blocks:
                 dl = [b.setup.dl[e] for e in range(3) if b.setup.n[e] > 1]

@@ -96,6 +96,7 @@ class OState(C.Structure):
         ("tstep_attempt", C.c_int),
         ("repeat", C.c_int),
         ("redone", C.c_int),
+        ("cfl_c", C.c_double),
     ]
 
 
@@ -161,7 +162,7 @@ def make_cfg(setup) -> OCfg:
     c.cfl = setup.cfl
     c.cfl_glm = setup.cfl_glm
     c.glm_alpha = setup.glm_alpha
-    c.ch_grid = 1
+    c.ch_grid = int(getattr(setup, "ch_grid", True))
     c.integration_order = setup.integration_order
     c.dt_initial = setup.dt_initial
     c.dt_max_grow = setup.dt_max_grow
@@ -170,7 +171,8 @@ def make_cfg(setup) -> OCfg:
     c.tend = setup.tend
     for d in range(3):
         c.skip_sweep[d] = int(setup.skip_sweep[d])
-    c.cflcontrol = {"none": 0, "warn": 1, "redo": 2, "repeat": 2}[setup.cflcontrol]
+    c.cflcontrol = {"none": 0, "warn": 1, "redo": 2, "repeat": 2, "flex": 3, "flexible": 3, "auto": 4,
+                    "adaptive": 4}[setup.cflcontrol]
     c.cfl_max = setup.cfl_max
     c.dt_shrink = setup.dt_shrink
     c.max_redostep_attempts = setup.max_redostep_attempts
@@ -214,6 +216,7 @@ class OracleBlock:
         self.state.dt = 0.0
         self.state.dt_old = -1.0
         self.state.dt_cur_shrink = 1.0
+        self.state.cfl_c = 1.0
 
     def fill_guards(self):
         lib().o_fill_guards(C.byref(self.cfg), C.byref(self.blk))
@@ -257,6 +260,7 @@ def run_multi(blocks, nsteps: int, state: OState = None) -> OState:
         state = OState()
         state.dt_old = -1.0
         state.dt_cur_shrink = 1.0
+        state.cfl_c = 1.0
     arr = (C.POINTER(OBlock) * len(blocks))(*[C.pointer(b.blk) for b in blocks])
     rc = lib().o_run_multi(C.byref(blocks[0].cfg), arr, len(blocks), C.byref(state), nsteps)
     if rc:

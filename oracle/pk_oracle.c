@@ -913,11 +913,61 @@ static double o_min_dl(const o_block *blk, int *eff_dim)
     return m;
 }
 
+/* point_chspeed (hdc.F90:197-268) of interior cell (i, j, k), storage indices */
+static double o_point_chspeed(const o_cfg *cfg, const o_block *blk, int i, int j, int k)
+{
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    const int nv = o_nvar(cfg);
+    const size_t c = ((size_t)k * ext[1] + j) * ext[0] + i;
+    const double *u = blk->u + c * nv;                     /* u(:, i, j, k), fluid 0 first */
+    const double small = 1.1754943508222875e-38;           /* constants.F90:104 */
+    double ch = small;                                     /* :224 */
+    const double gam = cfg->gamma[0], gam_1 = gam - 1.0;
+    if (cfg->kind[0] == O_ION) {                           /* :231-249 */
+        const double *b = blk->b + c * 3;
+        const double pmag = 0.5 * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2]);          /* emag */
+        const double ek = (0.5 * ((u[1] * u[1] + u[2] * u[2]) + u[3] * u[3])) / u[0];   /* ekin */
+        const double pgam = ((0.5 * gam) * gam_1) * ((u[4] - ek) - pmag);
+        for (int d = 0; d < 3; ++d) {
+            if (blk->n[d] <= 1) continue;
+            const double s = pgam + pmag;
+            ch = f_max(ch, cfg->cfl_glm * (fabs(u[1 + d] / u[0]) +
+                                           sqrt((s + sqrt(s * s - (2.0 * pgam) * (b[d] * b[d]))) / u[0])));
+        }
+    } else if (cfg->kind[0] == O_NEU) {                    /* :250-259 */
+        const double ek = (0.5 * ((u[1] * u[1] + u[2] * u[2]) + u[3] * u[3])) / u[0];
+        const double pgam = ((0.5 * gam) * gam_1) * (u[4] - ek);
+        for (int d = 0; d < 3; ++d)
+            if (blk->n[d] > 1) ch = f_max(ch, cfg->cfl_glm * (fabs(u[1 + d] / u[0]) + sqrt((2.0 * pgam) / u[0])));
+    } else {                                               /* :260-266 */
+        for (int d = 0; d < 3; ++d)
+            if (blk->n[d] > 1) ch = f_max(ch, cfg->cfl_glm * fabs(u[1 + d] / u[0]));
+    }
+    return ch;
+}
+
+/* update_chspeed (hdc.F90:90-140) for one block: ch_grid, the grid bound
+   (the caller takes the minimum over blocks); otherwise the maximum of
+   point_chspeed over the block's leaf cells (the caller takes the maximum) */
 double o_chspeed(const o_cfg *cfg, const o_block *blk, double dt)
 {
-    (void)cfg;
     int eff;
     double mdl = o_min_dl(blk, &eff);
+    if (!cfg->ch_grid) {
+        int ext[3], g[3];
+        o_extents(blk, ext, g);
+        double ch = 1.1754943508222875e-38;                /* chspeed = small (:112) */
+        for (int k = g[2]; k < g[2] + blk->n[2]; ++k)
+            for (int j = g[1]; j < g[1] + blk->n[1]; ++j)
+                for (int i = g[0]; i < g[0] + blk->n[0]; ++i) {
+                    if (blk->leaf &&
+                        !blk->leaf[((size_t)(k - g[2]) * blk->n[1] + (j - g[1])) * blk->n[0] + (i - g[0])])
+                        continue;
+                    ch = f_max(ch, o_point_chspeed(cfg, blk, i, j, k));
+                }
+        return ch;
+    }
     double ch = DBL_MAX;                                   /* hdc.F90:112 */
     if (eff > 0) ch = f_min(ch, (cfg->cfl_glm * mdl) / dt);   /* :118-119 */
     return ch;
@@ -1010,6 +1060,26 @@ void o_timestep_raw(const o_cfg *cfg, const o_block *blk, double *dt_out, double
     *c_all_out = c_all;
 }
 
+/* cfl_auto (timestep.F90:368-405) in the main time_step call: dt x cfl_c
+   (the reference scales the module's dt while time_step holds it as its
+   dummy argument; the intended effect is restated) */
+static void o_cfl_auto(const o_cfg *cfg, o_state *st, double *dt, double c_all)
+{
+    double cfl_c = st->cfl_c > 0.0 ? st->cfl_c : 1.0;
+    double stepcfl_old = st->stepcfl;
+    double stepcfl = cfg->cfl;                             /* :382-387 */
+    if (st->c_all_old > 0.0) stepcfl = (c_all / st->c_all_old) * cfg->cfl;
+    else stepcfl_old = cfg->cfl;
+    if (stepcfl > 0.0 && st->dt_old > 0.0) {               /* :389-394 */
+        cfl_c = f_min(1.0, 0.5 * (cfl_c + f_min(1.0, ((stepcfl_old / stepcfl) * *dt) / st->dt_old)));
+        *dt = *dt * cfl_c;
+    } else {
+        cfl_c = 1.0;
+    }
+    st->stepcfl = stepcfl;
+    st->cfl_c = cfl_c;
+}
+
 int o_time_step(const o_cfg *cfg, const o_block *blk, o_state *st)
 {
     double dt, c_all;
@@ -1021,6 +1091,7 @@ int o_time_step(const o_cfg *cfg, const o_block *blk, o_state *st)
     } else {
         if (st->dt_old > 0.0) dt = f_min(dt, st->dt_old * cfg->dt_max_grow);
     }
+    if (cfg->cflcontrol == O_CFL_AUTO) o_cfl_auto(cfg, st, &dt, c_all);   /* cfl_manager (:210) */
     st->c_all = c_all;
     if (dt < cfg->dt_min) {                               /* :213-219 write_crashed */
         st->dt = dt;
@@ -1104,7 +1175,11 @@ static int o_check_cfl(const o_cfg *cfg, o_block *blk, o_state *st)
     st->stepcfl = o_stepcfl(cfg, st, c_all);              /* cfl_warn */
     int repeat = unwanted;
     if (st->stepcfl > o_cfl_max(cfg)) repeat = 1;
-    st->dt_cur_shrink = repeat ? o_powi(cfg->dt_shrink, st->tstep_attempt + 1) : 1.0;
+    if (!repeat) st->dt_cur_shrink = 1.0;
+    else if (cfg->cflcontrol == O_CFL_FLEX) {             /* flexible_shrink (:347-349) */
+        st->dt_cur_shrink = o_cfl_max(cfg) / st->stepcfl;
+        if (st->tstep_attempt >= 1) st->dt_cur_shrink = st->dt_cur_shrink * cfg->dt_shrink;
+    } else st->dt_cur_shrink = o_powi(cfg->dt_shrink, st->tstep_attempt + 1);   /* :351 */
     if (dt < cfg->dt_min) return 3;                       /* write_crashed */
     st->repeat = repeat;                                  /* c_all keeps the main call's value */
     return 0;
@@ -1114,7 +1189,7 @@ static int o_check_cfl(const o_cfg *cfg, o_block *blk, o_state *st)
    counts as an iteration) */
 int o_run(const o_cfg *cfg, o_block *blk, o_state *st, int nsteps)
 {
-    const int redo = cfg->cflcontrol == O_CFL_REDO;
+    const int redo = cfg->cflcontrol == O_CFL_REDO || cfg->cflcontrol == O_CFL_FLEX;   /* repetitive_steps */
     for (int s = 0; s < nsteps; ++s) {
         if (!(st->t < cfg->tend) && !st->repeat) break;
         int rc;
@@ -1223,6 +1298,7 @@ int o_time_step_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *s
     } else {
         if (st->dt_old > 0.0) dt = f_min(dt, st->dt_old * cfg->dt_max_grow);
     }
+    if (cfg->cflcontrol == O_CFL_AUTO) o_cfl_auto(cfg, st, &dt, c_all);
     st->c_all = c_all;
     if (dt < cfg->dt_min) {
         st->dt = dt;
@@ -1241,8 +1317,9 @@ int o_fluid_update_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state
     const double dt = st->dt;
     int rc;
     if (cfg->magnetic) {
-        double ch = DBL_MAX;
-        for (int i = 0; i < nb; ++i) ch = f_min(ch, o_chspeed(cfg, blks[i], dt));
+        double ch = cfg->ch_grid ? DBL_MAX : 1.1754943508222875e-38;
+        for (int i = 0; i < nb; ++i)                       /* MPI_Allreduce pMIN / pMAX (:138) */
+            ch = cfg->ch_grid ? f_min(ch, o_chspeed(cfg, blks[i], dt)) : f_max(ch, o_chspeed(cfg, blks[i], dt));
         st->chspeed = ch;
     }
     double fac = 1.0;
@@ -1279,6 +1356,7 @@ int o_run_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state *st, int
     for (int s = 0; s < nsteps; ++s) {
         if (!(st->t < cfg->tend)) break;
         int rc = o_time_step_multi(cfg, blks, nb, st);
+        st->c_all_old = st->c_all;                         /* timestep.F90:211 */
         if (rc) return rc;
         rc = o_fluid_update_multi(cfg, blks, nb, st);
         if (rc) return rc;

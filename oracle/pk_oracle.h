@@ -64,6 +64,8 @@ typedef struct o_cfg {
 #define O_CFL_NONE 0
 #define O_CFL_WARN 1
 #define O_CFL_REDO 2
+#define O_CFL_FLEX 3             /* timestep.F90:81-84: redo with flexible_shrink */
+#define O_CFL_AUTO 4             /* timestep.F90:85-86: cfl_auto */
 
 /* Fine/coarse flux hooks of one block along one direction (fluxtypes.F90
  * ext_fluxes, set by grid_container_fcflx.F90:148-259).  Pencils are
@@ -100,6 +102,7 @@ typedef struct o_state {         /* the reference's global time-step state */
     /* step retry (timestep_retry.F90, timestep.F90:247-360) */
     double dt_full, c_all_old, dt_cur_shrink, stepcfl, t_saved;
     int nstep_saved, tstep_attempt, repeat, redone;
+    double cfl_c;                /* cfl_auto's factor (timestep_pub.F90:42, initially one) */
 } o_state;
 
 int    o_nvar(const o_cfg *cfg);

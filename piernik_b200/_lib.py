@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libpiernik_b200.so")
 
 PK_OK = 0
-PK_CFL = {"none": 0, "warn": 1, "redo": 2, "repeat": 2}
+PK_CFL = {"none": 0, "warn": 1, "redo": 2, "repeat": 2, "flex": 3, "flexible": 3, "auto": 4, "adaptive": 4}
 ERRORS = {-1: "PK_E_ARG", -2: "PK_E_CUDA", -3: "PK_E_NOMEM", -4: "PK_E_UNSUPPORTED", -5: "PK_E_STATE",
           -6: "PK_E_DTMIN"}
 PK_FLUID = {"ion": 0, "neu": 1, "dst": 2}
@@ -81,6 +81,7 @@ class PkConfig(C.Structure):
         ("solver", C.c_int32),
         ("ord_fluid_prolong", C.c_int32),
         ("ord_mag_prolong", C.c_int32),
+        ("ch_grid", C.c_int32),
     ]
 
 
@@ -110,6 +111,7 @@ class PkTimeState(C.Structure):
         ("tstep_attempt", C.c_int32),
         ("repeat_step", C.c_int32),
         ("redone", C.c_int32),
+        ("cfl_c", C.c_double),
     ]
 
 

@@ -48,6 +48,7 @@ class Setup:
     dt_min: float = DBL_TINY
     dt_max: float = DBL_HUGE
     cflcontrol: str = "none"         # the reference defaults to 'redo' (:218); 'none' keeps parity runs unforked
+    ch_grid: bool = True             # :254 (psi speed from the grid; False: from the gas, hdc.F90:118-131)
     cfl_max: float = 0.9             # :233
     dt_shrink: float = 0.5           # :245
     max_redostep_attempts: int = 10  # :258
@@ -94,8 +95,9 @@ class Setup:
             raise ValueError(f"solver {self.solver!r}: this library implements split and unsplit")
         if self.interpolation not in ("linear", "weno3"):
             raise ValueError(f"interpol_str {self.interpolation!r}: this library implements linear and weno3")
-        if self.cflcontrol not in ("none", "warn", "redo", "repeat"):
-            raise ValueError(f"cflcontrol {self.cflcontrol!r}: this library implements none, warn and redo")
+        if self.cflcontrol not in ("none", "warn", "redo", "repeat", "flex", "flexible", "auto", "adaptive"):
+            raise ValueError(f"cflcontrol {self.cflcontrol!r}: this library implements none, warn, redo, flex "
+                             f"and auto")
         kinds = [k for k, _ in self.fluids]
         if kinds != sorted(kinds, key=("ion", "neu", "dst").index) or len(set(kinds)) != len(kinds):
             raise ValueError("fluids must be a subset of (ion, neu, dst) in that order")

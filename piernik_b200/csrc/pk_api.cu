@@ -913,15 +913,55 @@ int step_sweeps(pk_ctx* h, double dt, double ch, double fac)
 }
 
 // update_chspeed and the glmdamping factor for dt (hdc.F90:112-119, 310-330)
-void glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fac)
+// update_chspeed with ch_grid = .false. (hdc.F90:118-131,138): the maximum of
+// point_chspeed over the leaf cells of every block, then over ranks
+int gas_chspeed(pk_ctx* h, double* ch)
+{
+    if (h->ninst > 1) return fail(h, PK_E_UNSUPPORTED, "ch_grid = 0 with stacked instances");
+    if (int rc = exchange_prepare(h)) return rc;      // a refined domain's leaf masks
+    if (int rc = build_batch(h)) return rc;           // the block table of the current parity
+    if (!h->d_ch) PK_CUDA(h, cudaMalloc(&h->d_ch, sizeof(unsigned long long)));
+    ChArgs a;
+    a.kind = h->cfg.fluid_kind[0];
+    a.gam = h->pp.gam[0];
+    a.gam_1 = h->pp.gam_1[0];
+    a.cfl_glm = h->cfg.cfl_glm;
+    a.ib = h->ib;
+    for (int d = 0; d < 3; ++d) {
+        a.has_dir[d] = 0;
+        for (const auto& b : h->blocks) a.has_dir[d] |= b.n[d] > 1;
+    }
+    const int nb = (int)h->blocks.size();
+    long long most = 1;
+    for (auto& b : h->blocks) most = std::max(most, ((long long)b.n[0] * b.n[1] * b.n[2] + 1023) / 1024);
+    PK_CUDA(h, cudaMemsetAsync(h->d_ch, 0, sizeof(unsigned long long), h->stream));
+    k_chspeed_blocks<<<dim3((unsigned)std::min<long long>(most, 1024), nb), 256, 0, h->stream>>>(h->d_desc[h->cur], a,
+                                                                                              h->d_ch);
+    PK_CUDA(h, cudaGetLastError());
+    h->launches += 1;
+    unsigned long long bits = 0;
+    PK_CUDA(h, cudaMemcpyAsync(&bits, h->d_ch, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    double c = 1.1754943508222875e-38;                // chspeed = small (:112), then max over the cells
+    double x;
+    std::memcpy(&x, &bits, sizeof x);
+    if (bits) c = (x > c) ? x : c;
+    if (h->reduce_cb) c = h->reduce_cb(h->comm_ctx, c, 1);   // piernik_MPI_Allreduce(chspeed, pMAX)
+    *ch = c;
+    return PK_OK;
+}
+
+int glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fac)
 {
     int eff;
     const double mdl = min_dl(h, &eff);
     *ch = ch_now;
     *fac = 1.0;
-    if (!h->cfg.magnetic) return;
+    if (!h->cfg.magnetic) return PK_OK;
     double c = DBL_MAX;
-    if (eff) {
+    if (!h->cfg.ch_grid) {
+        if (int rc = gas_chspeed(h, &c)) return rc;
+    } else if (eff) {
         const double x = (h->cfg.cfl_glm * mdl) / dt;
         c = (x < c) ? x : c;
     }
@@ -932,9 +972,10 @@ void glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fa
     }
     *ch = c;
     *fac = std::exp(-f);
+    return PK_OK;
 }
 
-void glm_scalars(pk_ctx* h, double dt, double* ch, double* fac) { glm_scalars_for(h, dt, h->ts.chspeed, ch, fac); }
+int glm_scalars(pk_ctx* h, double dt, double* ch, double* fac) { return glm_scalars_for(h, dt, h->ts.chspeed, ch, fac); }
 
 // the glmdamping factor for chspeed ch over dt_eff (hdc.F90:310-332)
 double glm_fac_for(pk_ctx* h, double dt_eff, double ch)
@@ -992,11 +1033,13 @@ void pk_config_default(pk_config* c)
     c->ord_fluid_prolong = 0;             // O_INJ (:260)
     c->ord_mag_prolong = 2;               // O_I2 (:259)
     c->w_epsilon = 1.0e-10;            // :255
+    c->ch_grid = 1;                    // :254
 }
 
 int pk_create(const pk_config* cfg, pk_handle* out)
 {
-    if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_REDO || cfg->max_redostep_attempts < 0 ||
+    if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_AUTO || cfg->max_redostep_attempts < 0 ||
+                cfg->ch_grid < 0 || cfg->ch_grid > 1 ||
                 cfg->interpolation < PK_INTERP_LINEAR || cfg->interpolation > PK_INTERP_WENO3 ||
                 cfg->solver < PK_SOLVER_SPLIT || cfg->solver > PK_SOLVER_UNSPLIT))
         return PK_E_ARG;
@@ -1055,6 +1098,7 @@ int pk_create(const pk_config* cfg, pk_handle* out)
     std::memset(&h->ts, 0, sizeof(h->ts));
     h->ts.dt_old = -1.0;
     h->ts.dt_cur_shrink = 1.0;                        // global.F90:571
+    h->ts.cfl_c = 1.0;                                // timestep_pub.F90:42
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&h->d_status, sizeof(unsigned)) != cudaSuccess ||
         cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
@@ -1106,6 +1150,7 @@ int pk_destroy(pk_handle h)
     cudaFree(h->d_status);
     cudaFree(h->d_counter);
     cudaFree(h->d_red);
+    cudaFree(h->d_ch);
     cudaFree(h->d_step);
     cudaFreeHost(h->h_red);
     cudaFreeHost(h->h_step);
@@ -1310,8 +1355,10 @@ int pk_set_instances(pk_handle h, int32_t count)
         for (int d = 0; d < 3; ++d)
             if (b.n[d] > 1 && (b.bnd[d][0] != PK_BND_PER || b.bnd[d][1] != PK_BND_PER))
                 return fail(h, PK_E_UNSUPPORTED, "stacked instances are periodic in every direction");
-        if (h->cfg.integration_order != 2 || h->connected || h->cfg.cflcontrol == PK_CFL_REDO)
-            return fail(h, PK_E_UNSUPPORTED, "stacked instances need RK2, one unconnected block and no step retry");
+        if (h->cfg.integration_order != 2 || h->connected || h->cfg.cflcontrol == PK_CFL_REDO ||
+            h->cfg.cflcontrol == PK_CFL_FLEX || !h->cfg.ch_grid)
+            return fail(h, PK_E_UNSUPPORTED,
+                        "stacked instances need RK2, one unconnected block, no step retry and ch_grid = 1");
         b.seg_len = seg;
     } else {
         b.seg_len = 0;
@@ -1575,6 +1622,31 @@ int pk_timestep_raw(pk_handle h, double* dt_out, double* c_all_out)
 
 // the sanity factors of time_step (timestep.F90:200-228) on a raw dt for one
 // time state; returns PK_E_DTMIN when dt < dt_min
+// cfl_auto (timestep.F90:368-405), the cfl_manager of cflcontrol = 'auto' in
+// the main time_step call: scales dt by cfl_c, a running factor that follows
+// the change of the signal speed c_all and of dt between steps.  (In the
+// reference the routine scales the module's dt while time_step holds it as
+// its dummy argument; this is the intended effect, dt x cfl_c.)
+static void cfl_auto(const pk_config& c, pk_time_state& ts, double& dt, double c_all)
+{
+    double cfl_c = ts.cfl_c > 0.0 ? ts.cfl_c : 1.0;   // an unset state reads as the initial one
+    double stepcfl_old = ts.stepcfl;
+    double stepcfl = c.cfl;
+    if (ts.c_all_old > 0.0) stepcfl = (c_all / ts.c_all_old) * c.cfl;
+    else stepcfl_old = c.cfl;
+    if (stepcfl > 0.0 && ts.dt_old > 0.0) {
+        double r = ((stepcfl_old / stepcfl) * dt) / ts.dt_old;
+        r = (r < 1.0) ? r : 1.0;                       // min(one, ...)
+        const double x = 0.5 * (cfl_c + r);
+        cfl_c = (x < 1.0) ? x : 1.0;
+        dt = dt * cfl_c;
+    } else {
+        cfl_c = 1.0;
+    }
+    ts.stepcfl = stepcfl;
+    ts.cfl_c = cfl_c;
+}
+
 static int clamp_dt(const pk_config& c, pk_time_state& ts, double dt, double c_all)
 {
     if (ts.nstep < 1) {                               // :200-208
@@ -1587,6 +1659,7 @@ static int clamp_dt(const pk_config& c, pk_time_state& ts, double dt, double c_a
         const double x = ts.dt_old * c.dt_max_grow;
         dt = (x < dt) ? x : dt;
     }
+    if (c.cflcontrol == PK_CFL_AUTO) cfl_auto(c, ts, dt, c_all);   // cfl_manager of the main call (:210)
     ts.c_all = c_all;
     if (dt < c.dt_min) {                              // :213-219
         ts.dt = dt;
@@ -1726,7 +1799,7 @@ static int unsplit_fluid_update(pk_ctx* h)
     double ch = h->ts.chspeed, fac = 1.0;
     if (h->cfg.magnetic) {
         double fac_full;
-        glm_scalars_for(h, dt, h->ts.chspeed, &ch, &fac_full);   // update_chspeed
+        if (int rc = glm_scalars_for(h, dt, h->ts.chspeed, &ch, &fac_full)) return rc;   // update_chspeed
         fac = glm_fac_for(h, dt / 2.0, ch);                      // glmdamping(half = .true.): dt_eff = dt/2
         h->ts.chspeed = ch;
     }
@@ -1795,7 +1868,7 @@ static int inst_fluid_update(pk_ctx* h, std::vector<StepRec>* record)
     for (int i = 0; i < ni; ++i) {
         pk_time_state& ts = h->its[i];
         double ch, fac;
-        glm_scalars_for(h, ts.dt, ts.chspeed, &ch, &fac);
+        if (int rc = glm_scalars_for(h, ts.dt, ts.chspeed, &ch, &fac)) return rc;
         ts.chspeed = ch;
         r[i] = StepRec{ts.dt, ch, fac};
     }
@@ -1840,7 +1913,7 @@ int pk_fluid_update(pk_handle h)
     if (h->ninst > 1) return inst_fluid_update(h, nullptr);
     const double dt = h->ts.dt;
     double ch, fac;
-    glm_scalars(h, dt, &ch, &fac);
+    if (int rc = glm_scalars(h, dt, &ch, &fac)) return rc;
     h->ts.chspeed = ch;
     if (int rc = put_step_params(h, dt, ch, fac)) return rc;
     if (int rc = run_step_sweeps(h, dt, ch, fac)) return rc;
@@ -1925,7 +1998,14 @@ static int check_cfl(pk_ctx* h)
     h->ts.stepcfl = stepcfl_of(h, h->ts.c_all_old, c_all);
     int repeat = unwanted;
     if (h->ts.stepcfl > cfl_max_of(c)) repeat = 1;
-    h->ts.dt_cur_shrink = repeat ? powi(c.dt_shrink, h->ts.tstep_attempt + 1) : 1.0;
+    if (!repeat) {
+        h->ts.dt_cur_shrink = 1.0;
+    } else if (c.cflcontrol == PK_CFL_FLEX) {          // flexible_shrink (timestep.F90:347-349)
+        h->ts.dt_cur_shrink = cfl_max_of(c) / h->ts.stepcfl;
+        if (h->ts.tstep_attempt >= 1) h->ts.dt_cur_shrink = h->ts.dt_cur_shrink * c.dt_shrink;
+    } else {
+        h->ts.dt_cur_shrink = powi(c.dt_shrink, h->ts.tstep_attempt + 1);
+    }
     if (dt < c.dt_min) return fail(h, PK_E_DTMIN, "dt < dt_min in the check after the step");
     h->ts.repeat_step = repeat;
     return PK_OK;
@@ -1945,7 +2025,7 @@ int pk_run(pk_handle h, int32_t nsteps)
         }
         return PK_OK;
     }
-    const int redo = h->cfg.cflcontrol == PK_CFL_REDO;
+    const int redo = h->cfg.cflcontrol == PK_CFL_REDO || h->cfg.cflcontrol == PK_CFL_FLEX;   // repetitive_steps
     for (int s = 0; s < nsteps; ++s) {
         if (!(h->ts.t < h->cfg.tend) && !h->ts.repeat_step) break;
         if (!h->ts.repeat_step) {
@@ -2298,7 +2378,7 @@ int pk_grad_forward(pk_handle h, int32_t nsteps, int32_t every, const double* dt
             if (int rc = pk_time_step(h, &dt)) return rc;
         }
         double ch, fac;
-        glm_scalars(h, dt, &ch, &fac);
+        if (int rc = glm_scalars(h, dt, &ch, &fac)) return rc;
         h->ts.chspeed = ch;
         if (int rc = put_step_params(h, dt, ch, fac)) return rc;
         if (int rc = step_sweeps(h, dt, ch, fac)) return rc;

@@ -157,6 +157,75 @@ k_cfl_blocks(const BlockDesc* __restrict__ blocks, CflArgs a, unsigned long long
 }
 
 
+// point_chspeed (hdc.F90:197-268): the gas-based GLM speed of one cell, from
+// the first fluid of the set (ionized if present, else neutral, else dust),
+// in the reference's operation order
+struct ChArgs {
+    int kind;                // K_ION / K_NEU / K_DST of fluid 0
+    double gam, gam_1, cfl_glm;
+    int has_dir[3];          // dom%has_dir
+    int ib;                  // first B plane
+};
+
+PK_DEV double point_chspeed(const double* __restrict__ u, long long plane, long long off, const ChArgs& a)
+{
+    const double small = 1.1754943508222875e-38;        // constants.F90:104
+    double ch = small;
+    const double dn = u[off];
+    const double m[3] = {u[plane + off], u[2 * plane + off], u[3 * plane + off]};
+    if (a.kind == K_ION) {
+        const double bx = u[(long long)a.ib * plane + off], by = u[(long long)(a.ib + 1) * plane + off],
+                     bz = u[(long long)(a.ib + 2) * plane + off];
+        const double bv[3] = {bx, by, bz};
+        const double pmag = 0.5 * ((bx * bx + by * by) + bz * bz);                      // emag
+        const double ek = (0.5 * ((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2])) / dn;     // ekin
+        const double pgam = ((0.5 * a.gam) * a.gam_1) * ((u[4 * plane + off] - ek) - pmag);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (!a.has_dir[d]) continue;
+            const double s = pgam + pmag;
+            const double c = a.cfl_glm * (fabs(m[d] / dn) + sqrt((s + sqrt(s * s - (2.0 * pgam) * (bv[d] * bv[d]))) / dn));
+            ch = f_max(ch, c);
+        }
+    } else if (a.kind == K_NEU) {
+        const double ek = (0.5 * ((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2])) / dn;
+        const double pgam = ((0.5 * a.gam) * a.gam_1) * (u[4 * plane + off] - ek);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (a.has_dir[d]) ch = f_max(ch, a.cfl_glm * (fabs(m[d] / dn) + sqrt((2.0 * pgam) / dn)));
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (a.has_dir[d]) ch = f_max(ch, a.cfl_glm * fabs(m[d] / dn));
+    }
+    return ch;
+}
+
+// update_chspeed with ch_grid = .false. (hdc.F90:118-131): the maximum of
+// point_chspeed over the interior leaf cells of every block (blockIdx.y picks
+// the block), reduced as bit patterns of positive doubles into *out
+static __global__ void __launch_bounds__(256, 3)
+k_chspeed_blocks(const BlockDesc* __restrict__ blocks, ChArgs a, unsigned long long* __restrict__ out)
+{
+    const BlockDesc d = blocks[blockIdx.y];
+    const long long ncell = (long long)d.n[0] * d.n[1] * d.n[2];
+    unsigned long long best = 0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        if (d.leaf && !d.leaf[c]) continue;
+        const long long i = c % d.n[0], r = c / d.n[0];
+        const long long j = r % d.n[1], k = r / d.n[1];
+        const long long off = ((k + d.g[2]) * d.ext[1] + (j + d.g[1])) * d.ext[0] + (i + d.g[0]);
+        const unsigned long long x = (unsigned long long)__double_as_longlong(point_chspeed(d.in, d.plane, off, a));
+        best = x > best ? x : best;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, best, o);
+        best = y > best ? y : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best) atomicMax(out, best);
+}
+
 // psi *= fac over the whole plane, guard cells included (hdc.F90:338)
 static __global__ void k_scale(double* __restrict__ p, long long n, double fac)
 {

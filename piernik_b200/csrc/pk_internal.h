@@ -117,6 +117,7 @@ struct pk_ctx {
     unsigned* d_status = nullptr;
     unsigned* d_counter = nullptr;      // work-list counters of the batched sweep (one per launch slot)
     unsigned long long* d_red = nullptr;
+    unsigned long long* d_ch = nullptr;     // the gas-based chspeed maximum (ch_grid = 0)
     unsigned long long* h_red = nullptr;
     int red_cap = 0;
     pk::StepParams* d_step = nullptr;   // device copy of the step scalars (one per instance)

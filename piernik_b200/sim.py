@@ -73,6 +73,7 @@ def make_config(setup: Setup) -> L.PkConfig:
     c.solver = {"split": 0, "unsplit": 1}[setup.solver]
     c.ord_fluid_prolong = setup.ord_fluid_prolong
     c.ord_mag_prolong = setup.ord_mag_prolong
+    c.ch_grid = int(setup.ch_grid)
     return c
 
 

@@ -326,3 +326,54 @@ def test_weno3_runs_bitexact(gpu_lib, oracle_lib, recipe):
     st = sim.time_state
     assert st.t == ob.state.t and st.dt == ob.state.dt
     compare(ob, sim, f"weno3 {recipe}")
+
+
+@pytest.mark.parametrize("mode", ["flex", "auto"])
+def test_cfl_flex_auto_match_oracle(gpu_lib, oracle_lib, mode):
+    """cflcontrol = flex (retries with dt_cur_shrink = cfl_max / stepcfl) and
+    auto (cfl_auto's dt x cfl_c in every main time step): the whole history
+    equals the oracle's."""
+    s, u, b, psi = problems.sedov(n=24)
+    s = s.replace(cfl=0.9 if mode == "flex" else 0.7, cflcontrol=mode)
+    ob = oracle.OracleBlock(s, u, b, psi)
+    sim = Simulation(s)
+    sim.upload(u, b, psi)
+    assert ob.run(30) == 0
+    sim.run(30)
+    st, ost = sim.time_state, ob.state
+    for f in ("t", "dt", "dt_old", "c_all", "dt_full", "c_all_old", "dt_cur_shrink", "stepcfl", "cfl_c"):
+        assert getattr(st, f) == getattr(ost, f), f
+    assert (st.nstep, st.redone) == (ost.nstep, ost.redone)
+    if mode == "flex":
+        assert st.redone > 0
+    else:
+        assert st.cfl_c < 1.0 or st.nstep == 30
+    compare(ob, sim, f"cflcontrol = {mode}")
+    sim.close()
+
+
+@pytest.mark.parametrize("case", ["split-mhd", "split-2d", "unsplit-mhd", "batched-3fluid"])
+def test_gas_chspeed_matches_oracle(gpu_lib, oracle_lib, case):
+    """ch_grid = .false.: chspeed is the maximum of point_chspeed over the
+    leaf cells (a device reduction), and with it the GLM fluxes and damping."""
+    if case == "batched-3fluid":
+        data = problems.batched_blocks(nblocks=5, seed=7, sizes=(8, 16, 24), n0=16)
+        data = [(st.replace(ch_grid=False), u, b, psi) for st, u, b, psi in data]
+        _multi(data, 3)
+        return
+    if case == "split-2d":
+        s, u, b, psi = problems.orszag_tang(n=32, seed=1)
+    else:
+        s, u, b, psi = problems.mhd_turbulence(n=20, seed=3)
+    s = s.replace(ch_grid=False)
+    if case.startswith("unsplit"):
+        s = s.replace(solver="unsplit", cfl=0.3, cfl_glm=0.3)
+    ob, sim = oracle.OracleBlock(s, u, b, psi), Simulation(s)
+    sim.upload(u, b, psi)
+    ob.run(4)
+    sim.run(4)
+    st = sim.time_state
+    assert st.chspeed == ob.state.chspeed and st.t == ob.state.t
+    assert st.chspeed != (s.cfl_glm * min(s.dl[d] for d in range(3) if s.n[d] > 1)) / st.dt
+    compare(ob, sim, f"ch_grid = .false. ({case})")
+    sim.close()

@@ -223,6 +223,93 @@ def test_cfl_redo_repeats_violating_steps(oracle_lib):
     assert st.dt_cur_shrink == 1.0
 
 
+def test_cfl_flex_repeats_with_flexible_shrink(oracle_lib):
+    """cflcontrol = flex: the same retries as redo, with dt_cur_shrink =
+    cfl_max / stepcfl on the first retry (x dt_shrink from the second on,
+    timestep.F90:81-84,347-351) instead of dt_shrink**attempt; a retried step
+    then lands at stepcfl = cfl_max, so it is not retried again."""
+    from piernik_b200 import problems
+    s, u, b, psi = problems.sedov(n=24)
+    runs = {}
+    for mode in ("redo", "flex"):
+        ob = oracle.OracleBlock(s.replace(cfl=0.9, cflcontrol=mode), u, b, psi)
+        assert ob.run(30) == 0
+        runs[mode] = ob
+    fl, rd = runs["flex"].state, runs["redo"].state
+    assert fl.redone > 0 and rd.redone > 0
+    assert fl.nstep == 30 - fl.redone
+    assert not np.array_equal(runs["flex"].u.view(np.uint64), runs["redo"].u.view(np.uint64))
+    assert fl.stepcfl <= oracle.lib().o_cfl_max(C.byref(runs["flex"].cfg))
+
+
+def test_cfl_auto_follows_its_recurrence(oracle_lib):
+    """cflcontrol = auto: every main time step is the CFL step (with the
+    dt_old x dt_max_grow clamp) times cfl_c, where cfl_c = min(1, (cfl_c +
+    min(1, stepcfl_old / stepcfl * dt / dt_old)) / 2) and stepcfl =
+    c_all / c_all_old * cfl (timestep.F90:368-405); restated here step by step
+    from the oracle's own CFL reduction on the state before each step."""
+    from piernik_b200 import problems
+    s, u, b, psi = problems.sedov(n=16)
+    s = s.replace(cfl=0.7, cflcontrol="auto")
+    ob = oracle.OracleBlock(s, u, b, psi)
+    cfl_c, stepcfl, c_old, dt_prev = 1.0, 0.0, 0.0, 0.0
+    shrunk = 0
+    for k in range(14):
+        dt_raw, c_all = ob.timestep_raw()
+        dt = dt_raw
+        if k >= 1 and dt_prev > 0.0:
+            dt = min(dt, dt_prev * s.dt_max_grow)
+        st_old = stepcfl
+        stepcfl = s.cfl
+        if c_old > 0.0:
+            stepcfl = (c_all / c_old) * s.cfl
+        else:
+            st_old = s.cfl
+        if stepcfl > 0.0 and dt_prev > 0.0:
+            r = min(1.0, ((st_old / stepcfl) * dt) / dt_prev)
+            cfl_c = min(1.0, 0.5 * (cfl_c + r))
+            dt = dt * cfl_c
+        else:
+            cfl_c = 1.0
+        assert ob.run(1) == 0
+        assert ob.state.dt == dt and ob.state.cfl_c == cfl_c and ob.state.stepcfl == stepcfl, k
+        shrunk += cfl_c < 1.0
+        c_old, dt_prev = c_all, dt
+    assert shrunk > 0
+
+
+@pytest.mark.parametrize("phys", ["mhd", "hd-neu"])
+def test_gas_chspeed_restated(oracle_lib, phys):
+    """ch_grid = .false.: chspeed is the maximum over the block's cells of
+    point_chspeed (hdc.F90:197-268), restated here with numpy in the same
+    operation order, bit for bit."""
+    from helpers import random_state, setup_for
+    s = setup_for("mhd" if phys == "mhd" else "hd", n=(12, 10, 8), lim="moncen").replace(ch_grid=False)
+    u, b, psi = random_state(s, seed=3)
+    ob = oracle.OracleBlock(s, u, b, psi)
+    got = oracle.lib().o_chspeed(C.byref(ob.cfg), C.byref(ob.blk), 0.01)
+    g, n = s.guards, s.n
+    cut = lambda a: a[g[2]:g[2] + n[2], g[1]:g[1] + n[1], g[0]:g[0] + n[0]]
+    U = cut(u)
+    dn, m, E = U[..., 0], [U[..., 1], U[..., 2], U[..., 3]], U[..., 4]
+    gam = s.fluids[0][1]
+    ek = (0.5 * ((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2])) / dn
+    best = np.float64(1.1754943508222875e-38)
+    if s.magnetic:
+        B = cut(b)
+        pmag = 0.5 * ((B[..., 0] * B[..., 0] + B[..., 1] * B[..., 1]) + B[..., 2] * B[..., 2])
+        pgam = ((0.5 * gam) * (gam - 1.0)) * ((E - ek) - pmag)
+        for d in range(3):
+            sp = pgam + pmag
+            c = s.cfl_glm * (np.abs(m[d] / dn) + np.sqrt((sp + np.sqrt(sp * sp - (2.0 * pgam) * (B[..., d] * B[..., d]))) / dn))
+            best = max(best, c.max())
+    else:
+        pgam = ((0.5 * gam) * (gam - 1.0)) * (E - ek)
+        for d in range(3):
+            best = max(best, (s.cfl_glm * (np.abs(m[d] / dn) + np.sqrt((2.0 * pgam) / dn))).max())
+    assert got == best
+
+
 def test_sedov_shock_follows_similarity_solution(oracle_lib):
     """Sedov-Taylor: the blast front (peak of the spherically averaged
     density) sits at R = xi0 (E t^2 / rho)^(1/5), xi0 = 1.1517 for gamma =
