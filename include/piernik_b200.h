@@ -394,6 +394,19 @@ int pk_halo_sizes(pk_handle h, int32_t peer, int64_t* send_doubles, int64_t* rec
 int pk_halo_pack(pk_handle h, int32_t peer, double* sendbuf_dev);
 int pk_halo_unpack(pk_handle h, int32_t peer, const double* recvbuf_dev);
 int pk_set_comm(pk_handle h, pk_halo_fn halo, pk_reduce_fn reduce, void* ctx);
+/* The same per sweep direction (no counterpart in the reference, which
+ * exchanges every guard cell before every sweep): dir 0..2 restricts a
+ * peer's traffic to the face boxes of the guard region along dir -- all a
+ * fused sweep along dir reads -- and dir = -1 is the whole halo as above.
+ * For z slabs of a periodic domain, x and y sweeps then move nothing between
+ * ranks.  Unlike pk_halo_pack / pk_halo_unpack these two do not wait: the
+ * copies are ordered on the handle's stream (pk_stream), so a transport that
+ * enqueues its sends after the pack and makes that stream wait for its
+ * receives (NCCL on the same stream) needs no host synchronisation; the
+ * buffers must stay valid until the stream has passed them. */
+int pk_halo_sizes_dir(pk_handle h, int32_t peer, int32_t dir, int64_t* send_doubles, int64_t* recv_doubles);
+int pk_halo_pack_dir(pk_handle h, int32_t peer, int32_t dir, double* sendbuf_dev);
+int pk_halo_unpack_dir(pk_handle h, int32_t peer, int32_t dir, const double* recvbuf_dev);
 
 /* ---- Differentiable path (one periodic block, one fluid, RK2) ----
  * Not in the reference, which has no derivatives: the adjoint (reverse

@@ -35,6 +35,7 @@ EXPORTS = (
     "pk_grad_forward", "pk_grad_backward", "pk_grad_release",
     "pk_timestep_raw_noalloc", "pk_set_adjoint_tile", "pk_set_domain", "pk_block_place",
     "pk_block_remote", "pk_halo_peers", "pk_halo_sizes", "pk_halo_pack", "pk_halo_unpack", "pk_set_comm",
+    "pk_halo_sizes_dir", "pk_halo_pack_dir", "pk_halo_unpack_dir",
     "pk_set_instances", "pk_get_instance_state", "pk_set_instance_state", "pk_block_place_level",
     "pk_set_stage_variant", "pk_fp64_peak", "pk_restrict",
     "pk_prolong_block",
@@ -189,6 +190,9 @@ def load(path: str = LIBPATH):
     L.pk_halo_peers.argtypes = [H, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]
     L.pk_halo_sizes.argtypes = [H, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.pk_halo_pack.argtypes = [H, C.c_int32, C.c_void_p]
+    L.pk_halo_sizes_dir.argtypes = [H, C.c_int32, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.pk_halo_pack_dir.argtypes = [H, C.c_int32, C.c_int32, C.c_void_p]
+    L.pk_halo_unpack_dir.argtypes = [H, C.c_int32, C.c_int32, C.c_void_p]
     L.pk_halo_unpack.argtypes = [H, C.c_int32, C.c_void_p]
     L.pk_set_comm.argtypes = [H, C.c_void_p, C.c_void_p, C.c_void_p]
     L.pk_timestep_raw_noalloc.argtypes = [C.POINTER(PkConfig), C.c_int32, C.POINTER(C.c_int32),

@@ -189,11 +189,29 @@ void free_segs(pk_ctx* h)
 {
     cudaFree(h->xlocal.dev);
     h->xlocal = XSegList();
+    for (int d = 0; d < 3; ++d) {
+        cudaFree(h->xlocal_dir[d].dev);
+        h->xlocal_dir[d] = XSegList();
+    }
+    h->x_dir = false;
     for (auto& p : h->xpeers) {
         cudaFree(p.send.dev);
         cudaFree(p.recv.dev);
+        for (int d = 0; d < 3; ++d) {
+            cudaFree(p.send_dir[d].dev);
+            cudaFree(p.recv_dir[d].dev);
+        }
     }
     h->xpeers.clear();
+}
+
+// the segments of face boxes along dir (seg_face_dir of their destination block)
+static std::vector<XSeg> face_segs(const std::vector<XBlock>& xb, const std::vector<XSeg>& segs, int dir)
+{
+    std::vector<XSeg> out;
+    for (const XSeg& s : segs)
+        if (seg_face_dir(xb[s.dst], s) == dir) out.push_back(s);
+    return out;
 }
 
 void free_levels(pk_ctx* h)
@@ -526,13 +544,21 @@ int exchange_prepare(pk_ctx* h)
         PK_CUDA(h, cudaStreamSynchronize(h->stream));
         free_segs(h);
         if (int rc = upload_segs(h, local, &h->xlocal)) return rc;
+        for (int d = 0; d < 3; ++d)
+            if (int rc = upload_segs(h, face_segs(xb, local, d), &h->xlocal_dir[d])) return rc;
         for (const XPeer& p : peers) {
             XPeerDev d;
             d.rank = p.rank;
             h->xpeers.push_back(d);
-            if (int rc = upload_segs(h, p.send, &h->xpeers.back().send)) return rc;
-            if (int rc = upload_segs(h, p.recv, &h->xpeers.back().recv)) return rc;
+            XPeerDev& q = h->xpeers.back();
+            if (int rc = upload_segs(h, p.send, &q.send)) return rc;
+            if (int rc = upload_segs(h, p.recv, &q.recv)) return rc;
+            for (int k = 0; k < 3; ++k) {   // canonical order kept: both sides filter their lists alike
+                if (int rc = upload_segs(h, face_segs(xb, p.send, k), &q.send_dir[k])) return rc;
+                if (int rc = upload_segs(h, face_segs(xb, p.recv, k), &q.recv_dir[k])) return rc;
+            }
         }
+        h->x_dir = true;
         h->x_dirty = false;
     }
     if (h->x_ptrs_dirty) {
@@ -566,7 +592,9 @@ int exchange_guards(pk_ctx* h, int dir = -1, int need = -1)
     if (!h->connected) return PK_OK;
     if (int rc = exchange_prepare(h)) return rc;
     if (need >= 0 && !(h->max_level > 0 && h->part[need].ok)) need = -1;
-    const XSegList& xs = need >= 0 ? h->part[need].segs : h->xlocal;
+    // before a fused sweep along dir only the face boxes along dir are read
+    const XSegList& xs = need >= 0 ? h->part[need].segs
+                                   : ((dir >= 0 && h->x_dir && h->max_level == 0) ? h->xlocal_dir[dir] : h->xlocal);
     if (xs.total > 0) {
         const int nblk = (int)(xs.n < grid_cap() ? xs.n : grid_cap());   // CTAs take whole segments
         k_exchange<<<nblk, 256, 0, h->stream>>>(xs.dev, xs.n, xs.total, h->d_xptr[h->cur], h->nplanes);
@@ -1473,44 +1501,74 @@ static XPeerDev* find_peer(pk_ctx* h, int peer)
     return nullptr;
 }
 
-int pk_halo_sizes(pk_handle h, int32_t peer, int64_t* send_doubles, int64_t* recv_doubles)
+// the segment lists of one peer for the exchange before a sweep along dir (-1: every guard cell)
+static int peer_lists(pk_ctx* h, int peer, int dir, const XSegList** send, const XSegList** recv)
 {
-    if (!h) return PK_E_ARG;
+    if (dir < -1 || dir > 2) return fail(h, PK_E_ARG, "dir must be -1..2");
     if (int rc = exchange_prepare(h)) return rc;
     XPeerDev* p = find_peer(h, peer);
     if (!p) return fail(h, PK_E_ARG, "no halo traffic with that rank");
-    if (send_doubles) *send_doubles = p->send.total * h->nplanes;
-    if (recv_doubles) *recv_doubles = p->recv.total * h->nplanes;
+    if (dir >= 0 && !h->x_dir) return fail(h, PK_E_UNSUPPORTED, "per-direction halos need a single-level domain");
+    *send = dir < 0 ? &p->send : &p->send_dir[dir];
+    *recv = dir < 0 ? &p->recv : &p->recv_dir[dir];
     return PK_OK;
 }
 
-static int halo_copy(pk_ctx* h, int peer, double* buf, int to_buf)
+int pk_halo_sizes_dir(pk_handle h, int32_t peer, int32_t dir, int64_t* send_doubles, int64_t* recv_doubles)
 {
-    if (int rc = exchange_prepare(h)) return rc;
-    XPeerDev* p = find_peer(h, peer);
-    if (!p) return fail(h, PK_E_ARG, "no halo traffic with that rank");
-    if (!buf) return fail(h, PK_E_ARG, "null buffer");
-    const XSegList& l = to_buf ? p->send : p->recv;
+    if (!h) return PK_E_ARG;
+    const XSegList *s, *r;
+    if (int rc = peer_lists(h, peer, dir, &s, &r)) return rc;
+    if (send_doubles) *send_doubles = s->total * h->nplanes;
+    if (recv_doubles) *recv_doubles = r->total * h->nplanes;
+    return PK_OK;
+}
+
+int pk_halo_sizes(pk_handle h, int32_t peer, int64_t* send_doubles, int64_t* recv_doubles)
+{
+    return pk_halo_sizes_dir(h, peer, -1, send_doubles, recv_doubles);
+}
+
+// sync: wait for the copy (the whole-halo calls); the per-direction calls
+// stay in the handle's stream order for a transport that follows it
+static int halo_copy(pk_ctx* h, int peer, int dir, double* buf, int to_buf, bool sync)
+{
+    const XSegList *s, *r;
+    if (int rc = peer_lists(h, peer, dir, &s, &r)) return rc;
+    if (!buf && (to_buf ? s : r)->total > 0) return fail(h, PK_E_ARG, "null buffer");
+    const XSegList& l = to_buf ? *s : *r;
     if (l.total > 0) {
         k_halo_copy<<<grid1d(l.total, 256), 256, 0, h->stream>>>(l.dev, l.n, l.total, h->d_xptr[h->cur], h->nplanes, buf,
                                                                 to_buf);
         PK_CUDA(h, cudaGetLastError());
         h->launches += 1;
     }
-    PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (sync) PK_CUDA(h, cudaStreamSynchronize(h->stream));
     return PK_OK;
 }
 
 int pk_halo_pack(pk_handle h, int32_t peer, double* sendbuf_dev)
 {
     if (!h) return PK_E_ARG;
-    return halo_copy(h, peer, sendbuf_dev, 1);
+    return halo_copy(h, peer, -1, sendbuf_dev, 1, true);
 }
 
 int pk_halo_unpack(pk_handle h, int32_t peer, const double* recvbuf_dev)
 {
     if (!h) return PK_E_ARG;
-    return halo_copy(h, peer, const_cast<double*>(recvbuf_dev), 0);
+    return halo_copy(h, peer, -1, const_cast<double*>(recvbuf_dev), 0, true);
+}
+
+int pk_halo_pack_dir(pk_handle h, int32_t peer, int32_t dir, double* sendbuf_dev)
+{
+    if (!h) return PK_E_ARG;
+    return halo_copy(h, peer, dir, sendbuf_dev, 1, false);
+}
+
+int pk_halo_unpack_dir(pk_handle h, int32_t peer, int32_t dir, const double* recvbuf_dev)
+{
+    if (!h) return PK_E_ARG;
+    return halo_copy(h, peer, dir, const_cast<double*>(recvbuf_dev), 0, false);
 }
 
 int pk_set_comm(pk_handle h, pk_halo_fn halo, pk_reduce_fn reduce, void* ctx)

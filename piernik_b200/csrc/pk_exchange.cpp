@@ -123,6 +123,19 @@ void sort_canonical(const std::vector<XBlock>& blocks, std::vector<XSeg>& segs)
     std::stable_sort(segs.begin(), segs.end(), [&](const XSeg& a, const XSeg& b) { return key(a) < key(b); });
 }
 
+int seg_face_dir(const XBlock& dst, const XSeg& s)
+{
+    int dir = -1, out = 0;
+    for (int d = 0; d < 3; ++d) {
+        const bool inside = s.lo[d] >= dst.g[d] && s.hi[d] <= dst.g[d] + dst.n[d];
+        if (!inside) {
+            dir = d;
+            ++out;
+        }
+    }
+    return out == 1 ? dir : -1;
+}
+
 void split_by_owner(const std::vector<XBlock>& blocks, const std::vector<int>& owner, int nlocal,
                     const std::vector<XSeg>& segs, std::vector<XSeg>& local, std::vector<XPeer>& peers)
 {

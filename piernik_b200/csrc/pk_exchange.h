@@ -41,6 +41,15 @@ bool build_exchange(const std::vector<XBlock>& blocks, const long long dom[3], c
 // block numbers, which differ between ranks.
 void sort_canonical(const std::vector<XBlock>& blocks, std::vector<XSeg>& segs);
 
+// The direction along which segment s's box is a face box of block dst's
+// guard region -- outside dst's interior along exactly that direction, inside
+// along the other two -- or -1 for an edge or corner box.  A fused sweep along
+// d reads guard cells of face boxes along d only, so the exchange before it
+// needs those alone.  (A segment is a source interior's image clipped to dst's
+// guard-inclusive box, so along each direction it lies wholly inside the
+// interior or wholly in one guard layer.)
+int seg_face_dir(const XBlock& dst, const XSeg& s);
+
 // Split the segments of blocks[0..nlocal) (this rank's) and of the remote
 // blocks (owner[i] >= 0 for i >= nlocal) into the local copies, and per peer
 // rank the copies received (destination local) and sent (source local).

@@ -81,6 +81,7 @@ struct XSegList {
 struct XPeerDev {
     int rank = -1;
     XSegList send, recv;
+    XSegList send_dir[3], recv_dir[3];   // the face boxes along one direction (seg_face_dir)
 };
 
 // a block held by another rank (connected domains spanning ranks)
@@ -154,6 +155,8 @@ struct pk_ctx {
     bool x_dirty = true;                // the exchange plan must be rebuilt
     bool x_ptrs_dirty = true;           // block buffers changed: rebuild the pointer tables
     pk::XSegList xlocal;                // copies between this rank's blocks
+    pk::XSegList xlocal_dir[3];         // the same restricted to face boxes along one direction
+    bool x_dir = false;                 // the per-direction lists are built (single-level domains)
     std::vector<pk::XPeerDev> xpeers;   // copies to and from each other rank
     std::vector<pk::RemoteBlock> remote;
     pk::XPtr* d_xptr[2] = {nullptr, nullptr};   // block states of parity 0 / 1

@@ -15,10 +15,15 @@ buffers between ranks through a transport:
   (tests): buffers handed over in host memory order, a barrier between the
   pack and the unpack.  No kernel ever waits for another rank's kernel.
 
-Every exchange is host-driven and synchronous, so all ranks take the same
-steps in the same order: the library calls the halo callback after each
-local guard exchange (once before every fused sweep) and the reduce callback
-twice per time step (dt minimum, c_all maximum).
+Every exchange is host-driven, so all ranks take the same steps in the same
+order: the library calls the halo callback after each local guard exchange
+(once before every fused sweep, with the sweep's direction) and the reduce
+callback twice per time step (dt minimum, c_all maximum).  Before a sweep
+only the face boxes along its direction are moved (``pk_halo_*_dir``): for z
+slabs the x and y sweeps move nothing and post no message, and the z sweeps
+move the z faces only.  The pack and unpack kernels and the NCCL transfers
+are ordered on the library's stream (NCCL waits on it for the pack, the
+stream waits on NCCL for the unpack), so no exchange stops the host.
 """
 from __future__ import annotations
 
@@ -76,17 +81,29 @@ class TorchTransport:
         self.device = device
 
     def exchange(self, rank: int, peers: Sequence[int], send: Dict[int, torch.Tensor],
-                 recv: Dict[int, torch.Tensor]) -> None:
+                 recv: Dict[int, torch.Tensor], stream: Optional[int] = None) -> None:
+        """Post every peer's send and receive (empty buffers are skipped; both
+        sides of a pair agree on which are empty) and wait for them.  With
+        ``stream`` (a cudaStream_t), NCCL is ordered after the work queued
+        there and that stream waits for the transfers; the host does not."""
         import torch.distributed as dist
         ops = []
         for p in peers:
-            ops.append(dist.P2POp(dist.isend, send[p], p))
-            ops.append(dist.P2POp(dist.irecv, recv[p], p))
-        if ops:
+            if send[p].numel():
+                ops.append(dist.P2POp(dist.isend, send[p], p))
+            if recv[p].numel():
+                ops.append(dist.P2POp(dist.irecv, recv[p], p))
+        if not ops:
+            return
+        if stream is not None and self.device.type == "cuda":
+            with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.device)):
+                for r in dist.batch_isend_irecv(ops):
+                    r.wait()
+        else:
             for r in dist.batch_isend_irecv(ops):
                 r.wait()
-        if self.device.type == "cuda":
-            torch.cuda.synchronize(self.device)
+            if self.device.type == "cuda":
+                torch.cuda.synchronize(self.device)
 
     def reduce(self, rank: int, x: float, op: int) -> float:
         import torch.distributed as dist
@@ -105,7 +122,8 @@ class ThreadTransport:
         self.box: Dict[Tuple[int, int], torch.Tensor] = {}
         self.vals: Dict[int, float] = {}
 
-    def exchange(self, rank, peers, send, recv):
+    def exchange(self, rank, peers, send, recv, stream=None):
+        torch.cuda.synchronize()                  # every rank's pack has landed
         for p in peers:
             self.box[(rank, p)] = send[p]
         self.barrier.wait()
@@ -153,13 +171,21 @@ class SlabRank:
         arr = (C.c_int32 * max(cnt.value, 1))()
         self.sim._chk(lib.pk_halo_peers(h, arr, cnt.value, C.byref(cnt)), "pk_halo_peers")
         self.peers = [arr[i] for i in range(cnt.value)]
-        self.send, self.recv = {}, {}
-        for p in self.peers:
-            s, r = C.c_int64(), C.c_int64()
-            self.sim._chk(lib.pk_halo_sizes(h, p, C.byref(s), C.byref(r)), "pk_halo_sizes")
-            self.send[p] = torch.empty(s.value, dtype=torch.float64, device=self.device)
-            self.recv[p] = torch.empty(r.value, dtype=torch.float64, device=self.device)
+        # buffers per direction: -1 the whole halo (guard refreshes), 0..2 the
+        # face boxes a sweep along that direction reads
+        self.bufs = {}
+        for direction in (-1, 0, 1, 2):
+            send, recv = {}, {}
+            for p in self.peers:
+                s, r = C.c_int64(), C.c_int64()
+                self.sim._chk(lib.pk_halo_sizes_dir(h, p, direction, C.byref(s), C.byref(r)), "pk_halo_sizes_dir")
+                send[p] = torch.empty(s.value, dtype=torch.float64, device=self.device)
+                recv[p] = torch.empty(r.value, dtype=torch.float64, device=self.device)
+            active = [p for p in self.peers if send[p].numel() or recv[p].numel()]
+            self.bufs[direction] = (send, recv, active)
+        self.send, self.recv, _ = self.bufs[-1]
         self.exchanges = 0
+        self.skipped = 0
         self.error = None
         self._halo_cb = L.HALO_FN(self._halo)
         self._reduce_cb = L.REDUCE_FN(self._reduce)
@@ -174,15 +200,21 @@ class SlabRank:
     # cannot cross the C boundary, so it is kept and raised by check()
     def _halo(self, ctx, direction):
         lib, h = self.sim.lib, self.sim.h
-        for p in self.peers:
-            rc = lib.pk_halo_pack(h, p, self.send[p].data_ptr())
-            if rc != L.PK_OK and self.error is None:
-                self.error = f"pk_halo_pack: {lib.pk_last_error(h).decode()}"
-        self.transport.exchange(self.rank, self.peers, self.send, self.recv)
-        for p in self.peers:
-            rc = lib.pk_halo_unpack(h, p, self.recv[p].data_ptr())
-            if rc != L.PK_OK and self.error is None:
-                self.error = f"pk_halo_unpack: {lib.pk_last_error(h).decode()}"
+        send, recv, active = self.bufs[direction if direction in self.bufs else -1]
+        if not active:                  # nothing crosses ranks for this sweep (the same on every rank)
+            self.skipped += 1
+            return
+        for p in active:
+            if send[p].numel():
+                rc = lib.pk_halo_pack_dir(h, p, direction, send[p].data_ptr())
+                if rc != L.PK_OK and self.error is None:
+                    self.error = f"pk_halo_pack_dir: {lib.pk_last_error(h).decode()}"
+        self.transport.exchange(self.rank, active, send, recv, self.sim.stream)
+        for p in active:
+            if recv[p].numel():
+                rc = lib.pk_halo_unpack_dir(h, p, direction, recv[p].data_ptr())
+                if rc != L.PK_OK and self.error is None:
+                    self.error = f"pk_halo_unpack_dir: {lib.pk_last_error(h).decode()}"
         self.exchanges += 1
 
     def check(self):

@@ -40,7 +40,7 @@ def run_ranks(full, state, world, nsteps, axis=2):
     assert not errors, errors
     for r in ranks:
         r.detach()
-    out = [(r.layout[r.rank], r.sim.download(), r.sim.time_state, r.exchanges) for r in ranks]
+    out = [(r.layout[r.rank], r.sim.download(), r.sim.time_state, (r.exchanges, r.skipped)) for r in ranks]
     for r in ranks:
         r.close()
     return out
@@ -62,10 +62,61 @@ def test_slabs_equal_one_block(gpu_lib, phys, world, axis, order):
     g = full.guards
     for (n, off), arrs, st_r, nex in run_ranks(full, state, world, 3, axis):
         assert st_r.t == st.t and st_r.dt == st.dt
-        assert nex >= 3 * 6 * (1 if order == 2 else 1)
+        moved, skipped = nex
+        if order == 2:      # fused sweeps: only the two sweeps along the slab axis per step cross ranks
+            assert moved == 3 * 2 and skipped == 3 * 4, nex
+        else:               # per-stage path: the whole halo after every stage
+            assert moved >= 3 * 6, nex
         for k in range(3):
             if arrs[k] is None:
                 continue
             mine = arrs[k][g[2]:g[2] + n[2], g[1]:g[1] + n[1], g[0]:g[0] + n[0]]
             want = ref[k][tuple(slice(g[d] + off[d], g[d] + off[d] + n[d]) for d in (2, 1, 0))]
             assert_bitexact(mine, want, f"{phys} slab {off} array {k}")
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_block_shards_equal_one_handle(gpu_lib, world):
+    """Independent uneven blocks (ion MHD + neutral + dust) split into
+    per-rank block lists, ranks as threads with the in-process transport:
+    with dt reduced over ranks every block evolves bit for bit as in one
+    handle holding them all."""
+    from piernik_b200 import problems
+    from piernik_b200.shard import BlockShard
+    data = problems.batched_blocks(nblocks=7, seed=5, sizes=(8, 16, 24), n0=16)
+    one = Simulation(data[0][0])
+    for s, *_ in data[1:]:
+        one.add_block(s)
+    for i, (s, u, b, psi) in enumerate(data):
+        one.upload(u, b, psi, block=i)
+    one.run(3)
+    ref = [one.download(block=i) for i in range(len(data))]
+    st = one.time_state
+    one.close()
+    tr = ThreadTransport(world)
+    shards = [BlockShard(data, r, world, tr) for r in range(world)]
+    errors = []
+
+    def go(sh):
+        try:
+            sh.run(3)
+        except Exception as e:          # noqa: BLE001 -- reported below
+            errors.append(e)
+
+    th = [threading.Thread(target=go, args=(sh,)) for sh in shards]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=300)
+    assert not errors, errors
+    seen = set()
+    for sh in shards:
+        ts = sh.sim.time_state
+        assert (ts.t, ts.dt, ts.nstep) == (st.t, st.dt, st.nstep)
+        for i in sh.mine:
+            for k, (x, y) in enumerate(zip(sh.download(i), ref[i])):
+                if x is not None:
+                    assert_bitexact(x, y, f"block {i} array {k} on rank {sh.rank}")
+            seen.add(i)
+        sh.close()
+    assert seen == set(range(len(data)))
