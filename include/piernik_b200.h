@@ -384,7 +384,11 @@ int pk_refine_candidates(pk_handle h, int32_t id, const int32_t bsize[3], int64_
  *   local guard exchange (dir = the sweep direction 0..2, or -1) and must
  *   pack, move and unpack for all peers; reduce(ctx, x, op) returns the
  *   minimum (op 0) or maximum (op 1) of x over ranks and is used for dt and
- *   c_all in pk_time_step.  With callbacks set, pk_run does not use graphs.
+ *   c_all in pk_time_step, for chspeed (grid: minimum, hdc.F90:138; gas:
+ *   maximum) and the glmdamping factor (minimum, hdc.F90:333) in each
+ *   fluid update, and for the negatives flag of the step retry (maximum);
+ *   every rank makes these calls in the same order.  With callbacks set,
+ *   pk_run does not use graphs.
  * Both sides order a peer's cells alike (by positions on the level's grid). */
 typedef void (*pk_halo_fn)(void* ctx, int32_t dir);
 typedef double (*pk_reduce_fn)(void* ctx, double x, int32_t op);

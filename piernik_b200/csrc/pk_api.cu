@@ -583,7 +583,9 @@ int exchange_prepare(pk_ctx* h)
 }
 
 // launch the exchange between this rank's blocks on the current state, then
-// let the host move the other ranks' halo (dir: sweep direction or -1)
+// let the host move the other ranks' halo.  dir >= 0: only the face boxes
+// along dir, all a fused sweep along dir reads (called right before it);
+// -1: every guard cell
 // need >= 0: only the guard cells the interior-trimmed stage kernel reads
 // when it next sweeps direction need (refined domains; every other guard cell
 // may stay stale until a full refresh)
@@ -890,7 +892,7 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
                 if (int rc = fill_guards_block(h, b)) return rc;
         // the batched stage reads two guard layers along the next stage's direction only
         const int need = !h->stage_batched ? -1 : (s < nst ? dir : next_dir);
-        if (int rc = exchange_guards(h, dir, need)) return rc;
+        if (int rc = exchange_guards(h, -1, need)) return rc;   // every guard cell (the next sweep's too)
     }
     if (h->cfg.magnetic && apply_fac) return glm_scale_dev(h);
     return PK_OK;
@@ -989,9 +991,12 @@ int glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fac
     double c = DBL_MAX;
     if (!h->cfg.ch_grid) {
         if (int rc = gas_chspeed(h, &c)) return rc;
-    } else if (eff) {
-        const double x = (h->cfg.cfl_glm * mdl) / dt;
-        c = (x < c) ? x : c;
+    } else {
+        if (eff) {
+            const double x = (h->cfg.cfl_glm * mdl) / dt;
+            c = (x < c) ? x : c;
+        }
+        if (h->reduce_cb) c = h->reduce_cb(h->comm_ctx, c, 0);   // piernik_MPI_Allreduce(chspeed, pMIN) (hdc.F90:138)
     }
     double f = 0.0;
     if (eff) {
@@ -1000,6 +1005,7 @@ int glm_scalars_for(pk_ctx* h, double dt, double ch_now, double* ch, double* fac
     }
     *ch = c;
     *fac = std::exp(-f);
+    if (h->reduce_cb) *fac = h->reduce_cb(h->comm_ctx, *fac, 0);   // piernik_MPI_Allreduce(fac, pMIN) (:333)
     return PK_OK;
 }
 
@@ -1015,7 +1021,8 @@ double glm_fac_for(pk_ctx* h, double dt_eff, double ch)
         const double x = (h->cfg.glm_alpha * ch) / (mdl / dt_eff);
         f = (x > f) ? x : f;
     }
-    return std::exp(-f);
+    const double fac = std::exp(-f);
+    return h->reduce_cb ? h->reduce_cb(h->comm_ctx, fac, 0) : fac;   // pMIN over ranks (hdc.F90:333)
 }
 
 }  // namespace
