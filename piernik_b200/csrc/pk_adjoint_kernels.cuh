@@ -38,10 +38,13 @@ struct AdjSmem {
 // computed (cells [max(va+3, ma+2), min(vb-3, mb-2)) ).  mp / mn: the slots
 // of the previous / next cell along the pencil; circ: the tile is a whole
 // periodic pencil (every cell valid, neighbours wrap).
+// The cell's V is read from vsrc (at off, swept order) in phase A and again
+// in phase E, not held in registers across the Riemann adjoint of phase C,
+// which needs every register it can get.
 template <class PH>
 PK_DEV void adj_divergence(const AdjSmem& sm, int me, int mp, int mn, bool circ, int t, bool active, int va, int vb,
-                           int ma, int mb, const double (&V)[PH::NV], const double (&mu)[PH::NV], double ch,
-                           const PhysParams& pp, double (&out)[PH::NV])
+                           int ma, int mb, const double* vsrc, long long off, const Geom& g,
+                           const double (&mu)[PH::NV], double ch, const PhysParams& pp, double (&out)[PH::NV])
 {
     constexpr int NV = PH::NV;
     const int PT = sm.PT;
@@ -51,7 +54,8 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int mp, int mn, bool circ,
     auto fv = [&](int x) { return sv(x) && sv(x + 1) && mv(x) && mv(x + 1); };   // face x+1/2
     // A: primitives and mu
     if (qv(t)) {
-        double q[NV];
+        double V[NV], q[NV];
+        load_cell<PH>(vsrc, off, g, V);
         utoq<PH>(V, q, pp);
 #pragma unroll
         for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = q[v];
@@ -121,6 +125,8 @@ PK_DEV void adj_divergence(const AdjSmem& sm, int me, int mp, int mn, bool circ,
             if (sn) x += sm.M[v * PT + mp];
             qb[v] = x;
         }
+        double V[NV];
+        load_cell<PH>(vsrc, off, g, V);
         utoq_adj<PH>(V, qb, out, pp);
     }
     __syncthreads();
@@ -202,31 +208,34 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage2(Geom g, Tile tl, cons
     const StepParams stp = sp[a.seg];
     const double dt = stp.dt, ch = stp.ch, fac = apply_fac ? stp.psi_fac : 1.0;
     const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
-    double V[NV], mu[NV], mu2[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) V[v] = mu[v] = 0.0;
-    unsigned short fl = 0;
-    if (a.active) {
-        load_cell<PH>(ustar, a.off, g, V);
-        load_cell<PH>(lam_out, a.off, g, mu);
-        fl = flags[a.off];
-        if (PH::MHD) mu[PH::IB + 3] = mu[PH::IB + 3] * fac;
-        const FloorRec r2 = unpack_floors(fl, 2);
+    // mu2 = floors2^T (fac-scaled lam''); formed before the divergence and
+    // again after it rather than kept in registers across it
+    auto mu2_of = [&](double (&m)[NV]) {
+        load_cell<PH>(lam_out, a.off, g, m);
+        if (PH::MHD) m[PH::IB + 3] = m[PH::IB + 3] * fac;
+        const FloorRec r2 = unpack_floors(flags[a.off], 2);
         if (r2.en || r2.dn) {
             double w[NV];
             load_cell<PH>(uout, a.off, g, w);
-            floors_adj<PH>(w, r2, mu);
+            floors_adj<PH>(w, r2, m);
         }
-    }
+    };
+    double mu[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        mu2[v] = mu[v];
-        mu[v] = c2 * mu[v];
+    for (int v = 0; v < NV; ++v) mu[v] = 0.0;
+    if (a.active) {
+        mu2_of(mu);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) mu[v] = c2 * mu[v];
     }
     double rho[NV];
-    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, ch, pp, rho);
+    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, ustar, a.off, g, mu, ch, pp,
+                       rho);
     if (a.own) {
-        floors_adj<PH>(V, unpack_floors(fl, 1), rho);
+        double V[NV], mu2[NV];
+        load_cell<PH>(ustar, a.off, g, V);
+        floors_adj<PH>(V, unpack_floors(flags[a.off], 1), rho);
+        mu2_of(mu2);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             mu2[v] += rho[v];
@@ -248,15 +257,13 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage1(Geom g, Tile tl, cons
     const int PT = tl.P * tl.T;
     const AdjSmem asm_{smem, smem + NV * PT, smem + 2 * NV * PT, smem + 3 * NV * PT, PT};
     const AdjPos a = adj_pos(g, tl);
-    double V[NV], mu[NV];
+    double mu[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) V[v] = mu[v] = 0.0;
-    if (a.active) {
-        load_cell<PH>(uin, a.off, g, V);
-        load_cell<PH>(m1, a.off, g, mu);
-    }
+    for (int v = 0; v < NV; ++v) mu[v] = 0.0;
+    if (a.active) load_cell<PH>(m1, a.off, g, mu);
     double rho[NV];
-    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, V, mu, sp[a.seg].ch, pp, rho);
+    adj_divergence<PH>(asm_, a.me, a.mp, a.mn, a.circ, a.t, a.active, 0, tl.T, 0, tl.T, uin, a.off, g, mu, sp[a.seg].ch,
+                       pp, rho);
     if (a.own) {
         double l[NV];
         load_cell<PH>(lam_io, a.off, g, l);
