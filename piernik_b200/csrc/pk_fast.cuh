@@ -7,7 +7,9 @@
 // divisions by a common denominator are replaced by one reciprocal and
 // products (1/rho in utoq; 1/(gamma-1) and 1/gamma from PhysParams; 1/slsm,
 // 1/srsm, 1/(coeff_1), 1/(add_dnsq) and 1/ch in the Riemann solver; the two
-// Alfven divisions by sqrt(rho*) through rsqrt).  Each replaced operation
+// Alfven divisions by sqrt(rho*) through the reciprocal square root), and
+// the remaining quotients, reciprocals and square roots of the solver and of
+// utoq are the branch-free refinements below (rcp_nr, div_nr, rsqrt_nr).  Each replaced operation
 // changes a result by a few units in the last place, so a time step agrees
 // with the bit-exact path to ~1e-15 relative; the tests hold it to 1e-12 per
 // step and 1e-9 after 100 steps.
@@ -16,6 +18,45 @@
 
 namespace pk {
 
+// Reciprocal, quotient and reciprocal square root without the IEEE
+// sequences' special-case branches: the hardware's approximate FP64
+// reciprocal and reciprocal square root (PTX rcp.approx.ftz.f64,
+// rsqrt.approx.ftz.f64, about 20 correct bits) refined by Newton-Raphson
+// iterations (r' = r + r(1 - x r) and y' = y(3/2 - x y^2/2): each doubles the
+// correct bits, two reach the double precision), the quotient finished with
+// one residual correction (Markstein, IBM J. Res. Dev. 34 (1990) 111-119).
+// Results are within about an ulp of the correctly rounded ones for normal
+// finite operands, which is all the tolerance arithmetic asks; subnormal
+// operands are flushed to zero by the seeds and are not expected in the
+// states.  Square roots keep the IEEE operation: a Newton-refined root
+// (tried) moved a three-fluid blast beyond the 1e-12 per-step bound.
+PK_DEV double rcp_nr(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+PK_DEV double div_nr(double a, double b)
+{
+    const double r = rcp_nr(b);
+    const double q = a * r;
+    return fma(r, fma(-b, q, a), q);
+}
+
+PK_DEV double rsqrt_nr(double x)
+{
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double hx = 0.5 * x;
+    y = y * fma(-hx * y, y, 1.5);
+    return y * fma(-hx * y, y, 1.5);
+}
+
+
 template <class PH>
 PK_DEV void utoq_fast(const double (&u)[PH::NV], double (&q)[PH::NV], const PhysParams& pp)
 {
@@ -23,7 +64,7 @@ PK_DEV void utoq_fast(const double (&u)[PH::NV], double (&q)[PH::NV], const Phys
     for (int f = 0; f < PH::NFL; ++f) {
         const int b = PH::beg(f);
         const double dn = u[b], mx = u[b + 1], my = u[b + 2], mz = u[b + 3];
-        const double rdn = 1.0 / dn;
+        const double rdn = rcp_nr(dn);
         q[b] = dn;
         q[b + 1] = mx * rdn;
         q[b + 2] = my * rdn;
@@ -69,7 +110,7 @@ PK_DEV void hlld_iface_fast(bool has_energy, double gamma, double rgam_1, double
         const double nl = al + sqrt(al * al - ((4.0 * gampr_l) * (bl[0] * bl[0])));
         const double nr = ar + sqrt(ar * ar - ((4.0 * gampr_r) * (br[0] * br[0])));
         // max(nl/rho_l, nr/rho_r) with one division (densities are positive)
-        const double cmax = (nl * ur[0] >= nr * ul[0]) ? nl / ul[0] : nr / ur[0];
+        const double cmax = (nl * ur[0] >= nr * ul[0]) ? div_nr(nl, ul[0]) : div_nr(nr, ur[0]);
         c_fastm = sqrt(0.5 * cmax);
     }
     const double sl = f_min(ul[1], ur[1]) - c_fastm;
@@ -90,10 +131,10 @@ PK_DEV void hlld_iface_fast(bool has_energy, double gamma, double rgam_1, double
         const double auxr = (sr - ur[1]) * ur[0];
         const double auxl = (sl - ul[1]) * ul[0];
         if (fabs(auxr - auxl) < f_spacing(auxr + auxl)) sm = (sl + sr) * 0.5;
-        else sm = ((auxr * ur[1] - prr) - (auxl * ul[1] - prl)) / (auxr - auxl);
+        else sm = div_nr((auxr * ur[1] - prr) - (auxl * ul[1] - prl), auxr - auxl);
     }
     const double slsm = sl - sm, srsm = sr - sm;
-    const double rslsm = 1.0 / slsm, rsrsm = 1.0 / srsm;
+    const double rslsm = rcp_nr(slsm), rsrsm = rcp_nr(srsm);
     const double slvxl = sl - ul[1], srvxr = sr - ur[1];
     const double srmsl = sr - sl;
     const double dn_l = ul[0] * slvxl, dn_r = ur[0] * srvxr;
@@ -112,17 +153,17 @@ PK_DEV void hlld_iface_fast(bool has_energy, double gamma, double rgam_1, double
         if (has_energy) ue = ur[4];
         const bool star_r = (fabs(coeff_r) > f_spacing(b_lr)) && b_lrgam <= ue;
         if (star_l) {
-            const double t = (dn_l * slvxl - b_lr) / coeff_1;
+            const double t = div_nr(dn_l * slvxl - b_lr, coeff_1);
             bsl[1] = bl[1] * t;
             bsl[2] = bl[2] * t;
         }
         if (star_r) {
-            const double t = (dn_r * srvxr - b_lr) / coeff_r;
+            const double t = div_nr(dn_r * srvxr - b_lr, coeff_r);
             bsr[1] = br[1] * t;
             bsr[2] = br[2] * t;
         }
         if (!star_l || !star_r) {                  // the HLL state of the transverse field
-            const double r = 1.0 / srmsl;
+            const double r = rcp_nr(srmsl);
             const double h1 = ((sr * br[1] - sl * bl[1]) - (side_bflux(ur, br, 1) - side_bflux(ul, bl, 1))) * r;
             const double h2 = ((sr * br[2] - sl * bl[2]) - (side_bflux(ur, br, 2) - side_bflux(ul, bl, 2))) * r;
             if (!star_l) {
@@ -139,7 +180,7 @@ PK_DEV void hlld_iface_fast(bool has_energy, double gamma, double rgam_1, double
     vsl[0] = sm;
     vsr[0] = sm;
     {
-        const double bxl_dnl = bl[0] / dn_l, bxr_dnr = br[0] / dn_r;
+        const double bxl_dnl = div_nr(bl[0], dn_l), bxr_dnr = div_nr(br[0], dn_r);
         vsl[1] = ul[2] + (bxl_dnl * (bl[1] - bsl[1]));
         vsl[2] = ul[3] + (bxl_dnl * (bl[2] - bsl[2]));
         vsr[1] = ur[2] + (bxr_dnr * (br[1] - bsr[1]));
@@ -180,7 +221,7 @@ PK_DEV void hlld_iface_fast(bool has_energy, double gamma, double rgam_1, double
     };
 
     if (fabs(bl[0]) > 0.0) {
-        const double rl = rsqrt(usl[0]), rr = rsqrt(usr[0]);
+        const double rl = rsqrt_nr(usl[0]), rr = rsqrt_nr(usr[0]);
         const double dn_lsqt = usl[0] * rl;            // sqrt(rho*_l)
         const double dn_rsqt = usr[0] * rr;
         const double alfven_l = sm - fabs(bl[0]) * rl;
@@ -190,7 +231,7 @@ PK_DEV void hlld_iface_fast(bool has_energy, double gamma, double rgam_1, double
             return;
         }
         const double b_sig = (bl[0] >= 0.0) ? 1.0 : -1.0;
-        const double radd = 1.0 / (dn_lsqt + dn_rsqt);
+        const double radd = rcp_nr(dn_lsqt + dn_rsqt);
         const double mul_dnsq = dn_lsqt * dn_rsqt;
         double v2[3], b2[3];
         v2[0] = sm;
@@ -276,7 +317,7 @@ PK_DEV void hllc_iface_fast(bool has_energy, double gamma, double rgam_1, const 
         enr = (ur[4] * rgam_1) + ((0.5 * ur[0]) * ((ur[1] * ur[1] + ur[2] * ur[2]) + ur[3] * ur[3]));
         const double gampr_l = gamma * ul[4];
         const double gampr_r = gamma * ur[4];
-        const double cmax = (gampr_l * ur[0] >= gampr_r * ul[0]) ? gampr_l / ul[0] : gampr_r / ur[0];
+        const double cmax = (gampr_l * ur[0] >= gampr_r * ul[0]) ? div_nr(gampr_l, ul[0]) : div_nr(gampr_r, ur[0]);
         c_fastm = sqrt(cmax);
     }
     const double sl = f_min(ul[1], ur[1]) - c_fastm;
@@ -308,13 +349,13 @@ PK_DEV void hllc_iface_fast(bool has_energy, double gamma, double rgam_1, const 
         const double auxr = (sr - ur[1]) * ur[0];
         const double auxl = (sl - ul[1]) * ul[0];
         if (fabs(auxr - auxl) < f_spacing(auxr + auxl)) sm = (sl + sr) * 0.5;
-        else sm = ((auxr * ur[1] - prr) - (auxl * ul[1] - prl)) / (auxr - auxl);
+        else sm = div_nr((auxr * ur[1] - prr) - (auxl * ul[1] - prl), auxr - auxl);
     }
     const double slvxl = sl - ul[1], srvxr = sr - ur[1];
     const double dn_l = ul[0] * slvxl, dn_r = ur[0] * srvxr;
     const double prt_star = 0.5 * ((prl + dn_l * (sm - ul[1])) + (prr + dn_r * (sm - ur[1])));
     if (sm >= 0.0) {
-        const double r = 1.0 / (sl - sm);
+        const double r = rcp_nr(sl - sm);
         usl[0] = dn_l * r;
         usl[1] = usl[0] * sm;
         usl[2] = usl[0] * ul[2];
@@ -322,7 +363,7 @@ PK_DEV void hllc_iface_fast(bool has_energy, double gamma, double rgam_1, const 
         if (has_energy) usl[4] = (((slvxl * enl) - (prl * ul[1])) + (prt_star * sm)) * r;
     }
     if (sm <= 0.0) {
-        const double r = 1.0 / (sr - sm);
+        const double r = rcp_nr(sr - sm);
         usr[0] = dn_r * r;
         usr[1] = usr[0] * sm;
         usr[2] = usr[0] * ur[2];

@@ -170,7 +170,7 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
     }
     __syncthreads();
     if (r.flux) {
-        if constexpr (FAST) riemann_tile_fast<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, 1.0 / ch, pp);
+        if constexpr (FAST) riemann_tile_fast<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, rcp_nr(ch), pp);
         else riemann_tile<PH>(sm.L, sm.R, sm.Q, PT, me, mn - me, ch, pp);
     }
     __syncthreads();
