@@ -43,17 +43,17 @@ NVAR = 9                         # dn, mx, my, mz, en, Bx, By, Bz, psi
 # DRAM bytes per cell of one sweep launch, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the TMA-staged y sweep of a
 # 128^3 block (181 MB with guards, above the 126 MB L2) in the tolerance
-# arithmetic: 163.45 MB read + 112.46 MB written over 128^3 cells.  Traffic
+# arithmetic: 161.11 MB read + 113.07 MB written over 128^3 cells.  Traffic
 # grows with the cell count, so the full-size figure is this times n^3.
-TRAFFIC_BYTES_PER_CELL = (163.454976e6 + 112.455424e6) / 128 ** 3
+TRAFFIC_BYTES_PER_CELL = (161.105664e6 + 113.074688e6) / 128 ** 3
 # FP64 flops per cell of one sweep (both RK2 stages) without halo
 # recomputation: 2 x DFMA + DMUL + DADD thread instructions (ncu
 # sm__sass_thread_inst_executed_op_{dfma,dmul,dadd}_pred_on.sum) of the
 # TMA-staged whole-pencil x sweep of a 128^3 block over its 128^3 cells, in
 # the bit-exact arithmetic (0.8408 G DFMA, 0.9312 G DMUL, 0.9150 G DADD) and in
-# the tolerance arithmetic (0.8082 G DFMA, 0.5069 G DMUL, 0.4459 G DADD)
+# the tolerance arithmetic (0.7899 G DFMA, 0.5277 G DMUL, 0.4303 G DADD)
 FP64_FLOP_PER_CELL_SWEEP = (2 * 840755524 + 931189733 + 915036464) / 128 ** 3
-FP64_FLOP_PER_CELL_SWEEP_FMA = (2 * 808225550 + 506923602 + 445894955) / 128 ** 3
+FP64_FLOP_PER_CELL_SWEEP_FMA = (2 * 789901529 + 527723486 + 430337951) / 128 ** 3
 ARITH_NOTE = {
     "fma": "fma: multiply-add contraction and hoisted reciprocals in the fused sweep; agrees with the "
            "reference's arithmetic to <= 1e-12 relative per step and <= 1e-9 after 100 steps (tests/test_gpu_fma.py)",
