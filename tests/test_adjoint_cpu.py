@@ -28,7 +28,7 @@ def P(a):
 
 @pytest.fixture(scope="module")
 def H():
-    deps = [SRC] + [os.path.join(HERE, "..", "piernik_b200", "csrc", f) for f in ("pk_device.cuh", "pk_adjoint.cuh")]
+    deps = [SRC] + [os.path.join(HERE, "..", "piernik_b200", "csrc", f) for f in ("pk_device.cuh", "pk_fast.cuh", "pk_adjoint.cuh")]
     if not os.path.exists(LIB) or any(os.path.getmtime(d) > os.path.getmtime(LIB) for d in deps):
         subprocess.check_call(["nvcc", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
                                "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, SRC])
