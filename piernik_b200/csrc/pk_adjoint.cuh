@@ -33,6 +33,11 @@ PK_PHYS double arcp(double x)
 #endif
 }
 
+// a*b + c in one rounding: the multiply-accumulates of the reverse pass (the
+// translation unit keeps --fmad=false for the primal recompute, so the fused
+// operation is written out).
+PK_PHYS double fm(double a, double b, double c) { return fma(a, b, c); }
+
 // Compile-time side of a Riemann interface.  The adjoints below pick the left
 // or right state's arrays with it, so that no array has to live in local
 // memory for a run-time pointer choice.
@@ -51,26 +56,28 @@ PK_PHYS void utoq_adj(const double (&u)[PH::NV], const double (&qb)[PH::NV], dou
         const int b = PH::beg(f);
         const double dn = u[b], mx = u[b + 1], my = u[b + 2], mz = u[b + 3];
         const double rdn = arcp(dn);
-        const double q1 = mx * rdn, q2 = my * rdn, q3 = mz * rdn;
-        ub[b] += qb[b] - (qb[b + 1] * q1 + qb[b + 2] * q2 + qb[b + 3] * q3) * rdn;
-        ub[b + 1] += qb[b + 1] * rdn;
-        ub[b + 2] += qb[b + 2] * rdn;
-        ub[b + 3] += qb[b + 3] * rdn;
+        const double qv = fm(qb[b + 3], mz, fm(qb[b + 2], my, qb[b + 1] * mx));   // qb . m
+        double u0 = fm(-qv, rdn * rdn, ub[b] + qb[b]);
+        ub[b + 1] = fm(qb[b + 1], rdn, ub[b + 1]);
+        ub[b + 2] = fm(qb[b + 2], rdn, ub[b + 2]);
+        ub[b + 3] = fm(qb[b + 3], rdn, ub[b + 3]);
         if (PH::has_en(f)) {
             const double g1 = pp.gam_1[f], pb = qb[b + 4];
-            ub[b + 4] += g1 * pb;
+            ub[b + 4] = fm(g1, pb, ub[b + 4]);
             const double ekb = -g1 * pb;                       // p = g1*(E - ek)
-            const double ek = (0.5 * ((mx * mx + my * my) + mz * mz)) * rdn;
-            ub[b] += -ekb * ek * rdn;
-            const double sqb = ekb * 0.5 * rdn;
-            ub[b + 1] += sqb * 2.0 * mx;
-            ub[b + 2] += sqb * 2.0 * my;
-            ub[b + 3] += sqb * 2.0 * mz;
+            const double ek = (0.5 * fm(mz, mz, fm(my, my, mx * mx))) * rdn;
+            u0 = fm(-ekb * ek, rdn, u0);
+            const double sqb2 = ekb * rdn;                     // d(ek)/dm = m/rho
+            ub[b + 1] = fm(sqb2, mx, ub[b + 1]);
+            ub[b + 2] = fm(sqb2, my, ub[b + 2]);
+            ub[b + 3] = fm(sqb2, mz, ub[b + 3]);
             if (PH::magn(f)) {                                 // p -= (0.5*g1)*|B|^2
+                const double t = -g1 * pb;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) ub[PH::IB + c] += -g1 * pb * u[PH::IB + c];
+                for (int c = 0; c < 3; ++c) ub[PH::IB + c] = fm(t, u[PH::IB + c], ub[PH::IB + c]);
             }
         }
+        ub[b] = u0;
     }
     if (PH::MHD) {
 #pragma unroll
@@ -165,44 +172,46 @@ PK_PHYS void floors_adj(const double (&uout)[PH::NV], const FloorRec& rec, doubl
 PK_PHYS void side_flux_adj(bool has_energy, const double* u, const double* b, double pr, double en, const double* fb,
                            const double* bfb, double* ub, double* bb, double& prb, double& enb)
 {
-    const double vb = (u[1] * b[0] + u[2] * b[1]) + u[3] * b[2];
+    const double vb = fm(u[3], b[2], fm(u[2], b[1], u[1] * b[0]));
     const double f4 = has_energy ? fb[4] : 0.0;
-    ub[0] += fb[0] * u[1] + fb[1] * (u[1] * u[1]) + fb[2] * u[2] * u[1] + fb[3] * u[3] * u[1];
-    ub[1] += fb[0] * u[0] + fb[1] * 2.0 * u[0] * u[1] + fb[2] * u[0] * u[2] + fb[3] * u[0] * u[3] +
-             f4 * ((en + pr) - b[0] * b[0]) + bfb[0] * b[1] + bfb[1] * b[2];
-    ub[2] += fb[2] * u[0] * u[1] - f4 * b[0] * b[1] - bfb[0] * b[0];
-    ub[3] += fb[3] * u[0] * u[1] - f4 * b[0] * b[2] - bfb[1] * b[0];
-    prb += fb[1] + f4 * u[1];
-    enb += f4 * u[1];
-    bb[0] += -2.0 * fb[1] * b[0] - fb[2] * b[1] - fb[3] * b[2] - f4 * (vb + b[0] * u[1]) - bfb[0] * u[2] - bfb[1] * u[3];
-    bb[1] += -fb[2] * b[0] - f4 * b[0] * u[2] + bfb[0] * u[1];
-    bb[2] += -fb[3] * b[0] - f4 * b[0] * u[3] + bfb[1] * u[1];
+    const double mv = fm(fb[3], u[3], fm(fb[2], u[2], fm(fb[1], u[1], fb[0])));   // fb[0..3] . (1, u1, u2, u3)
+    const double u0u1 = u[0] * u[1], f4b0 = f4 * b[0];
+    ub[0] = fm(mv, u[1], ub[0]);
+    ub[1] = fm(u[0], fm(fb[1], u[1], mv), fm(f4, fm(-b[0], b[0], en + pr), fm(bfb[1], b[2], fm(bfb[0], b[1], ub[1]))));
+    ub[2] = fm(fb[2], u0u1, fm(-f4b0, b[1], fm(-bfb[0], b[0], ub[2])));
+    ub[3] = fm(fb[3], u0u1, fm(-f4b0, b[2], fm(-bfb[1], b[0], ub[3])));
+    prb += fm(f4, u[1], fb[1]);
+    enb = fm(f4, u[1], enb);
+    bb[0] -= fm(2.0 * fb[1], b[0], fm(fb[2], b[1], fm(fb[3], b[2], fm(f4, fm(b[0], u[1], vb), fm(bfb[0], u[2], bfb[1] * u[3])))));
+    bb[1] += fm(-fb[2], b[0], fm(-f4b0, u[2], bfb[0] * u[1]));
+    bb[2] += fm(-fb[3], b[0], fm(-f4b0, u[3], bfb[1] * u[1]));
 }
 
 // adjoint of pr = p + |B|^2/2 and en = p/(g-1) + rho v^2/2 + |B|^2/2 (hlld.F90:258-269)
 PK_PHYS void pr_en_adj(bool mhd, double gamma, const double* u, const double* b, double prb, double enb, double* ub,
                        double* bb)
 {
-    ub[4] += prb + enb * arcp(gamma - 1.0);
-    const double vv = (u[1] * u[1] + u[2] * u[2]) + u[3] * u[3];
-    ub[0] += enb * 0.5 * vv;
-    ub[1] += enb * u[0] * u[1];
-    ub[2] += enb * u[0] * u[2];
-    ub[3] += enb * u[0] * u[3];
+    ub[4] = fm(enb, arcp(gamma - 1.0), ub[4] + prb);
+    const double vv = fm(u[3], u[3], fm(u[2], u[2], u[1] * u[1]));
+    ub[0] = fm(enb * 0.5, vv, ub[0]);
+    const double eu = enb * u[0];
+    ub[1] = fm(eu, u[1], ub[1]);
+    ub[2] = fm(eu, u[2], ub[2]);
+    ub[3] = fm(eu, u[3], ub[3]);
     if (mhd) {
         const double t = prb + enb;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) bb[c] += t * b[c];
+        for (int c = 0; c < 3; ++c) bb[c] = fm(t, b[c], bb[c]);
     }
 }
 
 // adjoint of cons = [u0, u0*u1, u0*u2, u0*u3, en] given consb
 PK_PHYS void cons_adj(bool has_energy, const double* u, const double* consb, double* ub, double& enb)
 {
-    ub[0] += consb[0] + consb[1] * u[1] + consb[2] * u[2] + consb[3] * u[3];
-    ub[1] += consb[1] * u[0];
-    ub[2] += consb[2] * u[0];
-    ub[3] += consb[3] * u[0];
+    ub[0] = fm(consb[3], u[3], fm(consb[2], u[2], fm(consb[1], u[1], ub[0] + consb[0])));
+    ub[1] = fm(consb[1], u[0], ub[1]);
+    ub[2] = fm(consb[2], u[0], ub[2]);
+    ub[3] = fm(consb[3], u[0], ub[3]);
     if (has_energy) enb += consb[4];
 }
 
@@ -271,7 +280,7 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
             for (int c = 0; c < nc; ++c) {
                 const double g = w * fb[c];
                 fsb[c] = g;
-                sb += g * (us[c] - cons[c]);
+                sb = fm(g, us[c] - cons[c], sb);
                 usb[c] = g * s;
                 consb[c] = -g * s;
             }
@@ -279,23 +288,24 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
             side_flux_adj(has_energy, u, zbv, pr, en, fsb, zb, ub, bdump, prb, enb);
             cons_adj(has_energy, u, consb, ub, enb);
             // us
-            double us0b = usb[0] + usb[1] * sm + usb[2] * u[2] + usb[3] * u[3];
-            smb += usb[1] * us[0];
-            ub[2] += usb[2] * us[0];
-            ub[3] += usb[3] * us[0];
+            double us0b = fm(usb[3], u[3], fm(usb[2], u[2], fm(usb[1], sm, usb[0])));
+            smb = fm(usb[1], us[0], smb);
+            ub[2] = fm(usb[2], us[0], ub[2]);
+            ub[3] = fm(usb[3], us[0], ub[3]);
             double ssmb = 0.0;
             if (has_energy) {
                 const double n4b = usb[4] * rssm;
-                ssmb -= usb[4] * us[4] * rssm;
-                if (left) slvxlb += n4b * en; else srvxrb += n4b * en;
-                enb += n4b * svx;
-                prb -= n4b * u[1];
-                ub[1] -= n4b * pr;
-                prtb += n4b * sm;
-                smb += n4b * prt;
+                ssmb = -n4b * us[4];
+                if (left) slvxlb = fm(n4b, en, slvxlb); else srvxrb = fm(n4b, en, srvxrb);
+                enb = fm(n4b, svx, enb);
+                prb = fm(-n4b, u[1], prb);
+                ub[1] = fm(-n4b, pr, ub[1]);
+                prtb = fm(n4b, sm, prtb);
+                smb = fm(n4b, prt, smb);
             }
-            if (left) dn_lb += us0b * rssm; else dn_rb += us0b * rssm;
-            ssmb -= us0b * us[0] * rssm;
+            const double t0 = us0b * rssm;
+            if (left) dn_lb += t0; else dn_rb += t0;
+            ssmb = fm(-t0, us[0], ssmb);
             sb += ssmb;
             smb -= ssmb;
             if (left) { slb += sb; prlb += prb; enlb += enb; }
@@ -305,18 +315,19 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
         else if (sm < 0.0) side(Side<false>{}, 1.0);
         else { side(Side<true>{}, 0.5); side(Side<false>{}, 0.5); }
         // prt
-        prlb += 0.5 * prtb;
-        prrb += 0.5 * prtb;
-        dn_lb += 0.5 * prtb * (sm - ul[1]);
-        dn_rb += 0.5 * prtb * (sm - ur[1]);
-        smb += 0.5 * prtb * (dn_l + dn_r);
-        ulb[1] -= 0.5 * prtb * dn_l;
-        urb[1] -= 0.5 * prtb * dn_r;
+        const double hp = 0.5 * prtb;
+        prlb += hp;
+        prrb += hp;
+        dn_lb = fm(hp, sm - ul[1], dn_lb);
+        dn_rb = fm(hp, sm - ur[1], dn_rb);
+        smb = fm(hp, dn_l + dn_r, smb);
+        ulb[1] = fm(-hp, dn_l, ulb[1]);
+        urb[1] = fm(-hp, dn_r, urb[1]);
         // dn = u0 * svx
-        ulb[0] += dn_lb * slvxl;
-        slvxlb += dn_lb * ul[0];
-        urb[0] += dn_rb * srvxr;
-        srvxrb += dn_rb * ur[0];
+        ulb[0] = fm(dn_lb, slvxl, ulb[0]);
+        slvxlb = fm(dn_lb, ul[0], slvxlb);
+        urb[0] = fm(dn_rb, srvxr, urb[0]);
+        srvxrb = fm(dn_rb, ur[0], srvxrb);
         slb += slvxlb;
         ulb[1] -= slvxlb;
         srb += srvxrb;
@@ -328,20 +339,20 @@ PK_PHYS void hllc_adj(bool has_energy, double gamma, const double* ul, const dou
             srb += smb / 2.0;
         } else {
             const double rden = arcp(den);
-            const double numb = smb * rden, denb = -smb * sm * rden;
-            auxrb += numb * ur[1] + denb;
-            urb[1] += numb * auxr;
+            const double numb = smb * rden, denb = -numb * sm;
+            auxrb = fm(numb, ur[1], denb);
+            urb[1] = fm(numb, auxr, urb[1]);
             prrb -= numb;
-            auxlb += -numb * ul[1] - denb;
-            ulb[1] -= numb * auxl;
+            auxlb = fm(-numb, ul[1], -denb);
+            ulb[1] = fm(-numb, auxl, ulb[1]);
             prlb += numb;
         }
-        srb += auxrb * ur[0];
-        urb[1] -= auxrb * ur[0];
-        urb[0] += auxrb * (sr - ur[1]);
-        slb += auxlb * ul[0];
-        ulb[1] -= auxlb * ul[0];
-        ulb[0] += auxlb * (sl - ul[1]);
+        srb = fm(auxrb, ur[0], srb);
+        urb[1] = fm(-auxrb, ur[0], urb[1]);
+        urb[0] = fm(auxrb, sr - ur[1], urb[0]);
+        slb = fm(auxlb, ul[0], slb);
+        ulb[1] = fm(-auxlb, ul[0], ulb[1]);
+        ulb[0] = fm(auxlb, sl - ul[1], ulb[0]);
     }
     // sl = min(ul1, ur1) - cf ; sr = max(ul1, ur1) + cf
     if (minr) urb[1] += slb; else ulb[1] += slb;
@@ -507,16 +518,16 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             for (int c = 0; c < nc; ++c) {
                 const double g = w * fb5[c];
                 fsb[c] = g;
-                sb += g * (us[c] - cons[c]);
-                usb[c] += g * s;
+                sb = fm(g, us[c] - cons[c], sb);
+                usb[c] = fm(g, s, usb[c]);
                 consb[c] = -g * s;
             }
             for (int c = 1; c < 3; ++c) {
                 const double g = w * bfb[c - 1];
                 bfsb[c - 1] = g;
-                sb += g * (bs[c] - b[c]);
-                bsb[c] += g * s;
-                bb[c] -= g * s;
+                sb = fm(g, bs[c] - b[c], sb);
+                bsb[c] = fm(g, s, bsb[c]);
+                bb[c] = fm(-g, s, bb[c]);
             }
             double prb = 0.0, enb = 0.0;
             side_flux_adj(has_energy, u, b, left ? prl : prr, en, fsb, bfsb, ub, bb, prb, enb);
@@ -548,23 +559,24 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             double fsb[5] = {0, 0, 0, 0, 0}, consb[5] = {0, 0, 0, 0, 0}, u2b[5] = {0, 0, 0, 0, 0}, bfsb[2];
             double ab = 0.0, sb = 0.0;
             // out = ((fs + a*u2) - (a - s)*us) - s*cons
+            const double ams = a - s;
             for (int c = 0; c < nc; ++c) {
                 const double g = w * fb5[c];
                 fsb[c] = g;
-                ab += g * (u2[c] - us[c]);
+                ab = fm(g, u2[c] - us[c], ab);
                 u2b[c] = g * a;
-                usb[c] -= g * (a - s);
-                sb += g * (us[c] - cons[c]);
+                usb[c] = fm(-g, ams, usb[c]);
+                sb = fm(g, us[c] - cons[c], sb);
                 consb[c] = -g * s;
             }
             for (int c = 1; c < 3; ++c) {
                 const double g = w * bfb[c - 1];
                 bfsb[c - 1] = g;
-                ab += g * (b2[c] - bs[c]);
-                b2b[c] += g * a;
-                bsb[c] -= g * (a - s);
-                sb += g * (bs[c] - b[c]);
-                bb[c] -= g * s;
+                ab = fm(g, b2[c] - bs[c], ab);
+                b2b[c] = fm(g, a, b2b[c]);
+                bsb[c] = fm(-g, ams, bsb[c]);
+                sb = fm(g, bs[c] - b[c], sb);
+                bb[c] = fm(-g, s, bb[c]);
             }
             double prb = 0.0, enb = 0.0;
             side_flux_adj(has_energy, u, b, left ? prl : prr, en, fsb, bfsb, ub, bb, prb, enb);
@@ -572,8 +584,8 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             // u2
             usb[0] += u2b[0];
             for (int c = 0; c < 3; ++c) {
-                usb[0] += u2b[1 + c] * v2[c];
-                v2b[c] += u2b[1 + c] * us[0];
+                usb[0] = fm(u2b[1 + c], v2[c], usb[0]);
+                v2b[c] = fm(u2b[1 + c], us[0], v2b[c]);
             }
             if (has_energy) {
                 const double sgn = left ? -1.0 : 1.0;   // us4 -/+ (b_sig*sq)*(vbs - vb2)
@@ -597,21 +609,21 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
                 else { alfven_adj(Side<true>{}, 0.5); alfven_adj(Side<false>{}, 0.5); }
                 // vb2 = (v2.b2)
                 for (int c = 0; c < 3; ++c) {
-                    v2b[c] += vb2b * b2[c];
-                    b2b[c] += vb2b * v2[c];
+                    v2b[c] = fm(vb2b, b2[c], v2b[c]);
+                    b2b[c] = fm(vb2b, v2[c], b2b[c]);
                 }
                 // b2[1..2] = ((sql*bsr + sqr*bsl) + bsm*(vsr - vsl))/add
                 double addb = 0.0, bsmb = 0.0;
                 for (int c = 1; c < 3; ++c) {
                     const double nb = b2b[c] * radd;
-                    addb -= nb * b2[c];
-                    sqlb += nb * bsr[c];
-                    bsrb[c] += nb * sql;
-                    sqrb += nb * bsl[c];
-                    bslb[c] += nb * sqr;
-                    bsmb += nb * (vsr[c] - vsl[c]);
-                    vsrb[c] += nb * bsm;
-                    vslb[c] -= nb * bsm;
+                    addb = fm(-nb, b2[c], addb);
+                    sqlb = fm(nb, bsr[c], sqlb);
+                    bsrb[c] = fm(nb, sql, bsrb[c]);
+                    sqrb = fm(nb, bsl[c], sqrb);
+                    bslb[c] = fm(nb, sqr, bslb[c]);
+                    bsmb = fm(nb, vsr[c] - vsl[c], bsmb);
+                    vsrb[c] = fm(nb, bsm, vsrb[c]);
+                    vslb[c] = fm(-nb, bsm, vslb[c]);
                 }
                 // b2[0] = 0.5*(bl0 + br0)
                 blb[0] += 0.5 * b2b[0];
@@ -621,29 +633,29 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
                 // v2[1..2] = ((sql*vsl + sqr*vsr) + b_sig*(bsr - bsl))/add
                 for (int c = 1; c < 3; ++c) {
                     const double nb = v2b[c] * radd;
-                    addb -= nb * v2[c];
-                    sqlb += nb * vsl[c];
-                    vslb[c] += nb * sql;
-                    sqrb += nb * vsr[c];
-                    vsrb[c] += nb * sqr;
-                    bsrb[c] += nb * b_sig;
-                    bslb[c] -= nb * b_sig;
+                    addb = fm(-nb, v2[c], addb);
+                    sqlb = fm(nb, vsl[c], sqlb);
+                    vslb[c] = fm(nb, sql, vslb[c]);
+                    sqrb = fm(nb, vsr[c], sqrb);
+                    vsrb[c] = fm(nb, sqr, vsrb[c]);
+                    bsrb[c] = fm(nb, b_sig, bsrb[c]);
+                    bslb[c] = fm(-nb, b_sig, bslb[c]);
                 }
                 // bsm = b_sig*mul, mul = sql*sqr, add = sql + sqr
                 const double mulb = bsmb * b_sig;
-                sqlb += mulb * sqr + addb;
-                sqrb += mulb * sql + addb;
+                sqlb += fm(mulb, sqr, addb);
+                sqrb += fm(mulb, sql, addb);
             }
             // alfl = sm - |bl0|/sql ; alfr = sm + |br0|/sqr (only the selected branch used them)
             const double rsql = arcp(sql), rsqr = arcp(sqr);
             smb += alflb + alfrb;
-            blb[0] -= alflb * f_sign1(bl[0]) * rsql;
-            sqlb += alflb * fabs(bl[0]) * (rsql * rsql);
-            brb[0] += alfrb * f_sign1(br[0]) * rsqr;
-            sqrb -= alfrb * fabs(br[0]) * (rsqr * rsqr);
+            blb[0] = fm(-alflb * f_sign1(bl[0]), rsql, blb[0]);
+            sqlb = fm(alflb * fabs(bl[0]), rsql * rsql, sqlb);
+            brb[0] = fm(alfrb * f_sign1(br[0]), rsqr, brb[0]);
+            sqrb = fm(-alfrb * fabs(br[0]), rsqr * rsqr, sqrb);
             // sql = sqrt(usl0)
-            uslb[0] += sqlb * 0.5 * rsql;
-            usrb[0] += sqrb * 0.5 * rsqr;
+            uslb[0] = fm(sqlb * 0.5, rsql, uslb[0]);
+            usrb[0] = fm(sqrb * 0.5, rsqr, usrb[0]);
         } else {
             if (sm > 0.0) star_adj(Side<true>{}, 1.0);
             else if (sm < 0.0) star_adj(Side<false>{}, 1.0);
@@ -667,19 +679,17 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             const double pr = left ? prl : prr;
             const double vbs = left ? vbsl : vbsr;
             const double vb = left ? vbl : vbr;
-            if (left) { slvxlb += n4b * en; enlb += n4b * svx; prlb -= n4b * u[1]; vbslb -= n4b * b[0]; }
-            else { srvxrb += n4b * en; enrb += n4b * svx; prrb -= n4b * u[1]; vbsrb -= n4b * b[0]; }
-            ub[1] -= n4b * pr;
-            prtb += n4b * sm;
-            smb += n4b * prt;
-            bb[0] += n4b * (vb - vbs);
+            if (left) { slvxlb = fm(n4b, en, slvxlb); enlb = fm(n4b, svx, enlb); prlb = fm(-n4b, u[1], prlb); vbslb = fm(-n4b, b[0], vbslb); }
+            else { srvxrb = fm(n4b, en, srvxrb); enrb = fm(n4b, svx, enrb); prrb = fm(-n4b, u[1], prrb); vbsrb = fm(-n4b, b[0], vbsrb); }
+            prtb = fm(n4b, sm, prtb);
+            smb = fm(n4b, prt, smb);
             const double vbb = n4b * b[0];                     // vb = (u1*b0 + u2*b1) + u3*b2
-            ub[1] += vbb * b[0];
-            ub[2] += vbb * b[1];
-            ub[3] += vbb * b[2];
-            bb[0] += vbb * u[1];
-            bb[1] += vbb * u[2];
-            bb[2] += vbb * u[3];
+            ub[1] = fm(vbb, b[0], fm(-n4b, pr, ub[1]));
+            ub[2] = fm(vbb, b[1], ub[2]);
+            ub[3] = fm(vbb, b[2], ub[3]);
+            bb[0] = fm(vbb, u[1], fm(n4b, vb - vbs, bb[0]));
+            bb[1] = fm(vbb, u[2], bb[1]);
+            bb[2] = fm(vbb, u[3], bb[2]);
         };
         us4_adj(Side<true>{});
         us4_adj(Side<false>{});
@@ -692,12 +702,12 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             double* vsb = left ? vslb : vsrb;
             const double rssm = left ? rslsm : rsrsm;
             for (int c = 0; c < 3; ++c) {
-                usb[0] += usb[1 + c] * vs[c];
-                vsb[c] += usb[1 + c] * us[0];
+                usb[0] = fm(usb[1 + c], vs[c], usb[0]);
+                vsb[c] = fm(usb[1 + c], us[0], vsb[c]);
             }
             const double t = usb[0] * rssm;
-            if (left) { dn_lb += t; slsmb -= t * us[0]; }
-            else { dn_rb += t; srsmb -= t * us[0]; }
+            if (left) { dn_lb += t; slsmb = fm(-t, us[0], slsmb); }
+            else { dn_rb += t; srsmb = fm(-t, us[0], srsmb); }
         };
         side_part1(Side<true>{});
         side_part1(Side<false>{});
@@ -710,11 +720,11 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             double* vsb = left ? vslb : vsrb;
             double* bsb = left ? bslb : bsrb;
             double* bb = left ? blb : brb;
-            smb += vbsb * bs[0];
-            bb[0] += vbsb * vs[0];
+            smb = fm(vbsb, bs[0], smb);
+            bb[0] = fm(vbsb, vs[0], bb[0]);
             for (int c = 1; c < 3; ++c) {
-                vsb[c] += vbsb * bs[c];
-                bsb[c] += vbsb * vs[c];
+                vsb[c] = fm(vbsb, bs[c], vsb[c]);
+                bsb[c] = fm(vbsb, vs[c], bsb[c]);
             }
             smb += vsb[0];
         };
@@ -734,13 +744,13 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             double kb = 0.0;
             for (int c = 1; c < 3; ++c) {
                 ub[1 + c] += vsb[c];
-                kb += vsb[c] * (b[c] - bs[c]);
-                bb[c] += vsb[c] * k;
-                bsb[c] -= vsb[c] * k;
+                kb = fm(vsb[c], b[c] - bs[c], kb);
+                bb[c] = fm(vsb[c], k, bb[c]);
+                bsb[c] = fm(-vsb[c], k, bsb[c]);
             }
             const double t = kb * rdn;
             bb[0] += t;
-            if (left) dn_lb -= t * k; else dn_rb -= t * k;
+            if (left) dn_lb = fm(-t, k, dn_lb); else dn_rb = fm(-t, k, dn_rb);
         };
         side_part3(Side<true>{});
         side_part3(Side<false>{});
@@ -759,20 +769,20 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
                 double ab = 0.0, coeffb = 0.0;
                 for (int c = 1; c < 3; ++c) {
                     const double t = bsb[c] * rc;
-                    bb[c] += t * a;
-                    ab += t * b[c];
-                    coeffb -= t * bs[c];
+                    bb[c] = fm(t, a, bb[c]);
+                    ab = fm(t, b[c], ab);
+                    coeffb = fm(-t, bs[c], coeffb);
                 }
                 // a = dn*svx - b_lr ; coeff = dn*ssm - b_lr
                 const double svx = left ? slvxl : srvxr;
                 const double ssm = left ? slsm : srsm;
                 const double dn = left ? dn_l : dn_r;
-                const double dnb = ab * svx + coeffb * ssm;
-                if (left) { dn_lb += dnb; slvxlb += ab * dn; slsmb += coeffb * dn; }
-                else { dn_rb += dnb; srvxrb += ab * dn; srsmb += coeffb * dn; }
+                const double dnb = fm(ab, svx, coeffb * ssm);
+                if (left) { dn_lb += dnb; slvxlb = fm(ab, dn, slvxlb); slsmb = fm(coeffb, dn, slsmb); }
+                else { dn_rb += dnb; srvxrb = fm(ab, dn, srvxrb); srsmb = fm(coeffb, dn, srsmb); }
                 const double blrb = -ab - coeffb;
-                blb[0] += blrb * br[0];
-                brb[0] += blrb * bl[0];
+                blb[0] = fm(blrb, br[0], blb[0]);
+                brb[0] = fm(blrb, bl[0], brb[0]);
             } else {
                 hll1b += bsb[1];
                 hll2b += bsb[2];
@@ -786,36 +796,34 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             const double hv[3] = {0.0, hll1, hll2};
             for (int c = 1; c < 3; ++c) {
                 const double nb = hb[c] * rsrmsl;
-                srmslb -= nb * hv[c];
-                srb += nb * br[c];
-                brb[c] += nb * sr;
-                slb -= nb * bl[c];
-                blb[c] -= nb * sl;
+                srmslb = fm(-nb, hv[c], srmslb);
+                srb = fm(nb, br[c], srb);
+                slb = fm(-nb, bl[c], slb);
                 // -(bcrf_c - bclf_c); bcf_c = b_c*u1 - b0*u_{1+c}
-                const double fr_b = -nb, fl_b = nb;
-                brb[c] += fr_b * ur[1];
-                urb[1] += fr_b * br[c];
-                brb[0] -= fr_b * ur[1 + c];
-                urb[1 + c] -= fr_b * br[0];
-                blb[c] += fl_b * ul[1];
-                ulb[1] += fl_b * bl[c];
-                blb[0] -= fl_b * ul[1 + c];
-                ulb[1 + c] -= fl_b * bl[0];
+                brb[c] = fm(nb, sr - ur[1], brb[c]);
+                urb[1] = fm(-nb, br[c], urb[1]);
+                brb[0] = fm(nb, ur[1 + c], brb[0]);
+                urb[1 + c] = fm(nb, br[0], urb[1 + c]);
+                blb[c] = fm(nb, ul[1] - sl, blb[c]);
+                ulb[1] = fm(nb, bl[c], ulb[1]);
+                blb[0] = fm(-nb, ul[1 + c], blb[0]);
+                ulb[1 + c] = fm(-nb, bl[0], ulb[1 + c]);
             }
         }
         // prt = 0.5*((prl + dn_l*(sm - ul1)) + (prr + dn_r*(sm - ur1)))
-        prlb += 0.5 * prtb;
-        prrb += 0.5 * prtb;
-        dn_lb += 0.5 * prtb * (sm - ul[1]);
-        dn_rb += 0.5 * prtb * (sm - ur[1]);
-        smb += 0.5 * prtb * (dn_l + dn_r);
-        ulb[1] -= 0.5 * prtb * dn_l;
-        urb[1] -= 0.5 * prtb * dn_r;
+        const double hp = 0.5 * prtb;
+        prlb += hp;
+        prrb += hp;
+        dn_lb = fm(hp, sm - ul[1], dn_lb);
+        dn_rb = fm(hp, sm - ur[1], dn_rb);
+        smb = fm(hp, dn_l + dn_r, smb);
+        ulb[1] = fm(-hp, dn_l, ulb[1]);
+        urb[1] = fm(-hp, dn_r, urb[1]);
         // dn = u0*svx
-        ulb[0] += dn_lb * slvxl;
-        slvxlb += dn_lb * ul[0];
-        urb[0] += dn_rb * srvxr;
-        srvxrb += dn_rb * ur[0];
+        ulb[0] = fm(dn_lb, slvxl, ulb[0]);
+        slvxlb = fm(dn_lb, ul[0], slvxlb);
+        urb[0] = fm(dn_rb, srvxr, urb[0]);
+        srvxrb = fm(dn_rb, ur[0], srvxrb);
         // speed differences
         slb += slvxlb + slsmb - srmslb;
         ulb[1] -= slvxlb;
@@ -829,20 +837,20 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
             srb += smb / 2.0;
         } else {
             const double rden = arcp(den);
-            const double numb = smb * rden, denb = -smb * sm * rden;
-            auxrb += numb * ur[1] + denb;
-            urb[1] += numb * auxr;
+            const double numb = smb * rden, denb = -numb * sm;
+            auxrb = fm(numb, ur[1], denb);
+            urb[1] = fm(numb, auxr, urb[1]);
             prrb -= numb;
-            auxlb += -numb * ul[1] - denb;
-            ulb[1] -= numb * auxl;
+            auxlb = fm(-numb, ul[1], -denb);
+            ulb[1] = fm(-numb, auxl, ulb[1]);
             prlb += numb;
         }
-        srb += auxrb * ur[0];
-        urb[1] -= auxrb * ur[0];
-        urb[0] += auxrb * (sr - ur[1]);
-        slb += auxlb * ul[0];
-        ulb[1] -= auxlb * ul[0];
-        ulb[0] += auxlb * (sl - ul[1]);
+        srb = fm(auxrb, ur[0], srb);
+        urb[1] = fm(-auxrb, ur[0], urb[1]);
+        urb[0] = fm(auxrb, sr - ur[1], urb[0]);
+        slb = fm(auxlb, ul[0], slb);
+        ulb[1] = fm(-auxlb, ul[0], ulb[1]);
+        ulb[0] = fm(auxlb, sl - ul[1], ulb[0]);
     }
     // sl, sr
     if (minr) urb[1] += slb; else ulb[1] += slb;
@@ -863,18 +871,18 @@ PK_PHYS void hlld_adj(bool has_energy, double gamma, const double* ul, const dou
                 const double root = right ? rootr : rootl;
                 const double gp = right ? gpr : gpl;
                 const double numb = cmb * arcp(u[0]);
-                ub[0] -= numb * c;
+                ub[0] = fm(-numb, c, ub[0]);
                 double abb = numb, rootb = numb;
                 double gpb = 0.0;
                 if (root > 0.0) {
                     const double rb = rootb * 0.5 * arcp(root);   // d(root^2)
-                    abb += rb * 2.0 * a;
-                    gpb += -rb * 4.0 * (b[0] * b[0]);
-                    bb[0] += -rb * (4.0 * gp) * 2.0 * b[0];
+                    abb = fm(rb * 2.0, a, abb);
+                    gpb = -rb * 4.0 * (b[0] * b[0]);
+                    bb[0] = fm(-rb * (4.0 * gp) * 2.0, b[0], bb[0]);
                 }
                 gpb += abb;                                    // a = gp + bb
-                for (int k = 0; k < 3; ++k) bb[k] += abb * 2.0 * b[k];
-                ub[4] += gpb * gamma;
+                for (int k = 0; k < 3; ++k) bb[k] = fm(abb * 2.0, b[k], bb[k]);
+                ub[4] = fm(gpb, gamma, ub[4]);
             };
             if (cr > cl) cf_adj(Side<true>{});
             else cf_adj(Side<false>{});

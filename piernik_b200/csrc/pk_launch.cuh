@@ -262,13 +262,15 @@ int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
 // Launch-bound variants of the two adjoint kernels (threads per CTA, CTAs per SM)
 constexpr int NADJ_VARIANT = 5;
 constexpr int ADJ_T[NADJ_VARIANT] = {256, 256, 192, 128, 128};
-// defaults, measured on B200 (MHD, 128^3 and 256^3) over variants x owned
-// lengths: the 128-register variant (spilling) beats every variant with more
-// registers; the whole periodic pencil without halo beats 8 pencils x 26 + 6
-// halo cells along x always (256^3: 29.9 vs 35.3 ms per adjoint sweep) and
-// along y and z while at least two pencils share the CTA (128^3: 3.97 vs
-// 4.23 ms), but not with one pencil per CTA (256^3 y: 34.7 vs 31.8 ms)
-constexpr int DEF_ADJ_V[3] = {1, 1, 1};
+// defaults, measured on B200 (MHD, 256^3) over variants x owned lengths: the
+// unspilled 255-register variant is the fastest or within 1% of it along
+// every axis (x 16.2, y 19.0, z 19.3 ms per adjoint sweep; the spilling
+// 128-register variant 17.2, 19.0, 19.4); the whole periodic pencil without
+// halo beats 8 pencils x 26 + 6 halo cells along x (16.2 vs 18.9 ms) and
+// along y and z while at least two pencils share the CTA, but not with one
+// pencil per CTA (256^3 y: 33.5 ms for 250-cell chunks), and longer chunks
+// lose coalescing (58 cells, 4 pencils: 19.4 ms along y)
+constexpr int DEF_ADJ_V[3] = {0, 0, 0};
 constexpr int DEF_ADJ_CHUNK = 26;
 
 inline int default_adj_length(int dir, int n, int threads)
