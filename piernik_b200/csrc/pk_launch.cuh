@@ -185,7 +185,7 @@ int launch_fused_ptr(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
         const int threads = (b.n[dir] + 31) / 32 * 32;
         if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
         k_sweep_staged<PH, FAST><<<grid, threads, staged_smem(PH::NV, b.n[dir]), h->stream>>>(
-            tin, tout, g, h->pp, b.dl[dir], h->d_step, apply_fac, dir, h->d_status);
+            tin, tout, g, h->pp, b.dl[dir], h->d_step, apply_fac, dir, h->d_status, nullptr, nullptr);
     } else {
         const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
         if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
@@ -227,7 +227,8 @@ RecFn<PH> rec_variant(int v)
 }
 
 // The forward sweep of the backward pass's recomputation, in the forward
-// sweep's tile and variant: also stores U* and the floor records
+// sweep's tile and variant (the TMA-staged kernel where the forward's tile is
+// the staged one): also stores U* and the floor records
 template <class PH>
 int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out, double* ustar,
                      unsigned short* flags)
@@ -240,18 +241,31 @@ int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
             for (int v = 0; v < NVARIANT; ++v)
                 PK_CUDA(h, cudaFuncSetAttribute(rec_variant<PH>(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 220 * 1024));
+            PK_CUDA(h, cudaFuncSetAttribute(k_sweep_staged<PH, false, true>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
             attr = true;
         }
         Geom g = make_geom(b, dir);
         Tile tl;
         dim3 grid;
         int var;
-        if (int rc = fused_geometry(h, b, dir, g, &tl, &grid, &var)) return rc;
-        const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+        if (int rc = fused_geometry(h, b, dir, g, &tl, &grid, &var, true)) return rc;
         std::pair<cudaEvent_t, cudaEvent_t> ev;
-        if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-        rec_variant<PH>(var)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, ustar, flags, h->pp, b.dl[dir],
-                                                                    h->d_step, apply_fac, h->d_status);
+        if (var == VAR_STAGED) {
+            CUtensorMap tin, tout;
+            if (!encode_state_map(&tin, in, b.n, b.ext, b.plane, PH::NV, dir) ||
+                !encode_state_map(&tout, out, b.n, b.ext, b.plane, PH::NV, dir))
+                return fail(h, PK_E_CUDA, "cuTensorMapEncodeTiled failed for the staged sweep");
+            const int threads = (b.n[dir] + 31) / 32 * 32;
+            if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+            k_sweep_staged<PH, false, true><<<grid, threads, staged_smem(PH::NV, b.n[dir]), h->stream>>>(
+                tin, tout, g, h->pp, b.dl[dir], h->d_step, apply_fac, dir, h->d_status, ustar, flags);
+        } else {
+            const size_t smem = 3ull * PH::NV * tl.P * tl.T * sizeof(double);
+            if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+            rec_variant<PH>(var)<<<grid, tl.P * tl.T, smem, h->stream>>>(g, tl, in, out, ustar, flags, h->pp,
+                                                                        b.dl[dir], h->d_step, apply_fac, h->d_status);
+        }
         PK_CUDA(h, cudaGetLastError());
         if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
         h->launches += 1;

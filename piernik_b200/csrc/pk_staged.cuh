@@ -23,6 +23,11 @@
 // reconstruction.  Shared memory: 2n planes-worth of doubles for the box plus
 // the three n-cell planes of the tile per component.
 //
+// REC (the backward pass's recomputation, bit-exact arithmetic only): also
+// store each cell's stage-1 state in ustar and its floor records in flags, as
+// k_sweep_fused_rec does; these go out with plain stores at the cell's own
+// offset.
+//
 // The wait for the load is bounded: a CTA that gives up raises
 // PK_ST_TIMEOUT in the status word and returns without touching the output.
 #pragma once
@@ -82,12 +87,14 @@ PK_DEV void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" 
 // ---------------------------------------------------------------------------
 // grid: x = pairs of pencils along ortho-1, y = 1, z = ortho-2; blockDim.x >= n
 // ---------------------------------------------------------------------------
-template <class PH, bool FAST = false>
+template <class PH, bool FAST = false, bool REC = false>
 __global__ void __launch_bounds__(256, 2) k_sweep_staged(const __grid_constant__ CUtensorMap tin,
                                                          const __grid_constant__ CUtensorMap tout, Geom g,
                                                          PhysParams pp, double dl, const StepParams* __restrict__ sp,
-                                                         int apply_fac, int dir, unsigned* __restrict__ gstatus)
+                                                         int apply_fac, int dir, unsigned* __restrict__ gstatus,
+                                                         double* __restrict__ ustar, unsigned short* __restrict__ flags)
 {
+    static_assert(!(REC && FAST), "the recording sweep runs in the bit-exact arithmetic");
     constexpr int NV = PH::NV;
     extern __shared__ __align__(128) double smem[];
     const int n = g.n_d;
@@ -143,15 +150,30 @@ __global__ void __launch_bounds__(256, 2) k_sweep_staged(const __grid_constant__
         r.end = 0;
         r.keep = false;
         r.q = r.slope = r.flux = r.upd = active;
+        // the cell's offset in the block (REC's plain stores)
+        const long long off = (long long)(g.g_d + t) * g.sd + (long long)(g.g1 + i1_0 + p) * g.s1 +
+                              (long long)(g.g2 + i2) * g.s2;
+        FloorRec rec1{0, 0}, rec2{0, 0};
 #pragma unroll 1
-        for (int s = 0; s < 2; ++s)
-            rk_stage<PH, false, false, false, FAST, true>(sm, t, mp, mn, r, w, nullptr, nullptr, 0, g,
-                                                          s == 0 ? dtodx1 : dtodx2, ch, pp, status, nullptr, nullptr,
-                                                          nullptr, mine, 2 * n);
+        for (int s = 0; s < 2; ++s) {
+            FloorRec rec{0, 0};
+            rk_stage<PH, REC, false, false, FAST, true>(sm, t, mp, mn, r, w, nullptr, nullptr, 0, g,
+                                                        s == 0 ? dtodx1 : dtodx2, ch, pp, status, &rec, nullptr,
+                                                        nullptr, mine, 2 * n);
+            if constexpr (REC) {
+                if (s == 0) {
+                    rec1 = rec;
+                    if (active) store_cell<PH>(ustar, off, g, w);
+                } else {
+                    rec2 = rec;
+                }
+            }
+        }
         if (active) {
             if (PH::MHD) w[PH::IB + 3] = w[PH::IB + 3] * psi_fac;   // glmdamping fused into the last sweep
 #pragma unroll
             for (int v = 0; v < NV; ++v) mine[plane_of<PH>(v, perm) * 2 * n] = w[v];
+            if constexpr (REC) flags[off] = pack_floors(rec1, rec2);
         }
     }
     fence_proxy_async();
