@@ -442,7 +442,9 @@ int pk_grad_backward(pk_handle h);
 int pk_grad_release(pk_handle h);
 
 /* Tile of the adjoint sweep kernels along dir (0..2, -1: all): owned cells
- * per pencil (0: default) and launch-bound variant (-1: default). */
+ * per pencil (0: default) and launch-bound variant (-1: default; 0..4 tiled
+ * variants; 5 the TMA-staged whole-pencil kernels, which fall back to variant
+ * 0 where the block does not allow them). */
 int pk_set_adjoint_tile(pk_handle h, int32_t dir, int32_t length, int32_t variant);
 
 /* ---- Measurement utility ----

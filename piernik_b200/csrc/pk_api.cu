@@ -2729,8 +2729,8 @@ int pk_set_stage_variant(pk_handle h, int32_t variant)
 int pk_set_adjoint_tile(pk_handle h, int32_t dir, int32_t length, int32_t variant)
 {
     if (!h) return PK_E_ARG;
-    if (dir < -1 || dir > 2 || length < 0 || length > 256 || variant < -1 || variant > 4)
-        return fail(h, PK_E_ARG, "adjoint tile: dir -1..2, length 0..256, variant -1..4");
+    if (dir < -1 || dir > 2 || length < 0 || length > 256 || variant < -1 || variant > 5)
+        return fail(h, PK_E_ARG, "adjoint tile: dir -1..2, length 0..256, variant -1..5");
     for (int d = 0; d < 3; ++d)
         if (dir < 0 || dir == d) {
             h->adjL[d] = length;

@@ -273,18 +273,24 @@ int launch_fused_rec(pk_ctx* h, Block& b, int dir, int apply_fac, const double* 
     }
 }
 
-// Launch-bound variants of the two adjoint kernels (threads per CTA, CTAs per SM)
-constexpr int NADJ_VARIANT = 5;
-constexpr int ADJ_T[NADJ_VARIANT] = {256, 256, 192, 128, 128};
-// defaults, measured on B200 (MHD, 256^3) over variants x owned lengths: the
-// unspilled 255-register variant is the fastest or within 1% of it along
-// every axis (x 16.2, y 19.0, z 19.3 ms per adjoint sweep; the spilling
-// 128-register variant 17.2, 19.0, 19.4); the whole periodic pencil without
-// halo beats 8 pencils x 26 + 6 halo cells along x (16.2 vs 18.9 ms) and
-// along y and z while at least two pencils share the CTA, but not with one
-// pencil per CTA (256^3 y: 33.5 ms for 250-cell chunks), and longer chunks
-// lose coalescing (58 cells, 4 pencils: 19.4 ms along y)
-constexpr int DEF_ADJ_V[3] = {0, 0, 0};
+// Launch-bound variants of the two adjoint kernels (threads per CTA, CTAs per
+// SM); variant ADJ_VAR_STAGED is the TMA-staged whole-pencil pair
+// (k_adj_staged2 / k_adj_staged1: two pencils per CTA, n <= 256 and the
+// staged forward kernel's alignment conditions; elsewhere variant 0)
+constexpr int NADJ_VARIANT = 6;
+constexpr int ADJ_VAR_STAGED = 5;
+constexpr int ADJ_T[NADJ_VARIANT] = {256, 256, 192, 128, 128, 256};
+// defaults, measured on B200 (MHD, 256^3, adjoint sweep = staged recording
+// sweep + the two adjoint kernels): the staged pair 11.2 / 13.8 / 14.5 ms
+// along x / y / z against 12.5 / 15.8 / 16.2 for the best tiled variant.
+// Among the tiled variants (where the staged pair does not apply) the
+// unspilled 255-register variant 0 is the fastest or within 1 % of it on
+// every axis; the whole periodic pencil without halo beats 8 pencils x 26 + 6
+// halo cells along x and along y and z while at least two pencils share the
+// CTA, but not with one pencil per CTA (250-cell chunks along y: 33.5 ms
+// against 19.0), and chunks that do not divide the pencil waste their last
+// tile (58 cells: 19.4 ms along y)
+constexpr int DEF_ADJ_V[3] = {ADJ_VAR_STAGED, ADJ_VAR_STAGED, ADJ_VAR_STAGED};
 constexpr int DEF_ADJ_CHUNK = 26;
 
 inline int default_adj_length(int dir, int n, int threads)
@@ -323,15 +329,43 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
     } else {
         static bool attr = false;
         if (!attr) {
-            for (int v = 0; v < NADJ_VARIANT; ++v) {
+            for (int v = 0; v < ADJ_VAR_STAGED; ++v) {
                 const AdjKernels<PH> k = adj_variant<PH>(v);
                 PK_CUDA(h, cudaFuncSetAttribute(k.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
                 PK_CUDA(h, cudaFuncSetAttribute(k.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
             }
+            PK_CUDA(h, cudaFuncSetAttribute(k_adj_staged2<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            PK_CUDA(h, cudaFuncSetAttribute(k_adj_staged1<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
             attr = true;
         }
-        const int var = (h->adjV[dir] >= 0 && h->adjV[dir] < NADJ_VARIANT) ? h->adjV[dir] : DEF_ADJ_V[dir];
+        int var = (h->adjV[dir] >= 0 && h->adjV[dir] < NADJ_VARIANT) ? h->adjV[dir] : DEF_ADJ_V[dir];
         Geom g = make_geom(b, dir);
+        if (var == ADJ_VAR_STAGED) {
+            if (staged_ok(b.n, b.g, b.ext, h->nplanes, dir, g.seg_len)) {
+                CUtensorMap m_ustar, m_lamout, m_lamin, m_m1, m_uin;
+                if (!encode_state_map(&m_ustar, ustar, b.n, b.ext, b.plane, PH::NV, dir) ||
+                    !encode_state_map(&m_lamout, lam_out, b.n, b.ext, b.plane, PH::NV, dir) ||
+                    !encode_state_map(&m_lamin, lam_in, b.n, b.ext, b.plane, PH::NV, dir) ||
+                    !encode_state_map(&m_m1, m1, b.n, b.ext, b.plane, PH::NV, dir) ||
+                    !encode_state_map(&m_uin, uin, b.n, b.ext, b.plane, PH::NV, dir))
+                    return fail(h, PK_E_CUDA, "cuTensorMapEncodeTiled failed for the staged adjoint sweep");
+                const int threads = (b.n[dir] + 31) / 32 * 32;
+                const dim3 grid((g.n1 + 1) / 2, 1, g.n2);
+                std::pair<cudaEvent_t, cudaEvent_t> ev;
+                if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+                k_adj_staged2<PH><<<grid, threads, adj_staged_smem(PH::NV, b.n[dir], 2), h->stream>>>(
+                    m_ustar, m_lamout, m_lamin, m_m1, g, uout, flags, h->pp, b.dl[dir], h->d_step, apply_fac, dir,
+                    h->d_status);
+                PK_CUDA(h, cudaGetLastError());
+                k_adj_staged1<PH><<<grid, threads, adj_staged_smem(PH::NV, b.n[dir], 1), h->stream>>>(
+                    m_uin, m_m1, m_lamin, g, h->pp, h->d_step, dir, h->d_status);
+                PK_CUDA(h, cudaGetLastError());
+                if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+                h->launches += 2;
+                return PK_OK;
+            }
+            var = 0;                                  // not stageable here: the tiled default
+        }
         Tile tl;
         int L = h->adjL[dir] > 0 ? h->adjL[dir] : default_adj_length(dir, b.n[dir], ADJ_T[var]);
         if (L > b.n[dir]) L = b.n[dir];
