@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256, 1) k_adj_staged2(const __grid_constant__ 
     Geom gb = g;                        // the boxes as component planes of 2n cells
     gb.plane = 2 * n;
     const int st_t = dir == 0 ? 1 : 2, st_p = dir == 0 ? n : 1;
-    const StepParams stp = sp[0];
+    const StepParams stp = sp[g.seg_len ? i2 / g.seg_len : 0];   // stacked instances: this CTA's
     const double dt = stp.dt, ch = stp.ch, fac = apply_fac ? stp.psi_fac : 1.0;
     const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
     const int t = threadIdx.x;
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(256, 1) k_adj_staged1(const __grid_constant__ 
     Geom gb = g;
     gb.plane = 2 * n;
     const int st_t = dir == 0 ? 1 : 2, st_p = dir == 0 ? n : 1;
-    const double ch = sp[0].ch;
+    const double ch = sp[g.seg_len ? i2 / g.seg_len : 0].ch;
     const int t = threadIdx.x;
     const int mp = t == 0 ? n - 1 : t - 1, mn = t == n - 1 ? 0 : t + 1;
 #pragma unroll 1

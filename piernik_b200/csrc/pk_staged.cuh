@@ -17,7 +17,8 @@
 // bit (or, in the tolerance mode, the other tolerance-mode kernels).
 //
 // Requirements (checked on the host before the launch): a single periodic
-// block read with wrap (not connected, no stacked instances), n <= 256 along
+// block read with wrap (not connected; stacked instances only along x and y,
+// each CTA taking its instance's step scalars), n <= 256 along
 // the sweep, an even x extent and an even x guard width (the box's x
 // coordinate and the tensor strides must be multiples of 16 bytes), linear
 // reconstruction.  Shared memory: 2n planes-worth of doubles for the box plus
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_staged(const __grid_constant__
         return;
     }
 
-    const StepParams stp = sp[0];
+    const StepParams stp = sp[g.seg_len ? i2 / g.seg_len : 0];   // stacked instances: this CTA's
     const double dtodx1 = (0.5 * stp.dt) / dl;           // rk_coef(RK2_1) * dt / cg%dl(ddim)
     const double dtodx2 = (1.0 * stp.dt) / dl;           // rk_coef(RK2_2) * dt / cg%dl(ddim)
     const double ch = stp.ch, psi_fac = apply_fac ? stp.psi_fac : 1.0;
@@ -208,7 +209,9 @@ inline EncodeTiledFn encode_tiled_fn()
 // whether the staged kernel can sweep block b along dir (see the requirements above)
 inline bool staged_ok(const int n[3], const int g[3], const int ext[3], int nplanes, int dir, int seg_len)
 {
-    if (seg_len || n[dir] > 256 || n[dir] < 2 || nplanes > 256) return false;
+    // stacked instances (along z) are staged along x and y, where a pencil
+    // stays inside one instance; along z a pencil would cross them
+    if ((seg_len && dir == 2) || n[dir] > 256 || n[dir] < 2 || nplanes > 256) return false;
     if ((ext[0] & 1) || (g[0] & 1)) return false;        // 16-byte strides and x coordinates
     if (dir == 0 && (n[0] & 1)) return false;            // the box's x rows: 16-byte multiples
     return encode_tiled_fn() != nullptr;
