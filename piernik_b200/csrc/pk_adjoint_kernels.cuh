@@ -275,44 +275,49 @@ __global__ void __launch_bounds__(MAXT, MINB) k_adj_stage1(Geom g, Tile tl, cons
 }
 
 // ---------------------------------------------------------------------------
-// TMA-staged whole-pencil adjoint kernels.  As k_sweep_staged: a CTA owns two
+// TMA-staged whole-pencil adjoint kernels.  As in k_sweep_staged a tile is two
 // neighbouring pencils, whole along the sweep (n <= 256, periodic, no halo),
-// and one thread loads the boxes [2 pencils x n cells x NV planes] of its
-// inputs with cp.async.bulk.tensor on one mbarrier (a bounded wait); the CTA
-// then runs the pencils one after the other through the same per-cell code as
-// k_adj_stage2 / k_adj_stage1 (adj_divergence over a circular tile), reading
-// its inputs from the boxes (a Geom whose plane stride is the box's 2n), and
-// writes each cell's results into the box slots it alone read; TMA stores
-// write the boxes out.  The rarely needed sweep output (energy floors) and
-// the floor records are plain loads at the cell's offset in the block.
-// Results equal the tiled kernels' bit for bit.
+// run one after the other through the same per-cell code as k_adj_stage2 /
+// k_adj_stage1 (adj_divergence over a circular tile) with the inputs read from
+// shared-memory boxes [2 pencils x n cells x NV planes] (a Geom whose plane
+// stride is the box's 2n).  The kernels are persistent, one 256-thread CTA per
+// SM (the Riemann adjoint takes 255 registers) walking the tiles with stride
+// gridDim.x, and the input boxes are double-buffered: thread 0 issues the
+// cp.async.bulk.tensor loads of the next tile into the other buffer while the
+// CTA computes the current one, so the gather of the y/z boxes' 16-byte rows
+// is not waited for.  Each buffer has its own mbarrier (bounded waits:
+// PK_ST_TIMEOUT after 2^24 polls).  Results equal the tiled kernels' bit for
+// bit.
 // ---------------------------------------------------------------------------
 
-// mbarrier of the staged adjoint kernels: initialised by thread 0 and made
-// visible to the TMA engine before any load is issued
-PK_DEV void adj_bar_init(unsigned long long* bar)
+PK_DEV void adj_bars_init(unsigned long long* bars)
 {
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
+        mbar_init(bars, 1);
+        mbar_init(bars + 1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         fence_proxy_async();
     }
     __syncthreads();
 }
 
-// bounded wait for the boxes' bytes; false (for every thread) if it gave up
-PK_DEV bool adj_bar_wait(unsigned long long* bar)
+// bounded wait for phase `parity` of bar; false (for every thread) if it gave up
+PK_DEV bool adj_bar_wait(unsigned long long* bar, unsigned parity)
 {
     bool ready = false;
-    for (int it = 0; it < (1 << 24) && !ready; ++it) ready = mbar_try_wait(bar, 0);
+    for (int it = 0; it < (1 << 24) && !ready; ++it) ready = mbar_try_wait(bar, parity);
     return __syncthreads_and(ready) != 0;
 }
 
 // doubles per box, rounded up to 128 bytes (each box starts 128-byte aligned)
 PK_PHYS int adj_box_doubles(int nv, int n) { return (2 * nv * n + 15) / 16 * 16; }
 
-PK_DEV void adj_box_coords(const Geom& g, int dir, int i1_0, int i2, int (&c)[4])
+// tile tau: pencil pair (2 * (tau % npair), +1) along ortho-1 at ortho-2 index
+// tau / npair; c = the box's tensor coordinates (x, y, z, plane)
+PK_DEV void adj_tile(const Geom& g, int dir, int tau, int npair, int& i1_0, int& i2, int (&c)[4])
 {
+    i1_0 = 2 * (tau % npair);
+    i2 = tau / npair;
     const int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;
     c[dir] = g.g_d;
     c[o1] = g.g1 + i1_0;
@@ -320,10 +325,12 @@ PK_DEV void adj_box_coords(const Geom& g, int dir, int i1_0, int i2, int (&c)[4]
     c[3] = 0;
 }
 
-// grid: x = pairs of pencils along ortho-1, z = ortho-2; blockDim.x >= n.
-// Shared memory: boxes U* (then m1) and lam'' (then lam_acc), 2 NV n doubles
-// each (rounded up to 128 bytes), the four planes of the tile (4 NV n), the
-// mbarrier.
+// Stage 2.  Buffer b holds the boxes U* (then m1) and lam'' (then lam_acc);
+// each cell's results go into the box slots only it read and TMA stores write
+// both boxes out; the next tile's loads into the other buffer wait for the
+// previous tile's stores to have read it (issued between the two pencils).
+// Shared memory: 2 buffers x 2 boxes of 2 NV n doubles (each rounded up to
+// 128 bytes), the four planes of the tile (4 NV n), two mbarriers.
 template <class PH>
 __global__ void __launch_bounds__(256, 1) k_adj_staged2(const __grid_constant__ CUtensorMap t_ustar,
                                                         const __grid_constant__ CUtensorMap t_lamout,
@@ -338,113 +345,220 @@ __global__ void __launch_bounds__(256, 1) k_adj_staged2(const __grid_constant__ 
     extern __shared__ __align__(128) double smem[];
     const int n = g.n_d;
     const int bd = adj_box_doubles(NV, n);
-    double* bv = smem;                  // U*, then m1
-    double* bl = smem + bd;             // lam'', then lam_acc
-    double* pl = smem + 2 * bd;
+    double* pl = smem + 4 * bd;
     const AdjSmem asm_{pl, pl + NV * n, pl + 2 * NV * n, pl + 3 * NV * n, n};
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(pl + 4 * NV * n);
-    const int i1_0 = 2 * blockIdx.x, i2 = blockIdx.z;
-    int c[4];
-    adj_box_coords(g, dir, i1_0, i2, c);
-    adj_bar_init(bar);
-    if (threadIdx.x == 0) {
-        mbar_expect_tx(bar, (unsigned)(2 * (2 * NV * n * sizeof(double))));
-        tma_load_4d(bv, &t_ustar, c[0], c[1], c[2], c[3], bar);
-        tma_load_4d(bl, &t_lamout, c[0], c[1], c[2], c[3], bar);
-    }
-    if (!adj_bar_wait(bar)) {
-        if (threadIdx.x == 0) atomicOr(gstatus, ST_TIMEOUT);
-        return;
-    }
-    Geom gb = g;                        // the boxes as component planes of 2n cells
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(pl + 4 * NV * n);
+    const int npair = (g.n1 + 1) / 2, ntiles = npair * g.n2, G = (int)gridDim.x;
+    const unsigned bytes = (unsigned)(2 * (2 * NV * n * sizeof(double)));
+    auto issue = [&](int tau, int b) {                   // thread 0: the tile's input boxes into buffer b
+        int i1, j2, c[4];
+        adj_tile(g, dir, tau, npair, i1, j2, c);
+        mbar_expect_tx(bars + b, bytes);
+        tma_load_4d(smem + 2 * b * bd, &t_ustar, c[0], c[1], c[2], c[3], bars + b);
+        tma_load_4d(smem + (2 * b + 1) * bd, &t_lamout, c[0], c[1], c[2], c[3], bars + b);
+    };
+    adj_bars_init(bars);
+    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    Geom gb = g;                                         // the boxes as component planes of 2n cells
     gb.plane = 2 * n;
     const int st_t = dir == 0 ? 1 : 2, st_p = dir == 0 ? n : 1;
-    const StepParams stp = sp[g.seg_len ? i2 / g.seg_len : 0];   // stacked instances: this CTA's
-    const double dt = stp.dt, ch = stp.ch, fac = apply_fac ? stp.psi_fac : 1.0;
-    const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
     const int t = threadIdx.x;
     const int mp = t == 0 ? n - 1 : t - 1, mn = t == n - 1 ? 0 : t + 1;
+    int k = 0;
+    for (int tau = blockIdx.x; tau < ntiles; tau += G, ++k) {
+        const int b = k & 1;
+        if (!adj_bar_wait(bars + b, (unsigned)((k >> 1) & 1))) {
+            if (threadIdx.x == 0) {
+                atomicOr(gstatus, ST_TIMEOUT);
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+            }
+            return;
+        }
+        double* bv = smem + 2 * b * bd;                  // U*, then m1
+        double* bl = bv + bd;                            // lam'', then lam_acc
+        int i1_0, i2, c[4];
+        adj_tile(g, dir, tau, npair, i1_0, i2, c);
+        const StepParams stp = sp[g.seg_len ? i2 / g.seg_len : 0];   // stacked instances: this tile's
+        const double dt = stp.dt, ch = stp.ch, fac = apply_fac ? stp.psi_fac : 1.0;
+        const double c1 = (0.5 * dt) / dl, c2 = (1.0 * dt) / dl;
 #pragma unroll 1
-    for (int p = 0; p < 2; ++p) {
-        if (i1_0 + p >= g.n1) break;                     // the same for the whole CTA
-        const bool active = t < n;
-        const int slot = active ? t * st_t + p * st_p : 0;
-        const long long goff = (long long)(g.g_d + (active ? t : 0)) * g.sd + (long long)(g.g1 + i1_0 + p) * g.s1 +
-                               (long long)(g.g2 + i2) * g.s2;
-        const unsigned short fl = active ? flags[goff] : (unsigned short)0;
-        auto mu2_of = [&](double (&m)[NV]) {
-            load_cell<PH>(bl, slot, gb, m);
-            if (PH::MHD) m[PH::IB + 3] = m[PH::IB + 3] * fac;
-            const FloorRec r2 = unpack_floors(fl, 2);
-            if (r2.en || r2.dn) {
-                double w[NV];
-                load_cell<PH>(uout, goff, g, w);
-                floors_adj<PH>(w, r2, m);
+        for (int p = 0; p < 2; ++p) {
+            if (p == 1 && threadIdx.x == 0 && tau + G < ntiles) {
+                // the other buffer held the previous tile: its stores must have read it
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                issue(tau + G, b ^ 1);
             }
-        };
-        double mu[NV];
+            if (i1_0 + p >= g.n1) break;                 // the same for the whole CTA
+            const bool active = t < n;
+            const int slot = active ? t * st_t + p * st_p : 0;
+            const long long goff = (long long)(g.g_d + (active ? t : 0)) * g.sd +
+                                   (long long)(g.g1 + i1_0 + p) * g.s1 + (long long)(g.g2 + i2) * g.s2;
+            const unsigned short fl = active ? flags[goff] : (unsigned short)0;
+            auto mu2_of = [&](double (&m)[NV]) {
+                load_cell<PH>(bl, slot, gb, m);
+                if (PH::MHD) m[PH::IB + 3] = m[PH::IB + 3] * fac;
+                const FloorRec r2 = unpack_floors(fl, 2);
+                if (r2.en || r2.dn) {
+                    double w[NV];
+                    load_cell<PH>(uout, goff, g, w);
+                    floors_adj<PH>(w, r2, m);
+                }
+            };
+            double mu[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) mu[v] = 0.0;
-        if (active) {
-            mu2_of(mu);
+            for (int v = 0; v < NV; ++v) mu[v] = 0.0;
+            if (active) {
+                mu2_of(mu);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) mu[v] = c2 * mu[v];
+                for (int v = 0; v < NV; ++v) mu[v] = c2 * mu[v];
+            }
+            double rho[NV];
+            adj_divergence<PH>(asm_, t, mp, mn, true, t, active, 0, n, 0, n, bv, slot, gb, mu, ch, pp, rho);
+            if (active) {
+                double V[NV], mu2[NV];
+                load_cell<PH>(bv, slot, gb, V);
+                floors_adj<PH>(V, unpack_floors(fl, 1), rho);
+                mu2_of(mu2);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    mu2[v] += rho[v];
+                    rho[v] = c1 * rho[v];
+                }
+                store_cell<PH>(bl, slot, gb, mu2);
+                store_cell<PH>(bv, slot, gb, rho);
+            }
         }
-        double rho[NV];
-        adj_divergence<PH>(asm_, t, mp, mn, true, t, active, 0, n, 0, n, bv, slot, gb, mu, ch, pp, rho);
-        if (active) {
-            double V[NV], mu2[NV];
-            load_cell<PH>(bv, slot, gb, V);
-            floors_adj<PH>(V, unpack_floors(fl, 1), rho);
-            mu2_of(mu2);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                mu2[v] += rho[v];
-                rho[v] = c1 * rho[v];
-            }
-            store_cell<PH>(bl, slot, gb, mu2);
-            store_cell<PH>(bv, slot, gb, rho);
+        fence_proxy_async();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tma_store_4d(&t_lamacc, bl, c[0], c[1], c[2], c[3]);
+            tma_store_4d(&t_m1, bv, c[0], c[1], c[2], c[3]);
         }
     }
-    fence_proxy_async();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        tma_store_4d(&t_lamacc, bl, c[0], c[1], c[2], c[3]);
-        tma_store_4d(&t_m1, bv, c[0], c[1], c[2], c[3]);
-        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-    }
+    if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
-// Shared memory: boxes U, m1 and lam (in, then out), 2 NV n doubles each
-// (rounded up to 128 bytes), the four planes of the tile, the mbarrier.
+// Stage 1.  Buffer b holds the boxes U and m1 (inputs only); lam is updated in
+// place with plain loads and stores at the cell's offset, so a buffer is free
+// as soon as its tile is computed and the load of the tile after next goes
+// into it at once.  Shared memory as stage 2.
 template <class PH>
 __global__ void __launch_bounds__(256, 1) k_adj_staged1(const __grid_constant__ CUtensorMap t_uin,
-                                                        const __grid_constant__ CUtensorMap t_m1,
-                                                        const __grid_constant__ CUtensorMap t_lam, Geom g,
-                                                        PhysParams pp, const StepParams* __restrict__ sp, int dir,
+                                                        const __grid_constant__ CUtensorMap t_m1, Geom g,
+                                                        double* __restrict__ lam, PhysParams pp,
+                                                        const StepParams* __restrict__ sp, int dir,
                                                         unsigned* __restrict__ gstatus)
 {
     constexpr int NV = PH::NV;
     extern __shared__ __align__(128) double smem[];
     const int n = g.n_d;
     const int bd = adj_box_doubles(NV, n);
-    double* bv = smem;                  // U
-    double* bm = smem + bd;             // m1
-    double* bl = smem + 2 * bd;         // lam in, lam out
+    double* pl = smem + 4 * bd;
+    const AdjSmem asm_{pl, pl + NV * n, pl + 2 * NV * n, pl + 3 * NV * n, n};
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(pl + 4 * NV * n);
+    const int npair = (g.n1 + 1) / 2, ntiles = npair * g.n2, G = (int)gridDim.x;
+    const unsigned bytes = (unsigned)(2 * (2 * NV * n * sizeof(double)));
+    auto issue = [&](int tau, int b) {
+        int i1, j2, c[4];
+        adj_tile(g, dir, tau, npair, i1, j2, c);
+        mbar_expect_tx(bars + b, bytes);
+        tma_load_4d(smem + 2 * b * bd, &t_uin, c[0], c[1], c[2], c[3], bars + b);
+        tma_load_4d(smem + (2 * b + 1) * bd, &t_m1, c[0], c[1], c[2], c[3], bars + b);
+    };
+    adj_bars_init(bars);
+    if (threadIdx.x == 0) {
+        if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+        if ((int)blockIdx.x + G < ntiles) issue(blockIdx.x + G, 1);
+    }
+    Geom gb = g;
+    gb.plane = 2 * n;
+    const int st_t = dir == 0 ? 1 : 2, st_p = dir == 0 ? n : 1;
+    const int t = threadIdx.x;
+    const int mp = t == 0 ? n - 1 : t - 1, mn = t == n - 1 ? 0 : t + 1;
+    int k = 0;
+    for (int tau = blockIdx.x; tau < ntiles; tau += G, ++k) {
+        const int b = k & 1;
+        if (!adj_bar_wait(bars + b, (unsigned)((k >> 1) & 1))) {
+            if (threadIdx.x == 0) {
+                atomicOr(gstatus, ST_TIMEOUT);
+                // the other buffer's load (the next tile) may still be in
+                // flight: let it land (bounded) before the CTA's memory goes
+                if (tau + G < ntiles) {
+                    bool done = false;
+                    for (int it = 0; it < (1 << 24) && !done; ++it)
+                        done = mbar_try_wait(bars + (b ^ 1), (unsigned)(((k + 1) >> 1) & 1));
+                }
+            }
+            return;
+        }
+        const double* bv = smem + 2 * b * bd;            // U
+        const double* bm = bv + bd;                      // m1
+        int i1_0, i2, c[4];
+        adj_tile(g, dir, tau, npair, i1_0, i2, c);
+        const double ch = sp[g.seg_len ? i2 / g.seg_len : 0].ch;
+#pragma unroll 1
+        for (int p = 0; p < 2; ++p) {
+            if (i1_0 + p >= g.n1) break;
+            const bool active = t < n;
+            const int slot = active ? t * st_t + p * st_p : 0;
+            const long long goff = (long long)(g.g_d + (active ? t : 0)) * g.sd +
+                                   (long long)(g.g1 + i1_0 + p) * g.s1 + (long long)(g.g2 + i2) * g.s2;
+            double mu[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) mu[v] = 0.0;
+            if (active) load_cell<PH>(bm, slot, gb, mu);
+            double rho[NV];
+            adj_divergence<PH>(asm_, t, mp, mn, true, t, active, 0, n, 0, n, bv, slot, gb, mu, ch, pp, rho);
+            if (active) {
+                double l[NV];
+                load_cell<PH>(lam, goff, g, l);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) l[v] += rho[v];
+                store_cell<PH>(lam, goff, g, l);
+            }
+        }
+        __syncthreads();                                 // every thread is done with buffer b
+        if (threadIdx.x == 0 && tau + 2 * G < ntiles) {
+            fence_proxy_async();
+            issue(tau + 2 * G, b);
+        }
+    }
+}
+
+// Stage 1 with lam staged too, one tile per CTA (grid: x = pairs of pencils,
+// z = ortho-2): the boxes U, m1 and lam are loaded together, lam is updated in
+// its box and written back by a TMA store.  Used along y and z, where the
+// persistent kernel's plain lam accesses would touch one 8-byte row fragment
+// per thread; along x those accesses are contiguous and the persistent kernel
+// is faster.  Shared memory: three boxes, the four planes, one mbarrier.
+template <class PH>
+__global__ void __launch_bounds__(256, 1) k_adj_staged1_boxed(const __grid_constant__ CUtensorMap t_uin,
+                                                              const __grid_constant__ CUtensorMap t_m1,
+                                                              const __grid_constant__ CUtensorMap t_lam, Geom g,
+                                                              PhysParams pp, const StepParams* __restrict__ sp,
+                                                              int dir, unsigned* __restrict__ gstatus)
+{
+    constexpr int NV = PH::NV;
+    extern __shared__ __align__(128) double smem[];
+    const int n = g.n_d;
+    const int bd = adj_box_doubles(NV, n);
+    double* bv = smem;                                   // U
+    double* bm = smem + bd;                              // m1
+    double* bl = smem + 2 * bd;                          // lam in, lam out
     double* pl = smem + 3 * bd;
     const AdjSmem asm_{pl, pl + NV * n, pl + 2 * NV * n, pl + 3 * NV * n, n};
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(pl + 4 * NV * n);
-    const int i1_0 = 2 * blockIdx.x, i2 = blockIdx.z;
-    int c[4];
-    adj_box_coords(g, dir, i1_0, i2, c);
-    adj_bar_init(bar);
+    const int npair = (g.n1 + 1) / 2;
+    int i1_0, i2, c[4];
+    adj_tile(g, dir, (int)(blockIdx.z * npair + blockIdx.x), npair, i1_0, i2, c);
+    adj_bars_init(bar);                                  // (initialises bar and bar + 1; only bar is used)
     if (threadIdx.x == 0) {
         mbar_expect_tx(bar, (unsigned)(3 * (2 * NV * n * sizeof(double))));
         tma_load_4d(bv, &t_uin, c[0], c[1], c[2], c[3], bar);
         tma_load_4d(bm, &t_m1, c[0], c[1], c[2], c[3], bar);
         tma_load_4d(bl, &t_lam, c[0], c[1], c[2], c[3], bar);
     }
-    if (!adj_bar_wait(bar)) {
+    if (!adj_bar_wait(bar, 0)) {
         if (threadIdx.x == 0) atomicOr(gstatus, ST_TIMEOUT);
         return;
     }
@@ -481,11 +595,16 @@ __global__ void __launch_bounds__(256, 1) k_adj_staged1(const __grid_constant__ 
     }
 }
 
-// dynamic shared memory of the staged adjoint kernels (stage 2: two boxes,
-// stage 1: three) for nv planes and n cells, with the mbarrier
-inline size_t adj_staged_smem(int nv, int n, int stage)
+inline size_t adj_staged1_boxed_smem(int nv, int n)
 {
-    return ((size_t)(stage == 2 ? 2 : 3) * adj_box_doubles(nv, n) + (size_t)4 * nv * n) * sizeof(double) + 16;
+    return ((size_t)3 * adj_box_doubles(nv, n) + (size_t)4 * nv * n) * sizeof(double) + 16;
+}
+
+// dynamic shared memory of the staged adjoint kernels (two buffers of two
+// boxes, the four planes, two mbarriers) for nv planes and n cells
+inline size_t adj_staged_smem(int nv, int n)
+{
+    return ((size_t)4 * adj_box_doubles(nv, n) + (size_t)4 * nv * n) * sizeof(double) + 16;
 }
 
 }  // namespace pk

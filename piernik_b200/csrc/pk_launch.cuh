@@ -2,6 +2,8 @@
 // pk_phys_*.cu instantiates these for its PH, so the heavy kernels compile in
 // parallel translation units.
 #pragma once
+#include <algorithm>
+
 #include "pk_adjoint_kernels.cuh"
 #include "pk_aux.cuh"
 #include "pk_internal.h"
@@ -281,8 +283,11 @@ constexpr int NADJ_VARIANT = 6;
 constexpr int ADJ_VAR_STAGED = 5;
 constexpr int ADJ_T[NADJ_VARIANT] = {256, 256, 192, 128, 128, 256};
 // defaults, measured on B200 (MHD, 256^3, adjoint sweep = staged recording
-// sweep + the two adjoint kernels): the staged pair 11.2 / 13.8 / 14.5 ms
-// along x / y / z against 12.5 / 15.8 / 16.2 for the best tiled variant.
+// sweep + the two adjoint kernels): the staged pair 10.9 / 12.5 / 13.0 ms
+// along x / y / z against 12.5 / 15.8 / 16.2 for the best tiled variant
+// (persistent double-buffered stage 2 everywhere; stage 1 persistent along x,
+// one tile per CTA with lam staged along y and z: the persistent stage 1's
+// plain lam accesses there cost 14.5 / 14.8 ms).
 // Among the tiled variants (where the staged pair does not apply) the
 // unspilled 255-register variant 0 is the fastest or within 1 % of it on
 // every axis; the whole periodic pencil without halo beats 8 pencils x 26 + 6
@@ -336,6 +341,8 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
             }
             PK_CUDA(h, cudaFuncSetAttribute(k_adj_staged2<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
             PK_CUDA(h, cudaFuncSetAttribute(k_adj_staged1<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            PK_CUDA(h, cudaFuncSetAttribute(k_adj_staged1_boxed<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            220 * 1024));
             attr = true;
         }
         int var = (h->adjV[dir] >= 0 && h->adjV[dir] < NADJ_VARIANT) ? h->adjV[dir] : DEF_ADJ_V[dir];
@@ -350,15 +357,24 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
                     !encode_state_map(&m_uin, uin, b.n, b.ext, b.plane, PH::NV, dir))
                     return fail(h, PK_E_CUDA, "cuTensorMapEncodeTiled failed for the staged adjoint sweep");
                 const int threads = (b.n[dir] + 31) / 32 * 32;
-                const dim3 grid((g.n1 + 1) / 2, 1, g.n2);
+                // persistent: one CTA per SM over the tiles (pairs of pencils)
+                const long long ntiles = (long long)((g.n1 + 1) / 2) * g.n2;
+                const int ctas = (int)std::min<long long>(ntiles, sm_count());
+                const size_t smem = adj_staged_smem(PH::NV, b.n[dir]);
                 std::pair<cudaEvent_t, cudaEvent_t> ev;
                 if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
-                k_adj_staged2<PH><<<grid, threads, adj_staged_smem(PH::NV, b.n[dir], 2), h->stream>>>(
-                    m_ustar, m_lamout, m_lamin, m_m1, g, uout, flags, h->pp, b.dl[dir], h->d_step, apply_fac, dir,
-                    h->d_status);
+                k_adj_staged2<PH><<<ctas, threads, smem, h->stream>>>(m_ustar, m_lamout, m_lamin, m_m1, g, uout,
+                                                                      flags, h->pp, b.dl[dir], h->d_step,
+                                                                      apply_fac, dir, h->d_status);
                 PK_CUDA(h, cudaGetLastError());
-                k_adj_staged1<PH><<<grid, threads, adj_staged_smem(PH::NV, b.n[dir], 1), h->stream>>>(
-                    m_uin, m_m1, m_lamin, g, h->pp, h->d_step, dir, h->d_status);
+                if (dir == 0) {
+                    k_adj_staged1<PH><<<ctas, threads, smem, h->stream>>>(m_uin, m_m1, g, lam_in, h->pp, h->d_step,
+                                                                          dir, h->d_status);
+                } else {
+                    const dim3 grid((g.n1 + 1) / 2, 1, g.n2);
+                    k_adj_staged1_boxed<PH><<<grid, threads, adj_staged1_boxed_smem(PH::NV, b.n[dir]), h->stream>>>(
+                        m_uin, m_m1, m_lamin, g, h->pp, h->d_step, dir, h->d_status);
+                }
                 PK_CUDA(h, cudaGetLastError());
                 if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
                 h->launches += 2;
