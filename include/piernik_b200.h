@@ -238,6 +238,15 @@ int pk_set_arithmetic(pk_handle h, int32_t mode);
  * launch-bound variant (-1 keeps the current one). */
 int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant);
 
+/* Refined domains (sweeps.F90:218-262, the finer level's boundary fluxes
+ * replacing the coarser level's within each RK stage): one_launch = 1 sweeps
+ * every level of a stage in one persistent launch whose work list holds the
+ * levels' pencil tiles and the flux restriction between them, ordered so that
+ * an item waits only for items listed before it; 0 (the default, about 3 %
+ * faster on B200 for the 515-block three-level layout) launches level by
+ * level with a restriction launch between.  Results are identical. */
+int pk_set_refined_launch(pk_handle h, int32_t one_launch);
+
 /* Replay the sweeps of a step (fluid_update) as one captured CUDA graph; the
  * step scalars (dt, chspeed, glmdamping factor) are read by the kernels from
  * device memory, so one capture serves every step. */

@@ -30,7 +30,7 @@ EXPORTS = (
     "pk_upload", "pk_download", "pk_solve_cg", "pk_fill_guards", "pk_sweep", "pk_glm_damp",
     "pk_timestep_raw", "pk_time_step", "pk_fluid_update", "pk_run", "pk_get_time_state",
     "pk_set_time_state", "pk_status", "pk_sync", "pk_set_tile", "pk_stream", "pk_profile_enable",
-    "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_use_graph", "pk_set_arithmetic",
+    "pk_profile_read", "pk_tile_variants", "pk_set_batch", "pk_set_refined_launch", "pk_use_graph", "pk_set_arithmetic",
     "pk_upload_device", "pk_download_device", "pk_adjoint_set", "pk_adjoint_get", "pk_adjoint_sweep",
     "pk_grad_forward", "pk_grad_backward", "pk_grad_release",
     "pk_timestep_raw_noalloc", "pk_set_adjoint_tile", "pk_set_domain", "pk_block_place",
@@ -160,6 +160,7 @@ def load(path: str = LIBPATH):
     L.pk_set_tile.argtypes = [H, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.pk_tile_variants.argtypes = [C.POINTER(C.c_int32)] * 3
     L.pk_set_batch.argtypes = [H, C.c_int32, C.c_int32, C.c_int32]
+    L.pk_set_refined_launch.argtypes = [H, C.c_int32]
     L.pk_use_graph.argtypes = [H, C.c_int32]
     L.pk_set_arithmetic.argtypes = [H, C.c_int32]
     L.pk_set_instances.argtypes = [H, C.c_int32]

@@ -662,6 +662,75 @@ int ensure_pingpong(pk_ctx* h)
 }
 
 // block tables (both parities) and per-direction work lists of the batched sweep
+// The one-launch work list of a refined stage along dir (k_stage_refined):
+// first every stage item of a block without replaced fluxes, finest level
+// first; then per coarse level, finest first, the restriction chunks of its in
+// slots (each waits for all stage items of the level above) and the stage
+// items of its blocks with replaced fluxes (each waits for all of those
+// chunks).  Every item comes after all items it waits for.
+int build_refined_list(pk_ctx* h, int dir, const std::vector<std::vector<StageItem>>& items, int maxl)
+{
+    constexpr int CHUNK = 64;                         // in slots per restriction chunk
+    const int nlev = maxl + 1;
+    auto dependent = [&](int blk) { return h->blocks[blk].fc[dir].in_slot != nullptr; };
+    auto stage_item = [&](const StageItem& w, int level, int wait, int count) {
+        RefItem r{};
+        r.kind = 0;
+        r.block = w.block;
+        r.i1_0 = w.i1_0;
+        r.P = w.P;
+        r.level = level;
+        r.wait = wait;
+        r.wait_count = count;
+        r.fence = h->blocks[w.block].fc[dir].out_slot != nullptr;
+        return r;
+    };
+    std::vector<RefItem> ri;
+    for (int L = maxl; L >= 0; --L)
+        for (const StageItem& w : items[L])
+            if (!dependent(w.block)) ri.push_back(stage_item(w, L, -1, 0));
+    for (int L = maxl; L >= 1; --L) {
+        const int cl = L - 1;
+        int nchunk = 0;
+        if (h->d_src[dir] && (int)h->in_level_beg[dir].size() > L) {
+            const int beg = h->in_level_beg[dir][cl], end = h->in_level_beg[dir][L];
+            for (int s0 = beg; s0 < end; s0 += CHUNK) {
+                RefItem r{};
+                r.kind = 1;
+                r.level = cl;
+                r.beg = s0;
+                r.end = std::min(s0 + CHUNK, end);
+                r.wait = 1 + L;                       // every stage item of level L done
+                r.wait_count = (int)items[L].size();
+                r.fence = 1;
+                ri.push_back(r);
+                ++nchunk;
+            }
+        }
+        for (const StageItem& w : items[cl])
+            if (dependent(w.block)) ri.push_back(stage_item(w, cl, nchunk ? 1 + nlev + cl : -1, nchunk));
+    }
+    size_t smem = 0;
+    for (const StageList& sl : h->sbatch[dir]) smem = std::max(smem, sl.smem);
+    cudaFree(h->rdev[dir]);
+    h->rdev[dir] = nullptr;
+    h->rn[dir] = (int)ri.size();
+    h->rsmem[dir] = smem;
+    if (!ri.empty()) {
+        PK_CUDA(h, cudaMalloc(&h->rdev[dir], sizeof(RefItem) * ri.size()));
+        PK_CUDA(h, cudaMemcpyAsync(h->rdev[dir], ri.data(), sizeof(RefItem) * ri.size(), cudaMemcpyHostToDevice,
+                                   h->stream));
+        PK_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    if (h->rcount_n < 1 + 2 * nlev) {
+        cudaFree(h->d_rcount);
+        h->d_rcount = nullptr;
+        h->rcount_n = 1 + 2 * nlev;
+        PK_CUDA(h, cudaMalloc(&h->d_rcount, sizeof(unsigned) * h->rcount_n));
+    }
+    return PK_OK;
+}
+
 int build_batch(pk_ctx* h)
 {
     if (int rc = ensure_pingpong(h)) return rc;
@@ -734,6 +803,9 @@ int build_batch(pk_ctx* h)
     for (int dir = 0; dir < 3; ++dir) {
         for (StageList& s : h->sbatch[dir]) cudaFree(s.dev);
         h->sbatch[dir].assign(maxl + 1, StageList());
+        cudaFree(h->rdev[dir]);
+        h->rdev[dir] = nullptr;
+        h->rn[dir] = 0;
         if (!h->stage_batched) continue;
         items.assign(maxl + 1, {});
         const int o1 = ORTHO1[dir], o2 = ORTHO2[dir];
@@ -757,6 +829,8 @@ int build_batch(pk_ctx* h)
                                        h->stream));
             PK_CUDA(h, cudaStreamSynchronize(h->stream));
         }
+        if (maxl > 0)
+            if (int rc = build_refined_list(h, dir, items, maxl)) return rc;
     }
     PK_CUDA(h, cudaStreamSynchronize(h->stream));   // host vectors of the tables may change after return
     h->batch_dirty = false;
@@ -860,10 +934,13 @@ int sweep_impl(pk_ctx* h, int dir, double dt, double ch, int apply_fac, double f
     if (int rc = exchange_prepare(h)) return rc;       // a refined domain's couplings
     if (h->blocks.size() > 1)
         if (int rc = build_batch(h)) return rc;
+    const bool one_launch = h->stage_batched && h->max_level > 0 && h->refined_one_launch && h->rn[dir] > 0;
     for (int s = 1; s <= nst; ++s) {
         const double rk = (h->cfg.integration_order == 1) ? 1.0 : (s == 1 ? 0.5 : 1.0);
         // finest level first: its boundary fluxes replace the coarser level's (sweeps.F90:218-262)
-        for (int L = h->max_level; L >= 0; --L) {
+        if (one_launch)
+            if (int rc = ops->stage_refined(h, dir, s == 1, rk)) return rc;
+        for (int L = one_launch ? -1 : h->max_level; L >= 0; --L) {
             if (h->stage_batched) {
                 if (int rc = ops->stage_batched(h, dir, L, s == 1, rk)) return rc;
             } else {
@@ -1165,7 +1242,9 @@ int pk_destroy(pk_handle h)
     for (int d = 0; d < 3; ++d) {
         cudaFree(h->batch[d].dev);
         for (StageList& s : h->sbatch[d]) cudaFree(s.dev);
+        cudaFree(h->rdev[d]);
     }
+    cudaFree(h->d_rcount);
     for (double* p : h->grad_ckpt) cudaFree(p);
     for (double* p : h->grad_pool) cudaFree(p);
     for (double* p : h->grad_star) cudaFree(p);
@@ -2194,6 +2273,14 @@ int pk_set_batch(pk_handle h, int32_t enable, int32_t length, int32_t variant)
     h->batch_variant = v;
     h->batch_L = L;
     h->batch_dirty = true;
+    invalidate_graph(h);
+    return PK_OK;
+}
+
+int pk_set_refined_launch(pk_handle h, int32_t one_launch)
+{
+    if (!h) return PK_E_ARG;
+    h->refined_one_launch = one_launch != 0;
     invalidate_graph(h);
     return PK_OK;
 }

@@ -131,6 +131,14 @@ struct pk_ctx {
     pk::BatchList batch[3];
     std::vector<pk::StageList> sbatch[3];       // batched stage per direction, per level
     bool stage_batched = false;                 // every block's pencils fit one stage CTA
+    // refined domains: every level's stage items and the restriction chunks
+    // between them as one work list per direction (k_stage_refined)
+    pk::RefItem* rdev[3] = {nullptr, nullptr, nullptr};
+    int rn[3] = {0, 0, 0};
+    size_t rsmem[3] = {0, 0, 0};
+    unsigned* d_rcount = nullptr;               // its counters (1 + 2 levels), zeroed before each launch
+    int rcount_n = 0;
+    bool refined_one_launch = false;            // pk_set_refined_launch
     int stage_variant = 0;                      // launch-bound variant of k_stage_batched (SV_T / SV_B)
     pk::FcArgs* d_fcargs[3] = {nullptr, nullptr, nullptr};   // per block flux couplings (refined domains)
     pk_time_state ts;
@@ -236,6 +244,7 @@ struct PhysOps {
     int (*fused)(pk_ctx* h, Block& b, int dir, int apply_fac);
     int (*stage)(pk_ctx* h, Block& b, int dir, int first, double rk);           // dt, ch from d_step
     int (*stage_batched)(pk_ctx* h, int dir, int level, int first, double rk);  // all blocks of a level
+    int (*stage_refined)(pk_ctx* h, int dir, int first, double rk);             // all levels, one launch
     int (*batched)(pk_ctx* h, int dir, int apply_fac, unsigned* counter);
     int (*fused_ptr)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out);
     int (*fused_rec)(pk_ctx* h, Block& b, int dir, int apply_fac, const double* in, double* out, double* ustar,

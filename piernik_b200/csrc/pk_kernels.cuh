@@ -177,7 +177,7 @@ PK_DEV void rk_stage(const Smem& sm, int me, int mp, int mn, const Roles& r, dou
     if constexpr (FC) {
         if (r.flux && fc_in) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = fc_in[v];
+            for (int v = 0; v < NV; ++v) sm.Q[v * PT + me] = __ldcg(fc_in + v);
         }
         if (r.flux && fc_out) {
 #pragma unroll
@@ -559,6 +559,139 @@ __global__ void __launch_bounds__(MAXT, MINB) k_stage_batched(const BlockDesc* _
     double* u = const_cast<double*>(b.in);
     stage_tile<PH, W3, FC>(g, tl, w.i1_0, b.g[dir] - 2, w.i2, u, u, b.uh, pp, first, dtodx, spar->ch, fc, smem, status,
                            true, true);
+    flush_status(status, gstatus);
+}
+
+// -------------------------------------------------------------------------
+// One RK stage of every block of a refined domain along dir in ONE persistent
+// launch (sweeps.F90:218-262: the finer level's boundary fluxes replace the
+// coarser level's; the per-level launches do level by level with a
+// restriction launch between).  CTAs (occupancy x SMs of them) take work
+// items in list order from counters[0]: stage items (P pencils of one block,
+// as k_stage_batched) and restriction chunks (in slots [beg, end) of one
+// coarse level, as k_restrict_flux).  An item that needs earlier work waits
+// until a completion counter reaches its count: a restriction chunk of
+// coarse level L-1 for every stage item of level L, a stage item of a block
+// with replaced fluxes for every restriction chunk of its level.  The host
+// lists every item after all items it waits for, so the earliest unfinished
+// item never waits and the launch cannot deadlock while its CTAs are
+// resident; the wait is bounded all the same (PK_ST_TIMEOUT after about 4 s,
+// the item skipped).  Producers fence their global writes before counting;
+// consumers read the replaced and the fine fluxes with L1-bypassing loads.
+// Counters: [0] next item, [1 + L] stage items of level L done, [1 + nlev +
+// L] restriction chunks for coarse level L done (zeroed before each launch).
+// -------------------------------------------------------------------------
+struct RefItem {
+    int kind;                 // 0 stage item, 1 restriction chunk
+    int block, i1_0, P;       // stage item
+    int level;                // stage: the block's level; restriction: the coarse level of its slots
+    int beg, end;             // restriction: in slots [beg, end)
+    int wait;                 // counter to wait on, -1 none
+    int wait_count;           // ... until it reaches this
+    int fence;                // 1: other items read what it writes (boundary or restricted fluxes)
+};
+
+struct RefArgs {
+    const int* src;           // 4 fine out slots per in slot (k_restrict_flux's table), -1 none
+    const double* out_flux;   // fine boundary fluxes, NV per out slot
+    double* in_flux;          // restricted fluxes, NV per in slot
+    double scale;             // 1 / 2^(dim-1)
+    int nlev;                 // levels
+};
+
+template <class PH, int MAXT, int MINB, bool W3 = false>
+__global__ void __launch_bounds__(MAXT, MINB) k_stage_refined(const BlockDesc* __restrict__ blocks,
+                                                       const RefItem* __restrict__ items, int nitems, int dir,
+                                                       PhysParams pp, int first, double rk,
+                                                       const StepParams* __restrict__ spar,
+                                                       const FcArgs* __restrict__ fcs, RefArgs ra,
+                                                       unsigned* __restrict__ counters, unsigned* __restrict__ gstatus)
+{
+    extern __shared__ double smem[];
+    __shared__ int s_item, s_ok;
+    constexpr int NV = PH::NV;
+    unsigned status = 0;
+    const int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;
+    // thread 0 claims the next item while the current one runs (an item only
+    // waits for items listed before it, so holding a claim cannot block them)
+    int claim = threadIdx.x == 0 ? (int)atomicAdd(counters, 1u) : 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int idx = claim;
+            if (idx < nitems) claim = (int)atomicAdd(counters, 1u);
+            int ok = 1;
+            if (idx < nitems) {
+                const int wt = items[idx].wait, wc = items[idx].wait_count;
+                if (wt >= 0) {
+                    const volatile unsigned* c = counters + wt;
+                    for (long long spin = 0; *c < (unsigned)wc; ++spin) {
+                        if (spin > (1LL << 26)) {
+                            ok = 0;
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                    __threadfence();
+                }
+            }
+            s_item = idx;
+            s_ok = ok;
+        }
+        __syncthreads();
+        const int idx = s_item;
+        if (idx >= nitems) break;
+        if (!s_ok) {
+            status |= 4u;                                  // PK_ST_TIMEOUT
+            break;
+        }
+        const RefItem it = items[idx];
+        if (it.kind == 0) {
+            const BlockDesc b = blocks[it.block];
+            Geom g;
+            const long long st3[3] = {1, b.ext[0], (long long)b.ext[0] * b.ext[1]};
+            g.plane = b.plane;
+            g.sd = st3[dir];
+            g.s1 = st3[o1];
+            g.s2 = st3[o2];
+            g.ext_d = b.ext[dir];
+            g.n_d = b.n[dir];
+            g.g_d = b.g[dir];
+            g.n1 = b.n[o1];
+            g.g1 = b.g[o1];
+            g.n2 = b.n[o2];
+            g.g2 = b.g[o2];
+            g.perm[0] = dir;                               // iarr_swp: (x,y,z) (y,x,z) (z,y,x)
+            g.perm[1] = dir == 1 ? 0 : 1;
+            g.perm[2] = dir == 2 ? 0 : 2;
+            Tile tl;
+            tl.P = it.P;
+            tl.T = b.n[dir] + 4;                           // [g-2, g+n+2): the interior updates' stencil
+            tl.L = tl.T;
+            tl.halo = 0;
+            tl.xfast = dir == 0;
+            const double dtodx = (rk * spar->dt) / b.dl[dir];
+            const FcArgs fc = fcs ? fcs[it.block] : FcArgs{};
+            double* u = const_cast<double*>(b.in);
+            stage_tile<PH, W3, true>(g, tl, it.i1_0, b.g[dir] - 2, 0, u, u, b.uh, pp, first, dtodx, spar->ch, fc,
+                                     smem, status, true, true);
+        } else {
+            const long long n = (long long)(it.end - it.beg) * NV;
+            for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+                const int slot = it.beg + (int)(t / NV);
+                const int v = (int)(t % NV);
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int sfine = ra.src[4 * slot + q];
+                    if (sfine >= 0) acc = acc + __ldcg(ra.out_flux + (long long)sfine * NV + v);
+                }
+                ra.in_flux[(long long)slot * NV + v] = ra.scale * acc;
+            }
+        }
+        if (it.fence) __threadfence();                     // this CTA's writes before its count
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(counters + 1 + (it.kind == 0 ? 0 : ra.nlev) + it.level, 1u);
+    }
     flush_status(status, gstatus);
 }
 

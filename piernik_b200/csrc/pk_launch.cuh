@@ -90,6 +90,19 @@ auto stage_batched_variant(int v, bool w3, bool fc) -> decltype(&k_stage_batched
     }
 }
 
+// the one-launch refined stage kernel of launch-bound variant v (SV_T / SV_B)
+template <class PH>
+auto stage_refined_variant(int v, bool w3) -> decltype(&k_stage_refined<PH, 320, 1, false>)
+{
+    if (w3) return k_stage_refined<PH, 320, 1, true>;
+    switch (v) {
+    case 1: return k_stage_refined<PH, 128, 3, false>;
+    case 2: return k_stage_refined<PH, 192, 2, false>;
+    case 3: return k_stage_refined<PH, 384, 1, false>;
+    default: return k_stage_refined<PH, 320, 1, false>;
+    }
+}
+
 template <class PH>
 int set_smem_attr(pk_ctx* h)
 {
@@ -111,6 +124,10 @@ int set_smem_attr(pk_ctx* h)
                 for (int fc = 0; fc < 2; ++fc)
                     PK_CUDA(h, cudaFuncSetAttribute(stage_batched_variant<PH>(v, w3, fc),
                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        for (int v = 0; v < NSTAGE_VARIANT; ++v)
+            for (int w3 = 0; w3 < 2; ++w3)
+                PK_CUDA(h, cudaFuncSetAttribute(stage_refined_variant<PH>(v, w3),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         done = true;
     }
     return PK_OK;
@@ -523,6 +540,39 @@ int launch_stage_batched(pk_ctx* h, int dir, int level, int first, double rk)
     return PK_OK;
 }
 
+// One stage of every level of a refined domain along dir in one persistent
+// launch (k_stage_refined): as many CTAs as can be resident, at most one per
+// work item; its counters are zeroed on the stream first.
+template <class PH>
+int launch_stage_refined(pk_ctx* h, int dir, int first, double rk)
+{
+    const int n = h->rn[dir];
+    if (!n) return PK_OK;
+    if (int rc = set_smem_attr<PH>(h)) return rc;
+    const int v = h->pp.weno3 ? 0 : h->stage_variant;
+    auto* kern = stage_refined_variant<PH>(v, h->pp.weno3);
+    const size_t smem = h->rsmem[dir];
+    int per_sm = 0;
+    PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SV_T[v], smem));
+    if (per_sm < 1) return fail(h, PK_E_CUDA, "the refined stage kernel does not fit an SM");
+    const int ctas = std::min(n, per_sm * sm_count());
+    RefArgs ra;
+    ra.src = h->d_src[dir];
+    ra.out_flux = h->d_out_flux[dir];
+    ra.in_flux = h->d_in_flux[dir];
+    ra.scale = h->fc_scale;
+    ra.nlev = h->max_level + 1;
+    PK_CUDA(h, cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned) * h->rcount_n, h->stream));
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
+    kern<<<ctas, SV_T[v], smem, h->stream>>>(h->d_desc[h->cur], h->rdev[dir], n, dir, h->pp, first, rk, h->d_step,
+                                             h->d_fcargs[dir], ra, h->d_rcount, h->d_status);
+    PK_CUDA(h, cudaGetLastError());
+    if (int rc = ev_end(h, ev)) return fail(h, rc, "cudaEventRecord failed");
+    h->launches += 1;
+    return PK_OK;
+}
+
 // the face fluxes of one direction for the unsplit scheme (k_unsplit_flux),
 // tiles as the stage kernel's
 template <class PH>
@@ -597,7 +647,7 @@ template <class PH>
 const PhysOps* make_ops()
 {
     static PhysOps o{PH::NV, set_smem_attr<PH>, launch_fused<PH>, launch_stage<PH>, launch_stage_batched<PH>,
-                     launch_batched<PH>, launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>,
+                     launch_stage_refined<PH>, launch_batched<PH>, launch_fused_ptr<PH>, launch_fused_rec<PH>, launch_adj<PH>,
                      launch_unsplit_flux<PH>, launch_unsplit_apply<PH>};
     return &o;
 }

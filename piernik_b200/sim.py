@@ -243,6 +243,11 @@ class Simulation:
         """Replay each step's sweeps as a captured CUDA graph."""
         self._chk(self.lib.pk_use_graph(self.h, int(enable)), "pk_use_graph")
 
+    def set_refined_launch(self, one_launch: bool = True) -> None:
+        """Refined domains: sweep every level of an RK stage in one persistent
+        launch, or level by level (the default)."""
+        self._chk(self.lib.pk_set_refined_launch(self.h, int(one_launch)), "pk_set_refined_launch")
+
     # -- independent instances stacked along z -------------------------------
     def set_instances(self, count: int) -> None:
         """Run ``count`` independent periodic problems, stacked along z in the

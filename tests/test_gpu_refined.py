@@ -91,6 +91,30 @@ def test_refined_matches_oracle(gpu_lib, name):
     sim.close()
 
 
+@pytest.mark.parametrize("name", ["mhd-3d-moncen", "hd-3d", "mhd-2d", "mhd-3d-moncen+graph"])
+def test_refined_one_launch_equals_per_level(gpu_lib, name):
+    """The one-launch refined stage (every level's tiles and the flux
+    restriction between them in one persistent work list, pk_set_refined_launch)
+    against the default level-by-level launches: 3 steps, every block bit for
+    bit, guard cells included, and no bounded wait gave up."""
+    from piernik_b200._lib import PK_ST_TIMEOUT
+    graph = name.endswith("+graph")
+    c = CASES[name.split("+")[0]]
+    blocks = case(**c)
+    out = []
+    for one in (False, True):
+        sim = library(c["dom"], blocks, graph=graph)
+        sim.set_refined_launch(one)
+        sim.run(3)
+        assert not sim.status() & PK_ST_TIMEOUT
+        out.append([sim.download(block=i) for i in range(len(blocks))])
+        sim.close()
+    for i, (ref, got) in enumerate(zip(*out)):
+        for k, (x, y) in enumerate(zip(ref, got)):
+            if x is not None:
+                assert_bitexact(y, x, f"{name}: array {k} of block {i}")
+
+
 def test_refined_three_fluids_blast(gpu_lib):
     """Ion MHD + neutral + dust with an off-centre blast across all levels."""
     fl = [("ion", 5.0 / 3.0), ("neu", 1.4), ("dst", -1.0)]
