@@ -374,10 +374,16 @@ int launch_adj(pk_ctx* h, Block& b, int dir, int apply_fac, const double* uin, c
                     !encode_state_map(&m_uin, uin, b.n, b.ext, b.plane, PH::NV, dir))
                     return fail(h, PK_E_CUDA, "cuTensorMapEncodeTiled failed for the staged adjoint sweep");
                 const int threads = (b.n[dir] + 31) / 32 * 32;
-                // persistent: one CTA per SM over the tiles (pairs of pencils)
+                // persistent: as many CTAs as can be resident (one per SM at
+                // 256 threads, more for shorter pencils), over the tiles (pairs of pencils)
                 const long long ntiles = (long long)((g.n1 + 1) / 2) * g.n2;
-                const int ctas = (int)std::min<long long>(ntiles, sm_count());
                 const size_t smem = adj_staged_smem(PH::NV, b.n[dir]);
+                int per_sm = 0;
+                PK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                               &per_sm, dir == 0 ? (const void*)k_adj_staged1<PH> : (const void*)k_adj_staged2<PH>,
+                               threads, smem));
+                if (per_sm < 1) per_sm = 1;
+                const int ctas = (int)std::min<long long>(ntiles, (long long)per_sm * sm_count());
                 std::pair<cudaEvent_t, cudaEvent_t> ev;
                 if (int rc = ev_begin(h, &ev)) return fail(h, rc, "cudaEventRecord failed");
                 k_adj_staged2<PH><<<ctas, threads, smem, h->stream>>>(m_ustar, m_lamout, m_lamin, m_m1, g, uout,
