@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PK_ABI_VERSION 5
+#define PK_ABI_VERSION 6
 
 enum {
     PK_OK = 0,
@@ -95,6 +95,15 @@ typedef struct pk_config {
      * cells of point_chspeed (hdc.F90:118-131,197-268), reduced over ranks
      * with MAX (one device reduction per step) */
     int32_t ch_grid;
+    /* use_eglm (global.F90:109, default .false. :252): the E-GLM sources of
+     * hdc.F90:355-457 after each triple of sweeps, before the psi damping --
+     * on the ionized fluid, m -= dt divB B, B -= dt divB v, E -= dt (divB v.B
+     * - B.grad psi), psi -= dt v.grad psi, with divB and grad psi of order 2
+     * from the cells' neighbours (the guard cells refreshed around them).
+     * RIEMANN_SPLIT only (the reference stops otherwise, hdc.F90:388), and
+     * here on single-level domains without stacked instances, outside the
+     * differentiable path (ABI version 6) */
+    int32_t use_eglm;
 } pk_config;
 
 #define PK_SOLVER_SPLIT   0

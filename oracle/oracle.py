@@ -56,6 +56,7 @@ class OCfg(C.Structure):
         ("interpolation", C.c_int),
         ("w_epsilon", C.c_double),
         ("solver", C.c_int),
+        ("use_eglm", C.c_int),
     ]
 
 
@@ -125,6 +126,7 @@ def lib():
         L.o_glm_fac.argtypes = [P, B, C.c_double, C.c_double]
         L.o_glm_fac.restype = C.c_double
         L.o_glm_apply.argtypes = [P, B, C.c_double]
+        L.o_eglm.argtypes = [P, B, C.c_double]
         L.o_chspeed.argtypes = [P, B, C.c_double]
         L.o_chspeed.restype = C.c_double
         L.o_timestep_raw.argtypes = [P, B, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -179,6 +181,7 @@ def make_cfg(setup) -> OCfg:
     c.interpolation = {"linear": 0, "weno3": 1}[setup.interpolation]
     c.w_epsilon = setup.w_epsilon
     c.solver = {"split": 0, "unsplit": 1}[setup.solver]
+    c.use_eglm = int(getattr(setup, "use_eglm", False))
     return c
 
 
@@ -226,6 +229,11 @@ class OracleBlock:
 
     def sweep(self, cdim, dt, ch):
         return lib().o_sweep(C.byref(self.cfg), C.byref(self.blk), cdim, dt, ch)
+
+    def eglm(self, dt):
+        """E-GLM sources for dt and the boundary update (a no-op unless the
+        setup has use_eglm)."""
+        lib().o_eglm(C.byref(self.cfg), C.byref(self.blk), dt)
 
     def timestep_raw(self):
         dt, c = C.c_double(), C.c_double()

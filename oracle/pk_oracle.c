@@ -991,6 +991,72 @@ void o_glm_apply(const o_cfg *cfg, o_block *blk, double fac)
     for (size_t i = 0; i < nc; ++i) blk->psi[i] = blk->psi[i] * fac;   /* :338 */
 }
 
+/* E-GLM sources (hdc.F90:355-457, Dedner et al. 2002 Eq. 38), applied after
+ * each triple of sweeps before glmdamping (fluidupdate.F90:229-230) when
+ * use_eglm (off by default, global.F90:252), to the ionized fluid only:
+ *   divB   the cell-centred second-order divergence, divB(order 2) with
+ *          coeff_c(1) = 1/2 (divB.F90:146-249, sixpoint :297-338):
+ *          1/2 * (dBx/dx + dBy/dy + dBz/dz) from the +-1 neighbours, a
+ *          collapsed direction contributing (b - b)/dl = 0;
+ *   gp     grad(psi) = half * [psi(i+1) - psi(i-1), ...] / dl (:396-401),
+ *          all computed before any cell changes (":don't fuse these loops");
+ * then per interior cell, each line using the previous lines' results
+ * (:414-432): m -= dt*divB*B; B -= dt*divB*(m/rho); e -= dt*(divB*(m/rho).B
+ * - B.gp); psi -= dt*(m/rho).gp, dot_product accumulating from zero; then
+ * the fluid, psi and B boundaries (:439-445). */
+void o_eglm(const o_cfg *cfg, o_block *blk, double dt)
+{
+    if (!cfg->use_eglm || !cfg->magnetic) return;
+    o_lay L;
+    o_layout(cfg, &L);
+    int ion = -1;
+    for (int f = 0; f < L.nfl; ++f)
+        if (L.kind[f] == O_ION) ion = f;
+    int ext[3], g[3];
+    o_extents(blk, ext, g);
+    const size_t cst[3] = {1, (size_t)ext[0], (size_t)ext[0] * ext[1]};
+    const size_t nc = (size_t)ext[0] * ext[1] * ext[2];
+    const int nv = L.nv;
+    int D[3];
+    for (int d = 0; d < 3; ++d) D[d] = blk->n[d] > 1 ? 1 : 0;      /* dom%D_x, D_y, D_z */
+    double *w = (double *)calloc(4 * nc, sizeof(double));       /* divB, gp (x, y, z) */
+    for (int k = g[2]; k < g[2] + blk->n[2]; ++k)
+        for (int j = g[1]; j < g[1] + blk->n[1]; ++j)
+            for (int i = g[0]; i < g[0] + blk->n[0]; ++i) {
+                const size_t s = (size_t)i + (size_t)j * cst[1] + (size_t)k * cst[2];
+                double t[3];
+                for (int d = 0; d < 3; ++d) {
+                    const size_t sp = s + (size_t)D[d] * cst[d], sm = s - (size_t)D[d] * cst[d];
+                    t[d] = (blk->b[sp * 3 + d] - blk->b[sm * 3 + d]) / blk->dl[d];
+                    w[4 * s + 1 + d] = (0.5 * (blk->psi[sp] - blk->psi[sm])) / blk->dl[d];
+                }
+                w[4 * s] = 0.5 * ((t[0] + t[1]) + t[2]);
+            }
+    if (ion >= 0) {
+        const int idn = L.idn[ion], imx = L.imx[ion], ien = L.ien[ion];
+        for (int k = g[2]; k < g[2] + blk->n[2]; ++k)
+            for (int j = g[1]; j < g[1] + blk->n[1]; ++j)
+                for (int i = g[0]; i < g[0] + blk->n[0]; ++i) {
+                    const size_t s = (size_t)i + (size_t)j * cst[1] + (size_t)k * cst[2];
+                    double *u = blk->u + s * nv, *bb = blk->b + s * 3;
+                    const double q = w[4 * s], *gp = w + 4 * s + 1;
+                    for (int c = 0; c < 3; ++c) u[imx + c] = u[imx + c] - (dt * q) * bb[c];
+                    double v[3];
+                    for (int c = 0; c < 3; ++c) v[c] = u[imx + c] / u[idn];
+                    for (int c = 0; c < 3; ++c) bb[c] = bb[c] - (dt * q) * v[c];
+                    if (L.has_en[ion]) {
+                        const double vb = ((0.0 + v[0] * bb[0]) + v[1] * bb[1]) + v[2] * bb[2];
+                        const double bg = ((0.0 + bb[0] * gp[0]) + bb[1] * gp[1]) + bb[2] * gp[2];
+                        u[ien] = u[ien] - dt * (q * vb - bg);
+                    }
+                    const double vg = ((0.0 + v[0] * gp[0]) + v[1] * gp[1]) + v[2] * gp[2];
+                    blk->psi[s] = blk->psi[s] - dt * vg;
+                }
+    }
+    free(w);
+    o_fill_guards(cfg, blk);
+}
+
 /* sound speeds: ion_cs (fluids/ionized/initionized.F90:89-145), neu_cs
  * (fluids/neutral/initneutral.F90:82-109), dust_cs (fluids/dust/initdust.F90:74-87) */
 static double o_get_cs(const o_cfg *cfg, const o_lay *L, int f, const double *u, const double *b)
@@ -1119,6 +1185,7 @@ int o_fluid_update(const o_cfg *cfg, o_block *blk, o_state *st)
             if (cfg->skip_sweep[d] || blk->n[d] <= 1) continue;
             if ((rc = o_sweep(cfg, blk, d, dt, st->chspeed))) return rc;
         }
+        o_eglm(cfg, blk, dt);                               /* eglm (:229) */
         if (cfg->magnetic) o_glm_apply(cfg, blk, o_glm_fac(cfg, blk, dt, st->chspeed));   /* glmdamping */
     }
     return 0;
@@ -1345,6 +1412,7 @@ int o_fluid_update_multi(const o_cfg *cfg, o_block *const *blks, int nb, o_state
                 for (int i = 0; i < nb; ++i) o_fill_guards(cfg, blks[i]);
             }
         }
+        for (int i = 0; i < nb; ++i) o_eglm(cfg, blks[i], dt);
         if (cfg->magnetic)
             for (int i = 0; i < nb; ++i) o_glm_apply(cfg, blks[i], fac);
     }

@@ -59,6 +59,7 @@ typedef struct o_cfg {
     int interpolation;           /* 0 linear, 1 weno3 (interpol_str, global.F90:220) */
     double w_epsilon;            /* global.F90:255 */
     int solver;                  /* 0 RIEMANN_SPLIT, 1 RIEMANN_UNSPLIT (solver_str, global.F90:423-437) */
+    int use_eglm;                /* E-GLM sources after each triple of sweeps (global.F90:109,252; hdc.F90:355-457) */
 } o_cfg;
 
 #define O_CFL_NONE 0
@@ -124,6 +125,8 @@ int    o_unsplit_stage(const o_cfg *cfg, o_block *blk, int istep, double dt, dou
 int    o_unsplit_sweep(const o_cfg *cfg, o_block *blk, double dt, double ch);
 int    o_fluid_update_unsplit(const o_cfg *cfg, o_block *blk, o_state *st);
 void   o_glm_apply(const o_cfg *cfg, o_block *blk, double fac);
+/* E-GLM sources of one block for dt (hdc.F90:eglm), then its boundary update */
+void   o_eglm(const o_cfg *cfg, o_block *blk, double dt);
 /* update_chspeed with ch_grid (hdc.F90:90-140) */
 double o_chspeed(const o_cfg *cfg, const o_block *blk, double dt);
 /* timestep_fluid over all fluids, before clamps (timestep.F90:431-495) */

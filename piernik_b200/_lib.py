@@ -83,6 +83,7 @@ class PkConfig(C.Structure):
         ("ord_fluid_prolong", C.c_int32),
         ("ord_mag_prolong", C.c_int32),
         ("ch_grid", C.c_int32),
+        ("use_eglm", C.c_int32),
     ]
 
 

@@ -49,6 +49,7 @@ class Setup:
     dt_max: float = DBL_HUGE
     cflcontrol: str = "none"         # the reference defaults to 'redo' (:218); 'none' keeps parity runs unforked
     ch_grid: bool = True             # :254 (psi speed from the grid; False: from the gas, hdc.F90:118-131)
+    use_eglm: bool = False           # :252 (E-GLM sources after each triple of sweeps, hdc.F90:355-457)
     cfl_max: float = 0.9             # :233
     dt_shrink: float = 0.5           # :245
     max_redostep_attempts: int = 10  # :258

@@ -724,6 +724,7 @@ int build_refined_list(pk_ctx* h, int dir, const std::vector<std::vector<StageIt
     }
     if (h->rcount_n < 1 + 2 * nlev) {
         cudaFree(h->d_rcount);
+    cudaFree(h->d_eglm);
         h->d_rcount = nullptr;
         h->rcount_n = 1 + 2 * nlev;
         PK_CUDA(h, cudaMalloc(&h->d_rcount, sizeof(unsigned) * h->rcount_n));
@@ -1000,18 +1001,89 @@ void step_dirs(pk_ctx* h, int* dirs, int* nd)
 }
 
 // the launches of fluid_update_full after the step scalars are on the device
+// E-GLM scratch for the largest block (outside any graph capture)
+int eglm_alloc(pk_ctx* h)
+{
+    if (!(h->cfg.use_eglm && h->cfg.magnetic)) return PK_OK;
+    long long mp = 0;
+    for (auto& b : h->blocks) mp = std::max(mp, b.plane);
+    if (mp <= h->eglm_plane) return PK_OK;
+    cudaFree(h->d_eglm);
+    h->d_eglm = nullptr;
+    h->eglm_plane = 0;
+    if (cudaMalloc(&h->d_eglm, sizeof(double) * 4 * mp) != cudaSuccess)
+        return fail(h, PK_E_NOMEM, "cudaMalloc for the E-GLM scratch failed");
+    h->eglm_plane = mp;
+    return PK_OK;
+}
+
+// every guard cell of every block from the current state (the reference's
+// boundary updates at the end of each sweep and of eglm)
+int refresh_all(pk_ctx* h)
+{
+    if (h->connected) return refresh_guards(h, h->blocks[0]);
+    for (auto& b : h->blocks)
+        if (int rc = fill_guards_block(h, b)) return rc;
+    return PK_OK;
+}
+
+// eglm (hdc.F90:355-457) on every block: guards refreshed, divB and grad(psi)
+// of all interior cells, the sources, the boundary update; dt from d_step
+int eglm_dev(pk_ctx* h)
+{
+    if (h->max_level > 0) return fail(h, PK_E_UNSUPPORTED, "use_eglm on refined domains");
+    if (h->ninst > 1) return fail(h, PK_E_UNSUPPORTED, "use_eglm with stacked instances");
+    if (int rc = eglm_alloc(h)) return rc;
+    if (int rc = refresh_all(h)) return rc;
+    int idn = -1, off = 0;
+    for (int f = 0; f < h->cfg.nfluids; ++f) {
+        if (h->cfg.fluid_kind[f] == PK_FLUID_ION && idn < 0) idn = off;
+        off += h->cfg.fluid_kind[f] == PK_FLUID_DST ? 4 : 5;
+    }
+    if (idn >= 0) {
+        for (auto& b : h->blocks) {
+            EglmArgs a;
+            for (int d = 0; d < 3; ++d) {
+                a.n[d] = b.n[d];
+                a.g[d] = b.g[d];
+                a.ext[d] = b.ext[d];
+                a.D[d] = b.n[d] > 1 ? 1 : 0;
+                a.dl[d] = b.dl[d];
+            }
+            a.plane = b.plane;
+            a.ib = h->ib;
+            a.idn = idn;
+            const long long cells = (long long)b.n[0] * b.n[1] * b.n[2];
+            k_eglm_grad<<<grid1d(cells, 256), 256, 0, h->stream>>>(state(h, b), h->d_eglm, a);
+            PK_CUDA(h, cudaGetLastError());
+            k_eglm_apply<<<grid1d(cells, 256), 256, 0, h->stream>>>(state(h, b), h->d_eglm, a, h->d_step);
+            PK_CUDA(h, cudaGetLastError());
+            h->launches += 2;
+        }
+    }
+    return refresh_all(h);
+}
+
 int step_sweeps(pk_ctx* h, double dt, double ch, double fac)
 {
     int dirs[3], nd;
     step_dirs(h, dirs, &nd);
+    // use_eglm: eglm runs between the triple's last sweep and glmdamping
+    // (fluidupdate.F90:229-230), so the damping is not fused into that sweep
+    const bool eglm = h->cfg.use_eglm && h->cfg.magnetic;
     for (int half = 0; half < 2; ++half) {
         for (int s = 0; s < nd; ++s) {
             const int d = half == 0 ? dirs[s] : dirs[nd - 1 - s];
-            const int last = h->cfg.magnetic && s == nd - 1;
+            const int last = h->cfg.magnetic && s == nd - 1 && !eglm;
             int next = -1;                                // the sweep after this one in the same step
             if (half == 0) next = s + 1 < nd ? dirs[s + 1] : dirs[nd - 1];
             else if (s + 1 < nd) next = dirs[nd - 2 - s];
             if (int rc = sweep_impl(h, d, dt, ch, last, fac, next)) return rc;
+        }
+        if (eglm) {
+            if (int rc = eglm_dev(h)) return rc;
+            if (nd > 0)
+                if (int rc = glm_scale_dev(h)) return rc;
         }
         if (h->cfg.magnetic && nd == 0)
             if (int rc = glm_scale(h, fac)) return rc;
@@ -1146,14 +1218,16 @@ void pk_config_default(pk_config* c)
     c->ord_mag_prolong = 2;               // O_I2 (:259)
     c->w_epsilon = 1.0e-10;            // :255
     c->ch_grid = 1;                    // :254
+    c->use_eglm = 0;                   // :252
 }
 
 int pk_create(const pk_config* cfg, pk_handle* out)
 {
     if (cfg && (cfg->cflcontrol < PK_CFL_NONE || cfg->cflcontrol > PK_CFL_AUTO || cfg->max_redostep_attempts < 0 ||
-                cfg->ch_grid < 0 || cfg->ch_grid > 1 ||
+                cfg->ch_grid < 0 || cfg->ch_grid > 1 || cfg->use_eglm < 0 || cfg->use_eglm > 1 ||
                 cfg->interpolation < PK_INTERP_LINEAR || cfg->interpolation > PK_INTERP_WENO3 ||
-                cfg->solver < PK_SOLVER_SPLIT || cfg->solver > PK_SOLVER_UNSPLIT))
+                cfg->solver < PK_SOLVER_SPLIT || cfg->solver > PK_SOLVER_UNSPLIT ||
+                (cfg->use_eglm && cfg->solver != PK_SOLVER_SPLIT)))   // hdc.F90:388: eglm needs RIEMANN_SPLIT
         return PK_E_ARG;
     if (!cfg || !out) return PK_E_ARG;
     *out = nullptr;
@@ -1245,6 +1319,7 @@ int pk_destroy(pk_handle h)
         cudaFree(h->rdev[d]);
     }
     cudaFree(h->d_rcount);
+    cudaFree(h->d_eglm);
     for (double* p : h->grad_ckpt) cudaFree(p);
     for (double* p : h->grad_pool) cudaFree(p);
     for (double* p : h->grad_star) cudaFree(p);
@@ -1829,6 +1904,7 @@ static int run_step_sweeps(pk_ctx* h, double dt, double ch, double fac)
         if (int rc = ensure_pingpong(h)) return rc;
         for (auto& b : h->blocks)
             if (!b.uh && !fused_ok(h)) PK_CUDA(h, cudaMalloc(&b.uh, sizeof(double) * h->nplanes * b.plane));
+        if (int rc = eglm_alloc(h)) return rc;
         if (!h->graph_exec) {
             // capture the sweeps of one step once; the step scalars are read from d_step
             const int cur0 = h->cur;
@@ -2357,6 +2433,7 @@ int grad_check(pk_ctx* h)
         return fail(h, PK_E_UNSUPPORTED, "the differentiable path runs on one block of one rank");
     if (!fused_ok(h)) return fail(h, PK_E_UNSUPPORTED, "the differentiable path needs RK2 and periodic boundaries");
     if (h->cfg.nfluids != 1) return fail(h, PK_E_UNSUPPORTED, "the differentiable path is built for one fluid");
+    if (h->cfg.use_eglm) return fail(h, PK_E_UNSUPPORTED, "the differentiable path has no E-GLM sources");
     if (h->cfg.interpolation != PK_INTERP_LINEAR)
         return fail(h, PK_E_UNSUPPORTED, "the differentiable path differentiates the linear (limited) reconstruction");
     int dirs[3], nd;

@@ -454,6 +454,93 @@ static __global__ void k_copy_pencils(BoxGeom b, int dir, const double* __restri
 // The fine->coarse flux sum of send_cg_coarsebnd (fc_fluxes.F90:213-225): each
 // coarse face takes 0 + the fine faces' fluxes in the reference's loop order
 // (ORTHO1 outer, ORTHO2 inner), times 1 / 2**(eff_dim - 1).
+// ---------------------------------------------------------------------------
+// E-GLM sources (hdc.F90:355-457; use_eglm, off by default, global.F90:252),
+// applied after each triple of sweeps, before glmdamping, to the ionized
+// fluid of one block whose guard cells are current.  k_eglm_grad stores, for
+// every interior cell, divB of order 2 (divB.F90:146-249: coeff_c(1) = 1/2
+// times the sum over directions of (b(+1) - b(-1)) / dl, sixpoint :297-338)
+// and grad(psi) = (1/2 (psi(+1) - psi(-1))) / dl (:396-401) in w (4 planes of
+// the block's plane size) before any cell changes; k_eglm_apply then updates
+// each interior cell in the reference's statement order (:414-432), every
+// line using the previous lines' results:
+//   m -= (dt divB) B;  B -= (dt divB) (m/rho);
+//   E -= dt (divB (m/rho).B - B.grad(psi));  psi -= dt (m/rho).grad(psi)
+// with dot products accumulated from zero as dot_product does.  A direction
+// of extent 1 (D = 0) contributes (b - b) / dl = 0.
+// ---------------------------------------------------------------------------
+struct EglmArgs {
+    int n[3], g[3], ext[3];
+    int D[3];               // 1 where the direction has more than one cell (dom%D_x, D_y, D_z)
+    long long plane;
+    double dl[3];
+    int ib;                 // first B plane; psi is plane ib + 3
+    int idn;                // the ionized fluid's density plane (momenta idn+1..3, energy idn+4); -1 none
+};
+
+PK_DEV long long eglm_cell(const EglmArgs& a, long long c)
+{
+    const int i = (int)(c % a.n[0]) + a.g[0];
+    const long long r = c / a.n[0];
+    const int j = (int)(r % a.n[1]) + a.g[1];
+    const int k = (int)(r / a.n[1]) + a.g[2];
+    return (long long)i + (long long)j * a.ext[0] + (long long)k * a.ext[0] * a.ext[1];
+}
+
+static __global__ void k_eglm_grad(const double* __restrict__ u, double* __restrict__ w, EglmArgs a)
+{
+    const long long ncell = (long long)a.n[0] * a.n[1] * a.n[2];
+    const long long st[3] = {1, a.ext[0], (long long)a.ext[0] * a.ext[1]};
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const long long s = eglm_cell(a, c);
+        double t[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const long long sp = s + a.D[d] * st[d], sm = s - a.D[d] * st[d];
+            const double* bd = u + (long long)(a.ib + d) * a.plane;
+            const double* ps = u + (long long)(a.ib + 3) * a.plane;
+            t[d] = (bd[sp] - bd[sm]) / a.dl[d];
+            w[(long long)(1 + d) * a.plane + s] = (0.5 * (ps[sp] - ps[sm])) / a.dl[d];
+        }
+        w[s] = 0.5 * ((t[0] + t[1]) + t[2]);
+    }
+}
+
+static __global__ void k_eglm_apply(double* __restrict__ u, const double* __restrict__ w, EglmArgs a,
+                                    const StepParams* __restrict__ sp)
+{
+    const double dt = sp->dt;
+    const long long ncell = (long long)a.n[0] * a.n[1] * a.n[2];
+    const long long P = a.plane;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const long long s = eglm_cell(a, c);
+        const double q = w[s], dq = dt * q;
+        const double gp[3] = {w[P + s], w[2 * P + s], w[3 * P + s]};
+        const double rho = u[(long long)a.idn * P + s];
+        double m[3], B[3], v[3];
+#pragma unroll
+        for (int c3 = 0; c3 < 3; ++c3) {
+            m[c3] = u[(long long)(a.idn + 1 + c3) * P + s] - dq * u[(long long)(a.ib + c3) * P + s];
+            v[c3] = m[c3] / rho;
+            B[c3] = u[(long long)(a.ib + c3) * P + s] - dq * v[c3];
+        }
+        const double vb = ((0.0 + v[0] * B[0]) + v[1] * B[1]) + v[2] * B[2];
+        const double bg = ((0.0 + B[0] * gp[0]) + B[1] * gp[1]) + B[2] * gp[2];
+        const double vg = ((0.0 + v[0] * gp[0]) + v[1] * gp[1]) + v[2] * gp[2];
+        double* e = u + (long long)(a.idn + 4) * P + s;
+        *e = *e - dt * (q * vb - bg);
+        double* ps = u + (long long)(a.ib + 3) * P + s;
+        *ps = *ps - dt * vg;
+#pragma unroll
+        for (int c3 = 0; c3 < 3; ++c3) {
+            u[(long long)(a.idn + 1 + c3) * P + s] = m[c3];
+            u[(long long)(a.ib + c3) * P + s] = B[c3];
+        }
+    }
+}
+
 static __global__ void k_restrict_flux(const int* __restrict__ src, int beg, int end, int nv,
                                        const double* __restrict__ out_flux, double* __restrict__ in_flux, double scale)
 {

@@ -139,6 +139,8 @@ struct pk_ctx {
     unsigned* d_rcount = nullptr;               // its counters (1 + 2 levels), zeroed before each launch
     int rcount_n = 0;
     bool refined_one_launch = false;            // pk_set_refined_launch
+    double* d_eglm = nullptr;                   // E-GLM scratch: divB and grad(psi), 4 planes of the largest block
+    long long eglm_plane = 0;
     int stage_variant = 0;                      // launch-bound variant of k_stage_batched (SV_T / SV_B)
     pk::FcArgs* d_fcargs[3] = {nullptr, nullptr, nullptr};   // per block flux couplings (refined domains)
     pk_time_state ts;

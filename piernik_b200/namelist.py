@@ -158,7 +158,7 @@ def read_problem_par(text: str, cmdline: Optional[str] = None, setup: Optional[S
                 "dt_max", "cfl_max", "dt_shrink"):
         if key in ns:
             kw[key] = float(ns[key])
-    for key in ("use_smalld", "use_smallei", "disallow_negatives", "ch_grid"):
+    for key in ("use_smalld", "use_smallei", "disallow_negatives", "ch_grid", "use_eglm"):
         if key in ns:
             kw[key] = bool(ns[key])
     if "limiter" in ns:

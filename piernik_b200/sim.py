@@ -74,6 +74,7 @@ def make_config(setup: Setup) -> L.PkConfig:
     c.ord_fluid_prolong = setup.ord_fluid_prolong
     c.ord_mag_prolong = setup.ord_mag_prolong
     c.ch_grid = int(setup.ch_grid)
+    c.use_eglm = int(setup.use_eglm)
     return c
 
 

@@ -121,7 +121,7 @@ def test_library_builds_and_exports():
     for name in _header_symbols():
         assert hasattr(lib, name), name
     lib.pk_abi_version.restype = ctypes.c_int
-    assert lib.pk_abi_version() == 5
+    assert lib.pk_abi_version() == 6
     cfg = L.PkConfig()
     lib.pk_config_default(ctypes.byref(cfg))
     assert cfg.cfl == 0.7 and cfg.glm_alpha == 0.1 and cfg.nb == 4 and cfg.integration_order == 2
