@@ -52,6 +52,13 @@ def test_namelist_cmdline_override():
     assert s.cfl == 0.5 and s.limiter == "moncen" and s.limiter_b == "vanleer"
 
 
+def test_namelist_logical_switches():
+    s = read_problem_par(SEDOV_PAR, fluids=["neu"])
+    assert s.use_eglm is False and s.ch_grid is True                 # global.F90:252, :254
+    s = read_problem_par(SEDOV_PAR, cmdline="&NUMERICAL_SETUP use_eglm=.true., ch_grid=.false./", fluids=["neu"])
+    assert s.use_eglm is True and s.ch_grid is False
+
+
 def test_namelist_rejects_other_solvers():
     with pytest.raises(ValueError):
         read_problem_par("&NUMERICAL_SETUP solver_str='rtvd' /")
