@@ -30,6 +30,29 @@ def test_cpaw_oracle_known_answer(oracle_lib, res):
     assert f"{problems.cpaw_error(s, ob.b, ini):.8f}" == KNOWN[res]
 
 
+@pytest.mark.parametrize("lim", ["vanleer", "moncen"])
+def test_cpaw_split_scheme_converges(oracle_lib, lim):
+    """The split sweep (the benchmarked path: HLLD + GLM with the named
+    limiter) on the same wave, for which the reference tabulates no error:
+    second-order convergence of the L2 error of B over one period (measured
+    ratios 9.8 (vanleer) and 10.7 (moncen) from 32 x 16 to 128 x 64), and at
+    128 x 64 an error of the size of the reference's unsplit known answer
+    (vanleer 0.000986 against 0.00102726; moncen 0.000581)."""
+    errs = {}
+    for res in [(32, 16), (64, 32), (128, 64)]:
+        s, u, b, psi, ini = problems.cpaw(*res)
+        s = s.replace(solver="split", limiter=lim, limiter_b=lim)
+        ob = oracle.OracleBlock(s, u, b, psi)
+        ob.fill_guards()
+        assert ob.run(100000) == 0
+        assert abs(ob.state.t - s.tend) <= 1e-12 * s.tend
+        errs[res] = problems.cpaw_error(s, ob.b, ini)
+    e = [errs[r] for r in sorted(errs)]
+    assert e[0] > e[1] > e[2], errs
+    assert e[0] / e[2] > 8.0, errs
+    assert 0.5 < e[2] / float(KNOWN[(128, 64)]) < 1.5, errs
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("res", [(128, 64), (256, 128)])
 def test_cpaw_library_known_answer(gpu_lib, res):
