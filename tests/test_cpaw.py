@@ -30,18 +30,20 @@ def test_cpaw_oracle_known_answer(oracle_lib, res):
     assert f"{problems.cpaw_error(s, ob.b, ini):.8f}" == KNOWN[res]
 
 
-@pytest.mark.parametrize("lim", ["vanleer", "moncen"])
+@pytest.mark.parametrize("lim", ["vanleer", "moncen", "weno3"])
 def test_cpaw_split_scheme_converges(oracle_lib, lim):
     """The split sweep (the benchmarked path: HLLD + GLM with the named
-    limiter) on the same wave, for which the reference tabulates no error:
-    second-order convergence of the L2 error of B over one period (measured
-    ratios 9.8 (vanleer) and 10.7 (moncen) from 32 x 16 to 128 x 64), and at
-    128 x 64 an error of the size of the reference's unsplit known answer
-    (vanleer 0.000986 against 0.00102726; moncen 0.000581)."""
+    limiter, or interpol_str = 'weno3') on the same wave, for which the
+    reference tabulates no error: second-order convergence of the L2 error
+    of B over one period (measured ratios 9.8 (vanleer), 10.7 (moncen) and
+    10.6 (weno3) from 32 x 16 to 128 x 64), and at 128 x 64 an error of the
+    size of the reference's unsplit known answer (vanleer 0.000986, weno3
+    0.000954 against 0.00102726; moncen 0.000581)."""
     errs = {}
     for res in [(32, 16), (64, 32), (128, 64)]:
         s, u, b, psi, ini = problems.cpaw(*res)
-        s = s.replace(solver="split", limiter=lim, limiter_b=lim)
+        s = (s.replace(solver="split", interpolation="weno3") if lim == "weno3"
+             else s.replace(solver="split", limiter=lim, limiter_b=lim))
         ob = oracle.OracleBlock(s, u, b, psi)
         ob.fill_guards()
         assert ob.run(100000) == 0
