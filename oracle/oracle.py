@@ -2,9 +2,13 @@
 
 Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
 import this module.  It drives ``liboracle.so`` (oracle/pk_oracle.c), a C
-restatement of PIERNIK's RIEMANN_SPLIT sweep whose parity with the Fortran
-reference is UNPINNED (no Fortran compiler here, no golden vectors in the
-reference for this path); see pk_oracle.h.
+restatement of PIERNIK's RIEMANN_SPLIT sweep.  No Fortran compiler exists
+here, so it cannot be run against the reference itself; it is pinned by the
+reference's own known answers instead (the CPAW test's tabulated L2 errors,
+reproduced to the 8 printed decimals, tests/test_cpaw.py) and, where the
+reference holds none, by exact solutions (tests/test_exact_riemann_cpu.py,
+tests/test_stationary_discontinuities_cpu.py, tests/test_dust_advection_cpu.py);
+see pk_oracle.h.
 
 Arrays use the reference's guard-cell layout:
 ``u[k, j, i, v]`` (= Fortran ``cg%u(v, i, j, k)``), ``b[k, j, i, d]``,

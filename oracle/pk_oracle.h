@@ -17,7 +17,10 @@
  * reference sources operation by operation (evaluation order, Fortran
  * intrinsics spacing/sign/min/max, the -0.0 normalisation done by
  * internal_sources) and is cross-checked by physics properties in tests/
- * (conservation, axis-permutation symmetry).
+ * (conservation, axis-permutation symmetry) and exact solutions (Sod's shock
+ * tube for HLLC with every limiter, stationary contacts and tangential
+ * discontinuities for HLLC / HLLD, dust advection, second-order convergence
+ * of the split sweep on the CPAW wave).
  *
  * Layout mirrors the reference's named arrays with guard cells:
  *   u  (nvar, i, j, k)  -> u[((k*NY + j)*NX + i)*nvar + v]   (cg%u, cg%w(uh))
